@@ -1,0 +1,158 @@
+/*
+ * maple_b200 — C ABI of the B200-native inverse-homogenization inner loop.
+ *
+ * Every entry point takes plain pointers and sizes (device pointers unless a
+ * name says "host"), enqueues its work on the caller's CUDA stream and returns
+ * an int status (MAPLE_OK = 0).  On failure maple_last_error_string() returns a
+ * thread-local message.  Per-cell solver outcomes are returned in arrays and
+ * never raised, so one bad cell does not abort a batch.
+ *
+ * Layouts: a batch holds B periodic cells of r^3 voxels; element / node id is
+ * x*r*r + y*r + z.  Design variables, densities and sensitivities are [B][N]
+ * FP64; solution fields are [B][N][R][D] FP64 (R load cases of D components).
+ *
+ * Each declaration names the reference interface (xing-yuu/MAPLE, paths under
+ * src/maple/core) whose role it takes over.
+ */
+#ifndef MAPLE_B200_H
+#define MAPLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct maple_ctx maple_ctx;
+typedef void* maple_stream_t; /* cudaStream_t */
+
+enum {
+  MAPLE_OK = 0,
+  MAPLE_E_BADARG = 1,
+  MAPLE_E_CUDA = 2,
+  MAPLE_E_NOT_CONVERGED = 3,
+  MAPLE_E_BREAKDOWN = 4,
+  MAPLE_E_TIMEOUT = 5,
+  MAPLE_E_NOMEM = 6
+};
+
+enum { MAPLE_ELASTIC = 0, MAPLE_THERMAL = 1 };
+enum { MAPLE_FP64 = 0, MAPLE_MIXED = 1 };
+
+/* Per-cell solver status bits (maple_solve status_out). */
+enum { MAPLE_CELL_CONVERGED = 1, MAPLE_CELL_BREAKDOWN = 2, MAPLE_CELL_MAXIT = 4 };
+
+const char* maple_last_error_string(void);
+int maple_version(void);
+
+/* Element tables for a voxel of edge 1/r (FP64, host memory).
+ * Replaces utils/_utils.py:39-48 isotropic_elastic_tensor,
+ * utils/_utils.py:49-109 hexahedron and utils/_utils.py:116-196
+ * hexahedron_scalar.  Ke3 24x24, Fe3 24x6, X03 24x6, Ke1 8x8, Fe1 8x3,
+ * X01 8x3, all row-major.  C has the float32 entries of the reference. */
+int maple_element_matrices(int r, double E, double nu, double kappa, double* Ke3_host, double* Fe3_host,
+                           double* X03_host, double* Ke1_host, double* Fe1_host, double* X01_host);
+
+/* Context: B cells of r^3 voxels, `levels` multigrid levels (0 = automatic:
+ * coarsen until the coarsest grid is 4^3).  All device workspace is allocated
+ * here and on first use of a precision; no allocation happens inside solves.
+ * Replaces the per-call hierarchy build of utils/EBE_GMG.py:790-849 and
+ * utils/EBE_GMG_scalar.py:650-698, and the IHD module state of
+ * utils/model.py:12-32. */
+int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double kappa, maple_ctx** out);
+int maple_ctx_destroy(maple_ctx* ctx);
+int maple_ctx_info(const maple_ctx* ctx, int* levels_out, int* coarsest_n_out, size_t* bytes_out);
+
+/* Solver tuning (defaults: chebyshev degree 2, interval ratio 10, 12 power
+ * iterations, inner FP32 tolerance 1e-5, convergence check every iteration). */
+int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio, int power_iters, double inner_rtol,
+                             int check_every);
+
+/* Per-cell active mask (host int[B], nonzero = active). Inactive cells are
+ * skipped by every kernel.  NULL = all active. */
+int maple_set_active(maple_ctx* ctx, const int* active_host, maple_stream_t stream);
+
+/* Load element densities rho [B][N] (FP64 device) and build the operator
+ * hierarchy of one physics: Galerkin coarse element matrices
+ * (utils/EBE_GMG.py:226-337, utils/EBE_GMG_scalar.py:135-230), node stencils,
+ * Chebyshev bounds and the FP64 coarsest inverse.  `precision` selects which
+ * operator copies are built (MAPLE_FP64 or MAPLE_MIXED). */
+int maple_set_density(maple_ctx* ctx, int physics, const double* rho, int precision, maple_stream_t stream);
+
+/* Solve K(rho) u = F(rho) for all R load cases of all cells by MG-PCG
+ * (plain FP64, or FP32 PCG inside FP64 iterative refinement).  `warm` = 1
+ * starts from the previous solution of this physics, 0 from zero.  Replaces
+ * utils/EBE_GMG.py:758-885 GMGSolver.solve (and the scalar
+ * utils/EBE_GMG_scalar.py:617-725) as called by utils/model.py:111-124 and
+ * 140-152.  iters_out/status_out: host int[B] (nullable). */
+int maple_solve(maple_ctx* ctx, int physics, int precision, double rtol, int maxit, int warm, int* iters_out_host,
+                int* status_out_host, maple_stream_t stream);
+
+/* Solve with a caller-provided RHS F [B][N][R][D] and initial guess x0
+ * (nullable) on the density of the last maple_set_density: the
+ * GMGSolver.solve(fine_ke, global_f, ...) surface of utils/EBE_GMG.py:758.
+ * The solution is written to u_out [B][N][R][D] and the final residual
+ * F - K u to r_out (nullable). */
+int maple_solve_rhs(maple_ctx* ctx, int physics, int precision, const double* F, const double* x0, double rtol,
+                    int maxit, double* u_out, double* r_out, int* iters_out_host, int* status_out_host,
+                    maple_stream_t stream);
+
+/* Copy the current solution [B][N][R][D] of a physics into u_out. */
+int maple_get_solution(maple_ctx* ctx, int physics, double* u_out, maple_stream_t stream);
+
+/* Homogenized tensor H [B][R][R] = sum_e (X0-u_e)^T rho_e Ke0 (X0-u_e) and the
+ * per-element energies kept for maple_sensitivity.  Replaces
+ * utils/model.py:33-44 homogenized_batch_3d and 47-95
+ * homogenized_batch_thermal.  energy_out [B][N][R][R] (nullable) receives a
+ * copy of the per-element energies. */
+int maple_homogenize(maple_ctx* ctx, int physics, double* H_out, double* energy_out, maple_stream_t stream);
+
+/* out[b][e] (+)= sum_{r,s} g[b][r][s] * energy[b][e][r][s]: the contraction of
+ * saved per-element energies [B][N][RR] (RR = R*R) with dJ/dH [B][RR]; the
+ * backward pass of the homogenization (main_IHD_v3.py:688).  accumulate != 0
+ * adds to out. */
+int maple_energy_contract(int ncells, int N, int RR, const double* energy, const double* g, int accumulate,
+                          double* out, maple_stream_t stream);
+
+/* dJ/drho_e = sum_ij gC_ij dC_ij/drho_e + sum_ij gK_ij dkappa_ij/drho_e from
+ * the energies of the last homogenization (the analytic adjoint of the
+ * autograd call at main_IHD_v3.py:688).  gC [B][6][6], gK [B][3][3] (either
+ * nullable), dJdrho [B][N]. */
+int maple_sensitivity(maple_ctx* ctx, const double* gC, const double* gK, double* dJdrho, maple_stream_t stream);
+
+/* RHS assembly F = sum_e rho_e Fe0 [B][N][R][D] (utils/_utils.py:453-507,
+ * assemble_F_fast / assemble_F_fast_scalar). */
+int maple_assemble_rhs(maple_ctx* ctx, int physics, const double* rho, double* F_out, maple_stream_t stream);
+
+/* y = K(rho) u on the fine level, FP64 (utils/EBE_GMG.py:412-430
+ * EBEOperator.matvec with Ke_e = rho_e Ke0). */
+int maple_matvec(maple_ctx* ctx, int physics, const double* rho, const double* u, double* y, maple_stream_t stream);
+
+/* Periodic k^3 box filter of [B][N] (main_IHD_v3.py:342-359). */
+int maple_box_filter(int r, int ncells, int k, const double* in, double* out, maple_stream_t stream);
+
+/* OC update: 60 bisection steps on lambda in [1e-12, 1e6] per cell
+ * (main_IHD_v3.py:362-380).  volfrac [B] device, xnew [B][N]; stats [B][2]
+ * = (max|dx|, mean|dx|) (nullable). */
+int maple_oc_update(maple_ctx* ctx, const double* x, const double* dJdx, const double* volfrac, double move, double xmin,
+                    double* xnew, double* stats, maple_stream_t stream);
+
+/* One full OC iteration on device for every active cell (main_IHD_v3.py:
+ * 620-716 with symmetry "none" and no manufacturing penalties): SIMP map,
+ * both solves (as needed by the weights), C^H / kappa^H, objective
+ * J = wE*E + wG*G + wK*trace(kappa) (utils/objective.py:11-41, 180-251),
+ * analytic sensitivities, k^3 sensitivity filter and OC update.
+ * x [B][N] in, x_next [B][N] out; weights [B][3] and volfrac [B] device.
+ * Per-cell outputs (device, nullable): J [B], terms [B][3] (E, G, trace k),
+ * CH [B][6][6], kappa [B][3][3], stats [B][2] (max|dx|, mean|dx|). */
+int maple_oc_step(maple_ctx* ctx, const double* x, const double* weights, const double* volfrac, double penal,
+                  double rho_min, double move, double xmin, int filter_k, int precision, double rtol, int maxit,
+                  int warm, double* x_next, double* J, double* terms, double* CH, double* kappa, double* stats,
+                  int* iters_out_host, maple_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAPLE_B200_H */

@@ -1,0 +1,86 @@
+"""ctypes binding of ``libmaple_b200.so`` (the C ABI of include/maple_b200.h).
+
+The library is mandatory: there is no CPU or PyTorch fallback for any compute
+entry point.  Loading fails loudly with the reason when the shared object is
+missing or does not load.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libmaple_b200.so")
+
+MAPLE_OK = 0
+ELASTIC, THERMAL = 0, 1
+FP64, MIXED = 0, 1
+CELL_CONVERGED, CELL_BREAKDOWN, CELL_MAXIT = 1, 2, 4
+
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+_IP = C.POINTER(C.c_int)
+_DP = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes); must match include/maple_b200.h
+SIGNATURES = {
+    "maple_last_error_string": (C.c_char_p, []),
+    "maple_version": (_I, []),
+    "maple_element_matrices": (_I, [_I, _D, _D, _D, _DP, _DP, _DP, _DP, _DP, _DP]),
+    "maple_ctx_create": (_I, [_I, _I, _I, _D, _D, _D, C.POINTER(_P)]),
+    "maple_ctx_destroy": (_I, [_P]),
+    "maple_ctx_info": (_I, [_P, _IP, _IP, C.POINTER(C.c_size_t)]),
+    "maple_set_solver_options": (_I, [_P, _I, _D, _I, _D, _I]),
+    "maple_set_active": (_I, [_P, _IP, _P]),
+    "maple_set_density": (_I, [_P, _I, _P, _I, _P]),
+    "maple_solve": (_I, [_P, _I, _I, _D, _I, _I, _IP, _IP, _P]),
+    "maple_solve_rhs": (_I, [_P, _I, _I, _P, _P, _D, _I, _P, _P, _IP, _IP, _P]),
+    "maple_get_solution": (_I, [_P, _I, _P, _P]),
+    "maple_homogenize": (_I, [_P, _I, _P, _P, _P]),
+    "maple_energy_contract": (_I, [_I, _I, _I, _P, _P, _I, _P, _P]),
+    "maple_sensitivity": (_I, [_P, _P, _P, _P, _P]),
+    "maple_assemble_rhs": (_I, [_P, _I, _P, _P, _P]),
+    "maple_matvec": (_I, [_P, _I, _P, _P, _P, _P]),
+    "maple_box_filter": (_I, [_I, _I, _I, _P, _P, _P]),
+    "maple_oc_update": (_I, [_P, _P, _P, _P, _D, _D, _P, _P, _P]),
+    "maple_oc_step": (_I, [_P, _P, _P, _P, _D, _D, _D, _D, _I, _I, _D, _I, _I, _P, _P, _P, _P, _P, _P, _IP, _P]),
+}
+
+_lib = None
+
+
+class MapleError(RuntimeError):
+    """Error status returned by the maple_b200 C ABI."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"maple_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library (once) and declare every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            f"maple_b200 CUDA library not found at {path}; build it with "
+            "`python -m maple_b200._build` (there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != MAPLE_OK:
+        msg = load().maple_last_error_string()
+        raise MapleError(status, msg.decode() if msg else "")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args))

@@ -1,0 +1,1284 @@
+// sm_100a kernels for the periodic voxel homogenization path.
+//
+// Data layout (one "cell" = one periodic r^3 unit cell; B cells per context):
+//   * element / node id  x*n*n + y*n + z (maple/core/main_IHD_v3.py:175-186)
+//   * vectors: [cell][node][rhs][comp]  (DOF-interleaved, all load cases of a
+//     node contiguous: 18 values elastic, 3 thermal)
+//   * coarse stencils: [cell][27][D*D][node]  (node fastest: coalesced)
+//   * element matrices of coarse levels: [cell][elem][8D][8D]  (FP64)
+// The element stiffness of the fine level lives in __constant__ memory for a
+// voxel of edge 1; every kernel multiplies by the context's scale factor.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <utility>
+
+namespace maple {
+
+constexpr int kThreads = 256;
+
+__constant__ double c_Ke3d[576];
+__constant__ float c_Ke3f[576];
+__constant__ double c_Ke1d[64];
+__constant__ float c_Ke1f[64];
+__constant__ double c_Fe3[144];
+__constant__ double c_X03[144];
+__constant__ double c_KX3[144];
+__constant__ double c_Fe1[24];
+__constant__ double c_X01[24];
+__constant__ double c_KX1[24];
+__constant__ double c_W[512];
+
+template <typename T, int D>
+__device__ __forceinline__ T ke(int i, int j);
+template <>
+__device__ __forceinline__ double ke<double, 3>(int i, int j) { return c_Ke3d[i * 24 + j]; }
+template <>
+__device__ __forceinline__ float ke<float, 3>(int i, int j) { return c_Ke3f[i * 24 + j]; }
+template <>
+__device__ __forceinline__ double ke<double, 1>(int i, int j) { return c_Ke1d[i * 8 + j]; }
+template <>
+__device__ __forceinline__ float ke<float, 1>(int i, int j) { return c_Ke1f[i * 8 + j]; }
+
+template <int D>
+__device__ __forceinline__ double fe(int i, int r) { return D == 3 ? c_Fe3[i * 6 + r] : c_Fe1[i * 3 + r]; }
+template <int D>
+__device__ __forceinline__ double x0(int i, int r) { return D == 3 ? c_X03[i * 6 + r] : c_X01[i * 3 + r]; }
+template <int D>
+__device__ __forceinline__ double kx(int i, int r) { return D == 3 ? c_KX3[i * 6 + r] : c_KX1[i * 3 + r]; }
+
+// element-local corner index of corner bits (cx,cy,cz): 000,100,110,010,001,101,111,011
+__host__ __device__ constexpr int lidx(int cx, int cy, int cz) { return cz * 4 + (cy ? (cx ? 2 : 3) : (cx ? 1 : 0)); }
+__host__ __device__ constexpr int corner_x(int a) { return (a == 1 || a == 2 || a == 5 || a == 6) ? 1 : 0; }
+__host__ __device__ constexpr int corner_y(int a) { return (a == 2 || a == 3 || a == 6 || a == 7) ? 1 : 0; }
+__host__ __device__ constexpr int corner_z(int a) { return a >= 4 ? 1 : 0; }
+
+__device__ __forceinline__ int wrapn(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// ----------------------------------------------------------------------------
+// block reductions (deterministic: fixed shuffle tree + fixed warp order)
+// ----------------------------------------------------------------------------
+template <int K>
+__device__ __forceinline__ void block_sum_store(double (&v)[K], double* out) {
+  __shared__ double sm[kThreads / 32][K];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) sm[warp][k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    double s = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) s += sm[w][threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+__device__ __forceinline__ double block_max(double v) {
+  __shared__ double sm[kThreads / 32];
+  __shared__ double res;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+  if (lane == 0) sm[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = sm[0];
+    for (int w = 1; w < kThreads / 32; ++w) m = fmax(m, sm[w]);
+    res = m;
+  }
+  __syncthreads();
+  return res;
+}
+
+// sum part[cell][0..nblk)[K] -> out[cell][K]; one block per cell, fixed order
+template <int K>
+__global__ void k_reduce_partials(const double* __restrict__ part, int nblk, double* __restrict__ out) {
+  const int b = blockIdx.x;
+  double v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = 0;
+  for (int i = threadIdx.x; i < nblk; i += kThreads) {
+    const double* p = part + ((size_t)b * nblk + i) * K;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += p[k];
+  }
+  block_sum_store<K>(v, out + (size_t)b * K);
+}
+
+// ----------------------------------------------------------------------------
+// small dense helpers
+// ----------------------------------------------------------------------------
+template <typename T, int D>
+__device__ __forceinline__ void block_inverse(const T (&A)[D][D], T (&Ai)[D][D]) {
+  if constexpr (D == 1) {
+    Ai[0][0] = A[0][0] != T(0) ? T(1) / A[0][0] : T(1);
+  } else {
+    T c00 = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+    T c01 = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+    T c02 = A[1][0] * A[2][1] - A[1][1] * A[2][0];
+    T det = A[0][0] * c00 + A[0][1] * c01 + A[0][2] * c02;
+    if (det == T(0)) {
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Ai[i][j] = (i == j) ? T(1) : T(0);
+      return;
+    }
+    T id = T(1) / det;
+    Ai[0][0] = c00 * id;
+    Ai[1][0] = c01 * id;
+    Ai[2][0] = c02 * id;
+    Ai[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * id;
+    Ai[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id;
+    Ai[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * id;
+    Ai[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id;
+    Ai[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * id;
+    Ai[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
+  }
+}
+
+// Chebyshev step coefficients on [hi/ratio, hi]: step 0 -> (0, 1/theta);
+// step k -> (rho_k rho_{k-1}, 2 rho_k / delta).
+__device__ __forceinline__ void cheb_coeffs(double hi, double ratio, int step, double& alpha, double& beta) {
+  const double lo = hi / ratio;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+  const double sigma = theta / delta;
+  if (step == 0) {
+    alpha = 0.0;
+    beta = 1.0 / theta;
+    return;
+  }
+  double rp = 1.0 / sigma, rk = rp;
+  for (int k = 1; k <= step; ++k) {
+    rk = 1.0 / (2.0 * sigma - rp);
+    if (k < step) rp = rk;
+  }
+  alpha = rk * rp;
+  beta = 2.0 * rk / delta;
+}
+
+// ----------------------------------------------------------------------------
+// operator application: fine level (matrix-free from rho) and coarse levels
+// (stored 27-point stencils)
+// ----------------------------------------------------------------------------
+enum ApplyMode { M_MV = 0, M_RES = 1, M_CHEB = 2, M_JAC0 = 3, M_POWER = 4 };
+
+template <typename T>
+struct ApplyArgs {
+  int n, N;
+  T scale;                 // fine level: stiffness scale (E/r or kappa/r)
+  const T* rho;            // fine level densities [B][N]
+  const T* S;              // coarse stencils [B][27][D*D][N]
+  const T* Dinv;           // coarse block-diagonal inverses [B][D*D][N]
+  const T* u;              // input iterate
+  const T* f;              // right-hand side (RES, CHEB, JAC0)
+  const T* din;            // Chebyshev direction in (may alias dout)
+  T* dout;                 // Chebyshev direction out
+  T* out;                  // MV/RES/POWER output, CHEB/JAC0 new iterate
+  const double* hi;        // per-cell Chebyshev upper bound (CHEB, JAC0)
+  double ratio;            // Chebyshev interval ratio hi/lo
+  int step;                // Chebyshev step index
+  double* part;            // per-block partial dots [B][nblk][R or 2] (nullable)
+  int dot_f_out;           // CHEB: partial sum of f.out (PCG r.z) instead of nothing
+  const int* active;       // per-cell flag (nullable)
+};
+
+// Loads the 8 element densities around node (x,y,z): element q = 4qx+2qy+qz at
+// offset (qx-1, qy-1, qz-1).
+template <typename T>
+__device__ __forceinline__ void load_rho8(const T* __restrict__ rho, int n, int x, int y, int z, T (&rq)[8]) {
+  const int xs[2] = {wrapn(x - 1, n), x}, ys[2] = {wrapn(y - 1, n), y}, zs[2] = {wrapn(z - 1, n), z};
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
+    rq[q] = __ldg(rho + ((size_t)xs[qx] * n + ys[qy]) * n + zs[qz]);
+  }
+}
+
+// Assembled 3x3 (or 1x1) coupling block between node n and n+o on the fine
+// level: sum over the elements sharing both nodes of rho_e * Ke0 block.
+template <typename T, int D, int O>
+__device__ __forceinline__ void fine_block(const T (&rq)[8], T (&C)[D][D]) {
+  constexpr int ox = O / 9 - 1, oy = (O / 3) % 3 - 1, oz = O % 3 - 1;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) C[i][j] = T(0);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
+    const int cx = 1 - qx, cy = 1 - qy, cz = 1 - qz;
+    const int nx = cx + ox, ny = cy + oy, nz = cz + oz;
+    if (nx < 0 || nx > 1 || ny < 0 || ny > 1 || nz < 0 || nz > 1) continue;
+    const int a = lidx(cx, cy, cz), bb = lidx(nx, ny, nz);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) C[i][j] += rq[q] * ke<T, D>(D * a + i, D * bb + j);
+  }
+}
+
+template <typename T, int D, int R, int O>
+__device__ __forceinline__ void fine_accumulate(const T (&rq)[8], const T* __restrict__ u, size_t cell_off, int n,
+                                                const int (&xs)[3], const int (&ys)[3], const int (&zs)[3],
+                                                T (&acc)[R][D], T (&C0)[D][D]) {
+  T C[D][D];
+  fine_block<T, D, O>(rq, C);
+  constexpr int ox = O / 9, oy = (O / 3) % 3, oz = O % 3;
+  const T* __restrict__ un = u + (cell_off + ((size_t)xs[ox] * n + ys[oy]) * n + zs[oz]) * (R * D);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    T uv[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) uv[j] = __ldg(un + r * D + j);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) acc[r][i] += C[i][j] * uv[j];
+  }
+  if constexpr (O == 13) {
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) C0[i][j] = C[i][j];
+  }
+}
+
+template <typename T, int D, int R, int... Os>
+__device__ __forceinline__ void fine_all(std::integer_sequence<int, Os...>, const T (&rq)[8], const T* __restrict__ u,
+                                         size_t cell_off, int n, const int (&xs)[3], const int (&ys)[3],
+                                         const int (&zs)[3], T (&acc)[R][D], T (&C0)[D][D]) {
+  (fine_accumulate<T, D, R, Os>(rq, u, cell_off, n, xs, ys, zs, acc, C0), ...);
+}
+
+// Shared epilogue of both apply kernels.
+template <typename T, int D, int R, int MODE>
+__device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, size_t vo, bool valid, T (&acc)[R][D],
+                                               const T (&Di)[D][D]) {
+  constexpr int K = R;
+  double dots[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) dots[k] = 0;
+  if (valid) {
+    if constexpr (MODE == M_MV) {
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          const T y = a.scale * acc[r][i];
+          a.out[vo + r * D + i] = y;
+          if (a.part) dots[r] += (double)y * (double)a.u[vo + r * D + i];
+        }
+    } else if constexpr (MODE == M_RES) {
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          const T y = a.f[vo + r * D + i] - a.scale * acc[r][i];
+          a.out[vo + r * D + i] = y;
+          dots[r] += (double)y * (double)y;
+        }
+    } else if constexpr (MODE == M_CHEB || MODE == M_JAC0) {
+      double al, be;
+      cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, al, be);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        T res[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          if constexpr (MODE == M_JAC0)
+            res[i] = a.f[vo + r * D + i];
+          else
+            res[i] = a.f[vo + r * D + i] - a.scale * acc[r][i];
+        }
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          T z = 0;
+#pragma unroll
+          for (int j = 0; j < D; ++j) z += Di[i][j] * res[j];
+          T d = T(be) * z;
+          if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + r * D + i];
+          a.dout[vo + r * D + i] = d;
+          const T un = (MODE == M_JAC0) ? d : a.u[vo + r * D + i] + d;
+          a.out[vo + r * D + i] = un;
+          if (a.dot_f_out) dots[r] += (double)a.f[vo + r * D + i] * (double)un;
+        }
+      }
+    }
+  }
+  if (a.part && (MODE != M_CHEB || a.dot_f_out)) {
+    block_sum_store<K>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * K);
+  }
+}
+
+template <typename T, int D, int R, int MODE>
+__global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
+  const int n = a.n;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  const bool valid = idx < a.N;
+  const int id = valid ? idx : 0;
+  const int z = id % n, y = (id / n) % n, x = id / (n * n);
+  const size_t cell = (size_t)b * a.N;
+  T rq[8];
+  load_rho8<T>(a.rho + cell, n, x, y, z, rq);
+  T acc[R][D];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int i = 0; i < D; ++i) acc[r][i] = T(0);
+  T C0[D][D];
+  if constexpr (MODE == M_JAC0) {
+    fine_block<T, D, 13>(rq, C0);
+  } else {
+    const int xs[3] = {wrapn(x - 1, n), x, wrapn(x + 1, n)};
+    const int ys[3] = {wrapn(y - 1, n), y, wrapn(y + 1, n)};
+    const int zs[3] = {wrapn(z - 1, n), z, wrapn(z + 1, n)};
+    fine_all<T, D, R>(std::make_integer_sequence<int, 27>{}, rq, a.u, cell, n, xs, ys, zs, acc, C0);
+  }
+  T Di[D][D];
+  T C0s[D][D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) C0s[i][j] = a.scale * C0[i][j];
+  block_inverse<T, D>(C0s, Di);
+  const size_t vo = (cell + id) * (R * D);
+  if constexpr (MODE == M_POWER) {
+    // second Rayleigh term u.Du with the assembled diagonal block
+    double ud = 0;
+    if (valid)
+      for (int i = 0; i < D; ++i)
+        for (int j = 0; j < D; ++j) ud += (double)a.u[vo + i] * (double)C0s[i][j] * (double)a.u[vo + j];
+    double dots[2] = {0, 0};
+    if (valid) {
+      T Au[D];
+      for (int i = 0; i < D; ++i) Au[i] = a.scale * acc[0][i];
+      for (int i = 0; i < D; ++i) {
+        T w = 0;
+        for (int j = 0; j < D; ++j) w += Di[i][j] * Au[j];
+        a.out[vo + i] = w;
+        dots[0] += (double)a.u[vo + i] * (double)Au[i];
+      }
+      dots[1] = ud;
+    }
+    block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
+  } else {
+    apply_epilogue<T, D, R, MODE>(a, b, vo, valid, acc, Di);
+  }
+}
+
+template <typename T, int D, int R, int MODE>
+__global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
+  const int n = a.n, N = a.N;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  const bool valid = idx < N;
+  const int id = valid ? idx : 0;
+  const int z = id % n, y = (id / n) % n, x = id / (n * n);
+  const size_t cell = (size_t)b * N;
+  T acc[R][D];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int i = 0; i < D; ++i) acc[r][i] = T(0);
+  const T* __restrict__ S = a.S + (size_t)b * 27 * D * D * N + id;
+  if constexpr (MODE != M_JAC0) {
+    const int xs[3] = {wrapn(x - 1, n), x, wrapn(x + 1, n)};
+    const int ys[3] = {wrapn(y - 1, n), y, wrapn(y + 1, n)};
+    const int zs[3] = {wrapn(z - 1, n), z, wrapn(z + 1, n)};
+#pragma unroll 3
+    for (int o = 0; o < 27; ++o) {
+      const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+      T C[D][D];
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) C[i][j] = __ldg(S + ((size_t)o * D * D + i * D + j) * N);
+      const T* __restrict__ un = a.u + (cell + ((size_t)xs[ox] * n + ys[oy]) * n + zs[oz]) * (R * D);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        T uv[D];
+#pragma unroll
+        for (int j = 0; j < D; ++j) uv[j] = __ldg(un + r * D + j);
+#pragma unroll
+        for (int i = 0; i < D; ++i)
+#pragma unroll
+          for (int j = 0; j < D; ++j) acc[r][i] += C[i][j] * uv[j];
+      }
+    }
+  }
+  T Di[D][D];
+  const T* __restrict__ Dp = a.Dinv + (size_t)b * D * D * N + id;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) Di[i][j] = __ldg(Dp + (size_t)(i * D + j) * N);
+  const size_t vo = (cell + id) * (R * D);
+  if constexpr (MODE == M_POWER) {
+    double dots[2] = {0, 0};
+    if (valid) {
+      T C0[D][D];
+      for (int i = 0; i < D; ++i)
+        for (int j = 0; j < D; ++j) C0[i][j] = __ldg(S + ((size_t)13 * D * D + i * D + j) * N);
+      for (int i = 0; i < D; ++i) {
+        T w = 0;
+        for (int j = 0; j < D; ++j) w += Di[i][j] * acc[0][j];
+        a.out[vo + i] = w;
+        dots[0] += (double)a.u[vo + i] * (double)acc[0][i];
+        for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i] * (double)C0[i][j] * (double)a.u[vo + j];
+      }
+    }
+    block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
+  } else {
+    apply_epilogue<T, D, R, MODE>(a, b, vo, valid, acc, Di);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// grid transfer: periodic trilinear P (EBE_GMG.py:38-79, 531-647)
+// ----------------------------------------------------------------------------
+// rc = P^T rf : coarse node gathers its 27 fine neighbours 2X+d, weight prod(1-|d|/2)
+template <typename T, int K>
+__global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ rc, int nc, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int Nc = nc * nc * nc, nf = 2 * nc, Nf = Nc * 8;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= Nc) return;
+  const int Z = idx % nc, Y = (idx / nc) % nc, X = idx / (nc * nc);
+  T acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0;
+  const T* __restrict__ base = rf + (size_t)b * Nf * K;
+#pragma unroll
+  for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz) {
+        const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
+        const int fx = wrapn(2 * X + dx, nf), fy = wrapn(2 * Y + dy, nf), fz = wrapn(2 * Z + dz, nf);
+        const T* p = base + (((size_t)fx * nf + fy) * nf + fz) * K;
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] += w * __ldg(p + k);
+      }
+  T* o = rc + ((size_t)b * Nc + idx) * K;
+#pragma unroll
+  for (int k = 0; k < K; ++k) o[k] = acc[k];
+}
+
+// uf += P uc
+template <typename T, int K>
+__global__ void k_prolong_add(const T* __restrict__ uc, T* __restrict__ uf, int nc, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int nf = 2 * nc, Nf = nf * nf * nf, Nc = nc * nc * nc;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= Nf) return;
+  const int z = idx % nf, y = (idx / nf) % nf, x = idx / (nf * nf);
+  const int bx = x >> 1, by = y >> 1, bz = z >> 1, rx = x & 1, ry = y & 1, rz = z & 1;
+  T acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0;
+  const T* __restrict__ base = uc + (size_t)b * Nc * K;
+#pragma unroll
+  for (int o = 0; o < 8; ++o) {
+    const int ox = (o >> 2) & 1, oy = (o >> 1) & 1, oz = o & 1;
+    if ((ox && !rx) || (oy && !ry) || (oz && !rz)) continue;
+    const T w = T((rx ? 0.5 : 1.0) * (ry ? 0.5 : 1.0) * (rz ? 0.5 : 1.0));
+    const int cx = bx + ox == nc ? 0 : bx + ox, cy = by + oy == nc ? 0 : by + oy, cz = bz + oz == nc ? 0 : bz + oz;
+    const T* p = base + (((size_t)cx * nc + cy) * nc + cz) * K;
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] += w * __ldg(p + k);
+  }
+  T* o = uf + ((size_t)b * Nf + idx) * K;
+#pragma unroll
+  for (int k = 0; k < K; ++k) o[k] += acc[k];
+}
+
+// coarsest level: u = Ainv f with the FP64 (regularised) inverse, per cell
+template <typename T, int R>
+__global__ void k_coarse_solve(const double* __restrict__ Ainv, const T* __restrict__ f, T* __restrict__ u, int ndof,
+                               int D, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int row = blockIdx.x * kThreads + threadIdx.x;
+  if (row >= ndof) return;
+  const double* Acol = Ainv + (size_t)b * ndof * ndof + row;
+  const T* fb = f + (size_t)b * ndof * R;  // [node][R][D] with ndof = nodes*D
+  double acc[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r] = 0;
+  for (int col = 0; col < ndof; ++col) {
+    const int node = col / D, c = col - node * D;
+    const double a = Acol[(size_t)col * ndof];  // symmetric: read column-wise (coalesced)
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] += a * (double)fb[(node * R + r) * D + c];
+  }
+  const int node = row / D, c = row - node * D;
+  T* ub = u + (size_t)b * ndof * R;
+#pragma unroll
+  for (int r = 0; r < R; ++r) ub[(node * R + r) * D + c] = (T)acc[r];
+}
+
+// ----------------------------------------------------------------------------
+// hierarchy construction (FP64)
+// ----------------------------------------------------------------------------
+// level-1 element matrices: K_E = sum_c rho_c M_c  (exact Galerkin of rho*Ke0)
+template <int D>
+__global__ void k_level1_elements(const double* __restrict__ rho, const double* __restrict__ M, double* __restrict__ KE,
+                                  int nc, double scale, const int* active) {
+  constexpr int k = 8 * D, kk = k * k;
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int Nc = nc * nc * nc, nf = 2 * nc;
+  const size_t t = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  if (t >= (size_t)Nc * kk) return;
+  const int e = (int)(t / kk), ij = (int)(t % kk);
+  const int Z = e % nc, Y = (e / nc) % nc, X = e / (nc * nc);
+  const double* rb = rho + (size_t)b * nf * nf * nf;
+  double s = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
+    const double r = rb[((size_t)(2 * X + cx) * nf + (2 * Y + cy)) * nf + (2 * Z + cz)];
+    s += r * M[c * kk + ij];
+  }
+  KE[((size_t)b * Nc + e) * kk + ij] = scale * s;
+}
+
+// K_{l+1}[E] = sum_c (W_c (x) I)^T K_l[child c] (W_c (x) I), one block per coarse element
+template <int D>
+__global__ void k_coarsen_elements(const double* __restrict__ Kf, double* __restrict__ Kc, int nc, const int* active) {
+  constexpr int k = 8 * D, kk = k * k;
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  extern __shared__ double smem_c[];
+  double(*sK)[kk] = reinterpret_cast<double(*)[kk]>(smem_c);
+  double(*sT)[kk] = reinterpret_cast<double(*)[kk]>(smem_c + 8 * kk);
+  const int e = blockIdx.x;
+  const int Z = e % nc, Y = (e / nc) % nc, X = e / (nc * nc);
+  const int nf = 2 * nc, Nf = nf * nf * nf, Nc = nc * nc * nc;
+  for (int t = threadIdx.x; t < 8 * kk; t += blockDim.x) {
+    const int c = t / kk, ij = t % kk;
+    const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
+    const size_t fe = ((size_t)(2 * X + cx) * nf + (2 * Y + cy)) * nf + (2 * Z + cz);
+    sK[c][ij] = Kf[((size_t)b * Nf + fe) * kk + ij];
+  }
+  __syncthreads();
+  // stage 1: T_c[(a',al)][(bb,be)] = sum_b' K_c[(a',al)][(b',be)] W_c[b'][bb]
+  for (int t = threadIdx.x; t < 8 * kk; t += blockDim.x) {
+    const int c = t / kk, ij = t % kk, row = ij / k, col = ij % k;
+    const int bb = col / D, be = col % D;
+    double s = 0;
+#pragma unroll
+    for (int b2 = 0; b2 < 8; ++b2) s += sK[c][row * k + D * b2 + be] * c_W[(c * 8 + b2) * 8 + bb];
+    sT[c][ij] = s;
+  }
+  __syncthreads();
+  // stage 2: out[(a,al)][col] = sum_c sum_a' W_c[a'][a] T_c[(a',al)][col]
+  for (int t = threadIdx.x; t < kk; t += blockDim.x) {
+    const int row = t / k, col = t % k, aa = row / D, al = row % D;
+    double s = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+#pragma unroll
+      for (int a2 = 0; a2 < 8; ++a2) s += c_W[(c * 8 + a2) * 8 + aa] * sT[c][(D * a2 + al) * k + col];
+    Kc[((size_t)b * Nc + e) * kk + t] = s;
+  }
+}
+
+// node stencils from element matrices; block-diagonal inverse at o = 13.
+template <typename T, int D>
+__global__ void k_stencil_from_elements(const double* __restrict__ KE, T* __restrict__ S, T* __restrict__ Dinv,
+                                        double* __restrict__ S64, int n, const int* active) {
+  constexpr int k = 8 * D, kk = k * k;
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n;
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= N * 27) return;
+  const int node = t % N, o = t / N;
+  const int z = node % n, y = (node / n) % n, x = node / (n * n);
+  const int ox = o / 9 - 1, oy = (o / 3) % 3 - 1, oz = o % 3 - 1;
+  double C[D][D] = {};
+  for (int q = 0; q < 8; ++q) {
+    const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
+    const int cx = 1 - qx, cy = 1 - qy, cz = 1 - qz;
+    const int nx = cx + ox, ny = cy + oy, nz = cz + oz;
+    if (nx < 0 || nx > 1 || ny < 0 || ny > 1 || nz < 0 || nz > 1) continue;
+    const int ex = wrapn(x + qx - 1, n), ey = wrapn(y + qy - 1, n), ez = wrapn(z + qz - 1, n);
+    const double* K = KE + ((size_t)b * N + ((size_t)ex * n + ey) * n + ez) * kk;
+    const int aa = lidx(cx, cy, cz), bb = lidx(nx, ny, nz);
+    for (int i = 0; i < D; ++i)
+      for (int j = 0; j < D; ++j) C[i][j] += K[(D * aa + i) * k + D * bb + j];
+  }
+  for (int i = 0; i < D; ++i)
+    for (int j = 0; j < D; ++j) {
+      const size_t si = (((size_t)b * 27 + o) * D * D + i * D + j) * N + node;
+      if (S) S[si] = (T)C[i][j];
+      if (S64) S64[si] = C[i][j];
+    }
+  if (o == 13 && Dinv) {
+    double Ci[D][D];
+    block_inverse<double, D>(C, Ci);
+    for (int i = 0; i < D; ++i)
+      for (int j = 0; j < D; ++j) Dinv[((size_t)b * D * D + i * D + j) * N + node] = (T)Ci[i][j];
+  }
+}
+
+// dense coarsest matrix from the FP64 stencil (n >= 3: the 27 neighbours are
+// distinct), plus alpha * Z Z^T on the D translation modes.
+template <int D>
+__global__ void k_dense_from_stencil(const double* __restrict__ S64, double* __restrict__ A, int n, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n, ndof = N * D;
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= N * 27) return;
+  const int node = t % N, o = t / N;
+  const int z = node % n, y = (node / n) % n, x = node / (n * n);
+  const int ox = o / 9 - 1, oy = (o / 3) % 3 - 1, oz = o % 3 - 1;
+  const int m = (wrapn(x + ox, n) * n + wrapn(y + oy, n)) * n + wrapn(z + oz, n);
+  double* Ab = A + (size_t)b * ndof * ndof;
+  for (int i = 0; i < D; ++i)
+    for (int j = 0; j < D; ++j)
+      Ab[(size_t)(node * D + i) * ndof + m * D + j] = S64[(((size_t)b * 27 + o) * D * D + i * D + j) * N + node];
+}
+
+// In-place inverse of the SPD matrix A + alpha Z Z^T (one block per cell).
+// Cholesky (lower) then inverse via L^-1; A is ndof x ndof FP64 in global memory,
+// work holds ndof x ndof scratch.
+__global__ void k_chol_inverse(double* __restrict__ A, double* __restrict__ work, int ndof, int D, const int* active,
+                               int* status) {
+  const int b = blockIdx.x;
+  if (active && !active[b]) return;
+  double* M = A + (size_t)b * ndof * ndof;
+  double* Li = work + (size_t)b * ndof * ndof;
+  __shared__ double s_alpha;
+  // regularise: alpha = mean diagonal, Z columns = unit translation per component / sqrt(N)
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int i = 0; i < ndof; ++i) s += M[(size_t)i * ndof + i];
+    s_alpha = s / ndof;
+  }
+  __syncthreads();
+  const double alpha = s_alpha;
+  const int Nn = ndof / D;
+  for (int t = threadIdx.x; t < ndof * ndof; t += blockDim.x) {
+    const int i = t / ndof, j = t % ndof;
+    if ((i % D) == (j % D)) M[t] += alpha / Nn;
+  }
+  __syncthreads();
+  // Cholesky, right-looking, lower triangle
+  for (int kcol = 0; kcol < ndof; ++kcol) {
+    __shared__ double s_piv;
+    if (threadIdx.x == 0) {
+      double d = M[(size_t)kcol * ndof + kcol];
+      if (!(d > 0)) {
+        if (status) status[b] = 1;
+        d = 1e-300;
+      }
+      s_piv = sqrt(d);
+      M[(size_t)kcol * ndof + kcol] = s_piv;
+    }
+    __syncthreads();
+    const double piv = s_piv;
+    for (int i = kcol + 1 + threadIdx.x; i < ndof; i += blockDim.x) M[(size_t)i * ndof + kcol] /= piv;
+    __syncthreads();
+    const int m = ndof - kcol - 1;
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+      const int i = kcol + 1 + t / m, j = kcol + 1 + t % m;
+      if (j <= i) M[(size_t)i * ndof + j] -= M[(size_t)i * ndof + kcol] * M[(size_t)j * ndof + kcol];
+    }
+    __syncthreads();
+  }
+  // Li = L^-1 (lower), column by column: thread per column
+  for (int j = threadIdx.x; j < ndof; j += blockDim.x) {
+    for (int i = 0; i < ndof; ++i) {
+      double s = (i == j) ? 1.0 : 0.0;
+      for (int p = j; p < i; ++p) s -= M[(size_t)i * ndof + p] * Li[(size_t)p * ndof + j];
+      Li[(size_t)i * ndof + j] = (i < j) ? 0.0 : s / M[(size_t)i * ndof + i];
+    }
+  }
+  __syncthreads();
+  // A^-1 = Li^T Li
+  for (int t = threadIdx.x; t < ndof * ndof; t += blockDim.x) {
+    const int i = t / ndof, j = t % ndof;
+    const int p0 = i > j ? i : j;
+    double s = 0;
+    for (int p = p0; p < ndof; ++p) s += Li[(size_t)p * ndof + i] * Li[(size_t)p * ndof + j];
+    M[t] = s;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// right-hand sides, vectors, PCG scalars
+// ----------------------------------------------------------------------------
+// F = sum_e rho_e Fe0 gathered at nodes (utils/_utils.py:453-507)
+template <int D, int R>
+__global__ void k_assemble_F(const double* __restrict__ rho, double* __restrict__ F, int n, double scale,
+                             const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= N) return;
+  const int z = idx % n, y = (idx / n) % n, x = idx / (n * n);
+  double rq[8];
+  load_rho8<double>(rho + (size_t)b * N, n, x, y, z, rq);
+  double acc[R][D] = {};
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
+    const int aa = lidx(1 - qx, 1 - qy, 1 - qz);
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < D; ++i) acc[r][i] += rq[q] * fe<D>(D * aa + i, r);
+  }
+  double* o = F + ((size_t)b * N + idx) * R * D;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int i = 0; i < D; ++i) o[r * D + i] = scale * acc[r][i];
+}
+
+// rho = rho_min + (1-rho_min) clamp(x,xmin,1)^p, FP64 and FP32 copies
+__global__ void k_simp(const double* __restrict__ x, double* __restrict__ rho64, float* __restrict__ rho32, size_t total,
+                       int N, double xmin, double penal, double rho_min, const int* active) {
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  if (i >= total) return;
+  if (active && !active[i / N]) return;
+  double xc = fmin(fmax(x[i], xmin), 1.0);
+  double r = rho_min + (1.0 - rho_min) * pow(xc, penal);
+  rho64[i] = r;
+  if (rho32) rho32[i] = (float)r;
+}
+
+__global__ void k_copy_rho(const double* __restrict__ rho, double* __restrict__ rho64, float* __restrict__ rho32,
+                           size_t total) {
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  if (i >= total) return;
+  rho64[i] = rho[i];
+  if (rho32) rho32[i] = (float)rho[i];
+}
+
+// partial dots x.y per rhs over [cell][node][R][D]
+template <typename T, int R, int D>
+__global__ void k_dot(const T* __restrict__ x, const T* __restrict__ y, double* __restrict__ part, int N,
+                      const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  double v[R] = {};
+  if (idx < N) {
+    const size_t o = ((size_t)b * N + idx) * R * D;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < D; ++i) v[r] += (double)x[o + r * D + i] * (double)y[o + r * D + i];
+  }
+  block_sum_store<R>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * R);
+}
+
+// x += alpha p ; r -= alpha q ; partial r.r   (alpha per cell/rhs)
+template <typename T, int R, int D>
+__global__ void k_pcg_update(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p, const T* __restrict__ q,
+                             const double* __restrict__ alpha, double* __restrict__ part, int N, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  double v[R] = {};
+  if (idx < N) {
+    const size_t o = ((size_t)b * N + idx) * R * D;
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      const T a = (T)alpha[b * R + c];
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        x[o + c * D + i] += a * p[o + c * D + i];
+        const T rn = r[o + c * D + i] - a * q[o + c * D + i];
+        r[o + c * D + i] = rn;
+        v[c] += (double)rn * (double)rn;
+      }
+    }
+  }
+  block_sum_store<R>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * R);
+}
+
+// p = z + beta p
+template <typename T, int R, int D>
+__global__ void k_pcg_direction(T* __restrict__ p, const T* __restrict__ z, const double* __restrict__ beta, int N,
+                                const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= N) return;
+  const size_t o = ((size_t)b * N + idx) * R * D;
+#pragma unroll
+  for (int c = 0; c < R; ++c) {
+    const T be = (T)beta[b * R + c];
+#pragma unroll
+    for (int i = 0; i < D; ++i) p[o + c * D + i] = z[o + c * D + i] + be * p[o + c * D + i];
+  }
+}
+
+// per-(cell,rhs) PCG scalar logic, one thread per (cell, rhs)
+struct PcgScalars {
+  double* rz;      // r.z
+  double* rz_new;  // reduced r.z of the new z
+  double* pq;      // reduced p.q
+  double* rr;      // reduced r.r
+  double* bnorm2;  // ||b||^2 of the system being solved
+  double* alpha;
+  double* beta;
+  int* done;       // per (cell,rhs)
+  int* cell_done;  // per cell
+  int* iters;      // per cell
+};
+
+// after q = A p: alpha = rz / pq (0 once the column converged or on breakdown)
+__global__ void k_pcg_alpha(PcgScalars s, int total, int* breakdown) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  double a = 0.0;
+  if (!s.done[i]) {
+    const double pq = s.pq[i];
+    if (pq > 0.0 && isfinite(pq)) {
+      a = s.rz[i] / pq;
+    } else {
+      s.done[i] = 2;  // breakdown: freeze this column
+      if (breakdown) atomicOr(breakdown, 1);
+    }
+  }
+  s.alpha[i] = a;
+}
+
+// after the update: convergence test on ||r|| <= rtol ||b||
+__global__ void k_pcg_check(PcgScalars s, int B, int R, double rtol2, int it) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  if (s.cell_done[b]) return;
+  int all = 1;
+  for (int c = 0; c < R; ++c) {
+    const int i = b * R + c;
+    if (!s.done[i] && s.rr[i] <= rtol2 * s.bnorm2[i]) s.done[i] = 1;
+    all &= (s.done[i] != 0);
+  }
+  s.iters[b] = it;
+  if (all) s.cell_done[b] = 1;
+}
+
+// after z = M r: beta = rz_new / rz; rz = rz_new
+__global__ void k_pcg_beta(PcgScalars s, int total) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  double be = 0.0;
+  if (!s.done[i] && s.rz[i] != 0.0) be = s.rz_new[i] / s.rz[i];
+  s.beta[i] = be;
+  s.rz[i] = s.rz_new[i];
+}
+
+// convert an FP64 vector to FP32 with a per-(cell,rhs) scale; and back (add)
+template <int R, int D>
+__global__ void k_to_f32_scaled(const double* __restrict__ src, float* __restrict__ dst, const double* __restrict__ inv_scale,
+                                int N, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= N) return;
+  const size_t o = ((size_t)b * N + idx) * R * D;
+#pragma unroll
+  for (int c = 0; c < R; ++c) {
+    const double s = inv_scale[b * R + c];
+#pragma unroll
+    for (int i = 0; i < D; ++i) dst[o + c * D + i] = (float)(src[o + c * D + i] * s);
+  }
+}
+
+template <int R, int D>
+__global__ void k_add_f32_scaled(double* __restrict__ dst, const float* __restrict__ src, const double* __restrict__ scale,
+                                 int N, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= N) return;
+  const size_t o = ((size_t)b * N + idx) * R * D;
+#pragma unroll
+  for (int c = 0; c < R; ++c) {
+    const double s = scale[b * R + c];
+#pragma unroll
+    for (int i = 0; i < D; ++i) dst[o + c * D + i] += s * (double)src[o + c * D + i];
+  }
+}
+
+// deterministic pseudo-random start vector for power iterations
+template <typename T>
+__global__ void k_power_init(T* __restrict__ v, size_t total) {
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  if (i >= total) return;
+  unsigned h = (unsigned)(i * 2654435761u) ^ 0x9e3779b9u;
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  v[i] = (T)(((h & 0xffffff) / 8388608.0) - 1.0);
+}
+
+// hi[cell] = safety * (u.Au)/(u.Du) from the reduced Rayleigh terms
+__global__ void k_power_finish(const double* __restrict__ red, double* __restrict__ hi, int B, double safety) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const double num = red[2 * b], den = red[2 * b + 1];
+  double lam = (den > 0 && num > 0) ? num / den : 2.0;
+  hi[b] = safety * lam;
+}
+
+// ----------------------------------------------------------------------------
+// homogenization, sensitivity, objective, filter, OC
+// ----------------------------------------------------------------------------
+// per element (X0-u_e)^T Ke0 (X0-u_e) -> energy[cell][e][R][R]; partial sums of
+// rho_e * energy for C^H / kappa^H (model.py:33-95)
+template <int D, int R>
+__global__ void __launch_bounds__(kThreads) k_homogenize(const double* __restrict__ u, const double* __restrict__ rho,
+                                                         double* __restrict__ energy, double* __restrict__ part, int n,
+                                                         double kscale, double xscale, const int* active) {
+  constexpr int k = 8 * D;
+  constexpr int K = R * (R + 1) / 2;
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n;
+  const int e = blockIdx.x * kThreads + threadIdx.x;
+  const bool valid = e < N;
+  const int ee = valid ? e : 0;
+  const int z = ee % n, y = (ee / n) % n, x = ee / (n * n);
+  int nodes[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+    nodes[a] = (wrapn(x + corner_x(a), n) * n + wrapn(y + corner_y(a), n)) * n + wrapn(z + corner_z(a), n);
+  const double* __restrict__ ub = u + (size_t)b * N * R * D;
+  const double re = valid ? rho[(size_t)b * N + ee] : 0.0;
+  double* eo = energy + ((size_t)b * N + ee) * R * R;
+  double v[K];
+#pragma unroll
+  for (int s = 0; s < R; ++s) {
+    double KL[k];
+    {
+      double L[k];
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int i = 0; i < D; ++i) L[D * a + i] = xscale * x0<D>(D * a + i, s) - __ldg(ub + ((size_t)nodes[a] * R + s) * D + i);
+#pragma unroll
+      for (int p = 0; p < k; ++p) {
+        double acc = 0;
+#pragma unroll
+        for (int q = 0; q < k; ++q) acc += ke<double, D>(p, q) * L[q];
+        KL[p] = kscale * acc;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r <= s; ++r) {
+      double acc = 0;
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int i = 0; i < D; ++i)
+          acc += (xscale * x0<D>(D * a + i, r) - __ldg(ub + ((size_t)nodes[a] * R + r) * D + i)) * KL[D * a + i];
+      // index of (r,s), r <= s, in the packed upper triangle
+      v[r * R - r * (r - 1) / 2 + (s - r)] = re * acc;
+      if (valid) {
+        eo[r * R + s] = acc;
+        eo[s * R + r] = acc;
+      }
+    }
+  }
+  block_sum_store<K>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * K);
+}
+
+// unpack reduced upper triangles into full symmetric matrices H[cell][R][R]
+__global__ void k_unpack_sym(const double* __restrict__ red, double* __restrict__ H, int B, int R) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const int K = R * (R + 1) / 2;
+  int m = 0;
+  for (int r = 0; r < R; ++r)
+    for (int s = r; s < R; ++s) {
+      const double v = red[b * K + m++];
+      H[(b * R + r) * R + s] = v;
+      H[(b * R + s) * R + r] = v;
+    }
+}
+
+// objective J = wE*E + wG*G + wK*trace(kappa) and its gradients
+// (maple/core/utils/objective.py:11-41, 180-251), one thread per cell.
+__device__ void inv6(const double (&A)[6][6], double (&Ai)[6][6]) {
+  double M[6][12];
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      M[i][j] = A[i][j];
+      M[i][6 + j] = (i == j) ? 1.0 : 0.0;
+    }
+  for (int k = 0; k < 6; ++k) {
+    int p = k;
+    for (int i = k + 1; i < 6; ++i)
+      if (fabs(M[i][k]) > fabs(M[p][k])) p = i;
+    if (p != k)
+      for (int j = 0; j < 12; ++j) {
+        double t = M[k][j];
+        M[k][j] = M[p][j];
+        M[p][j] = t;
+      }
+    const double d = M[k][k];
+    for (int j = 0; j < 12; ++j) M[k][j] /= d;
+    for (int i = 0; i < 6; ++i)
+      if (i != k) {
+        const double f = M[i][k];
+        for (int j = 0; j < 12; ++j) M[i][j] -= f * M[k][j];
+      }
+  }
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) Ai[i][j] = M[i][6 + j];
+}
+
+__global__ void k_objective(const double* __restrict__ CH, const double* __restrict__ KAP, const double* __restrict__ w,
+                            double* __restrict__ J, double* __restrict__ terms, double* __restrict__ G3,
+                            double* __restrict__ G1, int B, int need_ch, int need_k, const int* active) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  if (active && !active[b]) return;
+  const double wE = w[3 * b], wG = w[3 * b + 1], wK = w[3 * b + 2];
+  double j = 0, tE = 0, tG = 0, tK = 0;
+  double g3[6][6] = {};
+  if (need_ch) {
+    double C[6][6], S[6][6];
+    for (int r = 0; r < 6; ++r)
+      for (int s = 0; s < 6; ++s) C[r][s] = 0.5 * (CH[(b * 6 + r) * 6 + s] + CH[(b * 6 + s) * 6 + r]) + (r == s ? 1e-9 : 0.0);
+    inv6(C, S);
+    for (int t = 0; t < 2; ++t) {
+      const double wt = t == 0 ? wE : wG;
+      double val = 0;
+      for (int ii = 0; ii < 3; ++ii) {
+        const int i = 3 * t + ii;
+        val += 1.0 / S[i][i];
+        if (wt != 0.0) {
+          const double f = wt / 3.0 / (S[i][i] * S[i][i]);
+          for (int r = 0; r < 6; ++r)
+            for (int s = 0; s < 6; ++s) g3[r][s] += f * S[r][i] * S[i][s];
+        }
+      }
+      val /= 3.0;
+      if (t == 0) tE = val; else tG = val;
+      j += wt * val;
+    }
+  }
+  if (need_k) {
+    tK = KAP[b * 9 + 0] + KAP[b * 9 + 4] + KAP[b * 9 + 8];
+    j += wK * tK;
+  }
+  J[b] = j;
+  terms[3 * b] = tE;
+  terms[3 * b + 1] = tG;
+  terms[3 * b + 2] = tK;
+  for (int r = 0; r < 6; ++r)
+    for (int s = 0; s < 6; ++s) G3[(b * 6 + r) * 6 + s] = 0.5 * (g3[r][s] + g3[s][r]);
+  for (int r = 0; r < 3; ++r)
+    for (int s = 0; s < 3; ++s) G1[(b * 3 + r) * 3 + s] = (r == s) ? wK : 0.0;
+}
+
+// dJ/dx_e = p (1-rho_min) xc^(p-1) * (G3 : E3_e + G1 : E1_e)
+__global__ void k_sensitivity(const double* __restrict__ x, const double* __restrict__ E3, const double* __restrict__ E1,
+                              const double* __restrict__ G3, const double* __restrict__ G1, double* __restrict__ dJdx,
+                              double* __restrict__ dJdrho, int N, double xmin, double penal, double rho_min,
+                              const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int e = blockIdx.x * kThreads + threadIdx.x;
+  if (e >= N) return;
+  const size_t i = (size_t)b * N + e;
+  double s = 0;
+  if (E3) {
+    const double* Ee = E3 + i * 36;
+    const double* G = G3 + (size_t)b * 36;
+#pragma unroll
+    for (int k = 0; k < 36; ++k) s += G[k] * Ee[k];
+  }
+  if (E1) {
+    const double* Ee = E1 + i * 9;
+    const double* G = G1 + (size_t)b * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s += G[k] * Ee[k];
+  }
+  if (dJdrho) dJdrho[i] = s;
+  if (dJdx) {
+    const double xv = x[i];
+    const double xc = fmin(fmax(xv, xmin), 1.0);
+    const double inside = (xv >= xmin && xv <= 1.0) ? 1.0 : 0.0;
+    dJdx[i] = inside * s * penal * (1.0 - rho_min) * pow(xc, penal - 1.0);
+  }
+}
+
+// out[b][e] (+)= sum_k g[b][k] * energy[b][e][k]
+__global__ void k_energy_contract(const double* __restrict__ energy, const double* __restrict__ g,
+                                  double* __restrict__ out, int N, int RR, int accumulate) {
+  const int b = blockIdx.y;
+  const int e = blockIdx.x * kThreads + threadIdx.x;
+  if (e >= N) return;
+  const size_t i = (size_t)b * N + e;
+  const double* Ee = energy + i * RR;
+  const double* gb = g + (size_t)b * RR;
+  double s = 0;
+  for (int k = 0; k < RR; ++k) s += gb[k] * Ee[k];
+  out[i] = accumulate ? out[i] + s : s;
+}
+
+// periodic k^3 box mean (main_IHD_v3.py:342-359)
+__global__ void k_box_filter(const double* __restrict__ in, double* __restrict__ out, int n, int kf, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n;
+  const int e = blockIdx.x * kThreads + threadIdx.x;
+  if (e >= N) return;
+  const int z = e % n, y = (e / n) % n, x = e / (n * n);
+  const int p = kf / 2;
+  const double* ib = in + (size_t)b * N;
+  double s = 0;
+  for (int dx = -p; dx <= p; ++dx) {
+    const int xx = ((x + dx) % n + n) % n;
+    for (int dy = -p; dy <= p; ++dy) {
+      const int yy = ((y + dy) % n + n) % n;
+      for (int dz = -p; dz <= p; ++dz) {
+        const int zz = ((z + dz) % n + n) % n;
+        s += ib[((size_t)xx * n + yy) * n + zz];
+      }
+    }
+  }
+  out[(size_t)b * N + e] = s / (double)(kf * kf * kf);
+}
+
+// Bounded grid barrier for co-resident (cooperatively launched) blocks: a spin
+// that gives up after `limit` polls and raises *err instead of hanging.
+__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = gen;
+    const unsigned g = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(count, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      long polls = 0;
+      while (*vgen == g) {
+        if (++polls > (1L << 24)) {
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// OC update with 60 bisection steps on lambda in [1e-12, 1e6]
+// (main_IHD_v3.py:362-380).  Grid (G, B): G co-resident blocks per cell.
+// The returned x is that of the last bisection step, as in the reference.
+struct OcArgs {
+  const double* x;
+  const double* dJ;
+  double* xnew;
+  const double* volfrac;  // [B]
+  double move, xmin;
+  int N;
+  double* part;       // [B][4][G]: bisection sums (double-buffered) + |dx| sum/max
+  double* stats;      // [B][2]: dx_max, dx_mean
+  double* lam_out;    // [B]
+  unsigned* bar;      // [2] barrier counter, generation
+  int* err;
+  const int* active;
+};
+
+__global__ void __launch_bounds__(kThreads) k_oc_update(OcArgs a) {
+  const int G = gridDim.x, g = blockIdx.x, b = blockIdx.y;
+  const unsigned nblocks = gridDim.x * gridDim.y;
+  const bool act = !a.active || a.active[b];
+  const int N = a.N;
+  const int chunk = (N + G - 1) / G;
+  const int lo = g * chunk, hi = min(N, lo + chunk);
+  const double* xb = a.x + (size_t)b * N;
+  const double* db = a.dJ + (size_t)b * N;
+  const double vf = act ? a.volfrac[b] : 0.0;
+  double l1 = 1e-12, l2 = 1e6, lam = 0;
+  for (int it = 0; it < 60; ++it) {
+    lam = 0.5 * (l1 + l2);
+    double s = 0;
+    if (act) {
+      for (int i = lo + threadIdx.x; i < hi; i += kThreads) {
+        const double xv = xb[i];
+        const double dj = fmax(db[i], 1e-12);
+        double xn = xv * sqrt(dj / lam);
+        xn = fmin(fmax(xn, xv - a.move), xv + a.move);
+        xn = fmin(fmax(xn, a.xmin), 1.0);
+        s += xn;
+      }
+    }
+    double v[1] = {s};
+    block_sum_store<1>(v, a.part + ((size_t)b * 4 + (it & 1)) * G + g);
+    grid_barrier(a.bar, a.bar + 1, nblocks, a.err);
+    if (act) {
+      double tot = 0;
+      const double* pp = a.part + ((size_t)b * 4 + (it & 1)) * G;
+      for (int k = 0; k < G; ++k) tot += __ldcg(pp + k);
+      if (tot / (double)N > vf)
+        l1 = lam;
+      else
+        l2 = lam;
+    }
+  }
+  // final x (that of the last step) and |dx| statistics
+  double dmax = 0, dsum = 0;
+  if (act) {
+    double* xo = a.xnew + (size_t)b * N;
+    for (int i = lo + threadIdx.x; i < hi; i += kThreads) {
+      const double xv = xb[i];
+      const double dj = fmax(db[i], 1e-12);
+      double xn = xv * sqrt(dj / lam);
+      xn = fmin(fmax(xn, xv - a.move), xv + a.move);
+      xn = fmin(fmax(xn, a.xmin), 1.0);
+      xo[i] = xn;
+      const double d = fabs(xn - xv);
+      dmax = fmax(dmax, d);
+      dsum += d;
+    }
+  }
+  dmax = block_max(dmax);
+  double v[1] = {dsum};
+  __syncthreads();
+  block_sum_store<1>(v, a.part + ((size_t)b * 4 + 2) * G + g);
+  if (threadIdx.x == 0) a.part[((size_t)b * 4 + 3) * G + g] = dmax;
+  grid_barrier(a.bar, a.bar + 1, nblocks, a.err);
+  if (act && g == 0 && threadIdx.x == 0) {
+    double m = 0, t = 0;
+    for (int k = 0; k < G; ++k) {
+      t += __ldcg(a.part + ((size_t)b * 4 + 2) * G + k);
+      m = fmax(m, __ldcg(a.part + ((size_t)b * 4 + 3) * G + k));
+    }
+    a.stats[2 * b] = m;
+    a.stats[2 * b + 1] = t / (double)N;
+    if (a.lam_out) a.lam_out[b] = lam;
+  }
+}
+
+}  // namespace maple

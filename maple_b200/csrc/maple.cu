@@ -1,0 +1,1086 @@
+// maple_b200 runtime: context, operator hierarchy, MG-PCG driver, OC step and
+// the C ABI declared in include/maple_b200.h.
+#include "../../include/maple_b200.h"
+#include "kernels.cuh"
+#include "tables.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace maple {
+
+static thread_local std::string g_err;
+
+struct Failure {
+  int code;
+  std::string msg;
+};
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      throw Failure{MAPLE_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) + " at " +   \
+                                      std::string(__FILE__) + ":" + std::to_string(__LINE__)};    \
+  } while (0)
+#define CKL() CK(cudaGetLastError())
+
+static void require(bool ok, const std::string& msg) {
+  if (!ok) throw Failure{MAPLE_E_BADARG, msg};
+}
+
+constexpr int kMaxLevels = 8;
+
+// ---------------------------------------------------------------------------
+// per-device constant tables (unit voxel; one Poisson ratio per process)
+// ---------------------------------------------------------------------------
+static std::mutex g_mu;
+static double g_nu = -1.0;
+static bool g_dev_ready[128];
+static ElementTables g_tab;
+
+static void ensure_tables(double nu) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_nu < 0) {
+    element_tables(1.0, nu, 1.0, &g_tab);
+    g_nu = nu;
+  } else {
+    require(g_nu == nu, "all contexts of a process must share one Poisson ratio");
+  }
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  require(dev >= 0 && dev < 128, "device index out of range");
+  if (!g_dev_ready[dev]) {
+    float f3[576], f1[64];
+    for (int i = 0; i < 576; ++i) f3[i] = (float)g_tab.Ke3[i];
+    for (int i = 0; i < 64; ++i) f1[i] = (float)g_tab.Ke1[i];
+    CK(cudaMemcpyToSymbol(c_Ke3d, g_tab.Ke3, sizeof(g_tab.Ke3)));
+    CK(cudaMemcpyToSymbol(c_Ke3f, f3, sizeof(f3)));
+    CK(cudaMemcpyToSymbol(c_Ke1d, g_tab.Ke1, sizeof(g_tab.Ke1)));
+    CK(cudaMemcpyToSymbol(c_Ke1f, f1, sizeof(f1)));
+    CK(cudaMemcpyToSymbol(c_Fe3, g_tab.Fe3, sizeof(g_tab.Fe3)));
+    CK(cudaMemcpyToSymbol(c_X03, g_tab.X03, sizeof(g_tab.X03)));
+    CK(cudaMemcpyToSymbol(c_KX3, g_tab.KX3, sizeof(g_tab.KX3)));
+    CK(cudaMemcpyToSymbol(c_Fe1, g_tab.Fe1, sizeof(g_tab.Fe1)));
+    CK(cudaMemcpyToSymbol(c_X01, g_tab.X01, sizeof(g_tab.X01)));
+    CK(cudaMemcpyToSymbol(c_KX1, g_tab.KX1, sizeof(g_tab.KX1)));
+    CK(cudaMemcpyToSymbol(c_W, g_tab.W, sizeof(g_tab.W)));
+    g_dev_ready[dev] = true;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Ops {
+  bool alloc = false;
+  T* rho = nullptr;                      // fine densities [B][N0]
+  T* S[kMaxLevels] = {};                 // stencils (1 <= l < L-1)
+  T* Dinv[kMaxLevels] = {};
+  T* F[kMaxLevels] = {};                 // level RHS (l >= 1)
+  T* U[kMaxLevels][2] = {};              // iterate ping-pong; result in U[l][1]
+  T* Dd[kMaxLevels] = {};                // Chebyshev direction
+  T* Res[kMaxLevels] = {};               // residual
+  double* hi[kMaxLevels] = {};           // per-cell Chebyshev upper bound
+  T *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;  // PCG (level 0)
+};
+
+struct Phys {
+  int D = 0, R = 0;
+  double kscale = 0, fscale = 0, xscale = 0;  // stiffness, load and X0 scale at resolution r
+  bool alloc = false, built = false, solved = false, energies = false;
+  int built_prec = -1;
+  double* KE[kMaxLevels] = {};   // FP64 element matrices of level l >= 1
+  double* S64c = nullptr;        // FP64 coarsest stencil
+  double* Ainv = nullptr;        // FP64 coarsest inverse [B][ndof][ndof]
+  double* cwork = nullptr;
+  double* F64 = nullptr;         // RHS [B][N][R][D]
+  double* u64 = nullptr;         // solution
+  double* r64 = nullptr;         // outer residual
+  double* energy = nullptr;      // [B][N][R][R]
+  double* H = nullptr;           // [B][R][R]
+  Ops<double> o64;
+  Ops<float> o32;
+};
+
+struct Scalars {
+  double *rz, *rz_new, *pq, *rr, *bnorm2, *alpha, *beta;
+  int *done, *cell_done, *iters, *run;
+};
+
+}  // namespace maple
+
+struct maple_ctx {
+  int dev = 0;
+  int r = 0, B = 0, L = 0;
+  int n[maple::kMaxLevels] = {};
+  double E = 1, nu = 0.3, kappa = 1;
+  maple::Phys ph[2];
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  int* active = nullptr;          // device [B]
+  std::vector<int> h_active;
+  double* part = nullptr;         // partial sums [B][nblk0][32]
+  double* red = nullptr;          // reduced values [B][32]
+  maple::Scalars sc{};            // inner PCG scalars
+  double *o_rr = nullptr, *o_bn = nullptr, *o_scale = nullptr, *o_inv = nullptr;  // outer refinement
+  int *o_done = nullptr, *o_run = nullptr;
+  int* h_flags = nullptr;         // pinned host [B]
+  int* breakdown = nullptr;
+  // OC step buffers
+  double *x_rho = nullptr, *dJdx = nullptr, *dJf = nullptr, *Jv = nullptr, *terms = nullptr, *G3 = nullptr,
+         *G1 = nullptr, *stats = nullptr, *ocpart = nullptr, *ocvf = nullptr;
+  unsigned* bar = nullptr;
+  int* err = nullptr;
+  int oc_G = 0;
+  // options
+  int cheb_degree = 2;
+  double cheb_ratio = 10.0;
+  int power_iters = 12;
+  double power_safety = 1.15;
+  double inner_rtol = 1e-5;
+  int check_every = 1;
+};
+
+namespace maple {
+
+static void* dalloc(maple_ctx* c, size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) throw Failure{MAPLE_E_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e)};
+  c->allocs.push_back(p);
+  c->bytes += bytes;
+  return p;
+}
+template <typename T>
+static T* dnew(maple_ctx* c, size_t count) {
+  return reinterpret_cast<T*>(dalloc(c, count * sizeof(T)));
+}
+
+static inline unsigned nblk(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+static inline dim3 g2(size_t n, int B) { return dim3(nblk(n), (unsigned)B); }
+
+static int nodes(int n) { return n * n * n; }
+
+template <typename T>
+static void alloc_ops(maple_ctx* c, Phys& p, Ops<T>& o, bool vectors) {
+  if (o.alloc) return;
+  const int B = c->B, RD = p.R * p.D, DD = p.D * p.D;
+  const size_t N0 = nodes(c->n[0]);
+  o.rho = dnew<T>(c, (size_t)B * N0);
+  if (vectors) {
+    for (int l = 0; l < c->L; ++l) {
+      const size_t Nl = nodes(c->n[l]);
+      if (l >= 1 && l < c->L - 1) {
+        o.S[l] = dnew<T>(c, (size_t)B * 27 * DD * Nl);
+        o.Dinv[l] = dnew<T>(c, (size_t)B * DD * Nl);
+      }
+      if (l >= 1) o.F[l] = dnew<T>(c, (size_t)B * Nl * RD);
+      o.U[l][0] = dnew<T>(c, (size_t)B * Nl * RD);
+      o.U[l][1] = dnew<T>(c, (size_t)B * Nl * RD);
+      o.Dd[l] = dnew<T>(c, (size_t)B * Nl * RD);
+      o.Res[l] = dnew<T>(c, (size_t)B * Nl * RD);
+      o.hi[l] = dnew<double>(c, B);
+    }
+    o.x = dnew<T>(c, (size_t)B * N0 * RD);
+    o.r = dnew<T>(c, (size_t)B * N0 * RD);
+    o.p = dnew<T>(c, (size_t)B * N0 * RD);
+    o.q = dnew<T>(c, (size_t)B * N0 * RD);
+  }
+  o.alloc = true;
+}
+
+static void alloc_phys(maple_ctx* c, int phys) {
+  Phys& p = c->ph[phys];
+  if (p.alloc) return;
+  const int B = c->B, D = p.D, R = p.R, k = 8 * D;
+  const size_t N0 = nodes(c->n[0]);
+  for (int l = 1; l < c->L; ++l) p.KE[l] = dnew<double>(c, (size_t)B * nodes(c->n[l]) * k * k);
+  const int nc = c->n[c->L - 1], ndof = nodes(nc) * D;
+  p.S64c = dnew<double>(c, (size_t)B * 27 * D * D * nodes(nc));
+  p.Ainv = dnew<double>(c, (size_t)B * ndof * ndof);
+  p.cwork = dnew<double>(c, (size_t)B * ndof * ndof);
+  p.F64 = dnew<double>(c, (size_t)B * N0 * R * D);
+  p.u64 = dnew<double>(c, (size_t)B * N0 * R * D);
+  p.r64 = dnew<double>(c, (size_t)B * N0 * R * D);
+  p.energy = dnew<double>(c, (size_t)B * N0 * R * R);
+  p.H = dnew<double>(c, (size_t)B * R * R);
+  CK(cudaMemset(p.u64, 0, (size_t)B * N0 * R * D * sizeof(double)));
+  p.alloc = true;
+}
+
+template <typename T>
+static Ops<T>& ops(Phys& p);
+template <>
+Ops<double>& ops<double>(Phys& p) { return p.o64; }
+template <>
+Ops<float>& ops<float>(Phys& p) { return p.o32; }
+
+// ---------------------------------------------------------------------------
+// operator application dispatch
+// ---------------------------------------------------------------------------
+template <typename T, int D, int R, int MODE>
+static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const int* act, cudaStream_t s) {
+  a.n = c->n[l];
+  a.N = nodes(a.n);
+  a.scale = (T)p.kscale;
+  a.active = act;
+  a.ratio = c->cheb_ratio;
+  const dim3 g = g2(a.N, c->B);
+  if (l == 0) {
+    a.rho = o.rho;
+    k_apply_fine<T, D, R, MODE><<<g, kThreads, 0, s>>>(a);
+  } else {
+    a.S = o.S[l];
+    a.Dinv = o.Dinv[l];
+    k_apply_stencil<T, D, R, MODE><<<g, kThreads, 0, s>>>(a);
+  }
+  CKL();
+}
+
+template <int K>
+static void reduce(maple_ctx* c, const double* part, unsigned nb, double* out, cudaStream_t s) {
+  k_reduce_partials<K><<<c->B, kThreads, 0, s>>>(part, (int)nb, out);
+  CKL();
+}
+
+// ---------------------------------------------------------------------------
+// hierarchy
+// ---------------------------------------------------------------------------
+template <typename T, int D>
+static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
+  // level 0: the element bound holds for every density
+  std::vector<double> h0(c->B, g_tab.lam_elem[D == 3 ? 0 : 1]);
+  CK(cudaMemcpyAsync(o.hi[0], h0.data(), c->B * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  for (int l = 1; l < c->L - 1; ++l) {
+    const int Nl = nodes(c->n[l]);
+    T* v = o.U[l][0];
+    T* w = o.U[l][1];
+    k_power_init<T><<<nblk((size_t)c->B * Nl * D), kThreads, 0, s>>>(v, (size_t)c->B * Nl * D);
+    CKL();
+    for (int it = 0; it < c->power_iters; ++it) {
+      ApplyArgs<T> a{};
+      a.u = v;
+      a.out = w;
+      a.part = c->part;
+      apply<T, D, 1, M_POWER>(c, p, o, l, a, c->active, s);
+      std::swap(v, w);
+    }
+    reduce<2>(c, c->part, nblk(Nl), c->red, s);
+    k_power_finish<<<nblk(c->B), kThreads, 0, s>>>(c->red, o.hi[l], c->B, c->power_safety);
+    CKL();
+  }
+}
+
+template <int D>
+static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
+  Phys& p = c->ph[phys];
+  const int B = c->B, k = 8 * D, L = c->L;
+  const int* act = c->active;
+  // level-1 element matrices from the fine densities
+  {
+    const int nc = c->n[1];
+    const size_t tot = (size_t)nodes(nc) * k * k;
+    const double* M = nullptr;
+    static double* dM[128][2] = {};
+    int dev = c->dev;
+    if (!dM[dev][D == 3 ? 0 : 1]) {
+      std::lock_guard<std::mutex> lk(g_mu);
+      double* m = nullptr;
+      const size_t bytes = (size_t)8 * k * k * sizeof(double);
+      CK(cudaMalloc(&m, bytes));
+      CK(cudaMemcpy(m, D == 3 ? g_tab.M3 : g_tab.M1, bytes, cudaMemcpyHostToDevice));
+      dM[dev][D == 3 ? 0 : 1] = m;
+    }
+    M = dM[dev][D == 3 ? 0 : 1];
+    k_level1_elements<D><<<g2(tot, B), kThreads, 0, s>>>(p.o64.rho, M, p.KE[1], nc, p.kscale, act);
+    CKL();
+  }
+  for (int l = 1; l < L; ++l) {
+    const int n = c->n[l], N = nodes(n);
+    if (l < L - 1) {
+      if (prec == MAPLE_FP64) {
+        k_stencil_from_elements<double, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.KE[l], p.o64.S[l],
+                                                                                      p.o64.Dinv[l], nullptr, n, act);
+      } else {
+        k_stencil_from_elements<float, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.KE[l], p.o32.S[l],
+                                                                                     p.o32.Dinv[l], nullptr, n, act);
+      }
+      CKL();
+      // coarsen to the next level
+      const int nc = c->n[l + 1];
+      const size_t smem = (size_t)2 * 8 * k * k * sizeof(double);
+      CK(cudaFuncSetAttribute(k_coarsen_elements<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_coarsen_elements<D><<<dim3(nodes(nc), B), 256, smem, s>>>(p.KE[l], p.KE[l + 1], nc, act);
+      CKL();
+    } else {
+      const int ndof = N * D;
+      k_stencil_from_elements<double, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.KE[l], (double*)nullptr,
+                                                                                    (double*)nullptr, p.S64c, n, act);
+      CKL();
+      CK(cudaMemsetAsync(p.Ainv, 0, (size_t)B * ndof * ndof * sizeof(double), s));
+      k_dense_from_stencil<D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.S64c, p.Ainv, n, act);
+      CKL();
+      k_chol_inverse<<<B, 512, 0, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr);
+      CKL();
+    }
+  }
+  if (prec == MAPLE_FP64)
+    power_bounds<double, D>(c, p, p.o64, s);
+  else
+    power_bounds<float, D>(c, p, p.o32, s);
+  p.built = true;
+  p.built_prec = prec;
+  p.solved = false;
+  p.energies = false;
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle (symmetric: Chebyshev pre/post, exact FP64 coarsest solve)
+// ---------------------------------------------------------------------------
+template <typename T, int D, int R>
+static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const int* act, double* rz_part,
+                   cudaStream_t s) {
+  const int B = c->B;
+  if (l == c->L - 1) {
+    const int ndof = nodes(c->n[l]) * D;
+    k_coarse_solve<T, R><<<g2(ndof, B), kThreads, 0, s>>>(p.Ainv, f, o.U[l][1], ndof, D, act);
+    CKL();
+    return;
+  }
+  const int deg = c->cheb_degree;
+  int cur = 0;
+  {
+    ApplyArgs<T> a{};
+    a.f = f;
+    a.u = nullptr;
+    a.out = o.U[l][0];
+    a.din = o.Dd[l];
+    a.dout = o.Dd[l];
+    a.hi = o.hi[l];
+    a.step = 0;
+    apply<T, D, R, M_JAC0>(c, p, o, l, a, act, s);
+  }
+  for (int st = 1; st < deg; ++st) {
+    ApplyArgs<T> a{};
+    a.f = f;
+    a.u = o.U[l][cur];
+    a.out = o.U[l][1 - cur];
+    a.din = o.Dd[l];
+    a.dout = o.Dd[l];
+    a.hi = o.hi[l];
+    a.step = st;
+    apply<T, D, R, M_CHEB>(c, p, o, l, a, act, s);
+    cur ^= 1;
+  }
+  {
+    ApplyArgs<T> a{};
+    a.f = f;
+    a.u = o.U[l][cur];
+    a.out = o.Res[l];
+    apply<T, D, R, M_RES>(c, p, o, l, a, act, s);
+  }
+  const int nc = c->n[l + 1];
+  k_restrict<T, R * D><<<g2(nodes(nc), B), kThreads, 0, s>>>(o.Res[l], o.F[l + 1], nc, act);
+  CKL();
+  vcycle<T, D, R>(c, p, o, l + 1, o.F[l + 1], act, nullptr, s);
+  k_prolong_add<T, R * D><<<g2(nodes(c->n[l]), B), kThreads, 0, s>>>(o.U[l + 1][1], o.U[l][cur], nc, act);
+  CKL();
+  for (int st = 0; st < deg; ++st) {
+    ApplyArgs<T> a{};
+    a.f = f;
+    a.u = o.U[l][cur];
+    a.out = o.U[l][1 - cur];
+    a.din = o.Dd[l];
+    a.dout = o.Dd[l];
+    a.hi = o.hi[l];
+    a.step = st;
+    if (st == deg - 1 && rz_part) {
+      a.part = rz_part;
+      a.dot_f_out = 1;
+    }
+    apply<T, D, R, M_CHEB>(c, p, o, l, a, act, s);
+    cur ^= 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PCG on level 0 in precision T
+// ---------------------------------------------------------------------------
+static bool all_done(maple_ctx* c, const int* cell_done, const int* run_ref, cudaStream_t s) {
+  CK(cudaMemcpyAsync(c->h_flags, cell_done, c->B * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int b = 0; b < c->B; ++b)
+    if (!c->h_flags[b] && c->h_active[b]) return false;
+  return true;
+}
+
+__global__ void k_init_flags(const int* active, const int* outer_run, int* done, int* cell_done, int* run, int* iters,
+                             int B, int R) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const int a = (active ? active[b] : 1) && (outer_run ? outer_run[b] : 1);
+  run[b] = a;
+  cell_done[b] = a ? 0 : 1;
+  iters[b] = 0;
+  for (int r = 0; r < R; ++r) done[b * R + r] = a ? 0 : 1;
+}
+
+__global__ void k_sync_run(const int* cell_done, int* run, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  if (cell_done[b]) run[b] = 0;
+}
+
+__global__ void k_set_rz(double* rz, const double* rz_new, int total) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) rz[i] = rz_new[i];
+}
+
+template <typename T, int D, int R>
+static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, double rtol, int maxit,
+                const int* outer_run, cudaStream_t s) {
+  const int B = c->B, N = nodes(c->n[0]);
+  const size_t vbytes = (size_t)B * N * R * D * sizeof(T);
+  Scalars& sc = c->sc;
+  const unsigned nb = nblk(N);
+  PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
+  k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, outer_run, sc.done, sc.cell_done, sc.run, sc.iters, B, R);
+  CKL();
+  const int* run = sc.run;
+  // r = b - A x
+  if (x_zero) {
+    CK(cudaMemsetAsync(o.x, 0, vbytes, s));
+    CK(cudaMemcpyAsync(o.r, b, vbytes, cudaMemcpyDeviceToDevice, s));
+  } else {
+    ApplyArgs<T> a{};
+    a.u = o.x;
+    a.f = b;
+    a.out = o.r;
+    apply<T, D, R, M_RES>(c, p, o, 0, a, run, s);
+  }
+  k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, c->part, N, run);
+  CKL();
+  reduce<R>(c, c->part, nb, sc.bnorm2, s);
+  k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.r, o.r, c->part, N, run);
+  CKL();
+  reduce<R>(c, c->part, nb, sc.rr, s);
+  k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0);
+  CKL();
+  k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B);
+  CKL();
+  if (all_done(c, sc.cell_done, run, s)) return;
+  // z = M r ; rz ; p = z
+  vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, s);
+  reduce<R>(c, c->part, nb, sc.rz_new, s);
+  k_set_rz<<<nblk(B * R), kThreads, 0, s>>>(sc.rz, sc.rz_new, B * R);
+  CKL();
+  CK(cudaMemcpyAsync(o.p, o.U[0][1], vbytes, cudaMemcpyDeviceToDevice, s));
+  for (int it = 1; it <= maxit; ++it) {
+    {
+      ApplyArgs<T> a{};
+      a.u = o.p;
+      a.out = o.q;
+      a.part = c->part;
+      apply<T, D, R, M_MV>(c, p, o, 0, a, run, s);
+    }
+    reduce<R>(c, c->part, nb, sc.pq, s);
+    k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown);
+    CKL();
+    k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.x, o.r, o.p, o.q, sc.alpha, c->part, N, run);
+    CKL();
+    reduce<R>(c, c->part, nb, sc.rr, s);
+    k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, it);
+    CKL();
+    k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B);
+    CKL();
+    if (it == maxit) break;
+    if (it % c->check_every == 0 && all_done(c, sc.cell_done, run, s)) break;
+    vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, s);
+    reduce<R>(c, c->part, nb, sc.rz_new, s);
+    k_pcg_beta<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R);
+    CKL();
+    k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.p, o.U[0][1], sc.beta, N, run);
+    CKL();
+  }
+}
+
+// outer refinement bookkeeping: per (cell, rhs) residual scale and cell done
+__global__ void k_outer_check(const double* rr, const double* bn, double rtol2, double* scale, double* inv, int* done,
+                              int* run, const int* active, int B, int R) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  if (active && !active[b]) {
+    done[b] = 1;
+    run[b] = 0;
+    return;
+  }
+  int all = 1;
+  for (int r = 0; r < R; ++r) {
+    const double v = rr[b * R + r];
+    all &= (v <= rtol2 * bn[b * R + r]);
+    const double nrm = sqrt(v);
+    scale[b * R + r] = nrm > 0 ? 1.0 / nrm : 0.0;
+    inv[b * R + r] = nrm;
+  }
+  done[b] = all;
+  run[b] = !all;
+}
+
+template <int D, int R>
+static void solve_phys(maple_ctx* c, int phys, int prec, const double* F, double* x64, bool x_zero, double rtol,
+                       int maxit, int* iters_host, int* status_host, cudaStream_t s) {
+  Phys& p = c->ph[phys];
+  const int B = c->B, N = nodes(c->n[0]);
+  const unsigned nb = nblk(N);
+  const size_t vb64 = (size_t)B * N * R * D * sizeof(double);
+  std::vector<int> it_total(B, 0);
+  int conv_all = 0;
+  if (prec == MAPLE_FP64) {
+    Ops<double>& o = p.o64;
+    if (!x_zero) CK(cudaMemcpyAsync(o.x, x64, vb64, cudaMemcpyDeviceToDevice, s));
+    pcg<double, D, R>(c, p, o, F, x_zero, rtol, maxit, nullptr, s);
+    CK(cudaMemcpyAsync(x64, o.x, vb64, cudaMemcpyDeviceToDevice, s));
+    std::vector<int> it(B), cd(B);
+    CK(cudaMemcpyAsync(it.data(), c->sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(cd.data(), c->sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int b = 0; b < B; ++b) {
+      it_total[b] = it[b];
+      if (status_host) status_host[b] = cd[b] ? MAPLE_CELL_CONVERGED : MAPLE_CELL_MAXIT;
+    }
+  } else {
+    Ops<double>& o64 = p.o64;
+    Ops<float>& o = p.o32;
+    if (x_zero) CK(cudaMemsetAsync(x64, 0, vb64, s));
+    k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(F, F, c->part, N, c->active);
+    CKL();
+    reduce<R>(c, c->part, nb, c->o_bn, s);
+    bool converged = false;
+    for (int outer = 0; outer < 12; ++outer) {
+      ApplyArgs<double> a{};
+      a.u = x64;
+      a.f = F;
+      a.out = p.r64;
+      a.part = c->part;
+      apply<double, D, R, M_RES>(c, p, o64, 0, a, c->active, s);
+      reduce<R>(c, c->part, nb, c->o_rr, s);
+      k_outer_check<<<nblk(B), kThreads, 0, s>>>(c->o_rr, c->o_bn, rtol * rtol, c->o_scale, c->o_inv, c->o_done,
+                                                  c->o_run, c->active, B, R);
+      CKL();
+      if (all_done(c, c->o_done, nullptr, s)) {
+        converged = true;
+        break;
+      }
+      k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(p.r64, o.Res[0], c->o_scale, N, c->o_run);
+      CKL();
+      // inner solve: A d = r (unit-norm columns), d in o.x
+      pcg<float, D, R>(c, p, o, o.Res[0], true, c->inner_rtol, maxit, c->o_run, s);
+      k_add_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(x64, o.x, c->o_inv, N, c->o_run);
+      CKL();
+      std::vector<int> it(B);
+      CK(cudaMemcpyAsync(it.data(), c->sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (int b = 0; b < B; ++b) it_total[b] += it[b];
+    }
+    std::vector<int> od(B);
+    CK(cudaMemcpyAsync(od.data(), c->o_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int b = 0; b < B; ++b)
+      if (status_host) status_host[b] = od[b] ? MAPLE_CELL_CONVERGED : MAPLE_CELL_MAXIT;
+    (void)converged;
+  }
+  if (iters_host)
+    for (int b = 0; b < B; ++b) iters_host[b] = it_total[b];
+  (void)conv_all;
+}
+
+static void dispatch_solve(maple_ctx* c, int phys, int prec, const double* F, double* x64, bool x_zero, double rtol,
+                           int maxit, int* iters, int* status, cudaStream_t s) {
+  if (phys == MAPLE_ELASTIC)
+    solve_phys<3, 6>(c, phys, prec, F, x64, x_zero, rtol, maxit, iters, status, s);
+  else
+    solve_phys<1, 3>(c, phys, prec, F, x64, x_zero, rtol, maxit, iters, status, s);
+}
+
+static void ensure_prec(maple_ctx* c, int phys, int prec) {
+  Phys& p = c->ph[phys];
+  alloc_phys(c, phys);
+  alloc_ops<double>(c, p, p.o64, prec == MAPLE_FP64);
+  if (prec == MAPLE_MIXED) alloc_ops<float>(c, p, p.o32, true);
+}
+
+static void load_density(maple_ctx* c, int phys, const double* rho, int prec, cudaStream_t s) {
+  Phys& p = c->ph[phys];
+  const size_t tot = (size_t)c->B * nodes(c->n[0]);
+  k_copy_rho<<<nblk(tot), kThreads, 0, s>>>(rho, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot);
+  CKL();
+}
+
+static void build(maple_ctx* c, int phys, int prec, cudaStream_t s) {
+  if (phys == MAPLE_ELASTIC)
+    build_hierarchy<3>(c, phys, prec, s);
+  else
+    build_hierarchy<1>(c, phys, prec, s);
+}
+
+static void assemble_rhs(maple_ctx* c, int phys, const double* rho, double* F, cudaStream_t s) {
+  Phys& p = c->ph[phys];
+  const int N = nodes(c->n[0]);
+  if (phys == MAPLE_ELASTIC)
+    k_assemble_F<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(rho, F, c->n[0], p.fscale, c->active);
+  else
+    k_assemble_F<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(rho, F, c->n[0], p.fscale, c->active);
+  CKL();
+}
+
+static void homogenize(maple_ctx* c, int phys, cudaStream_t s) {
+  Phys& p = c->ph[phys];
+  const int N = nodes(c->n[0]);
+  const unsigned nb = nblk(N);
+  if (phys == MAPLE_ELASTIC) {
+    k_homogenize<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, c->part, c->n[0], p.kscale,
+                                                        p.xscale, c->active);
+    CKL();
+    reduce<21>(c, c->part, nb, c->red, s);
+    k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(c->red, p.H, c->B, 6);
+  } else {
+    k_homogenize<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, c->part, c->n[0], p.kscale,
+                                                        p.xscale, c->active);
+    CKL();
+    reduce<6>(c, c->part, nb, c->red, s);
+    k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(c->red, p.H, c->B, 3);
+  }
+  CKL();
+  p.energies = true;
+}
+
+static void oc_update(maple_ctx* c, const double* x, const double* dJ, const double* vf, double move, double xmin,
+                      double* xnew, double* stats, cudaStream_t s) {
+  const int N = nodes(c->n[0]);
+  int per_sm = 0, sms = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oc_update, kThreads, 0));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
+  const int maxres = per_sm * sms;
+  require(maxres >= 1, "OC kernel cannot be resident");
+  // cells per launch and blocks per cell
+  const int want_G = std::max(1, std::min(sms, (N + 4 * kThreads - 1) / (4 * kThreads)));
+  int cells_per_launch = std::max(1, std::min(c->B, maxres / want_G));
+  for (int c0 = 0; c0 < c->B; c0 += cells_per_launch) {
+    const int nb = std::min(cells_per_launch, c->B - c0);
+    const int G = std::max(1, std::min(want_G, maxres / nb));
+    OcArgs a{};
+    a.x = x + (size_t)c0 * N;
+    a.dJ = dJ + (size_t)c0 * N;
+    a.xnew = xnew + (size_t)c0 * N;
+    a.volfrac = vf + c0;
+    a.move = move;
+    a.xmin = xmin;
+    a.N = N;
+    a.part = c->ocpart;
+    a.stats = stats ? stats + 2 * c0 : c->stats + 2 * c0;
+    a.lam_out = nullptr;
+    a.bar = c->bar;
+    a.err = c->err;
+    a.active = c->active ? c->active + c0 : nullptr;
+    CK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned), s));
+    void* args[] = {&a};
+    CK(cudaLaunchCooperativeKernel((void*)k_oc_update, dim3(G, nb), dim3(kThreads), args, 0, s));
+  }
+}
+
+}  // namespace maple
+
+using namespace maple;
+
+template <typename F>
+static int guarded(F&& f) {
+  try {
+    f();
+    return MAPLE_OK;
+  } catch (const Failure& e) {
+    g_err = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return MAPLE_E_CUDA;
+  }
+}
+
+static cudaStream_t S(maple_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+extern "C" {
+
+const char* maple_last_error_string(void) { return g_err.c_str(); }
+int maple_version(void) { return 100; }
+
+int maple_element_matrices(int r, double E, double nu, double kappa, double* Ke3, double* Fe3, double* X03,
+                           double* Ke1, double* Fe1, double* X01) {
+  return guarded([&] {
+    require(r >= 1, "resolution must be positive");
+    ElementTables t;
+    element_tables(E, nu, kappa, &t);
+    const double h = 1.0 / r;
+    for (int i = 0; i < 576; ++i) if (Ke3) Ke3[i] = t.Ke3[i] * h;
+    for (int i = 0; i < 144; ++i) {
+      if (Fe3) Fe3[i] = t.Fe3[i] * h * h;
+      if (X03) X03[i] = t.X03[i] * h;
+    }
+    for (int i = 0; i < 64; ++i) if (Ke1) Ke1[i] = t.Ke1[i] * h;
+    for (int i = 0; i < 24; ++i) {
+      if (Fe1) Fe1[i] = t.Fe1[i] * h * h;
+      if (X01) X01[i] = t.X01[i] * h;
+    }
+  });
+}
+
+int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double kappa, maple_ctx** out) {
+  return guarded([&] {
+    require(out != nullptr, "out is NULL");
+    *out = nullptr;
+    require(r >= 6 && r % 2 == 0, "resolution must be even and >= 6");
+    require(ncells >= 1 && ncells <= 65535, "ncells must be in [1, 65535]");
+    require((size_t)r * r * r * 27 < (size_t)1 << 31, "resolution too large");
+    require(E > 0 && kappa > 0 && nu > -1.0 && nu < 0.5, "invalid material constants");
+    ensure_tables(nu);
+    maple_ctx* c = new maple_ctx();
+    try {
+      CK(cudaGetDevice(&c->dev));
+      c->r = r;
+      c->B = ncells;
+      c->E = E;
+      c->nu = nu;
+      c->kappa = kappa;
+      // levels: coarsen while the grid stays even and the coarse grid has n >= 3
+      int n = r, L = 1;
+      c->n[0] = r;
+      const int maxL = levels > 0 ? std::min(levels, kMaxLevels) : kMaxLevels;
+      while (L < maxL && n % 2 == 0 && n / 2 >= 3 && (levels > 0 || n > 4)) {
+        n /= 2;
+        c->n[L++] = n;
+      }
+      require(L >= 2, "resolution admits no coarse level");
+      require(nodes(n) * 3 <= 1536, "coarsest grid too large for the dense FP64 solve; use more levels");
+      c->L = L;
+      const double h = 1.0 / r;
+      c->ph[0].D = 3;
+      c->ph[0].R = 6;
+      c->ph[0].kscale = E * h;
+      c->ph[0].fscale = E * h * h;
+      c->ph[0].xscale = h;
+      c->ph[1].D = 1;
+      c->ph[1].R = 3;
+      c->ph[1].kscale = kappa * h;
+      c->ph[1].fscale = kappa * h * h;
+      c->ph[1].xscale = h;
+      const int B = ncells;
+      const size_t N0 = nodes(r);
+      c->part = dnew<double>(c, (size_t)B * nblk(N0) * 32);
+      c->red = dnew<double>(c, (size_t)B * 32);
+      c->sc.rz = dnew<double>(c, B * 6);
+      c->sc.rz_new = dnew<double>(c, B * 6);
+      c->sc.pq = dnew<double>(c, B * 6);
+      c->sc.rr = dnew<double>(c, B * 6);
+      c->sc.bnorm2 = dnew<double>(c, B * 6);
+      c->sc.alpha = dnew<double>(c, B * 6);
+      c->sc.beta = dnew<double>(c, B * 6);
+      c->sc.done = dnew<int>(c, B * 6);
+      c->sc.cell_done = dnew<int>(c, B);
+      c->sc.iters = dnew<int>(c, B);
+      c->sc.run = dnew<int>(c, B);
+      c->o_rr = dnew<double>(c, B * 6);
+      c->o_bn = dnew<double>(c, B * 6);
+      c->o_scale = dnew<double>(c, B * 6);
+      c->o_inv = dnew<double>(c, B * 6);
+      c->o_done = dnew<int>(c, B);
+      c->o_run = dnew<int>(c, B);
+      c->breakdown = dnew<int>(c, 1);
+      c->active = dnew<int>(c, B);
+      c->h_active.assign(B, 1);
+      CK(cudaMemcpy(c->active, c->h_active.data(), B * sizeof(int), cudaMemcpyHostToDevice));
+      CK(cudaMallocHost(&c->h_flags, B * sizeof(int)));
+      c->x_rho = dnew<double>(c, (size_t)B * N0);
+      c->dJdx = dnew<double>(c, (size_t)B * N0);
+      c->dJf = dnew<double>(c, (size_t)B * N0);
+      c->Jv = dnew<double>(c, B);
+      c->terms = dnew<double>(c, B * 3);
+      c->G3 = dnew<double>(c, B * 36);
+      c->G1 = dnew<double>(c, B * 9);
+      c->stats = dnew<double>(c, B * 2);
+      c->ocvf = dnew<double>(c, B);
+      int sms = 0;
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
+      c->ocpart = dnew<double>(c, (size_t)4 * std::max(B, 1) * std::max(sms, 1) * 8);
+      c->bar = dnew<unsigned>(c, 2);
+      c->err = dnew<int>(c, 1);
+      CK(cudaMemset(c->err, 0, sizeof(int)));
+      CK(cudaMemset(c->breakdown, 0, sizeof(int)));
+    } catch (...) {
+      for (void* p : c->allocs) cudaFree(p);
+      if (c->h_flags) cudaFreeHost(c->h_flags);
+      delete c;
+      throw;
+    }
+    *out = c;
+  });
+}
+
+int maple_ctx_destroy(maple_ctx* c) {
+  return guarded([&] {
+    if (!c) return;
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->h_flags) cudaFreeHost(c->h_flags);
+    delete c;
+  });
+}
+
+int maple_ctx_info(const maple_ctx* c, int* levels, int* coarsest, size_t* bytes) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    if (levels) *levels = c->L;
+    if (coarsest) *coarsest = c->n[c->L - 1];
+    if (bytes) *bytes = c->bytes;
+  });
+}
+
+int maple_set_solver_options(maple_ctx* c, int deg, double ratio, int piters, double inner_rtol, int check_every) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(deg >= 1 && deg <= 8, "chebyshev degree must be in [1, 8]");
+    require(ratio > 1.0, "chebyshev ratio must exceed 1");
+    require(piters >= 1 && piters <= 100, "power iterations must be in [1, 100]");
+    require(inner_rtol > 0 && inner_rtol < 1, "inner tolerance must be in (0, 1)");
+    require(check_every >= 1, "check_every must be >= 1");
+    c->cheb_degree = deg;
+    c->cheb_ratio = ratio;
+    c->power_iters = piters;
+    c->inner_rtol = inner_rtol;
+    c->check_every = check_every;
+  });
+}
+
+int maple_set_active(maple_ctx* c, const int* act, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    for (int b = 0; b < c->B; ++b) c->h_active[b] = act ? (act[b] != 0) : 1;
+    CK(cudaMemcpyAsync(c->active, c->h_active.data(), c->B * sizeof(int), cudaMemcpyHostToDevice, S(s)));
+    CK(cudaStreamSynchronize(S(s)));
+  });
+}
+
+int maple_set_density(maple_ctx* c, int phys, const double* rho, int prec, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && rho != nullptr, "NULL argument");
+    require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
+    require(prec == MAPLE_FP64 || prec == MAPLE_MIXED, "unknown precision");
+    ensure_prec(c, phys, prec);
+    load_density(c, phys, rho, prec, S(s));
+    build(c, phys, prec, S(s));
+  });
+}
+
+int maple_solve(maple_ctx* c, int phys, int prec, double rtol, int maxit, int warm, int* iters, int* status,
+                maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
+    Phys& p = c->ph[phys];
+    require(p.built, "maple_set_density must be called before maple_solve");
+    require(p.built_prec == prec, "precision differs from the one the hierarchy was built for");
+    require(rtol > 0 && maxit >= 1, "rtol must be > 0 and maxit >= 1");
+    assemble_rhs(c, phys, p.o64.rho, p.F64, S(s));
+    dispatch_solve(c, phys, prec, p.F64, p.u64, !(warm && p.solved), rtol, maxit, iters, status, S(s));
+    p.solved = true;
+    p.energies = false;
+  });
+}
+
+int maple_solve_rhs(maple_ctx* c, int phys, int prec, const double* F, const double* x0, double rtol, int maxit,
+                    double* u_out, double* r_out, int* iters, int* status, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && F != nullptr && u_out != nullptr, "NULL argument");
+    require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
+    Phys& p = c->ph[phys];
+    require(p.built && p.built_prec == prec, "maple_set_density (same precision) must precede maple_solve_rhs");
+    const size_t vb = (size_t)c->B * nodes(c->n[0]) * p.R * p.D * sizeof(double);
+    if (x0) CK(cudaMemcpyAsync(u_out, x0, vb, cudaMemcpyDeviceToDevice, S(s)));
+    dispatch_solve(c, phys, prec, F, u_out, x0 == nullptr, rtol, maxit, iters, status, S(s));
+    if (r_out) {
+      ApplyArgs<double> a{};
+      a.u = u_out;
+      a.f = F;
+      a.out = r_out;
+      if (phys == MAPLE_ELASTIC)
+        apply<double, 3, 6, M_RES>(c, p, p.o64, 0, a, c->active, S(s));
+      else
+        apply<double, 1, 3, M_RES>(c, p, p.o64, 0, a, c->active, S(s));
+    }
+  });
+}
+
+int maple_get_solution(maple_ctx* c, int phys, double* u_out, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && u_out != nullptr, "NULL argument");
+    Phys& p = c->ph[phys];
+    require(p.solved, "no solution available");
+    const size_t vb = (size_t)c->B * nodes(c->n[0]) * p.R * p.D * sizeof(double);
+    CK(cudaMemcpyAsync(u_out, p.u64, vb, cudaMemcpyDeviceToDevice, S(s)));
+  });
+}
+
+int maple_homogenize(maple_ctx* c, int phys, double* H_out, double* energy_out, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
+    Phys& p = c->ph[phys];
+    require(p.solved, "maple_solve must precede maple_homogenize");
+    homogenize(c, phys, S(s));
+    if (H_out) CK(cudaMemcpyAsync(H_out, p.H, (size_t)c->B * p.R * p.R * sizeof(double), cudaMemcpyDeviceToDevice, S(s)));
+    if (energy_out)
+      CK(cudaMemcpyAsync(energy_out, p.energy, (size_t)c->B * nodes(c->n[0]) * p.R * p.R * sizeof(double),
+                         cudaMemcpyDeviceToDevice, S(s)));
+  });
+}
+
+int maple_energy_contract(int ncells, int N, int RR, const double* energy, const double* g, int accumulate,
+                          double* out, maple_stream_t s) {
+  return guarded([&] {
+    require(energy && g && out, "NULL argument");
+    require(ncells >= 1 && N >= 1 && (RR == 36 || RR == 9), "bad sizes");
+    k_energy_contract<<<g2(N, ncells), kThreads, 0, S(s)>>>(energy, g, out, N, RR, accumulate);
+    CKL();
+  });
+}
+
+int maple_sensitivity(maple_ctx* c, const double* gC, const double* gK, double* dJdrho, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && dJdrho != nullptr, "NULL argument");
+    require(gC || gK, "at least one of gC, gK is required");
+    if (gC) require(c->ph[0].energies, "elastic energies missing: call maple_homogenize first");
+    if (gK) require(c->ph[1].energies, "thermal energies missing: call maple_homogenize first");
+    const int N = nodes(c->n[0]);
+    k_sensitivity<<<g2(N, c->B), kThreads, 0, S(s)>>>(nullptr, gC ? c->ph[0].energy : nullptr,
+                                                       gK ? c->ph[1].energy : nullptr, gC, gK, nullptr, dJdrho, N, 0, 1,
+                                                       0, c->active);
+    CKL();
+  });
+}
+
+int maple_assemble_rhs(maple_ctx* c, int phys, const double* rho, double* F, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && rho != nullptr && F != nullptr, "NULL argument");
+    require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
+    assemble_rhs(c, phys, rho, F, S(s));
+  });
+}
+
+int maple_matvec(maple_ctx* c, int phys, const double* rho, const double* u, double* y, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && rho != nullptr && u != nullptr && y != nullptr, "NULL argument");
+    require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
+    Phys& p = c->ph[phys];
+    Ops<double> o{};
+    o.rho = const_cast<double*>(rho);
+    ApplyArgs<double> a{};
+    a.u = u;
+    a.out = y;
+    if (phys == MAPLE_ELASTIC)
+      apply<double, 3, 6, M_MV>(c, p, o, 0, a, c->active, S(s));
+    else
+      apply<double, 1, 3, M_MV>(c, p, o, 0, a, c->active, S(s));
+  });
+}
+
+int maple_box_filter(int r, int ncells, int k, const double* in, double* out, maple_stream_t s) {
+  return guarded([&] {
+    require(in != nullptr && out != nullptr, "NULL argument");
+    require(k > 0 && k % 2 == 1, "filter size must be a positive odd integer");
+    require(r >= 1 && ncells >= 1, "bad sizes");
+    require(in != out, "in-place filtering is not supported");
+    k_box_filter<<<g2((size_t)r * r * r, ncells), kThreads, 0, S(s)>>>(in, out, r, k, nullptr);
+    CKL();
+  });
+}
+
+int maple_oc_update(maple_ctx* c, const double* x, const double* dJdx, const double* vf, double move, double xmin,
+                    double* xnew, double* stats, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && x && dJdx && vf && xnew, "NULL argument");
+    require(xnew != x, "xnew must not alias x");
+    oc_update(c, x, dJdx, vf, move, xmin, xnew, stats, S(s));
+  });
+}
+
+int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* vf, double penal, double rho_min,
+                  double move, double xmin, int filter_k, int prec, double rtol, int maxit, int warm, double* x_next,
+                  double* J, double* terms, double* CH, double* kappa, double* stats, int* iters, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && x && w && vf && x_next, "NULL argument");
+    require(x_next != x, "x_next must not alias x");
+    require(prec == MAPLE_FP64 || prec == MAPLE_MIXED, "unknown precision");
+    cudaStream_t st = S(s);
+    const int B = c->B, N = nodes(c->n[0]);
+    std::vector<double> hw(3 * B);
+    CK(cudaMemcpyAsync(hw.data(), w, 3 * B * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    bool need_ch = false, need_k = false;
+    for (int b = 0; b < B; ++b) {
+      if (!c->h_active[b]) continue;
+      need_ch |= (hw[3 * b] != 0.0 || hw[3 * b + 1] != 0.0);
+      need_k |= (hw[3 * b + 2] != 0.0);
+    }
+    std::vector<int> it_tmp(B, 0), it_sum(B, 0);
+    for (int phys = 0; phys < 2; ++phys) {
+      if ((phys == 0 && !need_ch) || (phys == 1 && !need_k)) {
+        c->ph[phys].energies = false;
+        continue;
+      }
+      Phys& p = c->ph[phys];
+      ensure_prec(c, phys, prec);
+      const size_t tot = (size_t)B * N;
+      k_simp<<<nblk(tot), kThreads, 0, st>>>(x, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot, N, xmin,
+                                             penal, rho_min, c->active);
+      CKL();
+      build(c, phys, prec, st);
+      assemble_rhs(c, phys, p.o64.rho, p.F64, st);
+      const bool was_solved = p.solved;
+      dispatch_solve(c, phys, prec, p.F64, p.u64, !(warm && was_solved), rtol, maxit, it_tmp.data(), nullptr, st);
+      p.solved = true;
+      for (int b = 0; b < B; ++b) it_sum[b] += it_tmp[b];
+      homogenize(c, phys, st);
+    }
+    k_objective<<<nblk(B), kThreads, 0, st>>>(c->ph[0].H, c->ph[1].H, w, c->Jv, c->terms, c->G3, c->G1, B,
+                                              need_ch ? 1 : 0, need_k ? 1 : 0, c->active);
+    CKL();
+    k_sensitivity<<<g2(N, B), kThreads, 0, st>>>(x, need_ch ? c->ph[0].energy : nullptr,
+                                                 need_k ? c->ph[1].energy : nullptr, c->G3, c->G1, c->dJdx, nullptr, N,
+                                                 xmin, penal, rho_min, c->active);
+    CKL();
+    const double* dJ = c->dJdx;
+    if (filter_k > 1) {
+      require(filter_k % 2 == 1, "filter size must be odd");
+      k_box_filter<<<g2(N, B), kThreads, 0, st>>>(c->dJdx, c->dJf, c->n[0], filter_k, c->active);
+      CKL();
+      dJ = c->dJf;
+    }
+    oc_update(c, x, dJ, vf, move, xmin, x_next, c->stats, st);
+    if (J) CK(cudaMemcpyAsync(J, c->Jv, B * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (terms) CK(cudaMemcpyAsync(terms, c->terms, 3 * B * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (CH && need_ch) CK(cudaMemcpyAsync(CH, c->ph[0].H, 36 * B * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (kappa && need_k) CK(cudaMemcpyAsync(kappa, c->ph[1].H, 9 * B * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (stats) CK(cudaMemcpyAsync(stats, c->stats, 2 * B * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (iters)
+      for (int b = 0; b < B; ++b) iters[b] = it_sum[b];
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,77 @@
+"""``GMGSolver`` / ``GMGSolverScalar``: drop-ins for the reference's element-by-
+element multigrid solvers (``maple/core/utils/EBE_GMG.py:466-984`` and
+``EBE_GMG_scalar.py:343-832``).
+
+``solve(fine_ke, global_f, node_coords_L0, fine_elem_coords,
+fine_topo_indices, ...)`` keeps its signature and returns ``(u, r)``.  The
+operator must be the periodic structured cell the reference builds with
+``build_unitcell_batch`` and ``Ke_e = rho_e * Ke0`` (utils/model.py:108); the
+densities are recovered from ``fine_ke`` and checked.  The solve runs MG-PCG
+on the GPU to ``rtol`` (keyword, default 1e-10) instead of a fixed number of
+V-cycles; ``max_iter`` is honoured as a lower bound of the PCG iteration cap.
+The converged u may differ from the reference's by a rigid translation (the
+periodic operator's null space), which leaves C^H unchanged.
+``init_list`` may carry a dense level-0 initial guess (a tensor of the shape
+of ``global_f``); per-level sparse (spconv) initial fields are not supported.
+"""
+from __future__ import annotations
+
+import torch
+import torch.nn as nn
+
+from .core import element_matrices
+from .utils import cached_context, cube_root
+
+
+class GMGSolver(nn.Module):
+    D, R, PHYSICS = 3, 6, "elastic"
+
+    def _reference_ke(self, r):
+        Ke3, _, _, Ke1, _, _ = element_matrices(r)
+        return Ke3 if self.D == 3 else Ke1
+
+    def solve(self, fine_ke, global_f, node_coords_L0, fine_elem_coords, fine_topo_indices, max_iter: int = 50,
+              smooth_iter=1, init_list=None, init_batch=None, init_feat_slice=slice(0, 3),
+              init_is_solution: bool = False, max_levels: int = 5, fixed_mask=None, dtype=torch.float, *,
+              rtol: float = 1e-10, precision: str = "fp64"):
+        if fixed_mask is not None:
+            raise NotImplementedError("fixed_mask: periodic unit cells have no Dirichlet DOFs")
+        D = self.D
+        f = global_f.reshape(-1, D)
+        n = f.shape[0]
+        r = cube_root(n)
+        if r < 0:
+            raise ValueError(f"{n} nodes do not form a periodic r^3 cell")
+        k = 8 * D
+        if fine_ke.shape != (n, k, k):
+            raise ValueError(f"fine_ke must be ({n},{k},{k}), got {tuple(fine_ke.shape)}")
+        dev = fine_ke.device
+        Kref = torch.tensor(self._reference_ke(r), dtype=torch.float64, device=dev)
+        ke64 = fine_ke.detach().to(torch.float64)
+        rho = (ke64 * Kref).sum(dim=(1, 2)) / (Kref * Kref).sum()
+        err = (ke64 - rho[:, None, None] * Kref).abs().max()
+        tol = 1e-5 * ke64.abs().max() if fine_ke.dtype == torch.float32 else 1e-10 * ke64.abs().max()
+        if float(err) > float(tol):
+            raise ValueError("fine_ke is not rho_e * Ke0 of this resolution: only SIMP-scaled copies of the "
+                             "voxel element matrix are supported")
+        ctx = cached_context(r, dev)
+        ctx.set_density(self.PHYSICS, rho.reshape(1, n).contiguous(), precision)
+        F = torch.zeros((1, n, self.R, D), dtype=torch.float64, device=ctx.device)
+        F[0, :, 0, :] = f.to(device=ctx.device, dtype=torch.float64)
+        x0 = None
+        if init_list is not None:
+            if isinstance(init_list, torch.Tensor) and init_list.numel() == n * D:
+                x0 = torch.zeros_like(F)
+                x0[0, :, 0, :] = init_list.reshape(n, D).to(device=ctx.device, dtype=torch.float64)
+            else:
+                raise NotImplementedError("init_list: only a dense level-0 tensor shaped like global_f is supported")
+        u, res, _ = ctx.solve_rhs(self.PHYSICS, F, x0, precision=precision, rtol=rtol, maxit=max(int(max_iter), 500))
+        out_u = u[0, :, 0, :].to(device=dev, dtype=dtype)
+        out_r = res[0, :, 0, :].to(device=dev, dtype=dtype)
+        if D == 1:
+            return out_u.reshape(n, 1), out_r.reshape(n, 1)
+        return out_u, out_r
+
+
+class GMGSolverScalar(GMGSolver):
+    D, R, PHYSICS = 1, 3, "thermal"

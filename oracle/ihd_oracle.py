@@ -1,0 +1,566 @@
+"""FP64 CPU oracle for MAPLE's inverse-homogenization inner loop.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: only ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference``
+legs of ``bench.py`` may import it.  The product path (``maple_b200``) never
+calls it and fails loudly when its CUDA library is missing.
+
+It restates, in numpy/scipy FP64, the algorithm of the reference package
+``maple`` (xing-yuu/MAPLE, ``src/maple``).  Each function cites the reference
+file:line it follows.  Paths are relative to ``src/maple/core``.
+
+Parity pin: ``tests/golden/make_golden.py`` runs the reference's own code
+(imported from its source tree, FP64 element matrices, converged V-cycles,
+autograd sensitivities) and stores the results as ``tests/golden/*.npz``;
+``tests/test_oracle_golden.py`` checks this module against them.
+
+Conventions (same as the reference):
+  * ``r`` voxels per axis, ``N = r**3`` elements = nodes (periodic cell).
+  * element / node id ``x*r*r + y*r + z`` (main_IHD_v3.py:175-186).
+  * element-local node order ``000,100,110,010,001,101,111,011``
+    (main_IHD_v3.py:189-193).
+  * DOF id ``3*node + c`` (EBE_GMG.py:796); Voigt order xx,yy,zz,xy,yz,zx
+    (utils/_utils.py:91-100).
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+# element-local corner offsets (main_IHD_v3.py:189-193, EBE_GMG.py:480-489)
+HEX8 = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                 [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], dtype=np.int64)
+_SIGNS = 2 * HEX8 - 1                                   # (8,3) in {-1,+1}
+_GP = np.array([-np.sqrt(3.0 / 5.0), 0.0, np.sqrt(3.0 / 5.0)])
+_GW = np.array([5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0])
+ELASTIC_FIXED_DOFS = (0, 1, 2, 4, 5, 11)                # utils/_utils.py:105-106
+
+
+# ---------------------------------------------------------------------------
+# element matrices
+# ---------------------------------------------------------------------------
+def isotropic_elastic_tensor(E: float = 1.0, nu: float = 0.3, f32_entries: bool = True) -> np.ndarray:
+    """6x6 isotropic stiffness in Voigt form (utils/_utils.py:39-48).
+
+    The reference builds it with ``torch.as_tensor`` of Python floats, i.e. in
+    float32 (utils/_utils.py:42), and every FP64 use of it casts those float32
+    values up.  ``f32_entries`` reproduces that rounding of lambda+2mu, lambda,
+    mu (a 1e-8 relative effect on every element matrix)."""
+    lam = nu / (1.0 + nu) / (1.0 - 2.0 * nu) * E
+    mu = 1.0 / (2.0 * (1.0 + nu)) * E
+    if f32_entries:
+        lam2mu = float(np.float32(lam + 2 * mu))
+        lam, mu = float(np.float32(lam)), float(np.float32(mu))
+    else:
+        lam2mu = lam + 2 * mu
+    C = np.zeros((6, 6))
+    C[:3, :3] = lam
+    C[np.arange(3), np.arange(3)] = lam2mu
+    C[np.arange(3, 6), np.arange(3, 6)] = mu
+    return C
+
+
+def _shape_grads(xi, eta, zeta):
+    """d N_a / d(xi,eta,zeta) for the 8 trilinear corners, shape (3,8)."""
+    s = _SIGNS
+    g = np.empty((3, 8))
+    g[0] = s[:, 0] * (1 + s[:, 1] * eta) * (1 + s[:, 2] * zeta) / 8.0
+    g[1] = s[:, 1] * (1 + s[:, 0] * xi) * (1 + s[:, 2] * zeta) / 8.0
+    g[2] = s[:, 2] * (1 + s[:, 0] * xi) * (1 + s[:, 1] * eta) / 8.0
+    return g
+
+
+def _gauss_points():
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                yield _GP[i], _GP[j], _GP[k], _GW[i] * _GW[j] * _GW[k]
+
+
+def hexahedron(r: int, C: np.ndarray):
+    """Ke0 (24,24), Fe0 (24,6), X0 (24,6) of one voxel of edge 1/r.
+
+    3x3x3 Gauss quadrature of B^T C B and B^T C; X0 solves Ke0 X0 = Fe0 with
+    DOFs 0,1,2,4,5,11 pinned to zero (utils/_utils.py:49-109).
+    """
+    h = 1.0 / r / 2.0
+    corners = _SIGNS * h                                  # (8,3) physical coords
+    Ke = np.zeros((24, 24))
+    Fe = np.zeros((24, 6))
+    for xi, eta, zeta, w in _gauss_points():
+        dN = _shape_grads(xi, eta, zeta)                  # (3,8)
+        J = dN @ corners
+        dNx = np.linalg.solve(J, dN)                      # (3,8)
+        B = np.zeros((6, 24))
+        for a in range(8):
+            gx, gy, gz = dNx[:, a]
+            c = 3 * a
+            B[0, c] = gx
+            B[1, c + 1] = gy
+            B[2, c + 2] = gz
+            B[3, c], B[3, c + 1] = gy, gx
+            B[4, c + 1], B[4, c + 2] = gz, gy
+            B[5, c], B[5, c + 2] = gz, gx
+        wd = np.linalg.det(J) * w
+        Ke += wd * B.T @ C @ B
+        Fe += wd * B.T @ C
+    free = np.ones(24, dtype=bool)
+    free[list(ELASTIC_FIXED_DOFS)] = False
+    X0 = np.zeros((24, 6))
+    X0[free] = np.linalg.solve(Ke[np.ix_(free, free)], Fe[free])
+    return Ke, Fe, X0
+
+
+def hexahedron_scalar(r: int, kappa: float = 1.0):
+    """Ke0 (8,8), Fe0 (8,3), X0 (8,3) for scalar conduction, node 0 anchored
+    (utils/_utils.py:116-196)."""
+    h = 1.0 / r / 2.0
+    corners = _SIGNS * h
+    Ke = np.zeros((8, 8))
+    Fe = np.zeros((8, 3))
+    for xi, eta, zeta, w in _gauss_points():
+        dN = _shape_grads(xi, eta, zeta)
+        J = dN @ corners
+        G = np.linalg.solve(J, dN)                        # (3,8)
+        wd = np.linalg.det(J) * w * kappa
+        Ke += wd * G.T @ G
+        Fe += wd * G.T
+    X0 = np.zeros((8, 3))
+    X0[1:] = np.linalg.solve(Ke[1:, 1:], Fe[1:])
+    return Ke, Fe, X0
+
+
+class Elements:
+    """Element matrices of both physics at resolution r (model.py:18-28)."""
+
+    def __init__(self, r: int, E: float = 1.0, nu: float = 0.3, kappa: float = 1.0):
+        self.r = r
+        self.C = isotropic_elastic_tensor(E, nu)
+        self.Ke3, self.Fe3, self.X03 = hexahedron(r, self.C)
+        self.Ke1, self.Fe1, self.X01 = hexahedron_scalar(r, kappa)
+
+    def get(self, d: int):
+        return (self.Ke3, self.Fe3, self.X03) if d == 3 else (self.Ke1, self.Fe1, self.X01)
+
+
+# ---------------------------------------------------------------------------
+# structured periodic grid
+# ---------------------------------------------------------------------------
+def grid_coords(n: int) -> np.ndarray:
+    g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1)
+    return g.reshape(-1, 3)
+
+
+def node_index(n: int) -> np.ndarray:
+    """Periodic element->node table (N,8) (main_IHD_v3.py:174-197)."""
+    g = grid_coords(n)
+    c = (g[:, None, :] + HEX8[None]) % n
+    return (c[..., 0] * n + c[..., 1]) * n + c[..., 2]
+
+
+def dof_index(n: int, d: int) -> np.ndarray:
+    ni = node_index(n)
+    return (ni[:, :, None] * d + np.arange(d)[None, None]).reshape(ni.shape[0], 8 * d)
+
+
+def assemble_F(rho: np.ndarray, Fe: np.ndarray, n: int, d: int) -> np.ndarray:
+    """F = sum_e rho_e Fe0 scattered to nodes -> (N*d, R)
+    (utils/_utils.py:453-507, assemble_F_fast / assemble_F_fast_scalar)."""
+    di = dof_index(n, d)
+    R = Fe.shape[1]
+    F = np.zeros((n ** 3 * d, R))
+    vals = rho.reshape(-1, 1, 1) * Fe[None]
+    np.add.at(F, di.reshape(-1), vals.reshape(-1, R))
+    return F
+
+
+def assemble_K(ke: np.ndarray, n: int, d: int) -> sp.csr_matrix:
+    """Assembled operator of per-element matrices ke (M,8d,8d) on an n^3
+    periodic grid: the EBE matvec of EBE_GMG.py:412-430 as a sparse matrix."""
+    di = dof_index(n, d)
+    k = 8 * d
+    rows = np.repeat(di, k, axis=1).reshape(-1)
+    cols = np.tile(di, (1, k)).reshape(-1)
+    K = sp.coo_matrix((ke.reshape(-1), (rows, cols)), shape=(n ** 3 * d,) * 2).tocsr()
+    K.sum_duplicates()
+    return K
+
+
+def _child_prolongation():
+    """Per child c of a coarse element, the 8x8 trilinear weights from the
+    coarse corners to the child's corners (EBE_GMG.py:202-224, 226-337)."""
+    out = np.zeros((8, 8, 8))
+    for c in range(8):
+        co = np.array([(c >> 2) & 1, (c >> 1) & 1, c & 1])
+        for a in range(8):
+            p = co + HEX8[a]                                # position in {0,1,2}^3
+            for b in range(8):
+                out[c, a, b] = np.prod(1.0 - np.abs(p / 2.0 - HEX8[b]))
+    return out
+
+
+_PCHILD = _child_prolongation()
+
+
+def coarsen_elements(ke: np.ndarray, n: int, d: int) -> np.ndarray:
+    """Galerkin coarse element matrices  Kc_E = sum_children P_c^T K_c P_c
+    (EBE_GMG.py:226-337 / EBE_GMG_scalar.py:135-230).  Equivalent to
+    P_loc^T K_patch P_loc because each child's corners interpolate only from
+    the coarse element's own corners."""
+    nc = n // 2
+    g = grid_coords(n)
+    cid = ((g[:, 0] // 2) * nc + g[:, 1] // 2) * nc + g[:, 2] // 2
+    child = (g[:, 0] % 2) * 4 + (g[:, 1] % 2) * 2 + (g[:, 2] % 2)
+    k = 8 * d
+    out = np.zeros((nc ** 3, k, k))
+    I = np.eye(d)
+    for c in range(8):
+        Pc = np.kron(_PCHILD[c], I)                          # (8d, 8d)
+        m = child == c
+        contrib = np.einsum("ai,eab,bj->eij", Pc, ke[m], Pc, optimize=True)
+        np.add.at(out, cid[m], contrib)
+    return out
+
+
+def prolongation(nf: int, d: int) -> sp.csr_matrix:
+    """Global periodic trilinear P: coarse (nf/2)^3 -> fine nf^3
+    (EBE_GMG.py:531-647, weights prod(1 - |rem/2 - off|))."""
+    nc = nf // 2
+    g = grid_coords(nf)
+    base, rem = g // 2, g % 2
+    rows, cols, vals = [], [], []
+    for o in range(8):
+        off = np.array([(o >> 2) & 1, (o >> 1) & 1, o & 1])
+        t = (base + off) % nc
+        w = np.prod(1.0 - np.abs(0.5 * rem - off), axis=1)
+        ci = (t[:, 0] * nc + t[:, 1]) * nc + t[:, 2]
+        keep = w != 0
+        fi = np.arange(nf ** 3)[keep]
+        for c in range(d):
+            rows.append(fi * d + c)
+            cols.append(ci[keep] * d + c)
+            vals.append(w[keep])
+    P = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(nf ** 3 * d, nc ** 3 * d)).tocsr()
+    P.sum_duplicates()
+    return P
+
+
+def colors(n: int) -> np.ndarray:
+    """Parity colour of each node (EBE_GMG.py:354-374)."""
+    g = grid_coords(n)
+    return (g[:, 0] % 2) * 4 + (g[:, 1] % 2) * 2 + (g[:, 2] % 2)
+
+
+# ---------------------------------------------------------------------------
+# geometric multigrid (reference algorithm: V-cycles with 8-colour GS)
+# ---------------------------------------------------------------------------
+class Level:
+    def __init__(self, ke: np.ndarray, n: int, d: int):
+        self.n, self.d = n, d
+        self.ke = ke
+        self.K = assemble_K(ke, n, d)
+        diag = self.K.diagonal().copy()
+        diag[diag == 0] = 1.0                               # EBE_GMG.py:387-388
+        self.dinv = 1.0 / diag
+        col = np.repeat(colors(n), d)
+        self.color_rows = [np.nonzero(col == c)[0] for c in range(8)]
+        self.Kc = [self.K[rows] for rows in self.color_rows]
+        self.P = None                                       # fine(level-1) <- this level
+
+
+class Hierarchy:
+    """Operator hierarchy of GMGSolver.solve (EBE_GMG.py:790-849) for the
+    per-element matrices rho_e * Ke0."""
+
+    def __init__(self, rho: np.ndarray, Ke0: np.ndarray, n: int, d: int, levels: int):
+        ke = rho.reshape(-1, 1, 1) * Ke0[None]             # model.py:108
+        self.levels = [Level(ke, n, d)]
+        for _ in range(1, levels):
+            if n % 2 or n < 2:
+                break
+            ke = coarsen_elements(ke, n, d)
+            P = prolongation(n, d)
+            n //= 2
+            lv = Level(ke, n, d)
+            lv.P = P
+            self.levels.append(lv)
+
+    def gs_sweeps(self, lv: Level, u, f, sweeps: int, reverse: bool = False):
+        """8-colour Gauss-Seidel, omega=1 (EBE_GMG.py:431-459)."""
+        order = range(7, -1, -1) if reverse else range(8)
+        for _ in range(sweeps):
+            for c in order:
+                rows = lv.color_rows[c]
+                if rows.size == 0:
+                    continue
+                r = f[rows] - lv.Kc[c] @ u
+                u[rows] += lv.dinv[rows, None] * r
+        return u
+
+    def vcycle(self, l: int, u, f, smooth_iter, coarse_default: int | None):
+        """One V-cycle (EBE_GMG.py:886-984).  ``coarse_default`` reproduces the
+        elastic solver's recursion, which does not forward ``smooth_iter`` and so
+        smooths coarser levels with the default of 1 sweep (EBE_GMG.py:955-963);
+        the scalar solver forwards it (EBE_GMG_scalar.py:802-811): pass None."""
+        lv = self.levels[l]
+        if l > 0 and coarse_default is not None:
+            nu = coarse_default
+        elif isinstance(smooth_iter, (list, tuple)):
+            nu = 1 if len(smooth_iter) == 0 else smooth_iter[min(l, len(smooth_iter) - 1)]
+        else:
+            nu = int(smooth_iter)
+        u = self.gs_sweeps(lv, u, f, nu)
+        if l == len(self.levels) - 1:
+            return self.gs_sweeps(lv, u, f, 1)
+        r = f - lv.K @ u
+        nxt = self.levels[l + 1]
+        rc = nxt.P.T @ r
+        uc = self.vcycle(l + 1, np.zeros_like(rc), rc, smooth_iter, coarse_default)
+        u = u + nxt.P @ uc
+        return self.gs_sweeps(lv, u, f, nu)
+
+
+def gmg_solve(hier: Hierarchy, f: np.ndarray, max_iter: int, smooth_iter=(2, 2, 3, 4, 5),
+              coarse_default: int | None = 1, rtol: float = 0.0, u0=None):
+    """V-cycle iteration from u=0 (EBE_GMG.py:758-885).  Returns (u, r, cycles).
+    ``rtol`` > 0 stops early once ||r|| <= rtol ||f|| per column (the reference
+    has no test; it runs ``max_iter`` cycles)."""
+    u = np.zeros_like(f) if u0 is None else u0.copy()
+    K = hier.levels[0].K
+    fn = np.linalg.norm(f, axis=0)
+    it = 0
+    r = f - K @ u
+    for it in range(1, max_iter + 1):
+        u = hier.vcycle(0, u, f, smooth_iter, coarse_default)
+        r = f - K @ u
+        if rtol > 0 and np.all(np.linalg.norm(r, axis=0) <= rtol * np.maximum(fn, 1e-300)):
+            break
+    return u, r, it
+
+
+# ---------------------------------------------------------------------------
+# homogenization, sensitivities, objectives
+# ---------------------------------------------------------------------------
+def element_fields(u: np.ndarray, n: int, d: int) -> np.ndarray:
+    """Gather per-element DOF blocks (N, 8d, R) (model.py:39-41)."""
+    return u[dof_index(n, d)]
+
+
+def homogenize(u: np.ndarray, rho: np.ndarray, Ke0: np.ndarray, X0: np.ndarray, n: int, d: int):
+    """C^H (or kappa^H) = sum_e (X0-u_e)^T rho_e Ke0 (X0-u_e), volume 1
+    (model.py:33-44, 47-95)."""
+    L = X0[None] - element_fields(u, n, d)
+    KL = np.einsum("ij,ejk->eik", Ke0, L, optimize=True)
+    return np.einsum("eij,e,eik->jk", L, rho.reshape(-1), KL, optimize=True)
+
+
+def element_energy(u: np.ndarray, Ke0: np.ndarray, X0: np.ndarray, n: int, d: int) -> np.ndarray:
+    """Per-element (X0-u_e)^T Ke0 (X0-u_e): (N,R,R) = dC^H/drho_e at a converged
+    solve (the analytic adjoint of the autograd call at main_IHD_v3.py:688)."""
+    L = X0[None] - element_fields(u, n, d)
+    KL = np.einsum("ij,ejk->eik", Ke0, L, optimize=True)
+    return np.einsum("eij,eik->ejk", L, KL, optimize=True)
+
+
+def _sym_inv(CH):
+    C = 0.5 * (CH + CH.T)
+    return np.linalg.inv(C + 1e-9 * np.eye(6))
+
+
+def stiffness_objective(CH):
+    """mean(1/S_ii), i=0..2, S=inv(sym(C)+1e-9 I) (utils/objective.py:11-19)."""
+    S = _sym_inv(CH)
+    return float(np.mean(1.0 / np.diag(S)[:3]))
+
+
+def shear_objective(CH):
+    """mean(1/S_ii), i=3..5 (utils/objective.py:22-30)."""
+    S = _sym_inv(CH)
+    return float(np.mean(1.0 / np.diag(S)[3:]))
+
+
+def thermal_objective(kappa):
+    """trace(kappa) (utils/objective.py:33-41)."""
+    return float(np.trace(kappa))
+
+
+def _grad_modulus(CH, idx):
+    """d/dCH of mean(1/S_ii over idx): with dS = -S dC S on sym(C),
+    d(1/S_ii) = S[:,i] S[i,:] / S_ii^2, then symmetrised by C=(CH+CH^T)/2."""
+    S = _sym_inv(CH)
+    G = np.zeros((6, 6))
+    for i in idx:
+        G += np.outer(S[:, i], S[i, :]) / S[i, i] ** 2
+    G /= len(idx)
+    return 0.5 * (G + G.T)
+
+
+_ALIASES = {"stiff": "stiffness", "stiffness": "stiffness", "e": "stiffness", "young": "stiffness",
+            "youngs": "stiffness", "shear": "shear", "g": "shear", "thermal": "thermal",
+            "kappa": "thermal", "conductivity": "thermal", "heat": "thermal"}
+
+
+def parse_objective_spec(spec) -> dict:
+    """Weighted-term parser (utils/objective.py:93-157)."""
+    import re
+    if spec is None or not str(spec).strip():
+        return {"shear": 1.0}
+    s = str(spec).strip()
+    if s.lower() in _ALIASES:
+        return {_ALIASES[s.lower()]: 1.0}
+    out: dict = {}
+    for part in [p for p in re.split(r"[,+]", s.replace(" ", "")) if p]:
+        if ":" in part or "=" in part:
+            name, w = re.split(r"[:=]", part, maxsplit=1)
+            w = float(w)
+        elif "*" in part:
+            a, b = part.split("*", 1)
+            try:
+                w, name = float(a), b
+            except ValueError:
+                w, name = float(b), a
+        else:
+            name, w = part, 1.0
+        key = _ALIASES[name.lower()]
+        out[key] = out.get(key, 0.0) + w
+    return out
+
+
+def objective_and_grads(weights: dict, CH, kappa):
+    """J = sum_t w_t term_t and (dJ/dCH, dJ/dkappa) (utils/objective.py:180-251)."""
+    J = 0.0
+    gC = np.zeros((6, 6))
+    gK = np.zeros((3, 3))
+    for t, w in weights.items():
+        if t == "stiffness":
+            J += w * stiffness_objective(CH)
+            gC += w * _grad_modulus(CH, (0, 1, 2))
+        elif t == "shear":
+            J += w * shear_objective(CH)
+            gC += w * _grad_modulus(CH, (3, 4, 5))
+        else:
+            J += w * thermal_objective(kappa)
+            gK += w * np.eye(3)
+    return J, gC, gK
+
+
+# ---------------------------------------------------------------------------
+# filter, OC
+# ---------------------------------------------------------------------------
+def box_filter_periodic(v: np.ndarray, n: int, k: int = 3) -> np.ndarray:
+    """Periodic k^3 box mean (main_IHD_v3.py:342-359)."""
+    if k <= 0 or k % 2 == 0:
+        raise ValueError(f"filter size must be a positive odd integer, got {k}")
+    vol = v.reshape(n, n, n)
+    acc = np.zeros_like(vol)
+    p = k // 2
+    for dx in range(-p, p + 1):
+        for dy in range(-p, p + 1):
+            for dz in range(-p, p + 1):
+                acc += np.roll(vol, (-dx, -dy, -dz), axis=(0, 1, 2))
+    return (acc / float(k ** 3)).reshape(v.shape)
+
+
+def oc_update(x: np.ndarray, dJdx: np.ndarray, volfrac: float, move: float = 0.1,
+              xmin: float = 1e-3) -> np.ndarray:
+    """60-step OC bisection (main_IHD_v3.py:362-380); returns the x of the last
+    bisection step, exactly as the reference does."""
+    dJ = np.maximum(dJdx, 1e-12)
+    l1, l2 = 1e-12, 1e6
+    xn = x
+    for _ in range(60):
+        lam = 0.5 * (l1 + l2)
+        xn = x * np.sqrt(dJ / lam)
+        xn = np.minimum(np.maximum(xn, x - move), x + move)
+        xn = np.minimum(np.maximum(xn, xmin), 1.0)
+        if xn.mean() > volfrac:
+            l1 = lam
+        else:
+            l2 = lam
+    return xn
+
+
+# ---------------------------------------------------------------------------
+# seeded synthetic densities (benchmark inputs)
+# ---------------------------------------------------------------------------
+def seed_density(seed: int, r: int, sigma: float, vf: float, scale: float = 0.25,
+                 xmin: float = 1e-3) -> np.ndarray:
+    """N(0,1) voxels, periodic Gaussian smoothing (FFT), standardise, affine map
+    to mean vf with scale 0.25, clip to [xmin,1], mean-matching rounds until
+    |mean - vf| < 1e-12 (at most 200).
+    Returns x of shape (r,r,r), float64."""
+    z = np.random.default_rng(seed).standard_normal((r, r, r))
+    k = np.fft.fftfreq(r)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2
+    z = np.real(np.fft.ifftn(np.fft.fftn(z) * np.exp(-2.0 * (np.pi ** 2) * (sigma ** 2) * k2)))
+    z = (z - z.mean()) / z.std()
+    x = np.clip(vf + scale * z, xmin, 1.0)
+    for _ in range(200):  # mean matching; converges geometrically unless vf is tiny
+        x = np.clip(x - x.mean() + vf, xmin, 1.0)
+        if abs(x.mean() - vf) < 1e-12:
+            break
+    return x
+
+
+# ---------------------------------------------------------------------------
+# one full homogenization + sensitivity evaluation
+# ---------------------------------------------------------------------------
+def solve_cell(rho: np.ndarray, r: int, elems: Elements | None = None, levels: int = 3,
+               max_cycles: int = 200, rtol: float = 1e-12, physics=("elastic", "thermal"),
+               smooth_iter=(2, 2, 3, 4, 5)):
+    """Both physics on one cell: returns dict with CH, kappa, u3, u1 and the
+    per-element energies (dC/drho, dkappa/drho)."""
+    elems = elems or Elements(r)
+    out = {}
+    rho = rho.reshape(-1)
+    for ph in physics:
+        d = 3 if ph == "elastic" else 1
+        Ke0, Fe0, X0 = elems.get(d)
+        hier = Hierarchy(rho, Ke0, r, d, levels)
+        F = assemble_F(rho, Fe0, r, d)
+        u, res, cyc = gmg_solve(hier, F, max_cycles, smooth_iter,
+                                coarse_default=1 if d == 3 else None, rtol=rtol)
+        H = homogenize(u, rho, Ke0, X0, r, d)
+        dH = element_energy(u, Ke0, X0, r, d)
+        key = "CH" if d == 3 else "kappa"
+        out[key] = H
+        out["d" + key] = dH
+        out["u3" if d == 3 else "u1"] = u
+        out["cycles_" + ph] = cyc
+        out["relres_" + ph] = np.linalg.norm(res, axis=0) / np.maximum(np.linalg.norm(F, axis=0), 1e-300)
+    return out
+
+
+def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal: float = 3.0,
+                 rho_min: float = 1e-9, move: float = 0.2, xmin: float = 1e-3, filter_k: int = 3,
+                 elems: Elements | None = None, levels: int = 3, rtol: float = 1e-12,
+                 max_cycles: int = 200):
+    """One OC iteration of main_IHD_v3.py:620-716 (symmetry none, no penalties)
+    with the analytic adjoint in place of autograd.  Returns (x_next, info)."""
+    x = x.reshape(-1)
+    xc = np.clip(x, xmin, 1.0)
+    rho = rho_min + (1.0 - rho_min) * xc ** penal
+    phys = []
+    if any(t in ("stiffness", "shear") for t in weights):
+        phys.append("elastic")
+    if "thermal" in weights:
+        phys.append("thermal")
+    res = solve_cell(rho, r, elems, levels, max_cycles, rtol, tuple(phys))
+    CH = res.get("CH")
+    kap = res.get("kappa")
+    J, gC, gK = objective_and_grads(weights, CH if CH is not None else np.eye(6),
+                                    kap if kap is not None else np.eye(3))
+    dJdrho = np.zeros(r ** 3)
+    if CH is not None:
+        dJdrho += np.einsum("eij,ij->e", res["dCH"], gC)
+    if kap is not None:
+        dJdrho += np.einsum("eij,ij->e", res["dkappa"], gK)
+    dJdx = dJdrho * penal * (1.0 - rho_min) * xc ** (penal - 1.0)
+    if filter_k and filter_k > 1:
+        dJdx = box_filter_periodic(dJdx, r, filter_k)
+    x_new = oc_update(x, dJdx, volfrac, move, xmin)
+    x_next = np.clip(x_new, xmin, 1.0)
+    info = dict(J=J, CH=CH, kappa=kap, dJdx=dJdx, dx_max=float(np.abs(x_next - x).max()),
+                dx_mean=float(np.abs(x_next - x).mean()), res=res)
+    return x_next, info

@@ -1,0 +1,221 @@
+"""Generate golden vectors by running the reference implementation (xing-yuu/MAPLE).
+
+Run in a container where the reference source tree is available:
+
+    python tests/golden/make_golden.py /path/to/MAPLE/src
+
+It imports the reference package, runs its own functions in FP64 and writes
+``tests/golden/*.npz``.  Nothing at test time reads the reference tree: the
+tests only read the committed .npz files.
+
+What is recorded (all FP64):
+  * element tables: ``hexahedron(r, isotropic_elastic_tensor(1,0.3).double())``
+    and ``hexahedron_scalar(r, kappa=float64 1.0)`` (utils/_utils.py:39-196);
+  * RHS assembly ``assemble_F_fast`` / ``assemble_F_fast_scalar``;
+  * converged homogenization: ``GMGSolver.solve`` / ``GMGSolverScalar.solve``
+    with ``dtype=torch.float64`` and enough V-cycles for relres ~1e-14, then the
+    energy sums of ``IHD.homogenized_batch_3d`` / ``homogenized_batch_thermal``
+    (utils/model.py:33-95);
+  * dJ/dx by ``torch.autograd.grad`` through those converged solves
+    (main_IHD_v3.py:620-688), for two objective specs;
+  * ``avg_filter3d_x_periodic`` and ``oc_update`` on seeded inputs;
+  * objective values and their autograd gradients w.r.t. C^H / kappa;
+  * a 3-iteration OC trajectory at 8^3 built from the reference's own pieces.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import types
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _import_reference(src):
+    sys.path.insert(0, src)
+    # main_IHD_v3 imports skimage for mesh export only; it is never called here
+    sk = types.ModuleType("skimage")
+    sk.measure = types.ModuleType("skimage.measure")
+    sys.modules.setdefault("skimage", sk)
+    sys.modules.setdefault("skimage.measure", sk.measure)
+    from maple.core import main_IHD_v3 as M
+    from maple.core.utils import _utils as U
+    from maple.core.utils import model as Mo
+    from maple.core.utils import objective as Ob
+    from maple.core.utils.EBE_GMG import GMGSolver
+    from maple.core.utils.EBE_GMG_scalar import GMGSolverScalar
+    return M, U, Mo, Ob, GMGSolver, GMGSolverScalar
+
+
+def seed_density(seed, r, sigma, vf, scale=0.25, xmin=1e-3):
+    z = np.random.default_rng(seed).standard_normal((r, r, r))
+    k = np.fft.fftfreq(r)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2
+    z = np.real(np.fft.ifftn(np.fft.fftn(z) * np.exp(-2.0 * (np.pi ** 2) * (sigma ** 2) * k2)))
+    z = (z - z.mean()) / z.std()
+    x = np.clip(vf + scale * z, xmin, 1.0)
+    for _ in range(200):  # mean matching; converges geometrically unless vf is tiny
+        x = np.clip(x - x.mean() + vf, xmin, 1.0)
+        if abs(x.mean() - vf) < 1e-12:
+            break
+    return x
+
+
+def main(src):
+    M, U, Mo, Ob, GMGSolver, GMGSolverScalar = _import_reference(src)
+    # torch's default dtype stays float32: the reference's
+    # isotropic_elastic_tensor (utils/_utils.py:42) relies on it
+    dev = torch.device("cpu")
+    ihd = Mo.IHD.__new__(Mo.IHD)
+    torch.nn.Module.__init__(ihd)
+
+    def tables(r):
+        C = U.isotropic_elastic_tensor(1.0, 0.3).double()
+        Ke, Fe, X0 = U.hexahedron(r, C)
+        K1, F1, X1 = U.hexahedron_scalar(r, kappa=torch.tensor(1.0, dtype=torch.float64))
+        return Ke, Fe, X0, K1, F1, X1
+
+    def homogenize(r, rho, cycles, levels=3, want_u=False):
+        """Reference forward in FP64 (differentiable w.r.t. rho)."""
+        Ke, Fe, X0, K1, F1, X1 = tables(r)
+        batch = M.build_unitcell_batch(dev, r, rho.detach().reshape(r, r, r))
+        rr = rho.reshape(-1, 1)
+        n = r ** 3
+        out = {}
+        # elastic (utils/model.py:98-130 with dtype float64)
+        F = U.assemble_F_fast(batch["node_index"], Fe, n, rr)
+        Ke_ = Ke.unsqueeze(0).expand(n, -1, -1) * rr.reshape(-1, 1, 1)
+        us, res = [], []
+        g = GMGSolver()
+        for i in range(6):
+            u, rv = g.solve(Ke_, F[:, :, i], batch["coord"].int(), batch["elem_coords"], batch["node_index"],
+                            max_iter=cycles, smooth_iter=[2, 2, 3, 4, 5], max_levels=levels, dtype=torch.float64)
+            us.append(u)
+            res.append((rv.norm() / F[:, :, i].norm()).item())
+        Uel = torch.cat(us, 1)
+        out["CH"] = ihd.homogenized_batch_3d(Uel, Ke_, X0, batch["coord"][:, 0], batch["node_index"],
+                                             batch["voxel_batch_id"], 1)[0]
+        out["relres_elastic"] = np.array(res)
+        # thermal (utils/model.py:131-159 with dtype float64)
+        Ft = U.assemble_F_fast_scalar(batch["node_index"], F1, n, rr)
+        K1_ = K1.unsqueeze(0).expand(n, -1, -1) * rr.reshape(-1, 1, 1)
+        gs = GMGSolverScalar()
+        ut, res = [], []
+        for i in range(3):
+            u, rv = gs.solve(K1_, Ft[:, i], batch["coord"].int(), batch["elem_coords"], batch["node_index"],
+                             max_iter=cycles, smooth_iter=[2, 2, 3, 4, 5], max_levels=levels, dtype=torch.float64)
+            ut.append(u)
+            res.append((rv.norm() / Ft[:, i].norm()).item())
+        Uth = torch.cat(ut, 1)
+        out["kappa"] = ihd.homogenized_batch_thermal(Uth, K1_, X1, batch["coord"][:, 0], batch["node_index"],
+                                                     batch["voxel_batch_id"], 1)[0]
+        out["relres_thermal"] = np.array(res)
+        if want_u:
+            out["u_elastic"] = Uel.detach().numpy().reshape(n, 6, 3).transpose(0, 2, 1).copy()  # (N,3,6)
+            out["u_thermal"] = Uth.detach().numpy()
+            out["F_elastic"] = F.detach().numpy()
+            out["F_thermal"] = Ft.detach().numpy()
+        return out
+
+    rec = {}
+    # ---------------------------------------------------------------- tables
+    for r in (8, 16, 32):
+        Ke, Fe, X0, K1, F1, X1 = tables(r)
+        for k, v in dict(Ke3=Ke, Fe3=Fe, X03=X0, Ke1=K1, Fe1=F1, X01=X1).items():
+            rec[f"r{r}_{k}"] = v.numpy()
+    np.savez_compressed(os.path.join(HERE, "element_tables.npz"), **rec)
+
+    # ------------------------------------------------- converged homogenization
+    specs = {"bi": "stiffness:0.5,thermal:0.5", "tri": "stiffness:0.3333333333333333,shear:0.3333333333333333,"
+                                                       "thermal:0.3333333333333333"}
+    cases = [(8, 0, 2.0, 0.25), (8, 1, 1.0, 0.30), (16, 0, 2.0, 0.25)]
+    for (r, seed, sigma, vf) in cases:
+        x = seed_density(seed, r, sigma, vf)
+        rec = dict(x=x.reshape(-1), r=r, seed=seed, sigma=sigma, vf=vf)
+        penal, rho_min = 3.0, 1e-9
+        # the reference's coarsest level is only smoothed, so deeper hierarchies
+        # are needed for a converged FP64 solve at 16^3
+        cycles, levels = (60, 3) if r == 8 else (70, 5)
+        xt = torch.tensor(x.reshape(-1, 1))
+        rho = rho_min + (1 - rho_min) * xt ** penal
+        out = homogenize(r, rho, cycles, levels=levels, want_u=(r == 8))
+        for k, v in out.items():
+            rec[k] = v.detach().numpy() if torch.is_tensor(v) else v
+        if r == 8:
+            # dJ/dx by autograd through the converged solves (main_IHD_v3.py:622-688)
+            for tag, spec in specs.items():
+                xv = xt.clone().requires_grad_(True)
+                xc = xv.clamp(1e-3, 1.0)
+                rv = rho_min + (1 - rho_min) * xc ** penal
+                o = homogenize(r, rv, cycles, levels=3)
+                J = Ob.objective_from_spec(obj=spec, CH=o["CH"], kappa=o["kappa"])
+                (g,) = torch.autograd.grad(J, xv)
+                rec[f"J_{tag}"] = J.item()
+                rec[f"dJdx_{tag}"] = g.numpy().reshape(-1)
+        name = f"homog_r{r}_s{seed}.npz"
+        np.savez_compressed(os.path.join(HERE, name), **rec)
+        print("wrote", name, "relres", out["relres_elastic"].max(), out["relres_thermal"].max())
+
+    # ------------------------------------------------ filter / OC / objectives
+    rng = np.random.default_rng(7)
+    rec = {}
+    for r in (6, 8):
+        n = r ** 3
+        v = rng.standard_normal(n)
+        batch = M.build_unitcell_batch(dev, r, torch.zeros(r, r, r))
+        for k in (1, 3, 5):
+            rec[f"filter_r{r}_k{k}_in"] = v
+            rec[f"filter_r{r}_k{k}_out"] = M.avg_filter3d_x_periodic(torch.tensor(v).reshape(-1, 1),
+                                                                       batch["elem_coords"], r, k).numpy().reshape(-1)
+    for i, (vf, move, xmin) in enumerate([(0.25, 0.2, 1e-3), (0.1, 0.05, 1e-5), (0.4, 0.2, 1e-3)]):
+        n = 512
+        x = np.clip(vf + 0.2 * rng.standard_normal(n), xmin, 1.0)
+        dJ = np.abs(rng.standard_normal(n)) * 1e-2
+        dJ[:5] = -1.0  # negative sensitivities are clamped to 1e-12
+        xn = M.oc_update(torch.tensor(x).reshape(-1, 1), torch.tensor(dJ).reshape(-1, 1), volfrac=vf, move=move,
+                         xmin=xmin).numpy().reshape(-1)
+        rec.update({f"oc{i}_x": x, f"oc{i}_dJ": dJ, f"oc{i}_xnew": xn, f"oc{i}_params": np.array([vf, move, xmin])})
+    for i in range(3):
+        A = rng.standard_normal((6, 6)) * 0.05
+        CH = torch.tensor(A @ A.T + np.eye(6) * (0.1 + 0.1 * i) + 0.01 * rng.standard_normal((6, 6)),
+                          requires_grad=True)
+        kap = torch.tensor(np.diag(rng.uniform(0.05, 0.3, 3)) + 0.01, requires_grad=True)
+        for tag, spec in dict(stiff="stiffness", shear="shear", therm="thermal", bi=specs["bi"],
+                              tri=specs["tri"], mixw="0.4*stiffness+0.6*thermal").items():
+            J = Ob.objective_from_spec(obj=spec, CH=CH, kappa=kap)
+            gC, gK = torch.autograd.grad(J, (CH, kap), allow_unused=True)
+            rec[f"obj{i}_{tag}_J"] = J.item()
+            rec[f"obj{i}_{tag}_gC"] = gC.numpy() if gC is not None else np.zeros((6, 6))
+            rec[f"obj{i}_{tag}_gK"] = gK.numpy() if gK is not None else np.zeros((3, 3))
+        rec[f"obj{i}_CH"] = CH.detach().numpy()
+        rec[f"obj{i}_kappa"] = kap.detach().numpy()
+    for spec in ["stiffness", "0.4*stiffness+0.6*thermal", "shear=0.3+thermal=0.7", "stiffness,thermal",
+                 "E:0.5,kappa:0.5", " Shear "]:
+        rec["spec::" + spec] = np.array(sorted(Ob.parse_objective_spec(spec).items()), dtype=object).astype(str)
+    np.savez_compressed(os.path.join(HERE, "ops.npz"), **rec)
+
+    # ------------------------------------------------------ short OC trajectory
+    r, vf, move, xmin, penal, rho_min, fk = 8, 0.25, 0.2, 1e-3, 3.0, 1e-9, 3
+    x = torch.tensor(seed_density(0, r, 2.0, vf).reshape(-1, 1))
+    batch = M.build_unitcell_batch(dev, r, torch.zeros(r, r, r))
+    traj = dict(x0=x.numpy().reshape(-1))
+    for it in range(3):
+        xv = x.detach().clone().requires_grad_(True)
+        rv = rho_min + (1 - rho_min) * xv.clamp(xmin, 1.0) ** penal
+        o = homogenize(r, rv, 60, levels=3)
+        J = Ob.objective_from_spec(obj=specs["bi"], CH=o["CH"], kappa=o["kappa"])
+        (g,) = torch.autograd.grad(J, xv)
+        g = M.avg_filter3d_x_periodic(g, batch["elem_coords"], r, fk)
+        xn = M.oc_update(x.detach(), g.detach(), volfrac=vf, move=move, xmin=xmin).clamp(xmin, 1.0)
+        traj[f"J{it}"] = J.item()
+        traj[f"x{it + 1}"] = xn.numpy().reshape(-1)
+        x = xn
+        print("traj it", it, "J", J.item())
+    np.savez_compressed(os.path.join(HERE, "traj_r8.npz"), **traj)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")

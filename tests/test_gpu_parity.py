@@ -1,0 +1,206 @@
+"""GPU parity of the sm_100a kernels against the FP64 oracle and the golden
+vectors recorded from the reference (called through the C ABI)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import ihd_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def T(a):
+    return torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=DEV)
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def simp(x, p=3.0, rmin=1e-9):
+    return rmin + (1 - rmin) * np.clip(x, 1e-3, 1.0) ** p
+
+
+@pytest.fixture(scope="module")
+def ctx8(lib):
+    from maple_b200.core import HomogenizationContext
+    c = HomogenizationContext(8, ncells=2)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def dens8(golden):
+    g0, g1 = golden("homog_r8_s0.npz"), golden("homog_r8_s1.npz")
+    return (g0, g1), np.stack([simp(g0["x"]), simp(g1["x"])])
+
+
+def test_matvec_elastic_and_thermal(ctx8, dens8):
+    _, rho = dens8
+    r, N = 8, 512
+    rng = np.random.default_rng(0)
+    e = O.Elements(r)
+    for phys, d, R, Ke0 in (("elastic", 3, 6, e.Ke3), ("thermal", 1, 3, e.Ke1)):
+        u = rng.standard_normal((2, N, R, d))
+        y = ctx8.matvec(phys, T(rho), T(u)).cpu().numpy()
+        for b in range(2):
+            K = O.assemble_K(rho[b].reshape(-1, 1, 1) * Ke0[None], r, d)
+            umat = u[b].transpose(0, 2, 1).reshape(N * d, R)
+            ref = (K @ umat).reshape(N, d, R).transpose(0, 2, 1)
+            assert rel(y[b], ref) < 1e-13, (phys, b)
+
+
+def test_assemble_rhs(ctx8, dens8):
+    _, rho = dens8
+    e = O.Elements(8)
+    for phys, d, R, Fe in (("elastic", 3, 6, e.Fe3), ("thermal", 1, 3, e.Fe1)):
+        F = ctx8.assemble_rhs(phys, T(rho)).cpu().numpy()
+        for b in range(2):
+            ref = O.assemble_F(rho[b], Fe, 8, d).reshape(512, d, R).transpose(0, 2, 1)
+            assert rel(F[b], ref) < 1e-13
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-9)])
+def test_homogenization_matches_reference(ctx8, dens8, precision, tol):
+    (g0, g1), rho = dens8
+    for phys, key in (("elastic", "CH"), ("thermal", "kappa")):
+        ctx8.set_density(phys, T(rho), precision)
+        info = ctx8.solve(phys, precision, rtol=1e-12, maxit=300)
+        assert (info.status & 1).all(), info
+        H = ctx8.homogenize(phys).cpu().numpy()
+        assert rel(H[0], g0[key]) < tol, (phys, precision)
+        assert rel(H[1], g1[key]) < tol, (phys, precision)
+
+
+def test_solution_field_matches_reference(ctx8, dens8):
+    (g0, _), rho = dens8
+    ctx8.set_density("elastic", T(rho), "fp64")
+    ctx8.solve("elastic", "fp64", rtol=1e-13, maxit=300)
+    u = ctx8.solution("elastic").cpu().numpy()[0]          # (N, 6, 3)
+    ug = g0["u_elastic"].transpose(0, 2, 1)                 # (N, 6, 3)
+    du = (u - u.mean(0)) - (ug - ug.mean(0))
+    assert np.abs(du).max() / np.abs(ug).max() < 1e-9
+
+
+@pytest.mark.parametrize("tag,w", [("bi", (0.5, 0.0, 0.5)), ("tri", (1 / 3, 1 / 3, 1 / 3))])
+def test_sensitivity_matches_autograd(ctx8, dens8, tag, w):
+    (g0, g1), rho = dens8
+    H = {}
+    for phys in ("elastic", "thermal"):
+        ctx8.set_density(phys, T(rho), "fp64")
+        ctx8.solve(phys, "fp64", rtol=1e-13, maxit=300)
+        H[phys] = ctx8.homogenize(phys).cpu().numpy()
+    weights = {"stiffness": w[0], "shear": w[1], "thermal": w[2]}
+    weights = {k: v for k, v in weights.items() if v}
+    gC = np.zeros((2, 6, 6))
+    gK = np.zeros((2, 3, 3))
+    for b in range(2):
+        _, gC[b], gK[b] = O.objective_and_grads(weights, H["elastic"][b], H["thermal"][b])
+    dJdrho = ctx8.sensitivity(T(gC), T(gK)).cpu().numpy()
+    for b, g in enumerate((g0, g1)):
+        if f"dJdx_{tag}" not in g:
+            continue
+        dJdx = dJdrho[b] * 3 * (1 - 1e-9) * np.clip(g["x"], 1e-3, 1) ** 2
+        assert rel(dJdx, g[f"dJdx_{tag}"]) < 1e-8
+
+
+@pytest.mark.parametrize("r", [6, 8])
+@pytest.mark.parametrize("k", [1, 3, 5])
+def test_box_filter(lib, golden, r, k):
+    from maple_b200.core import box_filter
+    g = golden("ops.npz")
+    out = box_filter(T(g[f"filter_r{r}_k{k}_in"][None]), r, k).cpu().numpy()[0]
+    assert rel(out, g[f"filter_r{r}_k{k}_out"]) < 1e-14
+
+
+def test_oc_update_matches_reference(ctx8, golden, lib):
+    from maple_b200.core import HomogenizationContext
+    g = golden("ops.npz")
+    # cases 0 and 2 share move/xmin: one batched call
+    x = np.stack([g["oc0_x"], g["oc2_x"]])
+    dJ = np.stack([g["oc0_dJ"], g["oc2_dJ"]])
+    vf = np.array([g["oc0_params"][0], g["oc2_params"][0]])
+    xn, stats = ctx8.oc_update(T(x), T(dJ), T(vf), move=0.2, xmin=1e-3)
+    xn = xn.cpu().numpy()
+    assert np.abs(xn[0] - g["oc0_xnew"]).max() < 1e-10
+    assert np.abs(xn[1] - g["oc2_xnew"]).max() < 1e-10
+    st = stats.cpu().numpy()
+    assert abs(st[0, 0] - np.abs(xn[0] - x[0]).max()) < 1e-15
+    assert abs(st[0, 1] - np.abs(xn[0] - x[0]).mean()) < 1e-14
+    c1 = HomogenizationContext(8, ncells=1)
+    vf1, mv1, xm1 = g["oc1_params"]
+    xn1, _ = c1.oc_update(T(g["oc1_x"][None]), T(g["oc1_dJ"][None]), T(np.array([vf1])), move=mv1, xmin=xm1)
+    assert np.abs(xn1.cpu().numpy()[0] - g["oc1_xnew"]).max() < 1e-10
+    c1.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-8), ("mixed", 1e-7)])
+def test_oc_step_trajectory(lib, golden, precision, tol):
+    """Three fused OC iterations on device follow the reference trajectory."""
+    from maple_b200.core import HomogenizationContext
+    g = golden("traj_r8.npz")
+    c = HomogenizationContext(8, ncells=1)
+    x = T(g["x0"][None])
+    w = T(np.array([[0.5, 0.0, 0.5]]))
+    vf = T(np.array([0.25]))
+    for it in range(3):
+        out = c.oc_step(x, w, vf, penal=3.0, rho_min=1e-9, move=0.2, xmin=1e-3, filter_k=3, precision=precision,
+                        rtol=1e-12, maxit=300, warm=True)
+        J = out["J"].cpu().numpy()[0]
+        assert abs(J - float(g[f"J{it}"])) / abs(J) < tol * 1e-1
+        xn = out["x_next"].cpu().numpy()[0]
+        assert np.abs(xn - g[f"x{it + 1}"]).max() < tol
+        x = out["x_next"].clone()
+    c.close()
+
+
+def test_r16_matches_reference(lib, golden):
+    from maple_b200.core import HomogenizationContext
+    g = golden("homog_r16_s0.npz")
+    c = HomogenizationContext(16, ncells=1)
+    rho = T(simp(g["x"])[None])
+    for phys, key in (("elastic", "CH"), ("thermal", "kappa")):
+        c.set_density(phys, rho, "fp64")
+        info = c.solve(phys, "fp64", rtol=1e-12, maxit=300)
+        assert (info.status & 1).all()
+        assert rel(c.homogenize(phys).cpu().numpy()[0], g[key]) < 1e-9
+    c.close()
+
+
+def test_solid_cell_known_answer(lib):
+    from maple_b200.core import HomogenizationContext
+    c = HomogenizationContext(8, ncells=1)
+    rho = torch.ones((1, 512), dtype=torch.float64, device=DEV)
+    for phys, ref in (("elastic", O.isotropic_elastic_tensor(1.0, 0.3)), ("thermal", np.eye(3))):
+        c.set_density(phys, rho, "fp64")
+        c.solve(phys, "fp64", rtol=1e-12, maxit=50)
+        assert rel(c.homogenize(phys).cpu().numpy()[0], ref) < 1e-12
+    c.close()
+
+
+def test_deterministic(ctx8, dens8):
+    _, rho = dens8
+    out = []
+    for _ in range(2):
+        ctx8.set_density("elastic", T(rho), "mixed")
+        ctx8.solve("elastic", "mixed", rtol=1e-10, maxit=300)
+        out.append(ctx8.homogenize("elastic").cpu().numpy())
+    assert np.array_equal(out[0], out[1])
+
+
+def test_bad_arguments(lib):
+    from maple_b200 import MapleError
+    from maple_b200.core import HomogenizationContext
+    with pytest.raises(MapleError):
+        HomogenizationContext(5, ncells=1)
+    c = HomogenizationContext(8, ncells=1)
+    with pytest.raises(ValueError):
+        c.set_density("elastic", torch.ones((1, 100), dtype=torch.float64, device=DEV))
+    with pytest.raises(ValueError):
+        c.set_density("elastic", torch.ones((1, 512), dtype=torch.float32, device=DEV))
+    with pytest.raises(MapleError):
+        c.solve("elastic", "fp64")  # no density loaded yet
+    c.close()
