@@ -151,6 +151,18 @@ int maple_oc_step(maple_ctx* ctx, const double* x, const double* weights, const 
                   int warm, double* x_next, double* J, double* terms, double* CH, double* kappa, double* stats,
                   int* iters_out_host, maple_stream_t stream);
 
+/* Number of kernels this library has launched in this process (all
+ * contexts); used to count device launches inside a timed region. */
+unsigned long long maple_launch_count(void);
+
+/* Instrumentation: when enabled, every fine-level operator launch of this
+ * context is bracketed by CUDA events (at most max_launches are kept).
+ * maple_profile_read writes a JSON object {kernel class: {launches, total_ms,
+ * bytes_per_launch}} into buf, bytes_per_launch being the algorithmic bytes
+ * (each input read once, each output written once). */
+int maple_profile_enable(maple_ctx* ctx, int enable, int max_launches);
+int maple_profile_read(maple_ctx* ctx, char* buf, int buflen);
+
 #ifdef __cplusplus
 }
 #endif

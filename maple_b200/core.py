@@ -106,6 +106,16 @@ class HomogenizationContext:
         with torch.cuda.device(self.device):
             _lib.check(self._lib.maple_set_active(self._h, arr, _stream(self.device)))
 
+    def profile(self, enable: bool, max_launches: int = 100000):
+        """Bracket every fine-level operator launch with CUDA events."""
+        _lib.check(self._lib.maple_profile_enable(self._h, int(bool(enable)), int(max_launches)))
+
+    def profile_read(self) -> dict:
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        _lib.check(self._lib.maple_profile_read(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     # ------------------------------------------------------------------
     def _check(self, t: torch.Tensor, name: str, shape=None):
         if not isinstance(t, torch.Tensor):
@@ -237,6 +247,11 @@ class HomogenizationContext:
                 _ptr(out["stats"]), it.ctypes.data_as(C.POINTER(C.c_int)), _stream(dev)))
         out["iters"] = it
         return out
+
+
+def launch_count() -> int:
+    """Kernels launched by libmaple_b200 in this process so far."""
+    return int(_lib.load().maple_launch_count())
 
 
 def box_filter(x: torch.Tensor, r: int, k: int = 3) -> torch.Tensor:

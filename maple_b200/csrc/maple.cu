@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
+#include <map>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -29,7 +31,12 @@ struct Failure {
       throw Failure{MAPLE_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) + " at " +   \
                                       std::string(__FILE__) + ":" + std::to_string(__LINE__)};    \
   } while (0)
-#define CKL() CK(cudaGetLastError())
+static std::atomic<unsigned long long> g_launches{0};
+#define CKL()                         \
+  do {                                \
+    CK(cudaGetLastError());           \
+    g_launches.fetch_add(1);          \
+  } while (0)
 
 static void require(bool ok, const std::string& msg) {
   if (!ok) throw Failure{MAPLE_E_BADARG, msg};
@@ -140,6 +147,16 @@ struct maple_ctx {
   unsigned* bar = nullptr;
   int* err = nullptr;
   int oc_G = 0;
+  // per-kernel-class event timing of fine-level launches (bench instrumentation)
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  struct Rec {
+    std::string name;
+    double bytes;
+    size_t ev;
+  };
+  std::vector<Rec> recs;
   // options
   int cheb_degree = 2;
   double cheb_ratio = 10.0;
@@ -237,7 +254,20 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
   const dim3 g = g2(a.N, c->B);
   if (l == 0) {
     a.rho = o.rho;
+    const bool rec = c->profiling && c->ev_used + 2 <= c->ev_pool.size();
+    if (rec) CK(cudaEventRecord(c->ev_pool[c->ev_used], s));
     k_apply_fine<T, D, R, MODE><<<g, kThreads, 0, s>>>(a);
+    if (rec) {
+      CK(cudaEventRecord(c->ev_pool[c->ev_used + 1], s));
+      static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
+      // algorithmic bytes: rho once, each vector read or written once
+      const int nvec = MODE == M_MV ? 2 : MODE == M_RES ? 3 : MODE == M_CHEB ? 5 : MODE == M_JAC0 ? 3 : 2;
+      const double bytes = (double)c->B * a.N * ((double)sizeof(T) + (double)nvec * R * D * sizeof(T));
+      c->recs.push_back({std::string("k_apply_fine<") + (sizeof(T) == 8 ? "f64," : "f32,") + std::to_string(D) +
+                             "," + std::to_string(R) + "," + mname[MODE] + ">",
+                         bytes, c->ev_used});
+      c->ev_used += 2;
+    }
   } else {
     a.S = o.S[l];
     a.Dinv = o.Dinv[l];
@@ -695,6 +725,7 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
     CK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned), s));
     void* args[] = {&a};
     CK(cudaLaunchCooperativeKernel((void*)k_oc_update, dim3(G, nb), dim3(kThreads), args, 0, s));
+    g_launches.fetch_add(1);
   }
 }
 
@@ -834,9 +865,63 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
   });
 }
 
+unsigned long long maple_launch_count(void) { return g_launches.load(); }
+
+int maple_profile_enable(maple_ctx* c, int enable, int max_launches) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    if (enable) {
+      require(max_launches >= 1 && max_launches <= (1 << 20), "max_launches out of range");
+      const size_t want = (size_t)2 * max_launches;
+      while (c->ev_pool.size() < want) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        c->ev_pool.push_back(e);
+      }
+    }
+    c->ev_used = 0;
+    c->recs.clear();
+    c->profiling = enable != 0;
+  });
+}
+
+int maple_profile_read(maple_ctx* c, char* buf, int buflen) {
+  return guarded([&] {
+    require(c != nullptr && buf != nullptr && buflen > 0, "NULL argument");
+    for (auto& e : c->ev_pool) (void)e;
+    if (!c->recs.empty()) CK(cudaEventSynchronize(c->ev_pool[c->recs.back().ev + 1]));
+    struct Acc {
+      long n = 0;
+      double ms = 0, bytes = 0;
+    };
+    std::map<std::string, Acc> acc;
+    for (const auto& r : c->recs) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, c->ev_pool[r.ev], c->ev_pool[r.ev + 1]));
+      Acc& a = acc[r.name];
+      a.n += 1;
+      a.ms += ms;
+      a.bytes = r.bytes;
+    }
+    std::string out = "{";
+    bool first = true;
+    for (const auto& kv : acc) {
+      char tmp[512];
+      snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %ld, \"total_ms\": %.6f, \"bytes_per_launch\": %.1f}",
+               first ? "" : ", ", kv.first.c_str(), kv.second.n, kv.second.ms, kv.second.bytes);
+      out += tmp;
+      first = false;
+    }
+    out += "}";
+    require((int)out.size() < buflen, "profile buffer too small");
+    memcpy(buf, out.c_str(), out.size() + 1);
+  });
+}
+
 int maple_ctx_destroy(maple_ctx* c) {
   return guarded([&] {
     if (!c) return;
+    for (auto& e : c->ev_pool) cudaEventDestroy(e);
     for (void* p : c->allocs) cudaFree(p);
     if (c->h_flags) cudaFreeHost(c->h_flags);
     delete c;
