@@ -16,6 +16,7 @@
 namespace maple {
 
 constexpr int kThreads = 256;
+constexpr int TX = 4, TY = 8, TZ = 8;  // fine-level node tile per CTA (z fastest)
 
 __constant__ double c_Ke3d[576];
 __constant__ float c_Ke3f[576];
@@ -256,6 +257,37 @@ __device__ __forceinline__ void fine_all(std::integer_sequence<int, Os...>, cons
   (fine_accumulate<T, D, R, Os>(rq, u, cell_off, n, xs, ys, zs, acc, C0), ...);
 }
 
+template <typename T, int D, int R, int RW, int NS, int O>
+__device__ __forceinline__ void fine_tile_accumulate(const T (&rq)[8], const T* __restrict__ base, T (&acc)[R][D],
+                                                     T (&C0)[D][D]) {
+  T C[D][D];
+  fine_block<T, D, O>(rq, C);
+  constexpr int ox = O / 9, oy = (O / 3) % 3, oz = O % 3;
+  const T* un = base + (ox * (TY + 2) + oy) * RW + oz * NS;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    T uv[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) uv[j] = un[r * D + j];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) acc[r][i] += C[i][j] * uv[j];
+  }
+  if constexpr (O == 13) {
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) C0[i][j] = C[i][j];
+  }
+}
+
+template <typename T, int D, int R, int RW, int NS, int... Os>
+__device__ __forceinline__ void fine_tile_all(std::integer_sequence<int, Os...>, const T (&rq)[8],
+                                              const T* __restrict__ base, T (&acc)[R][D], T (&C0)[D][D]) {
+  (fine_tile_accumulate<T, D, R, RW, NS, Os>(rq, base, acc, C0), ...);
+}
+
 // Shared epilogue of both apply kernels.
 template <typename T, int D, int R, int MODE>
 __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, size_t vo, bool valid, T (&acc)[R][D],
@@ -316,18 +348,75 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fine-level tile geometry: a CTA owns TX x TY x TZ nodes (z fastest, 256
+// threads) and stages the (TX+2)(TY+2)(TZ+2) halo'd nodes' R*D values in
+// shared memory.  Node stride NS is odd and each (x,y) row is padded so that
+// the 32 lanes of a warp (tz 0..7, ty 0..3) hit 32 distinct banks.
+// ---------------------------------------------------------------------------
+static_assert(TX * TY * TZ == kThreads, "tile must match the block size");
+
+template <typename T, int RD>
+struct FineTile {
+  static constexpr int NS = (RD % 2) ? RD : RD + 1;        // node stride (words of T)
+  static constexpr int ROW0 = (TZ + 2) * NS;
+  static constexpr int MOD = sizeof(T) == 8 ? 16 : 32;      // bank period in units of T
+  static constexpr int WANT = (8 * NS) % MOD;
+  static constexpr int RW = ROW0 + ((WANT - ROW0 % MOD) % MOD + MOD) % MOD;  // row stride
+  static constexpr int HALO_NODES = (TX + 2) * (TY + 2) * (TZ + 2);
+  static constexpr int U_WORDS = (TX + 2) * (TY + 2) * RW;
+  static constexpr int RHO_WORDS = (TX + 1) * (TY + 1) * (TZ + 1);
+  static constexpr size_t BYTES = (size_t)(U_WORDS + RHO_WORDS) * sizeof(T);
+  static_assert(RW % MOD == WANT, "row padding");
+};
+
+__host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+__host__ __device__ inline int fine_tiles(int n) { return ceil_div(n, TX) * ceil_div(n, TY) * ceil_div(n, TZ); }
+
 template <typename T, int D, int R, int MODE>
 __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
+  using G = FineTile<T, R * D>;
+  constexpr int RD = R * D;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* su = reinterpret_cast<T*>(smem_raw);
+  T* srho = su + G::U_WORDS;
   const int b = blockIdx.y;
   if (a.active && !a.active[b]) return;
   const int n = a.n;
-  const int idx = blockIdx.x * kThreads + threadIdx.x;
-  const bool valid = idx < a.N;
-  const int id = valid ? idx : 0;
-  const int z = id % n, y = (id / n) % n, x = id / (n * n);
+  const int ntz = ceil_div(n, TZ), nty = ceil_div(n, TY);
+  const int tile = blockIdx.x;
+  const int z0 = (tile % ntz) * TZ, y0 = ((tile / ntz) % nty) * TY, x0 = (tile / (ntz * nty)) * TX;
+  const int tz = threadIdx.x % TZ, ty = (threadIdx.x / TZ) % TY, tx = threadIdx.x / (TZ * TY);
+  const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
+  const bool valid = x < n && y < n && z < n;
   const size_t cell = (size_t)b * a.N;
+  // ---- stage densities of the (TX+1)(TY+1)(TZ+1) elements touching the tile
+  for (int w = threadIdx.x; w < G::RHO_WORDS; w += kThreads) {
+    const int iz = w % (TZ + 1), iy = (w / (TZ + 1)) % (TY + 1), ix = w / ((TZ + 1) * (TY + 1));
+    const int gx = wrapn(x0 - 1 + ix, n), gy = wrapn(y0 - 1 + iy, n), gz = wrapn(z0 - 1 + iz, n);
+    const int ox = gx < n ? gx : gx % n, oy = gy < n ? gy : gy % n, oz = gz < n ? gz : gz % n;
+    srho[w] = __ldg(a.rho + cell + ((size_t)ox * n + oy) * n + oz);
+  }
+  // ---- stage the halo'd node values (skipped when only the diagonal is needed)
+  if constexpr (MODE != M_JAC0) {
+    for (int w = threadIdx.x; w < G::HALO_NODES * RD; w += kThreads) {
+      const int node = w / RD, k = w - node * RD;
+      const int iz = node % (TZ + 2), iy = (node / (TZ + 2)) % (TY + 2), ix = node / ((TZ + 2) * (TY + 2));
+      int gx = x0 - 1 + ix, gy = y0 - 1 + iy, gz = z0 - 1 + iz;
+      gx = ((gx % n) + n) % n;
+      gy = ((gy % n) + n) % n;
+      gz = ((gz % n) + n) % n;
+      su[(ix * (TY + 2) + iy) * G::RW + iz * G::NS + k] =
+          __ldg(a.u + (cell + ((size_t)gx * n + gy) * n + gz) * RD + k);
+    }
+  }
+  __syncthreads();
   T rq[8];
-  load_rho8<T>(a.rho + cell, n, x, y, z, rq);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
+    rq[q] = srho[((tx + qx) * (TY + 1) + (ty + qy)) * (TZ + 1) + (tz + qz)];
+  }
   T acc[R][D];
 #pragma unroll
   for (int r = 0; r < R; ++r)
@@ -337,10 +426,8 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
   if constexpr (MODE == M_JAC0) {
     fine_block<T, D, 13>(rq, C0);
   } else {
-    const int xs[3] = {wrapn(x - 1, n), x, wrapn(x + 1, n)};
-    const int ys[3] = {wrapn(y - 1, n), y, wrapn(y + 1, n)};
-    const int zs[3] = {wrapn(z - 1, n), z, wrapn(z + 1, n)};
-    fine_all<T, D, R>(std::make_integer_sequence<int, 27>{}, rq, a.u, cell, n, xs, ys, zs, acc, C0);
+    const T* base = su + (tx * (TY + 2) + ty) * G::RW + tz * G::NS;
+    fine_tile_all<T, D, R, G::RW, G::NS>(std::make_integer_sequence<int, 27>{}, rq, base, acc, C0);
   }
   T Di[D][D];
   T C0s[D][D];
@@ -349,13 +436,9 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
 #pragma unroll
     for (int j = 0; j < D; ++j) C0s[i][j] = a.scale * C0[i][j];
   block_inverse<T, D>(C0s, Di);
-  const size_t vo = (cell + id) * (R * D);
+  const int id = valid ? (x * n + y) * n + z : 0;
+  const size_t vo = (cell + id) * RD;
   if constexpr (MODE == M_POWER) {
-    // second Rayleigh term u.Du with the assembled diagonal block
-    double ud = 0;
-    if (valid)
-      for (int i = 0; i < D; ++i)
-        for (int j = 0; j < D; ++j) ud += (double)a.u[vo + i] * (double)C0s[i][j] * (double)a.u[vo + j];
     double dots[2] = {0, 0};
     if (valid) {
       T Au[D];
@@ -365,8 +448,8 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
         for (int j = 0; j < D; ++j) w += Di[i][j] * Au[j];
         a.out[vo + i] = w;
         dots[0] += (double)a.u[vo + i] * (double)Au[i];
+        for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i] * (double)C0s[i][j] * (double)a.u[vo + j];
       }
-      dots[1] = ud;
     }
     block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
   } else {
@@ -919,6 +1002,55 @@ __global__ void k_add_f32_scaled(double* __restrict__ dst, const float* __restri
 #pragma unroll
     for (int i = 0; i < D; ++i) dst[o + c * D + i] += s * (double)src[o + c * D + i];
   }
+}
+
+// per (cell, rhs): scale = 1/||r||, inv = ||r|| from the reduced r.r
+__global__ void k_col_scales(const double* __restrict__ rr, double* __restrict__ scale, double* __restrict__ inv,
+                             int total) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const double nrm = sqrt(fmax(rr[i], 0.0));
+  scale[i] = nrm > 0 ? 1.0 / nrm : 0.0;
+  inv[i] = nrm;
+}
+
+// z = inv * z32 (FP64) with partial dots r.z and (optionally) q.z
+template <int R, int D>
+__global__ void k_precond_back(const float* __restrict__ z32, const double* __restrict__ inv, double* __restrict__ z,
+                               const double* __restrict__ r, const double* __restrict__ q, double* __restrict__ part,
+                               int N, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  double v[2 * R] = {};
+  if (idx < N) {
+    const size_t o = ((size_t)b * N + idx) * R * D;
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      const double s = inv[b * R + c];
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const double zv = s * (double)z32[o + c * D + i];
+        z[o + c * D + i] = zv;
+        v[c] += r[o + c * D + i] * zv;
+        if (q) v[R + c] += q[o + c * D + i] * zv;
+      }
+    }
+  }
+  block_sum_store<2 * R>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * 2 * R);
+}
+
+// flexible (Polak-Ribiere) beta = -alpha (z.q) / (r.z)_old ; rz <- rz_new.
+// red holds [cell][rz_new (R), zq (R)].
+__global__ void k_pcg_beta_flex(PcgScalars s, const double* __restrict__ red, int B, int R, int first) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= B * R) return;
+  const int b = i / R, c = i % R;
+  const double rz_new = red[b * 2 * R + c], zq = red[b * 2 * R + R + c];
+  double be = 0.0;
+  if (!first && !s.done[i] && s.rz[i] != 0.0) be = -s.alpha[i] * zq / s.rz[i];
+  s.beta[i] = be;
+  s.rz[i] = rz_new;
 }
 
 // deterministic pseudo-random start vector for power iterations

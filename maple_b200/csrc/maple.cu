@@ -110,7 +110,8 @@ struct Phys {
   double* cwork = nullptr;
   double* F64 = nullptr;         // RHS [B][N][R][D]
   double* u64 = nullptr;         // solution
-  double* r64 = nullptr;         // outer residual
+  double* r64 = nullptr;         // residual (FP64)
+  double *p64 = nullptr, *q64 = nullptr, *z64 = nullptr;  // mixed-precision PCG vectors
   double* energy = nullptr;      // [B][N][R][R]
   double* H = nullptr;           // [B][R][R]
   Ops<double> o64;
@@ -248,15 +249,24 @@ template <typename T, int D, int R, int MODE>
 static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const int* act, cudaStream_t s) {
   a.n = c->n[l];
   a.N = nodes(a.n);
-  a.scale = (T)p.kscale;
+  // the fine level applies the unit-voxel Ke0 and scales it; coarse stencils
+  // were built from scaled element matrices already
+  a.scale = l == 0 ? (T)p.kscale : (T)1;
   a.active = act;
   a.ratio = c->cheb_ratio;
   const dim3 g = g2(a.N, c->B);
   if (l == 0) {
     a.rho = o.rho;
     const bool rec = c->profiling && c->ev_used + 2 <= c->ev_pool.size();
+    using G = FineTile<T, R * D>;
+    static bool attr_set = false;  // one per template instantiation
+    if (!attr_set) {
+      CK(cudaFuncSetAttribute(k_apply_fine<T, D, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)G::BYTES));
+      attr_set = true;
+    }
     if (rec) CK(cudaEventRecord(c->ev_pool[c->ev_used], s));
-    k_apply_fine<T, D, R, MODE><<<g, kThreads, 0, s>>>(a);
+    k_apply_fine<T, D, R, MODE><<<dim3(fine_tiles(a.n), c->B), kThreads, G::BYTES, s>>>(a);
     if (rec) {
       CK(cudaEventRecord(c->ev_pool[c->ev_used + 1], s));
       static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
@@ -482,7 +492,8 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
   const int B = c->B, N = nodes(c->n[0]);
   const size_t vbytes = (size_t)B * N * R * D * sizeof(T);
   Scalars& sc = c->sc;
-  const unsigned nb = nblk(N);
+  const unsigned nb = nblk(N);                    // partials of the vector kernels
+  const unsigned nbf = (unsigned)fine_tiles(c->n[0]);  // partials of the fine-level operator
   PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
   k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, outer_run, sc.done, sc.cell_done, sc.run, sc.iters, B, R);
   CKL();
@@ -511,7 +522,7 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
   if (all_done(c, sc.cell_done, run, s)) return;
   // z = M r ; rz ; p = z
   vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, s);
-  reduce<R>(c, c->part, nb, sc.rz_new, s);
+  reduce<R>(c, c->part, nbf, sc.rz_new, s);
   k_set_rz<<<nblk(B * R), kThreads, 0, s>>>(sc.rz, sc.rz_new, B * R);
   CKL();
   CK(cudaMemcpyAsync(o.p, o.U[0][1], vbytes, cudaMemcpyDeviceToDevice, s));
@@ -523,7 +534,7 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
       a.part = c->part;
       apply<T, D, R, M_MV>(c, p, o, 0, a, run, s);
     }
-    reduce<R>(c, c->part, nb, sc.pq, s);
+    reduce<R>(c, c->part, nbf, sc.pq, s);
     k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown);
     CKL();
     k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.x, o.r, o.p, o.q, sc.alpha, c->part, N, run);
@@ -536,10 +547,96 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
     if (it == maxit) break;
     if (it % c->check_every == 0 && all_done(c, sc.cell_done, run, s)) break;
     vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, s);
-    reduce<R>(c, c->part, nb, sc.rz_new, s);
+    reduce<R>(c, c->part, nbf, sc.rz_new, s);
     k_pcg_beta<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R);
     CKL();
     k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.p, o.U[0][1], sc.beta, N, run);
+    CKL();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision: FP64 flexible PCG (FP64 fine operator, residuals and dots)
+// preconditioned by the FP32 V-cycle; the coarsest solve stays FP64.
+// ---------------------------------------------------------------------------
+template <int D, int R>
+static void precondition_f32(maple_ctx* c, Phys& p, const double* r, const double* q, const int* run,
+                             cudaStream_t s) {
+  const int B = c->B, N = nodes(c->n[0]);
+  Scalars& sc = c->sc;
+  Ops<float>& o = p.o32;
+  k_col_scales<<<nblk(B * R), kThreads, 0, s>>>(sc.rr, c->o_scale, c->o_inv, B * R);
+  CKL();
+  k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, c->o_scale, N, run);
+  CKL();
+  vcycle<float, D, R>(c, p, o, 0, o.r, run, nullptr, s);
+  k_precond_back<R, D><<<g2(N, B), kThreads, 0, s>>>(o.U[0][1], c->o_inv, p.z64, r, q, c->part, N, run);
+  CKL();
+  reduce<2 * R>(c, c->part, nblk(N), c->red, s);
+}
+
+template <int D, int R>
+static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_zero, double rtol, int maxit,
+                      cudaStream_t s) {
+  const int B = c->B, N = nodes(c->n[0]);
+  const size_t vbytes = (size_t)B * N * R * D * sizeof(double);
+  Scalars& sc = c->sc;
+  const unsigned nb = nblk(N), nbf = (unsigned)fine_tiles(c->n[0]);
+  PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
+  Ops<double>& o64 = p.o64;
+  double *r = p.r64, *pv = p.p64, *q = p.q64, *z = p.z64;
+  k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, nullptr, sc.done, sc.cell_done, sc.run, sc.iters, B, R);
+  CKL();
+  const int* run = sc.run;
+  if (x_zero) {
+    CK(cudaMemsetAsync(x, 0, vbytes, s));
+    CK(cudaMemcpyAsync(r, b, vbytes, cudaMemcpyDeviceToDevice, s));
+  } else {
+    ApplyArgs<double> a{};
+    a.u = x;
+    a.f = b;
+    a.out = r;
+    apply<double, D, R, M_RES>(c, p, o64, 0, a, run, s);
+  }
+  k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, c->part, N, run);
+  CKL();
+  reduce<R>(c, c->part, nb, sc.bnorm2, s);
+  k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(r, r, c->part, N, run);
+  CKL();
+  reduce<R>(c, c->part, nb, sc.rr, s);
+  k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0);
+  CKL();
+  k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B);
+  CKL();
+  if (all_done(c, sc.cell_done, run, s)) return;
+  precondition_f32<D, R>(c, p, r, nullptr, run, s);
+  k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 1);
+  CKL();
+  CK(cudaMemcpyAsync(pv, z, vbytes, cudaMemcpyDeviceToDevice, s));
+  for (int it = 1; it <= maxit; ++it) {
+    {
+      ApplyArgs<double> a{};
+      a.u = pv;
+      a.out = q;
+      a.part = c->part;
+      apply<double, D, R, M_MV>(c, p, o64, 0, a, run, s);
+    }
+    reduce<R>(c, c->part, nbf, sc.pq, s);
+    k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown);
+    CKL();
+    k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, s>>>(x, r, pv, q, sc.alpha, c->part, N, run);
+    CKL();
+    reduce<R>(c, c->part, nb, sc.rr, s);
+    k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, it);
+    CKL();
+    k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B);
+    CKL();
+    if (it == maxit) break;
+    if (it % c->check_every == 0 && all_done(c, sc.cell_done, run, s)) break;
+    precondition_f32<D, R>(c, p, r, q, run, s);
+    k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 0);
+    CKL();
+    k_pcg_direction<double, R, D><<<g2(N, B), kThreads, 0, s>>>(pv, z, sc.beta, N, run);
     CKL();
   }
 }
@@ -589,45 +686,15 @@ static void solve_phys(maple_ctx* c, int phys, int prec, const double* F, double
       if (status_host) status_host[b] = cd[b] ? MAPLE_CELL_CONVERGED : MAPLE_CELL_MAXIT;
     }
   } else {
-    Ops<double>& o64 = p.o64;
-    Ops<float>& o = p.o32;
-    if (x_zero) CK(cudaMemsetAsync(x64, 0, vb64, s));
-    k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(F, F, c->part, N, c->active);
-    CKL();
-    reduce<R>(c, c->part, nb, c->o_bn, s);
-    bool converged = false;
-    for (int outer = 0; outer < 12; ++outer) {
-      ApplyArgs<double> a{};
-      a.u = x64;
-      a.f = F;
-      a.out = p.r64;
-      a.part = c->part;
-      apply<double, D, R, M_RES>(c, p, o64, 0, a, c->active, s);
-      reduce<R>(c, c->part, nb, c->o_rr, s);
-      k_outer_check<<<nblk(B), kThreads, 0, s>>>(c->o_rr, c->o_bn, rtol * rtol, c->o_scale, c->o_inv, c->o_done,
-                                                  c->o_run, c->active, B, R);
-      CKL();
-      if (all_done(c, c->o_done, nullptr, s)) {
-        converged = true;
-        break;
-      }
-      k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(p.r64, o.Res[0], c->o_scale, N, c->o_run);
-      CKL();
-      // inner solve: A d = r (unit-norm columns), d in o.x
-      pcg<float, D, R>(c, p, o, o.Res[0], true, c->inner_rtol, maxit, c->o_run, s);
-      k_add_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(x64, o.x, c->o_inv, N, c->o_run);
-      CKL();
-      std::vector<int> it(B);
-      CK(cudaMemcpyAsync(it.data(), c->sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      for (int b = 0; b < B; ++b) it_total[b] += it[b];
-    }
-    std::vector<int> od(B);
-    CK(cudaMemcpyAsync(od.data(), c->o_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    pcg_mixed<D, R>(c, p, F, x64, x_zero, rtol, maxit, s);
+    std::vector<int> it(B), cd(B);
+    CK(cudaMemcpyAsync(it.data(), c->sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(cd.data(), c->sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    for (int b = 0; b < B; ++b)
-      if (status_host) status_host[b] = od[b] ? MAPLE_CELL_CONVERGED : MAPLE_CELL_MAXIT;
-    (void)converged;
+    for (int b = 0; b < B; ++b) {
+      it_total[b] = it[b];
+      if (status_host) status_host[b] = cd[b] ? MAPLE_CELL_CONVERGED : MAPLE_CELL_MAXIT;
+    }
   }
   if (iters_host)
     for (int b = 0; b < B; ++b) iters_host[b] = it_total[b];
@@ -646,7 +713,15 @@ static void ensure_prec(maple_ctx* c, int phys, int prec) {
   Phys& p = c->ph[phys];
   alloc_phys(c, phys);
   alloc_ops<double>(c, p, p.o64, prec == MAPLE_FP64);
-  if (prec == MAPLE_MIXED) alloc_ops<float>(c, p, p.o32, true);
+  if (prec == MAPLE_MIXED) {
+    alloc_ops<float>(c, p, p.o32, true);
+    if (!p.p64) {
+      const size_t n = (size_t)c->B * nodes(c->n[0]) * p.R * p.D;
+      p.p64 = dnew<double>(c, n);
+      p.q64 = dnew<double>(c, n);
+      p.z64 = dnew<double>(c, n);
+    }
+  }
 }
 
 static void load_density(maple_ctx* c, int phys, const double* rho, int prec, cudaStream_t s) {
@@ -815,7 +890,7 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
       c->ph[1].xscale = h;
       const int B = ncells;
       const size_t N0 = nodes(r);
-      c->part = dnew<double>(c, (size_t)B * nblk(N0) * 32);
+      c->part = dnew<double>(c, (size_t)B * std::max<size_t>(nblk(N0), fine_tiles(r)) * 32);
       c->red = dnew<double>(c, (size_t)B * 32);
       c->sc.rz = dnew<double>(c, B * 6);
       c->sc.rz_new = dnew<double>(c, B * 6);

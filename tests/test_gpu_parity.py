@@ -204,3 +204,26 @@ def test_bad_arguments(lib):
     with pytest.raises(MapleError):
         c.solve("elastic", "fp64")  # no density loaded yet
     c.close()
+
+
+def test_multigrid_quality_iteration_counts(lib):
+    """A CPU emulation of this exact MG-PCG (Chebyshev-2 block-Jacobi smoothing,
+    Galerkin levels down to 4^3, dense FP64 coarsest) needs 25 elastic and 13
+    thermal iterations to rtol 1e-10 on this 32^3 density from zero; a defective
+    level (operator, transfer or smoother) shows up as extra iterations."""
+    from maple_b200.core import HomogenizationContext
+    r = 32
+    x = O.seed_density(0, r, 2.0, 0.25)
+    rho = T(simp(x).reshape(1, -1))
+    c = HomogenizationContext(r, ncells=1)
+    H = {}
+    for prec in ("fp64", "mixed"):
+        for phys, cap in (("elastic", 30), ("thermal", 16)):
+            c.set_density(phys, rho, prec)
+            info = c.solve(phys, prec, rtol=1e-10, maxit=300)
+            assert info.status[0] & 1
+            assert info.iters[0] <= cap + (3 if prec == "mixed" else 0), (prec, phys, info.iters[0])
+            H[(prec, phys)] = c.homogenize(phys).cpu().numpy()[0]
+    for phys in ("elastic", "thermal"):
+        assert rel(H[("mixed", phys)], H[("fp64", phys)]) < 1e-9
+    c.close()
