@@ -257,6 +257,67 @@ __device__ __forceinline__ void fine_all(std::integer_sequence<int, Os...>, cons
   (fine_accumulate<T, D, R, Os>(rq, u, cell_off, n, xs, ys, zs, acc, C0), ...);
 }
 
+template <typename T, int RD>
+struct FineTile {
+  // Vector width (elements of T) of shared-memory reads and async copies:
+  // pairs (8 B for float, 16 B for double) when a node holds an even count.
+  static constexpr int VW = (RD % 2 == 0) ? 2 : 1;
+  static constexpr int NS = RD;                            // node stride (T)
+  static constexpr int ROW0 = (TZ + 2) * NS;
+  // Row stride: warp lanes are (tz 0..7, ty 0..3).  Scalar reads need
+  // RW = 8*NS (mod 32 banks, 16 for double) with NS odd; float2 reads are
+  // issued per half-warp and need RW = 8*NS (mod 32); double2 reads per
+  // quarter-warp are conflict-free for any even RW.
+  static constexpr int MOD = (VW == 2 && sizeof(T) == 8) ? 2 : (sizeof(T) == 8 ? 16 : 32);
+  static constexpr int WANT = (VW == 2 && sizeof(T) == 8) ? 0 : (8 * NS) % MOD;
+  static constexpr int RW = ROW0 + ((WANT - ROW0 % MOD) % MOD + MOD) % MOD;
+  static constexpr int HALO_NODES = (TX + 2) * (TY + 2) * (TZ + 2);
+  static constexpr int U_WORDS = (TX + 2) * (TY + 2) * RW;
+  static constexpr int RHO_WORDS = (TX + 1) * (TY + 1) * (TZ + 1);
+  static constexpr int RHO_OFF = (U_WORDS + 1) / 2 * 2;     // keep rho 8/16-byte aligned
+  static constexpr size_t BYTES = (size_t)(RHO_OFF + RHO_WORDS) * sizeof(T);
+  static_assert(RW % MOD == WANT, "row padding");
+  static_assert(VW == 1 || (NS % 2 == 0 && RW % 2 == 0), "vector alignment");
+};
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+
+// asynchronous global -> shared copy of BYTES (4, 8 or 16) bytes
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gsrc), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
+template <typename T, int RD, int VW>
+__device__ __forceinline__ void lds_node(const T* __restrict__ p, T (&v)[RD]) {
+  if constexpr (VW == 2) {
+    using V = typename Vec2<T>::type;
+#pragma unroll
+    for (int i = 0; i < RD / 2; ++i) {
+      const V t = reinterpret_cast<const V*>(p)[i];
+      v[2 * i] = t.x;
+      v[2 * i + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < RD; ++i) v[i] = p[i];
+  }
+}
+
 template <typename T, int D, int R, int RW, int NS, int O>
 __device__ __forceinline__ void fine_tile_accumulate(const T (&rq)[8], const T* __restrict__ base, T (&acc)[R][D],
                                                      T (&C0)[D][D]) {
@@ -264,16 +325,14 @@ __device__ __forceinline__ void fine_tile_accumulate(const T (&rq)[8], const T* 
   fine_block<T, D, O>(rq, C);
   constexpr int ox = O / 9, oy = (O / 3) % 3, oz = O % 3;
   const T* un = base + (ox * (TY + 2) + oy) * RW + oz * NS;
+  T uv[R * D];
+  lds_node<T, R * D, (R * D) % 2 == 0 ? 2 : 1>(un, uv);
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    T uv[D];
-#pragma unroll
-    for (int j = 0; j < D; ++j) uv[j] = un[r * D + j];
+  for (int r = 0; r < R; ++r)
 #pragma unroll
     for (int i = 0; i < D; ++i)
 #pragma unroll
-      for (int j = 0; j < D; ++j) acc[r][i] += C[i][j] * uv[j];
-  }
+      for (int j = 0; j < D; ++j) acc[r][i] += C[i][j] * uv[r * D + j];
   if constexpr (O == 13) {
 #pragma unroll
     for (int i = 0; i < D; ++i)
@@ -356,20 +415,6 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
 // ---------------------------------------------------------------------------
 static_assert(TX * TY * TZ == kThreads, "tile must match the block size");
 
-template <typename T, int RD>
-struct FineTile {
-  static constexpr int NS = (RD % 2) ? RD : RD + 1;        // node stride (words of T)
-  static constexpr int ROW0 = (TZ + 2) * NS;
-  static constexpr int MOD = sizeof(T) == 8 ? 16 : 32;      // bank period in units of T
-  static constexpr int WANT = (8 * NS) % MOD;
-  static constexpr int RW = ROW0 + ((WANT - ROW0 % MOD) % MOD + MOD) % MOD;  // row stride
-  static constexpr int HALO_NODES = (TX + 2) * (TY + 2) * (TZ + 2);
-  static constexpr int U_WORDS = (TX + 2) * (TY + 2) * RW;
-  static constexpr int RHO_WORDS = (TX + 1) * (TY + 1) * (TZ + 1);
-  static constexpr size_t BYTES = (size_t)(U_WORDS + RHO_WORDS) * sizeof(T);
-  static_assert(RW % MOD == WANT, "row padding");
-};
-
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 __host__ __device__ inline int fine_tiles(int n) { return ceil_div(n, TX) * ceil_div(n, TY) * ceil_div(n, TZ); }
 
@@ -379,7 +424,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
   constexpr int RD = R * D;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);
-  T* srho = su + G::U_WORDS;
+  T* srho = su + G::RHO_OFF;
   const int b = blockIdx.y;
   if (a.active && !a.active[b]) return;
   const int n = a.n;
@@ -391,25 +436,34 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
   const bool valid = x < n && y < n && z < n;
   const size_t cell = (size_t)b * a.N;
   // ---- stage densities of the (TX+1)(TY+1)(TZ+1) elements touching the tile
+  //      and the halo'd node values, all as asynchronous copies in flight
+  const int xm = x0 - 1, ym = y0 - 1, zm = z0 - 1;
   for (int w = threadIdx.x; w < G::RHO_WORDS; w += kThreads) {
     const int iz = w % (TZ + 1), iy = (w / (TZ + 1)) % (TY + 1), ix = w / ((TZ + 1) * (TY + 1));
-    const int gx = wrapn(x0 - 1 + ix, n), gy = wrapn(y0 - 1 + iy, n), gz = wrapn(z0 - 1 + iz, n);
-    const int ox = gx < n ? gx : gx % n, oy = gy < n ? gy : gy % n, oz = gz < n ? gz : gz % n;
-    srho[w] = __ldg(a.rho + cell + ((size_t)ox * n + oy) * n + oz);
+    int gx = xm + ix, gy = ym + iy, gz = zm + iz;
+    gx += gx < 0 ? n : (gx >= n ? -n : 0);
+    gy += gy < 0 ? n : (gy >= n ? -n : 0);
+    gz += gz < 0 ? n : (gz >= n ? -n : 0);
+    cp_async<sizeof(T)>(srho + w, a.rho + cell + ((size_t)gx * n + gy) * n + gz);
   }
-  // ---- stage the halo'd node values (skipped when only the diagonal is needed)
   if constexpr (MODE != M_JAC0) {
-    for (int w = threadIdx.x; w < G::HALO_NODES * RD; w += kThreads) {
-      const int node = w / RD, k = w - node * RD;
-      const int iz = node % (TZ + 2), iy = (node / (TZ + 2)) % (TY + 2), ix = node / ((TZ + 2) * (TY + 2));
-      int gx = x0 - 1 + ix, gy = y0 - 1 + iy, gz = z0 - 1 + iz;
-      gx = ((gx % n) + n) % n;
-      gy = ((gy % n) + n) % n;
-      gz = ((gz % n) + n) % n;
-      su[(ix * (TY + 2) + iy) * G::RW + iz * G::NS + k] =
-          __ldg(a.u + (cell + ((size_t)gx * n + gy) * n + gz) * RD + k);
+    constexpr int VW = G::VW;
+    constexpr int CH_NODE = RD / VW;                  // vector chunks per node
+    constexpr int CH_ROW = (TZ + 2) * CH_NODE;        // chunks per (x,y) row
+    constexpr int CH_ALL = (TX + 2) * (TY + 2) * CH_ROW;
+    for (int w = threadIdx.x; w < CH_ALL; w += kThreads) {
+      const int row = w / CH_ROW, cr = w - row * CH_ROW;
+      const int iz = cr / CH_NODE, kc = cr - iz * CH_NODE;
+      const int iy = row % (TY + 2), ix = row / (TY + 2);
+      int gx = xm + ix, gy = ym + iy, gz = zm + iz;
+      gx += gx < 0 ? n : (gx >= n ? -n : 0);
+      gy += gy < 0 ? n : (gy >= n ? -n : 0);
+      gz += gz < 0 ? n : (gz >= n ? -n : 0);
+      cp_async<VW * sizeof(T)>(su + row * G::RW + iz * G::NS + kc * VW,
+                               a.u + (cell + ((size_t)gx * n + gy) * n + gz) * RD + kc * VW);
     }
   }
+  cp_async_wait_all();
   __syncthreads();
   T rq[8];
 #pragma unroll
