@@ -9,7 +9,8 @@
  *
  * Layouts: a batch holds B periodic cells of r^3 voxels; element / node id is
  * x*r*r + y*r + z.  Design variables, densities and sensitivities are [B][N]
- * FP64; solution fields are [B][N][R][D] FP64 (R load cases of D components).
+ * FP64; solution fields are [B][R][D][N] FP64 (R load cases of D components,
+ * component-major so that consecutive nodes are contiguous).
  *
  * Each declaration names the reference interface (xing-yuu/MAPLE, paths under
  * src/maple/core) whose role it takes over.
@@ -89,27 +90,27 @@ int maple_set_density(maple_ctx* ctx, int physics, const double* rho, int precis
 int maple_solve(maple_ctx* ctx, int physics, int precision, double rtol, int maxit, int warm, int* iters_out_host,
                 int* status_out_host, maple_stream_t stream);
 
-/* Solve with a caller-provided RHS F [B][N][R][D] and initial guess x0
+/* Solve with a caller-provided RHS F [B][R][D][N] and initial guess x0
  * (nullable) on the density of the last maple_set_density: the
  * GMGSolver.solve(fine_ke, global_f, ...) surface of utils/EBE_GMG.py:758.
- * The solution is written to u_out [B][N][R][D] and the final residual
+ * The solution is written to u_out [B][R][D][N] and the final residual
  * F - K u to r_out (nullable). */
 int maple_solve_rhs(maple_ctx* ctx, int physics, int precision, const double* F, const double* x0, double rtol,
                     int maxit, double* u_out, double* r_out, int* iters_out_host, int* status_out_host,
                     maple_stream_t stream);
 
-/* Copy the current solution [B][N][R][D] of a physics into u_out. */
+/* Copy the current solution [B][R][D][N] of a physics into u_out. */
 int maple_get_solution(maple_ctx* ctx, int physics, double* u_out, maple_stream_t stream);
 
 /* Homogenized tensor H [B][R][R] = sum_e (X0-u_e)^T rho_e Ke0 (X0-u_e) and the
  * per-element energies kept for maple_sensitivity.  Replaces
  * utils/model.py:33-44 homogenized_batch_3d and 47-95
- * homogenized_batch_thermal.  energy_out [B][N][R][R] (nullable) receives a
+ * homogenized_batch_thermal.  energy_out [B][R][R][N] (nullable) receives a
  * copy of the per-element energies. */
 int maple_homogenize(maple_ctx* ctx, int physics, double* H_out, double* energy_out, maple_stream_t stream);
 
-/* out[b][e] (+)= sum_{r,s} g[b][r][s] * energy[b][e][r][s]: the contraction of
- * saved per-element energies [B][N][RR] (RR = R*R) with dJ/dH [B][RR]; the
+/* out[b][e] (+)= sum_{r,s} g[b][r][s] * energy[b][r][s][e]: the contraction of
+ * saved per-element energies [B][RR][N] (RR = R*R) with dJ/dH [B][RR]; the
  * backward pass of the homogenization (main_IHD_v3.py:688).  accumulate != 0
  * adds to out. */
 int maple_energy_contract(int ncells, int N, int RR, const double* energy, const double* g, int accumulate,
@@ -121,7 +122,7 @@ int maple_energy_contract(int ncells, int N, int RR, const double* energy, const
  * nullable), dJdrho [B][N]. */
 int maple_sensitivity(maple_ctx* ctx, const double* gC, const double* gK, double* dJdrho, maple_stream_t stream);
 
-/* RHS assembly F = sum_e rho_e Fe0 [B][N][R][D] (utils/_utils.py:453-507,
+/* RHS assembly F = sum_e rho_e Fe0 [B][R][D][N] (utils/_utils.py:453-507,
  * assemble_F_fast / assemble_F_fast_scalar). */
 int maple_assemble_rhs(maple_ctx* ctx, int physics, const double* rho, double* F_out, maple_stream_t stream);
 

@@ -132,7 +132,7 @@ class HomogenizationContext:
 
     def _vec_shape(self, phys):
         D, R = DR[phys]
-        return (self.B, self.N, R, D)
+        return (self.B, R, D, self.N)
 
     def set_density(self, physics, rho: torch.Tensor, precision="fp64"):
         """rho: (B, N) float64 element densities; builds that physics' hierarchy."""
@@ -176,11 +176,11 @@ class HomogenizationContext:
         return u
 
     def homogenize(self, physics, want_energy=False):
-        """Returns H (B,R,R) and, if asked, the per-element energies (B,N,R,R)."""
+        """Returns H (B,R,R) and, if asked, the per-element energies (B,R,R,N)."""
         ph = PHYSICS[physics]
         R = DR[ph][1]
         H = torch.empty((self.B, R, R), dtype=torch.float64, device=self.device)
-        E = torch.empty((self.B, self.N, R, R), dtype=torch.float64, device=self.device) if want_energy else None
+        E = torch.empty((self.B, R, R, self.N), dtype=torch.float64, device=self.device) if want_energy else None
         with torch.cuda.device(self.device):
             _lib.check(self._lib.maple_homogenize(self._h, ph, _ptr(H), _ptr(E), _stream(self.device)))
         return (H, E) if want_energy else H
@@ -269,10 +269,10 @@ def box_filter(x: torch.Tensor, r: int, k: int = 3) -> torch.Tensor:
 
 def energy_contract(energy: torch.Tensor, g: torch.Tensor, out: torch.Tensor | None = None,
                     accumulate: bool = False) -> torch.Tensor:
-    """out[b,e] (+)= sum_rs g[b,r,s] energy[b,e,r,s] on the device."""
-    B, N, R, R2 = energy.shape
+    """out[b,e] (+)= sum_rs g[b,r,s] energy[b,r,s,e] on the device."""
+    B, R, R2, N = energy.shape
     if R != R2 or g.shape != (B, R, R):
-        raise ValueError("energy (B,N,R,R) and g (B,R,R) shapes disagree")
+        raise ValueError("energy (B,R,R,N) and g (B,R,R) shapes disagree")
     for name, t in (("energy", energy), ("g", g)):
         if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
             raise ValueError(f"{name} must be a contiguous float64 CUDA tensor")

@@ -2,8 +2,8 @@
 //
 // Data layout (one "cell" = one periodic r^3 unit cell; B cells per context):
 //   * element / node id  x*n*n + y*n + z (maple/core/main_IHD_v3.py:175-186)
-//   * vectors: [cell][node][rhs][comp]  (DOF-interleaved, all load cases of a
-//     node contiguous: 18 values elastic, 3 thermal)
+//   * vectors: [cell][rhs][comp][node]  (component-major: a warp's accesses to
+//     consecutive nodes are contiguous for every load case and component)
 //   * coarse stencils: [cell][27][D*D][node]  (node fastest: coalesced)
 //   * element matrices of coarse levels: [cell][elem][8D][8D]  (FP64)
 // The element stiffness of the fine level lives in __constant__ memory for a
@@ -348,9 +348,11 @@ __device__ __forceinline__ void fine_tile_all(std::integer_sequence<int, Os...>,
 }
 
 // Shared epilogue of both apply kernels.
+// vo = cell*R*D*N + node; component (r, i) lives at vo + (r*D + i) * N.
 template <typename T, int D, int R, int MODE>
 __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, size_t vo, bool valid, T (&acc)[R][D],
                                                const T (&Di)[D][D]) {
+  const size_t NN = (size_t)a.N;
   constexpr int K = R;
   double dots[K];
 #pragma unroll
@@ -362,16 +364,16 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
 #pragma unroll
         for (int i = 0; i < D; ++i) {
           const T y = a.scale * acc[r][i];
-          a.out[vo + r * D + i] = y;
-          if (a.part) dots[r] += (double)y * (double)a.u[vo + r * D + i];
+          a.out[vo + (size_t)(r * D + i) * NN] = y;
+          if (a.part) dots[r] += (double)y * (double)a.u[vo + (size_t)(r * D + i) * NN];
         }
     } else if constexpr (MODE == M_RES) {
 #pragma unroll
       for (int r = 0; r < R; ++r)
 #pragma unroll
         for (int i = 0; i < D; ++i) {
-          const T y = a.f[vo + r * D + i] - a.scale * acc[r][i];
-          a.out[vo + r * D + i] = y;
+          const T y = a.f[vo + (size_t)(r * D + i) * NN] - a.scale * acc[r][i];
+          a.out[vo + (size_t)(r * D + i) * NN] = y;
           dots[r] += (double)y * (double)y;
         }
     } else if constexpr (MODE == M_CHEB || MODE == M_JAC0) {
@@ -383,9 +385,9 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
 #pragma unroll
         for (int i = 0; i < D; ++i) {
           if constexpr (MODE == M_JAC0)
-            res[i] = a.f[vo + r * D + i];
+            res[i] = a.f[vo + (size_t)(r * D + i) * NN];
           else
-            res[i] = a.f[vo + r * D + i] - a.scale * acc[r][i];
+            res[i] = a.f[vo + (size_t)(r * D + i) * NN] - a.scale * acc[r][i];
         }
 #pragma unroll
         for (int i = 0; i < D; ++i) {
@@ -393,11 +395,11 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
 #pragma unroll
           for (int j = 0; j < D; ++j) z += Di[i][j] * res[j];
           T d = T(be) * z;
-          if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + r * D + i];
-          a.dout[vo + r * D + i] = d;
-          const T un = (MODE == M_JAC0) ? d : a.u[vo + r * D + i] + d;
-          a.out[vo + r * D + i] = un;
-          if (a.dot_f_out) dots[r] += (double)a.f[vo + r * D + i] * (double)un;
+          if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + (size_t)(r * D + i) * NN];
+          a.dout[vo + (size_t)(r * D + i) * NN] = d;
+          const T un = (MODE == M_JAC0) ? d : a.u[vo + (size_t)(r * D + i) * NN] + d;
+          a.out[vo + (size_t)(r * D + i) * NN] = un;
+          if (a.dot_f_out) dots[r] += (double)a.f[vo + (size_t)(r * D + i) * NN] * (double)un;
         }
       }
     }
@@ -428,15 +430,17 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
   const int b = blockIdx.y;
   if (a.active && !a.active[b]) return;
   const int n = a.n;
+  const size_t NN = (size_t)a.N;
   const int ntz = ceil_div(n, TZ), nty = ceil_div(n, TY);
   const int tile = blockIdx.x;
   const int z0 = (tile % ntz) * TZ, y0 = ((tile / ntz) % nty) * TY, x0 = (tile / (ntz * nty)) * TX;
   const int tz = threadIdx.x % TZ, ty = (threadIdx.x / TZ) % TY, tx = threadIdx.x / (TZ * TY);
   const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
   const bool valid = x < n && y < n && z < n;
-  const size_t cell = (size_t)b * a.N;
+  const size_t cell = (size_t)b * NN;
   // ---- stage densities of the (TX+1)(TY+1)(TZ+1) elements touching the tile
-  //      and the halo'd node values, all as asynchronous copies in flight
+  //      and the halo'd node values (component-major in global memory,
+  //      node-major in shared memory), all as asynchronous copies in flight
   const int xm = x0 - 1, ym = y0 - 1, zm = z0 - 1;
   for (int w = threadIdx.x; w < G::RHO_WORDS; w += kThreads) {
     const int iz = w % (TZ + 1), iy = (w / (TZ + 1)) % (TY + 1), ix = w / ((TZ + 1) * (TY + 1));
@@ -447,20 +451,16 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
     cp_async<sizeof(T)>(srho + w, a.rho + cell + ((size_t)gx * n + gy) * n + gz);
   }
   if constexpr (MODE != M_JAC0) {
-    constexpr int VW = G::VW;
-    constexpr int CH_NODE = RD / VW;                  // vector chunks per node
-    constexpr int CH_ROW = (TZ + 2) * CH_NODE;        // chunks per (x,y) row
-    constexpr int CH_ALL = (TX + 2) * (TY + 2) * CH_ROW;
-    for (int w = threadIdx.x; w < CH_ALL; w += kThreads) {
-      const int row = w / CH_ROW, cr = w - row * CH_ROW;
-      const int iz = cr / CH_NODE, kc = cr - iz * CH_NODE;
-      const int iy = row % (TY + 2), ix = row / (TY + 2);
+    const T* __restrict__ ub = a.u + cell * RD;
+    for (int w = threadIdx.x; w < G::HALO_NODES * RD; w += kThreads) {
+      const int k = w / G::HALO_NODES, hn = w - k * G::HALO_NODES;
+      const int iz = hn % (TZ + 2), iy = (hn / (TZ + 2)) % (TY + 2), ix = hn / ((TZ + 2) * (TY + 2));
       int gx = xm + ix, gy = ym + iy, gz = zm + iz;
       gx += gx < 0 ? n : (gx >= n ? -n : 0);
       gy += gy < 0 ? n : (gy >= n ? -n : 0);
       gz += gz < 0 ? n : (gz >= n ? -n : 0);
-      cp_async<VW * sizeof(T)>(su + row * G::RW + iz * G::NS + kc * VW,
-                               a.u + (cell + ((size_t)gx * n + gy) * n + gz) * RD + kc * VW);
+      cp_async<sizeof(T)>(su + (ix * (TY + 2) + iy) * G::RW + iz * G::NS + k,
+                          ub + (size_t)k * NN + ((size_t)gx * n + gy) * n + gz);
     }
   }
   cp_async_wait_all();
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
     for (int j = 0; j < D; ++j) C0s[i][j] = a.scale * C0[i][j];
   block_inverse<T, D>(C0s, Di);
   const int id = valid ? (x * n + y) * n + z : 0;
-  const size_t vo = (cell + id) * RD;
+  const size_t vo = cell * RD + id;
   if constexpr (MODE == M_POWER) {
     double dots[2] = {0, 0};
     if (valid) {
@@ -500,9 +500,9 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
       for (int i = 0; i < D; ++i) {
         T w = 0;
         for (int j = 0; j < D; ++j) w += Di[i][j] * Au[j];
-        a.out[vo + i] = w;
-        dots[0] += (double)a.u[vo + i] * (double)Au[i];
-        for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i] * (double)C0s[i][j] * (double)a.u[vo + j];
+        a.out[vo + i * NN] = w;
+        dots[0] += (double)a.u[vo + i * NN] * (double)Au[i];
+        for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i * NN] * (double)C0s[i][j] * (double)a.u[vo + j * NN];
       }
     }
     block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
@@ -516,6 +516,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
   const int b = blockIdx.y;
   if (a.active && !a.active[b]) return;
   const int n = a.n, N = a.N;
+  const size_t NN = (size_t)N;
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   const bool valid = idx < N;
   const int id = valid ? idx : 0;
@@ -531,6 +532,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
     const int xs[3] = {wrapn(x - 1, n), x, wrapn(x + 1, n)};
     const int ys[3] = {wrapn(y - 1, n), y, wrapn(y + 1, n)};
     const int zs[3] = {wrapn(z - 1, n), z, wrapn(z + 1, n)};
+    const T* __restrict__ ub = a.u + cell * R * D;
 #pragma unroll 3
     for (int o = 0; o < 27; ++o) {
       const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
@@ -539,12 +541,12 @@ __global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
       for (int i = 0; i < D; ++i)
 #pragma unroll
         for (int j = 0; j < D; ++j) C[i][j] = __ldg(S + ((size_t)o * D * D + i * D + j) * N);
-      const T* __restrict__ un = a.u + (cell + ((size_t)xs[ox] * n + ys[oy]) * n + zs[oz]) * (R * D);
+      const T* __restrict__ un = ub + ((size_t)xs[ox] * n + ys[oy]) * n + zs[oz];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         T uv[D];
 #pragma unroll
-        for (int j = 0; j < D; ++j) uv[j] = __ldg(un + r * D + j);
+        for (int j = 0; j < D; ++j) uv[j] = __ldg(un + (size_t)(r * D + j) * NN);
 #pragma unroll
         for (int i = 0; i < D; ++i)
 #pragma unroll
@@ -558,7 +560,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
   for (int i = 0; i < D; ++i)
 #pragma unroll
     for (int j = 0; j < D; ++j) Di[i][j] = __ldg(Dp + (size_t)(i * D + j) * N);
-  const size_t vo = (cell + id) * (R * D);
+  const size_t vo = cell * R * D + id;
   if constexpr (MODE == M_POWER) {
     double dots[2] = {0, 0};
     if (valid) {
@@ -568,9 +570,9 @@ __global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
       for (int i = 0; i < D; ++i) {
         T w = 0;
         for (int j = 0; j < D; ++j) w += Di[i][j] * acc[0][j];
-        a.out[vo + i] = w;
-        dots[0] += (double)a.u[vo + i] * (double)acc[0][i];
-        for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i] * (double)C0[i][j] * (double)a.u[vo + j];
+        a.out[vo + i * NN] = w;
+        dots[0] += (double)a.u[vo + i * NN] * (double)acc[0][i];
+        for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i * NN] * (double)C0[i][j] * (double)a.u[vo + j * NN];
       }
     }
     block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
@@ -603,13 +605,13 @@ __global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ rc, int nc,
       for (int dz = -1; dz <= 1; ++dz) {
         const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
         const int fx = wrapn(2 * X + dx, nf), fy = wrapn(2 * Y + dy, nf), fz = wrapn(2 * Z + dz, nf);
-        const T* p = base + (((size_t)fx * nf + fy) * nf + fz) * K;
+        const T* p = base + ((size_t)fx * nf + fy) * nf + fz;
 #pragma unroll
-        for (int k = 0; k < K; ++k) acc[k] += w * __ldg(p + k);
+        for (int k = 0; k < K; ++k) acc[k] += w * __ldg(p + (size_t)k * Nf);
       }
-  T* o = rc + ((size_t)b * Nc + idx) * K;
+  T* o = rc + (size_t)b * Nc * K + idx;
 #pragma unroll
-  for (int k = 0; k < K; ++k) o[k] = acc[k];
+  for (int k = 0; k < K; ++k) o[(size_t)k * Nc] = acc[k];
 }
 
 // uf += P uc
@@ -632,13 +634,13 @@ __global__ void k_prolong_add(const T* __restrict__ uc, T* __restrict__ uf, int 
     if ((ox && !rx) || (oy && !ry) || (oz && !rz)) continue;
     const T w = T((rx ? 0.5 : 1.0) * (ry ? 0.5 : 1.0) * (rz ? 0.5 : 1.0));
     const int cx = bx + ox == nc ? 0 : bx + ox, cy = by + oy == nc ? 0 : by + oy, cz = bz + oz == nc ? 0 : bz + oz;
-    const T* p = base + (((size_t)cx * nc + cy) * nc + cz) * K;
+    const T* p = base + ((size_t)cx * nc + cy) * nc + cz;
 #pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] += w * __ldg(p + k);
+    for (int k = 0; k < K; ++k) acc[k] += w * __ldg(p + (size_t)k * Nc);
   }
-  T* o = uf + ((size_t)b * Nf + idx) * K;
+  T* o = uf + (size_t)b * Nf * K + idx;
 #pragma unroll
-  for (int k = 0; k < K; ++k) o[k] += acc[k];
+  for (int k = 0; k < K; ++k) o[(size_t)k * Nf] += acc[k];
 }
 
 // coarsest level: u = Ainv f with the FP64 (regularised) inverse, per cell
@@ -650,7 +652,8 @@ __global__ void k_coarse_solve(const double* __restrict__ Ainv, const T* __restr
   const int row = blockIdx.x * kThreads + threadIdx.x;
   if (row >= ndof) return;
   const double* Acol = Ainv + (size_t)b * ndof * ndof + row;
-  const T* fb = f + (size_t)b * ndof * R;  // [node][R][D] with ndof = nodes*D
+  const int Nc = ndof / D;
+  const T* fb = f + (size_t)b * ndof * R;  // [rhs][comp][node]; dof = node*D + comp
   double acc[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) acc[r] = 0;
@@ -658,12 +661,12 @@ __global__ void k_coarse_solve(const double* __restrict__ Ainv, const T* __restr
     const int node = col / D, c = col - node * D;
     const double a = Acol[(size_t)col * ndof];  // symmetric: read column-wise (coalesced)
 #pragma unroll
-    for (int r = 0; r < R; ++r) acc[r] += a * (double)fb[(node * R + r) * D + c];
+    for (int r = 0; r < R; ++r) acc[r] += a * (double)fb[(size_t)(r * D + c) * Nc + node];
   }
   const int node = row / D, c = row - node * D;
   T* ub = u + (size_t)b * ndof * R;
 #pragma unroll
-  for (int r = 0; r < R; ++r) ub[(node * R + r) * D + c] = (T)acc[r];
+  for (int r = 0; r < R; ++r) ub[(size_t)(r * D + c) * Nc + node] = (T)acc[r];
 }
 
 // ----------------------------------------------------------------------------
@@ -882,11 +885,11 @@ __global__ void k_assemble_F(const double* __restrict__ rho, double* __restrict_
 #pragma unroll
       for (int i = 0; i < D; ++i) acc[r][i] += rq[q] * fe<D>(D * aa + i, r);
   }
-  double* o = F + ((size_t)b * N + idx) * R * D;
+  double* o = F + (size_t)b * N * R * D + idx;
 #pragma unroll
   for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int i = 0; i < D; ++i) o[r * D + i] = scale * acc[r][i];
+    for (int i = 0; i < D; ++i) o[(size_t)(r * D + i) * N] = scale * acc[r][i];
 }
 
 // rho = rho_min + (1-rho_min) clamp(x,xmin,1)^p, FP64 and FP32 copies
@@ -918,11 +921,14 @@ __global__ void k_dot(const T* __restrict__ x, const T* __restrict__ y, double* 
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   double v[R] = {};
   if (idx < N) {
-    const size_t o = ((size_t)b * N + idx) * R * D;
+    const size_t o = (size_t)b * N * R * D + idx;
 #pragma unroll
     for (int r = 0; r < R; ++r)
 #pragma unroll
-      for (int i = 0; i < D; ++i) v[r] += (double)x[o + r * D + i] * (double)y[o + r * D + i];
+      for (int i = 0; i < D; ++i) {
+        const size_t j = o + (size_t)(r * D + i) * N;
+        v[r] += (double)x[j] * (double)y[j];
+      }
   }
   block_sum_store<R>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * R);
 }
@@ -936,15 +942,16 @@ __global__ void k_pcg_update(T* __restrict__ x, T* __restrict__ r, const T* __re
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   double v[R] = {};
   if (idx < N) {
-    const size_t o = ((size_t)b * N + idx) * R * D;
+    const size_t o = (size_t)b * N * R * D + idx;
 #pragma unroll
     for (int c = 0; c < R; ++c) {
       const T a = (T)alpha[b * R + c];
 #pragma unroll
       for (int i = 0; i < D; ++i) {
-        x[o + c * D + i] += a * p[o + c * D + i];
-        const T rn = r[o + c * D + i] - a * q[o + c * D + i];
-        r[o + c * D + i] = rn;
+        const size_t j = o + (size_t)(c * D + i) * N;
+        x[j] += a * p[j];
+        const T rn = r[j] - a * q[j];
+        r[j] = rn;
         v[c] += (double)rn * (double)rn;
       }
     }
@@ -960,12 +967,15 @@ __global__ void k_pcg_direction(T* __restrict__ p, const T* __restrict__ z, cons
   if (active && !active[b]) return;
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= N) return;
-  const size_t o = ((size_t)b * N + idx) * R * D;
+  const size_t o = (size_t)b * N * R * D + idx;
 #pragma unroll
   for (int c = 0; c < R; ++c) {
     const T be = (T)beta[b * R + c];
 #pragma unroll
-    for (int i = 0; i < D; ++i) p[o + c * D + i] = z[o + c * D + i] + be * p[o + c * D + i];
+    for (int i = 0; i < D; ++i) {
+      const size_t j = o + (size_t)(c * D + i) * N;
+      p[j] = z[j] + be * p[j];
+    }
   }
 }
 
@@ -1033,12 +1043,15 @@ __global__ void k_to_f32_scaled(const double* __restrict__ src, float* __restric
   if (active && !active[b]) return;
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= N) return;
-  const size_t o = ((size_t)b * N + idx) * R * D;
+  const size_t o = (size_t)b * N * R * D + idx;
 #pragma unroll
   for (int c = 0; c < R; ++c) {
     const double s = inv_scale[b * R + c];
 #pragma unroll
-    for (int i = 0; i < D; ++i) dst[o + c * D + i] = (float)(src[o + c * D + i] * s);
+    for (int i = 0; i < D; ++i) {
+      const size_t j = o + (size_t)(c * D + i) * N;
+      dst[j] = (float)(src[j] * s);
+    }
   }
 }
 
@@ -1049,12 +1062,15 @@ __global__ void k_add_f32_scaled(double* __restrict__ dst, const float* __restri
   if (active && !active[b]) return;
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   if (idx >= N) return;
-  const size_t o = ((size_t)b * N + idx) * R * D;
+  const size_t o = (size_t)b * N * R * D + idx;
 #pragma unroll
   for (int c = 0; c < R; ++c) {
     const double s = scale[b * R + c];
 #pragma unroll
-    for (int i = 0; i < D; ++i) dst[o + c * D + i] += s * (double)src[o + c * D + i];
+    for (int i = 0; i < D; ++i) {
+      const size_t j = o + (size_t)(c * D + i) * N;
+      dst[j] += s * (double)src[j];
+    }
   }
 }
 
@@ -1078,16 +1094,17 @@ __global__ void k_precond_back(const float* __restrict__ z32, const double* __re
   const int idx = blockIdx.x * kThreads + threadIdx.x;
   double v[2 * R] = {};
   if (idx < N) {
-    const size_t o = ((size_t)b * N + idx) * R * D;
+    const size_t o = (size_t)b * N * R * D + idx;
 #pragma unroll
     for (int c = 0; c < R; ++c) {
       const double s = inv[b * R + c];
 #pragma unroll
       for (int i = 0; i < D; ++i) {
-        const double zv = s * (double)z32[o + c * D + i];
-        z[o + c * D + i] = zv;
-        v[c] += r[o + c * D + i] * zv;
-        if (q) v[R + c] += q[o + c * D + i] * zv;
+        const size_t j = o + (size_t)(c * D + i) * N;
+        const double zv = s * (double)z32[j];
+        z[j] = zv;
+        v[c] += r[j] * zv;
+        if (q) v[R + c] += q[j] * zv;
       }
     }
   }
@@ -1152,7 +1169,7 @@ __global__ void __launch_bounds__(kThreads) k_homogenize(const double* __restric
     nodes[a] = (wrapn(x + corner_x(a), n) * n + wrapn(y + corner_y(a), n)) * n + wrapn(z + corner_z(a), n);
   const double* __restrict__ ub = u + (size_t)b * N * R * D;
   const double re = valid ? rho[(size_t)b * N + ee] : 0.0;
-  double* eo = energy + ((size_t)b * N + ee) * R * R;
+  double* eo = energy + (size_t)b * R * R * N + ee;  // [cell][r][s][elem]
   double v[K];
 #pragma unroll
   for (int s = 0; s < R; ++s) {
@@ -1162,7 +1179,8 @@ __global__ void __launch_bounds__(kThreads) k_homogenize(const double* __restric
 #pragma unroll
       for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int i = 0; i < D; ++i) L[D * a + i] = xscale * x0<D>(D * a + i, s) - __ldg(ub + ((size_t)nodes[a] * R + s) * D + i);
+        for (int i = 0; i < D; ++i)
+          L[D * a + i] = xscale * x0<D>(D * a + i, s) - __ldg(ub + (size_t)(s * D + i) * N + nodes[a]);
 #pragma unroll
       for (int p = 0; p < k; ++p) {
         double acc = 0;
@@ -1178,12 +1196,12 @@ __global__ void __launch_bounds__(kThreads) k_homogenize(const double* __restric
       for (int a = 0; a < 8; ++a)
 #pragma unroll
         for (int i = 0; i < D; ++i)
-          acc += (xscale * x0<D>(D * a + i, r) - __ldg(ub + ((size_t)nodes[a] * R + r) * D + i)) * KL[D * a + i];
+          acc += (xscale * x0<D>(D * a + i, r) - __ldg(ub + (size_t)(r * D + i) * N + nodes[a])) * KL[D * a + i];
       // index of (r,s), r <= s, in the packed upper triangle
       v[r * R - r * (r - 1) / 2 + (s - r)] = re * acc;
       if (valid) {
-        eo[r * R + s] = acc;
-        eo[s * R + r] = acc;
+        eo[(size_t)(r * R + s) * N] = acc;
+        eo[(size_t)(s * R + r) * N] = acc;
       }
     }
   }
@@ -1292,16 +1310,16 @@ __global__ void k_sensitivity(const double* __restrict__ x, const double* __rest
   const size_t i = (size_t)b * N + e;
   double s = 0;
   if (E3) {
-    const double* Ee = E3 + i * 36;
+    const double* Ee = E3 + (size_t)b * 36 * N + e;
     const double* G = G3 + (size_t)b * 36;
 #pragma unroll
-    for (int k = 0; k < 36; ++k) s += G[k] * Ee[k];
+    for (int k = 0; k < 36; ++k) s += G[k] * Ee[(size_t)k * N];
   }
   if (E1) {
-    const double* Ee = E1 + i * 9;
+    const double* Ee = E1 + (size_t)b * 9 * N + e;
     const double* G = G1 + (size_t)b * 9;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) s += G[k] * Ee[k];
+    for (int k = 0; k < 9; ++k) s += G[k] * Ee[(size_t)k * N];
   }
   if (dJdrho) dJdrho[i] = s;
   if (dJdx) {
@@ -1319,10 +1337,10 @@ __global__ void k_energy_contract(const double* __restrict__ energy, const doubl
   const int e = blockIdx.x * kThreads + threadIdx.x;
   if (e >= N) return;
   const size_t i = (size_t)b * N + e;
-  const double* Ee = energy + i * RR;
+  const double* Ee = energy + (size_t)b * RR * N + e;
   const double* gb = g + (size_t)b * RR;
   double s = 0;
-  for (int k = 0; k < RR; ++k) s += gb[k] * Ee[k];
+  for (int k = 0; k < RR; ++k) s += gb[k] * Ee[(size_t)k * N];
   out[i] = accumulate ? out[i] + s : s;
 }
 

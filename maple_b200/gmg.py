@@ -56,18 +56,18 @@ class GMGSolver(nn.Module):
                              "voxel element matrix are supported")
         ctx = cached_context(r, dev)
         ctx.set_density(self.PHYSICS, rho.reshape(1, n).contiguous(), precision)
-        F = torch.zeros((1, n, self.R, D), dtype=torch.float64, device=ctx.device)
-        F[0, :, 0, :] = f.to(device=ctx.device, dtype=torch.float64)
+        F = torch.zeros((1, self.R, D, n), dtype=torch.float64, device=ctx.device)
+        F[0, 0] = f.to(device=ctx.device, dtype=torch.float64).T
         x0 = None
         if init_list is not None:
             if isinstance(init_list, torch.Tensor) and init_list.numel() == n * D:
                 x0 = torch.zeros_like(F)
-                x0[0, :, 0, :] = init_list.reshape(n, D).to(device=ctx.device, dtype=torch.float64)
+                x0[0, 0] = init_list.reshape(n, D).to(device=ctx.device, dtype=torch.float64).T
             else:
                 raise NotImplementedError("init_list: only a dense level-0 tensor shaped like global_f is supported")
         u, res, _ = ctx.solve_rhs(self.PHYSICS, F, x0, precision=precision, rtol=rtol, maxit=max(int(max_iter), 500))
-        out_u = u[0, :, 0, :].to(device=dev, dtype=dtype)
-        out_r = res[0, :, 0, :].to(device=dev, dtype=dtype)
+        out_u = u[0, 0].T.contiguous().to(device=dev, dtype=dtype)
+        out_r = res[0, 0].T.contiguous().to(device=dev, dtype=dtype)
         if D == 1:
             return out_u.reshape(n, 1), out_r.reshape(n, 1)
         return out_u, out_r

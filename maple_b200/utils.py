@@ -94,8 +94,8 @@ def assemble_F_fast(node_index: torch.Tensor, Fe: torch.Tensor, n_nodes: int, rh
     if Fe.shape != (24, 6):
         raise ValueError(f"Expected Fe shape (24,6), got {tuple(Fe.shape)}")
     ctx = cached_context(r, node_index.device)
-    F = ctx.assemble_rhs("elastic", _rho_vector(rho, n_nodes, ctx.device))  # (1,N,6,3)
-    return F[0].transpose(1, 2).contiguous().to(Fe.dtype)
+    F = ctx.assemble_rhs("elastic", _rho_vector(rho, n_nodes, ctx.device))  # (1,6,3,N)
+    return F[0].permute(2, 1, 0).contiguous().to(Fe.dtype)
 
 
 def assemble_F_fast_scalar(node_index: torch.Tensor, Fe: torch.Tensor, n_nodes: int, rho) -> torch.Tensor:
@@ -107,8 +107,8 @@ def assemble_F_fast_scalar(node_index: torch.Tensor, Fe: torch.Tensor, n_nodes: 
         raise ValueError(f"Expected node_index shape (E,8), got {tuple(node_index.shape)}")
     _check_topology(node_index, r)
     ctx = cached_context(r, node_index.device)
-    F = ctx.assemble_rhs("thermal", _rho_vector(rho, n_nodes, ctx.device))  # (1,N,3,1)
-    return F[0, :, :, 0].contiguous().to(Fe.dtype)
+    F = ctx.assemble_rhs("thermal", _rho_vector(rho, n_nodes, ctx.device))  # (1,3,1,N)
+    return F[0, :, 0, :].T.contiguous().to(Fe.dtype)
 
 
 def cube_root(n: int) -> int:

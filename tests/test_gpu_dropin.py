@@ -1,0 +1,167 @@
+"""The reference-facing surface (IHD, GMGSolver, _utils, main_IHD_v3 functions,
+objectives) run on the GPU and checked against the reference's golden vectors."""
+import csv
+import json
+import os
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ihd_oracle as O
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def cfg(r):
+    return SimpleNamespace(resolution=r, GMG=SimpleNamespace(smooth_iter=[2, 2, 3, 4, 5], max_cycle=1))
+
+
+@pytest.fixture(scope="module")
+def ihd8(lib):
+    from maple_b200.model import IHD
+    return IHD(cfg(8), DEV, rtol=1e-12)
+
+
+def test_ihd_forward_matches_reference(ihd8, golden):
+    from maple_b200.optimize import build_unitcell_batch
+    from maple_b200.utils import assemble_F_fast, assemble_F_fast_scalar
+    g = golden("homog_r8_s0.npz")
+    rho = torch.tensor(1e-9 + (1 - 1e-9) * g["x"] ** 3, dtype=torch.float64, device=DEV).reshape(-1, 1)
+    batch = build_unitcell_batch(DEV, 8, rho.reshape(8, 8, 8))
+    batch["rho"] = rho
+    Fm = assemble_F_fast(batch["node_index"], ihd8.Fe_3d, 512, rho)
+    Ft = assemble_F_fast_scalar(batch["node_index"], ihd8.Fe_1d, 512, rho)
+    assert rel(Fm.cpu().numpy(), g["F_elastic"]) < 1e-13
+    assert rel(Ft.cpu().numpy(), g["F_thermal"]) < 1e-13
+    CH = ihd8.TO_homo_3d(batch, ihd8.Ke_3d, Fm, ihd8.X0_3d, batch_size=1)
+    kap = ihd8.TO_homo_1d(batch, ihd8.Ke_1d, Ft, ihd8.X0_1d, batch_size=1)
+    assert CH.shape == (6, 6) and kap.shape == (3, 3)
+    assert rel(CH.cpu().numpy(), g["CH"]) < 1e-10
+    assert rel(kap.cpu().numpy(), g["kappa"]) < 1e-10
+
+
+@pytest.mark.parametrize("tag,spec", [("bi", "stiffness:0.5,thermal:0.5"),
+                                      ("tri", "stiffness:0.3333333333333333,shear:0.3333333333333333,"
+                                              "thermal:0.3333333333333333")])
+def test_ihd_autograd_matches_reference(ihd8, golden, tag, spec):
+    """dJ/dx through IHD.TO_homo_* (analytic adjoint in backward) equals the
+    reference's autograd through converged solves (main_IHD_v3.py:622-688)."""
+    from maple_b200.objective import objective_from_spec
+    from maple_b200.optimize import build_unitcell_batch
+    g = golden("homog_r8_s0.npz")
+    x = torch.tensor(g["x"], dtype=torch.float64, device=DEV).reshape(-1, 1).requires_grad_(True)
+    rho = 1e-9 + (1 - 1e-9) * x.clamp(1e-3, 1.0) ** 3
+    batch = build_unitcell_batch(DEV, 8, torch.zeros(8, 8, 8, device=DEV))
+    batch["rho"] = rho
+    kap = ihd8.TO_homo_1d(batch, ihd8.Ke_1d, None, ihd8.X0_1d, batch_size=1)
+    CH = ihd8.TO_homo_3d(batch, ihd8.Ke_3d, None, ihd8.X0_3d, batch_size=1)
+    J = objective_from_spec(obj=spec, CH=CH, kappa=kap)
+    (dJdx,) = torch.autograd.grad(J, x)
+    assert abs(J.item() - float(g[f"J_{tag}"])) / abs(J.item()) < 1e-10
+    assert rel(dJdx.cpu().numpy().reshape(-1), g[f"dJdx_{tag}"]) < 1e-8
+
+
+def test_evaluate_terms_and_J(ihd8, golden):
+    from maple_b200.optimize import build_unitcell_batch, evaluate_homogenized_terms, evaluate_J
+    g = golden("homog_r8_s1.npz")
+    rho = torch.tensor(1e-9 + (1 - 1e-9) * g["x"] ** 3, dtype=torch.float64, device=DEV).reshape(-1, 1)
+    batch = build_unitcell_batch(DEV, 8, rho.reshape(8, 8, 8))
+    terms = evaluate_homogenized_terms(ihd8, batch, rho)
+    assert abs(terms["stiffness"] - O.stiffness_objective(g["CH"])) < 1e-10 * abs(terms["stiffness"])
+    assert abs(terms["shear"] - O.shear_objective(g["CH"])) < 1e-10 * abs(terms["shear"])
+    assert abs(terms["thermal"] - O.thermal_objective(g["kappa"])) < 1e-10 * abs(terms["thermal"])
+    J = evaluate_J(ihd8, batch, rho, "0.4*stiffness+0.6*thermal")
+    ref = 0.4 * O.stiffness_objective(g["CH"]) + 0.6 * O.thermal_objective(g["kappa"])
+    assert abs(J - ref) < 1e-10 * abs(ref)
+
+
+@pytest.mark.parametrize("solver,d", [("GMGSolver", 3), ("GMGSolverScalar", 1)])
+def test_gmg_solver_dropin(lib, golden, solver, d):
+    """GMGSolver.solve with the reference's arguments (fine_ke = rho_e Ke0)."""
+    from maple_b200 import gmg
+    from maple_b200.optimize import build_unitcell_batch
+    from maple_b200.utils import hexahedron, hexahedron_scalar, isotropic_elastic_tensor
+    g = golden("homog_r8_s0.npz")
+    rho = torch.tensor(1e-9 + (1 - 1e-9) * g["x"] ** 3, dtype=torch.float64, device=DEV)
+    batch = build_unitcell_batch(DEV, 8, rho.reshape(8, 8, 8))
+    if d == 3:
+        Ke, Fe, _ = hexahedron(8, isotropic_elastic_tensor(1.0, 0.3).double().to(DEV))
+        f = torch.tensor(g["F_elastic"][:, :, 2], device=DEV)          # load case 2, (N,3)
+    else:
+        Ke, Fe, _ = hexahedron_scalar(8, torch.tensor(1.0, dtype=torch.float64, device=DEV))
+        f = torch.tensor(g["F_thermal"][:, 1], device=DEV)             # load case 1, (N,)
+    fine_ke = Ke.unsqueeze(0).expand(512, -1, -1) * rho.reshape(-1, 1, 1)
+    u, r = getattr(gmg, solver)().solve(fine_ke, f, batch["coord"].int(), batch["elem_coords"], batch["node_index"],
+                                        max_iter=1, smooth_iter=[2, 2, 3, 4, 5], max_levels=5, dtype=torch.float64)
+    assert u.shape == (512, d) and r.shape == (512, d)
+    assert float(r.norm() / f.norm()) < 1e-9
+    if d == 3:
+        ug = g["u_elastic"][:, :, 2]
+    else:
+        ug = g["u_thermal"][:, 1:2]
+    un = u.cpu().numpy()
+    du = (un - un.mean(0)) - (ug - ug.mean(0))
+    assert np.abs(du).max() / np.abs(ug).max() < 1e-8
+    with pytest.raises(ValueError):
+        bad = fine_ke.clone()
+        bad[0, 0, 1] += 1.0
+        getattr(gmg, solver)().solve(bad, f, batch["coord"].int(), batch["elem_coords"], batch["node_index"])
+
+
+def test_filter_and_oc_dropins(lib, golden):
+    from maple_b200.optimize import avg_filter3d_x_periodic, build_unitcell_batch, oc_update
+    g = golden("ops.npz")
+    batch = build_unitcell_batch(DEV, 8, torch.zeros(8, 8, 8, device=DEV))
+    v = torch.tensor(g["filter_r8_k3_in"], device=DEV).reshape(-1, 1)
+    out = avg_filter3d_x_periodic(v, batch["elem_coords"], 8, 3)
+    assert out.shape == (512, 1)
+    assert rel(out.cpu().numpy().reshape(-1), g["filter_r8_k3_out"]) < 1e-14
+    with pytest.raises(ValueError):
+        avg_filter3d_x_periodic(v, batch["elem_coords"], 8, 2)
+    for i in range(3):
+        vf, move, xmin = g[f"oc{i}_params"]
+        xn = oc_update(torch.tensor(g[f"oc{i}_x"], device=DEV).reshape(-1, 1),
+                       torch.tensor(g[f"oc{i}_dJ"], device=DEV).reshape(-1, 1), volfrac=vf, move=move, xmin=xmin)
+        assert np.abs(xn.cpu().numpy().reshape(-1) - g[f"oc{i}_xnew"]).max() < 1e-10
+
+
+def test_optimize_inverse_homogenization(ihd8, golden, tmp_path):
+    """Three OC iterations through the reference's optimizer signature follow
+    the reference trajectory, with the reference's output files."""
+    from maple_b200.optimize import build_unitcell_batch, optimize_inverse_homogenization
+    g = golden("traj_r8.npz")
+    batch = build_unitcell_batch(DEV, 8, torch.zeros(8, 8, 8, device=DEV))
+    res = optimize_inverse_homogenization(
+        ihd8, batch, res=8, objective="stiffness:0.5,thermal:0.5", init_mode="noise", volfrac=0.25, penal=3.0,
+        rho_min=1e-9, move=0.2, xmin=1e-3, iters=3, seed=0, symmetry="none", lambda_print=0.0, overhang_deg=45.0,
+        lambda_cavity=0.0, cavity_thresh=0.5, cavity_beta=20.0, min_channel_rad=0, cavity_rad=1,
+        cavity_seed_faces="all", cavity_iters=128, cavity_tiles=1, cavity_tiles_xyz=None, cavity_focus_center=True,
+        filter_k=3, output_dir=str(tmp_path), mesh_every=0, mesh_res=32, mesh_iso=0.3, mesh_pad=2,
+        save_initial_mesh=False, verbose=False, x_init=torch.tensor(g["x0"]), rtol=1e-12)
+    assert res.iters_run == 3
+    rows = list(csv.reader(open(os.path.join(tmp_path, "iter_log.csv"))))
+    assert rows[0] == ["iter", "J_total", "J_raw", "P_print", "P_cavity", "mean_x", "mean_rho", "dx_max", "dx_mean",
+                       "time_sec"]
+    for it in range(3):
+        assert abs(float(rows[1 + it][2]) - float(g[f"J{it}"])) / float(g[f"J{it}"]) < 1e-9
+    summary = json.load(open(os.path.join(tmp_path, "summary.json")))
+    assert summary["iters_run"] == 3 and summary["resolution"] == 8
+    rho_final = np.load(os.path.join(tmp_path, "rho_final.npy"))
+    ref = (1e-9 + (1 - 1e-9) * g["x3"] ** 3).reshape(8, 8, 8).astype(np.float32)
+    assert rho_final.shape == (8, 8, 8) and np.abs(rho_final - ref).max() < 1e-6
+    with pytest.raises(NotImplementedError):
+        optimize_inverse_homogenization(
+            ihd8, batch, res=8, objective="shear", init_mode="noise", volfrac=0.25, penal=3.0, rho_min=1e-9,
+            move=0.2, xmin=1e-3, iters=1, seed=0, symmetry="cubic", lambda_print=0.0, overhang_deg=45.0,
+            lambda_cavity=0.0, cavity_thresh=0.5, cavity_beta=20.0, min_channel_rad=0, cavity_rad=1,
+            cavity_seed_faces="all", cavity_iters=128, cavity_tiles=1, cavity_tiles_xyz=None,
+            cavity_focus_center=True, filter_k=3, output_dir=str(tmp_path), mesh_every=0, mesh_res=32, mesh_iso=0.3,
+            mesh_pad=2, verbose=False)

@@ -44,12 +44,12 @@ def test_matvec_elastic_and_thermal(ctx8, dens8):
     rng = np.random.default_rng(0)
     e = O.Elements(r)
     for phys, d, R, Ke0 in (("elastic", 3, 6, e.Ke3), ("thermal", 1, 3, e.Ke1)):
-        u = rng.standard_normal((2, N, R, d))
+        u = rng.standard_normal((2, R, d, N))
         y = ctx8.matvec(phys, T(rho), T(u)).cpu().numpy()
         for b in range(2):
             K = O.assemble_K(rho[b].reshape(-1, 1, 1) * Ke0[None], r, d)
-            umat = u[b].transpose(0, 2, 1).reshape(N * d, R)
-            ref = (K @ umat).reshape(N, d, R).transpose(0, 2, 1)
+            umat = u[b].transpose(2, 1, 0).reshape(N * d, R)
+            ref = (K @ umat).reshape(N, d, R).transpose(2, 1, 0)
             assert rel(y[b], ref) < 1e-13, (phys, b)
 
 
@@ -59,7 +59,7 @@ def test_assemble_rhs(ctx8, dens8):
     for phys, d, R, Fe in (("elastic", 3, 6, e.Fe3), ("thermal", 1, 3, e.Fe1)):
         F = ctx8.assemble_rhs(phys, T(rho)).cpu().numpy()
         for b in range(2):
-            ref = O.assemble_F(rho[b], Fe, 8, d).reshape(512, d, R).transpose(0, 2, 1)
+            ref = O.assemble_F(rho[b], Fe, 8, d).reshape(512, d, R).transpose(2, 1, 0)
             assert rel(F[b], ref) < 1e-13
 
 
@@ -79,9 +79,9 @@ def test_solution_field_matches_reference(ctx8, dens8):
     (g0, _), rho = dens8
     ctx8.set_density("elastic", T(rho), "fp64")
     ctx8.solve("elastic", "fp64", rtol=1e-13, maxit=300)
-    u = ctx8.solution("elastic").cpu().numpy()[0]          # (N, 6, 3)
-    ug = g0["u_elastic"].transpose(0, 2, 1)                 # (N, 6, 3)
-    du = (u - u.mean(0)) - (ug - ug.mean(0))
+    u = ctx8.solution("elastic").cpu().numpy()[0]          # (6, 3, N)
+    ug = g0["u_elastic"].transpose(2, 1, 0)                 # (6, 3, N)
+    du = (u - u.mean(-1, keepdims=True)) - (ug - ug.mean(-1, keepdims=True))
     assert np.abs(du).max() / np.abs(ug).max() < 1e-9
 
 
