@@ -860,6 +860,75 @@ __global__ void k_chol_inverse(double* __restrict__ A, double* __restrict__ work
   }
 }
 
+// Same result for ndof <= kCholSmemMax, with the packed lower triangle of the
+// regularised matrix held in shared memory (one block of 1024 threads per
+// cell).  L^-1 goes through `work` in global memory (each thread owns columns).
+constexpr int kCholSmemMax = 192;
+__host__ __device__ constexpr size_t chol_smem_bytes(int ndof) { return (size_t)ndof * (ndof + 1) / 2 * sizeof(double); }
+
+__global__ void __launch_bounds__(1024) k_chol_inverse_smem(double* __restrict__ A, double* __restrict__ work,
+                                                            int ndof, int D, const int* active, int* status) {
+  const int b = blockIdx.x;
+  if (active && !active[b]) return;
+  extern __shared__ double Lp[];  // packed lower triangle, row i starts at i(i+1)/2
+  double* M = A + (size_t)b * ndof * ndof;
+  double* Li = work + (size_t)b * ndof * ndof;
+  const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+  __shared__ double s_alpha;
+  if (warp == 0) {
+    double t = 0;
+    for (int i = lane; i < ndof; i += 32) t += M[(size_t)i * ndof + i];
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    if (lane == 0) s_alpha = t / ndof;
+  }
+  __syncthreads();
+  const double reg = s_alpha / (ndof / D);
+  for (int i = warp; i < ndof; i += nw)
+    for (int j = lane; j <= i; j += 32)
+      Lp[(size_t)i * (i + 1) / 2 + j] = M[(size_t)i * ndof + j] + (((i - j) % D) == 0 ? reg : 0.0);
+  __syncthreads();
+  for (int k = 0; k < ndof; ++k) {
+    const size_t kk = (size_t)k * (k + 1) / 2 + k;
+    if (tid == 0) {
+      double d = Lp[kk];
+      if (!(d > 0)) {
+        if (status) status[b] = 1;
+        d = 1e-300;
+      }
+      Lp[kk] = sqrt(d);
+    }
+    __syncthreads();
+    const double piv = Lp[kk];
+    for (int i = k + 1 + tid; i < ndof; i += nth) Lp[(size_t)i * (i + 1) / 2 + k] /= piv;
+    __syncthreads();
+    for (int i = k + 1 + warp; i < ndof; i += nw) {
+      const size_t ri = (size_t)i * (i + 1) / 2;
+      const double lik = Lp[ri + k];
+      for (int j = k + 1 + lane; j <= i; j += 32) Lp[ri + j] -= lik * Lp[(size_t)j * (j + 1) / 2 + k];
+    }
+    __syncthreads();
+  }
+  // Li = L^-1 column by column (thread j owns column j)
+  for (int j = tid; j < ndof; j += nth) {
+    for (int i = 0; i < j; ++i) Li[(size_t)i * ndof + j] = 0.0;
+    for (int i = j; i < ndof; ++i) {
+      const size_t ri = (size_t)i * (i + 1) / 2;
+      double sacc = (i == j) ? 1.0 : 0.0;
+      for (int p = j; p < i; ++p) sacc -= Lp[ri + p] * Li[(size_t)p * ndof + j];
+      Li[(size_t)i * ndof + j] = sacc / Lp[ri + i];
+    }
+  }
+  __syncthreads();
+  // A^-1 = Li^T Li
+  for (int t = tid; t < ndof * ndof; t += nth) {
+    const int i = t / ndof, j = t % ndof;
+    const int p0 = i > j ? i : j;
+    double sacc = 0;
+    for (int p = p0; p < ndof; ++p) sacc += Li[(size_t)p * ndof + i] * Li[(size_t)p * ndof + j];
+    M[t] = sacc;
+  }
+}
+
 // ----------------------------------------------------------------------------
 // right-hand sides, vectors, PCG scalars
 // ----------------------------------------------------------------------------
@@ -1384,11 +1453,11 @@ __device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, uns
     } else {
       long polls = 0;
       while (*vgen == g) {
-        if (++polls > (1L << 24)) {
+        if (++polls > (1L << 26)) {  // a few seconds at most, then report
           atomicExch(err, 1);
           break;
         }
-        __nanosleep(100);
+        if (polls > 4096) __nanosleep(32);
       }
     }
     __threadfence();

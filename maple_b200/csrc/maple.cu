@@ -169,6 +169,29 @@ struct maple_ctx {
 
 namespace maple {
 
+// Optional event bracketing of every launch (bench instrumentation).
+static bool prof_on(maple_ctx* c) { return c->profiling && c->ev_used + 2 <= c->ev_pool.size(); }
+static void prof_begin(maple_ctx* c, cudaStream_t s) {
+  if (prof_on(c)) CK(cudaEventRecord(c->ev_pool[c->ev_used], s));
+}
+static void prof_end(maple_ctx* c, cudaStream_t s, const char* text, double bytes) {
+  if (!prof_on(c)) return;
+  CK(cudaEventRecord(c->ev_pool[c->ev_used + 1], s));
+  std::string name(text);
+  const size_t cut = name.find("<<<");
+  if (cut != std::string::npos) name = name.substr(0, cut);
+  name.erase(std::remove(name.begin(), name.end(), ' '), name.end());
+  c->recs.push_back({name, bytes, c->ev_used});
+  c->ev_used += 2;
+}
+#define KL(ctx, stream, ...)                \
+  do {                                      \
+    prof_begin(ctx, stream);                \
+    __VA_ARGS__;                            \
+    CKL();                                  \
+    prof_end(ctx, stream, #__VA_ARGS__, 0); \
+  } while (0)
+
 static void* dalloc(maple_ctx* c, size_t bytes) {
   void* p = nullptr;
   if (bytes == 0) bytes = 16;
@@ -257,7 +280,6 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
   const dim3 g = g2(a.N, c->B);
   if (l == 0) {
     a.rho = o.rho;
-    const bool rec = c->profiling && c->ev_used + 2 <= c->ev_pool.size();
     using G = FineTile<T, R * D>;
     static bool attr_set = false;  // one per template instantiation
     if (!attr_set) {
@@ -265,31 +287,37 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
                               (int)G::BYTES));
       attr_set = true;
     }
-    if (rec) CK(cudaEventRecord(c->ev_pool[c->ev_used], s));
+    prof_begin(c, s);
     k_apply_fine<T, D, R, MODE><<<dim3(fine_tiles(a.n), c->B), kThreads, G::BYTES, s>>>(a);
-    if (rec) {
-      CK(cudaEventRecord(c->ev_pool[c->ev_used + 1], s));
+    CKL();
+    if (prof_on(c)) {
       static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
       // algorithmic bytes: rho once, each vector read or written once
       const int nvec = MODE == M_MV ? 2 : MODE == M_RES ? 3 : MODE == M_CHEB ? 5 : MODE == M_JAC0 ? 3 : 2;
       const double bytes = (double)c->B * a.N * ((double)sizeof(T) + (double)nvec * R * D * sizeof(T));
-      c->recs.push_back({std::string("k_apply_fine<") + (sizeof(T) == 8 ? "f64," : "f32,") + std::to_string(D) +
-                             "," + std::to_string(R) + "," + mname[MODE] + ">",
-                         bytes, c->ev_used});
-      c->ev_used += 2;
+      const std::string nm = std::string("k_apply_fine<") + (sizeof(T) == 8 ? "f64," : "f32,") + std::to_string(D) +
+                             "," + std::to_string(R) + "," + mname[MODE] + ">";
+      prof_end(c, s, nm.c_str(), bytes);
     }
+    return;
   } else {
     a.S = o.S[l];
     a.Dinv = o.Dinv[l];
+    prof_begin(c, s);
     k_apply_stencil<T, D, R, MODE><<<g, kThreads, 0, s>>>(a);
+    CKL();
+    if (prof_on(c)) {
+      static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
+      const std::string nm = std::string("k_apply_stencil<") + (sizeof(T) == 8 ? "f64," : "f32,") +
+                             std::to_string(D) + "," + std::to_string(R) + "," + mname[MODE] + ">@L" + std::to_string(l);
+      prof_end(c, s, nm.c_str(), 0);
+    }
   }
-  CKL();
 }
 
 template <int K>
 static void reduce(maple_ctx* c, const double* part, unsigned nb, double* out, cudaStream_t s) {
-  k_reduce_partials<K><<<c->B, kThreads, 0, s>>>(part, (int)nb, out);
-  CKL();
+  KL(c, s, k_reduce_partials<K><<<c->B, kThreads, 0, s>>>(part, (int)nb, out));
 }
 
 // ---------------------------------------------------------------------------
@@ -305,8 +333,7 @@ static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
     const int Nl = nodes(c->n[l]);
     T* v = o.U[l][0];
     T* w = o.U[l][1];
-    k_power_init<T><<<nblk((size_t)c->B * Nl * D), kThreads, 0, s>>>(v, (size_t)c->B * Nl * D);
-    CKL();
+    KL(c, s, k_power_init<T><<<nblk((size_t)c->B * Nl * D), kThreads, 0, s>>>(v, (size_t)c->B * Nl * D));
     for (int it = 0; it < c->power_iters; ++it) {
       ApplyArgs<T> a{};
       a.u = v;
@@ -316,8 +343,7 @@ static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
       std::swap(v, w);
     }
     reduce<2>(c, c->part, nblk(Nl), c->red, s);
-    k_power_finish<<<nblk(c->B), kThreads, 0, s>>>(c->red, o.hi[l], c->B, c->power_safety);
-    CKL();
+    KL(c, s, k_power_finish<<<nblk(c->B), kThreads, 0, s>>>(c->red, o.hi[l], c->B, c->power_safety));
   }
 }
 
@@ -342,36 +368,36 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
       dM[dev][D == 3 ? 0 : 1] = m;
     }
     M = dM[dev][D == 3 ? 0 : 1];
-    k_level1_elements<D><<<g2(tot, B), kThreads, 0, s>>>(p.o64.rho, M, p.KE[1], nc, p.kscale, act);
-    CKL();
+    KL(c, s, k_level1_elements<D><<<g2(tot, B), kThreads, 0, s>>>(p.o64.rho, M, p.KE[1], nc, p.kscale, act));
   }
   for (int l = 1; l < L; ++l) {
     const int n = c->n[l], N = nodes(n);
     if (l < L - 1) {
       if (prec == MAPLE_FP64) {
-        k_stencil_from_elements<double, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.KE[l], p.o64.S[l],
-                                                                                      p.o64.Dinv[l], nullptr, n, act);
+        KL(c, s, k_stencil_from_elements<double, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(
+                     p.KE[l], p.o64.S[l], p.o64.Dinv[l], nullptr, n, act));
       } else {
-        k_stencil_from_elements<float, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.KE[l], p.o32.S[l],
-                                                                                     p.o32.Dinv[l], nullptr, n, act);
+        KL(c, s, k_stencil_from_elements<float, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(
+                     p.KE[l], p.o32.S[l], p.o32.Dinv[l], nullptr, n, act));
       }
-      CKL();
       // coarsen to the next level
       const int nc = c->n[l + 1];
       const size_t smem = (size_t)2 * 8 * k * k * sizeof(double);
       CK(cudaFuncSetAttribute(k_coarsen_elements<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_coarsen_elements<D><<<dim3(nodes(nc), B), 256, smem, s>>>(p.KE[l], p.KE[l + 1], nc, act);
-      CKL();
+      KL(c, s, k_coarsen_elements<D><<<dim3(nodes(nc), B), 256, smem, s>>>(p.KE[l], p.KE[l + 1], nc, act));
     } else {
       const int ndof = N * D;
-      k_stencil_from_elements<double, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.KE[l], (double*)nullptr,
-                                                                                    (double*)nullptr, p.S64c, n, act);
-      CKL();
+      KL(c, s, k_stencil_from_elements<double, D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.KE[l], (double*)nullptr,
+                                                                                    (double*)nullptr, p.S64c, n, act));
       CK(cudaMemsetAsync(p.Ainv, 0, (size_t)B * ndof * ndof * sizeof(double), s));
-      k_dense_from_stencil<D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.S64c, p.Ainv, n, act);
-      CKL();
-      k_chol_inverse<<<B, 512, 0, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr);
-      CKL();
+      KL(c, s, k_dense_from_stencil<D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.S64c, p.Ainv, n, act));
+      if (ndof <= kCholSmemMax) {
+        const size_t sm = chol_smem_bytes(ndof);
+        CK(cudaFuncSetAttribute(k_chol_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        KL(c, s, k_chol_inverse_smem<<<B, 1024, sm, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr));
+      } else {
+        KL(c, s, k_chol_inverse<<<B, 512, 0, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr));
+      }
     }
   }
   if (prec == MAPLE_FP64)
@@ -393,8 +419,7 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
   const int B = c->B;
   if (l == c->L - 1) {
     const int ndof = nodes(c->n[l]) * D;
-    k_coarse_solve<T, R><<<g2(ndof, B), kThreads, 0, s>>>(p.Ainv, f, o.U[l][1], ndof, D, act);
-    CKL();
+    KL(c, s, k_coarse_solve<T, R><<<g2(ndof, B), kThreads, 0, s>>>(p.Ainv, f, o.U[l][1], ndof, D, act));
     return;
   }
   const int deg = c->cheb_degree;
@@ -430,11 +455,9 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
     apply<T, D, R, M_RES>(c, p, o, l, a, act, s);
   }
   const int nc = c->n[l + 1];
-  k_restrict<T, R * D><<<g2(nodes(nc), B), kThreads, 0, s>>>(o.Res[l], o.F[l + 1], nc, act);
-  CKL();
+  KL(c, s, k_restrict<T, R * D><<<g2(nodes(nc), B), kThreads, 0, s>>>(o.Res[l], o.F[l + 1], nc, act));
   vcycle<T, D, R>(c, p, o, l + 1, o.F[l + 1], act, nullptr, s);
-  k_prolong_add<T, R * D><<<g2(nodes(c->n[l]), B), kThreads, 0, s>>>(o.U[l + 1][1], o.U[l][cur], nc, act);
-  CKL();
+  KL(c, s, k_prolong_add<T, R * D><<<g2(nodes(c->n[l]), B), kThreads, 0, s>>>(o.U[l + 1][1], o.U[l][cur], nc, act));
   for (int st = 0; st < deg; ++st) {
     ApplyArgs<T> a{};
     a.f = f;
@@ -495,8 +518,7 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
   const unsigned nb = nblk(N);                    // partials of the vector kernels
   const unsigned nbf = (unsigned)fine_tiles(c->n[0]);  // partials of the fine-level operator
   PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
-  k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, outer_run, sc.done, sc.cell_done, sc.run, sc.iters, B, R);
-  CKL();
+  KL(c, s, k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, outer_run, sc.done, sc.cell_done, sc.run, sc.iters, B, R));
   const int* run = sc.run;
   // r = b - A x
   if (x_zero) {
@@ -509,22 +531,17 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
     a.out = o.r;
     apply<T, D, R, M_RES>(c, p, o, 0, a, run, s);
   }
-  k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, c->part, N, run);
-  CKL();
+  KL(c, s, k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, c->part, N, run));
   reduce<R>(c, c->part, nb, sc.bnorm2, s);
-  k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.r, o.r, c->part, N, run);
-  CKL();
+  KL(c, s, k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.r, o.r, c->part, N, run));
   reduce<R>(c, c->part, nb, sc.rr, s);
-  k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0);
-  CKL();
-  k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B);
-  CKL();
+  KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0));
+  KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
   if (all_done(c, sc.cell_done, run, s)) return;
   // z = M r ; rz ; p = z
   vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, s);
   reduce<R>(c, c->part, nbf, sc.rz_new, s);
-  k_set_rz<<<nblk(B * R), kThreads, 0, s>>>(sc.rz, sc.rz_new, B * R);
-  CKL();
+  KL(c, s, k_set_rz<<<nblk(B * R), kThreads, 0, s>>>(sc.rz, sc.rz_new, B * R));
   CK(cudaMemcpyAsync(o.p, o.U[0][1], vbytes, cudaMemcpyDeviceToDevice, s));
   for (int it = 1; it <= maxit; ++it) {
     {
@@ -535,23 +552,17 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
       apply<T, D, R, M_MV>(c, p, o, 0, a, run, s);
     }
     reduce<R>(c, c->part, nbf, sc.pq, s);
-    k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown);
-    CKL();
-    k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.x, o.r, o.p, o.q, sc.alpha, c->part, N, run);
-    CKL();
+    KL(c, s, k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown));
+    KL(c, s, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.x, o.r, o.p, o.q, sc.alpha, c->part, N, run));
     reduce<R>(c, c->part, nb, sc.rr, s);
-    k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, it);
-    CKL();
-    k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B);
-    CKL();
+    KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, it));
+    KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
     if (it == maxit) break;
     if (it % c->check_every == 0 && all_done(c, sc.cell_done, run, s)) break;
     vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, s);
     reduce<R>(c, c->part, nbf, sc.rz_new, s);
-    k_pcg_beta<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R);
-    CKL();
-    k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.p, o.U[0][1], sc.beta, N, run);
-    CKL();
+    KL(c, s, k_pcg_beta<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R));
+    KL(c, s, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.p, o.U[0][1], sc.beta, N, run));
   }
 }
 
@@ -565,13 +576,10 @@ static void precondition_f32(maple_ctx* c, Phys& p, const double* r, const doubl
   const int B = c->B, N = nodes(c->n[0]);
   Scalars& sc = c->sc;
   Ops<float>& o = p.o32;
-  k_col_scales<<<nblk(B * R), kThreads, 0, s>>>(sc.rr, c->o_scale, c->o_inv, B * R);
-  CKL();
-  k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, c->o_scale, N, run);
-  CKL();
+  KL(c, s, k_col_scales<<<nblk(B * R), kThreads, 0, s>>>(sc.rr, c->o_scale, c->o_inv, B * R));
+  KL(c, s, k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, c->o_scale, N, run));
   vcycle<float, D, R>(c, p, o, 0, o.r, run, nullptr, s);
-  k_precond_back<R, D><<<g2(N, B), kThreads, 0, s>>>(o.U[0][1], c->o_inv, p.z64, r, q, c->part, N, run);
-  CKL();
+  KL(c, s, k_precond_back<R, D><<<g2(N, B), kThreads, 0, s>>>(o.U[0][1], c->o_inv, p.z64, r, q, c->part, N, run));
   reduce<2 * R>(c, c->part, nblk(N), c->red, s);
 }
 
@@ -585,8 +593,7 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
   PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
   Ops<double>& o64 = p.o64;
   double *r = p.r64, *pv = p.p64, *q = p.q64, *z = p.z64;
-  k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, nullptr, sc.done, sc.cell_done, sc.run, sc.iters, B, R);
-  CKL();
+  KL(c, s, k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, nullptr, sc.done, sc.cell_done, sc.run, sc.iters, B, R));
   const int* run = sc.run;
   if (x_zero) {
     CK(cudaMemsetAsync(x, 0, vbytes, s));
@@ -598,20 +605,15 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
     a.out = r;
     apply<double, D, R, M_RES>(c, p, o64, 0, a, run, s);
   }
-  k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, c->part, N, run);
-  CKL();
+  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, c->part, N, run));
   reduce<R>(c, c->part, nb, sc.bnorm2, s);
-  k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(r, r, c->part, N, run);
-  CKL();
+  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(r, r, c->part, N, run));
   reduce<R>(c, c->part, nb, sc.rr, s);
-  k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0);
-  CKL();
-  k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B);
-  CKL();
+  KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0));
+  KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
   if (all_done(c, sc.cell_done, run, s)) return;
   precondition_f32<D, R>(c, p, r, nullptr, run, s);
-  k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 1);
-  CKL();
+  KL(c, s, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 1));
   CK(cudaMemcpyAsync(pv, z, vbytes, cudaMemcpyDeviceToDevice, s));
   for (int it = 1; it <= maxit; ++it) {
     {
@@ -622,22 +624,16 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
       apply<double, D, R, M_MV>(c, p, o64, 0, a, run, s);
     }
     reduce<R>(c, c->part, nbf, sc.pq, s);
-    k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown);
-    CKL();
-    k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, s>>>(x, r, pv, q, sc.alpha, c->part, N, run);
-    CKL();
+    KL(c, s, k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown));
+    KL(c, s, k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, s>>>(x, r, pv, q, sc.alpha, c->part, N, run));
     reduce<R>(c, c->part, nb, sc.rr, s);
-    k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, it);
-    CKL();
-    k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B);
-    CKL();
+    KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, it));
+    KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
     if (it == maxit) break;
     if (it % c->check_every == 0 && all_done(c, sc.cell_done, run, s)) break;
     precondition_f32<D, R>(c, p, r, q, run, s);
-    k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 0);
-    CKL();
-    k_pcg_direction<double, R, D><<<g2(N, B), kThreads, 0, s>>>(pv, z, sc.beta, N, run);
-    CKL();
+    KL(c, s, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 0));
+    KL(c, s, k_pcg_direction<double, R, D><<<g2(N, B), kThreads, 0, s>>>(pv, z, sc.beta, N, run));
   }
 }
 
@@ -727,8 +723,7 @@ static void ensure_prec(maple_ctx* c, int phys, int prec) {
 static void load_density(maple_ctx* c, int phys, const double* rho, int prec, cudaStream_t s) {
   Phys& p = c->ph[phys];
   const size_t tot = (size_t)c->B * nodes(c->n[0]);
-  k_copy_rho<<<nblk(tot), kThreads, 0, s>>>(rho, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot);
-  CKL();
+  KL(c, s, k_copy_rho<<<nblk(tot), kThreads, 0, s>>>(rho, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot));
 }
 
 static void build(maple_ctx* c, int phys, int prec, cudaStream_t s) {
@@ -742,10 +737,9 @@ static void assemble_rhs(maple_ctx* c, int phys, const double* rho, double* F, c
   Phys& p = c->ph[phys];
   const int N = nodes(c->n[0]);
   if (phys == MAPLE_ELASTIC)
-    k_assemble_F<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(rho, F, c->n[0], p.fscale, c->active);
+    KL(c, s, k_assemble_F<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(rho, F, c->n[0], p.fscale, c->active));
   else
-    k_assemble_F<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(rho, F, c->n[0], p.fscale, c->active);
-  CKL();
+    KL(c, s, k_assemble_F<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(rho, F, c->n[0], p.fscale, c->active));
 }
 
 static void homogenize(maple_ctx* c, int phys, cudaStream_t s) {
@@ -753,19 +747,16 @@ static void homogenize(maple_ctx* c, int phys, cudaStream_t s) {
   const int N = nodes(c->n[0]);
   const unsigned nb = nblk(N);
   if (phys == MAPLE_ELASTIC) {
-    k_homogenize<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, c->part, c->n[0], p.kscale,
-                                                        p.xscale, c->active);
-    CKL();
+    KL(c, s, k_homogenize<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, c->part, c->n[0], p.kscale,
+                                                        p.xscale, c->active));
     reduce<21>(c, c->part, nb, c->red, s);
-    k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(c->red, p.H, c->B, 6);
+    KL(c, s, k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(c->red, p.H, c->B, 6));
   } else {
-    k_homogenize<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, c->part, c->n[0], p.kscale,
-                                                        p.xscale, c->active);
-    CKL();
+    KL(c, s, k_homogenize<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, c->part, c->n[0], p.kscale,
+                                                        p.xscale, c->active));
     reduce<6>(c, c->part, nb, c->red, s);
-    k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(c->red, p.H, c->B, 3);
+    KL(c, s, k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(c->red, p.H, c->B, 3));
   }
-  CKL();
   p.energies = true;
 }
 
@@ -799,8 +790,10 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
     a.active = c->active ? c->active + c0 : nullptr;
     CK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned), s));
     void* args[] = {&a};
+    prof_begin(c, s);
     CK(cudaLaunchCooperativeKernel((void*)k_oc_update, dim3(G, nb), dim3(kThreads), args, 0, s));
     g_launches.fetch_add(1);
+    prof_end(c, s, "k_oc_update", 0);
   }
 }
 
@@ -1128,10 +1121,9 @@ int maple_sensitivity(maple_ctx* c, const double* gC, const double* gK, double* 
     if (gC) require(c->ph[0].energies, "elastic energies missing: call maple_homogenize first");
     if (gK) require(c->ph[1].energies, "thermal energies missing: call maple_homogenize first");
     const int N = nodes(c->n[0]);
-    k_sensitivity<<<g2(N, c->B), kThreads, 0, S(s)>>>(nullptr, gC ? c->ph[0].energy : nullptr,
+    KL(c, S(s), k_sensitivity<<<g2(N, c->B), kThreads, 0, S(s)>>>(nullptr, gC ? c->ph[0].energy : nullptr,
                                                        gK ? c->ph[1].energy : nullptr, gC, gK, nullptr, dJdrho, N, 0, 1,
-                                                       0, c->active);
-    CKL();
+                                                       0, c->active));
   });
 }
 
@@ -1207,9 +1199,8 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       Phys& p = c->ph[phys];
       ensure_prec(c, phys, prec);
       const size_t tot = (size_t)B * N;
-      k_simp<<<nblk(tot), kThreads, 0, st>>>(x, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot, N, xmin,
-                                             penal, rho_min, c->active);
-      CKL();
+      KL(c, st, k_simp<<<nblk(tot), kThreads, 0, st>>>(x, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot, N, xmin,
+                                             penal, rho_min, c->active));
       build(c, phys, prec, st);
       assemble_rhs(c, phys, p.o64.rho, p.F64, st);
       const bool was_solved = p.solved;
@@ -1218,18 +1209,15 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       for (int b = 0; b < B; ++b) it_sum[b] += it_tmp[b];
       homogenize(c, phys, st);
     }
-    k_objective<<<nblk(B), kThreads, 0, st>>>(c->ph[0].H, c->ph[1].H, w, c->Jv, c->terms, c->G3, c->G1, B,
-                                              need_ch ? 1 : 0, need_k ? 1 : 0, c->active);
-    CKL();
-    k_sensitivity<<<g2(N, B), kThreads, 0, st>>>(x, need_ch ? c->ph[0].energy : nullptr,
+    KL(c, st, k_objective<<<nblk(B), kThreads, 0, st>>>(c->ph[0].H, c->ph[1].H, w, c->Jv, c->terms, c->G3, c->G1, B,
+                                              need_ch ? 1 : 0, need_k ? 1 : 0, c->active));
+    KL(c, st, k_sensitivity<<<g2(N, B), kThreads, 0, st>>>(x, need_ch ? c->ph[0].energy : nullptr,
                                                  need_k ? c->ph[1].energy : nullptr, c->G3, c->G1, c->dJdx, nullptr, N,
-                                                 xmin, penal, rho_min, c->active);
-    CKL();
+                                                 xmin, penal, rho_min, c->active));
     const double* dJ = c->dJdx;
     if (filter_k > 1) {
       require(filter_k % 2 == 1, "filter size must be odd");
-      k_box_filter<<<g2(N, B), kThreads, 0, st>>>(c->dJdx, c->dJf, c->n[0], filter_k, c->active);
-      CKL();
+      KL(c, st, k_box_filter<<<g2(N, B), kThreads, 0, st>>>(c->dJdx, c->dJf, c->n[0], filter_k, c->active));
       dJ = c->dJf;
     }
     oc_update(c, x, dJ, vf, move, xmin, x_next, c->stats, st);
