@@ -511,8 +511,78 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
   }
 }
 
+// Coarse levels: one thread per (node, load case) so that the small grids of
+// the deep levels still fill the machine; consecutive threads are consecutive
+// nodes of one load case (coalesced stencil and field loads).
 template <typename T, int D, int R, int MODE>
 __global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
+  static_assert(MODE != M_POWER, "power iterations use k_apply_stencil_power");
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
+  const int n = a.n, N = a.N;
+  const size_t NN = (size_t)N;
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= N * R) return;
+  const int r = t / N, id = t - r * N;
+  const int z = id % n, y = (id / n) % n, x = id / (n * n);
+  const size_t cell = (size_t)b * N;
+  T acc[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) acc[i] = T(0);
+  const T* __restrict__ S = a.S + (size_t)b * 27 * D * D * N + id;
+  if constexpr (MODE != M_JAC0) {
+    const int xs[3] = {wrapn(x - 1, n), x, wrapn(x + 1, n)};
+    const int ys[3] = {wrapn(y - 1, n), y, wrapn(y + 1, n)};
+    const int zs[3] = {wrapn(z - 1, n), z, wrapn(z + 1, n)};
+    const T* __restrict__ ub = a.u + (cell * R + (size_t)r * N) * D;
+#pragma unroll 9
+    for (int o = 0; o < 27; ++o) {
+      const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+      const int nb = (xs[ox] * n + ys[oy]) * n + zs[oz];
+      T uv[D];
+#pragma unroll
+      for (int j = 0; j < D; ++j) uv[j] = __ldg(ub + (size_t)j * NN + nb);
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) acc[i] += __ldg(S + ((size_t)o * D * D + i * D + j) * N) * uv[j];
+    }
+  }
+  T Di[D][D];
+  const T* __restrict__ Dp = a.Dinv + (size_t)b * D * D * N + id;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) Di[i][j] = __ldg(Dp + (size_t)(i * D + j) * N);
+  const size_t vo = (cell * R + (size_t)r * N) * D + id;  // component i at vo + i*N
+  if constexpr (MODE == M_MV) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.out[vo + i * NN] = acc[i];
+  } else if constexpr (MODE == M_RES) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.out[vo + i * NN] = a.f[vo + i * NN] - acc[i];
+  } else {
+    double al, be;
+    cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, al, be);
+    T res[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) res[i] = (MODE == M_JAC0) ? a.f[vo + i * NN] : a.f[vo + i * NN] - acc[i];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      T zz = 0;
+#pragma unroll
+      for (int j = 0; j < D; ++j) zz += Di[i][j] * res[j];
+      T d = T(be) * zz;
+      if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + i * NN];
+      a.dout[vo + i * NN] = d;
+      a.out[vo + i * NN] = (MODE == M_JAC0) ? d : a.u[vo + i * NN] + d;
+    }
+  }
+}
+
+// power iteration step on a coarse level: w = Dinv A u and the Rayleigh terms
+template <typename T, int D>
+__global__ void __launch_bounds__(kThreads) k_apply_stencil_power(ApplyArgs<T> a) {
   const int b = blockIdx.y;
   if (a.active && !a.active[b]) return;
   const int n = a.n, N = a.N;
@@ -522,151 +592,125 @@ __global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
   const int id = valid ? idx : 0;
   const int z = id % n, y = (id / n) % n, x = id / (n * n);
   const size_t cell = (size_t)b * N;
-  T acc[R][D];
+  T acc[D];
 #pragma unroll
-  for (int r = 0; r < R; ++r)
-#pragma unroll
-    for (int i = 0; i < D; ++i) acc[r][i] = T(0);
+  for (int i = 0; i < D; ++i) acc[i] = T(0);
   const T* __restrict__ S = a.S + (size_t)b * 27 * D * D * N + id;
-  if constexpr (MODE != M_JAC0) {
-    const int xs[3] = {wrapn(x - 1, n), x, wrapn(x + 1, n)};
-    const int ys[3] = {wrapn(y - 1, n), y, wrapn(y + 1, n)};
-    const int zs[3] = {wrapn(z - 1, n), z, wrapn(z + 1, n)};
-    const T* __restrict__ ub = a.u + cell * R * D;
-#pragma unroll 3
-    for (int o = 0; o < 27; ++o) {
-      const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
-      T C[D][D];
-#pragma unroll
-      for (int i = 0; i < D; ++i)
-#pragma unroll
-        for (int j = 0; j < D; ++j) C[i][j] = __ldg(S + ((size_t)o * D * D + i * D + j) * N);
-      const T* __restrict__ un = ub + ((size_t)xs[ox] * n + ys[oy]) * n + zs[oz];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        T uv[D];
-#pragma unroll
-        for (int j = 0; j < D; ++j) uv[j] = __ldg(un + (size_t)(r * D + j) * NN);
-#pragma unroll
-        for (int i = 0; i < D; ++i)
-#pragma unroll
-          for (int j = 0; j < D; ++j) acc[r][i] += C[i][j] * uv[j];
-      }
+  const int xs[3] = {wrapn(x - 1, n), x, wrapn(x + 1, n)};
+  const int ys[3] = {wrapn(y - 1, n), y, wrapn(y + 1, n)};
+  const int zs[3] = {wrapn(z - 1, n), z, wrapn(z + 1, n)};
+  const T* __restrict__ ub = a.u + cell * D;
+  for (int o = 0; o < 27; ++o) {
+    const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+    const int nb = (xs[ox] * n + ys[oy]) * n + zs[oz];
+    for (int i = 0; i < D; ++i)
+      for (int j = 0; j < D; ++j) acc[i] += __ldg(S + ((size_t)o * D * D + i * D + j) * N) * __ldg(ub + j * NN + nb);
+  }
+  double dots[2] = {0, 0};
+  if (valid) {
+    const size_t vo = cell * D + id;
+    for (int i = 0; i < D; ++i) {
+      T w = 0;
+      for (int j = 0; j < D; ++j) w += __ldg(a.Dinv + (size_t)b * D * D * N + (size_t)(i * D + j) * N + id) * acc[j];
+      a.out[vo + i * NN] = w;
+      dots[0] += (double)a.u[vo + i * NN] * (double)acc[i];
+      for (int j = 0; j < D; ++j)
+        dots[1] += (double)a.u[vo + i * NN] * (double)__ldg(S + ((size_t)13 * D * D + i * D + j) * N) *
+                   (double)a.u[vo + j * NN];
     }
   }
-  T Di[D][D];
-  const T* __restrict__ Dp = a.Dinv + (size_t)b * D * D * N + id;
-#pragma unroll
-  for (int i = 0; i < D; ++i)
-#pragma unroll
-    for (int j = 0; j < D; ++j) Di[i][j] = __ldg(Dp + (size_t)(i * D + j) * N);
-  const size_t vo = cell * R * D + id;
-  if constexpr (MODE == M_POWER) {
-    double dots[2] = {0, 0};
-    if (valid) {
-      T C0[D][D];
-      for (int i = 0; i < D; ++i)
-        for (int j = 0; j < D; ++j) C0[i][j] = __ldg(S + ((size_t)13 * D * D + i * D + j) * N);
-      for (int i = 0; i < D; ++i) {
-        T w = 0;
-        for (int j = 0; j < D; ++j) w += Di[i][j] * acc[0][j];
-        a.out[vo + i * NN] = w;
-        dots[0] += (double)a.u[vo + i * NN] * (double)acc[0][i];
-        for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i * NN] * (double)C0[i][j] * (double)a.u[vo + j * NN];
-      }
-    }
-    block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
-  } else {
-    apply_epilogue<T, D, R, MODE>(a, b, vo, valid, acc, Di);
-  }
+  block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
 }
 
 // ----------------------------------------------------------------------------
 // grid transfer: periodic trilinear P (EBE_GMG.py:38-79, 531-647)
 // ----------------------------------------------------------------------------
-// rc = P^T rf : coarse node gathers its 27 fine neighbours 2X+d, weight prod(1-|d|/2)
+// rc = P^T rf : coarse node gathers its 27 fine neighbours 2X+d, weight
+// prod(1-|d|/2).  One thread per (coarse node, component).
 template <typename T, int K>
 __global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ rc, int nc, const int* active) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   const int Nc = nc * nc * nc, nf = 2 * nc, Nf = Nc * 8;
-  const int idx = blockIdx.x * kThreads + threadIdx.x;
-  if (idx >= Nc) return;
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= Nc * K) return;
+  const int k = t / Nc, idx = t - k * Nc;
   const int Z = idx % nc, Y = (idx / nc) % nc, X = idx / (nc * nc);
-  T acc[K];
+  const T* __restrict__ base = rf + ((size_t)b * K + k) * Nf;
+  const int fx[3] = {wrapn(2 * X - 1, nf), 2 * X, 2 * X + 1};
+  const int fy[3] = {wrapn(2 * Y - 1, nf), 2 * Y, 2 * Y + 1};
+  const int fz[3] = {wrapn(2 * Z - 1, nf), 2 * Z, 2 * Z + 1};
+  T acc = 0;
 #pragma unroll
-  for (int k = 0; k < K; ++k) acc[k] = 0;
-  const T* __restrict__ base = rf + (size_t)b * Nf * K;
+  for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-    for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-      for (int dz = -1; dz <= 1; ++dz) {
-        const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
-        const int fx = wrapn(2 * X + dx, nf), fy = wrapn(2 * Y + dy, nf), fz = wrapn(2 * Z + dz, nf);
-        const T* p = base + ((size_t)fx * nf + fy) * nf + fz;
-#pragma unroll
-        for (int k = 0; k < K; ++k) acc[k] += w * __ldg(p + (size_t)k * Nf);
+      for (int dz = 0; dz < 3; ++dz) {
+        const T w = T((dx != 1 ? 0.5 : 1.0) * (dy != 1 ? 0.5 : 1.0) * (dz != 1 ? 0.5 : 1.0));
+        acc += w * __ldg(base + ((size_t)fx[dx] * nf + fy[dy]) * nf + fz[dz]);
       }
-  T* o = rc + (size_t)b * Nc * K + idx;
-#pragma unroll
-  for (int k = 0; k < K; ++k) o[(size_t)k * Nc] = acc[k];
+  rc[((size_t)b * K + k) * Nc + idx] = acc;
 }
 
-// uf += P uc
+// uf += P uc, one thread per (fine node, component)
 template <typename T, int K>
 __global__ void k_prolong_add(const T* __restrict__ uc, T* __restrict__ uf, int nc, const int* active) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   const int nf = 2 * nc, Nf = nf * nf * nf, Nc = nc * nc * nc;
-  const int idx = blockIdx.x * kThreads + threadIdx.x;
-  if (idx >= Nf) return;
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= Nf * K) return;
+  const int k = t / Nf, idx = t - k * Nf;
   const int z = idx % nf, y = (idx / nf) % nf, x = idx / (nf * nf);
   const int bx = x >> 1, by = y >> 1, bz = z >> 1, rx = x & 1, ry = y & 1, rz = z & 1;
-  T acc[K];
-#pragma unroll
-  for (int k = 0; k < K; ++k) acc[k] = 0;
-  const T* __restrict__ base = uc + (size_t)b * Nc * K;
+  const T* __restrict__ base = uc + ((size_t)b * K + k) * Nc;
+  const int cx[2] = {bx, bx + 1 == nc ? 0 : bx + 1};
+  const int cy[2] = {by, by + 1 == nc ? 0 : by + 1};
+  const int cz[2] = {bz, bz + 1 == nc ? 0 : bz + 1};
+  const T w = T((rx ? 0.5 : 1.0) * (ry ? 0.5 : 1.0) * (rz ? 0.5 : 1.0));
+  T acc = 0;
 #pragma unroll
   for (int o = 0; o < 8; ++o) {
     const int ox = (o >> 2) & 1, oy = (o >> 1) & 1, oz = o & 1;
     if ((ox && !rx) || (oy && !ry) || (oz && !rz)) continue;
-    const T w = T((rx ? 0.5 : 1.0) * (ry ? 0.5 : 1.0) * (rz ? 0.5 : 1.0));
-    const int cx = bx + ox == nc ? 0 : bx + ox, cy = by + oy == nc ? 0 : by + oy, cz = bz + oz == nc ? 0 : bz + oz;
-    const T* p = base + ((size_t)cx * nc + cy) * nc + cz;
-#pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] += w * __ldg(p + (size_t)k * Nc);
+    acc += w * __ldg(base + ((size_t)cx[ox] * nc + cy[oy]) * nc + cz[oz]);
   }
-  T* o = uf + (size_t)b * Nf * K + idx;
-#pragma unroll
-  for (int k = 0; k < K; ++k) o[(size_t)k * Nf] += acc[k];
+  uf[((size_t)b * K + k) * Nf + idx] += acc;
 }
 
-// coarsest level: u = Ainv f with the FP64 (regularised) inverse, per cell
+// coarsest level: u = Ainv f with the FP64 (regularised) inverse, per cell;
+// one warp per row, lanes over the columns.
 template <typename T, int R>
 __global__ void k_coarse_solve(const double* __restrict__ Ainv, const T* __restrict__ f, T* __restrict__ u, int ndof,
                                int D, const int* active) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
-  const int row = blockIdx.x * kThreads + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
   if (row >= ndof) return;
-  const double* Acol = Ainv + (size_t)b * ndof * ndof + row;
   const int Nc = ndof / D;
+  const double* A = Ainv + ((size_t)b * ndof + row) * ndof;
   const T* fb = f + (size_t)b * ndof * R;  // [rhs][comp][node]; dof = node*D + comp
   double acc[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) acc[r] = 0;
-  for (int col = 0; col < ndof; ++col) {
+  for (int col = lane; col < ndof; col += 32) {
     const int node = col / D, c = col - node * D;
-    const double a = Acol[(size_t)col * ndof];  // symmetric: read column-wise (coalesced)
+    const double a = A[col];
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[r] += a * (double)fb[(size_t)(r * D + c) * Nc + node];
   }
-  const int node = row / D, c = row - node * D;
-  T* ub = u + (size_t)b * ndof * R;
 #pragma unroll
-  for (int r = 0; r < R; ++r) ub[(size_t)(r * D + c) * Nc + node] = (T)acc[r];
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[r] += __shfl_down_sync(0xffffffffu, acc[r], off);
+  if (lane == 0) {
+    const int node = row / D, c = row - node * D;
+    T* ub = u + (size_t)b * ndof * R;
+#pragma unroll
+    for (int r = 0; r < R; ++r) ub[(size_t)(r * D + c) * Nc + node] = (T)acc[r];
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -1511,9 +1555,18 @@ __global__ void __launch_bounds__(kThreads) k_oc_update(OcArgs a) {
     block_sum_store<1>(v, a.part + ((size_t)b * 4 + (it & 1)) * G + g);
     grid_barrier(a.bar, a.bar + 1, nblocks, a.err);
     if (act) {
-      double tot = 0;
-      const double* pp = a.part + ((size_t)b * 4 + (it & 1)) * G;
-      for (int k = 0; k < G; ++k) tot += __ldcg(pp + k);
+      __shared__ double s_tot;
+      if (threadIdx.x < 32) {
+        const double* pp = a.part + ((size_t)b * 4 + (it & 1)) * G;
+        double t = 0;
+        for (int k = threadIdx.x; k < G; k += 32) t += __ldcg(pp + k);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+        if (threadIdx.x == 0) s_tot = t;
+      }
+      __syncthreads();
+      const double tot = s_tot;
+      __syncthreads();
       if (tot / (double)N > vf)
         l1 = lam;
       else

@@ -304,7 +304,13 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
     a.S = o.S[l];
     a.Dinv = o.Dinv[l];
     prof_begin(c, s);
-    k_apply_stencil<T, D, R, MODE><<<g, kThreads, 0, s>>>(a);
+    if constexpr (MODE == M_POWER) {
+      static_assert(R == 1, "power iterations run on one column");
+      k_apply_stencil_power<T, D><<<g, kThreads, 0, s>>>(a);
+    } else {
+      require(a.part == nullptr, "coarse-level applies produce no partial sums");
+      k_apply_stencil<T, D, R, MODE><<<g2((size_t)a.N * R, c->B), kThreads, 0, s>>>(a);
+    }
     CKL();
     if (prof_on(c)) {
       static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
@@ -419,7 +425,7 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
   const int B = c->B;
   if (l == c->L - 1) {
     const int ndof = nodes(c->n[l]) * D;
-    KL(c, s, k_coarse_solve<T, R><<<g2(ndof, B), kThreads, 0, s>>>(p.Ainv, f, o.U[l][1], ndof, D, act));
+    KL(c, s, k_coarse_solve<T, R><<<dim3((ndof + 7) / 8, B), kThreads, 0, s>>>(p.Ainv, f, o.U[l][1], ndof, D, act));
     return;
   }
   const int deg = c->cheb_degree;
@@ -455,9 +461,10 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
     apply<T, D, R, M_RES>(c, p, o, l, a, act, s);
   }
   const int nc = c->n[l + 1];
-  KL(c, s, k_restrict<T, R * D><<<g2(nodes(nc), B), kThreads, 0, s>>>(o.Res[l], o.F[l + 1], nc, act));
+  KL(c, s, k_restrict<T, R * D><<<g2((size_t)nodes(nc) * R * D, B), kThreads, 0, s>>>(o.Res[l], o.F[l + 1], nc, act));
   vcycle<T, D, R>(c, p, o, l + 1, o.F[l + 1], act, nullptr, s);
-  KL(c, s, k_prolong_add<T, R * D><<<g2(nodes(c->n[l]), B), kThreads, 0, s>>>(o.U[l + 1][1], o.U[l][cur], nc, act));
+  KL(c, s, k_prolong_add<T, R * D><<<g2((size_t)nodes(c->n[l]) * R * D, B), kThreads, 0, s>>>(o.U[l + 1][1],
+                                                                                             o.U[l][cur], nc, act));
   for (int st = 0; st < deg; ++st) {
     ApplyArgs<T> a{};
     a.f = f;
