@@ -70,6 +70,10 @@ int maple_ctx_info(const maple_ctx* ctx, int* levels_out, int* coarsest_n_out, s
 int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio, int power_iters, double inner_rtol,
                              int check_every);
 
+/* CUDA-graph replay of the PCG iteration body (default on).  Off runs every
+ * launch eagerly (same results). */
+int maple_set_graphs(maple_ctx* ctx, int enable);
+
 /* Per-cell active mask (host int[B], nonzero = active). Inactive cells are
  * skipped by every kernel.  NULL = all active. */
 int maple_set_active(maple_ctx* ctx, const int* active_host, maple_stream_t stream);

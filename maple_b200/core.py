@@ -106,6 +106,10 @@ class HomogenizationContext:
         with torch.cuda.device(self.device):
             _lib.check(self._lib.maple_set_active(self._h, arr, _stream(self.device)))
 
+    def set_graphs(self, enable: bool):
+        """Replay the PCG iteration body as a captured CUDA graph (default on)."""
+        _lib.check(self._lib.maple_set_graphs(self._h, int(bool(enable))))
+
     def profile(self, enable: bool, max_launches: int = 100000):
         """Bracket every fine-level operator launch with CUDA events."""
         _lib.check(self._lib.maple_profile_enable(self._h, int(bool(enable)), int(max_launches)))

@@ -182,6 +182,7 @@ struct ApplyArgs {
   T* dout;                 // Chebyshev direction out
   T* out;                  // MV/RES/POWER output, CHEB/JAC0 new iterate
   const double* hi;        // per-cell Chebyshev upper bound (CHEB, JAC0)
+  double cheb_al, cheb_be; // this block's step coefficients (set inside the kernels)
   double ratio;            // Chebyshev interval ratio hi/lo
   int step;                // Chebyshev step index
   double* part;            // per-block partial dots [B][nblk][R or 2] (nullable)
@@ -377,8 +378,7 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
           dots[r] += (double)y * (double)y;
         }
     } else if constexpr (MODE == M_CHEB || MODE == M_JAC0) {
-      double al, be;
-      cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, al, be);
+      const double al = a.cheb_al, be = a.cheb_be;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         T res[D];
@@ -451,16 +451,26 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
     cp_async<sizeof(T)>(srho + w, a.rho + cell + ((size_t)gx * n + gy) * n + gz);
   }
   if constexpr (MODE != M_JAC0) {
+    // 25 groups of 10 lanes: a group copies whole halo rows (10 nodes along z),
+    // lane iz owning one z position; the R*D components of a row then follow
+    // with incremental addresses (component-major global, node-major shared).
+    constexpr int ROWS = (TX + 2) * (TY + 2);
+    constexpr int GROUPS = kThreads / (TZ + 2);
     const T* __restrict__ ub = a.u + cell * RD;
-    for (int w = threadIdx.x; w < G::HALO_NODES * RD; w += kThreads) {
-      const int k = w / G::HALO_NODES, hn = w - k * G::HALO_NODES;
-      const int iz = hn % (TZ + 2), iy = (hn / (TZ + 2)) % (TY + 2), ix = hn / ((TZ + 2) * (TY + 2));
-      int gx = xm + ix, gy = ym + iy, gz = zm + iz;
-      gx += gx < 0 ? n : (gx >= n ? -n : 0);
-      gy += gy < 0 ? n : (gy >= n ? -n : 0);
+    const int g = threadIdx.x / (TZ + 2), iz = threadIdx.x - g * (TZ + 2);
+    if (g < GROUPS) {
+      int gz = zm + iz;
       gz += gz < 0 ? n : (gz >= n ? -n : 0);
-      cp_async<sizeof(T)>(su + (ix * (TY + 2) + iy) * G::RW + iz * G::NS + k,
-                          ub + (size_t)k * NN + ((size_t)gx * n + gy) * n + gz);
+      for (int row = g; row < ROWS; row += GROUPS) {
+        const int ix = row / (TY + 2), iy = row - ix * (TY + 2);
+        int gx = xm + ix, gy = ym + iy;
+        gx += gx < 0 ? n : (gx >= n ? -n : 0);
+        gy += gy < 0 ? n : (gy >= n ? -n : 0);
+        const T* src = ub + ((size_t)gx * n + gy) * n + gz;
+        T* dst = su + row * G::RW + iz * G::NS;
+#pragma unroll 6
+        for (int k = 0; k < RD; ++k) cp_async<sizeof(T)>(dst + k, src + (size_t)k * NN);
+      }
     }
   }
   cp_async_wait_all();
@@ -507,6 +517,13 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
     }
     block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
   } else {
+    if constexpr (MODE == M_CHEB || MODE == M_JAC0) {
+      __shared__ double s_coef[2];
+      if (threadIdx.x == 0) cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, s_coef[0], s_coef[1]);
+      __syncthreads();
+      a.cheb_al = s_coef[0];
+      a.cheb_be = s_coef[1];
+    }
     apply_epilogue<T, D, R, MODE>(a, b, vo, valid, acc, Di);
   }
 }
@@ -1124,17 +1141,19 @@ __global__ void k_pcg_alpha(PcgScalars s, int total, int* breakdown) {
 }
 
 // after the update: convergence test on ||r|| <= rtol ||b||
-__global__ void k_pcg_check(PcgScalars s, int B, int R, double rtol2, int it) {
+// `count` = 1 inside the iteration loop: the per-cell iteration counter is
+// advanced on the device so that the launch parameters stay fixed (graphs).
+__global__ void k_pcg_check(PcgScalars s, int B, int R, double rtol2, int count) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
   if (s.cell_done[b]) return;
+  if (count) s.iters[b] += 1;
   int all = 1;
   for (int c = 0; c < R; ++c) {
     const int i = b * R + c;
     if (!s.done[i] && s.rr[i] <= rtol2 * s.bnorm2[i]) s.done[i] = 1;
     all &= (s.done[i] != 0);
   }
-  s.iters[b] = it;
   if (all) s.cell_done[b] = 1;
 }
 

@@ -148,6 +148,13 @@ struct maple_ctx {
   unsigned* bar = nullptr;
   int* err = nullptr;
   int oc_G = 0;
+  // captured PCG iteration bodies: [physics][precision]
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    double rtol = -1;
+  } graphs[2][2];
+  cudaStream_t cap_stream = nullptr;
+  bool use_graphs = true;
   // per-kernel-class event timing of fine-level launches (bench instrumentation)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -516,6 +523,61 @@ __global__ void k_set_rz(double* rz, const double* rz_new, int total) {
   if (i < total) rz[i] = rz_new[i];
 }
 
+// Runs the PCG iteration body until every active cell has converged or maxit
+// iterations ran.  The body is captured once into a CUDA graph per
+// (physics, precision, rtol) and replayed; the convergence flags are read back
+// after every replay (cells that converged skip all further work on device).
+// Runs the PCG iteration body until every active cell has converged or maxit
+// iterations ran.  The body is captured once into a CUDA graph per
+// (physics, precision, rtol) and replayed; the convergence flags are read back
+// after every replay (cells that converged skip all further work on device).
+// The first iteration of a solve always runs eagerly, which also performs the
+// one-time kernel attribute setup outside of any capture.
+template <typename Body>
+static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, double rtol, int maxit, Body& body,
+                           cudaStream_t s) {
+  const bool graphs = c->use_graphs && !c->profiling;
+  for (int it = 1; it <= maxit; ++it) {
+    if (!graphs || it == 1) {
+      body(s);
+    } else {
+      if (ge.exec == nullptr || ge.rtol != rtol) {
+        if (ge.exec) {
+          CK(cudaGraphExecDestroy(ge.exec));
+          ge.exec = nullptr;
+        }
+        if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          body(c->cap_stream);
+        } catch (...) {
+          cudaStreamEndCapture(c->cap_stream, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          throw;
+        }
+        CK(cudaStreamEndCapture(c->cap_stream, &graph));
+        CK(cudaGraphInstantiate(&ge.exec, graph, 0));
+        CK(cudaGraphDestroy(graph));
+        ge.rtol = rtol;
+      }
+      CK(cudaGraphLaunch(ge.exec, s));
+    }
+    if (it % c->check_every == 0 || it == maxit) {
+      if (all_done(c, c->sc.cell_done, nullptr, s)) break;
+    }
+  }
+}
+
+static void drop_graphs(maple_ctx* c) {
+  for (auto& row : c->graphs)
+    for (auto& ge : row) {
+      if (ge.exec) cudaGraphExecDestroy(ge.exec);
+      ge.exec = nullptr;
+      ge.rtol = -1;
+    }
+}
+
 template <typename T, int D, int R>
 static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, double rtol, int maxit,
                 const int* outer_run, cudaStream_t s) {
@@ -550,27 +612,26 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
   reduce<R>(c, c->part, nbf, sc.rz_new, s);
   KL(c, s, k_set_rz<<<nblk(B * R), kThreads, 0, s>>>(sc.rz, sc.rz_new, B * R));
   CK(cudaMemcpyAsync(o.p, o.U[0][1], vbytes, cudaMemcpyDeviceToDevice, s));
-  for (int it = 1; it <= maxit; ++it) {
+  auto body = [&](cudaStream_t st) {
     {
       ApplyArgs<T> a{};
       a.u = o.p;
       a.out = o.q;
       a.part = c->part;
-      apply<T, D, R, M_MV>(c, p, o, 0, a, run, s);
+      apply<T, D, R, M_MV>(c, p, o, 0, a, run, st);
     }
-    reduce<R>(c, c->part, nbf, sc.pq, s);
-    KL(c, s, k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown));
-    KL(c, s, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.x, o.r, o.p, o.q, sc.alpha, c->part, N, run));
-    reduce<R>(c, c->part, nb, sc.rr, s);
-    KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, it));
-    KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
-    if (it == maxit) break;
-    if (it % c->check_every == 0 && all_done(c, sc.cell_done, run, s)) break;
-    vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, s);
-    reduce<R>(c, c->part, nbf, sc.rz_new, s);
-    KL(c, s, k_pcg_beta<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R));
-    KL(c, s, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.p, o.U[0][1], sc.beta, N, run));
-  }
+    reduce<R>(c, c->part, nbf, sc.pq, st);
+    KL(c, st, k_pcg_alpha<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R, c->breakdown));
+    KL(c, st, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.x, o.r, o.p, o.q, sc.alpha, c->part, N, run));
+    reduce<R>(c, c->part, nb, sc.rr, st);
+    KL(c, st, k_pcg_check<<<nblk(B), kThreads, 0, st>>>(ps, B, R, rtol * rtol, 1));
+    KL(c, st, k_sync_run<<<nblk(B), kThreads, 0, st>>>(sc.cell_done, sc.run, B));
+    vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, st);
+    reduce<R>(c, c->part, nbf, sc.rz_new, st);
+    KL(c, st, k_pcg_beta<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R));
+    KL(c, st, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.p, o.U[0][1], sc.beta, N, run));
+  };
+  run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_FP64], rtol, maxit, body, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -622,26 +683,25 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
   precondition_f32<D, R>(c, p, r, nullptr, run, s);
   KL(c, s, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 1));
   CK(cudaMemcpyAsync(pv, z, vbytes, cudaMemcpyDeviceToDevice, s));
-  for (int it = 1; it <= maxit; ++it) {
+  auto body = [&](cudaStream_t st) {
     {
       ApplyArgs<double> a{};
       a.u = pv;
       a.out = q;
       a.part = c->part;
-      apply<double, D, R, M_MV>(c, p, o64, 0, a, run, s);
+      apply<double, D, R, M_MV>(c, p, o64, 0, a, run, st);
     }
-    reduce<R>(c, c->part, nbf, sc.pq, s);
-    KL(c, s, k_pcg_alpha<<<nblk(B * R), kThreads, 0, s>>>(ps, B * R, c->breakdown));
-    KL(c, s, k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, s>>>(x, r, pv, q, sc.alpha, c->part, N, run));
-    reduce<R>(c, c->part, nb, sc.rr, s);
-    KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, it));
-    KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
-    if (it == maxit) break;
-    if (it % c->check_every == 0 && all_done(c, sc.cell_done, run, s)) break;
-    precondition_f32<D, R>(c, p, r, q, run, s);
-    KL(c, s, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 0));
-    KL(c, s, k_pcg_direction<double, R, D><<<g2(N, B), kThreads, 0, s>>>(pv, z, sc.beta, N, run));
-  }
+    reduce<R>(c, c->part, nbf, sc.pq, st);
+    KL(c, st, k_pcg_alpha<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R, c->breakdown));
+    KL(c, st, k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, st>>>(x, r, pv, q, sc.alpha, c->part, N, run));
+    reduce<R>(c, c->part, nb, sc.rr, st);
+    KL(c, st, k_pcg_check<<<nblk(B), kThreads, 0, st>>>(ps, B, R, rtol * rtol, 1));
+    KL(c, st, k_sync_run<<<nblk(B), kThreads, 0, st>>>(sc.cell_done, sc.run, B));
+    precondition_f32<D, R>(c, p, r, q, run, st);
+    KL(c, st, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, st>>>(ps, c->red, B, R, 0));
+    KL(c, st, k_pcg_direction<double, R, D><<<g2(N, B), kThreads, 0, st>>>(pv, z, sc.beta, N, run));
+  };
+  run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_MIXED], rtol, maxit, body, s);
 }
 
 // outer refinement bookkeeping: per (cell, rhs) residual scale and cell done
@@ -997,6 +1057,8 @@ int maple_ctx_destroy(maple_ctx* c) {
   return guarded([&] {
     if (!c) return;
     for (auto& e : c->ev_pool) cudaEventDestroy(e);
+    drop_graphs(c);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     for (void* p : c->allocs) cudaFree(p);
     if (c->h_flags) cudaFreeHost(c->h_flags);
     delete c;
@@ -1012,6 +1074,14 @@ int maple_ctx_info(const maple_ctx* c, int* levels, int* coarsest, size_t* bytes
   });
 }
 
+int maple_set_graphs(maple_ctx* c, int enable) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    drop_graphs(c);
+    c->use_graphs = enable != 0;
+  });
+}
+
 int maple_set_solver_options(maple_ctx* c, int deg, double ratio, int piters, double inner_rtol, int check_every) {
   return guarded([&] {
     require(c != nullptr, "ctx is NULL");
@@ -1020,6 +1090,7 @@ int maple_set_solver_options(maple_ctx* c, int deg, double ratio, int piters, do
     require(piters >= 1 && piters <= 100, "power iterations must be in [1, 100]");
     require(inner_rtol > 0 && inner_rtol < 1, "inner tolerance must be in (0, 1)");
     require(check_every >= 1, "check_every must be >= 1");
+    drop_graphs(c);  // captured launches embed these settings
     c->cheb_degree = deg;
     c->cheb_ratio = ratio;
     c->power_iters = piters;

@@ -227,3 +227,26 @@ def test_multigrid_quality_iteration_counts(lib):
     for phys in ("elastic", "thermal"):
         assert rel(H[("mixed", phys)], H[("fp64", phys)]) < 1e-9
     c.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replay_matches_eager(lib, precision):
+    """The captured PCG iteration replays the same launches: identical results
+    and iteration counts with graphs on and off."""
+    from maple_b200.core import HomogenizationContext
+    r = 16
+    rho = T(simp(O.seed_density(1, r, 2.0, 0.3)).reshape(1, -1))
+    out = []
+    for graphs in (False, True):
+        c = HomogenizationContext(r, ncells=1)
+        c.set_graphs(graphs)
+        res = []
+        for phys in ("elastic", "thermal"):
+            c.set_density(phys, rho, precision)
+            info = c.solve(phys, precision, rtol=1e-10, maxit=200)
+            res.append((int(info.iters[0]), c.homogenize(phys).cpu().numpy()))
+        out.append(res)
+        c.close()
+    for (i0, h0), (i1, h1) in zip(out[0], out[1]):
+        assert i0 == i1
+        assert np.array_equal(h0, h1)
