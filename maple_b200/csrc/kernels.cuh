@@ -597,6 +597,127 @@ __global__ void __launch_bounds__(kThreads) k_apply_stencil(ApplyArgs<T> a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Coarse levels, tiled: a CTA owns a 4x4x4 node tile and runs one thread per
+// (tile node, load case).  The tile's stencils, block-diagonal inverses and
+// the halo'd field values are staged into shared memory with asynchronous
+// copies that are all in flight together, which removes the dependent-load
+// latency chains that dominate small grids.  Requires n % 4 == 0.
+// ---------------------------------------------------------------------------
+constexpr int CT = 4;                         // tile edge
+constexpr int CT_NODES = CT * CT * CT;        // 64
+constexpr int CT_HALO = (CT + 2) * (CT + 2) * (CT + 2);  // 216
+
+template <typename T, int D, int R>
+struct CoarseTile {
+  static constexpr int RD = R * D;
+  static constexpr int NS = RD % 2 ? RD : RD + 1;   // odd node stride
+  static constexpr int S_WORDS = 27 * D * D * CT_NODES;
+  static constexpr int DI_WORDS = D * D * CT_NODES;
+  static constexpr int U_WORDS = CT_HALO * NS;
+  static constexpr size_t BYTES = (size_t)(S_WORDS + DI_WORDS + U_WORDS) * sizeof(T);
+  static constexpr int THREADS = CT_NODES * R;
+};
+
+template <typename T, int D, int R, int MODE>
+__global__ void __launch_bounds__(CT_NODES * 6) k_apply_stencil_tile(ApplyArgs<T> a) {
+  using G = CoarseTile<T, D, R>;
+  constexpr int RD = R * D;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sS = reinterpret_cast<T*>(smem_raw);          // [27*D*D][64]
+  T* sDi = sS + G::S_WORDS;                         // [D*D][64]
+  T* sU = sDi + G::DI_WORDS;                        // [216][NS]
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
+  const int n = a.n, N = a.N;
+  const size_t NN = (size_t)N;
+  const int nt = n / CT;
+  const int tile = blockIdx.x;
+  const int z0 = (tile % nt) * CT, y0 = ((tile / nt) % nt) * CT, x0 = (tile / (nt * nt)) * CT;
+  const int tid = threadIdx.x;
+  // ---- stage: stencil rows and Dinv of the 64 tile nodes (16-byte chunks of
+  //      4 consecutive z nodes), and the halo'd field values (scalar copies)
+  {
+    constexpr int CH = CT / (16 / (int)sizeof(T) < CT ? 16 / (int)sizeof(T) : CT);  // chunks per z-run
+    constexpr int CW = CT / CH;                     // elements per chunk (4 floats or 2 doubles)
+    const T* Sb = a.S + (size_t)b * 27 * D * D * N;
+    const T* Db = a.Dinv + (size_t)b * D * D * N;
+    constexpr int RUNS = CT * CT;                   // (x,y) runs per tile
+    for (int w = tid; w < (27 * D * D + D * D) * RUNS * CH; w += G::THREADS) {
+      const int ch = w % CH, run = (w / CH) % RUNS, k = w / (CH * RUNS);
+      const int ix = run / CT, iy = run % CT;
+      const size_t gofs = ((size_t)(x0 + ix) * n + (y0 + iy)) * n + z0 + ch * CW;
+      const int sofs = (ix * CT + iy) * CT + ch * CW;
+      if (k < 27 * D * D)
+        cp_async<CW * sizeof(T)>(sS + k * CT_NODES + sofs, Sb + (size_t)k * N + gofs);
+      else
+        cp_async<CW * sizeof(T)>(sDi + (k - 27 * D * D) * CT_NODES + sofs, Db + (size_t)(k - 27 * D * D) * N + gofs);
+    }
+    if constexpr (MODE != M_JAC0) {
+      const T* ub = a.u + (size_t)b * RD * N;
+      for (int w = tid; w < CT_HALO * RD; w += G::THREADS) {
+        const int k = w / CT_HALO, h = w - k * CT_HALO;
+        const int iz = h % (CT + 2), iy = (h / (CT + 2)) % (CT + 2), ix = h / ((CT + 2) * (CT + 2));
+        int gx = x0 - 1 + ix, gy = y0 - 1 + iy, gz = z0 - 1 + iz;
+        gx += gx < 0 ? n : (gx >= n ? -n : 0);
+        gy += gy < 0 ? n : (gy >= n ? -n : 0);
+        gz += gz < 0 ? n : (gz >= n ? -n : 0);
+        cp_async<sizeof(T)>(sU + h * G::NS + k, ub + (size_t)k * N + ((size_t)gx * n + gy) * n + gz);
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+  const int tn = tid % CT_NODES, r = tid / CT_NODES;
+  const int tz = tn % CT, ty = (tn / CT) % CT, tx = tn / (CT * CT);
+  T acc[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) acc[i] = T(0);
+  if constexpr (MODE != M_JAC0) {
+#pragma unroll
+    for (int o = 0; o < 27; ++o) {
+      const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+      const T* un = sU + (((tx + ox) * (CT + 2) + (ty + oy)) * (CT + 2) + (tz + oz)) * G::NS + r * D;
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) acc[i] += sS[((o * D + i) * D + j) * CT_NODES + tn] * un[j];
+    }
+  }
+  T Di[D][D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) Di[i][j] = sDi[(i * D + j) * CT_NODES + tn];
+  const int id = ((x0 + tx) * n + (y0 + ty)) * n + (z0 + tz);
+  const size_t vo = ((size_t)b * R + r) * D * NN + id;   // component i at vo + i*N
+  if constexpr (MODE == M_MV) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.out[vo + i * NN] = acc[i];
+  } else if constexpr (MODE == M_RES) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.out[vo + i * NN] = a.f[vo + i * NN] - acc[i];
+  } else {
+    __shared__ double s_coef[2];
+    if (tid == 0) cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, s_coef[0], s_coef[1]);
+    __syncthreads();
+    const double al = s_coef[0], be = s_coef[1];
+    T res[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) res[i] = (MODE == M_JAC0) ? a.f[vo + i * NN] : a.f[vo + i * NN] - acc[i];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      T zz = 0;
+#pragma unroll
+      for (int j = 0; j < D; ++j) zz += Di[i][j] * res[j];
+      T d = T(be) * zz;
+      if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + i * NN];
+      a.dout[vo + i * NN] = d;
+      a.out[vo + i * NN] = (MODE == M_JAC0) ? d : a.u[vo + i * NN] + d;
+    }
+  }
+}
+
 // power iteration step on a coarse level: w = Dinv A u and the Rayleigh terms
 template <typename T, int D>
 __global__ void __launch_bounds__(kThreads) k_apply_stencil_power(ApplyArgs<T> a) {

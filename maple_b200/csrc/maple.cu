@@ -316,7 +316,19 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
       k_apply_stencil_power<T, D><<<g, kThreads, 0, s>>>(a);
     } else {
       require(a.part == nullptr, "coarse-level applies produce no partial sums");
-      k_apply_stencil<T, D, R, MODE><<<g2((size_t)a.N * R, c->B), kThreads, 0, s>>>(a);
+      if (a.n % CT == 0) {
+        using G = CoarseTile<T, D, R>;
+        static bool attr_set = false;  // one per template instantiation
+        if (!attr_set) {
+          CK(cudaFuncSetAttribute(k_apply_stencil_tile<T, D, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)G::BYTES));
+          attr_set = true;
+        }
+        const int nt = a.n / CT;
+        k_apply_stencil_tile<T, D, R, MODE><<<dim3(nt * nt * nt, c->B), G::THREADS, G::BYTES, s>>>(a);
+      } else {
+        k_apply_stencil<T, D, R, MODE><<<g2((size_t)a.N * R, c->B), kThreads, 0, s>>>(a);
+      }
     }
     CKL();
     if (prof_on(c)) {
