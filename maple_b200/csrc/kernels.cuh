@@ -16,7 +16,8 @@
 namespace maple {
 
 constexpr int kThreads = 256;
-constexpr int TX = 4, TY = 8, TZ = 8;  // fine-level node tile per CTA (z fastest)
+constexpr int TX = 4, TY = 4, TZ = 8;  // fine-level node tile per CTA (z fastest)
+constexpr int kFineThreads = TX * TY * TZ;
 
 __constant__ double c_Ke3d[576];
 __constant__ float c_Ke3f[576];
@@ -59,9 +60,9 @@ __device__ __forceinline__ int wrapn(int i, int n) { return i < 0 ? i + n : (i >
 // ----------------------------------------------------------------------------
 // block reductions (deterministic: fixed shuffle tree + fixed warp order)
 // ----------------------------------------------------------------------------
-template <int K>
+template <int K, int NWARP = kThreads / 32>
 __device__ __forceinline__ void block_sum_store(double (&v)[K], double* out) {
-  __shared__ double sm[kThreads / 32][K];
+  __shared__ double sm[NWARP][K];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
@@ -76,7 +77,7 @@ __device__ __forceinline__ void block_sum_store(double (&v)[K], double* out) {
   if (threadIdx.x < K) {
     double s = 0;
 #pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) s += sm[w][threadIdx.x];
+    for (int w = 0; w < NWARP; ++w) s += sm[w][threadIdx.x];
     out[threadIdx.x] = s;
   }
 }
@@ -350,9 +351,9 @@ __device__ __forceinline__ void fine_tile_all(std::integer_sequence<int, Os...>,
 
 // Shared epilogue of both apply kernels.
 // vo = cell*R*D*N + node; component (r, i) lives at vo + (r*D + i) * N.
-template <typename T, int D, int R, int MODE>
+template <typename T, int D, int R, int MODE, int NWARP = kThreads / 32>
 __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, size_t vo, bool valid, T (&acc)[R][D],
-                                               const T (&Di)[D][D]) {
+                                               const T (&Di)[D][D], const T* uown = nullptr, size_t uown_stride = 0) {
   const size_t NN = (size_t)a.N;
   constexpr int K = R;
   double dots[K];
@@ -366,7 +367,8 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
         for (int i = 0; i < D; ++i) {
           const T y = a.scale * acc[r][i];
           a.out[vo + (size_t)(r * D + i) * NN] = y;
-          if (a.part) dots[r] += (double)y * (double)a.u[vo + (size_t)(r * D + i) * NN];
+          if (a.part)
+            dots[r] += (double)y * (double)(uown ? uown[(r * D + i) * uown_stride] : a.u[vo + (size_t)(r * D + i) * NN]);
         }
     } else if constexpr (MODE == M_RES) {
 #pragma unroll
@@ -397,7 +399,8 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
           T d = T(be) * z;
           if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + (size_t)(r * D + i) * NN];
           a.dout[vo + (size_t)(r * D + i) * NN] = d;
-          const T un = (MODE == M_JAC0) ? d : a.u[vo + (size_t)(r * D + i) * NN] + d;
+          const T uo = uown ? uown[(r * D + i) * uown_stride] : a.u[vo + (size_t)(r * D + i) * NN];
+          const T un = (MODE == M_JAC0) ? d : uo + d;
           a.out[vo + (size_t)(r * D + i) * NN] = un;
           if (a.dot_f_out) dots[r] += (double)a.f[vo + (size_t)(r * D + i) * NN] * (double)un;
         }
@@ -405,7 +408,7 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
     }
   }
   if (a.part && (MODE != M_CHEB || a.dot_f_out)) {
-    block_sum_store<K>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * K);
+    block_sum_store<K, NWARP>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * K);
   }
 }
 
@@ -415,13 +418,13 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
 // shared memory.  Node stride NS is odd and each (x,y) row is padded so that
 // the 32 lanes of a warp (tz 0..7, ty 0..3) hit 32 distinct banks.
 // ---------------------------------------------------------------------------
-static_assert(TX * TY * TZ == kThreads, "tile must match the block size");
+static_assert(kFineThreads % 32 == 0 && TZ * 4 == 32, "a warp spans tz 0..7 x ty 0..3");
 
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 __host__ __device__ inline int fine_tiles(int n) { return ceil_div(n, TX) * ceil_div(n, TY) * ceil_div(n, TZ); }
 
 template <typename T, int D, int R, int MODE>
-__global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
+__global__ void __launch_bounds__(kFineThreads) k_apply_fine(ApplyArgs<T> a) {
   using G = FineTile<T, R * D>;
   constexpr int RD = R * D;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -442,7 +445,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
   //      and the halo'd node values (component-major in global memory,
   //      node-major in shared memory), all as asynchronous copies in flight
   const int xm = x0 - 1, ym = y0 - 1, zm = z0 - 1;
-  for (int w = threadIdx.x; w < G::RHO_WORDS; w += kThreads) {
+  for (int w = threadIdx.x; w < G::RHO_WORDS; w += kFineThreads) {
     const int iz = w % (TZ + 1), iy = (w / (TZ + 1)) % (TY + 1), ix = w / ((TZ + 1) * (TY + 1));
     int gx = xm + ix, gy = ym + iy, gz = zm + iz;
     gx += gx < 0 ? n : (gx >= n ? -n : 0);
@@ -455,7 +458,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
     // lane iz owning one z position; the R*D components of a row then follow
     // with incremental addresses (component-major global, node-major shared).
     constexpr int ROWS = (TX + 2) * (TY + 2);
-    constexpr int GROUPS = kThreads / (TZ + 2);
+    constexpr int GROUPS = kFineThreads / (TZ + 2);
     const T* __restrict__ ub = a.u + cell * RD;
     const int g = threadIdx.x / (TZ + 2), iz = threadIdx.x - g * (TZ + 2);
     if (g < GROUPS) {
@@ -515,7 +518,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
         for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i * NN] * (double)C0s[i][j] * (double)a.u[vo + j * NN];
       }
     }
-    block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
+    block_sum_store<2, kFineThreads / 32>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
   } else {
     if constexpr (MODE == M_CHEB || MODE == M_JAC0) {
       __shared__ double s_coef[2];
@@ -524,7 +527,9 @@ __global__ void __launch_bounds__(kThreads) k_apply_fine(ApplyArgs<T> a) {
       a.cheb_al = s_coef[0];
       a.cheb_be = s_coef[1];
     }
-    apply_epilogue<T, D, R, MODE>(a, b, vo, valid, acc, Di);
+    // the node's own values are the centre of the staged tile (stride 1)
+    const T* uown = (MODE == M_JAC0) ? nullptr : su + ((tx + 1) * (TY + 2) + (ty + 1)) * G::RW + (tz + 1) * G::NS;
+    apply_epilogue<T, D, R, MODE, kFineThreads / 32>(a, b, vo, valid, acc, Di, uown, 1);
   }
 }
 
@@ -643,7 +648,8 @@ __global__ void __launch_bounds__(CT_NODES * 6) k_apply_stencil_tile(ApplyArgs<T
     const T* Sb = a.S + (size_t)b * 27 * D * D * N;
     const T* Db = a.Dinv + (size_t)b * D * D * N;
     constexpr int RUNS = CT * CT;                   // (x,y) runs per tile
-    for (int w = tid; w < (27 * D * D + D * D) * RUNS * CH; w += G::THREADS) {
+    constexpr int K0 = MODE == M_JAC0 ? 27 * D * D : 0;  // JAC0 needs only the inverses
+    for (int w = tid + K0 * RUNS * CH; w < (27 * D * D + D * D) * RUNS * CH; w += G::THREADS) {
       const int ch = w % CH, run = (w / CH) % RUNS, k = w / (CH * RUNS);
       const int ix = run / CT, iy = run % CT;
       const size_t gofs = ((size_t)(x0 + ix) * n + (y0 + iy)) * n + z0 + ch * CW;
@@ -806,13 +812,16 @@ __global__ void k_prolong_add(const T* __restrict__ uc, T* __restrict__ uf, int 
   const int cx[2] = {bx, bx + 1 == nc ? 0 : bx + 1};
   const int cy[2] = {by, by + 1 == nc ? 0 : by + 1};
   const int cz[2] = {bz, bz + 1 == nc ? 0 : bz + 1};
-  const T w = T((rx ? 0.5 : 1.0) * (ry ? 0.5 : 1.0) * (rz ? 0.5 : 1.0));
+  // branch-free: an even fine coordinate takes weight 1 from its own coarse
+  // node and 0 from the next one, an odd one 1/2 from each
+  const T wx[2] = {T(rx ? 0.5 : 1.0), T(rx ? 0.5 : 0.0)};
+  const T wy[2] = {T(ry ? 0.5 : 1.0), T(ry ? 0.5 : 0.0)};
+  const T wz[2] = {T(rz ? 0.5 : 1.0), T(rz ? 0.5 : 0.0)};
   T acc = 0;
 #pragma unroll
   for (int o = 0; o < 8; ++o) {
     const int ox = (o >> 2) & 1, oy = (o >> 1) & 1, oz = o & 1;
-    if ((ox && !rx) || (oy && !ry) || (oz && !rz)) continue;
-    acc += w * __ldg(base + ((size_t)cx[ox] * nc + cy[oy]) * nc + cz[oz]);
+    acc += (wx[ox] * wy[oy] * wz[oz]) * __ldg(base + ((size_t)cx[ox] * nc + cy[oy]) * nc + cz[oz]);
   }
   uf[((size_t)b * K + k) * Nf + idx] += acc;
 }

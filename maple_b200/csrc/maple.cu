@@ -295,7 +295,7 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
       attr_set = true;
     }
     prof_begin(c, s);
-    k_apply_fine<T, D, R, MODE><<<dim3(fine_tiles(a.n), c->B), kThreads, G::BYTES, s>>>(a);
+    k_apply_fine<T, D, R, MODE><<<dim3(fine_tiles(a.n), c->B), kFineThreads, G::BYTES, s>>>(a);
     CKL();
     if (prof_on(c)) {
       static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
