@@ -152,6 +152,7 @@ struct maple_ctx {
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
     double rtol = -1;
+    unsigned long long kernels = 0;  // kernel nodes per replay (for launch counting)
   } graphs[2][2];
   cudaStream_t cap_stream = nullptr;
   bool use_graphs = true;
@@ -560,6 +561,7 @@ static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, double rtol,
         }
         if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
         cudaGraph_t graph = nullptr;
+        const unsigned long long before = g_launches.load();
         CK(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
         try {
           body(c->cap_stream);
@@ -572,8 +574,11 @@ static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, double rtol,
         CK(cudaGraphInstantiate(&ge.exec, graph, 0));
         CK(cudaGraphDestroy(graph));
         ge.rtol = rtol;
+        ge.kernels = g_launches.load() - before;
+        g_launches.fetch_sub(ge.kernels);  // captured, not launched
       }
       CK(cudaGraphLaunch(ge.exec, s));
+      g_launches.fetch_add(ge.kernels);
     }
     if (it % c->check_every == 0 || it == maxit) {
       if (all_done(c, c->sc.cell_done, nullptr, s)) break;
