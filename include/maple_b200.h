@@ -143,6 +143,19 @@ int maple_box_filter(int r, int ncells, int k, const double* in, double* out, ma
 int maple_oc_update(maple_ctx* ctx, const double* x, const double* dJdx, const double* volfrac, double move, double xmin,
                     double* xnew, double* stats, maple_stream_t stream);
 
+/* The OC update of maple_oc_update without a context and without allocating
+ * anything: for host applications that manage all device memory themselves
+ * and cannot let a library call cudaMalloc.  Its scratch (partial sums,
+ * statistics when stats is NULL, barrier counters) lives in one fixed 256 KiB
+ * device array per GPU, held until the process exits.  N = elements per cell;
+ * at most 8191 cells per call with stats given (5460 with stats NULL); larger
+ * batches are rejected.  The first call on a device looks up the array's
+ * address; make it before any stream capture.  Calls share the array, so calls
+ * whose kernels overlap on the GPU race.  This entry point has no counterpart
+ * in the reference. */
+int maple_oc_update_noalloc(int N, int ncells, const double* x, const double* dJdx, const double* volfrac, double move,
+                            double xmin, double* xnew, double* stats, maple_stream_t stream);
+
 /* One full OC iteration on device for every active cell (main_IHD_v3.py:
  * 620-716 with symmetry "none" and no manufacturing penalties): SIMP map,
  * both solves (as needed by the weights), C^H / kappa^H, objective

@@ -45,6 +45,7 @@ SIGNATURES = {
     "maple_matvec": (_I, [_P, _I, _P, _P, _P, _P]),
     "maple_box_filter": (_I, [_I, _I, _I, _P, _P, _P]),
     "maple_oc_update": (_I, [_P, _P, _P, _P, _D, _D, _P, _P, _P]),
+    "maple_oc_update_noalloc": (_I, [_I, _I, _P, _P, _P, _D, _D, _P, _P, _P]),
     "maple_launch_count": (C.c_ulonglong, []),
     "maple_profile_enable": (_I, [_P, _I, _I]),
     "maple_profile_read": (_I, [_P, C.c_char_p, _I]),

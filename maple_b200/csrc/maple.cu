@@ -881,6 +881,46 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
   }
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free OC update.
+//
+// Some host applications own every byte of device memory through their own
+// allocator and do not let a library call cudaMalloc (which also synchronises
+// the whole device and so stalls their other streams).  For them the OC
+// bisection kernel can run with its scratch (per-block partial sums, per-cell
+// |dx| statistics when the caller passes none, and the grid-barrier counters)
+// in one fixed, file-scope device array instead of context workspace.
+//
+// * The array is 256 KiB (kNoAllocScratch doubles) and every GPU that loads
+//   this library holds it until the process exits.
+// * Host code cannot use the array's name as a device address: its address is
+//   fetched once per device with cudaGetSymbolAddress.  The first call on a
+//   device does that set-up, so make that first call before any stream capture.
+// * All calls share the array and it keeps the last call's contents; the
+//   barrier counters are cleared at the start of every call.  Calls whose
+//   kernels overlap on the GPU (for example on two streams) race on it.
+// ---------------------------------------------------------------------------
+static constexpr int kNoAllocScratch = 32768;  // doubles
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratch];
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_addr[128] = {};
+
+static double* noalloc_scratch_address() {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  require(dev >= 0 && dev < 128, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      throw Failure{MAPLE_E_CUDA, std::string("cudaGetSymbolAddress of the OC scratch array failed: ") +
+                                      cudaGetErrorString(e)};
+    g_noalloc_addr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_addr[dev];
+}
+
 }  // namespace maple
 
 using namespace maple;
@@ -1264,6 +1304,57 @@ int maple_oc_update(maple_ctx* c, const double* x, const double* dJdx, const dou
     require(c != nullptr && x && dJdx && vf && xnew, "NULL argument");
     require(xnew != x, "xnew must not alias x");
     oc_update(c, x, dJdx, vf, move, xmin, xnew, stats, S(s));
+  });
+}
+
+int maple_oc_update_noalloc(int N, int ncells, const double* x, const double* dJdx, const double* vf, double move,
+                            double xmin, double* xnew, double* stats, maple_stream_t s) {
+  return guarded([&] {
+    require(x && dJdx && vf && xnew, "NULL argument");
+    require(xnew != x, "xnew must not alias x");
+    require(N >= 1 && ncells >= 1, "N and ncells must be positive");
+    // layout of the array per launch: [4*nb*G partial sums][2*nb statistics if
+    // the caller passes none] ... [4 doubles: barrier count, generation, error]
+    constexpr int kTail = 4;
+    const int per_cell_min = 4 + (stats ? 0 : 2);  // G = 1
+    const int max_cells = (kNoAllocScratch - kTail) / per_cell_min;
+    require(ncells <= max_cells, "maple_oc_update_noalloc: " + std::to_string(ncells) + " cells exceed the " +
+                                     std::to_string(max_cells) + " cells its fixed 256 KiB scratch array holds");
+    double* scratch = noalloc_scratch_address();
+    cudaStream_t st = S(s);
+    int dev = 0, per_sm = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oc_update, kThreads, 0));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int maxres = per_sm * sms;
+    require(maxres >= 1, "OC kernel cannot be resident");
+    const int want_G = std::max(1, std::min(sms, (N + 4 * kThreads - 1) / (4 * kThreads)));
+    const int cells_per_launch = std::max(1, std::min(ncells, maxres / want_G));
+    unsigned* bar = reinterpret_cast<unsigned*>(scratch + kNoAllocScratch - kTail);
+    int* err = reinterpret_cast<int*>(scratch + kNoAllocScratch - kTail + 2);
+    for (int c0 = 0; c0 < ncells; c0 += cells_per_launch) {
+      const int nb = std::min(cells_per_launch, ncells - c0);
+      const int stats_words = stats ? 0 : 2 * nb;
+      const int G = std::max(1, std::min({want_G, maxres / nb, (kNoAllocScratch - kTail - stats_words) / (4 * nb)}));
+      OcArgs a{};
+      a.x = x + (size_t)c0 * N;
+      a.dJ = dJdx + (size_t)c0 * N;
+      a.xnew = xnew + (size_t)c0 * N;
+      a.volfrac = vf + c0;
+      a.move = move;
+      a.xmin = xmin;
+      a.N = N;
+      a.part = scratch;
+      a.stats = stats ? stats + 2 * c0 : scratch + (size_t)4 * nb * G;
+      a.lam_out = nullptr;
+      a.bar = bar;
+      a.err = err;
+      a.active = nullptr;
+      CK(cudaMemsetAsync(scratch + kNoAllocScratch - kTail, 0, kTail * sizeof(double), st));
+      void* args[] = {&a};
+      CK(cudaLaunchCooperativeKernel((void*)k_oc_update, dim3(G, nb), dim3(kThreads), args, 0, st));
+      g_launches.fetch_add(1);
+    }
   });
 }
 
