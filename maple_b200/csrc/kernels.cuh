@@ -353,9 +353,7 @@ __device__ __forceinline__ void fine_tile_all(std::integer_sequence<int, Os...>,
 // vo = cell*R*D*N + node; component (r, i) lives at vo + (r*D + i) * N.
 template <typename T, int D, int R, int MODE, int NWARP = kThreads / 32>
 __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, size_t vo, bool valid, T (&acc)[R][D],
-                                               const T (&Di)[D][D], const T* uown = nullptr, size_t uown_stride = 0,
-                                               const T* fown = nullptr, const T* down = nullptr,
-                                               size_t own_stride = 0, size_t part_idx = ~(size_t)0) {
+                                               const T (&Di)[D][D], const T* uown = nullptr, size_t uown_stride = 0) {
   const size_t NN = (size_t)a.N;
   constexpr int K = R;
   double dots[K];
@@ -377,7 +375,7 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
       for (int r = 0; r < R; ++r)
 #pragma unroll
         for (int i = 0; i < D; ++i) {
-          const T y = (fown ? fown[(r * D + i) * own_stride] : a.f[vo + (size_t)(r * D + i) * NN]) - a.scale * acc[r][i];
+          const T y = a.f[vo + (size_t)(r * D + i) * NN] - a.scale * acc[r][i];
           a.out[vo + (size_t)(r * D + i) * NN] = y;
           dots[r] += (double)y * (double)y;
         }
@@ -389,9 +387,9 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
 #pragma unroll
         for (int i = 0; i < D; ++i) {
           if constexpr (MODE == M_JAC0)
-            res[i] = (fown ? fown[(r * D + i) * own_stride] : a.f[vo + (size_t)(r * D + i) * NN]);
+            res[i] = a.f[vo + (size_t)(r * D + i) * NN];
           else
-            res[i] = (fown ? fown[(r * D + i) * own_stride] : a.f[vo + (size_t)(r * D + i) * NN]) - a.scale * acc[r][i];
+            res[i] = a.f[vo + (size_t)(r * D + i) * NN] - a.scale * acc[r][i];
         }
 #pragma unroll
         for (int i = 0; i < D; ++i) {
@@ -399,19 +397,18 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
 #pragma unroll
           for (int j = 0; j < D; ++j) z += Di[i][j] * res[j];
           T d = T(be) * z;
-          if (MODE == M_CHEB && al != 0.0) d += T(al) * (down ? down[(r * D + i) * own_stride] : a.din[vo + (size_t)(r * D + i) * NN]);
+          if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + (size_t)(r * D + i) * NN];
           a.dout[vo + (size_t)(r * D + i) * NN] = d;
           const T uo = uown ? uown[(r * D + i) * uown_stride] : a.u[vo + (size_t)(r * D + i) * NN];
           const T un = (MODE == M_JAC0) ? d : uo + d;
           a.out[vo + (size_t)(r * D + i) * NN] = un;
-          if (a.dot_f_out) dots[r] += (double)(fown ? fown[(r * D + i) * own_stride] : a.f[vo + (size_t)(r * D + i) * NN]) * (double)un;
+          if (a.dot_f_out) dots[r] += (double)a.f[vo + (size_t)(r * D + i) * NN] * (double)un;
         }
       }
     }
   }
   if (a.part && (MODE != M_CHEB || a.dot_f_out)) {
-    const size_t pi = part_idx != ~(size_t)0 ? part_idx : (size_t)b * gridDim.x + blockIdx.x;
-    block_sum_store<K, NWARP>(dots, a.part + pi * K);
+    block_sum_store<K, NWARP>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * K);
   }
 }
 
@@ -426,34 +423,28 @@ static_assert(kFineThreads % 32 == 0 && TZ * 4 == 32, "a warp spans tz 0..7 x ty
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 __host__ __device__ inline int fine_tiles(int n) { return ceil_div(n, TX) * ceil_div(n, TY) * ceil_div(n, TZ); }
 
-// Per-tile shared-memory stage of the fine kernel: halo'd field values and
-// element densities, plus the tile's own f and Chebyshev direction (SoA,
-// [component][tile node]) when the mode reads them.
-template <typename T, int RD, int MODE>
-struct FineStage {
-  using G = FineTile<T, RD>;
-  static constexpr bool NEED_U = MODE != M_JAC0;
-  static constexpr bool NEED_F = MODE == M_RES || MODE == M_CHEB || MODE == M_JAC0;
-  static constexpr bool NEED_DIN = MODE == M_CHEB;
-  static constexpr int F_OFF = (G::RHO_OFF + G::RHO_WORDS + 3) / 4 * 4;
-  static constexpr int DIN_OFF = F_OFF + (NEED_F ? RD * kFineThreads : 0);
-  static constexpr int WORDS = (DIN_OFF + (NEED_DIN ? RD * kFineThreads : 0) + 3) / 4 * 4;
-  static constexpr size_t BYTES = (size_t)WORDS * sizeof(T);
-};
-
-// Issue the asynchronous copies of one tile into a stage (no wait).
 template <typename T, int D, int R, int MODE>
-__device__ __forceinline__ void fine_stage_tile(const ApplyArgs<T>& a, int b, int tile, T* st) {
+__global__ void __launch_bounds__(kFineThreads) k_apply_fine(ApplyArgs<T> a) {
   using G = FineTile<T, R * D>;
-  using S = FineStage<T, R * D, MODE>;
   constexpr int RD = R * D;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* su = reinterpret_cast<T*>(smem_raw);
+  T* srho = su + G::RHO_OFF;
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
   const int n = a.n;
-  const size_t NN = (size_t)a.N, cell = (size_t)b * NN;
+  const size_t NN = (size_t)a.N;
   const int ntz = ceil_div(n, TZ), nty = ceil_div(n, TY);
+  const int tile = blockIdx.x;
   const int z0 = (tile % ntz) * TZ, y0 = ((tile / ntz) % nty) * TY, x0 = (tile / (ntz * nty)) * TX;
+  const int tz = threadIdx.x % TZ, ty = (threadIdx.x / TZ) % TY, tx = threadIdx.x / (TZ * TY);
+  const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
+  const bool valid = x < n && y < n && z < n;
+  const size_t cell = (size_t)b * NN;
+  // ---- stage densities of the (TX+1)(TY+1)(TZ+1) elements touching the tile
+  //      and the halo'd node values (component-major in global memory,
+  //      node-major in shared memory), all as asynchronous copies in flight
   const int xm = x0 - 1, ym = y0 - 1, zm = z0 - 1;
-  T* su = st;
-  T* srho = st + G::RHO_OFF;
   for (int w = threadIdx.x; w < G::RHO_WORDS; w += kFineThreads) {
     const int iz = w % (TZ + 1), iy = (w / (TZ + 1)) % (TY + 1), ix = w / ((TZ + 1) * (TY + 1));
     int gx = xm + ix, gy = ym + iy, gz = zm + iz;
@@ -462,10 +453,10 @@ __device__ __forceinline__ void fine_stage_tile(const ApplyArgs<T>& a, int b, in
     gz += gz < 0 ? n : (gz >= n ? -n : 0);
     cp_async<sizeof(T)>(srho + w, a.rho + cell + ((size_t)gx * n + gy) * n + gz);
   }
-  if constexpr (S::NEED_U) {
-    // groups of 10 lanes copy whole halo rows (10 nodes along z), lane iz owning
-    // one z position; the R*D components of a row follow with incremental
-    // addresses (component-major global, node-major shared)
+  if constexpr (MODE != M_JAC0) {
+    // 25 groups of 10 lanes: a group copies whole halo rows (10 nodes along z),
+    // lane iz owning one z position; the R*D components of a row then follow
+    // with incremental addresses (component-major global, node-major shared).
     constexpr int ROWS = (TX + 2) * (TY + 2);
     constexpr int GROUPS = kFineThreads / (TZ + 2);
     const T* __restrict__ ub = a.u + cell * RD;
@@ -485,120 +476,60 @@ __device__ __forceinline__ void fine_stage_tile(const ApplyArgs<T>& a, int b, in
       }
     }
   }
-  if constexpr (S::NEED_F || S::NEED_DIN) {
-    const int tz = threadIdx.x % TZ, ty = (threadIdx.x / TZ) % TY, tx = threadIdx.x / (TZ * TY);
-    const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
-    if (x < n && y < n && z < n) {
-      const size_t vo = cell * RD + ((size_t)x * n + y) * n + z;
-#pragma unroll 6
-      for (int k = 0; k < RD; ++k) {
-        if constexpr (S::NEED_F) cp_async<sizeof(T)>(st + S::F_OFF + k * kFineThreads + threadIdx.x, a.f + vo + k * NN);
-        if constexpr (S::NEED_DIN)
-          cp_async<sizeof(T)>(st + S::DIN_OFF + k * kFineThreads + threadIdx.x, a.din + vo + k * NN);
-      }
-    }
+  cp_async_wait_all();
+  __syncthreads();
+  T rq[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
+    rq[q] = srho[((tx + qx) * (TY + 1) + (ty + qy)) * (TZ + 1) + (tz + qz)];
   }
-  asm volatile("cp.async.commit_group;\n" ::);
-}
-
-// Fine level, persistent and double-buffered: a CTA walks the (cell, tile)
-// list with stride gridDim.x and stages tile t+1 while it computes tile t.
-// Partial dot products are stored per (cell, tile) like a one-tile-per-CTA
-// launch of fine_tiles(n) blocks would store them.
-template <typename T, int D, int R, int MODE>
-__global__ void __launch_bounds__(kFineThreads) k_apply_fine(ApplyArgs<T> a, int total_tiles) {
-  using G = FineTile<T, R * D>;
-  using S = FineStage<T, R * D, MODE>;
-  constexpr int RD = R * D;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* stage[2] = {reinterpret_cast<T*>(smem_raw), reinterpret_cast<T*>(smem_raw) + S::WORDS};
-  __shared__ double s_coef[2];
-  const int n = a.n;
-  const size_t NN = (size_t)a.N;
-  const int tpc = fine_tiles(n);
-  const int ntz = ceil_div(n, TZ), nty = ceil_div(n, TY);
-  const int tz = threadIdx.x % TZ, ty = (threadIdx.x / TZ) % TY, tx = threadIdx.x / (TZ * TY);
-  int t = blockIdx.x;
-  // skip tiles of inactive cells up front (uniform per block)
-  auto next_active = [&](int from) {
-    while (from < total_tiles && a.active && !a.active[from / tpc]) from += gridDim.x;
-    return from;
-  };
-  t = next_active(t);
-  if (t >= total_tiles) return;
-  fine_stage_tile<T, D, R, MODE>(a, t / tpc, t % tpc, stage[0]);
-  for (int it = 0; t < total_tiles; ++it) {
-    const int tn = next_active(t + gridDim.x);
-    if (tn < total_tiles) {
-      fine_stage_tile<T, D, R, MODE>(a, tn / tpc, tn % tpc, stage[(it + 1) & 1]);
-      asm volatile("cp.async.wait_group 1;\n" ::);
-    } else {
-      asm volatile("cp.async.wait_group 0;\n" ::);
-    }
-    __syncthreads();
-    const int b = t / tpc, tile = t % tpc;
-    T* st = stage[it & 1];
-    const T* su = st;
-    const T* srho = st + G::RHO_OFF;
-    const int z0 = (tile % ntz) * TZ, y0 = ((tile / ntz) % nty) * TY, x0 = (tile / (ntz * nty)) * TX;
-    const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
-    const bool valid = x < n && y < n && z < n;
-    T rq[8];
+  T acc[R][D];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
-      rq[q] = srho[((tx + qx) * (TY + 1) + (ty + qy)) * (TZ + 1) + (tz + qz)];
-    }
-    T acc[R][D];
+  for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int r = 0; r < R; ++r)
+    for (int i = 0; i < D; ++i) acc[r][i] = T(0);
+  T C0[D][D];
+  if constexpr (MODE == M_JAC0) {
+    fine_block<T, D, 13>(rq, C0);
+  } else {
+    const T* base = su + (tx * (TY + 2) + ty) * G::RW + tz * G::NS;
+    fine_tile_all<T, D, R, G::RW, G::NS>(std::make_integer_sequence<int, 27>{}, rq, base, acc, C0);
+  }
+  T Di[D][D];
+  T C0s[D][D];
 #pragma unroll
-      for (int i = 0; i < D; ++i) acc[r][i] = T(0);
-    T C0[D][D];
-    if constexpr (MODE == M_JAC0) {
-      fine_block<T, D, 13>(rq, C0);
-    } else {
-      const T* base = su + (tx * (TY + 2) + ty) * G::RW + tz * G::NS;
-      fine_tile_all<T, D, R, G::RW, G::NS>(std::make_integer_sequence<int, 27>{}, rq, base, acc, C0);
-    }
-    T Di[D][D];
-    T C0s[D][D];
+  for (int i = 0; i < D; ++i)
 #pragma unroll
-    for (int i = 0; i < D; ++i)
-#pragma unroll
-      for (int j = 0; j < D; ++j) C0s[i][j] = a.scale * C0[i][j];
-    block_inverse<T, D>(C0s, Di);
-    const int id = valid ? (x * n + y) * n + z : 0;
-    const size_t vo = (size_t)b * NN * RD + id;
-    const size_t pidx = (size_t)b * tpc + tile;
-    if constexpr (MODE == M_POWER) {
-      double dots[2] = {0, 0};
-      if (valid) {
-        const T* un = su + ((tx + 1) * (TY + 2) + (ty + 1)) * G::RW + (tz + 1) * G::NS;
-        for (int i = 0; i < D; ++i) {
-          T Au = a.scale * acc[0][i], w = 0;
-          for (int j = 0; j < D; ++j) w += Di[i][j] * (a.scale * acc[0][j]);
-          a.out[vo + i * NN] = w;
-          dots[0] += (double)un[i] * (double)Au;
-          for (int j = 0; j < D; ++j) dots[1] += (double)un[i] * (double)C0s[i][j] * (double)un[j];
-        }
+    for (int j = 0; j < D; ++j) C0s[i][j] = a.scale * C0[i][j];
+  block_inverse<T, D>(C0s, Di);
+  const int id = valid ? (x * n + y) * n + z : 0;
+  const size_t vo = cell * RD + id;
+  if constexpr (MODE == M_POWER) {
+    double dots[2] = {0, 0};
+    if (valid) {
+      T Au[D];
+      for (int i = 0; i < D; ++i) Au[i] = a.scale * acc[0][i];
+      for (int i = 0; i < D; ++i) {
+        T w = 0;
+        for (int j = 0; j < D; ++j) w += Di[i][j] * Au[j];
+        a.out[vo + i * NN] = w;
+        dots[0] += (double)a.u[vo + i * NN] * (double)Au[i];
+        for (int j = 0; j < D; ++j) dots[1] += (double)a.u[vo + i * NN] * (double)C0s[i][j] * (double)a.u[vo + j * NN];
       }
-      block_sum_store<2, kFineThreads / 32>(dots, a.part + pidx * 2);
-    } else {
-      if constexpr (MODE == M_CHEB || MODE == M_JAC0) {
-        if (threadIdx.x == 0) cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, s_coef[0], s_coef[1]);
-        __syncthreads();
-        a.cheb_al = s_coef[0];
-        a.cheb_be = s_coef[1];
-      }
-      const T* uown = S::NEED_U ? su + ((tx + 1) * (TY + 2) + (ty + 1)) * G::RW + (tz + 1) * G::NS : nullptr;
-      const T* fown = S::NEED_F ? st + S::F_OFF + threadIdx.x : nullptr;
-      const T* down = S::NEED_DIN ? st + S::DIN_OFF + threadIdx.x : nullptr;
-      apply_epilogue<T, D, R, MODE, kFineThreads / 32>(a, b, vo, valid, acc, Di, uown, 1, fown, down, kFineThreads,
-                                                        pidx);
     }
-    __syncthreads();  // the stage is overwritten by the copies issued next iteration
-    t = tn;
+    block_sum_store<2, kFineThreads / 32>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
+  } else {
+    if constexpr (MODE == M_CHEB || MODE == M_JAC0) {
+      __shared__ double s_coef[2];
+      if (threadIdx.x == 0) cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, s_coef[0], s_coef[1]);
+      __syncthreads();
+      a.cheb_al = s_coef[0];
+      a.cheb_be = s_coef[1];
+    }
+    // the node's own values are the centre of the staged tile (stride 1)
+    const T* uown = (MODE == M_JAC0) ? nullptr : su + ((tx + 1) * (TY + 2) + (ty + 1)) * G::RW + (tz + 1) * G::NS;
+    apply_epilogue<T, D, R, MODE, kFineThreads / 32>(a, b, vo, valid, acc, Di, uown, 1);
   }
 }
 

@@ -288,20 +288,15 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
   const dim3 g = g2(a.N, c->B);
   if (l == 0) {
     a.rho = o.rho;
-    using SG = FineStage<T, R * D, MODE>;
-    const size_t smem = 2 * SG::BYTES;
-    static int grid_cap[128] = {};  // resident CTAs per device, per template instantiation
-    if (!grid_cap[c->dev]) {
-      CK(cudaFuncSetAttribute(k_apply_fine<T, D, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      int per_sm = 0, sms = 0;
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_fine<T, D, R, MODE>, kFineThreads, smem));
-      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
-      grid_cap[c->dev] = std::max(1, per_sm) * sms;
+    using G = FineTile<T, R * D>;
+    static bool attr_set = false;  // one per template instantiation
+    if (!attr_set) {
+      CK(cudaFuncSetAttribute(k_apply_fine<T, D, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)G::BYTES));
+      attr_set = true;
     }
-    const int total = fine_tiles(a.n) * c->B;
-    const int grid = std::min(total, grid_cap[c->dev]);
     prof_begin(c, s);
-    k_apply_fine<T, D, R, MODE><<<grid, kFineThreads, smem, s>>>(a, total);
+    k_apply_fine<T, D, R, MODE><<<dim3(fine_tiles(a.n), c->B), kFineThreads, G::BYTES, s>>>(a);
     CKL();
     if (prof_on(c)) {
       static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
