@@ -165,3 +165,24 @@ def test_optimize_inverse_homogenization(ihd8, golden, tmp_path):
             cavity_seed_faces="all", cavity_iters=128, cavity_tiles=1, cavity_tiles_xyz=None,
             cavity_focus_center=True, filter_k=3, output_dir=str(tmp_path), mesh_every=0, mesh_res=32, mesh_iso=0.3,
             mesh_pad=2, verbose=False)
+
+
+def test_batched_cells_match_single_cell_runs(lib):
+    """B cells with different volume fractions and weights advanced together
+    follow the same trajectories as one-cell runs, and stop independently."""
+    from maple_b200.batch import oc_run, seeded_design
+    r, B = 8, 4
+    rng = np.random.default_rng(5)
+    vf = np.array([0.1, 0.2, 0.3, 0.35])
+    w = rng.dirichlet((1, 1, 1), B)
+    x0 = np.stack([seeded_design(b, r, 1.5, vf[b]).reshape(-1) for b in range(B)])
+    res = oc_run(x0, w, vf, precision="fp64", rtol=1e-12, max_iters=3, dx_tol=0.0)
+    assert (res.iters_run == 3).all()
+    for b in range(B):
+        one = oc_run(x0[b:b + 1], w[b:b + 1], vf[b:b + 1], precision="fp64", rtol=1e-12, max_iters=3, dx_tol=0.0)
+        assert abs(one.J[0] - res.J[b]) <= 1e-10 * abs(one.J[0])
+        assert np.abs(one.x.cpu().numpy() - res.x[b:b + 1].cpu().numpy()).max() < 1e-9
+    # independent stopping: a loose tolerance stops cells at different iterations
+    res2 = oc_run(x0, w, vf, precision="mixed", rtol=1e-8, max_iters=40, dx_tol=0.02)
+    assert res2.converged.any()
+    assert (res2.iters_run <= 40).all() and (res2.iters_run >= 1).all()
