@@ -169,9 +169,91 @@ int maple_oc_step(maple_ctx* ctx, const double* x, const double* weights, const 
                   int warm, double* x_next, double* J, double* terms, double* CH, double* kappa, double* stats,
                   int* iters_out_host, maple_stream_t stream);
 
+/* Initial iterate for the next warm-started solve: copies u [B][R][D][N]
+ * (device, FP64) into the context's solution of `physics`, so that
+ * maple_solve / maple_oc_step with warm = 1 start from it.  Takes the role of
+ * GMGSolver.solve(init_list=...) (EBE_GMG.py:648-757, 851-858), where the
+ * reference aligns network-predicted fields to the node order as initial u. */
+int maple_set_solution(maple_ctx* ctx, int physics, const double* u, maple_stream_t stream);
+
 /* Number of kernels this library has launched in this process (all
  * contexts); used to count device launches inside a timed region. */
 unsigned long long maple_launch_count(void);
+
+/* ---------------------------------------------------------------------------
+ * Learned initial guess: periodic 3-D convolution network kernels.
+ * No counterpart in the reference's FE path (its network-initialisation hook,
+ * EBE_GMG.py:733-757, is fed by no network on the live path).
+ *
+ * Activations are channels-last [B][n^3][C] BF16 (voxel id x*n*n + y*n + z);
+ * weights [taps][cin][cout] BF16, taps = 27 (3x3x3, tap = 9(dx+1)+3(dy+1)+dz+1)
+ * or 1; bias [cout] FP32.  All convolutions are periodic (circular padding).
+ * Errors: maple_nn_last_error_string().
+ * ------------------------------------------------------------------------- */
+enum { MAPLE_NN_POOL = 0, MAPLE_NN_UPSAMPLE = 1, MAPLE_NN_UPSAMPLE_ADJ = 2, MAPLE_NN_POOL_ADJ = 3 };
+
+const char* maple_nn_last_error_string(void);
+unsigned long long maple_nn_launch_count(void);
+
+/* out = act(conv(in, W) + bias + res); act = ReLU if relu.  out (BF16) and/or
+ * out_f32 (FP32, same layout); bias and res nullable (res may alias out).
+ * BF16 products with FP32 accumulation on the tensor cores. */
+int maple_nn_conv3d(const void* in, const void* W, const float* bias, const void* res, void* out, float* out_f32,
+                    int B, int n, int cin, int cout, int ksize, int relu, maple_stream_t stream);
+
+/* dW += sum over cells and voxels of in(shifted by tap) x dz (FP32 [taps][cin][cout]);
+ * db += sum of dz (nullable). */
+int maple_nn_conv3d_wgrad(const void* in, const void* dz, float* dW, float* db, int B, int n, int cin, int cout,
+                          int ksize, maple_stream_t stream);
+
+/* Wt[taps-1-tap][co][ci] = W[tap][ci][co]: the weights whose forward
+ * convolution of dz is the data gradient. */
+int maple_nn_flip_weights(const void* W, void* Wt, int cin, int cout, int ksize, maple_stream_t stream);
+
+/* 2x resampling between nc^3 and (2nc)^3 grids of C channels:
+ * POOL (fine src -> coarse dst, mean of 8), UPSAMPLE (coarse src -> fine dst,
+ * plus base if given), UPSAMPLE_ADJ (fine -> coarse, sum of 8), POOL_ADJ
+ * (coarse -> fine, 1/8 each).  add != 0 accumulates into dst. */
+int maple_nn_resample(int op, const void* src, const void* base, void* dst, int B, int nc, int C, int add,
+                      maple_stream_t stream);
+
+/* dst = src (+ dst when add) elementwise (BF16). */
+int maple_nn_accumulate(void* dst, const void* src, size_t total, int add, maple_stream_t stream);
+
+/* g = g * [y > 0] elementwise (BF16). */
+int maple_nn_relu_mask(const void* y, void* g, size_t total, maple_stream_t stream);
+
+/* loss += mean (pred - target)^2; grad = gscale * d loss / d pred (BF16, nullable). */
+int maple_nn_mse(const float* pred, const void* target, void* grad, float* loss, size_t total, float gscale,
+                 maple_stream_t stream);
+
+/* One Adam step (bias-corrected, decoupled weight decay) on FP32 weights w
+ * with gradient g / gscale; refreshes the BF16 copy wb (nullable). */
+int maple_nn_adam(float* w, const float* g, float* m, float* v, void* wb, size_t total, float lr, float beta1,
+                  float beta2, float eps, float weight_decay, float gscale, int step, maple_stream_t stream);
+
+int maple_nn_to_bf16(const float* src, void* dst, size_t total, maple_stream_t stream);
+
+/* Network input [B][N][C] BF16 from densities rho [B][N] FP64:
+ * channel 0 = rho^(1/3), channel 1 = rho, others 0. */
+int maple_nn_features(const double* rho, void* out, int B, int N, int C, maple_stream_t stream);
+
+/* Training targets: out[b][v][c0+f] = scale[f] * (u[b][f][v] - mean_v u[b][f][.])
+ * for F fields of a solver layout [B][F][N] (F = R*D).  mean_work [B*F] FP64
+ * (NULL: no mean removal); scale [F] FP64 device (NULL: 1). */
+int maple_nn_fields_to_channels(const double* u, double* mean_work, void* out, int B, int N, int F, int C, int c0,
+                                const double* scale, maple_stream_t stream);
+
+/* Initial iterates: u[b][f][v] = scale[f] * in[b][v][c0+f] (FP32 -> FP64);
+ * scale [F] FP64 device (NULL: 1). */
+int maple_nn_channels_to_fields(const float* in, double* u, int B, int N, int F, int C, int c0, const double* scale,
+                                maple_stream_t stream);
+
+/* Trilinear prolongation of periodic nodal fields [BF][nc^3] -> [BF][(factor*nc)^3]. */
+int maple_nn_prolong_fields(const double* uc, double* uf, int BF, int nc, int factor, maple_stream_t stream);
+
+/* Block average of element densities [B][(factor*nc)^3] -> [B][nc^3]. */
+int maple_nn_restrict_density(const double* rf, double* rc, int B, int nc, int factor, maple_stream_t stream);
 
 /* Instrumentation: when enabled, every fine-level operator launch of this
  * context is bracketed by CUDA events (at most max_launches are kept).

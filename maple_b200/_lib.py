@@ -20,6 +20,8 @@ CELL_CONVERGED, CELL_BREAKDOWN, CELL_MAXIT = 1, 2, 4
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
+_F = C.c_float
+_Z = C.c_size_t
 _IP = C.POINTER(C.c_int)
 _DP = C.POINTER(C.c_double)
 
@@ -50,7 +52,27 @@ SIGNATURES = {
     "maple_profile_enable": (_I, [_P, _I, _I]),
     "maple_profile_read": (_I, [_P, C.c_char_p, _I]),
     "maple_oc_step": (_I, [_P, _P, _P, _P, _D, _D, _D, _D, _I, _I, _D, _I, _I, _P, _P, _P, _P, _P, _P, _IP, _P]),
+    "maple_set_solution": (_I, [_P, _I, _P, _P]),
+    # learned initial guess: convolution network kernels
+    "maple_nn_last_error_string": (C.c_char_p, []),
+    "maple_nn_launch_count": (C.c_ulonglong, []),
+    "maple_nn_conv3d": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
+    "maple_nn_conv3d_wgrad": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
+    "maple_nn_flip_weights": (_I, [_P, _P, _I, _I, _I, _P]),
+    "maple_nn_resample": (_I, [_I, _P, _P, _P, _I, _I, _I, _I, _P]),
+    "maple_nn_accumulate": (_I, [_P, _P, _Z, _I, _P]),
+    "maple_nn_relu_mask": (_I, [_P, _P, _Z, _P]),
+    "maple_nn_mse": (_I, [_P, _P, _P, _P, _Z, _F, _P]),
+    "maple_nn_adam": (_I, [_P, _P, _P, _P, _P, _Z, _F, _F, _F, _F, _F, _F, _I, _P]),
+    "maple_nn_to_bf16": (_I, [_P, _P, _Z, _P]),
+    "maple_nn_features": (_I, [_P, _P, _I, _I, _I, _P]),
+    "maple_nn_fields_to_channels": (_I, [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P]),
+    "maple_nn_channels_to_fields": (_I, [_P, _P, _I, _I, _I, _I, _I, _P, _P]),
+    "maple_nn_prolong_fields": (_I, [_P, _P, _I, _I, _I, _P]),
+    "maple_nn_restrict_density": (_I, [_P, _P, _I, _I, _I, _P]),
 }
+
+NN_POOL, NN_UPSAMPLE, NN_UPSAMPLE_ADJ, NN_POOL_ADJ = 0, 1, 2, 3
 
 _lib = None
 
@@ -89,3 +111,12 @@ def check(status: int) -> None:
 
 def call(name: str, *args) -> None:
     check(getattr(load(), name)(*args))
+
+
+def nn_call(name: str, *args) -> None:
+    """Call a maple_nn_* entry point; raise MapleError with its message."""
+    lib = load()
+    status = getattr(lib, name)(*args)
+    if status != MAPLE_OK:
+        msg = lib.maple_nn_last_error_string()
+        raise MapleError(status, msg.decode() if msg else "")

@@ -39,14 +39,14 @@ class BatchResult:
 
 
 def config2_inputs(B: int = 256, r: int = 32, sigma: float = 2.0, rng_seed: int = 10_000, scale: float = 0.25,
-                   xmin: float = 1e-3):
-    """Seeded designs of the batched benchmark: cell b uses seed b and
+                   xmin: float = 1e-3, seed0: int = 0):
+    """Seeded designs of the batched benchmark: cell b uses seed seed0 + b and
     periodic Gaussian smoothing sigma; vf_b ~ U[0.01, 0.40] and weights ~
     Dirichlet(1,1,1), drawn from default_rng(rng_seed) in that order."""
     rng = np.random.default_rng(rng_seed)
     vf = rng.uniform(0.01, 0.40, B)
     w = rng.dirichlet((1.0, 1.0, 1.0), B)
-    x = np.stack([seeded_design(b, r, sigma, vf[b], scale, xmin).reshape(-1) for b in range(B)])
+    x = np.stack([seeded_design(seed0 + b, r, sigma, vf[b], scale, xmin).reshape(-1) for b in range(B)])
     return x, w, vf
 
 

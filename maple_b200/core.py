@@ -179,6 +179,13 @@ class HomogenizationContext:
             _lib.check(self._lib.maple_get_solution(self._h, ph, _ptr(u), _stream(self.device)))
         return u
 
+    def set_solution(self, physics, u: torch.Tensor):
+        """Initial iterate (B, R, D, N) for the next solve / OC step with warm=True."""
+        ph = PHYSICS[physics]
+        self._check(u, "u", self._vec_shape(ph))
+        with torch.cuda.device(self.device):
+            _lib.check(self._lib.maple_set_solution(self._h, ph, _ptr(u), _stream(self.device)))
+
     def homogenize(self, physics, want_energy=False):
         """Returns H (B,R,R) and, if asked, the per-element energies (B,R,R,N)."""
         ph = PHYSICS[physics]

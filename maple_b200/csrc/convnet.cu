@@ -1,0 +1,646 @@
+// Periodic 3-D convolution network kernels (BF16 storage, FP32 accumulation)
+// for the learned initial guess of the homogenization solves.
+//
+// Activations are channels-last [cell][voxel][channel] BF16 on an n^3
+// periodic grid (voxel id x*n*n + y*n + z).  Convolution weights are
+// [tap][cin][cout] BF16, tap = 9*(dx+1) + 3*(dy+1) + (dz+1) for a 3x3x3
+// kernel (a single tap for 1x1x1).  A convolution is an implicit GEMM on the
+// tensor cores (16x16x16 BF16 fragments, FP32 accumulators): rows are output
+// voxels, columns output channels, and the reduction runs over (tap, input
+// channel) with periodic neighbour gathers (circular padding).
+//
+// Training uses the same kernel for the data gradient (weights flipped and
+// transposed), a tiled weight-gradient GEMM whose reduction runs over
+// (cell, voxel), and elementwise kernels for pooling, upsampling, ReLU, the
+// MSE loss and Adam.  Conversion kernels move solver fields ([B][R][D][N]
+// FP64) to and from network channels.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <mma.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+#include "../../include/maple_b200.h"
+
+namespace maple_nn {
+
+using namespace nvcuda;
+using bf16 = __nv_bfloat16;
+
+static thread_local std::string g_nn_err;
+
+constexpr int BM = 64, BN = 64, BK = 16;
+constexpr int NT = 128;  // 4 warps; warp w owns rows [16w, 16w+16) of the tile
+constexpr int APAD = 8, BPAD = 8, CPAD = 4;
+
+__device__ __forceinline__ int wrapc(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+__device__ __forceinline__ int neighbour(int v, int n, int dx, int dy, int dz) {
+  const int z = v % n, y = (v / n) % n, x = v / (n * n);
+  return (wrapc(x + dx, n) * n + wrapc(y + dy, n)) * n + wrapc(z + dz, n);
+}
+
+__device__ __forceinline__ void tap_offsets(int tap, int taps, int& dx, int& dy, int& dz) {
+  if (taps == 1) {
+    dx = dy = dz = 0;
+  } else {
+    dx = tap / 9 - 1;
+    dy = (tap / 3) % 3 - 1;
+    dz = tap % 3 - 1;
+  }
+}
+
+// out[b][v][co] = act( sum_{tap,ci} in[b][nbr(v,tap)][ci] * W[tap][ci][co] + bias[co] + res[b][v][co] )
+// act = ReLU when relu != 0; BF16 and/or FP32 outputs.
+// res may alias out (gradient accumulation): each element is read, then written, by one thread.
+__global__ void __launch_bounds__(NT) k_conv3d(const bf16* __restrict__ in, const bf16* __restrict__ W,
+                                               const float* __restrict__ bias, const bf16* res, bf16* out,
+                                               float* __restrict__ out_f32, int n, int cin, int cout, int taps,
+                                               int relu) {
+  __shared__ __align__(32) bf16 sA[BM][BK + APAD];
+  __shared__ __align__(32) bf16 sB[BK][BN + BPAD];
+  __shared__ __align__(32) float sC[BM][BN + CPAD];
+  const int N = n * n * n;
+  const int b = blockIdx.z;
+  const int v0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int warp = threadIdx.x >> 5;
+  const bf16* inb = in + (size_t)b * N * cin;
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[BN / 16];
+#pragma unroll
+  for (int j = 0; j < BN / 16; ++j) wmma::fill_fragment(acc[j], 0.0f);
+  const bool vec = (cin % 8) == 0;
+  for (int tap = 0; tap < taps; ++tap) {
+    int dx, dy, dz;
+    tap_offsets(tap, taps, dx, dy, dz);
+    for (int c0 = 0; c0 < cin; c0 += BK) {
+      if (vec) {  // 16-byte gathers: 8 channels of one neighbour voxel
+        for (int t = threadIdx.x; t < BM * (BK / 8); t += NT) {
+          const int m = t / (BK / 8), h = t % (BK / 8);
+          const int v = v0 + m;
+          uint4 val = make_uint4(0, 0, 0, 0);
+          if (v < N && c0 + 8 * h < cin)
+            val = *reinterpret_cast<const uint4*>(inb + (size_t)neighbour(v, n, dx, dy, dz) * cin + c0 + 8 * h);
+          *reinterpret_cast<uint4*>(&sA[m][8 * h]) = val;
+        }
+      } else {
+        for (int t = threadIdx.x; t < BM * BK; t += NT) {
+          const int m = t / BK, k = t % BK;
+          const int v = v0 + m;
+          bf16 val = __float2bfloat16(0.0f);
+          if (v < N && c0 + k < cin) val = inb[(size_t)neighbour(v, n, dx, dy, dz) * cin + c0 + k];
+          sA[m][k] = val;
+        }
+      }
+      for (int t = threadIdx.x; t < BK * BN; t += NT) {
+        const int k = t / BN, j = t % BN;
+        bf16 val = __float2bfloat16(0.0f);
+        if (c0 + k < cin && n0 + j < cout) val = W[((size_t)tap * cin + c0 + k) * cout + n0 + j];
+        sB[k][j] = val;
+      }
+      __syncthreads();
+      wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> fa;
+      wmma::load_matrix_sync(fa, &sA[warp * 16][0], BK + APAD);
+#pragma unroll
+      for (int j = 0; j < BN / 16; ++j) {
+        wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> fb;
+        wmma::load_matrix_sync(fb, &sB[0][16 * j], BN + BPAD);
+        wmma::mma_sync(acc[j], fa, fb, acc[j]);
+      }
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < BN / 16; ++j)
+    wmma::store_matrix_sync(&sC[warp * 16][16 * j], acc[j], BN + CPAD, wmma::mem_row_major);
+  __syncthreads();
+  for (int t = threadIdx.x; t < BM * BN; t += NT) {
+    const int m = t / BN, j = t % BN;
+    const int v = v0 + m, co = n0 + j;
+    if (v >= N || co >= cout) continue;
+    const size_t o = ((size_t)b * N + v) * cout + co;
+    float val = sC[m][j];
+    if (bias) val += bias[co];
+    if (res) val += __bfloat162float(res[o]);
+    if (relu) val = fmaxf(val, 0.0f);
+    if (out) out[o] = __float2bfloat16(val);
+    if (out_f32) out_f32[o] = val;
+  }
+}
+
+// dW[tap][ci][co] += sum_{b,v} in[b][nbr(v,tap)][ci] * dz[b][v][co]  (FP32 atomics)
+// The reduction index kk runs over (b, v) flattened; CTA (x, y, z) owns
+// tap x / (cin tiles), a 64x64 (ci, co) tile and the z-th slice of kk.
+constexpr int WK = 32;
+__global__ void __launch_bounds__(NT) k_conv3d_wgrad(const bf16* __restrict__ in, const bf16* __restrict__ dz,
+                                                     float* __restrict__ dW, int B, int n, int cin, int cout, int taps,
+                                                     long long chunk) {
+  __shared__ __align__(32) bf16 sX[WK][BM + APAD];  // [kk][ci]: A = X^T is col-major
+  __shared__ __align__(32) bf16 sD[WK][BN + BPAD];  // [kk][co]
+  __shared__ __align__(32) float sC[BM][BN + CPAD];
+  const int N = n * n * n;
+  const int mt = (cin + BM - 1) / BM;
+  const int tap = blockIdx.x / mt, c0 = (blockIdx.x % mt) * BM;
+  const int n0 = blockIdx.y * BN;
+  int ox, oy, oz;
+  tap_offsets(tap, taps, ox, oy, oz);
+  const int warp = threadIdx.x >> 5;
+  const long long total = (long long)B * N;
+  const long long kbeg = (long long)blockIdx.z * chunk, kend = kbeg + chunk < total ? kbeg + chunk : total;
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[BN / 16];
+#pragma unroll
+  for (int j = 0; j < BN / 16; ++j) wmma::fill_fragment(acc[j], 0.0f);
+  const bool vec = (cin % 8) == 0;
+  for (long long k0 = kbeg; k0 < kend; k0 += WK) {
+    if (vec) {
+      for (int t = threadIdx.x; t < WK * (BM / 8); t += NT) {
+        const int k = t / (BM / 8), h = t % (BM / 8);
+        const long long kk = k0 + k;
+        uint4 val = make_uint4(0, 0, 0, 0);
+        if (kk < kend && c0 + 8 * h < cin) {
+          const long long b = kk / N;
+          const int v = (int)(kk - b * N);
+          val = *reinterpret_cast<const uint4*>(in + ((size_t)b * N + neighbour(v, n, ox, oy, oz)) * cin + c0 + 8 * h);
+        }
+        *reinterpret_cast<uint4*>(&sX[k][8 * h]) = val;
+      }
+    } else {
+      for (int t = threadIdx.x; t < WK * BM; t += NT) {
+        const int k = t / BM, m = t % BM;
+        const long long kk = k0 + k;
+        bf16 val = __float2bfloat16(0.0f);
+        if (kk < kend && c0 + m < cin) {
+          const long long b = kk / N;
+          const int v = (int)(kk - b * N);
+          val = in[((size_t)b * N + neighbour(v, n, ox, oy, oz)) * cin + c0 + m];
+        }
+        sX[k][m] = val;
+      }
+    }
+    if ((cout % 8) == 0) {
+      for (int t = threadIdx.x; t < WK * (BN / 8); t += NT) {
+        const int k = t / (BN / 8), h = t % (BN / 8);
+        const long long kk = k0 + k;
+        uint4 val = make_uint4(0, 0, 0, 0);
+        if (kk < kend && n0 + 8 * h < cout) val = *reinterpret_cast<const uint4*>(dz + (size_t)kk * cout + n0 + 8 * h);
+        *reinterpret_cast<uint4*>(&sD[k][8 * h]) = val;
+      }
+    } else {
+      for (int t = threadIdx.x; t < WK * BN; t += NT) {
+        const int k = t / BN, j = t % BN;
+        const long long kk = k0 + k;
+        bf16 val = __float2bfloat16(0.0f);
+        if (kk < kend && n0 + j < cout) val = dz[(size_t)kk * cout + n0 + j];
+        sD[k][j] = val;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < WK; ks += 16) {
+      wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::col_major> fa;
+      wmma::load_matrix_sync(fa, &sX[ks][16 * warp], BM + APAD);
+#pragma unroll
+      for (int j = 0; j < BN / 16; ++j) {
+        wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> fb;
+        wmma::load_matrix_sync(fb, &sD[ks][16 * j], BN + BPAD);
+        wmma::mma_sync(acc[j], fa, fb, acc[j]);
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < BN / 16; ++j)
+    wmma::store_matrix_sync(&sC[warp * 16][16 * j], acc[j], BN + CPAD, wmma::mem_row_major);
+  __syncthreads();
+  for (int t = threadIdx.x; t < BM * BN; t += NT) {
+    const int m = t / BN, j = t % BN;
+    if (c0 + m < cin && n0 + j < cout) atomicAdd(&dW[((size_t)tap * cin + c0 + m) * cout + n0 + j], sC[m][j]);
+  }
+}
+
+// db[co] += sum_rows dz[row][co]
+__global__ void k_bias_grad(const bf16* __restrict__ dz, float* __restrict__ db, long long rows, int cout) {
+  const int co = blockIdx.y * 32 + (threadIdx.x & 31);
+  if (co >= cout) return;
+  float s = 0;
+  const int wpb = blockDim.x / 32;
+  for (long long r = (long long)blockIdx.x * wpb + (threadIdx.x >> 5); r < rows; r += (long long)gridDim.x * wpb)
+    s += __bfloat162float(dz[r * cout + co]);
+  atomicAdd(&db[co], s);
+}
+
+// data-gradient weights: Wt[taps-1-tap][co][ci] = W[tap][ci][co]
+__global__ void k_flip_weights(const bf16* __restrict__ W, bf16* __restrict__ Wt, int cin, int cout, int taps) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t total = (size_t)taps * cin * cout;
+  if (i >= total) return;
+  const int co = i % cout, ci = (i / cout) % cin, tap = i / ((size_t)cout * cin);
+  Wt[((size_t)(taps - 1 - tap) * cout + co) * cin + ci] = W[i];
+}
+
+__device__ __forceinline__ size_t fine_of(size_t b, int X, int Y, int Z, int o, int nf) {
+  const int x = 2 * X + (o >> 2), y = 2 * Y + ((o >> 1) & 1), z = 2 * Z + (o & 1);
+  return b * nf * nf * nf + ((size_t)x * nf + y) * nf + z;
+}
+
+// fine -> coarse: w * (sum of the 8 children) [+ c]
+// (w = 1/8: average pooling; w = 1: adjoint of nearest upsampling)
+__global__ void k_fine_to_coarse(const bf16* __restrict__ f, bf16* __restrict__ c, int nc, int C, int B, float w,
+                                 int add) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t Nc = (size_t)nc * nc * nc, total = (size_t)B * Nc * C;
+  if (i >= total) return;
+  const int ch = i % C;
+  const size_t vc = (i / C) % Nc, b = i / (C * Nc);
+  const int Z = vc % nc, Y = (vc / nc) % nc, X = vc / ((size_t)nc * nc);
+  float s = 0;
+#pragma unroll
+  for (int o = 0; o < 8; ++o) s += __bfloat162float(f[fine_of(b, X, Y, Z, o, 2 * nc) * C + ch]);
+  s *= w;
+  if (add) s += __bfloat162float(c[i]);
+  c[i] = __float2bfloat16(s);
+}
+
+// coarse -> fine: w * parent [+ base] [+ f]
+// (w = 1: nearest upsampling, base = skip connection; w = 1/8: adjoint of pooling)
+__global__ void k_coarse_to_fine(const bf16* __restrict__ c, const bf16* __restrict__ base, bf16* __restrict__ f,
+                                 int nc, int C, int B, float w, int add) {
+  const int nf = 2 * nc;
+  const size_t Nf = (size_t)nf * nf * nf, total = (size_t)B * Nf * C;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int ch = i % C;
+  const size_t vf = (i / C) % Nf, b = i / (C * Nf);
+  const int z = vf % nf, y = (vf / nf) % nf, x = vf / ((size_t)nf * nf);
+  float v = w * __bfloat162float(c[((b * nc * nc * nc) + ((size_t)(x >> 1) * nc + (y >> 1)) * nc + (z >> 1)) * C + ch]);
+  if (base) v += __bfloat162float(base[i]);
+  if (add) v += __bfloat162float(f[i]);
+  f[i] = __float2bfloat16(v);
+}
+
+// dst = src (+ dst when add)
+__global__ void k_accumulate(bf16* __restrict__ dst, const bf16* __restrict__ src, size_t total, int add) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  float v = __bfloat162float(src[i]);
+  if (add) v += __bfloat162float(dst[i]);
+  dst[i] = __float2bfloat16(v);
+}
+
+// g <- g * [y > 0]
+__global__ void k_relu_mask(const bf16* __restrict__ y, bf16* __restrict__ g, size_t total) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  if (!(__bfloat162float(y[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
+}
+
+// mean squared error of an FP32 prediction against a BF16 target: loss +=
+// sum (p - t)^2 / total, grad = 2 (p - t) / total * gscale (BF16).
+__global__ void k_mse(const float* __restrict__ pred, const bf16* __restrict__ target, bf16* __restrict__ grad,
+                      float* __restrict__ loss, size_t total, float gscale) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0;
+  if (i < total) {
+    const float d = pred[i] - __bfloat162float(target[i]);
+    if (grad) grad[i] = __float2bfloat16(2.0f * d / (float)total * gscale);
+    l = d * d / (float)total;
+  }
+  for (int off = 16; off > 0; off >>= 1) l += __shfl_down_sync(0xffffffffu, l, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
+}
+
+// Adam on FP32 master weights (bias-corrected, decoupled weight decay),
+// refreshing the BF16 copy; the gradient is divided by gscale first.
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       bf16* __restrict__ wb, size_t total, float lr, float b1, float b2, float eps, float c1, float c2,
+                       float inv_gscale, float wd) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const float gi = g[i] * inv_gscale;
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  float wi = w[i] * (1.0f - lr * wd);
+  wi -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16(wi);
+}
+
+__global__ void k_f32_to_bf16(const float* __restrict__ a, bf16* __restrict__ b, size_t total) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) b[i] = __float2bfloat16(a[i]);
+}
+
+// input features from the element density: ch0 = rho^(1/3), ch1 = rho, rest 0
+__global__ void k_features(const double* __restrict__ rho, bf16* __restrict__ out, size_t total, int C) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const double r = rho[i];
+  bf16* o = out + i * C;
+  o[0] = __float2bfloat16((float)cbrt(r > 0 ? r : 0.0));
+  if (C > 1) o[1] = __float2bfloat16((float)r);
+  for (int c = 2; c < C; ++c) o[c] = __float2bfloat16(0.0f);
+}
+
+// per-(cell, field) mean over the N nodes of an SoA field [B*F][N]
+__global__ void k_field_mean(const double* __restrict__ u, double* __restrict__ mean, int N) {
+  __shared__ double red[32];
+  const double* p = u + (size_t)blockIdx.x * N;
+  double s = 0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s += p[i];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (threadIdx.x == 0) mean[blockIdx.x] = s / N;
+  }
+}
+
+// out[b][v][c0 + f] = scale[f] * (u[b][f][v] - mean[b][f])  for f < F  (BF16)
+__global__ void k_fields_to_channels(const double* __restrict__ u, const double* __restrict__ mean,
+                                     bf16* __restrict__ out, int N, int F, int C, int c0,
+                                     const double* __restrict__ scale, size_t total) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over B*F*N, node fastest
+  if (i >= total) return;
+  const int v = i % N;
+  const size_t bf = i / N;
+  const int f = bf % F;
+  const size_t b = bf / F;
+  const double m = mean ? mean[bf] : 0.0;
+  const double sc = scale ? scale[f] : 1.0;
+  out[(b * N + v) * C + c0 + f] = __float2bfloat16((float)(sc * (u[i] - m)));
+}
+
+// u[b][f][v] = scale[f] * in[b][v][c0 + f]  (FP32 channels -> FP64 field)
+__global__ void k_channels_to_fields(const float* __restrict__ in, double* __restrict__ u, int N, int F, int C, int c0,
+                                     const double* __restrict__ scale, size_t total) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int v = i % N;
+  const size_t bf = i / N;
+  const int f = bf % F;
+  const size_t b = bf / F;
+  u[i] = (scale ? scale[f] : 1.0) * (double)in[(b * N + v) * C + c0 + f];
+}
+
+// trilinear prolongation of periodic nodal fields [BF][nc^3] -> [BF][nf^3],
+// nf = s * nc: fine node j lies at coarse coordinate j / s.
+__global__ void k_prolong_fields(const double* __restrict__ uc, double* __restrict__ uf, int nc, int s, size_t total) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int nf = nc * s;
+  const size_t Nf = (size_t)nf * nf * nf, Nc = (size_t)nc * nc * nc;
+  const size_t bf = i / Nf;
+  const int vf = i % Nf;
+  const int z = vf % nf, y = (vf / nf) % nf, x = vf / (nf * nf);
+  const int X = x / s, Y = y / s, Z = z / s;
+  const double fx = (double)(x - X * s) / s, fy = (double)(y - Y * s) / s, fz = (double)(z - Z * s) / s;
+  const double* c = uc + bf * Nc;
+  double acc = 0;
+#pragma unroll
+  for (int o = 0; o < 8; ++o) {
+    const int ax = o >> 2, ay = (o >> 1) & 1, az = o & 1;
+    const double w = (ax ? fx : 1 - fx) * (ay ? fy : 1 - fy) * (az ? fz : 1 - fz);
+    const int cx = (X + ax) % nc, cy = (Y + ay) % nc, cz = (Z + az) % nc;
+    acc += w * c[((size_t)cx * nc + cy) * nc + cz];
+  }
+  uf[i] = acc;
+}
+
+// periodic average of element densities over s^3 blocks: [B][nf^3] -> [B][nc^3]
+__global__ void k_restrict_density(const double* __restrict__ rf, double* __restrict__ rc, int nc, int s,
+                                   size_t total) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int nf = nc * s;
+  const size_t Nc = (size_t)nc * nc * nc;
+  const size_t b = i / Nc;
+  const int vc = i % Nc;
+  const int Z = vc % nc, Y = (vc / nc) % nc, X = vc / (nc * nc);
+  const double* f = rf + b * (size_t)nf * nf * nf;
+  double acc = 0;
+  for (int a = 0; a < s; ++a)
+    for (int c = 0; c < s; ++c)
+      for (int d = 0; d < s; ++d) acc += f[((size_t)(X * s + a) * nf + (Y * s + c)) * nf + (Z * s + d)];
+  rc[i] = acc / ((double)s * s * s);
+}
+
+static inline unsigned blocks(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+template <typename F>
+static int nn_guard(F&& f) {
+  const char* msg = f();
+  if (msg) {
+    g_nn_err = msg;
+    return MAPLE_E_BADARG;
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_nn_err = std::string("CUDA error: ") + cudaGetErrorString(e);
+    return MAPLE_E_CUDA;
+  }
+  return MAPLE_OK;
+}
+
+static unsigned long long g_nn_launches = 0;
+
+}  // namespace maple_nn
+
+using namespace maple_nn;
+static cudaStream_t Sx(maple_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+#define NNL(launch)  \
+  do {               \
+    launch;          \
+    ++g_nn_launches; \
+  } while (0)
+
+extern "C" {
+
+const char* maple_nn_last_error_string(void) { return g_nn_err.c_str(); }
+unsigned long long maple_nn_launch_count(void) { return g_nn_launches; }
+
+int maple_nn_conv3d(const void* in, const void* W, const float* bias, const void* res, void* out, float* out_f32,
+                    int B, int n, int cin, int cout, int ksize, int relu, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!in || !W || (!out && !out_f32)) return "NULL argument";
+    if (B < 1 || n < 1 || cin < 1 || cout < 1) return "bad sizes";
+    if (ksize != 1 && ksize != 3) return "kernel size must be 1 or 3";
+    if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) != 0) return "input must be 16-byte aligned";
+    const int N = n * n * n;
+    dim3 g((N + BM - 1) / BM, (cout + BN - 1) / BN, B);
+    NNL((k_conv3d<<<g, NT, 0, Sx(s)>>>((const bf16*)in, (const bf16*)W, bias, (const bf16*)res, (bf16*)out, out_f32,
+                                       n, cin, cout, ksize == 3 ? 27 : 1, relu)));
+    return nullptr;
+  });
+}
+
+int maple_nn_conv3d_wgrad(const void* in, const void* dz, float* dW, float* db, int B, int n, int cin, int cout,
+                          int ksize, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!in || !dz || !dW) return "NULL argument";
+    if (B < 1 || n < 1 || cin < 1 || cout < 1) return "bad sizes";
+    if (ksize != 1 && ksize != 3) return "kernel size must be 1 or 3";
+    if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) != 0) return "input must be 16-byte aligned";
+    if ((cout % 8) == 0 && (reinterpret_cast<uintptr_t>(dz) & 15) != 0) return "gradient must be 16-byte aligned";
+    const int N = n * n * n, taps = ksize == 3 ? 27 : 1;
+    const long long total = (long long)B * N;
+    const long long tiles = (long long)taps * ((cin + BM - 1) / BM) * ((cout + BN - 1) / BN);
+    // about 8 CTAs per SM, each reducing at least 1024 (cell, voxel) pairs
+    long long splits = std::max(1LL, std::min((148LL * 8 + tiles - 1) / tiles, total / 1024));
+    long long chunk = (total + splits - 1) / splits;
+    chunk = (chunk + WK - 1) / WK * WK;
+    splits = (total + chunk - 1) / chunk;
+    dim3 g(taps * ((cin + BM - 1) / BM), (cout + BN - 1) / BN, (unsigned)splits);
+    NNL((k_conv3d_wgrad<<<g, NT, 0, Sx(s)>>>((const bf16*)in, (const bf16*)dz, dW, B, n, cin, cout, taps, chunk)));
+    if (db) {
+      dim3 gb((unsigned)std::min<long long>(512, (total + 7) / 8), (cout + 31) / 32);
+      NNL((k_bias_grad<<<gb, 256, 0, Sx(s)>>>((const bf16*)dz, db, total, cout)));
+    }
+    return nullptr;
+  });
+}
+
+int maple_nn_flip_weights(const void* W, void* Wt, int cin, int cout, int ksize, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!W || !Wt) return "NULL argument";
+    if (ksize != 1 && ksize != 3) return "kernel size must be 1 or 3";
+    const int taps = ksize == 3 ? 27 : 1;
+    const size_t total = (size_t)taps * cin * cout;
+    NNL((k_flip_weights<<<blocks(total), 256, 0, Sx(s)>>>((const bf16*)W, (bf16*)Wt, cin, cout, taps)));
+    return nullptr;
+  });
+}
+
+int maple_nn_resample(int op, const void* src, const void* base, void* dst, int B, int nc, int C, int add,
+                      maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!src || !dst) return "NULL argument";
+    if (B < 1 || nc < 1 || C < 1) return "bad sizes";
+    const size_t Nc = (size_t)nc * nc * nc, Nf = Nc * 8;
+    const bf16 *a = (const bf16*)src, *bs = (const bf16*)base;
+    bf16* o = (bf16*)dst;
+    switch (op) {
+      case MAPLE_NN_POOL:
+        NNL((k_fine_to_coarse<<<blocks((size_t)B * Nc * C), 256, 0, Sx(s)>>>(a, o, nc, C, B, 0.125f, add)));
+        break;
+      case MAPLE_NN_UPSAMPLE:
+        NNL((k_coarse_to_fine<<<blocks((size_t)B * Nf * C), 256, 0, Sx(s)>>>(a, bs, o, nc, C, B, 1.0f, add)));
+        break;
+      case MAPLE_NN_UPSAMPLE_ADJ:
+        NNL((k_fine_to_coarse<<<blocks((size_t)B * Nc * C), 256, 0, Sx(s)>>>(a, o, nc, C, B, 1.0f, add)));
+        break;
+      case MAPLE_NN_POOL_ADJ:
+        NNL((k_coarse_to_fine<<<blocks((size_t)B * Nf * C), 256, 0, Sx(s)>>>(a, bs, o, nc, C, B, 0.125f, add)));
+        break;
+      default: return "unknown resample op";
+    }
+    return nullptr;
+  });
+}
+
+int maple_nn_accumulate(void* dst, const void* src, size_t total, int add, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!dst || !src) return "NULL argument";
+    NNL((k_accumulate<<<blocks(total), 256, 0, Sx(s)>>>((bf16*)dst, (const bf16*)src, total, add)));
+    return nullptr;
+  });
+}
+
+int maple_nn_relu_mask(const void* y, void* g, size_t total, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!y || !g) return "NULL argument";
+    NNL((k_relu_mask<<<blocks(total), 256, 0, Sx(s)>>>((const bf16*)y, (bf16*)g, total)));
+    return nullptr;
+  });
+}
+
+int maple_nn_mse(const float* pred, const void* target, void* grad, float* loss, size_t total, float gscale,
+                 maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!pred || !target || !loss) return "NULL argument";
+    NNL((k_mse<<<blocks(total), 256, 0, Sx(s)>>>(pred, (const bf16*)target, (bf16*)grad, loss, total, gscale)));
+    return nullptr;
+  });
+}
+
+int maple_nn_adam(float* w, const float* g, float* m, float* v, void* wb, size_t total, float lr, float b1, float b2,
+                  float eps, float weight_decay, float gscale, int step, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!w || !g || !m || !v) return "NULL argument";
+    if (step < 1) return "step must be >= 1";
+    if (!(gscale > 0)) return "gscale must be > 0";
+    const float c1 = 1.0f - std::pow(b1, (float)step), c2 = 1.0f - std::pow(b2, (float)step);
+    NNL((k_adam<<<blocks(total), 256, 0, Sx(s)>>>(w, g, m, v, (bf16*)wb, total, lr, b1, b2, eps, c1, c2,
+                                                  1.0f / gscale, weight_decay)));
+    return nullptr;
+  });
+}
+
+int maple_nn_to_bf16(const float* src, void* dst, size_t total, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!src || !dst) return "NULL argument";
+    NNL((k_f32_to_bf16<<<blocks(total), 256, 0, Sx(s)>>>(src, (bf16*)dst, total)));
+    return nullptr;
+  });
+}
+
+int maple_nn_features(const double* rho, void* out, int B, int N, int C, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!rho || !out) return "NULL argument";
+    if (B < 1 || N < 1 || C < 1) return "bad sizes";
+    const size_t total = (size_t)B * N;
+    NNL((k_features<<<blocks(total), 256, 0, Sx(s)>>>(rho, (bf16*)out, total, C)));
+    return nullptr;
+  });
+}
+
+int maple_nn_fields_to_channels(const double* u, double* mean_work, void* out, int B, int N, int F, int C, int c0,
+                                const double* scale, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!u || !out) return "NULL argument";
+    if (B < 1 || N < 1 || F < 1 || c0 < 0 || c0 + F > C) return "bad sizes";
+    if (mean_work) NNL((k_field_mean<<<B * F, 256, 0, Sx(s)>>>(u, mean_work, N)));
+    const size_t total = (size_t)B * F * N;
+    NNL((k_fields_to_channels<<<blocks(total), 256, 0, Sx(s)>>>(u, mean_work, (bf16*)out, N, F, C, c0, scale,
+                                                                 total)));
+    return nullptr;
+  });
+}
+
+int maple_nn_channels_to_fields(const float* in, double* u, int B, int N, int F, int C, int c0, const double* scale,
+                                maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!in || !u) return "NULL argument";
+    if (B < 1 || N < 1 || F < 1 || c0 < 0 || c0 + F > C) return "bad sizes";
+    const size_t total = (size_t)B * F * N;
+    NNL((k_channels_to_fields<<<blocks(total), 256, 0, Sx(s)>>>(in, u, N, F, C, c0, scale, total)));
+    return nullptr;
+  });
+}
+
+int maple_nn_prolong_fields(const double* uc, double* uf, int BF, int nc, int factor, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!uc || !uf) return "NULL argument";
+    if (BF < 1 || nc < 1 || factor < 1) return "bad sizes";
+    const size_t nf = (size_t)nc * factor, total = (size_t)BF * nf * nf * nf;
+    NNL((k_prolong_fields<<<blocks(total), 256, 0, Sx(s)>>>(uc, uf, nc, factor, total)));
+    return nullptr;
+  });
+}
+
+int maple_nn_restrict_density(const double* rf, double* rc, int B, int nc, int factor, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!rf || !rc) return "NULL argument";
+    if (B < 1 || nc < 1 || factor < 1) return "bad sizes";
+    const size_t total = (size_t)B * nc * nc * nc;
+    NNL((k_restrict_density<<<blocks(total), 256, 0, Sx(s)>>>(rf, rc, nc, factor, total)));
+    return nullptr;
+  });
+}
+
+}  // extern "C"

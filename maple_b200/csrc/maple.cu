@@ -103,6 +103,7 @@ struct Phys {
   int D = 0, R = 0;
   double kscale = 0, fscale = 0, xscale = 0;  // stiffness, load and X0 scale at resolution r
   bool alloc = false, built = false, solved = false, energies = false;
+  bool current = false;  // the solution belongs to the current density
   int built_prec = -1;
   double* KE[kMaxLevels] = {};   // FP64 element matrices of level l >= 1
   double* S64c = nullptr;        // FP64 coarsest stencil
@@ -432,7 +433,8 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
     power_bounds<float, D>(c, p, p.o32, s);
   p.built = true;
   p.built_prec = prec;
-  p.solved = false;
+  // the current solution (if any) stays: it is the warm start for this density
+  p.current = false;
   p.energies = false;
 }
 
@@ -1188,6 +1190,7 @@ int maple_solve(maple_ctx* c, int phys, int prec, double rtol, int maxit, int wa
     assemble_rhs(c, phys, p.o64.rho, p.F64, S(s));
     dispatch_solve(c, phys, prec, p.F64, p.u64, !(warm && p.solved), rtol, maxit, iters, status, S(s));
     p.solved = true;
+    p.current = true;
     p.energies = false;
   });
 }
@@ -1225,12 +1228,26 @@ int maple_get_solution(maple_ctx* c, int phys, double* u_out, maple_stream_t s) 
   });
 }
 
+int maple_set_solution(maple_ctx* c, int phys, const double* u, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && u != nullptr, "NULL argument");
+    require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
+    Phys& p = c->ph[phys];
+    alloc_phys(c, phys);
+    const size_t vb = (size_t)c->B * nodes(c->n[0]) * p.R * p.D * sizeof(double);
+    CK(cudaMemcpyAsync(p.u64, u, vb, cudaMemcpyDeviceToDevice, S(s)));
+    p.solved = true;
+    p.current = false;
+    p.energies = false;
+  });
+}
+
 int maple_homogenize(maple_ctx* c, int phys, double* H_out, double* energy_out, maple_stream_t s) {
   return guarded([&] {
     require(c != nullptr, "ctx is NULL");
     require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
     Phys& p = c->ph[phys];
-    require(p.solved, "maple_solve must precede maple_homogenize");
+    require(p.current, "maple_solve must follow maple_set_density before maple_homogenize");
     homogenize(c, phys, S(s));
     if (H_out) CK(cudaMemcpyAsync(H_out, p.H, (size_t)c->B * p.R * p.R * sizeof(double), cudaMemcpyDeviceToDevice, S(s)));
     if (energy_out)
@@ -1392,6 +1409,7 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       const bool was_solved = p.solved;
       dispatch_solve(c, phys, prec, p.F64, p.u64, !(warm && was_solved), rtol, maxit, it_tmp.data(), nullptr, st);
       p.solved = true;
+      p.current = true;
       for (int b = 0; b < B; ++b) it_sum[b] += it_tmp[b];
       homogenize(c, phys, st);
     }
