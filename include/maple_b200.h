@@ -227,6 +227,32 @@ int maple_nn_relu_mask(const void* y, void* g, size_t total, maple_stream_t stre
 int maple_nn_mse(const float* pred, const void* target, void* grad, float* loss, size_t total, float gscale,
                  maple_stream_t stream);
 
+/* Node weights w [B][n^3] FP32 of densities rho [B][n^3]: the mean density of
+ * the 8 elements sharing a node over the cell's mean density (mean 1 per cell). */
+int maple_nn_node_weights(const double* rho, float* w, int B, int n, maple_stream_t stream);
+
+/* Weighted, offset-free squared error of pred [B][N][C] FP32 against target
+ * (BF16): e = pred - target - ebar[b][c], ebar = weighted mean of pred - target
+ * per cell and channel (computed into ebar [B][C] FP32; NULL: not removed);
+ * loss += sum w e^2 / (B N C); grad = gscale * d loss / d pred (BF16,
+ * nullable).  w [B][N] (NULL: 1).  C <= 64. */
+int maple_nn_mse_weighted(const float* pred, const void* target, const float* w, float* ebar, void* grad, float* loss,
+                          int B, int N, int C, float gscale, maple_stream_t stream);
+
+/* Energy-norm training loss, in three steps around maple_matvec:
+ * maple_nn_error_fields: e[b][f][v] = scale[f] * (pred - target)[b][v][c0+f]
+ *   as an FP64 solver field [B][F][N] (scale device [F], NULL: 1);
+ * maple_nn_block_dot: out[k] = sum_j a[k*len + j] * b[k*len + j], k < nblocks
+ *   (with len = D*N: the per-(cell, load case) products e_r^T (K e)_r);
+ * maple_nn_energy_grad: grad[b][v][c0 + r*D + d] = coef * scale[r*D+d] *
+ *   y[b][r][d][v] / norm[b][r] (BF16), the gradient of
+ *   coef/2 * sum e_r^T K e_r / norm[b][r] for y = K e. */
+int maple_nn_error_fields(const float* pred, const void* target, const double* scale, double* e, int B, int N, int F,
+                          int C, int c0, maple_stream_t stream);
+int maple_nn_block_dot(const double* a, const double* b, double* out, int nblocks, size_t len, maple_stream_t stream);
+int maple_nn_energy_grad(const double* y, const double* norm, const double* scale, void* grad, int B, int N, int R,
+                         int D, int C, int c0, double coef, maple_stream_t stream);
+
 /* One Adam step (bias-corrected, decoupled weight decay) on FP32 weights w
  * with gradient g / gscale; refreshes the BF16 copy wb (nullable). */
 int maple_nn_adam(float* w, const float* g, float* m, float* v, void* wb, size_t total, float lr, float beta1,

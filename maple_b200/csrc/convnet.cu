@@ -311,6 +311,123 @@ __global__ void k_mse(const float* __restrict__ pred, const bf16* __restrict__ t
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
 }
 
+// Stiffness weights of the nodes of a cell: w[b][v] = (mean of rho over the 8
+// elements sharing node v) / (mean of rho over the cell), so that the weights
+// average to 1 in every cell.  Element e = (x,y,z) has nodes (x+a, y+b, z+c),
+// a,b,c in {0,1}, periodically.  One block per cell.
+__global__ void k_node_weights(const double* __restrict__ rho, float* __restrict__ w, int n) {
+  __shared__ double red[32];
+  const int N = n * n * n;
+  const double* r = rho + (size_t)blockIdx.x * N;
+  double s = 0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s += r[i];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (threadIdx.x == 0) red[0] = s / N;
+  }
+  __syncthreads();
+  const double inv = red[0] > 0 ? 1.0 / red[0] : 0.0;
+  for (int v = threadIdx.x; v < N; v += blockDim.x) {
+    double acc = 0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) acc += r[neighbour(v, n, -(o >> 2), -((o >> 1) & 1), -(o & 1))];
+    w[(size_t)blockIdx.x * N + v] = (float)(0.125 * acc * inv);
+  }
+}
+
+// ebar[b][c] += sum_v w[b][v] * (pred - target)[b][v][c] / N  (weights average to 1)
+// grid (chunks, B); C <= 64 channels
+__global__ void k_weighted_error_mean(const float* __restrict__ pred, const bf16* __restrict__ target,
+                                      const float* __restrict__ w, float* __restrict__ ebar, int N, int C) {
+  __shared__ float acc[64];
+  for (int c = threadIdx.x; c < C; c += blockDim.x) acc[c] = 0.0f;
+  __syncthreads();
+  const size_t b = blockIdx.y, NC = (size_t)N * C;
+  const size_t per = (NC + gridDim.x - 1) / gridDim.x;
+  const size_t beg = blockIdx.x * per, end = beg + per < NC ? beg + per : NC;
+  for (size_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const size_t g = b * NC + i;
+    const float ww = w ? w[b * N + i / C] : 1.0f;
+    atomicAdd(&acc[i % C], ww * (pred[g] - __bfloat162float(target[g])));
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&ebar[b * C + c], acc[c] / N);
+}
+
+// loss += sum w (e - ebar)^2 / total, grad = 2 w (e - ebar) / total * gscale,
+// e = pred - target: the node-weighted squared error with the per-(cell,
+// channel) weighted mean error removed (a constant field is free).
+__global__ void k_mse_weighted(const float* __restrict__ pred, const bf16* __restrict__ target,
+                               const float* __restrict__ w, const float* __restrict__ ebar, bf16* __restrict__ grad,
+                               float* __restrict__ loss, int N, int C, size_t total, float gscale) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0;
+  if (i < total) {
+    const size_t row = i / C;
+    const int c = i % C;
+    const size_t b = row / N;
+    const float ww = w ? w[row] : 1.0f;
+    const float e = pred[i] - __bfloat162float(target[i]) - (ebar ? ebar[b * C + c] : 0.0f);
+    if (grad) grad[i] = __float2bfloat16(2.0f * ww * e / (float)total * gscale);
+    l = ww * e * e / (float)total;
+  }
+  for (int off = 16; off > 0; off >>= 1) l += __shfl_down_sync(0xffffffffu, l, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
+}
+
+// e[b][f][v] = scale[f] * (pred - target)[b][v][c0 + f]: the prediction error of
+// F fields as a solver field [B][F][N] (FP64)
+__global__ void k_error_fields(const float* __restrict__ pred, const bf16* __restrict__ target,
+                               const double* __restrict__ scale, double* __restrict__ e, int N, int F, int C, int c0,
+                               size_t total) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int v = i % N;
+  const size_t bf = i / N;
+  const int f = bf % F;
+  const size_t b = bf / F;
+  const size_t o = (b * N + v) * C + c0 + f;
+  e[i] = (scale ? scale[f] : 1.0) * (double)(pred[o] - __bfloat162float(target[o]));
+}
+
+// out[k] = sum_j a[k][j] * b[k][j] over blocks of L contiguous doubles (one CTA per block)
+__global__ void k_block_dot(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out,
+                            size_t L) {
+  __shared__ double red[32];
+  const double* pa = a + blockIdx.x * L;
+  const double* pb = b + blockIdx.x * L;
+  double s = 0;
+  for (size_t i = threadIdx.x; i < L; i += blockDim.x) s += pa[i] * pb[i];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (threadIdx.x == 0) out[blockIdx.x] = s;
+  }
+}
+
+// grad[b][v][c0 + r*D + d] = coef * scale[r*D + d] * y[b][r][d][v] / norm[b][r]  (BF16):
+// the gradient of sum_{b,r} e_r^T K e_r / norm[b][r] with y = K e, through e = scale * channels
+__global__ void k_energy_grad(const double* __restrict__ y, const double* __restrict__ norm,
+                              const double* __restrict__ scale, bf16* __restrict__ grad, int N, int R, int D, int C,
+                              int c0, double coef, size_t total) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over B*R*D*N, node fastest
+  if (i >= total) return;
+  const int v = i % N;
+  const size_t bf = i / N;
+  const int f = bf % (R * D);
+  const size_t b = bf / (R * D);
+  const int r = f / D;
+  const double g = coef * (scale ? scale[f] : 1.0) * y[i] / norm[b * R + r];
+  grad[(b * N + v) * C + c0 + f] = __float2bfloat16((float)g);
+}
+
 // Adam on FP32 master weights (bias-corrected, decoupled weight decay),
 // refreshing the BF16 copy; the gradient is divided by gscale first.
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
@@ -459,6 +576,12 @@ static cudaStream_t Sx(maple_stream_t s) { return reinterpret_cast<cudaStream_t>
     ++g_nn_launches; \
   } while (0)
 
+#define CKN(call)                                    \
+  do {                                               \
+    const cudaError_t e_ = (call);                   \
+    if (e_ != cudaSuccess) return cudaGetErrorString(e_); \
+  } while (0)
+
 extern "C" {
 
 const char* maple_nn_last_error_string(void) { return g_nn_err.c_str(); }
@@ -564,6 +687,63 @@ int maple_nn_mse(const float* pred, const void* target, void* grad, float* loss,
   return nn_guard([&]() -> const char* {
     if (!pred || !target || !loss) return "NULL argument";
     NNL((k_mse<<<blocks(total), 256, 0, Sx(s)>>>(pred, (const bf16*)target, (bf16*)grad, loss, total, gscale)));
+    return nullptr;
+  });
+}
+
+int maple_nn_node_weights(const double* rho, float* w, int B, int n, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!rho || !w) return "NULL argument";
+    if (B < 1 || n < 1) return "bad sizes";
+    NNL((k_node_weights<<<B, 512, 0, Sx(s)>>>(rho, w, n)));
+    return nullptr;
+  });
+}
+
+int maple_nn_mse_weighted(const float* pred, const void* target, const float* w, float* ebar, void* grad, float* loss,
+                          int B, int N, int C, float gscale, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!pred || !target || !loss) return "NULL argument";
+    if (B < 1 || N < 1 || C < 1 || C > 64) return "bad sizes (1 <= C <= 64)";
+    if (ebar) {
+      CKN(cudaMemsetAsync(ebar, 0, sizeof(float) * B * C, Sx(s)));
+      const unsigned chunks = (unsigned)std::max<size_t>(1, std::min<size_t>(256, ((size_t)N * C) / 8192));
+      NNL((k_weighted_error_mean<<<dim3(chunks, B), 256, 0, Sx(s)>>>(pred, (const bf16*)target, w, ebar, N, C)));
+    }
+    const size_t total = (size_t)B * N * C;
+    NNL((k_mse_weighted<<<blocks(total), 256, 0, Sx(s)>>>(pred, (const bf16*)target, w, ebar, (bf16*)grad, loss, N, C,
+                                                         total, gscale)));
+    return nullptr;
+  });
+}
+
+int maple_nn_error_fields(const float* pred, const void* target, const double* scale, double* e, int B, int N, int F,
+                          int C, int c0, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!pred || !target || !e) return "NULL argument";
+    if (B < 1 || N < 1 || F < 1 || c0 < 0 || c0 + F > C) return "bad sizes";
+    const size_t total = (size_t)B * F * N;
+    NNL((k_error_fields<<<blocks(total), 256, 0, Sx(s)>>>(pred, (const bf16*)target, scale, e, N, F, C, c0, total)));
+    return nullptr;
+  });
+}
+
+int maple_nn_block_dot(const double* a, const double* b, double* out, int nblocks, size_t len, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!a || !b || !out) return "NULL argument";
+    if (nblocks < 1 || len < 1) return "bad sizes";
+    NNL((k_block_dot<<<nblocks, 256, 0, Sx(s)>>>(a, b, out, len)));
+    return nullptr;
+  });
+}
+
+int maple_nn_energy_grad(const double* y, const double* norm, const double* scale, void* grad, int B, int N, int R,
+                         int D, int C, int c0, double coef, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!y || !norm || !grad) return "NULL argument";
+    if (B < 1 || N < 1 || R < 1 || D < 1 || c0 < 0 || c0 + R * D > C) return "bad sizes";
+    const size_t total = (size_t)B * R * D * N;
+    NNL((k_energy_grad<<<blocks(total), 256, 0, Sx(s)>>>(y, norm, scale, (bf16*)grad, N, R, D, C, c0, coef, total)));
     return nullptr;
   });
 }

@@ -13,7 +13,17 @@ Everything that computes runs in ``libmaple_b200.so``: BF16 tensor-core
 convolutions with FP32 accumulation (forward, data gradient, weight gradient),
 pooling / upsampling and their adjoints, ReLU masks, the MSE loss and Adam on
 FP32 master weights.  Training data are generated by the library's own solver.
-torch only allocates buffers and shuffles indices.
+torch allocates buffers, shuffles indices and computes the data set's
+per-field normalisation once.
+
+The training loss is the energy norm of the prediction error relative to the
+energy of the solution, per cell and load case: e_r^T K(rho) e_r / u_r^T K u_r,
+with K applied by the library's FP64 fine-level operator (maple_matvec).  That
+is the quantity that decides how many PCG iterations remain; it ignores what
+the solver ignores (a constant field, i.e. the periodic rigid translation, and
+errors in near-void regions) and weighs the strain of the error, not its
+long-range drift.  The per-field normalisation of the outputs is the RMS of the
+solutions weighted by the local stiffness (maple_nn_node_weights).
 
 Network (widths (32, 64, 96, 128), about 2.2M parameters):
   level l < 3: two 3x3x3 conv + ReLU, 2x2x2 average pool to level l+1
@@ -133,8 +143,10 @@ class WarmStartNet:
         self.step = 0
         # per-field scale: network output * scale = fluctuation field
         self.scale = torch.ones(OUT, dtype=torch.float64, device=dev)
-        self.loss = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=dev)  # written by the MSE kernels
+        self.last_loss = self.loss
         self._buf = {}
+        self._fe = {}  # batch size -> context applying K(rho) for the energy loss
         self._act = {}
         self.init_weights(seed)
 
@@ -218,6 +230,24 @@ class WarmStartNet:
     def free_buffers(self):
         self._buf.clear()
         self._act = {}
+        for ctx in self._fe.values():
+            ctx.close()
+        self._fe.clear()
+
+    def _t64(self, tag: str, shape):
+        key = (tag, shape)
+        t = self._buf.get(key)
+        if t is None:
+            t = torch.empty(shape, dtype=torch.float64, device=self.device)
+            self._buf[key] = t
+        return t
+
+    def _fe_ctx(self, B: int) -> HomogenizationContext:
+        ctx = self._fe.get(B)
+        if ctx is None:
+            ctx = HomogenizationContext(self.r, ncells=B, device=self.device)
+            self._fe[B] = ctx
+        return ctx
 
     # ------------------------------------------------------------------ primitives
     def _conv(self, L: ConvSpec, x, out, B, n, out_f32=None):
@@ -339,12 +369,25 @@ class WarmStartNet:
                 self._conv_back(self.by_name[f"enc{lv}a"], act[f"pool{lv}"], ga, gp, B, n)
 
     def mse(self, out: torch.Tensor, target: torch.Tensor, gscale: float = 1024.0):
-        """Loss into self.loss (device scalar) and its BF16 gradient x gscale."""
+        """Plain mean squared error into self.loss (device scalar) and its BF16
+        gradient x gscale."""
         B = out.shape[0]
         gout = self._t("g_out", B, self.r, OUT)
         self.loss.zero_()
         _lib.nn_call("maple_nn_mse", _ptr(out), _ptr(target), _ptr(gout), _ptr(self.loss), out.numel(),
                      float(gscale), _stream(self.device))
+        return gout
+
+    def weighted_loss(self, out: torch.Tensor, target: torch.Tensor, w: torch.Tensor, gscale: float = 1024.0,
+                      grad: bool = True):
+        """Node-weighted, offset-free squared error (see the module docstring)
+        into self.loss and, if grad, its BF16 gradient x gscale."""
+        B = out.shape[0]
+        gout = self._t("g_out", B, self.r, OUT) if grad else None
+        ebar = self._t("ebar", B, 1, OUT, torch.float32)
+        self.loss.zero_()
+        _lib.nn_call("maple_nn_mse_weighted", _ptr(out), _ptr(target), _ptr(w), _ptr(ebar), _ptr(gout),
+                     _ptr(self.loss), B, self.r ** 3, OUT, float(gscale), _stream(self.device))
         return gout
 
     def adam(self, lr: float, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0, gscale: float = 1024.0):
@@ -354,14 +397,56 @@ class WarmStartNet:
                      _stream(self.device))
         self._refresh()
 
-    def train_step(self, rho: torch.Tensor, target: torch.Tensor, lr: float, gscale: float = 1024.0):
-        """One Adam step on a batch: rho (B, N) float64, target (B, N, 21) BF16."""
+    def energy_loss(self, out: torch.Tensor, target: torch.Tensor, rho: torch.Tensor, energy: torch.Tensor,
+                    gscale: float = 1024.0, grad: bool = True, per_cell: bool = False):
+        """Relative energy error of the predicted fields, e = scale * (out -
+        target): the mean over cells and the 9 load cases of e_r^T K(rho) e_r
+        divided by the solution energy -- of that cell (per_cell) or the batch
+        mean of the load case (default; cells of tiny energy, i.e. nearly void
+        cells, then cannot dominate the gradient).  Returns (per-(cell, load
+        case) values (B, 9), BF16 gradient x gscale w.r.t. out or None);
+        self.last_loss holds the mean."""
+        B, N = rho.shape
+        if not per_cell:
+            energy = energy.mean(dim=0, keepdim=True).expand(B, 9)
+        s = _stream(self.device)
+        ctx = self._fe_ctx(B)
+        sc_th = C.c_void_p(self.scale.data_ptr() + OUT_ELASTIC * 8)
+        e_el = self._t64("e_el", (B, 6, 3, N))
+        e_th = self._t64("e_th", (B, 3, 1, N))
+        _lib.nn_call("maple_nn_error_fields", _ptr(out), _ptr(target), _ptr(self.scale), _ptr(e_el), B, N,
+                     OUT_ELASTIC, OUT, 0, s)
+        _lib.nn_call("maple_nn_error_fields", _ptr(out), _ptr(target), sc_th, _ptr(e_th), B, N, OUT_THERMAL, OUT,
+                     OUT_ELASTIC, s)
+        y_el = ctx.matvec("elastic", rho, e_el)
+        y_th = ctx.matvec("thermal", rho, e_th)
+        d = self._t64("edot", (B, 9))
+        d_el, d_th = self._t64("edot_el", (B, 6)), self._t64("edot_th", (B, 3))
+        _lib.nn_call("maple_nn_block_dot", _ptr(e_el), _ptr(y_el), _ptr(d_el), B * 6, 3 * N, s)
+        _lib.nn_call("maple_nn_block_dot", _ptr(e_th), _ptr(y_th), _ptr(d_th), B * 3, N, s)
+        E_el, E_th = energy[:, :6].contiguous(), energy[:, 6:].contiguous()
+        gout = None
+        if grad:
+            gout = self._t("g_out", B, self.r, OUT)
+            coef = 2.0 * gscale / (9.0 * B)
+            _lib.nn_call("maple_nn_energy_grad", _ptr(y_el), _ptr(E_el), _ptr(self.scale), _ptr(gout), B, N, 6, 3,
+                         OUT, 0, coef, s)
+            _lib.nn_call("maple_nn_energy_grad", _ptr(y_th), _ptr(E_th), sc_th, _ptr(gout), B, N, 3, 1, OUT,
+                         OUT_ELASTIC, coef, s)
+        torch.cat([d_el / E_el, d_th / E_th], dim=1, out=d)
+        self.last_loss = d.mean()
+        return d, gout
+
+    def train_step(self, rho: torch.Tensor, target: torch.Tensor, energy: torch.Tensor, lr: float,
+                   gscale: float = 1024.0):
+        """One Adam step on a batch: rho (B, N) float64, target (B, N, 21) BF16,
+        solution energies (B, 9) float64."""
         self.grad.zero_()
         out = self.forward(self.features(rho))
-        gout = self.mse(out, target, gscale)
+        _, gout = self.energy_loss(out, target, rho, energy, gscale)
         self.backward(gout)
         self.adam(lr, gscale=gscale)
-        return self.loss
+        return self.last_loss
 
     # ------------------------------------------------------------------ inference
     def predict(self, rho: torch.Tensor):
@@ -389,6 +474,7 @@ class WarmStartNet:
 class SolveSet:
     rho: torch.Tensor        # (S, N) float64 element densities
     target: torch.Tensor     # (S, N, 21) BF16 normalised, mean-free fields
+    energy: torch.Tensor     # (S, 9) float64 u_r^T K u_r per load case (6 elastic, 3 thermal)
     scale: torch.Tensor      # (21,) float64: field = scale * channel
     iters: np.ndarray        # (S, 2) PCG iterations from the zero guess (elastic, thermal)
     seconds: float = 0.0
@@ -408,10 +494,12 @@ def design_densities(n: int, r: int, seed0: int, sigma: Optional[float] = None, 
     return simp(x, penal, rho_min)
 
 
-def _field_scale(u: torch.Tensor) -> torch.Tensor:
-    """Per-field RMS over cells and nodes of mean-free fields (B, F, N)."""
-    d = u - u.mean(dim=2, keepdim=True)
-    return d.pow(2).mean(dim=(0, 2)).sqrt().clamp_min(1e-30)
+def _field_scale(u: torch.Tensor, w: torch.Tensor) -> torch.Tensor:
+    """Per-field weighted RMS over cells and nodes of fields (B, F, N) with
+    their weighted means removed; w (B, N) averages to 1 per cell."""
+    wd = w.double()[:, None, :]
+    d = u - (wd * u).mean(dim=2, keepdim=True)
+    return (wd * d.pow(2)).mean(dim=(0, 2)).sqrt().clamp_min(1e-30)
 
 
 def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, precision: str = "mixed",
@@ -426,6 +514,8 @@ def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, prec
     N = r ** 3
     rho_all = torch.empty((n, N), dtype=torch.float64, device=dev)
     target = torch.empty((n, N, OUT), dtype=torch.bfloat16, device=dev)
+    energy = torch.empty((n, 9), dtype=torch.float64, device=dev)
+    wb = torch.empty((batch, N), dtype=torch.float32, device=dev)
     iters = np.zeros((n, 2), dtype=np.int64)
     mean_work = torch.empty(batch * OUT_ELASTIC, dtype=torch.float64, device=dev)
     inv = None
@@ -443,13 +533,21 @@ def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, prec
             iters[start:start + b, k] = info.iters[:b]
             fields.append(ctx.solution(phys))
         ue, ut = fields
+        s = _stream(dev)
+        en = torch.empty((batch, 9), dtype=torch.float64, device=dev)
+        for u, phys, R, D, c0 in ((ue, "elastic", 6, 3, 0), (ut, "thermal", 3, 1, 6)):
+            y = ctx.matvec(phys, rho, u)
+            dots = torch.empty((batch, R), dtype=torch.float64, device=dev)
+            _lib.nn_call("maple_nn_block_dot", _ptr(u), _ptr(y), _ptr(dots), batch * R, D * N, s)
+            en[:, c0:c0 + R] = dots
+        energy[start:start + b] = en[:b]
         if inv is None:
             if scale is None:
-                scale = torch.cat([_field_scale(ue[:b].reshape(b, OUT_ELASTIC, N)),
-                                   _field_scale(ut[:b].reshape(b, OUT_THERMAL, N))])
+                _lib.nn_call("maple_nn_node_weights", _ptr(rho), _ptr(wb), batch, r, s)
+                scale = torch.cat([_field_scale(ue[:b].reshape(b, OUT_ELASTIC, N), wb[:b]),
+                                   _field_scale(ut[:b].reshape(b, OUT_THERMAL, N), wb[:b])])
             inv = (1.0 / scale).contiguous()
         tgt = target[start:start + b]
-        s = _stream(dev)
         _lib.nn_call("maple_nn_fields_to_channels", _ptr(ue), _ptr(mean_work), _ptr(tgt), b, N, OUT_ELASTIC, OUT, 0,
                      _ptr(inv), s)
         _lib.nn_call("maple_nn_fields_to_channels", _ptr(ut), _ptr(mean_work), _ptr(tgt), b, N, OUT_THERMAL, OUT,
@@ -459,10 +557,10 @@ def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, prec
             print(f"  solves {start + b}/{n}  {time.perf_counter() - t0:.1f}s", flush=True)
     ctx.set_active(None)
     torch.cuda.synchronize(dev)
-    return SolveSet(rho_all, target, scale, iters, time.perf_counter() - t0)
+    return SolveSet(rho_all, target, energy, scale, iters, time.perf_counter() - t0)
 
 
-def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: float = 2e-3, lr_min: float = 5e-5,
+def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: float = 5e-4, lr_min: float = 2e-5,
           warmup: int = 50, seed: int = 0, log_every: int = 0, time_limit: Optional[float] = None):
     """Adam with linear warm-up and cosine decay over `steps` mini-batches
     drawn without replacement (reshuffled every epoch).  Returns the loss
@@ -483,12 +581,13 @@ def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: fl
         pos += batch
         rho = data.rho.index_select(0, idx)
         tgt = data.target.index_select(0, idx)
+        en = data.energy.index_select(0, idx)
         if it < warmup:
             lr_t = lr * (it + 1) / warmup
         else:
             c = (it - warmup) / max(1, steps - warmup)
             lr_t = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * c))
-        loss = net.train_step(rho, tgt, lr_t)
+        loss = net.train_step(rho, tgt, en, lr_t)
         last = it == steps - 1 or (time_limit is not None and time.perf_counter() - t0 > time_limit)
         if (log_every and (it + 1) % log_every == 0) or last:
             hist.append((it + 1, float(loss.item())))
@@ -498,14 +597,15 @@ def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: fl
 
 
 def validation_loss(net: WarmStartNet, data: SolveSet, chunk: int = 32) -> float:
-    """Mean-square error of the normalised prediction over a solve set."""
+    """Training loss (relative energy error) of the prediction over a solve set."""
     tot, cnt = 0.0, 0
     for i in range(0, data.rho.shape[0], chunk):
         rho = data.rho[i:i + chunk].contiguous()
         out = net.forward(net.features(rho))
-        net.mse(out, data.target[i:i + chunk].contiguous())
+        net.energy_loss(out, data.target[i:i + chunk].contiguous(), rho, data.energy[i:i + chunk].contiguous(),
+                        grad=False)
         b = rho.shape[0]
-        tot += float(net.loss.item()) * b
+        tot += float(net.last_loss.item()) * b
         cnt += b
     return tot / max(cnt, 1)
 
@@ -538,6 +638,8 @@ def evaluate(net: WarmStartNet, rho: torch.Tensor, precision: str = "mixed", rto
     dev = net.device
     ctx = ctx or HomogenizationContext(net.r, ncells=B, device=dev)
     res = {}
+    converged = {}
+    guess = {}
     for _ in range(max(1, repeats)):
         for mode in ("zero", "learned"):
             its = np.zeros((B, 2), dtype=np.int64)
@@ -550,12 +652,92 @@ def evaluate(net: WarmStartNet, rho: torch.Tensor, precision: str = "mixed", rto
                 ue, ut = net.predict(rho)
                 ctx.set_solution("elastic", ue)
                 ctx.set_solution("thermal", ut)
+                guess = {"elastic": ue, "thermal": ut}
             e1.record()
             for k, phys in enumerate(("elastic", "thermal")):
                 info = ctx.solve(phys, precision, rtol=rtol, maxit=maxit, warm=(mode == "learned"))
                 its[:, k] = info.iters
+                if mode == "zero":
+                    converged[phys] = ctx.solution(phys)
             e2.record()
             torch.cuda.synchronize(dev)
             res[mode] = (its, e0.elapsed_time(e2), e0.elapsed_time(e1))
+    # energy-norm error of the network's guess relative to the converged solution
+    rel = []
+    s = _stream(dev)
+    for phys, R, D in (("elastic", 6, 3), ("thermal", 3, 1)):
+        u = converged[phys]
+        e = (guess[phys] - u).contiguous()
+        dots = torch.empty((2, B * R), dtype=torch.float64, device=dev)
+        for k, v in enumerate((e, u)):
+            y = ctx.matvec(phys, rho, v)
+            _lib.nn_call("maple_nn_block_dot", _ptr(v), _ptr(y), _ptr(dots[k]), B * R, D * N, s)
+        rel.append(float((dots[0] / dots[1]).mean()))
     return WarmStartReport(B, res["zero"][0], res["learned"][0], res["zero"][1], res["learned"][1],
-                           res["learned"][2])
+                           res["learned"][2], {"guess_energy_error": rel})
+
+
+def forward_tflops(net: WarmStartNet, rho: torch.Tensor, repeats: int = 10) -> dict:
+    """Device time of the network's forward pass on rho (B, N) and the
+    achieved BF16 tensor-core rate (2 x multiply-adds / time)."""
+    x = net.features(rho)
+    for _ in range(2):
+        net.forward(x)
+    torch.cuda.synchronize(net.device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(repeats):
+        net.forward(x)
+    e1.record()
+    torch.cuda.synchronize(net.device)
+    ms = e0.elapsed_time(e1) / repeats
+    flops = net.flops_per_cell() * rho.shape[0]
+    return {"cells": int(rho.shape[0]), "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+
+
+def main(argv=None):
+    """Learned-guess experiment: solver-generated training set (seeds
+    100,000+), training on the GPU, evaluation on held-out cells (seeds
+    200,000+) against the zero guess.  Prints one JSON object."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--res", type=int, default=32)
+    ap.add_argument("--samples", type=int, default=20_000)
+    ap.add_argument("--heldout", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--lr", type=float, default=5e-4)
+    ap.add_argument("--train-seconds", type=float, default=None)
+    ap.add_argument("--precision", default="mixed")
+    ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--save", default=None, help="write the trained weights (.npz)")
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t0 = time.perf_counter()
+    data = generate_solves(a.samples, a.res, seed0=100_000, precision=a.precision, rtol=a.rtol, device=dev)
+    held = generate_solves(a.heldout, a.res, seed0=200_000, precision=a.precision, rtol=a.rtol, device=dev,
+                           scale=data.scale)
+    t_gen = time.perf_counter() - t0
+    net = WarmStartNet(a.res, device=dev)
+    t1 = time.perf_counter()
+    hist = train(net, data, a.steps, batch=a.batch, lr=a.lr, log_every=max(1, a.steps // 20),
+                 time_limit=a.train_seconds)
+    torch.cuda.synchronize(dev)
+    t_train = time.perf_counter() - t1
+    val = validation_loss(net, held)
+    ctx = HomogenizationContext(a.res, ncells=held.rho.shape[0], device=dev)
+    rep = evaluate(net, held.rho, precision=a.precision, rtol=a.rtol, ctx=ctx, repeats=2)
+    speed = forward_tflops(net, held.rho[:min(64, held.rho.shape[0])].contiguous())
+    if a.save:
+        net.save(a.save)
+    out = {"res": a.res, "params": net.n_params, "samples": a.samples, "generation_s": round(t_gen, 1),
+           "solve_iters_train_mean": [float(v) for v in data.iters.mean(0)], "train_steps": hist[-1][0],
+           "batch": a.batch, "train_s": round(t_train, 1), "loss_history": hist, "heldout_energy_error": val,
+           "forward": speed, **rep.summary()}
+    print(json.dumps(out))
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -45,31 +45,41 @@ def conv3d_periodic(x, W, b=None):
     return F.conv3d(F.pad(x, (1, 1, 1, 1, 1, 1), mode="circular"), w, b)
 
 
-def unet_forward(params, x, r, widths, round_bf16=False):
+def unet_forward(params, x, r, widths, round_bf16=False, acts=None):
     """params: name -> (W [taps][cin][cout], b [cout]) FP32 tensors (names as
     the library: enc{l}a/b, mid_a/b, up{l}, dec{l}a/b, head).  x: (B, r^3, C)
-    input features.  Returns (B, r^3, 21) FP32."""
+    input features.  Returns (B, r^3, 21) FP32.  If `acts` is a dict, every
+    stored activation is kept there (NCDHW) under the library's buffer name
+    (enc{l}a/b, pool{l}, mid_a/b, up{l}, skip{l}, dec{l}a/b)."""
     L = len(widths)
     h = _to_ncdhw(x, r)
+    keep = acts if acts is not None else {}
 
     def conv(name, inp, relu):
         W, b = params[name]
         y = conv3d_periodic(inp, W, b)
         return F.relu(y) if relu else y
 
+    def store(name, t):
+        t = _bf16(t, round_bf16)
+        if acts is not None:
+            t.retain_grad() if t.requires_grad else None
+        keep[name] = t
+        return t
+
     skips = []
     for lv in range(L - 1):
-        a = _bf16(conv(f"enc{lv}a", h, True), round_bf16)
-        bb = _bf16(conv(f"enc{lv}b", a, True), round_bf16)
+        a = store(f"enc{lv}a", conv(f"enc{lv}a", h, True))
+        bb = store(f"enc{lv}b", conv(f"enc{lv}b", a, True))
         skips.append(bb)
-        h = _bf16(F.avg_pool3d(bb, 2), round_bf16)
-    h = _bf16(conv("mid_a", h, True), round_bf16)
-    h = _bf16(conv("mid_b", h, True), round_bf16)
+        h = store(f"pool{lv + 1}", F.avg_pool3d(bb, 2))
+    h = store("mid_a", conv("mid_a", h, True))
+    h = store("mid_b", conv("mid_b", h, True))
     for lv in reversed(range(L - 1)):
-        c = _bf16(conv(f"up{lv}", h, False), round_bf16)
-        d = _bf16(F.interpolate(c, scale_factor=2, mode="nearest") + skips[lv], round_bf16)
-        a = _bf16(conv(f"dec{lv}a", d, True), round_bf16)
-        h = _bf16(conv(f"dec{lv}b", a, True), round_bf16)
+        c = store(f"up{lv}", conv(f"up{lv}", h, False))
+        d = store(f"skip{lv}", F.interpolate(c, scale_factor=2, mode="nearest") + skips[lv])
+        a = store(f"dec{lv}a", conv(f"dec{lv}a", d, True))
+        h = store(f"dec{lv}b", conv(f"dec{lv}b", a, True))
     out = conv("head", h, False)
     return _to_nvc(out)
 
@@ -84,11 +94,12 @@ def features(rho, C=8):
     return x
 
 
-def mse_and_grads(params, x, target, r, widths, round_bf16=False):
+def mse_and_grads(params, x, target, r, widths, round_bf16=False, acts=None):
     """Loss mean((out - target)^2), the output, and the gradients w.r.t.
-    every parameter."""
+    every parameter (and, with `acts`, w.r.t. every stored activation in
+    acts[name].grad)."""
     leaves = {k: (W.clone().requires_grad_(True), b.clone().requires_grad_(True)) for k, (W, b) in params.items()}
-    out = unet_forward(leaves, x, r, widths, round_bf16)
+    out = unet_forward(leaves, x, r, widths, round_bf16, acts)
     loss = (out - target).pow(2).mean()
     loss.backward()
-    return float(loss), out.detach(), {k: (W.grad, b.grad) for k, (W, b) in leaves.items()}
+    return float(loss.detach()), out.detach(), {k: (W.grad, b.grad) for k, (W, b) in leaves.items()}
