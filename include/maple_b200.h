@@ -253,6 +253,9 @@ int maple_nn_block_dot(const double* a, const double* b, double* out, int nblock
 int maple_nn_energy_grad(const double* y, const double* norm, const double* scale, void* grad, int B, int N, int R,
                          int D, int C, int c0, double coef, maple_stream_t stream);
 
+/* *out = sum of g[i]^2 over n FP32 values (FP64 result, device). */
+int maple_nn_sumsq(const float* g, size_t n, double* out, maple_stream_t stream);
+
 /* One Adam step (bias-corrected, decoupled weight decay) on FP32 weights w
  * with gradient g / gscale; refreshes the BF16 copy wb (nullable). */
 int maple_nn_adam(float* w, const float* g, float* m, float* v, void* wb, size_t total, float lr, float beta1,

@@ -68,6 +68,7 @@ SIGNATURES = {
     "maple_nn_error_fields": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
     "maple_nn_block_dot": (_I, [_P, _P, _P, _I, _Z, _P]),
     "maple_nn_energy_grad": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _D, _P]),
+    "maple_nn_sumsq": (_I, [_P, _Z, _P, _P]),
     "maple_nn_adam": (_I, [_P, _P, _P, _P, _P, _Z, _F, _F, _F, _F, _F, _F, _I, _P]),
     "maple_nn_to_bf16": (_I, [_P, _P, _Z, _P]),
     "maple_nn_features": (_I, [_P, _P, _I, _I, _I, _P]),

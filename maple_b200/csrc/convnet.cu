@@ -428,6 +428,22 @@ __global__ void k_energy_grad(const double* __restrict__ y, const double* __rest
   grad[(b * N + v) * C + c0 + f] = __float2bfloat16((float)g);
 }
 
+// out += sum g^2 (FP64 accumulation across blocks)
+__global__ void k_sumsq(const float* __restrict__ g, size_t n, double* __restrict__ out) {
+  __shared__ double red[32];
+  double s = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    s += (double)g[i] * g[i];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+  }
+}
+
 // Adam on FP32 master weights (bias-corrected, decoupled weight decay),
 // refreshing the BF16 copy; the gradient is divided by gscale first.
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
@@ -744,6 +760,16 @@ int maple_nn_energy_grad(const double* y, const double* norm, const double* scal
     if (B < 1 || N < 1 || R < 1 || D < 1 || c0 < 0 || c0 + R * D > C) return "bad sizes";
     const size_t total = (size_t)B * R * D * N;
     NNL((k_energy_grad<<<blocks(total), 256, 0, Sx(s)>>>(y, norm, scale, (bf16*)grad, N, R, D, C, c0, coef, total)));
+    return nullptr;
+  });
+}
+
+int maple_nn_sumsq(const float* g, size_t n, double* out, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!g || !out) return "NULL argument";
+    CKN(cudaMemsetAsync(out, 0, sizeof(double), Sx(s)));
+    const unsigned nb = (unsigned)std::max<size_t>(1, std::min<size_t>(1184, (n + 255) / 256));
+    NNL((k_sumsq<<<nb, 256, 0, Sx(s)>>>(g, n, out)));
     return nullptr;
   });
 }

@@ -87,7 +87,7 @@ static void ensure_tables(double nu) {
 // ---------------------------------------------------------------------------
 template <typename T>
 struct Ops {
-  bool alloc = false;
+  bool alloc = false, vectors = false;  // density copy / solver vectors allocated
   T* rho = nullptr;                      // fine densities [B][N0]
   T* S[kMaxLevels] = {};                 // stencils (1 <= l < L-1)
   T* Dinv[kMaxLevels] = {};
@@ -222,11 +222,14 @@ static int nodes(int n) { return n * n * n; }
 
 template <typename T>
 static void alloc_ops(maple_ctx* c, Phys& p, Ops<T>& o, bool vectors) {
-  if (o.alloc) return;
   const int B = c->B, RD = p.R * p.D, DD = p.D * p.D;
   const size_t N0 = nodes(c->n[0]);
-  o.rho = dnew<T>(c, (size_t)B * N0);
-  if (vectors) {
+  if (!o.alloc) o.rho = dnew<T>(c, (size_t)B * N0);
+  o.alloc = true;
+  // the FP64 operator of a mixed-precision solve needs only the density copy;
+  // its solver vectors are added when the same context is first used in FP64
+  if (vectors && !o.vectors) {
+    o.vectors = true;
     for (int l = 0; l < c->L; ++l) {
       const size_t Nl = nodes(c->n[l]);
       if (l >= 1 && l < c->L - 1) {
@@ -245,7 +248,6 @@ static void alloc_ops(maple_ctx* c, Phys& p, Ops<T>& o, bool vectors) {
     o.p = dnew<T>(c, (size_t)B * N0 * RD);
     o.q = dnew<T>(c, (size_t)B * N0 * RD);
   }
-  o.alloc = true;
 }
 
 static void alloc_phys(maple_ctx* c, int phys) {

@@ -151,13 +151,14 @@ class WarmStartNet:
         self.init_weights(seed)
 
     # ------------------------------------------------------------------ weights
-    def init_weights(self, seed: int = 0):
+    def init_weights(self, seed: int = 0, head_std: float = 0.1):
         """He-normal weights (std sqrt(2/fan_in) before a ReLU, sqrt(1/fan_in)
-        otherwise; the head 0.1 of that), zero biases; deterministic in seed."""
+        otherwise; the head head_std of that), zero biases; deterministic in
+        seed."""
         g = torch.Generator().manual_seed(seed)
         w = torch.zeros(self.size, dtype=torch.float32)
         for L in self.layers:
-            std = math.sqrt((2.0 if L.relu else 1.0) / L.fan_in) * (0.1 if L.name == "head" else 1.0)
+            std = math.sqrt((2.0 if L.relu else 1.0) / L.fan_in) * (head_std if L.name == "head" else 1.0)
             vals = torch.randn(L.taps, L.cin, L.cout, generator=g) * std
             if L.name == "enc0a":
                 vals[:, USED_FEATURES:, :] = 0.0
@@ -390,6 +391,12 @@ class WarmStartNet:
                      _ptr(self.loss), B, self.r ** 3, OUT, float(gscale), _stream(self.device))
         return gout
 
+    def grad_norm(self, gscale: float = 1.0) -> float:
+        """Euclidean norm of the accumulated gradient (divided by gscale)."""
+        out = self._t64("sumsq", (1,))
+        _lib.nn_call("maple_nn_sumsq", _ptr(self.grad), self.size, _ptr(out), _stream(self.device))
+        return math.sqrt(float(out.item())) / gscale
+
     def adam(self, lr: float, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0, gscale: float = 1024.0):
         self.step += 1
         _lib.nn_call("maple_nn_adam", _ptr(self.w32), _ptr(self.grad), _ptr(self.m), _ptr(self.v), None, self.size,
@@ -401,14 +408,14 @@ class WarmStartNet:
                     gscale: float = 1024.0, grad: bool = True, per_cell: bool = False):
         """Relative energy error of the predicted fields, e = scale * (out -
         target): the mean over cells and the 9 load cases of e_r^T K(rho) e_r
-        divided by the solution energy -- of that cell (per_cell) or the batch
-        mean of the load case (default; cells of tiny energy, i.e. nearly void
-        cells, then cannot dominate the gradient).  Returns (per-(cell, load
-        case) values (B, 9), BF16 gradient x gscale w.r.t. out or None);
-        self.last_loss holds the mean."""
+        divided by the solution energy of that cell (per_cell), or by that
+        energy plus the batch mean of the load case (default: every term stays
+        bounded, so nearly void cells of tiny energy cannot dominate the
+        gradient).  Returns (per-(cell, load case) values (B, 9), BF16
+        gradient x gscale w.r.t. out or None); self.last_loss holds the mean."""
         B, N = rho.shape
         if not per_cell:
-            energy = energy.mean(dim=0, keepdim=True).expand(B, 9)
+            energy = energy + energy.mean(dim=0, keepdim=True)
         s = _stream(self.device)
         ctx = self._fe_ctx(B)
         sc_th = C.c_void_p(self.scale.data_ptr() + OUT_ELASTIC * 8)
@@ -438,14 +445,20 @@ class WarmStartNet:
         return d, gout
 
     def train_step(self, rho: torch.Tensor, target: torch.Tensor, energy: torch.Tensor, lr: float,
-                   gscale: float = 1024.0):
+                   gscale: float = 1024.0, clip: Optional[float] = None):
         """One Adam step on a batch: rho (B, N) float64, target (B, N, 21) BF16,
-        solution energies (B, 9) float64."""
+        solution energies (B, 9) float64.  The gradient is rescaled to norm
+        `clip` when it is larger (None: no clipping)."""
         self.grad.zero_()
         out = self.forward(self.features(rho))
         _, gout = self.energy_loss(out, target, rho, energy, gscale)
         self.backward(gout)
-        self.adam(lr, gscale=gscale)
+        scale = gscale
+        if clip is not None:
+            gn = self.grad_norm(gscale)
+            if gn > clip:
+                scale = gscale * gn / clip
+        self.adam(lr, gscale=scale)
         return self.last_loss
 
     # ------------------------------------------------------------------ inference
@@ -478,6 +491,7 @@ class SolveSet:
     scale: torch.Tensor      # (21,) float64: field = scale * channel
     iters: np.ndarray        # (S, 2) PCG iterations from the zero guess (elastic, thermal)
     seconds: float = 0.0
+    generated: int = 0       # cells solved (before dropping unconverged ones)
 
 
 def simp(x: np.ndarray, penal: float = 3.0, rho_min: float = 1e-9) -> np.ndarray:
@@ -505,9 +519,10 @@ def _field_scale(u: torch.Tensor, w: torch.Tensor) -> torch.Tensor:
 def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, precision: str = "mixed",
                     rtol: float = 1e-8, maxit: int = 500, sigma: Optional[float] = None, device=None,
                     ctx: Optional[HomogenizationContext] = None, scale: Optional[torch.Tensor] = None,
-                    verbose: bool = False) -> SolveSet:
+                    verbose: bool = False, keep_unconverged: bool = False) -> SolveSet:
     """Solve n seeded cells with the library's MG-PCG (zero initial guess) and
-    keep their normalised, mean-free fields as training targets."""
+    keep their normalised, mean-free fields as training targets; cells whose
+    solves did not converge within maxit are dropped unless keep_unconverged."""
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     batch = min(batch, n)
     ctx = ctx or HomogenizationContext(r, ncells=batch, device=dev)
@@ -515,6 +530,7 @@ def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, prec
     rho_all = torch.empty((n, N), dtype=torch.float64, device=dev)
     target = torch.empty((n, N, OUT), dtype=torch.bfloat16, device=dev)
     energy = torch.empty((n, 9), dtype=torch.float64, device=dev)
+    ok = np.ones(n, dtype=bool)
     wb = torch.empty((batch, N), dtype=torch.float32, device=dev)
     iters = np.zeros((n, 2), dtype=np.int64)
     mean_work = torch.empty(batch * OUT_ELASTIC, dtype=torch.float64, device=dev)
@@ -531,6 +547,7 @@ def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, prec
             ctx.set_density(phys, rho, precision)
             info = ctx.solve(phys, precision, rtol=rtol, maxit=maxit, warm=False)
             iters[start:start + b, k] = info.iters[:b]
+            ok[start:start + b] &= (info.status[:b] & _lib.CELL_CONVERGED) != 0
             fields.append(ctx.solution(phys))
         ue, ut = fields
         s = _stream(dev)
@@ -556,12 +573,19 @@ def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, prec
         if verbose:
             print(f"  solves {start + b}/{n}  {time.perf_counter() - t0:.1f}s", flush=True)
     ctx.set_active(None)
+    if keep_unconverged or ok.all():
+        return SolveSet(rho_all, target, energy, scale, iters, time.perf_counter() - t0, n)
+    # cells whose solve stopped at maxit carry no usable target
+    keep = torch.as_tensor(np.nonzero(ok)[0], device=dev)
+    out = SolveSet(rho_all.index_select(0, keep), target.index_select(0, keep), energy.index_select(0, keep), scale,
+                   iters[ok], time.perf_counter() - t0, n)
     torch.cuda.synchronize(dev)
-    return SolveSet(rho_all, target, energy, scale, iters, time.perf_counter() - t0)
+    return out
 
 
-def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: float = 5e-4, lr_min: float = 2e-5,
-          warmup: int = 50, seed: int = 0, log_every: int = 0, time_limit: Optional[float] = None):
+def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: float = 1e-3, lr_min: float = 2e-5,
+          warmup: int = 50, seed: int = 0, log_every: int = 0, time_limit: Optional[float] = None,
+          clip: Optional[float] = None):
     """Adam with linear warm-up and cosine decay over `steps` mini-batches
     drawn without replacement (reshuffled every epoch).  Returns the loss
     history [(step, loss)] read every log_every steps and at the end."""
@@ -587,7 +611,7 @@ def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: fl
         else:
             c = (it - warmup) / max(1, steps - warmup)
             lr_t = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * c))
-        loss = net.train_step(rho, tgt, en, lr_t)
+        loss = net.train_step(rho, tgt, en, lr_t, clip=clip)
         last = it == steps - 1 or (time_limit is not None and time.perf_counter() - t0 > time_limit)
         if (log_every and (it + 1) % log_every == 0) or last:
             hist.append((it + 1, float(loss.item())))
@@ -707,7 +731,7 @@ def main(argv=None):
     ap.add_argument("--heldout", type=int, default=256)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--steps", type=int, default=4000)
-    ap.add_argument("--lr", type=float, default=5e-4)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--train-seconds", type=float, default=None)
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--rtol", type=float, default=1e-8)
@@ -731,7 +755,8 @@ def main(argv=None):
     speed = forward_tflops(net, held.rho[:min(64, held.rho.shape[0])].contiguous())
     if a.save:
         net.save(a.save)
-    out = {"res": a.res, "params": net.n_params, "samples": a.samples, "generation_s": round(t_gen, 1),
+    out = {"res": a.res, "params": net.n_params, "samples": a.samples, "samples_converged": int(data.rho.shape[0]),
+           "heldout_converged": int(held.rho.shape[0]), "generation_s": round(t_gen, 1),
            "solve_iters_train_mean": [float(v) for v in data.iters.mean(0)], "train_steps": hist[-1][0],
            "batch": a.batch, "train_s": round(t_train, 1), "loss_history": hist, "heldout_energy_error": val,
            "forward": speed, **rep.summary()}

@@ -432,15 +432,15 @@ def test_trained_network_gain_over_zero_guess(lib):
     to the same tolerance."""
     from maple_b200.learned import WarmStartNet, evaluate, generate_solves, train, validation_loss
     r = 16
-    data = generate_solves(192, r, seed0=100_000, batch=96, precision="mixed", rtol=1e-8, device=DEV)
+    data = generate_solves(256, r, seed0=100_000, batch=128, precision="mixed", rtol=1e-8, device=DEV)
     held = generate_solves(32, r, seed0=200_000, batch=32, precision="mixed", rtol=1e-8, device=DEV, scale=data.scale)
     net = WarmStartNet(r, device=DEV, seed=0)
     net.scale.copy_(data.scale)
     before = validation_loss(net, held)
-    train(net, data, steps=400, batch=16, log_every=100)
+    train(net, data, steps=600, batch=16, log_every=100)
     after = validation_loss(net, held)
-    assert after < 0.5 * min(before, 1.0), (before, after)
+    assert after < 0.5 * before, (before, after)
     rep = evaluate(net, held.rho, precision="mixed", rtol=1e-8)
     s = rep.summary()
-    assert max(s["guess_energy_error"]) < 0.6, s
-    assert rep.iters_learned.sum() <= 1.02 * rep.iters_zero.sum(), s
+    assert max(s["guess_energy_error"]) < 0.5, s
+    assert rep.iters_learned.sum() <= rep.iters_zero.sum(), s

@@ -250,3 +250,24 @@ def test_graph_replay_matches_eager(lib, precision):
     for (i0, h0), (i1, h1) in zip(out[0], out[1]):
         assert i0 == i1
         assert np.array_equal(h0, h1)
+
+
+def test_precision_switch_on_one_context(lib):
+    """A context used first in mixed precision and then in FP64 (and back)
+    gives the results of contexts used in one precision only."""
+    from maple_b200.core import HomogenizationContext
+    r = 16
+    rho = T(simp(O.seed_density(3, r, 2.0, 0.25)).reshape(1, -1))
+    ref = {}
+    for prec in ("fp64", "mixed"):
+        c = HomogenizationContext(r, ncells=1)
+        c.set_density("elastic", rho, prec)
+        c.solve("elastic", prec, rtol=1e-12, maxit=300)
+        ref[prec] = c.homogenize("elastic").cpu().numpy()
+        c.close()
+    c = HomogenizationContext(r, ncells=1)
+    for prec in ("mixed", "fp64", "mixed"):
+        c.set_density("elastic", rho, prec)
+        c.solve("elastic", prec, rtol=1e-12, maxit=300)
+        assert rel(c.homogenize("elastic").cpu().numpy(), ref[prec]) < 1e-11, prec
+    c.close()
