@@ -125,6 +125,20 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
+TRAFFIC_FILE = "profiles/k_apply_fine_64cube_full.md"
+
+
+def measured_traffic(kernel, res):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    capture, which was taken on the 64^3 workload; None otherwise."""
+    import re
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), TRAFFIC_FILE)
+    if res != 64 or not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch\[" + re.escape(kernel) + r"\] = (\d+)", open(path).read())
+    return int(m.group(1)) if m else None
+
+
 def run_maple(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -202,10 +216,12 @@ def run_maple(args, rank, world, local_rank):
         achieved = top["bytes_per_launch"] / avg_s / 1e9
         roofline = {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": peak,
                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                    "traffic": None, "avg_launch_us": round(avg_s * 1e6, 2), "launches_per_step":
-                        top["launches"] / args.steps, "bytes_per_launch": top["bytes_per_launch"],
-                    "share_of_fine_operator_time": round(top["total_ms"] / sum(v["total_ms"] for v in prof.values()),
-                                                         3)}
+                    "traffic": measured_traffic(top_name, args.res), "avg_launch_us": round(avg_s * 1e6, 2),
+                    "launches_per_step": top["launches"] / args.steps, "bytes_per_launch": top["bytes_per_launch"],
+                    "share_of_step_kernel_time": round(top["total_ms"] / sum(v["total_ms"] for v in prof.values()),
+                                                       3)}
+        if roofline["traffic"] is not None:
+            roofline["traffic_source"] = TRAFFIC_FILE
 
     # end to end through the public API with host buffers
     e2e = None
