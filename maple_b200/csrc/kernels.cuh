@@ -423,8 +423,16 @@ static_assert(kFineThreads % 32 == 0 && TZ * 4 == 32, "a warp spans tz 0..7 x ty
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 __host__ __device__ inline int fine_tiles(int n) { return ceil_div(n, TX) * ceil_div(n, TY) * ceil_div(n, TZ); }
 
+// CTAs per SM the register allocation must allow: 8 for the FP32 elastic
+// operator (64 registers, no spills; the default allocation leaves 7), 4 for
+// its FP64 form, 8 or 12 for the small ones (their default allocation).
+template <typename T, int RD>
+constexpr int fine_min_blocks() {
+  return RD == 18 ? (sizeof(T) == 4 ? 8 : 4) : (RD == 3 && sizeof(T) == 8 ? 8 : 12);
+}
+
 template <typename T, int D, int R, int MODE>
-__global__ void __launch_bounds__(kFineThreads) k_apply_fine(ApplyArgs<T> a) {
+__global__ void __launch_bounds__(kFineThreads, fine_min_blocks<T, R * D>()) k_apply_fine(ApplyArgs<T> a) {
   using G = FineTile<T, R * D>;
   constexpr int RD = R * D;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -724,46 +732,64 @@ __global__ void __launch_bounds__(CT_NODES * 6) k_apply_stencil_tile(ApplyArgs<T
   }
 }
 
-// power iteration step on a coarse level: w = Dinv A u and the Rayleigh terms
+// power iteration step on a coarse level: w = Dinv A u and the Rayleigh terms.
+// One thread per (node, row i): a CTA covers kPowerNodes<D> nodes, rows
+// i-major so that consecutive threads read consecutive stencil entries; the
+// D row sums meet in shared memory for the Dinv product.
+template <int D>
+constexpr int kPowerNodes = D == 1 ? 256 : 64;
+
 template <typename T, int D>
-__global__ void __launch_bounds__(kThreads) k_apply_stencil_power(ApplyArgs<T> a) {
+__global__ void __launch_bounds__(D * kPowerNodes<D>) k_apply_stencil_power(ApplyArgs<T> a) {
+  constexpr int NB = kPowerNodes<D>;
+  __shared__ T sacc[D][NB];
   const int b = blockIdx.y;
   if (a.active && !a.active[b]) return;
   const int n = a.n, N = a.N;
   const size_t NN = (size_t)N;
-  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  const int i = threadIdx.x / NB, ln = threadIdx.x - i * NB;
+  const int idx = blockIdx.x * NB + ln;
   const bool valid = idx < N;
   const int id = valid ? idx : 0;
   const int z = id % n, y = (id / n) % n, x = id / (n * n);
   const size_t cell = (size_t)b * N;
-  T acc[D];
-#pragma unroll
-  for (int i = 0; i < D; ++i) acc[i] = T(0);
   const T* __restrict__ S = a.S + (size_t)b * 27 * D * D * N + id;
   const int xs[3] = {wrapn(x - 1, n), x, wrapn(x + 1, n)};
   const int ys[3] = {wrapn(y - 1, n), y, wrapn(y + 1, n)};
   const int zs[3] = {wrapn(z - 1, n), z, wrapn(z + 1, n)};
   const T* __restrict__ ub = a.u + cell * D;
+  T acc = T(0);
+#pragma unroll 9
   for (int o = 0; o < 27; ++o) {
     const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
     const int nb = (xs[ox] * n + ys[oy]) * n + zs[oz];
-    for (int i = 0; i < D; ++i)
-      for (int j = 0; j < D; ++j) acc[i] += __ldg(S + ((size_t)o * D * D + i * D + j) * N) * __ldg(ub + j * NN + nb);
+#pragma unroll
+    for (int j = 0; j < D; ++j) acc += __ldg(S + ((size_t)o * D * D + i * D + j) * N) * __ldg(ub + j * NN + nb);
   }
+  sacc[i][ln] = acc;
+  __syncthreads();
   double dots[2] = {0, 0};
   if (valid) {
     const size_t vo = cell * D + id;
-    for (int i = 0; i < D; ++i) {
-      T w = 0;
-      for (int j = 0; j < D; ++j) w += __ldg(a.Dinv + (size_t)b * D * D * N + (size_t)(i * D + j) * N + id) * acc[j];
-      a.out[vo + i * NN] = w;
-      dots[0] += (double)a.u[vo + i * NN] * (double)acc[i];
-      for (int j = 0; j < D; ++j)
-        dots[1] += (double)a.u[vo + i * NN] * (double)__ldg(S + ((size_t)13 * D * D + i * D + j) * N) *
-                   (double)a.u[vo + j * NN];
+    T w = 0;
+    double diag = 0;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      w += __ldg(a.Dinv + (size_t)b * D * D * N + (size_t)(i * D + j) * N + id) * sacc[j][ln];
+      diag += (double)__ldg(S + ((size_t)13 * D * D + i * D + j) * N) * (double)a.u[vo + j * NN];
     }
+    a.out[vo + i * NN] = w;
+    const double ui = (double)a.u[vo + i * NN];
+    dots[0] = ui * (double)acc;
+    dots[1] = ui * diag;
   }
-  block_sum_store<2>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
+  block_sum_store<2, D * NB / 32>(dots, a.part + ((size_t)b * gridDim.x + blockIdx.x) * 2);
+}
+
+template <typename T>
+__global__ void k_fill(T* __restrict__ p, size_t n, T v) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
 }
 
 // ----------------------------------------------------------------------------
@@ -1055,16 +1081,26 @@ __global__ void k_chol_inverse(double* __restrict__ A, double* __restrict__ work
 // regularised matrix held in shared memory (one block of 1024 threads per
 // cell).  L^-1 goes through `work` in global memory (each thread owns columns).
 constexpr int kCholSmemMax = 192;
-__host__ __device__ constexpr size_t chol_smem_bytes(int ndof) { return (size_t)ndof * (ndof + 1) / 2 * sizeof(double); }
+constexpr int kCholThreads = 1024;
+// packed lower triangle of L, the current column and one solve vector per warp
+__host__ __device__ constexpr size_t chol_smem_bytes(int ndof) {
+  return ((size_t)ndof * (ndof + 1) / 2 + (size_t)(kCholThreads / 32 + 1) * ndof) * sizeof(double);
+}
 
-__global__ void __launch_bounds__(1024) k_chol_inverse_smem(double* __restrict__ A, double* __restrict__ work,
-                                                            int ndof, int D, const int* active, int* status) {
+// A <- (A + reg * I_blocks)^-1 for one cell per CTA, A symmetric positive
+// (semi-)definite of order ndof <= kCholSmemMax: Cholesky factor L in shared
+// memory, then column j of the inverse by the forward solve L y = e_j and the
+// backward solve L^T x = y, one warp per column.  A zero or negative pivot
+// sets status[b] (nullable) and continues with a tiny pivot.
+__global__ void __launch_bounds__(kCholThreads) k_chol_inverse_smem(double* __restrict__ A, int ndof, int D,
+                                                                    const int* active, int* status) {
   const int b = blockIdx.x;
   if (active && !active[b]) return;
   extern __shared__ double Lp[];  // packed lower triangle, row i starts at i(i+1)/2
   double* M = A + (size_t)b * ndof * ndof;
-  double* Li = work + (size_t)b * ndof * ndof;
   const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+  double* colk = Lp + (size_t)ndof * (ndof + 1) / 2;  // column k of L below the pivot
+  double* yv = colk + ndof + (size_t)warp * ndof;
   __shared__ double s_alpha;
   if (warp == 0) {
     double t = 0;
@@ -1080,43 +1116,54 @@ __global__ void __launch_bounds__(1024) k_chol_inverse_smem(double* __restrict__
   __syncthreads();
   for (int k = 0; k < ndof; ++k) {
     const size_t kk = (size_t)k * (k + 1) / 2 + k;
-    if (tid == 0) {
-      double d = Lp[kk];
-      if (!(d > 0)) {
-        if (status) status[b] = 1;
-        d = 1e-300;
-      }
-      Lp[kk] = sqrt(d);
+    // every thread forms the pivot from the same value; column k is scaled
+    // into place and into the contiguous copy read by the trailing update
+    double d = Lp[kk];
+    if (!(d > 0)) {
+      if (status && tid == 0) status[b] = 1;
+      d = 1e-300;
+    }
+    const double piv = sqrt(d);
+    for (int i = k + 1 + tid; i < ndof; i += nth) {
+      const size_t e = (size_t)i * (i + 1) / 2 + k;
+      const double v = Lp[e] / piv;
+      Lp[e] = v;
+      colk[i] = v;
     }
     __syncthreads();
-    const double piv = Lp[kk];
-    for (int i = k + 1 + tid; i < ndof; i += nth) Lp[(size_t)i * (i + 1) / 2 + k] /= piv;
-    __syncthreads();
+    if (tid == 0) Lp[kk] = piv;
     for (int i = k + 1 + warp; i < ndof; i += nw) {
       const size_t ri = (size_t)i * (i + 1) / 2;
-      const double lik = Lp[ri + k];
-      for (int j = k + 1 + lane; j <= i; j += 32) Lp[ri + j] -= lik * Lp[(size_t)j * (j + 1) / 2 + k];
+      const double lik = colk[i];
+      for (int j = k + 1 + lane; j <= i; j += 32) Lp[ri + j] -= lik * colk[j];
     }
     __syncthreads();
   }
-  // Li = L^-1 column by column (thread j owns column j)
-  for (int j = tid; j < ndof; j += nth) {
-    for (int i = 0; i < j; ++i) Li[(size_t)i * ndof + j] = 0.0;
+  for (int j = warp; j < ndof; j += nw) {
+    // forward: y_i = (delta_ij - sum_{p=j}^{i-1} L_ip y_p) / L_ii for i >= j
     for (int i = j; i < ndof; ++i) {
       const size_t ri = (size_t)i * (i + 1) / 2;
-      double sacc = (i == j) ? 1.0 : 0.0;
-      for (int p = j; p < i; ++p) sacc -= Lp[ri + p] * Li[(size_t)p * ndof + j];
-      Li[(size_t)i * ndof + j] = sacc / Lp[ri + i];
+      double t = 0;
+      for (int q = j + lane; q < i; q += 32) t += Lp[ri + q] * yv[q];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+      if (lane == 0) yv[i] = ((i == j ? 1.0 : 0.0) - t) / Lp[ri + i];
+      __syncwarp();
     }
-  }
-  __syncthreads();
-  // A^-1 = Li^T Li
-  for (int t = tid; t < ndof * ndof; t += nth) {
-    const int i = t / ndof, j = t % ndof;
-    const int p0 = i > j ? i : j;
-    double sacc = 0;
-    for (int p = p0; p < ndof; ++p) sacc += Li[(size_t)p * ndof + i] * Li[(size_t)p * ndof + j];
-    M[t] = sacc;
+    for (int i = lane; i < j; i += 32) yv[i] = 0.0;
+    __syncwarp();
+    // backward: x_q = y_q / L_qq, then y_i -= L_qi x_q for i < q (row q of L is contiguous)
+    for (int q = ndof - 1; q >= 0; --q) {
+      const size_t rq = (size_t)q * (q + 1) / 2;
+      const double xq = yv[q] / Lp[rq + q];
+      __syncwarp();
+      if (lane == 0) yv[q] = xq;
+      for (int i = lane; i < q; i += 32) yv[i] -= Lp[rq + i] * xq;
+      __syncwarp();
+    }
+    // column j of the symmetric inverse, stored as row j
+    for (int i = lane; i < ndof; i += 32) M[(size_t)j * ndof + i] = yv[i];
+    __syncwarp();
   }
 }
 

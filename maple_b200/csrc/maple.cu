@@ -317,7 +317,8 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
     prof_begin(c, s);
     if constexpr (MODE == M_POWER) {
       static_assert(R == 1, "power iterations run on one column");
-      k_apply_stencil_power<T, D><<<g, kThreads, 0, s>>>(a);
+      k_apply_stencil_power<T, D>
+          <<<dim3(ceil_div(a.N, kPowerNodes<D>), c->B), D * kPowerNodes<D>, 0, s>>>(a);
     } else {
       require(a.part == nullptr, "coarse-level applies produce no partial sums");
       if (a.n % CT == 0) {
@@ -355,9 +356,7 @@ static void reduce(maple_ctx* c, const double* part, unsigned nb, double* out, c
 template <typename T, int D>
 static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
   // level 0: the element bound holds for every density
-  std::vector<double> h0(c->B, g_tab.lam_elem[D == 3 ? 0 : 1]);
-  CK(cudaMemcpyAsync(o.hi[0], h0.data(), c->B * sizeof(double), cudaMemcpyHostToDevice, s));
-  CK(cudaStreamSynchronize(s));
+  KL(c, s, k_fill<double><<<nblk(c->B), kThreads, 0, s>>>(o.hi[0], c->B, g_tab.lam_elem[D == 3 ? 0 : 1]));
   for (int l = 1; l < c->L - 1; ++l) {
     const int Nl = nodes(c->n[l]);
     T* v = o.U[l][0];
@@ -371,7 +370,7 @@ static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
       apply<T, D, 1, M_POWER>(c, p, o, l, a, c->active, s);
       std::swap(v, w);
     }
-    reduce<2>(c, c->part, nblk(Nl), c->red, s);
+    reduce<2>(c, c->part, ceil_div(Nl, kPowerNodes<D>), c->red, s);
     KL(c, s, k_power_finish<<<nblk(c->B), kThreads, 0, s>>>(c->red, o.hi[l], c->B, c->power_safety));
   }
 }
@@ -423,7 +422,7 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
       if (ndof <= kCholSmemMax) {
         const size_t sm = chol_smem_bytes(ndof);
         CK(cudaFuncSetAttribute(k_chol_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        KL(c, s, k_chol_inverse_smem<<<B, 1024, sm, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr));
+        KL(c, s, k_chol_inverse_smem<<<B, kCholThreads, sm, s>>>(p.Ainv, ndof, D, act, nullptr));
       } else {
         KL(c, s, k_chol_inverse<<<B, 512, 0, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr));
       }
