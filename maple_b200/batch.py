@@ -69,8 +69,12 @@ def seeded_design(seed, r, sigma, vf, scale=0.25, xmin=1e-3):
 def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, xmin: float = 1e-3,
            penal: float = 3.0, rho_min: float = 1e-9, filter_k: int = 3, precision: str = "mixed",
            rtol: float = 1e-8, maxit: int = 500, dx_tol: float = 0.01, max_iters: int = 200,
-           ctx: Optional[HomogenizationContext] = None, device=None, record: bool = False) -> BatchResult:
-    """Run B independent OC loops to their own stopping points."""
+           ctx: Optional[HomogenizationContext] = None, device=None, record: bool = False,
+           guess=None) -> BatchResult:
+    """Run B independent OC loops to their own stopping points.  `guess` =
+    (elastic (B, 6, 3, N), thermal (B, 3, 1, N)) float64 fields: the initial
+    iterates of the first iteration's solves (later iterations start from the
+    previous iteration's solutions)."""
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     x = torch.as_tensor(x0, dtype=torch.float64).to(dev).reshape(len(volfrac), -1).contiguous()
     B, N = x.shape
@@ -80,6 +84,9 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
     w = torch.as_tensor(np.asarray(weights), dtype=torch.float64).to(dev).reshape(B, 3).contiguous()
     vf = torch.as_tensor(np.asarray(volfrac), dtype=torch.float64).to(dev).reshape(B).contiguous()
     ctx = ctx or HomogenizationContext(r, ncells=B, device=dev)
+    if guess is not None:
+        ctx.set_solution("elastic", guess[0].contiguous())
+        ctx.set_solution("thermal", guess[1].contiguous())
     active = np.ones(B, dtype=np.int32)
     iters = np.zeros(B, dtype=np.int64)
     pcg = np.zeros(B, dtype=np.int64)
@@ -107,7 +114,7 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
         conv |= done
         active[done] = 0
         if record:
-            hist.append(dict(active=int(act.sum()), J=J.copy(), dx_max=st[:, 0].copy()))
+            hist.append(dict(active=int(act.sum()), J=J.copy(), dx_max=st[:, 0].copy(), pcg=np.array(out["iters"])))
     torch.cuda.synchronize(dev)
     return BatchResult(x=x, J=J, terms=terms, iters_run=iters, converged=conv, pcg_iters=pcg,
                        seconds=time.perf_counter() - t0, history=hist)

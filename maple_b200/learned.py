@@ -475,6 +475,28 @@ class WarmStartNet:
                      C.c_void_p(self.scale.data_ptr() + OUT_ELASTIC * 8), s)
         return ue, ut
 
+    def predict_prolonged(self, rho: torch.Tensor, r: int):
+        """Initial iterates for densities rho (B, r^3) on a finer grid than the
+        network's (r = factor * self.r): the densities are block-averaged to
+        self.r^3, the network predicts there and its fields are trilinearly
+        prolonged to the r^3 nodes (periodic).  Returns elastic (B, 6, 3, r^3)
+        and thermal (B, 3, 1, r^3) float64 fields."""
+        if r % self.r != 0:
+            raise ValueError(f"r={r} is not a multiple of the network resolution {self.r}")
+        factor = r // self.r
+        B = rho.shape[0]
+        s = _stream(self.device)
+        if factor == 1:
+            return self.predict(rho)
+        rc = torch.empty((B, self.r ** 3), dtype=torch.float64, device=self.device)
+        _lib.nn_call("maple_nn_restrict_density", _ptr(rho), _ptr(rc), B, self.r, factor, s)
+        ue_c, ut_c = self.predict(rc)
+        ue = torch.empty((B, 6, 3, r ** 3), dtype=torch.float64, device=self.device)
+        ut = torch.empty((B, 3, 1, r ** 3), dtype=torch.float64, device=self.device)
+        _lib.nn_call("maple_nn_prolong_fields", _ptr(ue_c), _ptr(ue), B * 18, self.r, factor, s)
+        _lib.nn_call("maple_nn_prolong_fields", _ptr(ut_c), _ptr(ut), B * 3, self.r, factor, s)
+        return ue, ut
+
     def flops_per_cell(self) -> float:
         """2 x multiply-adds of one forward pass on one r^3 cell."""
         return float(sum(2.0 * (self.r >> layer_level(L.name, self.levels)) ** 3 * L.taps * L.cin * L.cout
@@ -736,17 +758,26 @@ def main(argv=None):
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--save", default=None, help="write the trained weights (.npz)")
+    ap.add_argument("--load", default=None, help="skip training: use these weights (.npz)")
+    ap.add_argument("--fine-res", type=int, default=0,
+                    help="then run an OC loop at this resolution with the prolonged guess (e.g. 128)")
+    ap.add_argument("--fine-iters", type=int, default=30)
     a = ap.parse_args(argv)
     dev = torch.device("cuda", torch.cuda.current_device())
     t0 = time.perf_counter()
-    data = generate_solves(a.samples, a.res, seed0=100_000, precision=a.precision, rtol=a.rtol, device=dev)
+    if a.load:
+        net = WarmStartNet.load(a.load, r=a.res, device=dev)
+        data = generate_solves(min(a.samples, 256), a.res, seed0=100_000, precision=a.precision, rtol=a.rtol,
+                               device=dev, scale=net.scale.clone())
+    else:
+        data = generate_solves(a.samples, a.res, seed0=100_000, precision=a.precision, rtol=a.rtol, device=dev)
+        net = WarmStartNet(a.res, device=dev)
     held = generate_solves(a.heldout, a.res, seed0=200_000, precision=a.precision, rtol=a.rtol, device=dev,
                            scale=data.scale)
     t_gen = time.perf_counter() - t0
-    net = WarmStartNet(a.res, device=dev)
     t1 = time.perf_counter()
-    hist = train(net, data, a.steps, batch=a.batch, lr=a.lr, log_every=max(1, a.steps // 20),
-                 time_limit=a.train_seconds)
+    hist = [] if a.load else train(net, data, a.steps, batch=a.batch, lr=a.lr, log_every=max(1, a.steps // 20),
+                                   time_limit=a.train_seconds)
     torch.cuda.synchronize(dev)
     t_train = time.perf_counter() - t1
     val = validation_loss(net, held)
@@ -755,13 +786,44 @@ def main(argv=None):
     speed = forward_tflops(net, held.rho[:min(64, held.rho.shape[0])].contiguous())
     if a.save:
         net.save(a.save)
+    if a.fine_res:
+        out_fine = fine_oc_comparison(net, a.fine_res, a.fine_iters)
     out = {"res": a.res, "params": net.n_params, "samples": a.samples, "samples_converged": int(data.rho.shape[0]),
            "heldout_converged": int(held.rho.shape[0]), "generation_s": round(t_gen, 1),
-           "solve_iters_train_mean": [float(v) for v in data.iters.mean(0)], "train_steps": hist[-1][0],
+           "solve_iters_train_mean": [float(v) for v in data.iters.mean(0)],
+           "train_steps": hist[-1][0] if hist else 0,
            "batch": a.batch, "train_s": round(t_train, 1), "loss_history": hist, "heldout_energy_error": val,
            "forward": speed, **rep.summary()}
+    if a.fine_res:
+        out["fine_oc"] = out_fine
     print(json.dumps(out))
     return out
+
+
+def fine_oc_comparison(net: WarmStartNet, r: int = 128, iters: int = 30, seed: int = 0, sigma: float = 8.0,
+                       volfrac: float = 0.15, weights=(0.7, 0.0, 0.3)) -> dict:
+    """One fine cell (seeded design, bi-objective stiffness 0.7 / thermal 0.3
+    at vf 0.15) run for `iters` OC iterations in mixed precision twice: from
+    the zero initial guess and with the network's guess, evaluated at its own
+    resolution and prolonged, for the first iteration (later iterations start
+    from the previous iterate's solution in both runs)."""
+    from .batch import oc_run, seeded_design
+    x0 = seeded_design(seed, r, sigma, volfrac).reshape(1, -1)
+    res = {}
+    for mode in ("zero", "learned"):
+        ctx = HomogenizationContext(r, ncells=1, device=net.device)
+        guess = None
+        t0 = time.perf_counter()
+        if mode == "learned":
+            rho0 = torch.as_tensor(simp(x0), dtype=torch.float64).to(net.device)
+            guess = net.predict_prolonged(rho0, r)
+        out = oc_run(x0, np.asarray([weights]), np.asarray([volfrac]), precision="mixed", rtol=1e-10, maxit=500,
+                     dx_tol=0.0, max_iters=iters, ctx=ctx, record=True, guess=guess)
+        res[mode] = {"seconds": round(time.perf_counter() - t0, 3), "pcg_iters_total": int(out.pcg_iters.sum()),
+                     "pcg_iters_first": int(out.history[0]["pcg"][0]) if out.history else None,
+                     "J": float(out.J[0])}
+        ctx.close()
+    return {"res": r, "iters": iters, **res}
 
 
 if __name__ == "__main__":
