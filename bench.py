@@ -139,6 +139,19 @@ def measured_traffic(kernel, res):
     return int(m.group(1)) if m else None
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest of every rank's `value` (all ranks take part; world 1:
+    the value itself).  Device times of a multi-GPU run are reported as the
+    max over ranks."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_maple(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -192,11 +205,7 @@ def run_maple(args, rank, world, local_rank):
     barrier()
     clocks = sampler.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    t_dev = sum(step_ms) / 1000.0
-    if world > 1:
-        tt = torch.tensor([t_dev], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev = float(tt.item())
+    t_dev = max_over_ranks(sum(step_ms) / 1000.0, world, dev)
     value = world * args.steps / t_dev
 
     # live roofline of the dominant kernel class over K further steps
@@ -244,11 +253,7 @@ def run_maple(args, rank, world, local_rank):
             torch.cuda.synchronize()
             e_ms += e0.elapsed_time(e1)
             x_host.copy_(x_out)
-        t_e2e = e_ms / 1000.0
-        if world > 1:
-            tt = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t_e2e = float(tt.item())
+        t_e2e = max_over_ranks(e_ms / 1000.0, world, dev)
         e2e = {"value": round(world * args.steps / t_e2e, 3), "unit": UNIT,
                "h2d_bytes_per_step": int(x_host.numel() * 8), "d2h_bytes_per_step": int(x_out.numel() * 8 + 8)}
 
@@ -316,7 +321,7 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     res = run_maple(args, rank, world, local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
