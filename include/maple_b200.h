@@ -74,6 +74,13 @@ int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio,
  * launch eagerly (same results). */
 int maple_set_graphs(maple_ctx* ctx, int enable);
 
+/* Elastic and thermal solves of maple_oc_step at the same time (default on):
+ * the thermal build and solve run on a second stream driven by a second host
+ * thread of the library.  Off runs them one after the other on the caller's
+ * stream (same results).  maple_oc_step replaces the two TO_homo calls of
+ * main_IHD_v3.py:639-645, which the reference makes one after the other. */
+int maple_set_concurrency(maple_ctx* ctx, int enable);
+
 /* Per-cell active mask (host int[B], nonzero = active). Inactive cells are
  * skipped by every kernel.  NULL = all active. */
 int maple_set_active(maple_ctx* ctx, const int* active_host, maple_stream_t stream);

@@ -35,6 +35,7 @@ SIGNATURES = {
     "maple_ctx_info": (_I, [_P, _IP, _IP, C.POINTER(C.c_size_t)]),
     "maple_set_solver_options": (_I, [_P, _I, _D, _I, _D, _I]),
     "maple_set_graphs": (_I, [_P, _I]),
+    "maple_set_concurrency": (_I, [_P, _I]),
     "maple_set_active": (_I, [_P, _IP, _P]),
     "maple_set_density": (_I, [_P, _I, _P, _I, _P]),
     "maple_solve": (_I, [_P, _I, _I, _D, _I, _I, _IP, _IP, _P]),

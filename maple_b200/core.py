@@ -106,6 +106,10 @@ class HomogenizationContext:
         with torch.cuda.device(self.device):
             _lib.check(self._lib.maple_set_active(self._h, arr, _stream(self.device)))
 
+    def set_concurrency(self, enable: bool):
+        """Run the elastic and thermal solves of oc_step at the same time (default on)."""
+        _lib.check(self._lib.maple_set_concurrency(self._h, int(bool(enable))))
+
     def set_graphs(self, enable: bool):
         """Replay the PCG iteration body as a captured CUDA graph (default on)."""
         _lib.check(self._lib.maple_set_graphs(self._h, int(bool(enable))))

@@ -10,7 +10,9 @@
 #include <algorithm>
 #include <atomic>
 #include <map>
+#include <exception>
 #include <mutex>
+#include <thread>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -32,10 +34,12 @@ struct Failure {
                                       std::string(__FILE__) + ":" + std::to_string(__LINE__)};    \
   } while (0)
 static std::atomic<unsigned long long> g_launches{0};
+static thread_local unsigned long long tl_launches = 0;  // this thread's launches (graph capture accounting)
 #define CKL()                         \
   do {                                \
     CK(cudaGetLastError());           \
     g_launches.fetch_add(1);          \
+    ++tl_launches;                    \
   } while (0)
 
 static void require(bool ok, const std::string& msg) {
@@ -124,6 +128,29 @@ struct Scalars {
   int *done, *cell_done, *iters, *run;
 };
 
+// Per-solve scratch: the partial sums, PCG scalars, refinement scalars, pinned
+// convergence flags and capture stream of one solve in flight.  A context has
+// one lane per physics so that the elastic and thermal solves of an OC step
+// can run at the same time (from two host threads, on two streams).
+struct Lane {
+  double* part = nullptr;  // partial sums [B][nblk0][32]
+  double* red = nullptr;   // reduced values [B][32]
+  Scalars sc{};            // inner PCG scalars
+  double *o_rr = nullptr, *o_bn = nullptr, *o_scale = nullptr, *o_inv = nullptr;  // outer refinement
+  int *o_done = nullptr, *o_run = nullptr;
+  int* h_flags = nullptr;  // pinned host [B]
+  int* breakdown = nullptr;
+  cudaStream_t cap_stream = nullptr;
+};
+
+// lane of the calling thread: set by LaneScope around each physics' work
+static thread_local int tl_lane = 0;
+struct LaneScope {
+  int prev;
+  explicit LaneScope(int lane) : prev(tl_lane) { tl_lane = lane; }
+  ~LaneScope() { tl_lane = prev; }
+};
+
 }  // namespace maple
 
 struct maple_ctx {
@@ -136,13 +163,7 @@ struct maple_ctx {
   size_t bytes = 0;
   int* active = nullptr;          // device [B]
   std::vector<int> h_active;
-  double* part = nullptr;         // partial sums [B][nblk0][32]
-  double* red = nullptr;          // reduced values [B][32]
-  maple::Scalars sc{};            // inner PCG scalars
-  double *o_rr = nullptr, *o_bn = nullptr, *o_scale = nullptr, *o_inv = nullptr;  // outer refinement
-  int *o_done = nullptr, *o_run = nullptr;
-  int* h_flags = nullptr;         // pinned host [B]
-  int* breakdown = nullptr;
+  maple::Lane lanes[2];           // per-solve scratch, one lane per physics
   // OC step buffers
   double *x_rho = nullptr, *dJdx = nullptr, *dJf = nullptr, *Jv = nullptr, *terms = nullptr, *G3 = nullptr,
          *G1 = nullptr, *stats = nullptr, *ocpart = nullptr, *ocvf = nullptr;
@@ -155,8 +176,10 @@ struct maple_ctx {
     double rtol = -1;
     unsigned long long kernels = 0;  // kernel nodes per replay (for launch counting)
   } graphs[2][2];
-  cudaStream_t cap_stream = nullptr;
+  cudaStream_t aux_stream = nullptr;  // second physics of a concurrent OC step
+  cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
   bool use_graphs = true;
+  bool concurrent = true;  // elastic and thermal solves of an OC step on two streams
   // per-kernel-class event timing of fine-level launches (bench instrumentation)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -175,6 +198,8 @@ struct maple_ctx {
   double inner_rtol = 1e-5;
   int check_every = 1;
 };
+
+#define LN(c) ((c)->lanes[maple::tl_lane])
 
 namespace maple {
 
@@ -366,12 +391,12 @@ static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
       ApplyArgs<T> a{};
       a.u = v;
       a.out = w;
-      a.part = c->part;
+      a.part = LN(c).part;
       apply<T, D, 1, M_POWER>(c, p, o, l, a, c->active, s);
       std::swap(v, w);
     }
-    reduce<2>(c, c->part, ceil_div(Nl, kPowerNodes<D>), c->red, s);
-    KL(c, s, k_power_finish<<<nblk(c->B), kThreads, 0, s>>>(c->red, o.hi[l], c->B, c->power_safety));
+    reduce<2>(c, LN(c).part, ceil_div(Nl, kPowerNodes<D>), LN(c).red, s);
+    KL(c, s, k_power_finish<<<nblk(c->B), kThreads, 0, s>>>(LN(c).red, o.hi[l], c->B, c->power_safety));
   }
 }
 
@@ -421,7 +446,11 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
       KL(c, s, k_dense_from_stencil<D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.S64c, p.Ainv, n, act));
       if (ndof <= kCholSmemMax) {
         const size_t sm = chol_smem_bytes(ndof);
-        CK(cudaFuncSetAttribute(k_chol_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        static std::once_flag chol_attr;  // the largest size, once: both physics' builds may run concurrently
+        std::call_once(chol_attr, [] {
+          CK(cudaFuncSetAttribute(k_chol_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)chol_smem_bytes(kCholSmemMax)));
+        });
         KL(c, s, k_chol_inverse_smem<<<B, kCholThreads, sm, s>>>(p.Ainv, ndof, D, act, nullptr));
       } else {
         KL(c, s, k_chol_inverse<<<B, 512, 0, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr));
@@ -510,10 +539,10 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
 // PCG on level 0 in precision T
 // ---------------------------------------------------------------------------
 static bool all_done(maple_ctx* c, const int* cell_done, const int* run_ref, cudaStream_t s) {
-  CK(cudaMemcpyAsync(c->h_flags, cell_done, c->B * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(LN(c).h_flags, cell_done, c->B * sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   for (int b = 0; b < c->B; ++b)
-    if (!c->h_flags[b] && c->h_active[b]) return false;
+    if (!LN(c).h_flags[b] && c->h_active[b]) return false;
   return true;
 }
 
@@ -562,29 +591,30 @@ static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, double rtol,
           CK(cudaGraphExecDestroy(ge.exec));
           ge.exec = nullptr;
         }
-        if (!c->cap_stream) CK(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+        if (!LN(c).cap_stream) CK(cudaStreamCreateWithFlags(&LN(c).cap_stream, cudaStreamNonBlocking));
         cudaGraph_t graph = nullptr;
-        const unsigned long long before = g_launches.load();
-        CK(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
+        const unsigned long long before = tl_launches;
+        CK(cudaStreamBeginCapture(LN(c).cap_stream, cudaStreamCaptureModeThreadLocal));
         try {
-          body(c->cap_stream);
+          body(LN(c).cap_stream);
         } catch (...) {
-          cudaStreamEndCapture(c->cap_stream, &graph);
+          cudaStreamEndCapture(LN(c).cap_stream, &graph);
           if (graph) cudaGraphDestroy(graph);
           throw;
         }
-        CK(cudaStreamEndCapture(c->cap_stream, &graph));
+        CK(cudaStreamEndCapture(LN(c).cap_stream, &graph));
         CK(cudaGraphInstantiate(&ge.exec, graph, 0));
         CK(cudaGraphDestroy(graph));
         ge.rtol = rtol;
-        ge.kernels = g_launches.load() - before;
+        ge.kernels = tl_launches - before;
         g_launches.fetch_sub(ge.kernels);  // captured, not launched
+        tl_launches -= ge.kernels;
       }
       CK(cudaGraphLaunch(ge.exec, s));
       g_launches.fetch_add(ge.kernels);
     }
     if (it % c->check_every == 0 || it == maxit) {
-      if (all_done(c, c->sc.cell_done, nullptr, s)) break;
+      if (all_done(c, LN(c).sc.cell_done, nullptr, s)) break;
     }
   }
 }
@@ -603,7 +633,7 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
                 const int* outer_run, cudaStream_t s) {
   const int B = c->B, N = nodes(c->n[0]);
   const size_t vbytes = (size_t)B * N * R * D * sizeof(T);
-  Scalars& sc = c->sc;
+  Scalars& sc = LN(c).sc;
   const unsigned nb = nblk(N);                    // partials of the vector kernels
   const unsigned nbf = (unsigned)fine_tiles(c->n[0]);  // partials of the fine-level operator
   PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
@@ -620,16 +650,16 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
     a.out = o.r;
     apply<T, D, R, M_RES>(c, p, o, 0, a, run, s);
   }
-  KL(c, s, k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, c->part, N, run));
-  reduce<R>(c, c->part, nb, sc.bnorm2, s);
-  KL(c, s, k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.r, o.r, c->part, N, run));
-  reduce<R>(c, c->part, nb, sc.rr, s);
+  KL(c, s, k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, LN(c).part, N, run));
+  reduce<R>(c, LN(c).part, nb, sc.bnorm2, s);
+  KL(c, s, k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.r, o.r, LN(c).part, N, run));
+  reduce<R>(c, LN(c).part, nb, sc.rr, s);
   KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0));
   KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
   if (all_done(c, sc.cell_done, run, s)) return;
   // z = M r ; rz ; p = z
-  vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, s);
-  reduce<R>(c, c->part, nbf, sc.rz_new, s);
+  vcycle<T, D, R>(c, p, o, 0, o.r, run, LN(c).part, s);
+  reduce<R>(c, LN(c).part, nbf, sc.rz_new, s);
   KL(c, s, k_set_rz<<<nblk(B * R), kThreads, 0, s>>>(sc.rz, sc.rz_new, B * R));
   CK(cudaMemcpyAsync(o.p, o.U[0][1], vbytes, cudaMemcpyDeviceToDevice, s));
   auto body = [&](cudaStream_t st) {
@@ -637,17 +667,17 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
       ApplyArgs<T> a{};
       a.u = o.p;
       a.out = o.q;
-      a.part = c->part;
+      a.part = LN(c).part;
       apply<T, D, R, M_MV>(c, p, o, 0, a, run, st);
     }
-    reduce<R>(c, c->part, nbf, sc.pq, st);
-    KL(c, st, k_pcg_alpha<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R, c->breakdown));
-    KL(c, st, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.x, o.r, o.p, o.q, sc.alpha, c->part, N, run));
-    reduce<R>(c, c->part, nb, sc.rr, st);
+    reduce<R>(c, LN(c).part, nbf, sc.pq, st);
+    KL(c, st, k_pcg_alpha<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R, LN(c).breakdown));
+    KL(c, st, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.x, o.r, o.p, o.q, sc.alpha, LN(c).part, N, run));
+    reduce<R>(c, LN(c).part, nb, sc.rr, st);
     KL(c, st, k_pcg_check<<<nblk(B), kThreads, 0, st>>>(ps, B, R, rtol * rtol, 1));
     KL(c, st, k_sync_run<<<nblk(B), kThreads, 0, st>>>(sc.cell_done, sc.run, B));
-    vcycle<T, D, R>(c, p, o, 0, o.r, run, c->part, st);
-    reduce<R>(c, c->part, nbf, sc.rz_new, st);
+    vcycle<T, D, R>(c, p, o, 0, o.r, run, LN(c).part, st);
+    reduce<R>(c, LN(c).part, nbf, sc.rz_new, st);
     KL(c, st, k_pcg_beta<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R));
     KL(c, st, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.p, o.U[0][1], sc.beta, N, run));
   };
@@ -662,13 +692,13 @@ template <int D, int R>
 static void precondition_f32(maple_ctx* c, Phys& p, const double* r, const double* q, const int* run,
                              cudaStream_t s) {
   const int B = c->B, N = nodes(c->n[0]);
-  Scalars& sc = c->sc;
+  Scalars& sc = LN(c).sc;
   Ops<float>& o = p.o32;
-  KL(c, s, k_col_scales<<<nblk(B * R), kThreads, 0, s>>>(sc.rr, c->o_scale, c->o_inv, B * R));
-  KL(c, s, k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, c->o_scale, N, run));
+  KL(c, s, k_col_scales<<<nblk(B * R), kThreads, 0, s>>>(sc.rr, LN(c).o_scale, LN(c).o_inv, B * R));
+  KL(c, s, k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, LN(c).o_scale, N, run));
   vcycle<float, D, R>(c, p, o, 0, o.r, run, nullptr, s);
-  KL(c, s, k_precond_back<R, D><<<g2(N, B), kThreads, 0, s>>>(o.U[0][1], c->o_inv, p.z64, r, q, c->part, N, run));
-  reduce<2 * R>(c, c->part, nblk(N), c->red, s);
+  KL(c, s, k_precond_back<R, D><<<g2(N, B), kThreads, 0, s>>>(o.U[0][1], LN(c).o_inv, p.z64, r, q, LN(c).part, N, run));
+  reduce<2 * R>(c, LN(c).part, nblk(N), LN(c).red, s);
 }
 
 template <int D, int R>
@@ -676,7 +706,7 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
                       cudaStream_t s) {
   const int B = c->B, N = nodes(c->n[0]);
   const size_t vbytes = (size_t)B * N * R * D * sizeof(double);
-  Scalars& sc = c->sc;
+  Scalars& sc = LN(c).sc;
   const unsigned nb = nblk(N), nbf = (unsigned)fine_tiles(c->n[0]);
   PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
   Ops<double>& o64 = p.o64;
@@ -693,32 +723,32 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
     a.out = r;
     apply<double, D, R, M_RES>(c, p, o64, 0, a, run, s);
   }
-  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, c->part, N, run));
-  reduce<R>(c, c->part, nb, sc.bnorm2, s);
-  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(r, r, c->part, N, run));
-  reduce<R>(c, c->part, nb, sc.rr, s);
+  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, LN(c).part, N, run));
+  reduce<R>(c, LN(c).part, nb, sc.bnorm2, s);
+  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(r, r, LN(c).part, N, run));
+  reduce<R>(c, LN(c).part, nb, sc.rr, s);
   KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0));
   KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
   if (all_done(c, sc.cell_done, run, s)) return;
   precondition_f32<D, R>(c, p, r, nullptr, run, s);
-  KL(c, s, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, c->red, B, R, 1));
+  KL(c, s, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, LN(c).red, B, R, 1));
   CK(cudaMemcpyAsync(pv, z, vbytes, cudaMemcpyDeviceToDevice, s));
   auto body = [&](cudaStream_t st) {
     {
       ApplyArgs<double> a{};
       a.u = pv;
       a.out = q;
-      a.part = c->part;
+      a.part = LN(c).part;
       apply<double, D, R, M_MV>(c, p, o64, 0, a, run, st);
     }
-    reduce<R>(c, c->part, nbf, sc.pq, st);
-    KL(c, st, k_pcg_alpha<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R, c->breakdown));
-    KL(c, st, k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, st>>>(x, r, pv, q, sc.alpha, c->part, N, run));
-    reduce<R>(c, c->part, nb, sc.rr, st);
+    reduce<R>(c, LN(c).part, nbf, sc.pq, st);
+    KL(c, st, k_pcg_alpha<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R, LN(c).breakdown));
+    KL(c, st, k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, st>>>(x, r, pv, q, sc.alpha, LN(c).part, N, run));
+    reduce<R>(c, LN(c).part, nb, sc.rr, st);
     KL(c, st, k_pcg_check<<<nblk(B), kThreads, 0, st>>>(ps, B, R, rtol * rtol, 1));
     KL(c, st, k_sync_run<<<nblk(B), kThreads, 0, st>>>(sc.cell_done, sc.run, B));
     precondition_f32<D, R>(c, p, r, q, run, st);
-    KL(c, st, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, st>>>(ps, c->red, B, R, 0));
+    KL(c, st, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, st>>>(ps, LN(c).red, B, R, 0));
     KL(c, st, k_pcg_direction<double, R, D><<<g2(N, B), kThreads, 0, st>>>(pv, z, sc.beta, N, run));
   };
   run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_MIXED], rtol, maxit, body, s);
@@ -761,8 +791,8 @@ static void solve_phys(maple_ctx* c, int phys, int prec, const double* F, double
     pcg<double, D, R>(c, p, o, F, x_zero, rtol, maxit, nullptr, s);
     CK(cudaMemcpyAsync(x64, o.x, vb64, cudaMemcpyDeviceToDevice, s));
     std::vector<int> it(B), cd(B);
-    CK(cudaMemcpyAsync(it.data(), c->sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(cd.data(), c->sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(it.data(), LN(c).sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(cd.data(), LN(c).sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     for (int b = 0; b < B; ++b) {
       it_total[b] = it[b];
@@ -771,8 +801,8 @@ static void solve_phys(maple_ctx* c, int phys, int prec, const double* F, double
   } else {
     pcg_mixed<D, R>(c, p, F, x64, x_zero, rtol, maxit, s);
     std::vector<int> it(B), cd(B);
-    CK(cudaMemcpyAsync(it.data(), c->sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(cd.data(), c->sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(it.data(), LN(c).sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(cd.data(), LN(c).sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     for (int b = 0; b < B; ++b) {
       it_total[b] = it[b];
@@ -834,15 +864,15 @@ static void homogenize(maple_ctx* c, int phys, cudaStream_t s) {
   const int N = nodes(c->n[0]);
   const unsigned nb = nblk(N);
   if (phys == MAPLE_ELASTIC) {
-    KL(c, s, k_homogenize<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, c->part, c->n[0], p.kscale,
+    KL(c, s, k_homogenize<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, LN(c).part, c->n[0], p.kscale,
                                                         p.xscale, c->active));
-    reduce<21>(c, c->part, nb, c->red, s);
-    KL(c, s, k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(c->red, p.H, c->B, 6));
+    reduce<21>(c, LN(c).part, nb, LN(c).red, s);
+    KL(c, s, k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(LN(c).red, p.H, c->B, 6));
   } else {
-    KL(c, s, k_homogenize<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, c->part, c->n[0], p.kscale,
+    KL(c, s, k_homogenize<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, LN(c).part, c->n[0], p.kscale,
                                                         p.xscale, c->active));
-    reduce<6>(c, c->part, nb, c->red, s);
-    KL(c, s, k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(c->red, p.H, c->B, 3));
+    reduce<6>(c, LN(c).part, nb, LN(c).red, s);
+    KL(c, s, k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(LN(c).red, p.H, c->B, 3));
   }
   p.energies = true;
 }
@@ -1010,30 +1040,33 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
       c->ph[1].xscale = h;
       const int B = ncells;
       const size_t N0 = nodes(r);
-      c->part = dnew<double>(c, (size_t)B * std::max<size_t>(nblk(N0), fine_tiles(r)) * 32);
-      c->red = dnew<double>(c, (size_t)B * 32);
-      c->sc.rz = dnew<double>(c, B * 6);
-      c->sc.rz_new = dnew<double>(c, B * 6);
-      c->sc.pq = dnew<double>(c, B * 6);
-      c->sc.rr = dnew<double>(c, B * 6);
-      c->sc.bnorm2 = dnew<double>(c, B * 6);
-      c->sc.alpha = dnew<double>(c, B * 6);
-      c->sc.beta = dnew<double>(c, B * 6);
-      c->sc.done = dnew<int>(c, B * 6);
-      c->sc.cell_done = dnew<int>(c, B);
-      c->sc.iters = dnew<int>(c, B);
-      c->sc.run = dnew<int>(c, B);
-      c->o_rr = dnew<double>(c, B * 6);
-      c->o_bn = dnew<double>(c, B * 6);
-      c->o_scale = dnew<double>(c, B * 6);
-      c->o_inv = dnew<double>(c, B * 6);
-      c->o_done = dnew<int>(c, B);
-      c->o_run = dnew<int>(c, B);
-      c->breakdown = dnew<int>(c, 1);
+      for (Lane& L : c->lanes) {
+        L.part = dnew<double>(c, (size_t)B * std::max<size_t>(nblk(N0), fine_tiles(r)) * 32);
+        L.red = dnew<double>(c, (size_t)B * 32);
+        L.sc.rz = dnew<double>(c, B * 6);
+        L.sc.rz_new = dnew<double>(c, B * 6);
+        L.sc.pq = dnew<double>(c, B * 6);
+        L.sc.rr = dnew<double>(c, B * 6);
+        L.sc.bnorm2 = dnew<double>(c, B * 6);
+        L.sc.alpha = dnew<double>(c, B * 6);
+        L.sc.beta = dnew<double>(c, B * 6);
+        L.sc.done = dnew<int>(c, B * 6);
+        L.sc.cell_done = dnew<int>(c, B);
+        L.sc.iters = dnew<int>(c, B);
+        L.sc.run = dnew<int>(c, B);
+        L.o_rr = dnew<double>(c, B * 6);
+        L.o_bn = dnew<double>(c, B * 6);
+        L.o_scale = dnew<double>(c, B * 6);
+        L.o_inv = dnew<double>(c, B * 6);
+        L.o_done = dnew<int>(c, B);
+        L.o_run = dnew<int>(c, B);
+        L.breakdown = dnew<int>(c, 1);
+        CK(cudaMemset(L.breakdown, 0, sizeof(int)));
+        CK(cudaMallocHost(&L.h_flags, B * sizeof(int)));
+      }
       c->active = dnew<int>(c, B);
       c->h_active.assign(B, 1);
       CK(cudaMemcpy(c->active, c->h_active.data(), B * sizeof(int), cudaMemcpyHostToDevice));
-      CK(cudaMallocHost(&c->h_flags, B * sizeof(int)));
       c->x_rho = dnew<double>(c, (size_t)B * N0);
       c->dJdx = dnew<double>(c, (size_t)B * N0);
       c->dJf = dnew<double>(c, (size_t)B * N0);
@@ -1049,10 +1082,10 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
       c->bar = dnew<unsigned>(c, 2);
       c->err = dnew<int>(c, 1);
       CK(cudaMemset(c->err, 0, sizeof(int)));
-      CK(cudaMemset(c->breakdown, 0, sizeof(int)));
     } catch (...) {
       for (void* p : c->allocs) cudaFree(p);
-      if (c->h_flags) cudaFreeHost(c->h_flags);
+      for (Lane& L : c->lanes)
+        if (L.h_flags) cudaFreeHost(L.h_flags);
       delete c;
       throw;
     }
@@ -1118,9 +1151,14 @@ int maple_ctx_destroy(maple_ctx* c) {
     if (!c) return;
     for (auto& e : c->ev_pool) cudaEventDestroy(e);
     drop_graphs(c);
-    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    for (Lane& L : c->lanes) {
+      if (L.cap_stream) cudaStreamDestroy(L.cap_stream);
+      if (L.h_flags) cudaFreeHost(L.h_flags);
+    }
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+    if (c->aux_fork) cudaEventDestroy(c->aux_fork);
+    if (c->aux_join) cudaEventDestroy(c->aux_join);
     for (void* p : c->allocs) cudaFree(p);
-    if (c->h_flags) cudaFreeHost(c->h_flags);
     delete c;
   });
 }
@@ -1131,6 +1169,13 @@ int maple_ctx_info(const maple_ctx* c, int* levels, int* coarsest, size_t* bytes
     if (levels) *levels = c->L;
     if (coarsest) *coarsest = c->n[c->L - 1];
     if (bytes) *bytes = c->bytes;
+  });
+}
+
+int maple_set_concurrency(maple_ctx* c, int enable) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    c->concurrent = enable != 0;
   });
 }
 
@@ -1170,6 +1215,7 @@ int maple_set_active(maple_ctx* c, const int* act, maple_stream_t s) {
 
 int maple_set_density(maple_ctx* c, int phys, const double* rho, int prec, maple_stream_t s) {
   return guarded([&] {
+    LaneScope lane(phys == MAPLE_THERMAL ? 1 : 0);
     require(c != nullptr && rho != nullptr, "NULL argument");
     require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
     require(prec == MAPLE_FP64 || prec == MAPLE_MIXED, "unknown precision");
@@ -1182,6 +1228,7 @@ int maple_set_density(maple_ctx* c, int phys, const double* rho, int prec, maple
 int maple_solve(maple_ctx* c, int phys, int prec, double rtol, int maxit, int warm, int* iters, int* status,
                 maple_stream_t s) {
   return guarded([&] {
+    LaneScope lane(phys == MAPLE_THERMAL ? 1 : 0);
     require(c != nullptr, "ctx is NULL");
     require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
     Phys& p = c->ph[phys];
@@ -1199,6 +1246,7 @@ int maple_solve(maple_ctx* c, int phys, int prec, double rtol, int maxit, int wa
 int maple_solve_rhs(maple_ctx* c, int phys, int prec, const double* F, const double* x0, double rtol, int maxit,
                     double* u_out, double* r_out, int* iters, int* status, maple_stream_t s) {
   return guarded([&] {
+    LaneScope lane(phys == MAPLE_THERMAL ? 1 : 0);
     require(c != nullptr && F != nullptr && u_out != nullptr, "NULL argument");
     require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
     Phys& p = c->ph[phys];
@@ -1245,6 +1293,7 @@ int maple_set_solution(maple_ctx* c, int phys, const double* u, maple_stream_t s
 
 int maple_homogenize(maple_ctx* c, int phys, double* H_out, double* energy_out, maple_stream_t s) {
   return guarded([&] {
+    LaneScope lane(phys == MAPLE_THERMAL ? 1 : 0);
     require(c != nullptr, "ctx is NULL");
     require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
     Phys& p = c->ph[phys];
@@ -1394,26 +1443,61 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       need_ch |= (hw[3 * b] != 0.0 || hw[3 * b + 1] != 0.0);
       need_k |= (hw[3 * b + 2] != 0.0);
     }
-    std::vector<int> it_tmp(B, 0), it_sum(B, 0);
-    for (int phys = 0; phys < 2; ++phys) {
-      if ((phys == 0 && !need_ch) || (phys == 1 && !need_k)) {
-        c->ph[phys].energies = false;
-        continue;
-      }
+    // one physics: SIMP map, hierarchy, RHS, MG-PCG solve, energies
+    auto run_phys = [&](int phys, cudaStream_t ps, int* it_out) {
+      LaneScope lane(phys);
       Phys& p = c->ph[phys];
-      ensure_prec(c, phys, prec);
       const size_t tot = (size_t)B * N;
-      KL(c, st, k_simp<<<nblk(tot), kThreads, 0, st>>>(x, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot, N, xmin,
-                                             penal, rho_min, c->active));
-      build(c, phys, prec, st);
-      assemble_rhs(c, phys, p.o64.rho, p.F64, st);
+      KL(c, ps, k_simp<<<nblk(tot), kThreads, 0, ps>>>(x, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot,
+                                                       N, xmin, penal, rho_min, c->active));
+      build(c, phys, prec, ps);
+      assemble_rhs(c, phys, p.o64.rho, p.F64, ps);
       const bool was_solved = p.solved;
-      dispatch_solve(c, phys, prec, p.F64, p.u64, !(warm && was_solved), rtol, maxit, it_tmp.data(), nullptr, st);
+      dispatch_solve(c, phys, prec, p.F64, p.u64, !(warm && was_solved), rtol, maxit, it_out, nullptr, ps);
       p.solved = true;
       p.current = true;
-      for (int b = 0; b < B; ++b) it_sum[b] += it_tmp[b];
-      homogenize(c, phys, st);
+      homogenize(c, phys, ps);
+    };
+    std::vector<int> it_el(B, 0), it_th(B, 0), it_sum(B, 0);
+    if (!need_ch) c->ph[0].energies = false;
+    if (!need_k) c->ph[1].energies = false;
+    if (need_ch) ensure_prec(c, 0, prec);  // all allocation happens here, on this thread
+    if (need_k) ensure_prec(c, 1, prec);
+    if (need_ch && need_k && c->concurrent && !c->profiling) {
+      // the thermal solve runs on a second stream, driven by a second host
+      // thread (each solve waits on its own convergence checks)
+      if (!c->aux_stream) {
+        CK(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->aux_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->aux_join, cudaEventDisableTiming));
+      }
+      CK(cudaEventRecord(c->aux_fork, st));
+      CK(cudaStreamWaitEvent(c->aux_stream, c->aux_fork, 0));
+      std::exception_ptr thermal_err;
+      const int dev = c->dev;
+      std::thread worker([&] {
+        try {
+          CK(cudaSetDevice(dev));
+          run_phys(1, c->aux_stream, it_th.data());
+        } catch (...) {
+          thermal_err = std::current_exception();
+        }
+      });
+      try {
+        run_phys(0, st, it_el.data());
+      } catch (...) {
+        worker.join();
+        throw;
+      }
+      worker.join();
+      if (thermal_err) std::rethrow_exception(thermal_err);
+      CK(cudaEventRecord(c->aux_join, c->aux_stream));
+      CK(cudaStreamWaitEvent(st, c->aux_join, 0));
+    } else {
+      if (need_ch) run_phys(0, st, it_el.data());
+      if (need_k) run_phys(1, st, it_th.data());
     }
+    for (int b = 0; b < B; ++b) it_sum[b] = it_el[b] + it_th[b];
     KL(c, st, k_objective<<<nblk(B), kThreads, 0, st>>>(c->ph[0].H, c->ph[1].H, w, c->Jv, c->terms, c->G3, c->G1, B,
                                               need_ch ? 1 : 0, need_k ? 1 : 0, c->active));
     KL(c, st, k_sensitivity<<<g2(N, B), kThreads, 0, st>>>(x, need_ch ? c->ph[0].energy : nullptr,

@@ -405,17 +405,19 @@ class WarmStartNet:
         self._refresh()
 
     def energy_loss(self, out: torch.Tensor, target: torch.Tensor, rho: torch.Tensor, energy: torch.Tensor,
-                    gscale: float = 1024.0, grad: bool = True, per_cell: bool = False):
+                    gscale: float = 1024.0, grad: bool = True, per_cell: bool = False,
+                    floor: Optional[torch.Tensor] = None):
         """Relative energy error of the predicted fields, e = scale * (out -
         target): the mean over cells and the 9 load cases of e_r^T K(rho) e_r
         divided by the solution energy of that cell (per_cell), or by that
-        energy plus the batch mean of the load case (default: every term stays
-        bounded, so nearly void cells of tiny energy cannot dominate the
-        gradient).  Returns (per-(cell, load case) values (B, 9), BF16
-        gradient x gscale w.r.t. out or None); self.last_loss holds the mean."""
+        energy plus `floor` (9,) -- default the batch mean of each load case --
+        so that every term stays bounded and nearly void cells of tiny energy
+        cannot dominate the gradient.  Returns (per-(cell, load case) values
+        (B, 9), BF16 gradient x gscale w.r.t. out or None); self.last_loss
+        holds the mean."""
         B, N = rho.shape
         if not per_cell:
-            energy = energy + energy.mean(dim=0, keepdim=True)
+            energy = energy + (energy.mean(dim=0, keepdim=True) if floor is None else floor.reshape(1, 9))
         s = _stream(self.device)
         ctx = self._fe_ctx(B)
         sc_th = C.c_void_p(self.scale.data_ptr() + OUT_ELASTIC * 8)
@@ -445,13 +447,13 @@ class WarmStartNet:
         return d, gout
 
     def train_step(self, rho: torch.Tensor, target: torch.Tensor, energy: torch.Tensor, lr: float,
-                   gscale: float = 1024.0, clip: Optional[float] = None):
+                   gscale: float = 1024.0, clip: Optional[float] = None, floor: Optional[torch.Tensor] = None):
         """One Adam step on a batch: rho (B, N) float64, target (B, N, 21) BF16,
         solution energies (B, 9) float64.  The gradient is rescaled to norm
         `clip` when it is larger (None: no clipping)."""
         self.grad.zero_()
         out = self.forward(self.features(rho))
-        _, gout = self.energy_loss(out, target, rho, energy, gscale)
+        _, gout = self.energy_loss(out, target, rho, energy, gscale, floor=floor)
         self.backward(gout)
         scale = gscale
         if clip is not None:
@@ -607,11 +609,15 @@ def generate_solves(n: int, r: int, seed0: int = 100_000, batch: int = 256, prec
 
 def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: float = 1e-3, lr_min: float = 2e-5,
           warmup: int = 50, seed: int = 0, log_every: int = 0, time_limit: Optional[float] = None,
-          clip: Optional[float] = None):
+          clip: Optional[float] = None, val: Optional[SolveSet] = None, val_every: int = 100):
     """Adam with linear warm-up and cosine decay over `steps` mini-batches
-    drawn without replacement (reshuffled every epoch).  Returns the loss
-    history [(step, loss)] read every log_every steps and at the end."""
+    drawn without replacement (reshuffled every epoch).  With a validation
+    set, the weights are evaluated every val_every steps and the best ones
+    are kept at the end.  Returns the loss history [(step, loss)] read every
+    log_every steps and at the end."""
     net.scale.copy_(data.scale)
+    floor = data.energy.mean(dim=0).contiguous()  # per load case, fixed for the whole run
+    best = (math.inf, None)
     S = data.rho.shape[0]
     batch = min(batch, S)
     g = torch.Generator().manual_seed(seed)
@@ -633,12 +639,19 @@ def train(net: WarmStartNet, data: SolveSet, steps: int, batch: int = 16, lr: fl
         else:
             c = (it - warmup) / max(1, steps - warmup)
             lr_t = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * c))
-        loss = net.train_step(rho, tgt, en, lr_t, clip=clip)
+        loss = net.train_step(rho, tgt, en, lr_t, clip=clip, floor=floor)
         last = it == steps - 1 or (time_limit is not None and time.perf_counter() - t0 > time_limit)
         if (log_every and (it + 1) % log_every == 0) or last:
             hist.append((it + 1, float(loss.item())))
+        if val is not None and ((it + 1) % val_every == 0 or last):
+            v = validation_loss(net, val)
+            if v < best[0]:
+                best = (v, net.w32.clone())
         if last:
             break
+    if best[1] is not None:
+        net.w32.copy_(best[1])
+        net._refresh()
     return hist
 
 

@@ -271,3 +271,28 @@ def test_precision_switch_on_one_context(lib):
         c.solve("elastic", prec, rtol=1e-12, maxit=300)
         assert rel(c.homogenize("elastic").cpu().numpy(), ref[prec]) < 1e-11, prec
     c.close()
+
+
+def test_concurrent_physics_match_sequential(lib):
+    """OC steps with the elastic and thermal solves running at the same time
+    (two streams, two host threads) give bit-identical results to the same
+    steps run one physics after the other."""
+    from maple_b200.core import HomogenizationContext
+    r, B = 16, 2
+    x0 = np.stack([O.seed_density(s, r, 2.0, 0.3).reshape(-1) for s in (4, 5)])
+    w = T(np.array([[0.4, 0.2, 0.4], [1 / 3, 1 / 3, 1 / 3]]))
+    vf = T(np.array([0.3, 0.3]))
+    runs = []
+    for concurrent in (False, True):
+        c = HomogenizationContext(r, ncells=B)
+        c.set_concurrency(concurrent)
+        x = T(x0)
+        rec = []
+        for _ in range(3):
+            out = c.oc_step(x, w, vf, precision="mixed", rtol=1e-10, warm=True)
+            x = out["x_next"].clone()
+            rec.append((out["J"].cpu().numpy(), x.cpu().numpy(), np.array(out["iters"])))
+        runs.append(rec)
+        c.close()
+    for (j0, x0_, i0), (j1, x1, i1) in zip(*runs):
+        assert np.array_equal(j0, j1) and np.array_equal(x0_, x1) and np.array_equal(i0, i1)
