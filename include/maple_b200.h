@@ -81,6 +81,19 @@ int maple_set_graphs(maple_ctx* ctx, int enable);
  * main_IHD_v3.py:639-645, which the reference makes one after the other. */
 int maple_set_concurrency(maple_ctx* ctx, int enable);
 
+/* Symmetry projection (main_IHD_v3.py:221-337): kind MAPLE_SYM_MIRROR averages
+ * over the reflections about the centre planes of the axes in axes_mask
+ * (bit 0 = x, 1 = y, 2 = z; voxel i reflects to r-1-i); MAPLE_SYM_CUBIC over
+ * all 48 axis permutations and reflections.  maple_set_symmetry makes
+ * maple_oc_step solve at clamp(P(x)), project the gradient and return
+ * clamp(P(x_new)) (main_IHD_v3.py:625-626, 695-700; default none);
+ * maple_symmetrize applies P to [ncells][r^3] fields (symmetrize_vec,
+ * main_IHD_v3.py:329-337).  out must not alias in. */
+enum { MAPLE_SYM_NONE = 0, MAPLE_SYM_MIRROR = 1, MAPLE_SYM_CUBIC = 2 };
+int maple_set_symmetry(maple_ctx* ctx, int kind, int axes_mask);
+int maple_symmetrize(int r, int ncells, int kind, int axes_mask, const double* in, double* out,
+                     maple_stream_t stream);
+
 /* Per-cell active mask (host int[B], nonzero = active). Inactive cells are
  * skipped by every kernel.  NULL = all active. */
 int maple_set_active(maple_ctx* ctx, const int* active_host, maple_stream_t stream);

@@ -36,6 +36,8 @@ SIGNATURES = {
     "maple_set_solver_options": (_I, [_P, _I, _D, _I, _D, _I]),
     "maple_set_graphs": (_I, [_P, _I]),
     "maple_set_concurrency": (_I, [_P, _I]),
+    "maple_set_symmetry": (_I, [_P, _I, _I]),
+    "maple_symmetrize": (_I, [_I, _I, _I, _I, _P, _P, _P]),
     "maple_set_active": (_I, [_P, _IP, _P]),
     "maple_set_density": (_I, [_P, _I, _P, _I, _P]),
     "maple_solve": (_I, [_P, _I, _I, _D, _I, _I, _IP, _IP, _P]),
@@ -80,6 +82,7 @@ SIGNATURES = {
 }
 
 NN_POOL, NN_UPSAMPLE, NN_UPSAMPLE_ADJ, NN_POOL_ADJ = 0, 1, 2, 3
+SYM_NONE, SYM_MIRROR, SYM_CUBIC = 0, 1, 2
 
 _lib = None
 

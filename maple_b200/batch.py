@@ -70,8 +70,9 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
            penal: float = 3.0, rho_min: float = 1e-9, filter_k: int = 3, precision: str = "mixed",
            rtol: float = 1e-8, maxit: int = 500, dx_tol: float = 0.01, max_iters: int = 200,
            ctx: Optional[HomogenizationContext] = None, device=None, record: bool = False,
-           guess=None) -> BatchResult:
-    """Run B independent OC loops to their own stopping points.  `guess` =
+           guess=None, symmetry: str = "none") -> BatchResult:
+    """Run B independent OC loops to their own stopping points (with the
+    symmetry projection `symmetry`, a spec as in parse_symmetry).  `guess` =
     (elastic (B, 6, 3, N), thermal (B, 3, 1, N)) float64 fields: the initial
     iterates of the first iteration's solves (later iterations start from the
     previous iteration's solutions)."""
@@ -84,6 +85,12 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
     w = torch.as_tensor(np.asarray(weights), dtype=torch.float64).to(dev).reshape(B, 3).contiguous()
     vf = torch.as_tensor(np.asarray(volfrac), dtype=torch.float64).to(dev).reshape(B).contiguous()
     ctx = ctx or HomogenizationContext(r, ncells=B, device=dev)
+    from .optimize import parse_symmetry
+    sym_kind, sym_axes = parse_symmetry(symmetry)
+    ctx.set_symmetry(sym_kind, sym_axes)
+    if sym_kind != "none":
+        from .core import symmetrize
+        x = symmetrize(x, r, sym_kind, sym_axes).clamp(xmin, 1.0).contiguous()
     if guess is not None:
         ctx.set_solution("elastic", guess[0].contiguous())
         ctx.set_solution("thermal", guess[1].contiguous())

@@ -106,6 +106,12 @@ class HomogenizationContext:
         with torch.cuda.device(self.device):
             _lib.check(self._lib.maple_set_active(self._h, arr, _stream(self.device)))
 
+    def set_symmetry(self, kind: str = "none", axes=()):
+        """Symmetry projection applied by oc_step ("none", "mirror" with axes,
+        "cubic"); see ``symmetrize``."""
+        k, mask = _sym_args(kind, axes)
+        _lib.check(self._lib.maple_set_symmetry(self._h, k, mask))
+
     def set_concurrency(self, enable: bool):
         """Run the elastic and thermal solves of oc_step at the same time (default on)."""
         _lib.check(self._lib.maple_set_concurrency(self._h, int(bool(enable))))
@@ -267,6 +273,38 @@ class HomogenizationContext:
 def launch_count() -> int:
     """Kernels launched by libmaple_b200 in this process so far."""
     return int(_lib.load().maple_launch_count())
+
+
+SYMMETRY_KINDS = {"none": _lib.SYM_NONE, "mirror": _lib.SYM_MIRROR, "cubic": _lib.SYM_CUBIC}
+
+
+def _sym_args(kind: str, axes) -> tuple:
+    if kind not in SYMMETRY_KINDS:
+        raise ValueError(f"Unknown symmetry kind: {kind}")
+    mask = 0
+    for a in axes or []:
+        if int(a) not in (0, 1, 2):
+            raise ValueError(f"symmetry axes are 0, 1, 2; got {a}")
+        mask |= 1 << int(a)
+    if kind == "mirror" and mask == 0:
+        raise ValueError("mirror symmetry needs at least one axis")
+    return SYMMETRY_KINDS[kind], mask
+
+
+def symmetrize(x: torch.Tensor, r: int, kind: str, axes=()) -> torch.Tensor:
+    """Symmetry projection of (B, r^3) float64 CUDA element fields: "mirror"
+    about the centre planes of `axes` (0 = x, 1 = y, 2 = z) or the 48-map
+    "cubic" group (main_IHD_v3.py:259-337)."""
+    if x.dtype != torch.float64 or not x.is_cuda or not x.is_contiguous():
+        raise ValueError("symmetrize needs a contiguous float64 CUDA tensor")
+    B = x.numel() // (r ** 3)
+    if B * r ** 3 != x.numel():
+        raise ValueError(f"input size {x.numel()} is not a multiple of r^3={r ** 3}")
+    k, mask = _sym_args(kind, axes)
+    out = torch.empty_like(x)
+    with torch.cuda.device(x.device):
+        _lib.check(_lib.load().maple_symmetrize(int(r), int(B), k, mask, _ptr(x), _ptr(out), _stream(x.device)))
+    return out
 
 
 def box_filter(x: torch.Tensor, r: int, k: int = 3) -> torch.Tensor:

@@ -1653,6 +1653,87 @@ __global__ void k_energy_contract(const double* __restrict__ energy, const doubl
   out[i] = accumulate ? out[i] + s : s;
 }
 
+// Symmetry projection of element fields (main_IHD_v3.py:259-337): the mean of
+// the field over a group of cube maps, voxel index i reflecting to n-1-i.
+// kind 1 (mirror): the reflections about the centre planes of the axes in
+// mask (bit 0 = x, 1 = y, 2 = z); kind 2 (cubic): all 48 axis permutations and
+// reflections.  With clamp, inputs are clamped to [lo, hi] before averaging
+// and the mean after it (the clamps around the projection of the OC loop).
+enum { SYM_NONE = 0, SYM_MIRROR = 1, SYM_CUBIC = 2 };
+
+__global__ void k_symmetrize(const double* __restrict__ in, double* __restrict__ out, int n, int kind, int mask,
+                             int clamp, double lo, double hi, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n;
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  const int c[3] = {v / (n * n), (v / n) % n, v % n};
+  const double* src = in + (size_t)b * N;
+  auto at = [&](int a0, int a1, int a2) {
+    const double t = src[(a0 * n + a1) * n + a2];
+    return clamp ? fmin(fmax(t, lo), hi) : t;
+  };
+  double acc = 0.0;
+  int cnt = 0;
+  if (kind == SYM_MIRROR) {
+    for (int f = 0; f < 8; ++f) {
+      if (f & ~mask) continue;
+      acc += at((f & 1) ? n - 1 - c[0] : c[0], (f & 2) ? n - 1 - c[1] : c[1], (f & 4) ? n - 1 - c[2] : c[2]);
+      ++cnt;
+    }
+  } else if (kind == SYM_CUBIC) {
+    constexpr int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+#pragma unroll 1
+    for (int p = 0; p < 6; ++p) {
+      const int q0 = c[perm[p][0]], q1 = c[perm[p][1]], q2 = c[perm[p][2]];
+#pragma unroll
+      for (int f = 0; f < 8; ++f)
+        acc += at((f & 1) ? n - 1 - q0 : q0, (f & 2) ? n - 1 - q1 : q1, (f & 4) ? n - 1 - q2 : q2);
+    }
+    cnt = 48;
+  } else {
+    acc = at(c[0], c[1], c[2]);
+    cnt = 1;
+  }
+  double r = acc / cnt;
+  if (clamp) r = fmin(fmax(r, lo), hi);
+  out[(size_t)b * N + v] = r;
+}
+
+// per-cell max |x1 - x0| and mean |x1 - x0| into stats [B][2]; one CTA per cell
+__global__ void __launch_bounds__(1024) k_dx_stats(const double* __restrict__ x0, const double* __restrict__ x1,
+                                                   double* __restrict__ stats, int N, const int* active) {
+  const int b = blockIdx.x;
+  if (active && !active[b]) return;
+  __shared__ double smax[32], ssum[32];
+  double mx = 0.0, sm = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const double d = fabs(x1[(size_t)b * N + i] - x0[(size_t)b * N + i]);
+    mx = fmax(mx, d);
+    sm += d;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+    sm += __shfl_down_sync(0xffffffffu, sm, off);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smax[warp] = mx;
+    ssum[warp] = sm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0, t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      m = fmax(m, smax[w]);
+      t += ssum[w];
+    }
+    stats[2 * b] = m;
+    stats[2 * b + 1] = t / N;
+  }
+}
+
 // periodic k^3 box mean (main_IHD_v3.py:342-359)
 __global__ void k_box_filter(const double* __restrict__ in, double* __restrict__ out, int n, int kf, const int* active) {
   const int b = blockIdx.y;

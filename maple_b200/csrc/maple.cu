@@ -165,7 +165,7 @@ struct maple_ctx {
   std::vector<int> h_active;
   maple::Lane lanes[2];           // per-solve scratch, one lane per physics
   // OC step buffers
-  double *x_rho = nullptr, *dJdx = nullptr, *dJf = nullptr, *Jv = nullptr, *terms = nullptr, *G3 = nullptr,
+  double *x_sym = nullptr, *dJdx = nullptr, *dJf = nullptr, *Jv = nullptr, *terms = nullptr, *G3 = nullptr,
          *G1 = nullptr, *stats = nullptr, *ocpart = nullptr, *ocvf = nullptr;
   unsigned* bar = nullptr;
   int* err = nullptr;
@@ -180,6 +180,7 @@ struct maple_ctx {
   cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
   bool use_graphs = true;
   bool concurrent = true;  // elastic and thermal solves of an OC step on two streams
+  int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
   // per-kernel-class event timing of fine-level launches (bench instrumentation)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -1067,7 +1068,7 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
       c->active = dnew<int>(c, B);
       c->h_active.assign(B, 1);
       CK(cudaMemcpy(c->active, c->h_active.data(), B * sizeof(int), cudaMemcpyHostToDevice));
-      c->x_rho = dnew<double>(c, (size_t)B * N0);
+      c->x_sym = dnew<double>(c, (size_t)B * N0);  // projected design of a symmetric OC step
       c->dJdx = dnew<double>(c, (size_t)B * N0);
       c->dJf = dnew<double>(c, (size_t)B * N0);
       c->Jv = dnew<double>(c, B);
@@ -1169,6 +1170,29 @@ int maple_ctx_info(const maple_ctx* c, int* levels, int* coarsest, size_t* bytes
     if (levels) *levels = c->L;
     if (coarsest) *coarsest = c->n[c->L - 1];
     if (bytes) *bytes = c->bytes;
+  });
+}
+
+int maple_set_symmetry(maple_ctx* c, int kind, int axes_mask) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(kind == MAPLE_SYM_NONE || kind == MAPLE_SYM_MIRROR || kind == MAPLE_SYM_CUBIC, "unknown symmetry kind");
+    require(kind != MAPLE_SYM_MIRROR || (axes_mask > 0 && axes_mask < 8), "mirror symmetry needs axes (mask 1..7)");
+    c->sym_kind = kind;
+    c->sym_mask = kind == MAPLE_SYM_MIRROR ? axes_mask : (kind == MAPLE_SYM_CUBIC ? 7 : 0);
+  });
+}
+
+int maple_symmetrize(int r, int ncells, int kind, int axes_mask, const double* in, double* out, maple_stream_t s) {
+  return guarded([&] {
+    require(in != nullptr && out != nullptr, "NULL argument");
+    require(in != out, "out must not alias in");
+    require(r >= 1 && ncells >= 1, "bad sizes");
+    require(kind == MAPLE_SYM_NONE || kind == MAPLE_SYM_MIRROR || kind == MAPLE_SYM_CUBIC, "unknown symmetry kind");
+    require(kind != MAPLE_SYM_MIRROR || (axes_mask > 0 && axes_mask < 8), "mirror symmetry needs axes (mask 1..7)");
+    const size_t N = (size_t)r * r * r;
+    k_symmetrize<<<g2(N, ncells), kThreads, 0, S(s)>>>(in, out, r, kind, axes_mask, 0, 0.0, 0.0, nullptr);
+    CKL();
   });
 }
 
@@ -1443,13 +1467,21 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       need_ch |= (hw[3 * b] != 0.0 || hw[3 * b + 1] != 0.0);
       need_k |= (hw[3 * b + 2] != 0.0);
     }
+    // symmetric designs: the solves see clamp(P(clamp(x))) (main_IHD_v3.py:625-626)
+    const bool sym = c->sym_kind != SYM_NONE;
+    const double* xu = x;
+    if (sym) {
+      KL(c, st, k_symmetrize<<<g2(N, B), kThreads, 0, st>>>(x, c->x_sym, c->n[0], c->sym_kind, c->sym_mask, 1, xmin,
+                                                           1.0, c->active));
+      xu = c->x_sym;
+    }
     // one physics: SIMP map, hierarchy, RHS, MG-PCG solve, energies
     auto run_phys = [&](int phys, cudaStream_t ps, int* it_out) {
       LaneScope lane(phys);
       Phys& p = c->ph[phys];
       const size_t tot = (size_t)B * N;
-      KL(c, ps, k_simp<<<nblk(tot), kThreads, 0, ps>>>(x, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr, tot,
-                                                       N, xmin, penal, rho_min, c->active));
+      KL(c, ps, k_simp<<<nblk(tot), kThreads, 0, ps>>>(xu, p.o64.rho, prec == MAPLE_MIXED ? p.o32.rho : nullptr,
+                                                       tot, N, xmin, penal, rho_min, c->active));
       build(c, phys, prec, ps);
       assemble_rhs(c, phys, p.o64.rho, p.F64, ps);
       const bool was_solved = p.solved;
@@ -1500,16 +1532,27 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
     for (int b = 0; b < B; ++b) it_sum[b] = it_el[b] + it_th[b];
     KL(c, st, k_objective<<<nblk(B), kThreads, 0, st>>>(c->ph[0].H, c->ph[1].H, w, c->Jv, c->terms, c->G3, c->G1, B,
                                               need_ch ? 1 : 0, need_k ? 1 : 0, c->active));
-    KL(c, st, k_sensitivity<<<g2(N, B), kThreads, 0, st>>>(x, need_ch ? c->ph[0].energy : nullptr,
+    KL(c, st, k_sensitivity<<<g2(N, B), kThreads, 0, st>>>(xu, need_ch ? c->ph[0].energy : nullptr,
                                                  need_k ? c->ph[1].energy : nullptr, c->G3, c->G1, c->dJdx, nullptr, N,
                                                  xmin, penal, rho_min, c->active));
-    const double* dJ = c->dJdx;
+    double *dJ = c->dJdx, *spare = c->dJf;
+    if (sym) {  // the gradient through the (self-adjoint) projection
+      KL(c, st, k_symmetrize<<<g2(N, B), kThreads, 0, st>>>(dJ, spare, c->n[0], c->sym_kind, c->sym_mask, 0, 0.0,
+                                                           0.0, c->active));
+      std::swap(dJ, spare);
+    }
     if (filter_k > 1) {
       require(filter_k % 2 == 1, "filter size must be odd");
-      KL(c, st, k_box_filter<<<g2(N, B), kThreads, 0, st>>>(c->dJdx, c->dJf, c->n[0], filter_k, c->active));
-      dJ = c->dJf;
+      KL(c, st, k_box_filter<<<g2(N, B), kThreads, 0, st>>>(dJ, spare, c->n[0], filter_k, c->active));
+      std::swap(dJ, spare);
     }
     oc_update(c, x, dJ, vf, move, xmin, x_next, c->stats, st);
+    if (sym) {  // x_next = clamp(P(x_new)), statistics of x_next - x (main_IHD_v3.py:695-700)
+      KL(c, st, k_symmetrize<<<g2(N, B), kThreads, 0, st>>>(x_next, c->x_sym, c->n[0], c->sym_kind, c->sym_mask, 1,
+                                                           xmin, 1.0, c->active));
+      CK(cudaMemcpyAsync(x_next, c->x_sym, (size_t)B * N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      KL(c, st, k_dx_stats<<<B, 1024, 0, st>>>(x, x_next, c->stats, N, c->active));
+    }
     if (J) CK(cudaMemcpyAsync(J, c->Jv, B * sizeof(double), cudaMemcpyDeviceToDevice, st));
     if (terms) CK(cudaMemcpyAsync(terms, c->terms, 3 * B * sizeof(double), cudaMemcpyDeviceToDevice, st));
     if (CH && need_ch) CK(cudaMemcpyAsync(CH, c->ph[0].H, 36 * B * sizeof(double), cudaMemcpyDeviceToDevice, st));

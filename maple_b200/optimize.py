@@ -23,7 +23,7 @@ from typing import Dict, Optional, Tuple
 import numpy as np
 import torch
 
-from .core import box_filter
+from .core import box_filter, symmetrize
 from .model import IHD
 from .objective import (objective_from_spec, objective_requires, objective_weights, shear_objective,
                         stiffness_objective, thermal_objective)
@@ -82,6 +82,37 @@ def avg_filter3d_x_periodic(x_vec: torch.Tensor, elem_coords: torch.Tensor, res:
     vol = torch.empty(res ** 3, dtype=torch.float64, device=x_vec.device)
     vol[order] = x_vec.reshape(-1).to(torch.float64)
     out = box_filter(vol.reshape(1, -1).contiguous(), res, int(k)).reshape(-1)
+    return out[order].reshape(-1, 1).to(x_vec.dtype)
+
+
+def parse_symmetry(symmetry: str):
+    """(kind, axes) of a symmetry spec, as main_IHD_v3.py:221-256: "none";
+    "mirror" with the x/y/z letters present ("octant", "1/8", "one_eighth" =
+    all three); "cubic" for "cubic", "iso", "isotropic"."""
+    sym = (symmetry or "none").lower().strip()
+    if sym in ("none", ""):
+        return "none", []
+    if sym in ("octant", "1/8", "one_eighth"):
+        sym = "xyz"
+    if sym in ("cubic", "iso", "isotropic"):
+        return "cubic", [0, 1, 2]
+    axes = sorted({i for i, ch in enumerate("xyz") if ch in sym})
+    return ("mirror", axes) if axes else ("none", [])
+
+
+def symmetrize_vec(x_vec: torch.Tensor, elem_coords: torch.Tensor, res: int, kind: str, axes) -> torch.Tensor:
+    """Symmetry projection of an (N,1) design laid out by elem_coords
+    (main_IHD_v3.py:329-337), as a CUDA kernel."""
+    if kind == "none":
+        return x_vec.reshape(-1, 1)
+    if kind not in ("mirror", "cubic"):
+        raise ValueError(f"Unknown symmetry kind: {kind}")
+    if kind == "mirror" and not axes:
+        return x_vec.reshape(-1, 1)
+    order = _canonical_order(elem_coords, res).to(x_vec.device)
+    vol = torch.empty(res ** 3, dtype=torch.float64, device=x_vec.device)
+    vol[order] = x_vec.reshape(-1).to(torch.float64)
+    out = symmetrize(vol.reshape(1, -1).contiguous(), res, kind, axes).reshape(-1)
     return out[order].reshape(-1, 1).to(x_vec.dtype)
 
 
@@ -179,15 +210,14 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
                                     dx_tol: float = 0.01) -> RunResult:
     """OC loop of main_IHD_v3.py:492-891 on the GPU.
 
-    Same arguments and outputs as the reference.  Supported: symmetry "none"
-    and lambda_print = lambda_cavity = 0 (the manufacturability penalties are
-    not part of this package).  Extra keywords: ``x_init`` (an (N,1) design to
+    Same arguments and outputs as the reference.  Supported: every symmetry
+    ("none", mirror axes, "cubic"/"iso") and lambda_print = lambda_cavity = 0
+    (the manufacturability penalties are not part of this package).  Extra keywords: ``x_init`` (an (N,1) design to
     start from, bypassing ``init_mode``), ``precision``/``rtol`` (default: the
     IHD module's), ``stop_rule`` "reference" (stall test of
     main_IHD_v3.py:611-618, 711-714) or "dx" (stop when max|dx| < dx_tol).
     """
-    if str(symmetry).lower() != "none":
-        raise NotImplementedError("symmetry projections other than 'none' are not supported")
+    sym_kind, sym_axes = parse_symmetry(symmetry)
     if float(lambda_print) > 0 or float(lambda_cavity) > 0:
         raise NotImplementedError("printability / cavity penalties are not supported (use lambda = 0)")
     device = ihd_module.device
@@ -212,6 +242,8 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
         if volfrac <= 0:
             volfrac = float(x.mean().item())
     x = x.clamp(xmin, 1.0).reshape(1, -1).contiguous()
+    if sym_kind != "none":
+        x = symmetrize(x, res, sym_kind, sym_axes).clamp(xmin, 1.0).contiguous()
 
     def simp(xv):
         return (rho_min + (1.0 - rho_min) * (xv.clamp(xmin, 1.0) ** penal)).reshape(-1, 1).clamp(rho_min, 1.0)
@@ -224,6 +256,7 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
                                     "dx_mean", "time_sec"])
 
     hc = ihd_module.homog_ctx
+    hc.set_symmetry(sym_kind, sym_axes)
     w = torch.tensor([objective_weights(objective)], dtype=torch.float64, device=device)
     vf = torch.tensor([float(volfrac)], dtype=torch.float64, device=device)
     t0 = time.time()
@@ -259,6 +292,7 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
             converged = True
             break
 
+    hc.set_symmetry("none")
     rho_final = simp(x)
     J_raw_final = evaluate_J(ihd_module, batch, rho_final, obj=objective)
     rho_final_grid = rho_final.reshape(res, res, res).detach().cpu().numpy().astype(np.float32)

@@ -532,14 +532,56 @@ def solve_cell(rho: np.ndarray, r: int, elems: Elements | None = None, levels: i
     return out
 
 
+def parse_symmetry(symmetry: str):
+    """(kind, axes) of a symmetry spec (main_IHD_v3.py:221-256): "none";
+    "mirror" with the sorted axes named by x/y/z letters ("octant", "1/8",
+    "one_eighth" mean all three); "cubic" for "cubic", "iso", "isotropic"."""
+    sym = (symmetry or "none").lower().strip()
+    if sym in ("none", ""):
+        return "none", []
+    if sym in ("octant", "1/8", "one_eighth"):
+        sym = "xyz"
+    if sym in ("cubic", "iso", "isotropic"):
+        return "cubic", [0, 1, 2]
+    axes = sorted({i for i, ch in enumerate("xyz") if ch in sym})
+    return ("mirror", axes) if axes else ("none", [])
+
+
+def symmetrize(v: np.ndarray, r: int, kind: str, axes) -> np.ndarray:
+    """Group average of an element field (main_IHD_v3.py:259-337): mirror =
+    mean over the reflections about the centre planes of `axes`; cubic = mean
+    over the 48 axis permutations and reflections.  Index i reflects to r-1-i."""
+    if kind == "none":
+        return v.reshape(-1).copy()
+    vol = v.reshape(r, r, r)
+    if kind == "mirror":
+        out = vol
+        for ax in axes:
+            out = 0.5 * (out + np.flip(out, axis=ax))
+        return np.ascontiguousarray(out).reshape(-1)
+    if kind == "cubic":
+        import itertools
+        acc = np.zeros_like(vol)
+        for p in itertools.permutations((0, 1, 2)):
+            w = np.transpose(vol, p)
+            for f in itertools.product((0, 1), repeat=3):
+                dims = tuple(i for i in range(3) if f[i])
+                acc += np.flip(w, axis=dims) if dims else w
+        return (acc / 48.0).reshape(-1)
+    raise ValueError(f"Unknown symmetry kind: {kind}")
+
+
 def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal: float = 3.0,
                  rho_min: float = 1e-9, move: float = 0.2, xmin: float = 1e-3, filter_k: int = 3,
                  elems: Elements | None = None, levels: int = 3, rtol: float = 1e-12,
-                 max_cycles: int = 200):
-    """One OC iteration of main_IHD_v3.py:620-716 (symmetry none, no penalties)
-    with the analytic adjoint in place of autograd.  Returns (x_next, info)."""
+                 max_cycles: int = 200, symmetry: str = "none"):
+    """One OC iteration of main_IHD_v3.py:620-716 (no penalties) with the
+    analytic adjoint in place of autograd.  With a symmetry, the solve uses the
+    projected design, the gradient is projected (the group average is
+    self-adjoint) and so is the updated design.  Returns (x_next, info)."""
+    kind, axes = parse_symmetry(symmetry)
     x = x.reshape(-1)
-    xc = np.clip(x, xmin, 1.0)
+    xc = np.clip(symmetrize(np.clip(x, xmin, 1.0), r, kind, axes), xmin, 1.0)
     rho = rho_min + (1.0 - rho_min) * xc ** penal
     phys = []
     if any(t in ("stiffness", "shear") for t in weights):
@@ -556,11 +598,11 @@ def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal:
         dJdrho += np.einsum("eij,ij->e", res["dCH"], gC)
     if kap is not None:
         dJdrho += np.einsum("eij,ij->e", res["dkappa"], gK)
-    dJdx = dJdrho * penal * (1.0 - rho_min) * xc ** (penal - 1.0)
+    dJdx = symmetrize(dJdrho * penal * (1.0 - rho_min) * xc ** (penal - 1.0), r, kind, axes)
     if filter_k and filter_k > 1:
         dJdx = box_filter_periodic(dJdx, r, filter_k)
     x_new = oc_update(x, dJdx, volfrac, move, xmin)
-    x_next = np.clip(x_new, xmin, 1.0)
+    x_next = np.clip(symmetrize(x_new, r, kind, axes), xmin, 1.0)
     info = dict(J=J, CH=CH, kappa=kap, dJdx=dJdx, dx_max=float(np.abs(x_next - x).max()),
                 dx_mean=float(np.abs(x_next - x).mean()), res=res)
     return x_next, info

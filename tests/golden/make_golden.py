@@ -64,7 +64,7 @@ def seed_density(seed, r, sigma, vf, scale=0.25, xmin=1e-3):
     return x
 
 
-def main(src):
+def main(src, only=None):
     M, U, Mo, Ob, GMGSolver, GMGSolverScalar = _import_reference(src)
     # torch's default dtype stays float32: the reference's
     # isotropic_elastic_tensor (utils/_utils.py:42) relies on it
@@ -119,6 +119,9 @@ def main(src):
             out["F_elastic"] = F.detach().numpy()
             out["F_thermal"] = Ft.detach().numpy()
         return out
+
+    if only == "symmetry":
+        return symmetry_fixtures(M, Ob, homogenize, dev)
 
     rec = {}
     # ---------------------------------------------------------------- tables
@@ -217,5 +220,48 @@ def main(src):
     np.savez_compressed(os.path.join(HERE, "traj_r8.npz"), **traj)
 
 
+def symmetry_fixtures(M, Ob, homogenize, dev):
+    """sym.npz: parse_symmetry on several spellings, symmetrize_vec of a random
+    8^3 field for each kind, and 3-iteration 8^3 OC trajectories with cubic and
+    "xy" mirror symmetry built from the reference's own pieces
+    (main_IHD_v3.py:620-716 with lambda_print = lambda_cavity = 0)."""
+    rec = {}
+    for spec in ["none", "", "x", "xy", "yz", "xz", "xyz", "octant", "1/8", "cubic", "iso", "isotropic", "z"]:
+        kind, axes = M.parse_symmetry(spec)
+        rec["parse::" + spec] = np.array([kind] + [str(a) for a in axes])
+    r = 8
+    batch = M.build_unitcell_batch(dev, r, torch.zeros(r, r, r))
+    ec = batch["elem_coords"]
+    v = torch.tensor(np.random.default_rng(11).standard_normal((r ** 3, 1)))
+    rec["field"] = v.numpy().reshape(-1)
+    for spec in ["x", "xy", "yz", "xyz", "cubic"]:
+        kind, axes = M.parse_symmetry(spec)
+        rec["sym::" + spec] = M.symmetrize_vec(v, ec, res=r, kind=kind, axes=axes).numpy().reshape(-1)
+    vf, move, xmin, penal, rho_min, fk = 0.25, 0.2, 1e-3, 3.0, 1e-9, 3
+    spec_obj = "stiffness:0.5,thermal:0.5"
+    for spec in ["cubic", "xy"]:
+        kind, axes = M.parse_symmetry(spec)
+        x = torch.tensor(seed_density(0, r, 2.0, vf).reshape(-1, 1))
+        x = M.symmetrize_vec(x, ec, res=r, kind=kind, axes=axes).clamp(xmin, 1.0)
+        rec[f"traj_{spec}_x0"] = x.numpy().reshape(-1)
+        for it in range(3):
+            xv = x.detach().clone().requires_grad_(True)
+            xu = M.symmetrize_vec(xv.clamp(xmin, 1.0), ec, res=r, kind=kind, axes=axes).clamp(xmin, 1.0)
+            rv = rho_min + (1 - rho_min) * xu ** penal
+            o = homogenize(r, rv, 60, levels=3)
+            J = Ob.objective_from_spec(obj=spec_obj, CH=o["CH"], kappa=o["kappa"])
+            (g,) = torch.autograd.grad(J, xv)
+            g = M.avg_filter3d_x_periodic(g, ec, r, fk)
+            xn = M.oc_update(x.detach(), g.detach(), volfrac=vf, move=move, xmin=xmin)
+            xn = M.symmetrize_vec(xn, ec, res=r, kind=kind, axes=axes).clamp(xmin, 1.0)
+            rec[f"traj_{spec}_J{it}"] = J.item()
+            rec[f"traj_{spec}_x{it + 1}"] = xn.numpy().reshape(-1)
+            x = xn
+            print("sym traj", spec, it, J.item())
+    np.savez_compressed(os.path.join(HERE, "sym.npz"), **rec)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
+    only = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")), None)
+    main(args[0] if args else "/root/reference/src", only)

@@ -160,7 +160,7 @@ def test_optimize_inverse_homogenization(ihd8, golden, tmp_path):
     with pytest.raises(NotImplementedError):
         optimize_inverse_homogenization(
             ihd8, batch, res=8, objective="shear", init_mode="noise", volfrac=0.25, penal=3.0, rho_min=1e-9,
-            move=0.2, xmin=1e-3, iters=1, seed=0, symmetry="cubic", lambda_print=0.0, overhang_deg=45.0,
+            move=0.2, xmin=1e-3, iters=1, seed=0, symmetry="cubic", lambda_print=0.5, overhang_deg=45.0,
             lambda_cavity=0.0, cavity_thresh=0.5, cavity_beta=20.0, min_channel_rad=0, cavity_rad=1,
             cavity_seed_faces="all", cavity_iters=128, cavity_tiles=1, cavity_tiles_xyz=None,
             cavity_focus_center=True, filter_k=3, output_dir=str(tmp_path), mesh_every=0, mesh_res=32, mesh_iso=0.3,
@@ -186,3 +186,24 @@ def test_batched_cells_match_single_cell_runs(lib):
     res2 = oc_run(x0, w, vf, precision="mixed", rtol=1e-8, max_iters=40, dx_tol=0.02)
     assert res2.converged.any()
     assert (res2.iters_run <= 40).all() and (res2.iters_run >= 1).all()
+
+
+def test_optimize_with_symmetry_follows_reference(ihd8, golden, tmp_path):
+    """optimize_inverse_homogenization with symmetry "iso" (the cube group)
+    runs the reference's projected OC loop."""
+    from maple_b200.optimize import build_unitcell_batch, optimize_inverse_homogenization
+    g = golden("sym.npz")
+    batch = build_unitcell_batch(DEV, 8, torch.zeros(8, 8, 8, device=DEV))
+    res = optimize_inverse_homogenization(
+        ihd8, batch, res=8, objective="stiffness:0.5,thermal:0.5", init_mode="noise", volfrac=0.25, penal=3.0,
+        rho_min=1e-9, move=0.2, xmin=1e-3, iters=3, seed=0, symmetry="iso", lambda_print=0.0, overhang_deg=45.0,
+        lambda_cavity=0.0, cavity_thresh=0.5, cavity_beta=20.0, min_channel_rad=0, cavity_rad=1,
+        cavity_seed_faces="all", cavity_iters=128, cavity_tiles=1, cavity_tiles_xyz=None, cavity_focus_center=True,
+        filter_k=3, output_dir=str(tmp_path), mesh_every=0, mesh_res=32, mesh_iso=0.3, mesh_pad=2,
+        save_initial_mesh=False, verbose=False, x_init=torch.tensor(g["traj_cubic_x0"]), rtol=1e-12)
+    rows = list(csv.reader(open(os.path.join(tmp_path, "iter_log.csv"))))
+    for it in range(3):
+        ref = float(g[f"traj_cubic_J{it}"])
+        assert abs(float(rows[1 + it][2]) - ref) < 1e-8 * ref
+    assert res.iters_run == 3
+    assert ihd8.homog_ctx is not None

@@ -148,3 +148,36 @@ def test_solid_cell_known_answer():
     C = O.isotropic_elastic_tensor(1.0, 0.3)
     assert rel(res["CH"], C) < 1e-12
     assert rel(res["kappa"], np.eye(3)) < 1e-12
+
+
+def test_symmetry_parse_and_projection_match_reference(golden):
+    g = golden("sym.npz")
+    for key in g.files:
+        if key.startswith("parse::"):
+            spec = key.split("::", 1)[1]
+            kind, axes = O.parse_symmetry(spec)
+            assert [kind] + [str(a) for a in axes] == list(g[key]), spec
+    for spec in ["x", "xy", "yz", "xyz", "cubic"]:
+        kind, axes = O.parse_symmetry(spec)
+        out = O.symmetrize(g["field"], 8, kind, axes)
+        assert np.abs(out - g["sym::" + spec]).max() < 1e-14, spec
+        assert np.abs(O.symmetrize(out, 8, kind, axes) - out).max() < 1e-14  # a projection
+
+
+@pytest.mark.parametrize("spec", ["cubic", "xy"])
+def test_symmetric_trajectory_matches_reference(golden, spec):
+    g = golden("sym.npz")
+    x = g[f"traj_{spec}_x0"]
+    for it in range(3):
+        x, info = O.oc_iteration(x, 8, {"stiffness": 0.5, "thermal": 0.5}, volfrac=0.25, symmetry=spec, rtol=1e-12)
+        assert abs(info["J"] - g[f"traj_{spec}_J{it}"]) < 1e-8 * abs(g[f"traj_{spec}_J{it}"]), (spec, it)
+        assert np.abs(x - g[f"traj_{spec}_x{it + 1}"]).max() < 1e-7, (spec, it)
+
+
+def test_dropin_parse_symmetry_matches_reference(golden):
+    from maple_b200.optimize import parse_symmetry
+    g = golden("sym.npz")
+    for key in g.files:
+        if key.startswith("parse::"):
+            kind, axes = parse_symmetry(key.split("::", 1)[1])
+            assert [kind] + [str(a) for a in axes] == list(g[key])
