@@ -574,11 +574,14 @@ def symmetrize(v: np.ndarray, r: int, kind: str, axes) -> np.ndarray:
 def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal: float = 3.0,
                  rho_min: float = 1e-9, move: float = 0.2, xmin: float = 1e-3, filter_k: int = 3,
                  elems: Elements | None = None, levels: int = 3, rtol: float = 1e-12,
-                 max_cycles: int = 200, symmetry: str = "none"):
-    """One OC iteration of main_IHD_v3.py:620-716 (no penalties) with the
-    analytic adjoint in place of autograd.  With a symmetry, the solve uses the
-    projected design, the gradient is projected (the group average is
-    self-adjoint) and so is the updated design.  Returns (x_next, info)."""
+                 max_cycles: int = 200, symmetry: str = "none", lambda_print: float = 0.0,
+                 overhang_deg: float = 45.0, lambda_cavity: float = 0.0, cavity: dict | None = None):
+    """One OC iteration of main_IHD_v3.py:620-716 with the analytic adjoint in
+    place of autograd.  With a symmetry, the solve uses the projected design,
+    the gradient is projected (the group average is self-adjoint) and so is
+    the updated design.  Penalties (:649-686): J = J_raw - lambda_print *
+    P_overhang - lambda_cavity * P_cavity, `cavity` holding cavity_penalty's
+    keywords.  Returns (x_next, info)."""
     kind, axes = parse_symmetry(symmetry)
     x = x.reshape(-1)
     xc = np.clip(symmetrize(np.clip(x, xmin, 1.0), r, kind, axes), xmin, 1.0)
@@ -598,11 +601,204 @@ def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal:
         dJdrho += np.einsum("eij,ij->e", res["dCH"], gC)
     if kap is not None:
         dJdrho += np.einsum("eij,ij->e", res["dkappa"], gK)
+    J_raw = J
+    P_print = P_cav = 0.0
+    if lambda_print > 0:
+        P_print, gP = overhang_penalty(rho, r, overhang_deg, True)
+        J -= lambda_print * P_print
+        dJdrho = dJdrho - lambda_print * gP
+    if lambda_cavity > 0:
+        P_cav, gC = cavity_penalty(rho, r, **(cavity or {}))
+        J -= lambda_cavity * P_cav
+        dJdrho = dJdrho - lambda_cavity * gC
     dJdx = symmetrize(dJdrho * penal * (1.0 - rho_min) * xc ** (penal - 1.0), r, kind, axes)
     if filter_k and filter_k > 1:
         dJdx = box_filter_periodic(dJdx, r, filter_k)
     x_new = oc_update(x, dJdx, volfrac, move, xmin)
     x_next = np.clip(symmetrize(x_new, r, kind, axes), xmin, 1.0)
-    info = dict(J=J, CH=CH, kappa=kap, dJdx=dJdx, dx_max=float(np.abs(x_next - x).max()),
+    info = dict(J=J, J_raw=J_raw, P_print=P_print, P_cavity=P_cav, CH=CH, kappa=kap, dJdx=dJdx,
+                dx_max=float(np.abs(x_next - x).max()),
                 dx_mean=float(np.abs(x_next - x).mean()), res=res)
     return x_next, info
+
+
+# ---------------------------------------------------------------------------
+# Manufacturability penalties (utils/printability.py) with their gradients,
+# restated with the tie rules of the autograd the reference differentiates
+# them with: a max-pool window passes its gradient to the first maximum in
+# (x, y, z) scan order; torch.minimum splits it in half between equal
+# arguments; relu passes nothing at 0.
+# ---------------------------------------------------------------------------
+def _pool_windows(t: np.ndarray, rad: int, periodic: bool, pad_val: float):
+    """All (2 rad + 1)^d shifted views of t (d = t.ndim) in scan order, each
+    paired with the flat source index of every window element (-1 = padding)."""
+    d = t.ndim
+    n = t.shape
+    idx = np.arange(t.size).reshape(n)
+    if periodic:
+        tp = np.pad(t, rad, mode="wrap")
+        ip = np.pad(idx, rad, mode="wrap")
+    else:
+        tp = np.pad(t, rad, mode="constant", constant_values=pad_val)
+        ip = np.pad(idx, rad, mode="constant", constant_values=-1)
+    vals, srcs = [], []
+    import itertools
+    for off in itertools.product(range(2 * rad + 1), repeat=d):
+        sl = tuple(slice(o, o + n[k]) for k, o in enumerate(off))
+        vals.append(tp[sl])
+        srcs.append(ip[sl])
+    return np.stack(vals), np.stack(srcs)
+
+
+def max_pool(t: np.ndarray, rad: int, periodic: bool, pad_val: float = 0.0):
+    """(pooled, argmax source index) of a (2 rad+1)^d max pool over a padded
+    field: the first maximum in scan order wins (-1 if it is a pad cell)."""
+    if rad <= 0:
+        return t.copy(), np.arange(t.size).reshape(t.shape)
+    vals, srcs = _pool_windows(t, rad, periodic, pad_val)
+    k = np.argmax(vals, axis=0)
+    pooled = np.take_along_axis(vals, k[None], 0)[0]
+    src = np.take_along_axis(srcs, k[None], 0)[0]
+    return pooled, src
+
+
+def _pool_adjoint(g: np.ndarray, src: np.ndarray, size: int) -> np.ndarray:
+    out = np.zeros(size)
+    m = src.reshape(-1) >= 0
+    np.add.at(out, src.reshape(-1)[m], g.reshape(-1)[m])
+    return out
+
+
+def _minimum_grads(a, b, g):
+    """Gradients of torch.minimum(a, b) for upstream g (ties split in half)."""
+    ga = np.where(a == b, g / 2, g) * (a <= b)
+    gb = np.where(a == b, g / 2, g) * (b <= a)
+    return ga, gb
+
+
+def support_radius(overhang_deg: float) -> int:
+    """Lateral support radius per layer for an overhang angle from the plate
+    (utils/printability.py:76-90): ceil(tan(90 - deg)), at least 1."""
+    od = float(np.clip(overhang_deg, 1.0, 89.0))
+    return max(1, int(np.ceil(float(np.tan(np.deg2rad(90.0 - od))))))
+
+
+def overhang_penalty(rho: np.ndarray, r: int, overhang_deg: float = 45.0, periodic_xy: bool = True):
+    """(P, dP/drho) of printability_penalty_overhang (utils/printability.py:
+    91-134): build direction +z; support(0) = rho(:,:,0); per layer z
+    s = maxpool_xy(support(z-1)), P += mean(relu(rho_z - s)),
+    support(z) = min(rho_z, s); P /= r - 1."""
+    g = rho.reshape(r, r, r)
+    rad = support_radius(overhang_deg)
+    sup = g[:, :, 0].copy()
+    tape = []
+    P = 0.0
+    for z in range(1, r):
+        s, src = max_pool(sup, rad, periodic_xy, 0.0)
+        rz = g[:, :, z]
+        P += np.maximum(rz - s, 0.0).mean()
+        tape.append((s, src, rz))
+        sup = np.minimum(rz, s)
+    den = max(r - 1, 1)
+    P /= den
+    grad = np.zeros((r, r, r))
+    gsup = np.zeros((r, r))  # gradient arriving at support(z)
+    for z in range(r - 1, 0, -1):
+        s, src, rz = tape[z - 1]
+        grz, gs = _minimum_grads(rz, s, gsup)
+        act = (rz - s) > 0
+        grz = grz + act / (r * r) / den
+        gs = gs - act / (r * r) / den
+        grad[:, :, z] += grz
+        gsup = _pool_adjoint(gs, src, r * r).reshape(r, r)
+    grad[:, :, 0] += gsup
+    return P, grad.reshape(-1)
+
+
+SEED_FACES = ("all", "x", "y", "z", "xy")
+
+
+def _seed_mask(shape, seed_faces: str) -> np.ndarray:
+    sf = str(seed_faces).lower()
+    if sf not in SEED_FACES:
+        raise ValueError("seed_faces must be one of: all, x, y, z, xy")
+    seed = np.zeros(shape)
+    if sf in ("all", "x"):
+        seed[0], seed[-1] = 1, 1
+    if sf in ("all", "y"):
+        seed[:, 0], seed[:, -1] = 1, 1
+    if sf in ("all", "z", "xy"):
+        seed[:, :, 0], seed[:, :, -1] = 1, 1
+    return seed
+
+
+def _cavity(void: np.ndarray, periodic: bool, min_channel_rad: int, rad: int, nsteps: int, seed_faces: str):
+    """Trapped-void field relu(void - reach) of the flood fill (utils/
+    printability.py:199-220, 293-314) and a backward closure mapping its
+    upstream gradient to d/dvoid."""
+    shape = void.shape
+    size = void.size
+    if min_channel_rad > 0:
+        er_neg, er_src = max_pool(-void, min_channel_rad, periodic, -1.0)  # erosion = -maxpool(-x), pad 1
+        er = -er_neg
+        vconn, di_src = max_pool(er, min_channel_rad, periodic, 0.0)       # dilation, pad 0
+    else:
+        vconn = void
+    seed = _seed_mask(shape, seed_faces)
+    reach = vconn * seed
+    steps = []
+    if rad > 0:
+        for _ in range(nsteps):
+            dil, src = max_pool(reach, rad, periodic, 0.0)
+            steps.append((dil, src))
+            reach = np.minimum(vconn, dil)
+    trapped = np.maximum(void - reach, 0.0)
+
+    def backward(gt: np.ndarray) -> np.ndarray:
+        act = (void - reach) > 0
+        gvoid = gt * act
+        greach = -gt * act
+        gvconn = np.zeros(shape)
+        for dil, src in reversed(steps):
+            gv, gd = _minimum_grads(vconn, dil, greach)
+            gvconn += gv
+            greach = _pool_adjoint(gd, src, size).reshape(shape)
+        gvconn += greach * seed
+        if min_channel_rad > 0:
+            ger = _pool_adjoint(gvconn, di_src, size).reshape(shape)
+            gvoid += _pool_adjoint(ger, er_src, size).reshape(shape)   # d(-maxpool(-x)) routes +g to the argmin
+        else:
+            gvoid += gvconn
+        return gvoid
+
+    return trapped, backward
+
+
+def cavity_penalty(rho: np.ndarray, r: int, *, void_thresh: float = 0.5, beta: float = 20.0, min_channel_rad: int = 0,
+                   rad: int = 1, iters: int = 0, tiles=(1, 1, 1), focus_center: bool = True,
+                   seed_faces: str = "all"):
+    """(P, dP/drho) of cavity_penalty_closed_void (tiles (1,1,1), periodic
+    flood fill; utils/printability.py:139-220) or cavity_penalty_periodic_array
+    (tiles > 1: the cell tiled into a supercell with the supercell boundary as
+    the only outside, non-periodic; :226-323)."""
+    g = rho.reshape(r, r, r)
+    tx, ty, tz = (max(1, int(t)) for t in tiles)
+    array = max(tx, ty, tz) > 1
+    s = 1.0 / (1.0 + np.exp(-float(beta) * (float(void_thresh) - g)))
+    void = np.tile(s, (tx, ty, tz)) if array else s
+    nsteps = int(iters) if int(iters) > 0 else (max(void.shape) if array else r)
+    trapped, backward = _cavity(void, not array, int(max(0, min_channel_rad)), int(max(0, rad)), nsteps, seed_faces)
+    if array and focus_center and tx >= 3 and ty >= 3 and tz >= 3:
+        cx, cy, cz = tx // 2, ty // 2, tz // 2
+        sl = (slice(cx * r, (cx + 1) * r), slice(cy * r, (cy + 1) * r), slice(cz * r, (cz + 1) * r))
+        P = trapped[sl].mean()
+        gt = np.zeros(trapped.shape)
+        gt[sl] = 1.0 / (r ** 3)
+    else:
+        P = trapped.mean()
+        gt = np.full(trapped.shape, 1.0 / trapped.size)
+    gvoid = backward(gt)
+    if array:
+        gvoid = gvoid.reshape(tx, r, ty, r, tz, r).sum(axis=(0, 2, 4))
+    grad = gvoid * (-float(beta)) * s * (1.0 - s)
+    return float(P), grad.reshape(-1)

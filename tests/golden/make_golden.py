@@ -24,6 +24,7 @@ What is recorded (all FP64):
 """
 from __future__ import annotations
 
+import json
 import os
 import sys
 import types
@@ -122,6 +123,8 @@ def main(src, only=None):
 
     if only == "symmetry":
         return symmetry_fixtures(M, Ob, homogenize, dev)
+    if only == "print":
+        return printability_fixtures(M, Ob, homogenize, dev, src)
 
     rec = {}
     # ---------------------------------------------------------------- tables
@@ -218,6 +221,79 @@ def main(src, only=None):
         x = xn
         print("traj it", it, "J", J.item())
     np.savez_compressed(os.path.join(HERE, "traj_r8.npz"), **traj)
+
+
+def printability_fixtures(M, Ob, homogenize, dev, src):
+    """print.npz: the reference's printability / cavity penalties
+    (utils/printability.py) and their autograd gradients w.r.t. rho on two 8^3
+    fields (one continuous, one clipped SIMP design full of exact ties), and a
+    3-iteration OC trajectory with both penalties (lambda 0.9 each, the
+    experiment scripts' values) from the reference's own pieces."""
+    from maple.core.utils import printability as Pr
+    r = 8
+    rng = np.random.default_rng(21)
+    fields = {
+        "cont": rng.random(r ** 3),
+        "simp": 1e-9 + (1 - 1e-9) * np.clip(seed_density(3, r, 1.5, 0.3) + 0.3 * rng.standard_normal(r ** 3)
+                                             .reshape(r, r, r), 1e-3, 1.0).reshape(-1) ** 3,
+    }
+    rec = {}
+    cases = []
+    for deg in (45.0, 20.0):
+        for per in (True, False):
+            cases.append(("over", dict(overhang_deg=deg, periodic_xy=per)))
+    closed = [dict(), dict(min_channel_rad=1), dict(rad=0), dict(rad=2, iters=3), dict(seed_faces="x"),
+              dict(seed_faces="xy", void_thresh=0.3, beta=10.0), dict(periodic_xyz=False, min_channel_rad=1)]
+    for kw in closed:
+        cases.append(("closed", kw))
+    arrays = [dict(tiles_xyz=(2, 2, 2), min_channel_rad=1), dict(tiles_xyz=(2, 2, 2), min_channel_rad=3),
+              dict(tiles_xyz=(3, 3, 3), focus_center=True), dict(tiles_xyz=(3, 3, 3), focus_center=False, iters=5),
+              dict(tiles_xyz=(2, 1, 3), seed_faces="z")]
+    for kw in arrays:
+        cases.append(("array", kw))
+    for fname, f in fields.items():
+        rec[f"field_{fname}"] = f
+        for i, (kind, kw) in enumerate(cases):
+            rho = torch.tensor(f.reshape(r, r, r), requires_grad=True)
+            if kind == "over":
+                P = Pr.printability_penalty_overhang(rho, **kw)
+            elif kind == "closed":
+                P = Pr.cavity_penalty_closed_void(rho, **kw)
+            else:
+                P = Pr.cavity_penalty_periodic_array(rho, **kw)
+            (gr,) = torch.autograd.grad(P, rho)
+            rec[f"{fname}_{i}_P"] = P.item()
+            rec[f"{fname}_{i}_grad"] = gr.numpy().reshape(-1)
+    rec["cases"] = np.array([json.dumps([k, kw]) for k, kw in cases])
+    # OC trajectory with both penalties (main_IHD_v3.py:649-688)
+    vf, move, xmin, penal, rho_min, fk = 0.25, 0.2, 1e-3, 3.0, 1e-9, 3
+    lp, lc = 0.9, 0.9
+    spec_obj = "stiffness:0.5,thermal:0.5"
+    batch = M.build_unitcell_batch(dev, r, torch.zeros(r, r, r))
+    ec = batch["elem_coords"]
+    x = torch.tensor(seed_density(0, r, 2.0, vf).reshape(-1, 1))
+    rec["traj_x0"] = x.numpy().reshape(-1)
+    for it in range(3):
+        xv = x.detach().clone().requires_grad_(True)
+        rv = rho_min + (1 - rho_min) * xv.clamp(xmin, 1.0) ** penal
+        o = homogenize(r, rv, 60, levels=3)
+        J_raw = Ob.objective_from_spec(obj=spec_obj, CH=o["CH"], kappa=o["kappa"])
+        grid = rv.reshape(r, r, r)
+        Pp = Pr.printability_penalty_overhang(grid, overhang_deg=45.0, periodic_xy=True)
+        Pc = Pr.cavity_penalty_periodic_array(grid, tiles_xyz=(2, 2, 2), focus_center=True, void_thresh=0.5,
+                                              beta=20.0, min_channel_rad=1, rad=1, iters=0, seed_faces="all")
+        J = J_raw - lp * Pp - lc * Pc
+        (g,) = torch.autograd.grad(J, xv)
+        g = M.avg_filter3d_x_periodic(g, ec, r, fk)
+        xn = M.oc_update(x.detach(), g.detach(), volfrac=vf, move=move, xmin=xmin).clamp(xmin, 1.0)
+        rec[f"traj_J{it}"] = J.item()
+        rec[f"traj_Jraw{it}"] = J_raw.item()
+        rec[f"traj_Pp{it}"] = Pp.item()
+        rec[f"traj_Pc{it}"] = Pc.item()
+        rec[f"traj_x{it + 1}"] = xn.numpy().reshape(-1)
+        x = xn
+        print("print traj", it, J.item(), Pp.item(), Pc.item())
+    np.savez_compressed(os.path.join(HERE, "print.npz"), **rec)
 
 
 def symmetry_fixtures(M, Ob, homogenize, dev):

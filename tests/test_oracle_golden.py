@@ -181,3 +181,50 @@ def test_dropin_parse_symmetry_matches_reference(golden):
         if key.startswith("parse::"):
             kind, axes = parse_symmetry(key.split("::", 1)[1])
             assert [kind] + [str(a) for a in axes] == list(g[key])
+
+
+def _print_case(kind, kw, rho, r=8):
+    """Oracle call for one fixture case (reference keyword names)."""
+    if kind == "over":
+        return O.overhang_penalty(rho, r, kw.get("overhang_deg", 45.0), kw.get("periodic_xy", True))
+    tiles = tuple(kw.get("tiles_xyz", (1, 1, 1)))
+    if kind == "closed" and not kw.get("periodic_xyz", True):
+        pytest.skip("non-periodic single-cell flood fill is not on the optimizer's path")
+    return O.cavity_penalty(rho, r, void_thresh=kw.get("void_thresh", 0.5), beta=kw.get("beta", 20.0),
+                            min_channel_rad=kw.get("min_channel_rad", 0), rad=kw.get("rad", 1),
+                            iters=kw.get("iters", 0), tiles=tiles, focus_center=kw.get("focus_center", True),
+                            seed_faces=kw.get("seed_faces", "all"))
+
+
+def _print_cases(golden):
+    import json
+    g = golden("print.npz")
+    return g, [json.loads(c) for c in g["cases"]]
+
+
+@pytest.mark.parametrize("field", ["cont", "simp"])
+def test_printability_penalties_match_reference_autograd(golden, field):
+    g, cases = _print_cases(golden)
+    rho = g[f"field_{field}"]
+    for i, (kind, kw) in enumerate(cases):
+        if kind == "closed" and not kw.get("periodic_xyz", True):
+            continue
+        P, grad = _print_case(kind, kw, rho)
+        ref_P, ref_g = g[f"{field}_{i}_P"], g[f"{field}_{i}_grad"]
+        assert abs(P - ref_P) <= 1e-13 * max(1.0, abs(ref_P)), (i, kind, kw)
+        assert np.abs(grad - ref_g).max() <= 1e-12 * max(1e-300, np.abs(ref_g).max()), (i, kind, kw)
+
+
+PRINT_TRAJ_CAVITY = dict(void_thresh=0.5, beta=20.0, min_channel_rad=1, rad=1, iters=0, tiles=(2, 2, 2),
+                         focus_center=True, seed_faces="all")
+
+
+def test_penalised_trajectory_matches_reference(golden):
+    g = golden("print.npz")
+    x = g["traj_x0"]
+    for it in range(3):
+        x, info = O.oc_iteration(x, 8, {"stiffness": 0.5, "thermal": 0.5}, volfrac=0.25, rtol=1e-12,
+                                 lambda_print=0.9, overhang_deg=45.0, lambda_cavity=0.9, cavity=PRINT_TRAJ_CAVITY)
+        assert abs(info["J"] - g[f"traj_J{it}"]) < 1e-8 * abs(g[f"traj_J{it}"]), it
+        assert abs(info["P_print"] - g[f"traj_Pp{it}"]) < 1e-10 and abs(info["P_cavity"] - g[f"traj_Pc{it}"]) < 1e-10
+        assert np.abs(x - g[f"traj_x{it + 1}"]).max() < 1e-7, it
