@@ -94,6 +94,34 @@ int maple_set_symmetry(maple_ctx* ctx, int kind, int axes_mask);
 int maple_symmetrize(int r, int ncells, int kind, int axes_mask, const double* in, double* out,
                      maple_stream_t stream);
 
+/* Manufacturability penalties of the OC objective (utils/printability.py,
+ * main_IHD_v3.py:649-686): J = J_raw - lambda_print * P_overhang -
+ * lambda_cavity * P_cavity, differentiated with the tie rules of the
+ * reference's autograd.  Overhang: build direction +z, lateral support radius
+ * ceil(tan(90 - overhang_deg)), periodic in x and y if overhang_periodic
+ * (printability_penalty_overhang; the optimizer uses periodic).  Cavity: soft void sigmoid(beta (thresh -
+ * rho)), optional opening of radius min_channel_rad, flood fill of `iters`
+ * steps (0: the supercell's largest dimension) with windows of radius rad
+ * from the seed faces; tiles 1,1,1 = cavity_penalty_closed_void (periodic as
+ * given), more tiles = cavity_penalty_periodic_array (non-periodic supercell,
+ * focus_center: the centre tile only when every count >= 3).  Workspace is
+ * allocated here (the cavity tape grows with iters x supercell size).  A
+ * weight of 0 disables that penalty in maple_oc_step. */
+enum { MAPLE_SEED_ALL = 0, MAPLE_SEED_X = 1, MAPLE_SEED_Y = 2, MAPLE_SEED_Z = 3, MAPLE_SEED_XY = 4 };
+int maple_set_penalties(maple_ctx* ctx, double lambda_print, double overhang_deg, int overhang_periodic,
+                        double lambda_cavity, double void_thresh, double beta, int min_channel_rad, int rad, int iters,
+                        int tiles_x, int tiles_y, int tiles_z, int focus_center, int seed_faces, int periodic);
+
+/* The configured penalties of densities rho [B][N] (device): P [B] and dP/drho
+ * [B][N] (each nullable; a gradient needs its value).  A penalty must have
+ * been enabled (weight > 0) by maple_set_penalties. */
+int maple_penalties(maple_ctx* ctx, const double* rho, double* P_print, double* dP_print, double* P_cavity,
+                    double* dP_cavity, maple_stream_t stream);
+
+/* Terms of the last maple_oc_step per cell (device [B], nullable): the
+ * objective before penalties and both penalty values (0 when disabled). */
+int maple_get_oc_terms(maple_ctx* ctx, double* J_raw, double* P_print, double* P_cavity, maple_stream_t stream);
+
 /* Per-cell active mask (host int[B], nonzero = active). Inactive cells are
  * skipped by every kernel.  NULL = all active. */
 int maple_set_active(maple_ctx* ctx, const int* active_host, maple_stream_t stream);

@@ -37,6 +37,9 @@ SIGNATURES = {
     "maple_set_graphs": (_I, [_P, _I]),
     "maple_set_concurrency": (_I, [_P, _I]),
     "maple_set_symmetry": (_I, [_P, _I, _I]),
+    "maple_set_penalties": (_I, [_P, _D, _D, _I, _D, _D, _D, _I, _I, _I, _I, _I, _I, _I, _I, _I]),
+    "maple_penalties": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "maple_get_oc_terms": (_I, [_P, _P, _P, _P, _P]),
     "maple_symmetrize": (_I, [_I, _I, _I, _I, _P, _P, _P]),
     "maple_set_active": (_I, [_P, _IP, _P]),
     "maple_set_density": (_I, [_P, _I, _P, _I, _P]),
@@ -83,6 +86,7 @@ SIGNATURES = {
 
 NN_POOL, NN_UPSAMPLE, NN_UPSAMPLE_ADJ, NN_POOL_ADJ = 0, 1, 2, 3
 SYM_NONE, SYM_MIRROR, SYM_CUBIC = 0, 1, 2
+SEED_FACES = {"all": 0, "x": 1, "y": 2, "z": 3, "xy": 4}
 
 _lib = None
 

@@ -112,6 +112,42 @@ class HomogenizationContext:
         k, mask = _sym_args(kind, axes)
         _lib.check(self._lib.maple_set_symmetry(self._h, k, mask))
 
+    def set_penalties(self, lambda_print: float = 0.0, overhang_deg: float = 45.0, lambda_cavity: float = 0.0, *,
+                      overhang_periodic: bool = True, void_thresh: float = 0.5, beta: float = 20.0,
+                      min_channel_rad: int = 0, rad: int = 1, iters: int = 0, tiles=(1, 1, 1),
+                      focus_center: bool = True, seed_faces: str = "all", periodic: bool = True):
+        """Manufacturability penalties of oc_step: J = J_raw - lambda_print *
+        P_overhang - lambda_cavity * P_cavity (utils/printability.py); a zero
+        weight disables a penalty.  tiles (1,1,1): closed-void penalty of the
+        cell (periodic as given); more tiles: periodic-array penalty."""
+        sf = str(seed_faces).lower()
+        if sf not in _lib.SEED_FACES:
+            raise ValueError("seed_faces must be one of: all, x, y, z, xy")
+        tx, ty, tz = (int(t) for t in tiles)
+        _lib.check(self._lib.maple_set_penalties(
+            self._h, float(lambda_print), float(overhang_deg), int(bool(overhang_periodic)), float(lambda_cavity),
+            float(void_thresh), float(beta), int(min_channel_rad), int(rad), int(iters), tx, ty, tz,
+            int(bool(focus_center)), _lib.SEED_FACES[sf], int(bool(periodic))))
+
+    def penalties(self, rho: torch.Tensor, overhang: bool = True, cavity: bool = True, grad: bool = True):
+        """The configured penalties of rho (B, N): dict with P_print / dP_print
+        and P_cavity / dP_cavity (B,) and (B, N) float64 for the requested ones."""
+        self._check(rho, "rho", (self.B, self.N))
+        out = {}
+        t = lambda shape: torch.empty(shape, dtype=torch.float64, device=self.device)
+        Pp = t((self.B,)) if overhang else None
+        Pc = t((self.B,)) if cavity else None
+        gp = t((self.B, self.N)) if overhang and grad else None
+        gc = t((self.B, self.N)) if cavity and grad else None
+        with torch.cuda.device(self.device):
+            _lib.check(self._lib.maple_penalties(self._h, _ptr(rho), _ptr(Pp), _ptr(gp), _ptr(Pc), _ptr(gc),
+                                                 _stream(self.device)))
+        if overhang:
+            out.update(P_print=Pp, dP_print=gp)
+        if cavity:
+            out.update(P_cavity=Pc, dP_cavity=gc)
+        return out
+
     def set_concurrency(self, enable: bool):
         """Run the elastic and thermal solves of oc_step at the same time (default on)."""
         _lib.check(self._lib.maple_set_concurrency(self._h, int(bool(enable))))
@@ -247,7 +283,8 @@ class HomogenizationContext:
     def oc_step(self, x: torch.Tensor, weights: torch.Tensor, volfrac: torch.Tensor, *, penal=3.0, rho_min=1e-9,
                 move=0.2, xmin=1e-3, filter_k=3, precision="fp64", rtol=1e-8, maxit=500, warm=True, out=None):
         """One OC iteration for every active cell.  Returns a dict of device
-        tensors: x_next (B,N), J (B,), terms (B,3), CH (B,6,6), kappa (B,3,3),
+        tensors: x_next (B,N), J (B,) (with the configured penalties), J_raw,
+        P_print, P_cavity (B,), terms (B,3), CH (B,6,6), kappa (B,3,3),
         stats (B,2) and host iteration counts."""
         self._check(x, "x", (self.B, self.N))
         self._check(weights, "weights", (self.B, 3))
@@ -266,6 +303,11 @@ class HomogenizationContext:
                 float(xmin), int(filter_k), PRECISION[precision], float(rtol), int(maxit), int(bool(warm)),
                 _ptr(out["x_next"]), _ptr(out["J"]), _ptr(out["terms"]), _ptr(out["CH"]), _ptr(out["kappa"]),
                 _ptr(out["stats"]), it.ctypes.data_as(C.POINTER(C.c_int)), _stream(dev)))
+            for k in ("J_raw", "P_print", "P_cavity"):
+                if k not in out:
+                    out[k] = torch.zeros(B, dtype=torch.float64, device=dev)
+            _lib.check(self._lib.maple_get_oc_terms(self._h, _ptr(out["J_raw"]), _ptr(out["P_print"]),
+                                                    _ptr(out["P_cavity"]), _stream(dev)))
         out["iters"] = it
         return out
 

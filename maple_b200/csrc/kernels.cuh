@@ -1608,10 +1608,13 @@ __global__ void k_objective(const double* __restrict__ CH, const double* __restr
 }
 
 // dJ/dx_e = p (1-rho_min) xc^(p-1) * (G3 : E3_e + G1 : E1_e)
+// dJ/drho_e = sum_ij G_ij dH_ij/drho_e (energies E) - lp dPp/drho_e - lc dPc/drho_e
+// (penalty gradients nullable), and dJ/dx_e through the SIMP map
 __global__ void k_sensitivity(const double* __restrict__ x, const double* __restrict__ E3, const double* __restrict__ E1,
                               const double* __restrict__ G3, const double* __restrict__ G1, double* __restrict__ dJdx,
                               double* __restrict__ dJdrho, int N, double xmin, double penal, double rho_min,
-                              const int* active) {
+                              const int* active, const double* __restrict__ dPp = nullptr, double lp = 0.0,
+                              const double* __restrict__ dPc = nullptr, double lc = 0.0) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   const int e = blockIdx.x * kThreads + threadIdx.x;
@@ -1630,6 +1633,8 @@ __global__ void k_sensitivity(const double* __restrict__ x, const double* __rest
 #pragma unroll
     for (int k = 0; k < 9; ++k) s += G[k] * Ee[(size_t)k * N];
   }
+  if (dPp) s -= lp * dPp[i];
+  if (dPc) s -= lc * dPc[i];
   if (dJdrho) dJdrho[i] = s;
   if (dJdx) {
     const double xv = x[i];

@@ -2,6 +2,7 @@
 // the C ABI declared in include/maple_b200.h.
 #include "../../include/maple_b200.h"
 #include "kernels.cuh"
+#include "printability.h"
 #include "tables.h"
 
 #include <cmath>
@@ -181,6 +182,15 @@ struct maple_ctx {
   bool use_graphs = true;
   bool concurrent = true;  // elastic and thermal solves of an OC step on two streams
   int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
+  // manufacturability penalties of the OC objective (maple_set_penalties)
+  double lambda_print = 0, lambda_cavity = 0;
+  bool print_set = false, cavity_set = false;
+  maple_pr::OverhangPlan oplan;
+  maple_pr::CavityPlan cplan;
+  void* pen_work = nullptr;
+  size_t pen_bytes = 0;
+  double *pen_rho = nullptr, *P_print = nullptr, *P_cav = nullptr, *dP_print = nullptr, *dP_cav = nullptr,
+         *J_raw = nullptr;
   // per-kernel-class event timing of fine-level launches (bench instrumentation)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -934,6 +944,26 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
 //   barrier counters are cleared at the start of every call.  Calls whose
 //   kernels overlap on the GPU (for example on two streams) race on it.
 // ---------------------------------------------------------------------------
+// J = J_raw - lp P_print - lc P_cavity per cell
+__global__ void k_penalise_J(double* J, const double* Pp, double lp, const double* Pc, double lc, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  double j = J[b];
+  if (Pp) j -= lp * Pp[b];
+  if (Pc) j -= lc * Pc[b];
+  J[b] = j;
+}
+
+// the configured penalties of rho [B][N] and their gradients into the context
+static void run_penalties(maple_ctx* c, const double* rho, bool print, bool cavity, cudaStream_t s) {
+  try {
+    if (print) maple_pr::overhang(rho, c->oplan, c->P_print, c->dP_print, c->pen_work, s);
+    if (cavity) maple_pr::cavity(rho, c->cplan, c->P_cav, c->dP_cav, c->pen_work, s);
+  } catch (const std::runtime_error& e) {
+    throw Failure{MAPLE_E_CUDA, e.what()};
+  }
+}
+
 static constexpr int kNoAllocScratch = 32768;  // doubles
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratch];
 static std::mutex g_noalloc_mu;
@@ -1072,6 +1102,7 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
       c->dJdx = dnew<double>(c, (size_t)B * N0);
       c->dJf = dnew<double>(c, (size_t)B * N0);
       c->Jv = dnew<double>(c, B);
+      c->J_raw = dnew<double>(c, B);
       c->terms = dnew<double>(c, B * 3);
       c->G3 = dnew<double>(c, B * 36);
       c->G1 = dnew<double>(c, B * 9);
@@ -1156,6 +1187,7 @@ int maple_ctx_destroy(maple_ctx* c) {
       if (L.cap_stream) cudaStreamDestroy(L.cap_stream);
       if (L.h_flags) cudaFreeHost(L.h_flags);
     }
+    if (c->pen_work) cudaFree(c->pen_work);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     if (c->aux_fork) cudaEventDestroy(c->aux_fork);
     if (c->aux_join) cudaEventDestroy(c->aux_join);
@@ -1193,6 +1225,108 @@ int maple_symmetrize(int r, int ncells, int kind, int axes_mask, const double* i
     const size_t N = (size_t)r * r * r;
     k_symmetrize<<<g2(N, ncells), kThreads, 0, S(s)>>>(in, out, r, kind, axes_mask, 0, 0.0, 0.0, nullptr);
     CKL();
+  });
+}
+
+int maple_set_penalties(maple_ctx* c, double lambda_print, double overhang_deg, int overhang_periodic,
+                        double lambda_cavity, double void_thresh, double beta, int min_channel_rad, int rad, int iters,
+                        int tiles_x, int tiles_y, int tiles_z, int focus_center, int seed_faces, int periodic) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(lambda_print >= 0 && lambda_cavity >= 0, "penalty weights must be >= 0");
+    require(seed_faces >= MAPLE_SEED_ALL && seed_faces <= MAPLE_SEED_XY, "unknown seed faces");
+    require(tiles_x >= 1 && tiles_y >= 1 && tiles_z >= 1, "tiles must be >= 1");
+    require(min_channel_rad >= 0 && rad >= 0 && iters >= 0, "radii and iterations must be >= 0");
+    require(std::isfinite(overhang_deg) && std::isfinite(void_thresh) && std::isfinite(beta), "non-finite parameter");
+    const int r = c->r, B = c->B;
+    maple_pr::OverhangPlan op;
+    op.r = r;
+    op.B = B;
+    {  // lateral support radius for the overhang angle (utils/printability.py:76-90)
+      const double od = std::min(89.0, std::max(1.0, overhang_deg));
+      op.rad = std::max(1, (int)std::ceil(std::tan((90.0 - od) * M_PI / 180.0)));
+    }
+    op.periodic = overhang_periodic ? 1 : 0;
+    if (op.periodic) require(2 * op.rad + 1 <= r, "overhang support window wider than the cell");
+    maple_pr::CavityPlan cp;
+    cp.r = r;
+    cp.B = B;
+    cp.tiles[0] = tiles_x;
+    cp.tiles[1] = tiles_y;
+    cp.tiles[2] = tiles_z;
+    const bool array = tiles_x > 1 || tiles_y > 1 || tiles_z > 1;
+    cp.periodic = (periodic && !array) ? 1 : 0;
+    cp.min_channel_rad = min_channel_rad;
+    cp.rad = rad;
+    cp.nsteps = iters > 0 ? iters : (array ? std::max(cp.dims(0), std::max(cp.dims(1), cp.dims(2))) : r);
+    cp.seed = seed_faces;
+    cp.focus_center = focus_center ? 1 : 0;
+    cp.void_thresh = void_thresh;
+    cp.beta = beta;
+    if (cp.periodic) require(2 * std::max(rad, min_channel_rad) + 1 <= r, "cavity window wider than the cell");
+    const bool want_p = lambda_print > 0, want_c = lambda_cavity > 0;
+    const size_t bytes = std::max(want_p ? op.bytes() : 0, want_c ? cp.bytes() : 0);
+    if (bytes > c->pen_bytes) {
+      if (c->pen_work) CK(cudaFree(c->pen_work));
+      c->pen_work = nullptr;
+      c->pen_bytes = 0;
+      cudaError_t e = cudaMalloc(&c->pen_work, bytes);
+      if (e != cudaSuccess) throw Failure{MAPLE_E_NOMEM, std::string("penalty workspace: ") + cudaGetErrorString(e)};
+      c->pen_bytes = bytes;
+    }
+    if (!c->pen_rho) {
+      const size_t N = (size_t)nodes(r);
+      c->pen_rho = dnew<double>(c, (size_t)B * N);
+      c->dP_print = dnew<double>(c, (size_t)B * N);
+      c->dP_cav = dnew<double>(c, (size_t)B * N);
+      c->P_print = dnew<double>(c, B);
+      c->P_cav = dnew<double>(c, B);
+      CK(cudaMemset(c->P_print, 0, B * sizeof(double)));
+      CK(cudaMemset(c->P_cav, 0, B * sizeof(double)));
+    }
+    c->oplan = op;
+    c->cplan = cp;
+    c->lambda_print = lambda_print;
+    c->lambda_cavity = lambda_cavity;
+    c->print_set = want_p;
+    c->cavity_set = want_c;
+  });
+}
+
+int maple_penalties(maple_ctx* c, const double* rho, double* P_print, double* dP_print, double* P_cavity,
+                    double* dP_cavity, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && rho != nullptr, "NULL argument");
+    require(!P_print || c->print_set, "the overhang penalty is not configured (maple_set_penalties)");
+    require(!P_cavity || c->cavity_set, "the cavity penalty is not configured (maple_set_penalties)");
+    require(!dP_print || P_print, "dP_print needs P_print");
+    require(!dP_cavity || P_cavity, "dP_cavity needs P_cavity");
+    try {
+      if (P_print) maple_pr::overhang(rho, c->oplan, P_print, dP_print, c->pen_work, S(s));
+      if (P_cavity) maple_pr::cavity(rho, c->cplan, P_cavity, dP_cavity, c->pen_work, S(s));
+    } catch (const std::runtime_error& e) {
+      throw Failure{MAPLE_E_CUDA, e.what()};
+    }
+  });
+}
+
+int maple_get_oc_terms(maple_ctx* c, double* J_raw, double* P_print, double* P_cavity, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    const size_t nb = (size_t)c->B * sizeof(double);
+    if (J_raw) CK(cudaMemcpyAsync(J_raw, c->J_raw, nb, cudaMemcpyDeviceToDevice, S(s)));
+    if (P_print) {
+      if (c->P_print)
+        CK(cudaMemcpyAsync(P_print, c->P_print, nb, cudaMemcpyDeviceToDevice, S(s)));
+      else
+        CK(cudaMemsetAsync(P_print, 0, nb, S(s)));
+    }
+    if (P_cavity) {
+      if (c->P_cav)
+        CK(cudaMemcpyAsync(P_cavity, c->P_cav, nb, cudaMemcpyDeviceToDevice, S(s)));
+      else
+        CK(cudaMemsetAsync(P_cavity, 0, nb, S(s)));
+    }
   });
 }
 
@@ -1475,6 +1609,13 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
                                                            1.0, c->active));
       xu = c->x_sym;
     }
+    // manufacturability penalties at the solves' densities (main_IHD_v3.py:649-686)
+    const bool pen_p = c->lambda_print > 0 && c->print_set, pen_c = c->lambda_cavity > 0 && c->cavity_set;
+    if (pen_p || pen_c) {
+      KL(c, st, k_simp<<<nblk((size_t)B * N), kThreads, 0, st>>>(xu, c->pen_rho, nullptr, (size_t)B * N, N, xmin, penal,
+                                                               rho_min, c->active));
+      run_penalties(c, c->pen_rho, pen_p, pen_c, st);
+    }
     // one physics: SIMP map, hierarchy, RHS, MG-PCG solve, energies
     auto run_phys = [&](int phys, cudaStream_t ps, int* it_out) {
       LaneScope lane(phys);
@@ -1532,9 +1673,14 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
     for (int b = 0; b < B; ++b) it_sum[b] = it_el[b] + it_th[b];
     KL(c, st, k_objective<<<nblk(B), kThreads, 0, st>>>(c->ph[0].H, c->ph[1].H, w, c->Jv, c->terms, c->G3, c->G1, B,
                                               need_ch ? 1 : 0, need_k ? 1 : 0, c->active));
+    CK(cudaMemcpyAsync(c->J_raw, c->Jv, B * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (pen_p || pen_c)
+      KL(c, st, k_penalise_J<<<nblk(B), kThreads, 0, st>>>(c->Jv, pen_p ? c->P_print : nullptr, c->lambda_print,
+                                                          pen_c ? c->P_cav : nullptr, c->lambda_cavity, B));
     KL(c, st, k_sensitivity<<<g2(N, B), kThreads, 0, st>>>(xu, need_ch ? c->ph[0].energy : nullptr,
                                                  need_k ? c->ph[1].energy : nullptr, c->G3, c->G1, c->dJdx, nullptr, N,
-                                                 xmin, penal, rho_min, c->active));
+                                                 xmin, penal, rho_min, c->active, pen_p ? c->dP_print : nullptr,
+                                                 c->lambda_print, pen_c ? c->dP_cav : nullptr, c->lambda_cavity));
     double *dJ = c->dJdx, *spare = c->dJf;
     if (sym) {  // the gradient through the (self-adjoint) projection
       KL(c, st, k_symmetrize<<<g2(N, B), kThreads, 0, st>>>(dJ, spare, c->n[0], c->sym_kind, c->sym_mask, 0, 0.0,

@@ -1,0 +1,536 @@
+// Manufacturability penalties and their gradients (see printability.h).
+//
+// Overhang: one CTA per cell sweeps the layers z = 1..r-1 (each layer's
+// lateral max-pool needs the whole previous layer), recording the pooled
+// support and its argmax per voxel; the backward sweep runs the layers in
+// reverse.  Cavity: the (super)cell is materialised once, then every opening
+// and flood-fill step is one grid-wide kernel (one thread per supercell voxel),
+// each flood-fill step recording its dilation and argmax for the backward
+// pass.  Pool adjoints are gathers: a voxel sums the gradients of the windows
+// whose argmax it is, so no atomics are needed and results are deterministic.
+#include "printability.h"
+
+#include <algorithm>
+#include <atomic>
+#include <utility>
+#include <cmath>
+#include <stdexcept>
+#include <string>
+
+namespace maple_pr {
+
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long launches() { return g_launches.load(); }
+
+#define PR_LAUNCH(...)                                                                               \
+  do {                                                                                               \
+    __VA_ARGS__;                                                                                     \
+    const cudaError_t e_ = cudaGetLastError();                                                       \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string("penalty kernel: ") + cudaGetErrorString(e_)); \
+    g_launches.fetch_add(1);                                                                         \
+  } while (0)
+
+constexpr int kT = 256;
+static inline unsigned nb(size_t n) { return (unsigned)((n + kT - 1) / kT); }
+static inline size_t al(size_t b) { return (b + 255) / 256 * 256; }
+
+__device__ __forceinline__ int wrapi(int i, int n) { return ((i % n) + n) % n; }
+
+// gradient of torch.minimum(a, b) w.r.t. a for upstream g: g where a < b, g/2 where equal
+__device__ __forceinline__ double min_grad(double a, double b, double g) {
+  return a < b ? g : (a == b ? 0.5 * g : 0.0);
+}
+
+// block sum of v (blockDim.x <= 1024) returned to thread 0
+__device__ double block_sum(double v) {
+  __shared__ double sm[32];
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) s += sm[w];
+  __syncthreads();
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// overhang
+// ---------------------------------------------------------------------------
+struct OverhangWork {
+  double* tape_s;  // [B][r-1][r^2] pooled support of layer z-1
+  int* tape_src;   // [B][r-1][r^2] its argmax (layer index, -1 = padding)
+  double* buf;     // [B][3][r^2] two support / gradient layers and one scratch layer
+};
+
+static OverhangWork overhang_parts(const OverhangPlan& p, void* work) {
+  const size_t L = (size_t)p.r * p.r, T = (size_t)p.B * (p.r - 1) * L;
+  char* w = static_cast<char*>(work);
+  OverhangWork o;
+  o.tape_s = reinterpret_cast<double*>(w);
+  o.tape_src = reinterpret_cast<int*>(w + al(T * sizeof(double)));
+  o.buf = reinterpret_cast<double*>(w + al(T * sizeof(double)) + al(T * sizeof(int)));
+  return o;
+}
+
+size_t OverhangPlan::bytes() const {
+  const size_t L = (size_t)r * r, T = (size_t)B * (r - 1) * L;
+  return al(T * sizeof(double)) + al(T * sizeof(int)) + al((size_t)B * 3 * L * sizeof(double));
+}
+
+__global__ void __launch_bounds__(1024) k_overhang_fwd(const double* __restrict__ rho, int r, int rad, int periodic,
+                                                       OverhangWork w, double* __restrict__ P) {
+  const int b = blockIdx.x;
+  const int L = r * r;
+  const double* g = rho + (size_t)b * L * r;
+  double* cur = w.buf + (size_t)b * 3 * L;
+  double* nxt = cur + L;
+  for (int q = threadIdx.x; q < L; q += blockDim.x) cur[q] = g[(size_t)q * r];
+  __syncthreads();
+  double acc = 0.0;
+  for (int z = 1; z < r; ++z) {
+    double* ts = w.tape_s + ((size_t)b * (r - 1) + (z - 1)) * L;
+    int* tsrc = w.tape_src + ((size_t)b * (r - 1) + (z - 1)) * L;
+    for (int q = threadIdx.x; q < L; q += blockDim.x) {
+      const int x = q / r, y = q % r;
+      double best = -INFINITY;
+      int bsrc = -1;
+      for (int dx = -rad; dx <= rad; ++dx)
+        for (int dy = -rad; dy <= rad; ++dy) {
+          int xx = x + dx, yy = y + dy;
+          double v;
+          int src;
+          if (periodic) {
+            xx = wrapi(xx, r);
+            yy = wrapi(yy, r);
+            src = xx * r + yy;
+            v = cur[src];
+          } else if (xx < 0 || xx >= r || yy < 0 || yy >= r) {
+            src = -1;
+            v = 0.0;
+          } else {
+            src = xx * r + yy;
+            v = cur[src];
+          }
+          if (v > best) {
+            best = v;
+            bsrc = src;
+          }
+        }
+      ts[q] = best;
+      tsrc[q] = bsrc;
+      const double rz = g[(size_t)q * r + z];
+      acc += fmax(rz - best, 0.0);
+      nxt[q] = fmin(rz, best);
+    }
+    __syncthreads();
+    double* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  const double s = block_sum(acc);
+  if (threadIdx.x == 0) P[b] = s / ((double)L * (r > 1 ? r - 1 : 1));
+}
+
+__global__ void __launch_bounds__(1024) k_overhang_bwd(const double* __restrict__ rho, int r, int rad, int periodic,
+                                                       OverhangWork w, double* __restrict__ grad) {
+  const int b = blockIdx.x;
+  const int L = r * r;
+  const double den = (double)L * (r > 1 ? r - 1 : 1);
+  const double* g = rho + (size_t)b * L * r;
+  double* out = grad + (size_t)b * L * r;
+  double* gsup = w.buf + (size_t)b * 3 * L;  // gradient arriving at support(z)
+  double* gnew = gsup + L;
+  double* gs = gnew + L;                     // gradient at the pooled support of layer z
+  for (int q = threadIdx.x; q < L; q += blockDim.x) gsup[q] = 0.0;
+  __syncthreads();
+  for (int z = r - 1; z >= 1; --z) {
+    const double* ts = w.tape_s + ((size_t)b * (r - 1) + (z - 1)) * L;
+    const int* tsrc = w.tape_src + ((size_t)b * (r - 1) + (z - 1)) * L;
+    for (int q = threadIdx.x; q < L; q += blockDim.x) {
+      const double rz = g[(size_t)q * r + z], s = ts[q], up = gsup[q];
+      const double act = (rz - s) > 0.0 ? 1.0 / den : 0.0;
+      out[(size_t)q * r + z] = min_grad(rz, s, up) + act;
+      gs[q] = min_grad(s, rz, up) - act;
+    }
+    __syncthreads();
+    // pool adjoint: voxel p collects the windows whose argmax it is
+    for (int p = threadIdx.x; p < L; p += blockDim.x) {
+      const int x = p / r, y = p % r;
+      double acc = 0.0;
+      for (int dx = -rad; dx <= rad; ++dx)
+        for (int dy = -rad; dy <= rad; ++dy) {
+          int xx = x + dx, yy = y + dy;
+          if (periodic) {
+            xx = wrapi(xx, r);
+            yy = wrapi(yy, r);
+          } else if (xx < 0 || xx >= r || yy < 0 || yy >= r) {
+            continue;
+          }
+          const int q = xx * r + yy;
+          if (tsrc[q] == p) acc += gs[q];
+        }
+      gnew[p] = acc;
+    }
+    __syncthreads();
+    double* t = gsup;
+    gsup = gnew;
+    gnew = t;
+  }
+  for (int q = threadIdx.x; q < L; q += blockDim.x) out[(size_t)q * r] = gsup[q];
+}
+
+void overhang(const double* rho, const OverhangPlan& p, double* P, double* grad, void* work, cudaStream_t s) {
+  if (p.r < 2 || p.B < 1 || p.rad < 1) throw std::runtime_error("overhang penalty: bad sizes");
+  if (p.periodic && 2 * p.rad + 1 > p.r) throw std::runtime_error("overhang penalty: support window wider than the cell");
+  const OverhangWork w = overhang_parts(p, work);
+  PR_LAUNCH(k_overhang_fwd<<<p.B, 1024, 0, s>>>(rho, p.r, p.rad, p.periodic, w, P));
+  if (grad) PR_LAUNCH(k_overhang_bwd<<<p.B, 1024, 0, s>>>(rho, p.r, p.rad, p.periodic, w, grad));
+}
+
+// ---------------------------------------------------------------------------
+// cavity
+// ---------------------------------------------------------------------------
+struct CavGeo {
+  int r, X, Y, Z;  // cell size and supercell dims
+  size_t M;
+  int periodic;
+  __device__ void coords(size_t v, int& x, int& y, int& z) const {
+    z = (int)(v % Z);
+    y = (int)((v / Z) % Y);
+    x = (int)(v / ((size_t)Y * Z));
+  }
+  __device__ size_t index(int x, int y, int z) const { return ((size_t)x * Y + y) * Z + z; }
+  // neighbour at offset, or false (outside a non-periodic supercell)
+  __device__ bool shift(int x, int y, int z, int dx, int dy, int dz, size_t& out) const {
+    int a = x + dx, bb = y + dy, c = z + dz;
+    if (periodic) {
+      a = wrapi(a, X);
+      bb = wrapi(bb, Y);
+      c = wrapi(c, Z);
+    } else if (a < 0 || a >= X || bb < 0 || bb >= Y || c < 0 || c >= Z) {
+      return false;
+    }
+    out = index(a, bb, c);
+    return true;
+  }
+};
+
+struct CavWork {
+  double *void_uc, *vsc, *er, *vconn, *reach0, *reach1, *dil, *gr0, *gr1, *gvconn, *gvoid, *gtmp, *part;
+  int *er_src, *di_src, *src;
+};
+
+static size_t cav_parts(const CavityPlan& p, void* work, CavWork* o) {
+  const size_t B = p.B, M = p.M(), N = (size_t)p.r * p.r * p.r, S = (size_t)std::max(p.nsteps, 0);
+  const size_t nparts = (M + kT - 1) / kT;
+  size_t off = 0;
+  char* w = static_cast<char*>(work);
+  auto take = [&](size_t bytes) {
+    char* q = w ? w + off : nullptr;
+    off += al(bytes);
+    return q;
+  };
+  CavWork c{};
+  c.void_uc = reinterpret_cast<double*>(take(B * N * 8));
+  c.vsc = reinterpret_cast<double*>(take(B * M * 8));
+  if (p.min_channel_rad > 0) {
+    c.er = reinterpret_cast<double*>(take(B * M * 8));
+    c.vconn = reinterpret_cast<double*>(take(B * M * 8));
+    c.er_src = reinterpret_cast<int*>(take(B * M * 4));
+    c.di_src = reinterpret_cast<int*>(take(B * M * 4));
+  }
+  c.reach0 = reinterpret_cast<double*>(take(B * M * 8));
+  c.reach1 = reinterpret_cast<double*>(take(B * M * 8));
+  c.dil = reinterpret_cast<double*>(take(B * M * S * 8));
+  c.src = reinterpret_cast<int*>(take(B * M * S * 4));
+  c.gr0 = reinterpret_cast<double*>(take(B * M * 8));
+  c.gr1 = reinterpret_cast<double*>(take(B * M * 8));
+  c.gvconn = reinterpret_cast<double*>(take(B * M * 8));
+  c.gvoid = reinterpret_cast<double*>(take(B * M * 8));
+  c.gtmp = reinterpret_cast<double*>(take(B * M * 8));
+  c.part = reinterpret_cast<double*>(take(B * nparts * 8));
+  if (o) *o = c;
+  return off;
+}
+
+size_t CavityPlan::bytes() const { return cav_parts(*this, nullptr, nullptr); }
+
+__global__ void k_cav_void(const double* __restrict__ rho, double* __restrict__ void_uc, size_t N, double thresh,
+                           double beta) {
+  const size_t i = (size_t)blockIdx.x * kT + threadIdx.x + (size_t)blockIdx.y * N;
+  if ((size_t)blockIdx.x * kT + threadIdx.x >= N) return;
+  void_uc[i] = 1.0 / (1.0 + exp(-beta * (thresh - rho[i])));
+}
+
+__global__ void k_cav_tile(const double* __restrict__ void_uc, double* __restrict__ vsc, CavGeo G) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const int b = blockIdx.y;
+  int x, y, z;
+  G.coords(v, x, y, z);
+  const int r = G.r;
+  vsc[(size_t)b * G.M + v] = void_uc[(size_t)b * r * r * r + ((size_t)(x % r) * r + (y % r)) * r + (z % r)];
+}
+
+// out = sign * maxpool(sign * in) over a (2 rad + 1)^3 window (padding value pad
+// in the sign * in domain), first maximum in (x, y, z) scan order; src = its
+// index (-1: padding)
+__global__ void k_cav_pool(const double* __restrict__ in, double* __restrict__ out, int* __restrict__ src, CavGeo G,
+                           int rad, double sign, double pad) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const size_t base = (size_t)blockIdx.y * G.M;
+  int x, y, z;
+  G.coords(v, x, y, z);
+  double best = -INFINITY;
+  int bsrc = -1;
+  for (int dx = -rad; dx <= rad; ++dx)
+    for (int dy = -rad; dy <= rad; ++dy)
+      for (int dz = -rad; dz <= rad; ++dz) {
+        size_t q;
+        double val;
+        int s;
+        if (G.shift(x, y, z, dx, dy, dz, q)) {
+          val = sign * in[base + q];
+          s = (int)q;
+        } else {
+          val = pad;
+          s = -1;
+        }
+        if (val > best) {
+          best = val;
+          bsrc = s;
+        }
+      }
+  out[base + v] = sign * best;
+  src[base + v] = bsrc;
+}
+
+__device__ __forceinline__ bool is_seed(const CavGeo& G, int seed, int x, int y, int z) {
+  const bool fx = x == 0 || x == G.X - 1, fy = y == 0 || y == G.Y - 1, fz = z == 0 || z == G.Z - 1;
+  switch (seed) {
+    case SEED_ALL: return fx || fy || fz;
+    case SEED_X: return fx;
+    case SEED_Y: return fy;
+    default: return fz;  // SEED_Z, SEED_XY
+  }
+}
+
+__global__ void k_cav_seed(const double* __restrict__ vconn, double* __restrict__ reach, CavGeo G, int seed) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const size_t i = (size_t)blockIdx.y * G.M + v;
+  int x, y, z;
+  G.coords(v, x, y, z);
+  reach[i] = is_seed(G, seed, x, y, z) ? vconn[i] : 0.0;
+}
+
+// one flood-fill step: dil = maxpool(reach_in), reach_out = min(vconn, dil)
+__global__ void k_cav_step(const double* __restrict__ reach_in, const double* __restrict__ vconn,
+                           double* __restrict__ dil, int* __restrict__ src, double* __restrict__ reach_out, CavGeo G,
+                           int rad) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const size_t base = (size_t)blockIdx.y * G.M;
+  int x, y, z;
+  G.coords(v, x, y, z);
+  double best = -INFINITY;
+  int bsrc = -1;
+  for (int dx = -rad; dx <= rad; ++dx)
+    for (int dy = -rad; dy <= rad; ++dy)
+      for (int dz = -rad; dz <= rad; ++dz) {
+        size_t q;
+        double val;
+        int s;
+        if (G.shift(x, y, z, dx, dy, dz, q)) {
+          val = reach_in[base + q];
+          s = (int)q;
+        } else {
+          val = 0.0;
+          s = -1;
+        }
+        if (val > best) {
+          best = val;
+          bsrc = s;
+        }
+      }
+  dil[base + v] = best;
+  src[base + v] = bsrc;
+  reach_out[base + v] = fmin(vconn[base + v], best);
+}
+
+__device__ __forceinline__ bool in_region(const CavGeo& G, int focus, int x, int y, int z) {
+  if (!focus) return true;
+  const int r = G.r, cx = (G.X / r) / 2, cy = (G.Y / r) / 2, cz = (G.Z / r) / 2;
+  return x / r == cx && y / r == cy && z / r == cz;
+}
+
+// per-block partial sums of relu(void - reach) over the penalty region
+__global__ void k_cav_trapped(const double* __restrict__ vsc, const double* __restrict__ reach,
+                              double* __restrict__ part, CavGeo G, int focus) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  double t = 0.0;
+  if (v < G.M) {
+    const size_t i = (size_t)blockIdx.y * G.M + v;
+    int x, y, z;
+    G.coords(v, x, y, z);
+    if (in_region(G, focus, x, y, z)) t = fmax(vsc[i] - reach[i], 0.0);
+  }
+  const double s = block_sum(t);
+  if (threadIdx.x == 0) part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+__global__ void k_cav_total(const double* __restrict__ part, int nparts, double* __restrict__ P, double count) {
+  const int b = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[(size_t)b * nparts + i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) P[b] = s / count;
+}
+
+// upstream gradient of the mean of relu(void - reach) over the region
+__global__ void k_cav_bwd_init(const double* __restrict__ vsc, const double* __restrict__ reach,
+                               double* __restrict__ gvoid, double* __restrict__ greach, double* __restrict__ gvconn,
+                               CavGeo G, int focus, double inv_count) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const size_t i = (size_t)blockIdx.y * G.M + v;
+  int x, y, z;
+  G.coords(v, x, y, z);
+  const double g = (in_region(G, focus, x, y, z) && vsc[i] - reach[i] > 0.0) ? inv_count : 0.0;
+  gvoid[i] = g;
+  greach[i] = -g;
+  gvconn[i] = 0.0;
+}
+
+// backward of one flood-fill step reach_out = min(vconn, maxpool(reach_in))
+__global__ void k_cav_bwd_step(const double* __restrict__ gout, const double* __restrict__ vconn,
+                               const double* __restrict__ dil, const int* __restrict__ src,
+                               double* __restrict__ gin, double* __restrict__ gvconn, CavGeo G, int rad) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const size_t base = (size_t)blockIdx.y * G.M;
+  gvconn[base + v] += min_grad(vconn[base + v], dil[base + v], gout[base + v]);
+  int x, y, z;
+  G.coords(v, x, y, z);
+  double acc = 0.0;
+  for (int dx = -rad; dx <= rad; ++dx)
+    for (int dy = -rad; dy <= rad; ++dy)
+      for (int dz = -rad; dz <= rad; ++dz) {
+        size_t q;
+        if (!G.shift(x, y, z, dx, dy, dz, q)) continue;
+        if (src[base + q] == (int)v) acc += min_grad(dil[base + q], vconn[base + q], gout[base + q]);
+      }
+  gin[base + v] = acc;
+}
+
+// g_out += seed * g_reach (the seeded start of the flood fill)
+__global__ void k_cav_bwd_seed(const double* __restrict__ greach, double* __restrict__ gvconn, CavGeo G, int seed) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const size_t i = (size_t)blockIdx.y * G.M + v;
+  int x, y, z;
+  G.coords(v, x, y, z);
+  if (is_seed(G, seed, x, y, z)) gvconn[i] += greach[i];
+}
+
+// out (+)= adjoint of a max-pool with argmax src applied to g
+__global__ void k_cav_pool_adj(const double* __restrict__ g, const int* __restrict__ src, double* __restrict__ out,
+                               CavGeo G, int rad, int accumulate) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const size_t base = (size_t)blockIdx.y * G.M;
+  int x, y, z;
+  G.coords(v, x, y, z);
+  double acc = 0.0;
+  for (int dx = -rad; dx <= rad; ++dx)
+    for (int dy = -rad; dy <= rad; ++dy)
+      for (int dz = -rad; dz <= rad; ++dz) {
+        size_t q;
+        if (!G.shift(x, y, z, dx, dy, dz, q)) continue;
+        if (src[base + q] == (int)v) acc += g[base + q];
+      }
+  out[base + v] = accumulate ? out[base + v] + acc : acc;
+}
+
+__global__ void k_cav_add(double* __restrict__ a, const double* __restrict__ b, size_t n) {
+  const size_t i = (size_t)blockIdx.x * kT + threadIdx.x + (size_t)blockIdx.y * n;
+  if ((size_t)blockIdx.x * kT + threadIdx.x < n) a[i] += b[i];
+}
+
+// dP/drho of the cell: the tile copies summed, times d sigmoid / d rho
+__global__ void k_cav_untile(const double* __restrict__ gvoid, const double* __restrict__ void_uc,
+                             double* __restrict__ grad, CavGeo G, double beta) {
+  const int r = G.r;
+  const size_t N = (size_t)r * r * r;
+  const size_t i = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (i >= N) return;
+  const int b = blockIdx.y;
+  const int x = (int)(i / ((size_t)r * r)), y = (int)((i / r) % r), z = (int)(i % r);
+  double acc = 0.0;
+  for (int a = 0; a < G.X / r; ++a)
+    for (int c = 0; c < G.Y / r; ++c)
+      for (int d = 0; d < G.Z / r; ++d) acc += gvoid[(size_t)b * G.M + G.index(a * r + x, c * r + y, d * r + z)];
+  const double s = void_uc[(size_t)b * N + i];
+  grad[(size_t)b * N + i] = acc * (-beta) * s * (1.0 - s);
+}
+
+void cavity(const double* rho, const CavityPlan& p, double* P, double* grad, void* work, cudaStream_t s) {
+  if (p.r < 2 || p.B < 1 || p.rad < 0 || p.min_channel_rad < 0 || p.nsteps < 0)
+    throw std::runtime_error("cavity penalty: bad sizes");
+  for (int a = 0; a < 3; ++a)
+    if (p.tiles[a] < 1) throw std::runtime_error("cavity penalty: tiles must be >= 1");
+  const bool array = p.tiles[0] > 1 || p.tiles[1] > 1 || p.tiles[2] > 1;
+  CavGeo G{p.r, p.dims(0), p.dims(1), p.dims(2), p.M(), (p.periodic && !array) ? 1 : 0};
+  if (G.periodic) {
+    const int mn = std::min(G.X, std::min(G.Y, G.Z));
+    if (2 * p.rad + 1 > mn || 2 * p.min_channel_rad + 1 > mn)
+      throw std::runtime_error("cavity penalty: window wider than the periodic cell");
+  }
+  if (G.M > (size_t)INT32_MAX) throw std::runtime_error("cavity penalty: supercell too large");
+  CavWork w;
+  cav_parts(p, work, &w);
+  const size_t N = (size_t)p.r * p.r * p.r;
+  const dim3 gN(nb(N), p.B), gM(nb(G.M), p.B);
+  const int focus = p.focused() ? 1 : 0;
+  const double count = focus ? (double)N : (double)G.M;
+  PR_LAUNCH(k_cav_void<<<gN, kT, 0, s>>>(rho, w.void_uc, N, p.void_thresh, p.beta));
+  PR_LAUNCH(k_cav_tile<<<gM, kT, 0, s>>>(w.void_uc, w.vsc, G));
+  const double* vconn = w.vsc;
+  if (p.min_channel_rad > 0) {  // opening: erosion (-maxpool(-x), pad 1) then dilation (pad 0)
+    PR_LAUNCH(k_cav_pool<<<gM, kT, 0, s>>>(w.vsc, w.er, w.er_src, G, p.min_channel_rad, -1.0, -1.0));
+    PR_LAUNCH(k_cav_pool<<<gM, kT, 0, s>>>(w.er, w.vconn, w.di_src, G, p.min_channel_rad, 1.0, 0.0));
+    vconn = w.vconn;
+  }
+  PR_LAUNCH(k_cav_seed<<<gM, kT, 0, s>>>(vconn, w.reach0, G, p.seed));
+  double* reach = w.reach0;
+  double* other = w.reach1;
+  const int steps = p.rad > 0 ? p.nsteps : 0;
+  for (int t = 0; t < steps; ++t) {
+    PR_LAUNCH(k_cav_step<<<gM, kT, 0, s>>>(reach, vconn, w.dil + (size_t)t * p.B * G.M, w.src + (size_t)t * p.B * G.M,
+                                          other, G, p.rad));
+    std::swap(reach, other);
+  }
+  PR_LAUNCH(k_cav_trapped<<<gM, kT, 0, s>>>(w.vsc, reach, w.part, G, focus));
+  PR_LAUNCH(k_cav_total<<<p.B, kT, 0, s>>>(w.part, (int)gM.x, P, count));
+  if (!grad) return;
+  double* gr = w.gr0;
+  double* gr_other = w.gr1;
+  PR_LAUNCH(k_cav_bwd_init<<<gM, kT, 0, s>>>(w.vsc, reach, w.gvoid, gr, w.gvconn, G, focus, 1.0 / count));
+  for (int t = steps - 1; t >= 0; --t) {
+    PR_LAUNCH(k_cav_bwd_step<<<gM, kT, 0, s>>>(gr, vconn, w.dil + (size_t)t * p.B * G.M,
+                                              w.src + (size_t)t * p.B * G.M, gr_other, w.gvconn, G, p.rad));
+    std::swap(gr, gr_other);
+  }
+  PR_LAUNCH(k_cav_bwd_seed<<<gM, kT, 0, s>>>(gr, w.gvconn, G, p.seed));
+  if (p.min_channel_rad > 0) {
+    PR_LAUNCH(k_cav_pool_adj<<<gM, kT, 0, s>>>(w.gvconn, w.di_src, w.gtmp, G, p.min_channel_rad, 0));
+    PR_LAUNCH(k_cav_pool_adj<<<gM, kT, 0, s>>>(w.gtmp, w.er_src, w.gvoid, G, p.min_channel_rad, 1));
+  } else {
+    PR_LAUNCH(k_cav_add<<<gM, kT, 0, s>>>(w.gvoid, w.gvconn, G.M));
+  }
+  PR_LAUNCH(k_cav_untile<<<gN, kT, 0, s>>>(w.gvoid, w.void_uc, grad, G, p.beta));
+}
+
+}  // namespace maple_pr

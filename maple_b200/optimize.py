@@ -85,6 +85,17 @@ def avg_filter3d_x_periodic(x_vec: torch.Tensor, elem_coords: torch.Tensor, res:
     return out[order].reshape(-1, 1).to(x_vec.dtype)
 
 
+def _parse_tiles_xyz(tiles_xyz, tiles: int):
+    """(tx, ty, tz) from "tx,ty,tz" / "tx ty tz" or a single count (main_IHD_v3.py:101-115)."""
+    if tiles_xyz is None:
+        t = max(1, int(tiles))
+        return t, t, t
+    parts = [p for p in str(tiles_xyz).replace(" ", ",").split(",") if p != ""]
+    if len(parts) != 3:
+        raise ValueError("--cavity_tiles_xyz must have 3 integers, e.g. 3,3,3")
+    return tuple(max(1, int(p)) for p in parts)
+
+
 def parse_symmetry(symmetry: str):
     """(kind, axes) of a symmetry spec, as main_IHD_v3.py:221-256: "none";
     "mirror" with the x/y/z letters present ("octant", "1/8", "one_eighth" =
@@ -210,16 +221,14 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
                                     dx_tol: float = 0.01) -> RunResult:
     """OC loop of main_IHD_v3.py:492-891 on the GPU.
 
-    Same arguments and outputs as the reference.  Supported: every symmetry
-    ("none", mirror axes, "cubic"/"iso") and lambda_print = lambda_cavity = 0
-    (the manufacturability penalties are not part of this package).  Extra keywords: ``x_init`` (an (N,1) design to
+    Same arguments and outputs as the reference, including every symmetry
+    ("none", mirror axes, "cubic"/"iso") and the overhang / cavity penalties
+    (computed on the GPU with the gradients of the reference's autograd).  Extra keywords: ``x_init`` (an (N,1) design to
     start from, bypassing ``init_mode``), ``precision``/``rtol`` (default: the
     IHD module's), ``stop_rule`` "reference" (stall test of
     main_IHD_v3.py:611-618, 711-714) or "dx" (stop when max|dx| < dx_tol).
     """
     sym_kind, sym_axes = parse_symmetry(symmetry)
-    if float(lambda_print) > 0 or float(lambda_cavity) > 0:
-        raise NotImplementedError("printability / cavity penalties are not supported (use lambda = 0)")
     device = ihd_module.device
     setup_seed(seed)
     os.makedirs(output_dir, exist_ok=True)
@@ -248,14 +257,28 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
     def simp(xv):
         return (rho_min + (1.0 - rho_min) * (xv.clamp(xmin, 1.0) ** penal)).reshape(-1, 1).clamp(rho_min, 1.0)
 
+    hc = ihd_module.homog_ctx
+    use_print, use_cavity = float(lambda_print) > 0.0, float(lambda_cavity) > 0.0
+    if use_print or use_cavity:
+        hc.set_penalties(float(lambda_print), float(overhang_deg), float(lambda_cavity), void_thresh=float(cavity_thresh),
+                         beta=float(cavity_beta), min_channel_rad=int(min_channel_rad), rad=int(cavity_rad),
+                         iters=int(cavity_iters or 0), tiles=_parse_tiles_xyz(cavity_tiles_xyz, cavity_tiles),
+                         focus_center=bool(cavity_focus_center), seed_faces=str(cavity_seed_faces), periodic=True)
+
+    def penalties(rho_col):
+        if not (use_print or use_cavity):
+            return 0.0, 0.0
+        o = hc.penalties(rho_col.reshape(1, -1).contiguous(), overhang=use_print, cavity=use_cavity, grad=False)
+        return (float(o["P_print"][0]) if use_print else 0.0, float(o["P_cavity"][0]) if use_cavity else 0.0)
+
     J_raw_init = evaluate_J(ihd_module, batch, simp(x), obj=objective)
-    J_total_init = float(J_raw_init)
+    P_print_init, P_cavity_init = penalties(simp(x))
+    J_total_init = float(J_raw_init) - float(lambda_print) * P_print_init - float(lambda_cavity) * P_cavity_init
     if save_iter_log and log_csv is not None:
         with open(log_csv, "w", newline="") as f:
             csv.writer(f).writerow(["iter", "J_total", "J_raw", "P_print", "P_cavity", "mean_x", "mean_rho", "dx_max",
                                     "dx_mean", "time_sec"])
 
-    hc = ihd_module.homog_ctx
     hc.set_symmetry(sym_kind, sym_axes)
     w = torch.tensor([objective_weights(objective)], dtype=torch.float64, device=device)
     vf = torch.tensor([float(volfrac)], dtype=torch.float64, device=device)
@@ -269,6 +292,8 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
                          filter_k=int(filter_k) if filter_k and int(filter_k) > 1 else 0, precision=precision,
                          rtol=rtol, maxit=ihd_module.maxit, warm=ihd_module.warm_start)
         J_val = float(out["J"].item())
+        J_raw_val = float(out["J_raw"].item())
+        P_print_val, P_cavity_val = float(out["P_print"].item()), float(out["P_cavity"].item())
         dx_max, dx_mean = (float(v) for v in out["stats"][0].tolist())
         x_mean = float(x.clamp(xmin, 1.0).mean().item())
         rho_mean = float(simp(x).mean().item())
@@ -280,10 +305,11 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
         t_now = time.time() - t0
         if save_iter_log and log_csv is not None:
             with open(log_csv, "a", newline="") as f:
-                csv.writer(f).writerow([it_run, J_prev, J_val, 0.0, 0.0, x_mean, rho_mean, dx_max, dx_mean, t_now])
+                csv.writer(f).writerow([it_run, J_val, J_raw_val, P_print_val, P_cavity_val, x_mean, rho_mean, dx_max,
+                                        dx_mean, t_now])
         if verbose:
-            print(f"it={it_run:04d}  J_total={J_prev:.6e}  J_raw={J_val:.6e}  P_print=0.000000e+00  "
-                  f"P_cavity=0.000000e+00  mean_x={x_mean:.4f}  mean_rho={rho_mean:.4f}  "
+            print(f"it={it_run:04d}  J_total={J_val:.6e}  J_raw={J_raw_val:.6e}  P_print={P_print_val:.6e}  "
+                  f"P_cavity={P_cavity_val:.6e}  mean_x={x_mean:.4f}  mean_rho={rho_mean:.4f}  "
                   f"dx_max={dx_max:.3e}  dx_mean={dx_mean:.3e}  stall={stall}/{patience}")
         if stop_rule == "reference" and stall >= patience:
             converged = True
@@ -295,6 +321,10 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
     hc.set_symmetry("none")
     rho_final = simp(x)
     J_raw_final = evaluate_J(ihd_module, batch, rho_final, obj=objective)
+    P_print_final, P_cavity_final = penalties(rho_final)
+    J_total_final = float(J_raw_final) - float(lambda_print) * P_print_final - float(lambda_cavity) * P_cavity_final
+    if use_print or use_cavity:
+        hc.set_penalties(0.0, float(overhang_deg), 0.0)
     rho_final_grid = rho_final.reshape(res, res, res).detach().cpu().numpy().astype(np.float32)
     np.save(final_rho_npy, rho_final_grid)
     summary = {
@@ -310,8 +340,9 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
         "volfrac_target": float(volfrac), "penal": float(penal), "rho_min": float(rho_min), "move": float(move),
         "xmin": float(xmin), "mesh_every": int(mesh_every), "mesh_res": int(mesh_res), "mesh_iso": float(mesh_iso),
         "mesh_pad": int(mesh_pad), "J_raw_init": float(J_raw_init), "J_raw_final": float(J_raw_final),
-        "J_total_init": float(J_total_init), "J_total_final": float(J_raw_final), "P_print_init": 0.0,
-        "P_print_final": 0.0, "P_cavity_init": 0.0, "P_cavity_final": 0.0,
+        "J_total_init": float(J_total_init), "J_total_final": float(J_total_final),
+        "P_print_init": float(P_print_init), "P_print_final": float(P_print_final),
+        "P_cavity_init": float(P_cavity_init), "P_cavity_final": float(P_cavity_final),
         "log_csv": (None if log_csv is None else os.path.abspath(log_csv)),
         "rho_final_npy": os.path.abspath(final_rho_npy), "meshes_dir": os.path.abspath(meshes_dir),
         "time_sec": float(time.time() - t0),
@@ -320,7 +351,8 @@ def optimize_inverse_homogenization(ihd_module: IHD, batch: Dict[str, torch.Tens
         with open(summary_json, "w", encoding="utf-8") as f:
             json.dump(summary, f, ensure_ascii=False, indent=2)
     return RunResult(J_raw_init=float(J_raw_init), J_raw_final=float(J_raw_final), J_total_init=float(J_total_init),
-                     J_total_final=float(J_raw_final), P_print_init=0.0, P_print_final=0.0, P_cavity_init=0.0,
-                     P_cavity_final=0.0, iters_run=int(it_run), converged=bool(converged), rho_final=rho_final_grid,
+                     J_total_final=float(J_total_final), P_print_init=float(P_print_init),
+                     P_print_final=float(P_print_final), P_cavity_init=float(P_cavity_init),
+                     P_cavity_final=float(P_cavity_final), iters_run=int(it_run), converged=bool(converged), rho_final=rho_final_grid,
                      log_csv=log_csv, summary_json=summary_json, meshes_dir=meshes_dir,
                      rho_final_npy=final_rho_npy, final_obj=final_obj)

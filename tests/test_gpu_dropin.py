@@ -157,14 +157,6 @@ def test_optimize_inverse_homogenization(ihd8, golden, tmp_path):
     rho_final = np.load(os.path.join(tmp_path, "rho_final.npy"))
     ref = (1e-9 + (1 - 1e-9) * g["x3"] ** 3).reshape(8, 8, 8).astype(np.float32)
     assert rho_final.shape == (8, 8, 8) and np.abs(rho_final - ref).max() < 1e-6
-    with pytest.raises(NotImplementedError):
-        optimize_inverse_homogenization(
-            ihd8, batch, res=8, objective="shear", init_mode="noise", volfrac=0.25, penal=3.0, rho_min=1e-9,
-            move=0.2, xmin=1e-3, iters=1, seed=0, symmetry="cubic", lambda_print=0.5, overhang_deg=45.0,
-            lambda_cavity=0.0, cavity_thresh=0.5, cavity_beta=20.0, min_channel_rad=0, cavity_rad=1,
-            cavity_seed_faces="all", cavity_iters=128, cavity_tiles=1, cavity_tiles_xyz=None,
-            cavity_focus_center=True, filter_k=3, output_dir=str(tmp_path), mesh_every=0, mesh_res=32, mesh_iso=0.3,
-            mesh_pad=2, verbose=False)
 
 
 def test_batched_cells_match_single_cell_runs(lib):

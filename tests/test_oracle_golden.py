@@ -188,12 +188,10 @@ def _print_case(kind, kw, rho, r=8):
     if kind == "over":
         return O.overhang_penalty(rho, r, kw.get("overhang_deg", 45.0), kw.get("periodic_xy", True))
     tiles = tuple(kw.get("tiles_xyz", (1, 1, 1)))
-    if kind == "closed" and not kw.get("periodic_xyz", True):
-        pytest.skip("non-periodic single-cell flood fill is not on the optimizer's path")
     return O.cavity_penalty(rho, r, void_thresh=kw.get("void_thresh", 0.5), beta=kw.get("beta", 20.0),
                             min_channel_rad=kw.get("min_channel_rad", 0), rad=kw.get("rad", 1),
                             iters=kw.get("iters", 0), tiles=tiles, focus_center=kw.get("focus_center", True),
-                            seed_faces=kw.get("seed_faces", "all"))
+                            seed_faces=kw.get("seed_faces", "all"), periodic=kw.get("periodic_xyz", None))
 
 
 def _print_cases(golden):
@@ -207,8 +205,6 @@ def test_printability_penalties_match_reference_autograd(golden, field):
     g, cases = _print_cases(golden)
     rho = g[f"field_{field}"]
     for i, (kind, kw) in enumerate(cases):
-        if kind == "closed" and not kw.get("periodic_xyz", True):
-            continue
         P, grad = _print_case(kind, kw, rho)
         ref_P, ref_g = g[f"{field}_{i}_P"], g[f"{field}_{i}_grad"]
         assert abs(P - ref_P) <= 1e-13 * max(1.0, abs(ref_P)), (i, kind, kw)
