@@ -1125,7 +1125,7 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
   });
 }
 
-unsigned long long maple_launch_count(void) { return g_launches.load(); }
+unsigned long long maple_launch_count(void) { return g_launches.load() + maple_pr::launches(); }
 
 int maple_profile_enable(maple_ctx* c, int enable, int max_launches) {
   return guarded([&] {
@@ -1611,11 +1611,11 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
     }
     // manufacturability penalties at the solves' densities (main_IHD_v3.py:649-686)
     const bool pen_p = c->lambda_print > 0 && c->print_set, pen_c = c->lambda_cavity > 0 && c->cavity_set;
-    if (pen_p || pen_c) {
-      KL(c, st, k_simp<<<nblk((size_t)B * N), kThreads, 0, st>>>(xu, c->pen_rho, nullptr, (size_t)B * N, N, xmin, penal,
-                                                               rho_min, c->active));
-      run_penalties(c, c->pen_rho, pen_p, pen_c, st);
-    }
+    auto run_pen = [&](cudaStream_t ps) {
+      KL(c, ps, k_simp<<<nblk((size_t)B * N), kThreads, 0, ps>>>(xu, c->pen_rho, nullptr, (size_t)B * N, N, xmin,
+                                                               penal, rho_min, c->active));
+      run_penalties(c, c->pen_rho, pen_p, pen_c, ps);
+    };
     // one physics: SIMP map, hierarchy, RHS, MG-PCG solve, energies
     auto run_phys = [&](int phys, cudaStream_t ps, int* it_out) {
       LaneScope lane(phys);
@@ -1636,9 +1636,14 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
     if (!need_k) c->ph[1].energies = false;
     if (need_ch) ensure_prec(c, 0, prec);  // all allocation happens here, on this thread
     if (need_k) ensure_prec(c, 1, prec);
-    if (need_ch && need_k && c->concurrent && !c->profiling) {
-      // the thermal solve runs on a second stream, driven by a second host
-      // thread (each solve waits on its own convergence checks)
+    // work of the caller's stream and of the second stream: with concurrency,
+    // the penalties and (when both physics are needed) the thermal solve run
+    // on the second stream, driven by a second host thread (each solve waits
+    // on its own convergence checks)
+    const bool pen = pen_p || pen_c;
+    const bool conc = c->concurrent && !c->profiling;
+    const bool aux_thermal = conc && need_ch && need_k, aux_pen = conc && pen && (need_ch || need_k);
+    if (aux_thermal || aux_pen) {
       if (!c->aux_stream) {
         CK(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&c->aux_fork, cudaEventDisableTiming));
@@ -1651,13 +1656,15 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       std::thread worker([&] {
         try {
           CK(cudaSetDevice(dev));
-          run_phys(1, c->aux_stream, it_th.data());
+          if (aux_pen) run_pen(c->aux_stream);
+          if (aux_thermal) run_phys(1, c->aux_stream, it_th.data());
         } catch (...) {
           thermal_err = std::current_exception();
         }
       });
       try {
-        run_phys(0, st, it_el.data());
+        if (need_ch) run_phys(0, st, it_el.data());
+        if (need_k && !aux_thermal) run_phys(1, st, it_th.data());
       } catch (...) {
         worker.join();
         throw;
@@ -1667,6 +1674,7 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       CK(cudaEventRecord(c->aux_join, c->aux_stream));
       CK(cudaStreamWaitEvent(st, c->aux_join, 0));
     } else {
+      if (pen) run_pen(st);
       if (need_ch) run_phys(0, st, it_el.data());
       if (need_k) run_phys(1, st, it_th.data());
     }

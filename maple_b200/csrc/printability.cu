@@ -217,9 +217,11 @@ struct CavGeo {
 };
 
 struct CavWork {
-  double *void_uc, *vsc, *er, *vconn, *reach0, *reach1, *dil, *gr0, *gr1, *gvconn, *gvoid, *gtmp, *part;
-  int *er_src, *di_src, *src;
+  double *void_uc, *vsc, *er, *vconn, *reach0, *reach1, *t1, *t2, *dil, *gr0, *gr1, *g1, *g2, *gvconn, *gvoid, *part;
+  signed char *er_off, *di_off, *off;  // per-pass argmax offsets: [3][B][M] (opening) and [steps][3][B][M]
 };
+
+constexpr signed char kPadOff = 127;  // the pass picked a padding cell
 
 static size_t cav_parts(const CavityPlan& p, void* work, CavWork* o) {
   const size_t B = p.B, M = p.M(), N = (size_t)p.r * p.r * p.r, S = (size_t)std::max(p.nsteps, 0);
@@ -237,18 +239,21 @@ static size_t cav_parts(const CavityPlan& p, void* work, CavWork* o) {
   if (p.min_channel_rad > 0) {
     c.er = reinterpret_cast<double*>(take(B * M * 8));
     c.vconn = reinterpret_cast<double*>(take(B * M * 8));
-    c.er_src = reinterpret_cast<int*>(take(B * M * 4));
-    c.di_src = reinterpret_cast<int*>(take(B * M * 4));
+    c.er_off = reinterpret_cast<signed char*>(take(3 * B * M));
+    c.di_off = reinterpret_cast<signed char*>(take(3 * B * M));
   }
   c.reach0 = reinterpret_cast<double*>(take(B * M * 8));
   c.reach1 = reinterpret_cast<double*>(take(B * M * 8));
+  c.t1 = reinterpret_cast<double*>(take(B * M * 8));
+  c.t2 = reinterpret_cast<double*>(take(B * M * 8));
   c.dil = reinterpret_cast<double*>(take(B * M * S * 8));
-  c.src = reinterpret_cast<int*>(take(B * M * S * 4));
+  c.off = reinterpret_cast<signed char*>(take(3 * B * M * S));
   c.gr0 = reinterpret_cast<double*>(take(B * M * 8));
   c.gr1 = reinterpret_cast<double*>(take(B * M * 8));
+  c.g1 = reinterpret_cast<double*>(take(B * M * 8));
+  c.g2 = reinterpret_cast<double*>(take(B * M * 8));
   c.gvconn = reinterpret_cast<double*>(take(B * M * 8));
   c.gvoid = reinterpret_cast<double*>(take(B * M * 8));
-  c.gtmp = reinterpret_cast<double*>(take(B * M * 8));
   c.part = reinterpret_cast<double*>(take(B * nparts * 8));
   if (o) *o = c;
   return off;
@@ -273,38 +278,58 @@ __global__ void k_cav_tile(const double* __restrict__ void_uc, double* __restric
   vsc[(size_t)b * G.M + v] = void_uc[(size_t)b * r * r * r + ((size_t)(x % r) * r + (y % r)) * r + (z % r)];
 }
 
-// out = sign * maxpool(sign * in) over a (2 rad + 1)^3 window (padding value pad
-// in the sign * in domain), first maximum in (x, y, z) scan order; src = its
-// index (-1: padding)
-__global__ void k_cav_pool(const double* __restrict__ in, double* __restrict__ out, int* __restrict__ src, CavGeo G,
-                           int rad, double sign, double pad) {
+// One axis of a separable (2 rad + 1)^3 max pool:
+//   out(v) = so * max_{d=-rad..rad} (v + d e_axis inside ? si * in(v + d e_axis) : pad)
+// keeping the first maximum (strict >); off(v) = its d, or kPadOff for padding.
+// Passes along z, then y, then x reproduce the first maximum of the 3-D window
+// in (x, y, z) scan order: it is the lexicographically smallest (dx, dy, dz)
+// among the maxima, and each pass keeps the smallest offset of its axis.
+// With fuse_min, the result also gives min_out = min(vmin, out) (a flood-fill step).
+__global__ void k_cav_pass(const double* __restrict__ in, double* __restrict__ out, signed char* __restrict__ off,
+                           CavGeo G, int axis, int rad, double si, double so, double pad,
+                           const double* __restrict__ vmin, double* __restrict__ min_out) {
   const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
   if (v >= G.M) return;
   const size_t base = (size_t)blockIdx.y * G.M;
   int x, y, z;
   G.coords(v, x, y, z);
   double best = -INFINITY;
-  int bsrc = -1;
-  for (int dx = -rad; dx <= rad; ++dx)
-    for (int dy = -rad; dy <= rad; ++dy)
-      for (int dz = -rad; dz <= rad; ++dz) {
-        size_t q;
-        double val;
-        int s;
-        if (G.shift(x, y, z, dx, dy, dz, q)) {
-          val = sign * in[base + q];
-          s = (int)q;
-        } else {
-          val = pad;
-          s = -1;
-        }
-        if (val > best) {
-          best = val;
-          bsrc = s;
-        }
-      }
-  out[base + v] = sign * best;
-  src[base + v] = bsrc;
+  int bd = kPadOff;
+  for (int d = -rad; d <= rad; ++d) {
+    size_t q;
+    const bool inside = G.shift(x, y, z, axis == 0 ? d : 0, axis == 1 ? d : 0, axis == 2 ? d : 0, q);
+    const double val = inside ? si * in[base + q] : pad;
+    if (val > best) {
+      best = val;
+      bd = inside ? d : kPadOff;
+    }
+  }
+  const double res = so * best;
+  out[base + v] = res;
+  off[base + v] = (signed char)bd;
+  if (min_out) min_out[base + v] = fmin(vmin[base + v], res);
+}
+
+// Adjoint of one pass: gin(p) (+)= sum over the outputs q = p - d e_axis that
+// picked p (off(q) == d) of their gradient; with vmin, the output gradient is
+// first taken through min(vmin, out): the dil branch of min_grad.
+__global__ void k_cav_pass_adj(const double* __restrict__ gout, const signed char* __restrict__ off,
+                               double* __restrict__ gin, CavGeo G, int axis, int rad, int accumulate,
+                               const double* __restrict__ vmin, const double* __restrict__ outv) {
+  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
+  if (v >= G.M) return;
+  const size_t base = (size_t)blockIdx.y * G.M;
+  int x, y, z;
+  G.coords(v, x, y, z);
+  double acc = 0.0;
+  for (int d = -rad; d <= rad; ++d) {
+    size_t q;
+    if (!G.shift(x, y, z, axis == 0 ? -d : 0, axis == 1 ? -d : 0, axis == 2 ? -d : 0, q)) continue;
+    if (off[base + q] != d) continue;
+    const double g = gout[base + q];
+    acc += vmin ? min_grad(outv[base + q], vmin[base + q], g) : g;
+  }
+  gin[base + v] = accumulate ? gin[base + v] + acc : acc;
 }
 
 __device__ __forceinline__ bool is_seed(const CavGeo& G, int seed, int x, int y, int z) {
@@ -324,40 +349,6 @@ __global__ void k_cav_seed(const double* __restrict__ vconn, double* __restrict_
   int x, y, z;
   G.coords(v, x, y, z);
   reach[i] = is_seed(G, seed, x, y, z) ? vconn[i] : 0.0;
-}
-
-// one flood-fill step: dil = maxpool(reach_in), reach_out = min(vconn, dil)
-__global__ void k_cav_step(const double* __restrict__ reach_in, const double* __restrict__ vconn,
-                           double* __restrict__ dil, int* __restrict__ src, double* __restrict__ reach_out, CavGeo G,
-                           int rad) {
-  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
-  if (v >= G.M) return;
-  const size_t base = (size_t)blockIdx.y * G.M;
-  int x, y, z;
-  G.coords(v, x, y, z);
-  double best = -INFINITY;
-  int bsrc = -1;
-  for (int dx = -rad; dx <= rad; ++dx)
-    for (int dy = -rad; dy <= rad; ++dy)
-      for (int dz = -rad; dz <= rad; ++dz) {
-        size_t q;
-        double val;
-        int s;
-        if (G.shift(x, y, z, dx, dy, dz, q)) {
-          val = reach_in[base + q];
-          s = (int)q;
-        } else {
-          val = 0.0;
-          s = -1;
-        }
-        if (val > best) {
-          best = val;
-          bsrc = s;
-        }
-      }
-  dil[base + v] = best;
-  src[base + v] = bsrc;
-  reach_out[base + v] = fmin(vconn[base + v], best);
 }
 
 __device__ __forceinline__ bool in_region(const CavGeo& G, int focus, int x, int y, int z) {
@@ -404,25 +395,13 @@ __global__ void k_cav_bwd_init(const double* __restrict__ vsc, const double* __r
   gvconn[i] = 0.0;
 }
 
-// backward of one flood-fill step reach_out = min(vconn, maxpool(reach_in))
-__global__ void k_cav_bwd_step(const double* __restrict__ gout, const double* __restrict__ vconn,
-                               const double* __restrict__ dil, const int* __restrict__ src,
-                               double* __restrict__ gin, double* __restrict__ gvconn, CavGeo G, int rad) {
+// gvconn += the vconn branch of min(vconn, dil) for upstream gout
+__global__ void k_cav_min_vconn(const double* __restrict__ gout, const double* __restrict__ vconn,
+                                const double* __restrict__ dil, double* __restrict__ gvconn, size_t M) {
   const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
-  if (v >= G.M) return;
-  const size_t base = (size_t)blockIdx.y * G.M;
-  gvconn[base + v] += min_grad(vconn[base + v], dil[base + v], gout[base + v]);
-  int x, y, z;
-  G.coords(v, x, y, z);
-  double acc = 0.0;
-  for (int dx = -rad; dx <= rad; ++dx)
-    for (int dy = -rad; dy <= rad; ++dy)
-      for (int dz = -rad; dz <= rad; ++dz) {
-        size_t q;
-        if (!G.shift(x, y, z, dx, dy, dz, q)) continue;
-        if (src[base + q] == (int)v) acc += min_grad(dil[base + q], vconn[base + q], gout[base + q]);
-      }
-  gin[base + v] = acc;
+  if (v >= M) return;
+  const size_t i = (size_t)blockIdx.y * M + v;
+  gvconn[i] += min_grad(vconn[i], dil[i], gout[i]);
 }
 
 // g_out += seed * g_reach (the seeded start of the flood fill)
@@ -433,25 +412,6 @@ __global__ void k_cav_bwd_seed(const double* __restrict__ greach, double* __rest
   int x, y, z;
   G.coords(v, x, y, z);
   if (is_seed(G, seed, x, y, z)) gvconn[i] += greach[i];
-}
-
-// out (+)= adjoint of a max-pool with argmax src applied to g
-__global__ void k_cav_pool_adj(const double* __restrict__ g, const int* __restrict__ src, double* __restrict__ out,
-                               CavGeo G, int rad, int accumulate) {
-  const size_t v = (size_t)blockIdx.x * kT + threadIdx.x;
-  if (v >= G.M) return;
-  const size_t base = (size_t)blockIdx.y * G.M;
-  int x, y, z;
-  G.coords(v, x, y, z);
-  double acc = 0.0;
-  for (int dx = -rad; dx <= rad; ++dx)
-    for (int dy = -rad; dy <= rad; ++dy)
-      for (int dz = -rad; dz <= rad; ++dz) {
-        size_t q;
-        if (!G.shift(x, y, z, dx, dy, dz, q)) continue;
-        if (src[base + q] == (int)v) acc += g[base + q];
-      }
-  out[base + v] = accumulate ? out[base + v] + acc : acc;
 }
 
 __global__ void k_cav_add(double* __restrict__ a, const double* __restrict__ b, size_t n) {
@@ -479,6 +439,7 @@ __global__ void k_cav_untile(const double* __restrict__ gvoid, const double* __r
 void cavity(const double* rho, const CavityPlan& p, double* P, double* grad, void* work, cudaStream_t s) {
   if (p.r < 2 || p.B < 1 || p.rad < 0 || p.min_channel_rad < 0 || p.nsteps < 0)
     throw std::runtime_error("cavity penalty: bad sizes");
+  if (p.rad > 100 || p.min_channel_rad > 100) throw std::runtime_error("cavity penalty: radius too large");
   for (int a = 0; a < 3; ++a)
     if (p.tiles[a] < 1) throw std::runtime_error("cavity penalty: tiles must be >= 1");
   const bool array = p.tiles[0] > 1 || p.tiles[1] > 1 || p.tiles[2] > 1;
@@ -491,16 +452,31 @@ void cavity(const double* rho, const CavityPlan& p, double* P, double* grad, voi
   if (G.M > (size_t)INT32_MAX) throw std::runtime_error("cavity penalty: supercell too large");
   CavWork w;
   cav_parts(p, work, &w);
-  const size_t N = (size_t)p.r * p.r * p.r;
+  const size_t N = (size_t)p.r * p.r * p.r, BM = (size_t)p.B * G.M;
   const dim3 gN(nb(N), p.B), gM(nb(G.M), p.B);
   const int focus = p.focused() ? 1 : 0;
   const double count = focus ? (double)N : (double)G.M;
+  const int mcr = p.min_channel_rad;
+  // three passes z, y, x of a separable pool: in -> out, offsets off[0..2]
+  auto pool3 = [&](const double* in, double* out, signed char* off, int rad, double sign, double pad,
+                   const double* vmin, double* min_out) {
+    PR_LAUNCH(k_cav_pass<<<gM, kT, 0, s>>>(in, w.t1, off, G, 2, rad, sign, 1.0, pad, nullptr, nullptr));
+    PR_LAUNCH(k_cav_pass<<<gM, kT, 0, s>>>(w.t1, w.t2, off + BM, G, 1, rad, 1.0, 1.0, pad, nullptr, nullptr));
+    PR_LAUNCH(k_cav_pass<<<gM, kT, 0, s>>>(w.t2, out, off + 2 * BM, G, 0, rad, 1.0, sign, pad, vmin, min_out));
+  };
+  // adjoint of pool3: gout at the output -> gin (x, y, z passes in reverse)
+  auto pool3_adj = [&](const double* gout, const signed char* off, double* gin, int rad, int accumulate,
+                       const double* vmin, const double* outv) {
+    PR_LAUNCH(k_cav_pass_adj<<<gM, kT, 0, s>>>(gout, off + 2 * BM, w.g2, G, 0, rad, 0, vmin, outv));
+    PR_LAUNCH(k_cav_pass_adj<<<gM, kT, 0, s>>>(w.g2, off + BM, w.g1, G, 1, rad, 0, nullptr, nullptr));
+    PR_LAUNCH(k_cav_pass_adj<<<gM, kT, 0, s>>>(w.g1, off, gin, G, 2, rad, accumulate, nullptr, nullptr));
+  };
   PR_LAUNCH(k_cav_void<<<gN, kT, 0, s>>>(rho, w.void_uc, N, p.void_thresh, p.beta));
   PR_LAUNCH(k_cav_tile<<<gM, kT, 0, s>>>(w.void_uc, w.vsc, G));
   const double* vconn = w.vsc;
-  if (p.min_channel_rad > 0) {  // opening: erosion (-maxpool(-x), pad 1) then dilation (pad 0)
-    PR_LAUNCH(k_cav_pool<<<gM, kT, 0, s>>>(w.vsc, w.er, w.er_src, G, p.min_channel_rad, -1.0, -1.0));
-    PR_LAUNCH(k_cav_pool<<<gM, kT, 0, s>>>(w.er, w.vconn, w.di_src, G, p.min_channel_rad, 1.0, 0.0));
+  if (mcr > 0) {  // opening: erosion -maxpool(-x) with pad 1, then dilation with pad 0
+    pool3(w.vsc, w.er, w.er_off, mcr, -1.0, -1.0, nullptr, nullptr);
+    pool3(w.er, w.vconn, w.di_off, mcr, 1.0, 0.0, nullptr, nullptr);
     vconn = w.vconn;
   }
   PR_LAUNCH(k_cav_seed<<<gM, kT, 0, s>>>(vconn, w.reach0, G, p.seed));
@@ -508,8 +484,7 @@ void cavity(const double* rho, const CavityPlan& p, double* P, double* grad, voi
   double* other = w.reach1;
   const int steps = p.rad > 0 ? p.nsteps : 0;
   for (int t = 0; t < steps; ++t) {
-    PR_LAUNCH(k_cav_step<<<gM, kT, 0, s>>>(reach, vconn, w.dil + (size_t)t * p.B * G.M, w.src + (size_t)t * p.B * G.M,
-                                          other, G, p.rad));
+    pool3(reach, w.dil + (size_t)t * BM, w.off + (size_t)t * 3 * BM, p.rad, 1.0, 0.0, vconn, other);
     std::swap(reach, other);
   }
   PR_LAUNCH(k_cav_trapped<<<gM, kT, 0, s>>>(w.vsc, reach, w.part, G, focus));
@@ -519,14 +494,15 @@ void cavity(const double* rho, const CavityPlan& p, double* P, double* grad, voi
   double* gr_other = w.gr1;
   PR_LAUNCH(k_cav_bwd_init<<<gM, kT, 0, s>>>(w.vsc, reach, w.gvoid, gr, w.gvconn, G, focus, 1.0 / count));
   for (int t = steps - 1; t >= 0; --t) {
-    PR_LAUNCH(k_cav_bwd_step<<<gM, kT, 0, s>>>(gr, vconn, w.dil + (size_t)t * p.B * G.M,
-                                              w.src + (size_t)t * p.B * G.M, gr_other, w.gvconn, G, p.rad));
+    const double* dil = w.dil + (size_t)t * BM;
+    PR_LAUNCH(k_cav_min_vconn<<<gM, kT, 0, s>>>(gr, vconn, dil, w.gvconn, G.M));
+    pool3_adj(gr, w.off + (size_t)t * 3 * BM, gr_other, p.rad, 0, vconn, dil);
     std::swap(gr, gr_other);
   }
   PR_LAUNCH(k_cav_bwd_seed<<<gM, kT, 0, s>>>(gr, w.gvconn, G, p.seed));
-  if (p.min_channel_rad > 0) {
-    PR_LAUNCH(k_cav_pool_adj<<<gM, kT, 0, s>>>(w.gvconn, w.di_src, w.gtmp, G, p.min_channel_rad, 0));
-    PR_LAUNCH(k_cav_pool_adj<<<gM, kT, 0, s>>>(w.gtmp, w.er_src, w.gvoid, G, p.min_channel_rad, 1));
+  if (mcr > 0) {
+    pool3_adj(w.gvconn, w.di_off, gr_other, mcr, 0, nullptr, nullptr);  // through the dilation
+    pool3_adj(gr_other, w.er_off, w.gvoid, mcr, 1, nullptr, nullptr);   // through the erosion (signs cancel)
   } else {
     PR_LAUNCH(k_cav_add<<<gM, kT, 0, s>>>(w.gvoid, w.gvconn, G.M));
   }

@@ -776,18 +776,19 @@ def _cavity(void: np.ndarray, periodic: bool, min_channel_rad: int, rad: int, ns
 
 def cavity_penalty(rho: np.ndarray, r: int, *, void_thresh: float = 0.5, beta: float = 20.0, min_channel_rad: int = 0,
                    rad: int = 1, iters: int = 0, tiles=(1, 1, 1), focus_center: bool = True,
-                   seed_faces: str = "all"):
-    """(P, dP/drho) of cavity_penalty_closed_void (tiles (1,1,1), periodic
-    flood fill; utils/printability.py:139-220) or cavity_penalty_periodic_array
-    (tiles > 1: the cell tiled into a supercell with the supercell boundary as
-    the only outside, non-periodic; :226-323)."""
+                   seed_faces: str = "all", periodic: bool | None = None):
+    """(P, dP/drho) of cavity_penalty_closed_void (tiles (1,1,1); periodic
+    flood fill unless periodic=False; utils/printability.py:139-220) or
+    cavity_penalty_periodic_array (tiles > 1: the cell tiled into a supercell
+    whose boundary is the only outside, never periodic; :226-323)."""
     g = rho.reshape(r, r, r)
     tx, ty, tz = (max(1, int(t)) for t in tiles)
     array = max(tx, ty, tz) > 1
+    periodic = (not array) if periodic is None else (bool(periodic) and not array)
     s = 1.0 / (1.0 + np.exp(-float(beta) * (float(void_thresh) - g)))
     void = np.tile(s, (tx, ty, tz)) if array else s
     nsteps = int(iters) if int(iters) > 0 else (max(void.shape) if array else r)
-    trapped, backward = _cavity(void, not array, int(max(0, min_channel_rad)), int(max(0, rad)), nsteps, seed_faces)
+    trapped, backward = _cavity(void, periodic, int(max(0, min_channel_rad)), int(max(0, rad)), nsteps, seed_faces)
     if array and focus_center and tx >= 3 and ty >= 3 and tz >= 3:
         cx, cy, cz = tx // 2, ty // 2, tz // 2
         sl = (slice(cx * r, (cx + 1) * r), slice(cy * r, (cy + 1) * r), slice(cz * r, (cz + 1) * r))
