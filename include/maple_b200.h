@@ -235,10 +235,13 @@ unsigned long long maple_launch_count(void);
  *
  * Activations are channels-last [B][n^3][C] BF16 (voxel id x*n*n + y*n + z);
  * weights [taps][cin][cout] BF16, taps = 27 (3x3x3, tap = 9(dx+1)+3(dy+1)+dz+1)
- * or 1; bias [cout] FP32.  All convolutions are periodic (circular padding).
+ * or 1; bias [cout] FP32.  The guess network's convolutions are periodic
+ * (circular padding); maple_nn_conv3d_padded also takes zero padding
+ * (nn.Conv3d(padding=1), the Stage-II density generator's convolutions).
  * Errors: maple_nn_last_error_string().
  * ------------------------------------------------------------------------- */
 enum { MAPLE_NN_POOL = 0, MAPLE_NN_UPSAMPLE = 1, MAPLE_NN_UPSAMPLE_ADJ = 2, MAPLE_NN_POOL_ADJ = 3 };
+enum { MAPLE_NN_PAD_CIRCULAR = 0, MAPLE_NN_PAD_ZEROS = 1 };
 
 const char* maple_nn_last_error_string(void);
 unsigned long long maple_nn_launch_count(void);
@@ -248,6 +251,11 @@ unsigned long long maple_nn_launch_count(void);
  * BF16 products with FP32 accumulation on the tensor cores. */
 int maple_nn_conv3d(const void* in, const void* W, const float* bias, const void* res, void* out, float* out_f32,
                     int B, int n, int cin, int cout, int ksize, int relu, maple_stream_t stream);
+
+/* maple_nn_conv3d with the padding mode MAPLE_NN_PAD_CIRCULAR or MAPLE_NN_PAD_ZEROS. */
+int maple_nn_conv3d_padded(const void* in, const void* W, const float* bias, const void* res, void* out,
+                           float* out_f32, int B, int n, int cin, int cout, int ksize, int relu, int padding,
+                           maple_stream_t stream);
 
 /* dW += sum over cells and voxels of in(shifted by tap) x dz (FP32 [taps][cin][cout]);
  * db += sum of dz (nullable). */
@@ -331,6 +339,56 @@ int maple_nn_prolong_fields(const double* uc, double* uf, int BF, int nc, int fa
 
 /* Block average of element densities [B][(factor*nc)^3] -> [B][nc^3]. */
 int maple_nn_restrict_density(const double* rf, double* rc, int B, int nc, int factor, maple_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Stage-II density generator inference and warm-start post-processing of the
+ * Pareto dataset worker.  The generator is core/stage2/density_generator.py:
+ * 123-197 (Stage2DensityGenerator.encode_latent / decode_latent); its 3x3x3
+ * convolutions are maple_nn_conv3d_padded(..., MAPLE_NN_PAD_ZEROS).  FP32
+ * unless stated.  Errors: maple_gen_last_error_string().
+ * ------------------------------------------------------------------------- */
+const char* maple_gen_last_error_string(void);
+unsigned long long maple_gen_launch_count(void);
+
+/* y[rows][out] = x[rows][in] W^T + b (nn.Linear; W [out][in]; b nullable);
+ * SiLU after it when act. */
+int maple_gen_linear(const float* x, const float* W, const float* b, float* y, int rows, int in, int out, int act,
+                     maple_stream_t stream);
+
+/* nn.LayerNorm(dim, eps) of each row (gamma, beta nullable); SiLU after it when act. */
+int maple_gen_layernorm(const float* x, const float* gamma, const float* beta, float* y, int rows, int dim, float eps,
+                        int act, maple_stream_t stream);
+
+/* nn.Upsample(scale_factor=2, mode="trilinear", align_corners=False) of an
+ * n^3 grid of C channels read at in[b*cell_stride + v*voxel_stride +
+ * c*channel_stride] (v = x*n*n + y*n + z) into channels-last BF16
+ * out[B][(2n)^3][C]. */
+int maple_gen_upsample2(const float* in, long long cell_stride, long long voxel_stride, long long channel_stride,
+                        void* out, int B, int n, int C, maple_stream_t stream);
+
+/* nn.GroupNorm(groups, C, eps) of channels-last x[B][N][C] (gamma, beta
+ * nullable), SiLU after it when act, into out_bf16 (BF16) and/or out_f32.
+ * stats: B*groups*2 doubles of workspace. */
+int maple_gen_groupnorm(const float* x, const float* gamma, const float* beta, int groups, float eps, int act,
+                        void* out_bf16, float* out_f32, double* stats, int B, long long N, int C,
+                        maple_stream_t stream);
+
+/* out[B][N] = sigmoid(bias + sum_c w[c] x[B][N][c]) (1x1x1 conv to one channel). */
+int maple_gen_head_sigmoid(const float* x, const float* w, float bias, float* out, int B, long long N, int C,
+                           maple_stream_t stream);
+
+/* binomial_smooth_periodic_torch (pareto/densify_pareto_property_network_32.py:
+ * 1040-1052): `passes` times, along x, y, z, the periodic [1 4 6 4 1]/16
+ * filter, bit-identical to the reference's FP32 operation order.  in, out and
+ * work ([B][n^3] each) distinct; passes = 0 copies in to out. */
+int maple_gen_binomial_smooth(const float* in, float* out, float* work, int B, int n, int passes,
+                              maple_stream_t stream);
+
+/* match_mean_clamped_torch (same file, 1031-1037), per cell in place:
+ * max(1, iters) times x <- clamp(x - mean(x) + clamp(target[b], lo, hi), lo, hi)
+ * (target FP64 device array [B]; the mean is summed in FP64). */
+int maple_gen_match_mean(float* x, const double* target, int B, long long N, float lo, float hi, int iters,
+                         maple_stream_t stream);
 
 /* Instrumentation: when enabled, every fine-level operator launch of this
  * context is bracketed by CUDA events (at most max_launches are kept).

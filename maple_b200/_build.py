@@ -16,7 +16,7 @@ ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libmaple_b200.so")
 BUILD_DIR = os.path.join(ROOT, "_build")
 
-SOURCES = ["maple.cu", "tables.cpp", "convnet.cu", "printability.cu"]
+SOURCES = ["maple.cu", "tables.cpp", "convnet.cu", "printability.cu", "generator.cu"]
 HEADERS = ["kernels.cuh", "tables.h", "printability.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",

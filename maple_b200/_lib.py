@@ -22,6 +22,7 @@ _I = C.c_int
 _D = C.c_double
 _F = C.c_float
 _Z = C.c_size_t
+_L = C.c_longlong
 _IP = C.POINTER(C.c_int)
 _DP = C.POINTER(C.c_double)
 
@@ -82,9 +83,21 @@ SIGNATURES = {
     "maple_nn_channels_to_fields": (_I, [_P, _P, _I, _I, _I, _I, _I, _P, _P]),
     "maple_nn_prolong_fields": (_I, [_P, _P, _I, _I, _I, _P]),
     "maple_nn_restrict_density": (_I, [_P, _P, _I, _I, _I, _P]),
+    "maple_nn_conv3d_padded": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _P]),
+    # Stage-II density generator and warm-start post-processing
+    "maple_gen_last_error_string": (C.c_char_p, []),
+    "maple_gen_launch_count": (C.c_ulonglong, []),
+    "maple_gen_linear": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _P]),
+    "maple_gen_layernorm": (_I, [_P, _P, _P, _P, _I, _I, _F, _I, _P]),
+    "maple_gen_upsample2": (_I, [_P, _L, _L, _L, _P, _I, _I, _I, _P]),
+    "maple_gen_groupnorm": (_I, [_P, _P, _P, _I, _F, _I, _P, _P, _P, _I, _L, _I, _P]),
+    "maple_gen_head_sigmoid": (_I, [_P, _P, _F, _P, _I, _L, _I, _P]),
+    "maple_gen_binomial_smooth": (_I, [_P, _P, _P, _I, _I, _I, _P]),
+    "maple_gen_match_mean": (_I, [_P, _P, _I, _L, _F, _F, _I, _P]),
 }
 
 NN_POOL, NN_UPSAMPLE, NN_UPSAMPLE_ADJ, NN_POOL_ADJ = 0, 1, 2, 3
+NN_PAD_CIRCULAR, NN_PAD_ZEROS = 0, 1
 SYM_NONE, SYM_MIRROR, SYM_CUBIC = 0, 1, 2
 SEED_FACES = {"all": 0, "x": 1, "y": 2, "z": 3, "xy": 4}
 
@@ -133,4 +146,13 @@ def nn_call(name: str, *args) -> None:
     status = getattr(lib, name)(*args)
     if status != MAPLE_OK:
         msg = lib.maple_nn_last_error_string()
+        raise MapleError(status, msg.decode() if msg else "")
+
+
+def gen_call(name: str, *args) -> None:
+    """Call a maple_gen_* entry point; raise MapleError with its message."""
+    lib = load()
+    status = getattr(lib, name)(*args)
+    if status != MAPLE_OK:
+        msg = lib.maple_gen_last_error_string()
         raise MapleError(status, msg.decode() if msg else "")

@@ -32,6 +32,10 @@ class BatchResult:
     pcg_iters: np.ndarray       # (B,) PCG iterations summed over the run
     seconds: float
     history: list = field(default_factory=list)
+    J_raw: Optional[np.ndarray] = None     # (B,) unpenalised objective of the last iteration
+    P_print: Optional[np.ndarray] = None   # (B,) overhang penalty of the last iteration
+    P_cavity: Optional[np.ndarray] = None  # (B,) trapped-void penalty of the last iteration
+    logs: list = field(default_factory=list)  # per cell: iteration rows (ITER_LOG_COLUMNS)
 
     @property
     def oc_iterations(self) -> int:
@@ -66,16 +70,33 @@ def seeded_design(seed, r, sigma, vf, scale=0.25, xmin=1e-3):
     return x
 
 
+ITER_LOG_COLUMNS = ["iter", "J_total", "J_raw", "P_print", "P_cavity", "mean_x", "mean_rho", "dx_max", "dx_mean",
+                    "time_sec"]
+# stall test of main_IHD_v3.py:611-618, 711-714
+STALL_TOL_X, STALL_TOL_J, STALL_PATIENCE, STALL_MIN_ITERS = 1e-3, 1e-4, 10, 10
+
+
 def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, xmin: float = 1e-3,
            penal: float = 3.0, rho_min: float = 1e-9, filter_k: int = 3, precision: str = "mixed",
            rtol: float = 1e-8, maxit: int = 500, dx_tol: float = 0.01, max_iters: int = 200,
            ctx: Optional[HomogenizationContext] = None, device=None, record: bool = False,
-           guess=None, symmetry: str = "none") -> BatchResult:
+           guess=None, symmetry: str = "none", penalties: Optional[dict] = None, stop_rule: str = "dx",
+           log_rows: bool = False) -> BatchResult:
     """Run B independent OC loops to their own stopping points (with the
     symmetry projection `symmetry`, a spec as in parse_symmetry).  `guess` =
     (elastic (B, 6, 3, N), thermal (B, 3, 1, N)) float64 fields: the initial
     iterates of the first iteration's solves (later iterations start from the
-    previous iteration's solutions)."""
+    previous iteration's solutions).
+
+    stop_rule "dx": a cell stops when max|dx| < dx_tol; "reference": the
+    optimizer's stall test (main_IHD_v3.py:611-618, 711-714), i.e. after
+    STALL_PATIENCE consecutive iterations, from iteration STALL_MIN_ITERS on,
+    with max|dx| < STALL_TOL_X and |dJ|/|J_prev| < STALL_TOL_J.  `penalties`:
+    keyword arguments of HomogenizationContext.set_penalties, applied to every
+    cell (J is then the penalised objective).  log_rows: keep each cell's
+    iteration rows (ITER_LOG_COLUMNS, the optimizer's iter_log.csv)."""
+    if stop_rule not in ("dx", "reference"):
+        raise ValueError("stop_rule must be 'dx' or 'reference'")
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     x = torch.as_tensor(x0, dtype=torch.float64).to(dev).reshape(len(volfrac), -1).contiguous()
     B, N = x.shape
@@ -91,6 +112,8 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
     if sym_kind != "none":
         from .core import symmetrize
         x = symmetrize(x, r, sym_kind, sym_axes).clamp(xmin, 1.0).contiguous()
+    if penalties:
+        ctx.set_penalties(**penalties)
     if guess is not None:
         ctx.set_solution("elastic", guess[0].contiguous())
         ctx.set_solution("thermal", guess[1].contiguous())
@@ -98,30 +121,64 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
     iters = np.zeros(B, dtype=np.int64)
     pcg = np.zeros(B, dtype=np.int64)
     conv = np.zeros(B, dtype=bool)
-    J = np.zeros(B)
+    J, J_raw, P_print, P_cavity = np.zeros(B), np.zeros(B), np.zeros(B), np.zeros(B)
+    J_prev = np.full(B, np.nan)
+    stall = np.zeros(B, dtype=np.int64)
     terms = np.zeros((B, 3))
     hist = []
+    logs = [[] for _ in range(B)]
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    for _ in range(max_iters):
-        if not active.any():
-            break
-        ctx.set_active(active)
-        out = ctx.oc_step(x, w, vf, penal=penal, rho_min=rho_min, move=move, xmin=xmin, filter_k=filter_k,
-                          precision=precision, rtol=rtol, maxit=maxit, warm=True)
-        st = out["stats"].cpu().numpy()
-        act = active.astype(bool)
-        J[act] = out["J"].cpu().numpy()[act]
-        terms[act] = out["terms"].cpu().numpy()[act]
-        mask = torch.as_tensor(act, device=dev).reshape(B, 1)
-        x = torch.where(mask, out["x_next"], x).contiguous()
-        iters[act] += 1
-        pcg[act] += out["iters"][act]
-        done = act & (st[:, 0] < dx_tol)
-        conv |= done
-        active[done] = 0
-        if record:
-            hist.append(dict(active=int(act.sum()), J=J.copy(), dx_max=st[:, 0].copy(), pcg=np.array(out["iters"])))
-    torch.cuda.synchronize(dev)
+    try:
+        for it in range(max_iters):
+            if not active.any():
+                break
+            ctx.set_active(active)
+            if log_rows:
+                xc = x.clamp(xmin, 1.0)
+                means = torch.stack([xc.mean(1), (rho_min + (1.0 - rho_min) * xc ** penal).clamp(rho_min, 1.0)
+                                     .mean(1)], 1).cpu().numpy()
+            out = ctx.oc_step(x, w, vf, penal=penal, rho_min=rho_min, move=move, xmin=xmin, filter_k=filter_k,
+                              precision=precision, rtol=rtol, maxit=maxit, warm=True)
+            st = out["stats"].cpu().numpy()
+            act = active.astype(bool)
+            Jn = out["J"].cpu().numpy()
+            J[act] = Jn[act]
+            J_raw[act] = out["J_raw"].cpu().numpy()[act]
+            P_print[act] = out["P_print"].cpu().numpy()[act]
+            P_cavity[act] = out["P_cavity"].cpu().numpy()[act]
+            terms[act] = out["terms"].cpu().numpy()[act]
+            mask = torch.as_tensor(act, device=dev).reshape(B, 1)
+            x = torch.where(mask, out["x_next"].clamp(xmin, 1.0), x).contiguous()
+            iters[act] += 1
+            pcg[act] += out["iters"][act]
+            if stop_rule == "dx":
+                done = act & (st[:, 0] < dx_tol)
+            else:
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    dJ = np.where(np.isnan(J_prev), np.inf, np.abs(Jn - J_prev) / np.maximum(np.abs(J_prev), 1e-12))
+                ok = (it >= STALL_MIN_ITERS) & (st[:, 0] < STALL_TOL_X) & (dJ < STALL_TOL_J)
+                stall = np.where(act, np.where(ok, stall + 1, 0), stall)
+                done = act & (stall >= STALL_PATIENCE)
+            J_prev = np.where(act, Jn, J_prev)
+            if log_rows:
+                t_now = time.perf_counter() - t0
+                for b in np.nonzero(act)[0]:
+                    logs[b].append([int(iters[b]), float(J[b]), float(J_raw[b]), float(P_print[b]),
+                                    float(P_cavity[b]), float(means[b, 0]), float(means[b, 1]), float(st[b, 0]),
+                                    float(st[b, 1]), t_now])
+            conv |= done
+            active[done] = 0
+            if record:
+                hist.append(dict(active=int(act.sum()), J=J.copy(), dx_max=st[:, 0].copy(),
+                                 pcg=np.array(out["iters"])))
+        torch.cuda.synchronize(dev)
+    finally:
+        ctx.set_active(np.ones(B, dtype=np.int32))
+        if sym_kind != "none":
+            ctx.set_symmetry("none")
+        if penalties:
+            ctx.set_penalties(0.0, 45.0, 0.0)
     return BatchResult(x=x, J=J, terms=terms, iters_run=iters, converged=conv, pcg_iters=pcg,
-                       seconds=time.perf_counter() - t0, history=hist)
+                       seconds=time.perf_counter() - t0, history=hist, J_raw=J_raw, P_print=P_print,
+                       P_cavity=P_cavity, logs=logs)

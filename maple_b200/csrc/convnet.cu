@@ -43,6 +43,13 @@ __device__ __forceinline__ int neighbour(int v, int n, int dx, int dy, int dz) {
   return (wrapc(x + dx, n) * n + wrapc(y + dy, n)) * n + wrapc(z + dz, n);
 }
 
+// neighbour with zero padding outside the grid: -1 there
+__device__ __forceinline__ int neighbour_zp(int v, int n, int dx, int dy, int dz) {
+  const int z = v % n + dz, y = (v / n) % n + dy, x = v / (n * n) + dx;
+  if (x < 0 || x >= n || y < 0 || y >= n || z < 0 || z >= n) return -1;
+  return (x * n + y) * n + z;
+}
+
 __device__ __forceinline__ void tap_offsets(int tap, int taps, int& dx, int& dy, int& dz) {
   if (taps == 1) {
     dx = dy = dz = 0;
@@ -54,12 +61,13 @@ __device__ __forceinline__ void tap_offsets(int tap, int taps, int& dx, int& dy,
 }
 
 // out[b][v][co] = act( sum_{tap,ci} in[b][nbr(v,tap)][ci] * W[tap][ci][co] + bias[co] + res[b][v][co] )
-// act = ReLU when relu != 0; BF16 and/or FP32 outputs.
+// act = ReLU when relu != 0; BF16 and/or FP32 outputs.  Neighbours wrap
+// (circular padding) unless zero_pad, where taps outside the grid read zero.
 // res may alias out (gradient accumulation): each element is read, then written, by one thread.
 __global__ void __launch_bounds__(NT) k_conv3d(const bf16* __restrict__ in, const bf16* __restrict__ W,
                                                const float* __restrict__ bias, const bf16* res, bf16* out,
                                                float* __restrict__ out_f32, int n, int cin, int cout, int taps,
-                                               int relu) {
+                                               int relu, int zero_pad) {
   __shared__ __align__(32) bf16 sA[BM][BK + APAD];
   __shared__ __align__(32) bf16 sB[BK][BN + BPAD];
   __shared__ __align__(32) float sC[BM][BN + CPAD];
@@ -81,8 +89,10 @@ __global__ void __launch_bounds__(NT) k_conv3d(const bf16* __restrict__ in, cons
           const int m = t / (BK / 8), h = t % (BK / 8);
           const int v = v0 + m;
           uint4 val = make_uint4(0, 0, 0, 0);
-          if (v < N && c0 + 8 * h < cin)
-            val = *reinterpret_cast<const uint4*>(inb + (size_t)neighbour(v, n, dx, dy, dz) * cin + c0 + 8 * h);
+          if (v < N && c0 + 8 * h < cin) {
+            const int q = zero_pad ? neighbour_zp(v, n, dx, dy, dz) : neighbour(v, n, dx, dy, dz);
+            if (q >= 0) val = *reinterpret_cast<const uint4*>(inb + (size_t)q * cin + c0 + 8 * h);
+          }
           *reinterpret_cast<uint4*>(&sA[m][8 * h]) = val;
         }
       } else {
@@ -90,7 +100,10 @@ __global__ void __launch_bounds__(NT) k_conv3d(const bf16* __restrict__ in, cons
           const int m = t / BK, k = t % BK;
           const int v = v0 + m;
           bf16 val = __float2bfloat16(0.0f);
-          if (v < N && c0 + k < cin) val = inb[(size_t)neighbour(v, n, dx, dy, dz) * cin + c0 + k];
+          if (v < N && c0 + k < cin) {
+            const int q = zero_pad ? neighbour_zp(v, n, dx, dy, dz) : neighbour(v, n, dx, dy, dz);
+            if (q >= 0) val = inb[(size_t)q * cin + c0 + k];
+          }
           sA[m][k] = val;
         }
       }
@@ -603,19 +616,27 @@ extern "C" {
 const char* maple_nn_last_error_string(void) { return g_nn_err.c_str(); }
 unsigned long long maple_nn_launch_count(void) { return g_nn_launches; }
 
-int maple_nn_conv3d(const void* in, const void* W, const float* bias, const void* res, void* out, float* out_f32,
-                    int B, int n, int cin, int cout, int ksize, int relu, maple_stream_t s) {
+int maple_nn_conv3d_padded(const void* in, const void* W, const float* bias, const void* res, void* out,
+                           float* out_f32, int B, int n, int cin, int cout, int ksize, int relu, int padding,
+                           maple_stream_t s) {
   return nn_guard([&]() -> const char* {
     if (!in || !W || (!out && !out_f32)) return "NULL argument";
     if (B < 1 || n < 1 || cin < 1 || cout < 1) return "bad sizes";
     if (ksize != 1 && ksize != 3) return "kernel size must be 1 or 3";
+    if (padding != MAPLE_NN_PAD_CIRCULAR && padding != MAPLE_NN_PAD_ZEROS) return "unknown padding mode";
     if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) != 0) return "input must be 16-byte aligned";
     const int N = n * n * n;
     dim3 g((N + BM - 1) / BM, (cout + BN - 1) / BN, B);
     NNL((k_conv3d<<<g, NT, 0, Sx(s)>>>((const bf16*)in, (const bf16*)W, bias, (const bf16*)res, (bf16*)out, out_f32,
-                                       n, cin, cout, ksize == 3 ? 27 : 1, relu)));
+                                       n, cin, cout, ksize == 3 ? 27 : 1, relu,
+                                       padding == MAPLE_NN_PAD_ZEROS ? 1 : 0)));
     return nullptr;
   });
+}
+
+int maple_nn_conv3d(const void* in, const void* W, const float* bias, const void* res, void* out, float* out_f32,
+                    int B, int n, int cin, int cout, int ksize, int relu, maple_stream_t s) {
+  return maple_nn_conv3d_padded(in, W, bias, res, out, out_f32, B, n, cin, cout, ksize, relu, MAPLE_NN_PAD_CIRCULAR, s);
 }
 
 int maple_nn_conv3d_wgrad(const void* in, const void* dz, float* dW, float* db, int B, int n, int cin, int cout,

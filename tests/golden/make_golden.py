@@ -123,6 +123,8 @@ def main(src, only=None):
 
     if only == "symmetry":
         return symmetry_fixtures(M, Ob, homogenize, dev)
+    if only == "generator":
+        return generator_fixtures()
     if only == "print":
         return printability_fixtures(M, Ob, homogenize, dev, src)
 
@@ -335,6 +337,54 @@ def symmetry_fixtures(M, Ob, homogenize, dev):
             x = xn
             print("sym traj", spec, it, J.item())
     np.savez_compressed(os.path.join(HERE, "sym.npz"), **rec)
+
+
+GENERATOR_CONFIGS = {
+    "full": dict(cond_dim=7, out_res=32, base_res=4, latent_dim=256, base_channels=128),
+    "small": dict(cond_dim=7, out_res=16, base_res=4, latent_dim=64, base_channels=32),
+}
+
+
+def generator_fixtures():
+    """Stage2DensityGenerator (core/stage2/density_generator.py:123-197) with
+    seeded weights, and the Pareto worker's warm-start helpers
+    (pareto/densify_pareto_property_network_32.py:1031-1052), run from the
+    reference's own modules.  Densities are stored every 7th voxel plus
+    per-sample FP64 sums and sums of squares of the full field."""
+    from maple.core.stage2.density_generator import Stage2DensityGenerator
+    from maple.pareto import densify_pareto_property_network_32 as D
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.generator_oracle import synthetic_state_dict
+    rec = {}
+    for tag, cfg in GENERATOR_CONFIGS.items():
+        model = Stage2DensityGenerator(**cfg, use_noise_encoder=False)
+        model.load_state_dict(synthetic_state_dict(seed=11, **cfg))  # strict: names and shapes agree
+        model.eval()
+        cond = np.random.default_rng(5).uniform(0.0, 1.0, (3, cfg["cond_dim"])).astype(np.float32)
+        eta = np.array([0.25, 0.75], dtype=np.float32)
+        with torch.no_grad():
+            rho = model(torch.from_numpy(cond), None).numpy().reshape(3, -1)
+            lat = model.encode_latent(torch.from_numpy(cond), None)
+            mix = model.decode_latent(torch.sum(lat[:2] * torch.from_numpy(eta).reshape(-1, 1), dim=0,
+                                                keepdim=True)).numpy().reshape(1, -1)
+        rec[f"{tag}_cond"] = cond
+        rec[f"{tag}_eta"] = eta
+        rec[f"{tag}_latent"] = lat.numpy()
+        for name, a in (("rho", rho), ("mix", mix)):
+            rec[f"{tag}_{name}_sub"] = a[:, ::7].copy()
+            rec[f"{tag}_{name}_sum"] = a.astype(np.float64).sum(1)
+            rec[f"{tag}_{name}_sumsq"] = (a.astype(np.float64) ** 2).sum(1)
+        print("generator", tag, rho.mean(), rho.min(), rho.max())
+    vol = np.random.default_rng(9).uniform(-0.1, 1.1, (12, 12, 12)).astype(np.float32)
+    rec["warm_in"] = vol
+    for passes in (0, 1, 3):
+        rec[f"smooth_{passes}"] = D.binomial_smooth_periodic_torch(torch.from_numpy(vol), passes).numpy()
+    for i, (t, iters) in enumerate(((0.3, 8), (0.05, 1), (0.9, 20), (0.25, 0))):
+        rec[f"match_{i}"] = D.match_mean_clamped_torch(torch.from_numpy(vol), t, 1e-5, iters).numpy()
+        rec[f"match_{i}_args"] = np.array([t, iters], dtype=np.float64)
+    rec["fieldnames"] = np.array(D.FIELDNAMES)
+    rec["condition_columns"] = np.array(D.CONDITION_COLUMNS)
+    np.savez_compressed(os.path.join(HERE, "generator.npz"), **rec)
 
 
 if __name__ == "__main__":
