@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--rtol", type=float, default=1e-10)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--serial", action="store_true",
+                   help="run the elastic and thermal solves one after the other on one host thread")
     return p.parse_args()
 
 
@@ -162,6 +164,7 @@ def run_maple(args, rank, world, local_rank):
     torch.cuda.set_device(dev)
     r = args.res
     ctx = HomogenizationContext(r, ncells=1, device=dev)
+    ctx.set_concurrency(not args.serial)
     w = torch.tensor([[1 / 3, 1 / 3, 1 / 3]], dtype=torch.float64, device=dev)
     vf = torch.tensor([0.25], dtype=torch.float64, device=dev)
     x0 = seeded_design(rank, r, sigma=r / 16.0, vf=0.25)
@@ -334,6 +337,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": f"OC iteration, {args.res}^3 periodic cell (config 1: precision)",
                        "res": args.res, "precision": args.precision, "rtol": args.rtol,
+                       "solves": "one after the other" if args.serial else "elastic and thermal concurrent",
                        "objective": "(E+G+kappa)/3", "volfrac": 0.25, "move": 0.2, "filter_k": 3,
                        "mg_levels": res["levels"], "l2": "flushed between steps (256 MiB write outside the events)",
                        "parallelism": f"replicas x{world}", "pcg_iters_per_step": res["iters"]},

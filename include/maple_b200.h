@@ -74,6 +74,13 @@ int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio,
  * launch eagerly (same results). */
 int maple_set_graphs(maple_ctx* ctx, int enable);
 
+/* Coarse multigrid levels with n >= min_n nodes per axis (and n % 8 == 0)
+ * apply their stencils with the split-offset kernel (three threads per node,
+ * one per x-offset plane); the others with the shared-memory tile kernel.
+ * 0 disables the split kernel.  Default 32 (on B200 the tile kernel is
+ * faster below 32^3 nodes).  Results differ only by FP summation order. */
+int maple_set_stencil_split(maple_ctx* ctx, int min_n);
+
 /* Elastic and thermal solves of maple_oc_step at the same time (default on):
  * the thermal build and solve run on a second stream driven by a second host
  * thread of the library.  Off runs them one after the other on the caller's

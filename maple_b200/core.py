@@ -152,6 +152,11 @@ class HomogenizationContext:
         """Run the elastic and thermal solves of oc_step at the same time (default on)."""
         _lib.check(self._lib.maple_set_concurrency(self._h, int(bool(enable))))
 
+    def set_stencil_split(self, min_n: int = 32):
+        """Coarse levels with at least min_n nodes per axis use the
+        split-offset stencil kernel (0: never)."""
+        _lib.check(self._lib.maple_set_stencil_split(self._h, int(min_n)))
+
     def set_graphs(self, enable: bool):
         """Replay the PCG iteration body as a captured CUDA graph (default on)."""
         _lib.check(self._lib.maple_set_graphs(self._h, int(bool(enable))))

@@ -732,6 +732,145 @@ __global__ void __launch_bounds__(CT_NODES * 6) k_apply_stencil_tile(ApplyArgs<T
   }
 }
 
+// Coarse-level stencil apply with the 27-offset reduction split over three
+// threads per node: thread (node, px) sums the 9 offsets of x-offset plane
+// px - 1 for all R load cases, reading its 9 D x D stencil blocks straight from
+// global memory (coalesced: a warp is one 8 x 4 (z, y) slab of nodes; each
+// stencil entry is read once, by one thread).  The neighbour values come from
+// a halo'd shared-memory tile of the iterate; after the sums, the same shared
+// memory holds the three partial sums, which thread (node, g) adds in plane
+// order for load cases [g R/3, (g+1) R/3) and finishes (MV / RES / CHEB / JAC0
+// as in k_apply_stencil_tile).  Requires n % 8 == 0 and R % 3 == 0.
+constexpr int ST_Z = 8, ST_Y = 4, ST_X = 4;
+constexpr int ST_NODES = ST_Z * ST_Y * ST_X;                       // 128
+constexpr int ST_HALO = (ST_Z + 2) * (ST_Y + 2) * (ST_X + 2);      // 360
+constexpr int ST_THREADS = 3 * ST_NODES;                           // 384
+
+template <typename T, int D, int R>
+struct SplitTile {
+  static constexpr int RD = R * D;
+  static constexpr int NS = RD % 2 ? RD : RD + 1;  // odd node stride: conflict-free halo reads
+  static constexpr size_t HALO_BYTES = (size_t)ST_HALO * NS * sizeof(T);
+  static constexpr size_t RED_BYTES = (size_t)3 * RD * ST_NODES * sizeof(T);
+  static constexpr size_t BYTES = HALO_BYTES > RED_BYTES ? HALO_BYTES : RED_BYTES;
+};
+
+template <typename T, int D, int R, int MODE>
+__global__ void __launch_bounds__(ST_THREADS) k_apply_stencil_split(ApplyArgs<T> a) {
+  using G = SplitTile<T, D, R>;
+  constexpr int RD = R * D, R3 = R / 3;
+  static_assert(R % 3 == 0, "three threads per node share the load cases");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sU = reinterpret_cast<T*>(smem_raw);   // [ST_HALO][NS], then the partial sums [3][RD][ST_NODES]
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
+  const int n = a.n, N = a.N;
+  const size_t NN = (size_t)N;
+  const int ntz = n / ST_Z, nty = n / ST_Y;
+  const int tile = blockIdx.x;
+  const int z0 = (tile % ntz) * ST_Z, y0 = ((tile / ntz) % nty) * ST_Y, x0 = (tile / (ntz * nty)) * ST_X;
+  const int tid = threadIdx.x;
+  const int tn = tid % ST_NODES, px = tid / ST_NODES;
+  const int tz = tn % ST_Z, ty = (tn / ST_Z) % ST_Y, tx = tn / (ST_Z * ST_Y);
+  const int id = ((x0 + tx) * n + (y0 + ty)) * n + (z0 + tz);
+  T acc[R][D];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int i = 0; i < D; ++i) acc[r][i] = T(0);
+  if constexpr (MODE != M_JAC0) {
+    const T* ub = a.u + (size_t)b * RD * N;
+    for (int w = tid; w < ST_HALO * RD; w += ST_THREADS) {
+      const int k = w / ST_HALO, h = w - k * ST_HALO;
+      const int iz = h % (ST_Z + 2), iy = (h / (ST_Z + 2)) % (ST_Y + 2), ix = h / ((ST_Z + 2) * (ST_Y + 2));
+      int gx = x0 - 1 + ix, gy = y0 - 1 + iy, gz = z0 - 1 + iz;
+      gx += gx < 0 ? n : (gx >= n ? -n : 0);
+      gy += gy < 0 ? n : (gy >= n ? -n : 0);
+      gz += gz < 0 ? n : (gz >= n ? -n : 0);
+      cp_async<sizeof(T)>(sU + h * G::NS + k, ub + (size_t)k * N + ((size_t)gx * n + gy) * n + gz);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const T* Sb = a.S + (size_t)b * 27 * D * D * N + id;
+#pragma unroll 1
+    for (int q = 0; q < 9; ++q) {
+      const int oy = q / 3, oz = q % 3, o = px * 9 + q;
+      T sv[D][D];
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) sv[i][j] = Sb[(size_t)((o * D + i) * D + j) * N];
+      const T* un = sU + (((tx + px) * (ST_Y + 2) + (ty + oy)) * (ST_Z + 2) + (tz + oz)) * G::NS;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          const T uv = un[r * D + j];
+#pragma unroll
+          for (int i = 0; i < D; ++i) acc[r][i] += sv[i][j] * uv;
+        }
+    }
+    __syncthreads();  // the halo is consumed: its space takes the partial sums
+    T* red = sU;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < D; ++i) red[(px * RD + r * D + i) * ST_NODES + tn] = acc[r][i];
+    __syncthreads();
+  }
+  // finish load cases [px R3, (px+1) R3) of node tn
+  const int g = px;
+  T tot[R3][D];
+  if constexpr (MODE != M_JAC0) {
+    const T* red = sU;
+#pragma unroll
+    for (int rr = 0; rr < R3; ++rr)
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const int k = (g * R3 + rr) * D + i;
+        tot[rr][i] = (red[k * ST_NODES + tn] + red[(RD + k) * ST_NODES + tn]) + red[(2 * RD + k) * ST_NODES + tn];
+      }
+  }
+  const size_t cellv = (size_t)b * R * D * NN + id;
+  if constexpr (MODE == M_MV || MODE == M_RES) {
+#pragma unroll
+    for (int rr = 0; rr < R3; ++rr)
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const size_t o = cellv + ((size_t)(g * R3 + rr) * D + i) * NN;
+        a.out[o] = MODE == M_MV ? tot[rr][i] : a.f[o] - tot[rr][i];
+      }
+  } else {
+    __shared__ double s_coef[2];
+    if (tid == 0) cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, s_coef[0], s_coef[1]);
+    __syncthreads();
+    const double al = s_coef[0], be = s_coef[1];
+    T Di[D][D];
+    const T* Db = a.Dinv + (size_t)b * D * D * N + id;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) Di[i][j] = Db[(size_t)(i * D + j) * N];
+#pragma unroll
+    for (int rr = 0; rr < R3; ++rr) {
+      const size_t vo = cellv + (size_t)(g * R3 + rr) * D * NN;
+      T res[D];
+#pragma unroll
+      for (int i = 0; i < D; ++i) res[i] = (MODE == M_JAC0) ? a.f[vo + i * NN] : a.f[vo + i * NN] - tot[rr][i];
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        T zz = 0;
+#pragma unroll
+        for (int j = 0; j < D; ++j) zz += Di[i][j] * res[j];
+        T d = T(be) * zz;
+        if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + i * NN];
+        a.dout[vo + i * NN] = d;
+        a.out[vo + i * NN] = (MODE == M_JAC0) ? d : a.u[vo + i * NN] + d;
+      }
+    }
+  }
+}
+
 // power iteration step on a coarse level: w = Dinv A u and the Rayleigh terms.
 // One thread per (node, row i): a CTA covers kPowerNodes<D> nodes, rows
 // i-major so that consecutive threads read consecutive stencil entries; the

@@ -181,6 +181,7 @@ struct maple_ctx {
   cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
   bool use_graphs = true;
   bool concurrent = true;  // elastic and thermal solves of an OC step on two streams
+  int split_min_n = 32;    // coarse levels with n >= this (n % 8 == 0) use k_apply_stencil_split; 0: never
   int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
   // manufacturability penalties of the OC objective (maple_set_penalties)
   double lambda_print = 0, lambda_cavity = 0;
@@ -357,7 +358,22 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
           <<<dim3(ceil_div(a.N, kPowerNodes<D>), c->B), D * kPowerNodes<D>, 0, s>>>(a);
     } else {
       require(a.part == nullptr, "coarse-level applies produce no partial sums");
-      if (a.n % CT == 0) {
+      bool split = false;
+      if constexpr (R % 3 == 0) {
+        if (c->split_min_n > 0 && a.n >= c->split_min_n && a.n % ST_Z == 0) {
+          using G = SplitTile<T, D, R>;
+          static std::once_flag attr_once;  // one per template instantiation
+          std::call_once(attr_once, [] {
+            CK(cudaFuncSetAttribute(k_apply_stencil_split<T, D, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)G::BYTES));
+          });
+          const int tiles = (a.n / ST_Z) * (a.n / ST_Y) * (a.n / ST_X);
+          k_apply_stencil_split<T, D, R, MODE><<<dim3(tiles, c->B), ST_THREADS, G::BYTES, s>>>(a);
+          split = true;
+        }
+      }
+      if (split) {
+      } else if (a.n % CT == 0) {
         using G = CoarseTile<T, D, R>;
         static bool attr_set = false;  // one per template instantiation
         if (!attr_set) {
@@ -1342,6 +1358,15 @@ int maple_set_graphs(maple_ctx* c, int enable) {
     require(c != nullptr, "ctx is NULL");
     drop_graphs(c);
     c->use_graphs = enable != 0;
+  });
+}
+
+int maple_set_stencil_split(maple_ctx* c, int min_n) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(min_n >= 0, "min_n must be >= 0");
+    drop_graphs(c);
+    c->split_min_n = min_n;
   });
 }
 
