@@ -1217,20 +1217,19 @@ __global__ void k_chol_inverse(double* __restrict__ A, double* __restrict__ work
 }
 
 // Same result for ndof <= kCholSmemMax, with the packed lower triangle of the
-// regularised matrix held in shared memory (one block of 1024 threads per
-// cell).  L^-1 goes through `work` in global memory (each thread owns columns).
+// regularised matrix held in shared memory (one block of 1024 threads per cell).
 constexpr int kCholSmemMax = 192;
 constexpr int kCholThreads = 1024;
-// packed lower triangle of L, the current column and one solve vector per warp
+// packed lower triangle of L (then of L^-1) and one column buffer
 __host__ __device__ constexpr size_t chol_smem_bytes(int ndof) {
-  return ((size_t)ndof * (ndof + 1) / 2 + (size_t)(kCholThreads / 32 + 1) * ndof) * sizeof(double);
+  return ((size_t)ndof * (ndof + 1) / 2 + (size_t)ndof) * sizeof(double);
 }
 
 // A <- (A + reg * I_blocks)^-1 for one cell per CTA, A symmetric positive
 // (semi-)definite of order ndof <= kCholSmemMax: Cholesky factor L in shared
-// memory, then column j of the inverse by the forward solve L y = e_j and the
-// backward solve L^T x = y, one warp per column.  A zero or negative pivot
-// sets status[b] (nullable) and continues with a tiny pivot.
+// memory, its inverse X = L^{-1} in place, then A^{-1} = X^T X.  Every phase
+// runs all columns at once (one barrier-separated step per pivot).  A zero or
+// negative pivot sets status[b] (nullable) and continues with a tiny pivot.
 __global__ void __launch_bounds__(kCholThreads) k_chol_inverse_smem(double* __restrict__ A, int ndof, int D,
                                                                     const int* active, int* status) {
   const int b = blockIdx.x;
@@ -1239,7 +1238,6 @@ __global__ void __launch_bounds__(kCholThreads) k_chol_inverse_smem(double* __re
   double* M = A + (size_t)b * ndof * ndof;
   const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
   double* colk = Lp + (size_t)ndof * (ndof + 1) / 2;  // column k of L below the pivot
-  double* yv = colk + ndof + (size_t)warp * ndof;
   __shared__ double s_alpha;
   if (warp == 0) {
     double t = 0;
@@ -1278,31 +1276,62 @@ __global__ void __launch_bounds__(kCholThreads) k_chol_inverse_smem(double* __re
     }
     __syncthreads();
   }
-  for (int j = warp; j < ndof; j += nw) {
-    // forward: y_i = (delta_ij - sum_{p=j}^{i-1} L_ip y_p) / L_ii for i >= j
-    for (int i = j; i < ndof; ++i) {
-      const size_t ri = (size_t)i * (i + 1) / 2;
-      double t = 0;
-      for (int q = j + lane; q < i; q += 32) t += Lp[ri + q] * yv[q];
+  // X = L^{-1} in place of L: forward substitution L X = I for all columns at
+  // once, right-looking over p.  Entry (i, j), j < i, holds the running
+  // b_ij = -sum_{q<p} L_iq x_qj until step p = i turns it into x_ij.  Rows go
+  // to warps, columns to lanes (no index divisions in the inner loops).
+  for (int p = 0; p < ndof; ++p) {
+    const size_t rp = (size_t)p * (p + 1) / 2;
+    const double inv = 1.0 / Lp[rp + p];
+    for (int i = p + 1 + tid; i < ndof; i += nth) colk[i] = Lp[(size_t)i * (i + 1) / 2 + p];
+    __syncthreads();
+    for (int j = tid; j <= p; j += nth) Lp[rp + j] = (j == p) ? inv : Lp[rp + j] * inv;
+    __syncthreads();
+    for (int i = p + 1 + warp; i < ndof; i += nw) {
+      double* row = Lp + (size_t)i * (i + 1) / 2;
+      const double lip = colk[i];
+      for (int j = lane; j < p; j += 32) row[j] -= lip * Lp[rp + j];
+      if (lane == 0) row[p] = -lip * Lp[rp + p];
+    }
+    __syncthreads();
+  }
+  // A^{-1} = X^T X: entry (i, j) is sum_k X_ki X_kj over k >= max(i, j)
+  // (X_kj = 0 for j > k).  A thread owns a 4 x 4 block (I, J), I <= J, of the
+  // upper triangle and writes it and its mirror.
+  const int nb = (ndof + 3) / 4, nblocks = nb * (nb + 1) / 2;
+  for (int t = tid; t < nblocks; t += nth) {
+    int I = 0, rem = t;  // t-th block of the packed upper block triangle, row-major
+    while (rem >= nb - I) {
+      rem -= nb - I;
+      ++I;
+    }
+    const int J = I + rem;
+    const int i0 = 4 * I, j0 = 4 * J;
+    double acc[4][4] = {};
+    size_t rk = (size_t)j0 * (j0 + 1) / 2;
+    for (int k = j0; k < ndof; ++k) {
+      double xi[4], xj[4];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
-      if (lane == 0) yv[i] = ((i == j ? 1.0 : 0.0) - t) / Lp[ri + i];
-      __syncwarp();
+      for (int a = 0; a < 4; ++a) {
+        xi[a] = (i0 + a <= k && i0 + a < ndof) ? Lp[rk + i0 + a] : 0.0;
+        xj[a] = (j0 + a <= k && j0 + a < ndof) ? Lp[rk + j0 + a] : 0.0;
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] += xi[a] * xj[c];
+      rk += k + 1;
     }
-    for (int i = lane; i < j; i += 32) yv[i] = 0.0;
-    __syncwarp();
-    // backward: x_q = y_q / L_qq, then y_i -= L_qi x_q for i < q (row q of L is contiguous)
-    for (int q = ndof - 1; q >= 0; --q) {
-      const size_t rq = (size_t)q * (q + 1) / 2;
-      const double xq = yv[q] / Lp[rq + q];
-      __syncwarp();
-      if (lane == 0) yv[q] = xq;
-      for (int i = lane; i < q; i += 32) yv[i] -= Lp[rq + i] * xq;
-      __syncwarp();
-    }
-    // column j of the symmetric inverse, stored as row j
-    for (int i = lane; i < ndof; i += 32) M[(size_t)j * ndof + i] = yv[i];
-    __syncwarp();
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = i0 + a, j = j0 + c;
+        if (i < ndof && j < ndof) {
+          M[(size_t)i * ndof + j] = acc[a][c];
+          M[(size_t)j * ndof + i] = acc[a][c];
+        }
+      }
   }
 }
 

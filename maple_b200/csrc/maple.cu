@@ -142,6 +142,10 @@ struct Lane {
   int* h_flags = nullptr;  // pinned host [B]
   int* breakdown = nullptr;
   cudaStream_t cap_stream = nullptr;
+  // the coarsest-level inverse of a hierarchy build runs here, beside the
+  // power iterations of the other levels
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_fork = nullptr, side_join = nullptr;
 };
 
 // lane of the calling thread: set by LaneScope around each physics' work
@@ -430,6 +434,7 @@ static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
 template <int D>
 static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
   Phys& p = c->ph[phys];
+  bool side_inverse = false;
   const int B = c->B, k = 8 * D, L = c->L;
   const int* act = c->active;
   // level-1 element matrices from the fine densities
@@ -478,7 +483,17 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
           CK(cudaFuncSetAttribute(k_chol_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)chol_smem_bytes(kCholSmemMax)));
         });
-        KL(c, s, k_chol_inverse_smem<<<B, kCholThreads, sm, s>>>(p.Ainv, ndof, D, act, nullptr));
+        Lane& ln = LN(c);
+        if (!ln.side) {
+          CK(cudaStreamCreateWithFlags(&ln.side, cudaStreamNonBlocking));
+          CK(cudaEventCreateWithFlags(&ln.side_fork, cudaEventDisableTiming));
+          CK(cudaEventCreateWithFlags(&ln.side_join, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(ln.side_fork, s));
+        CK(cudaStreamWaitEvent(ln.side, ln.side_fork, 0));
+        KL(c, ln.side, k_chol_inverse_smem<<<B, kCholThreads, sm, ln.side>>>(p.Ainv, ndof, D, act, nullptr));
+        CK(cudaEventRecord(ln.side_join, ln.side));
+        side_inverse = true;
       } else {
         KL(c, s, k_chol_inverse<<<B, 512, 0, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr));
       }
@@ -488,6 +503,7 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
     power_bounds<double, D>(c, p, p.o64, s);
   else
     power_bounds<float, D>(c, p, p.o32, s);
+  if (side_inverse) CK(cudaStreamWaitEvent(s, LN(c).side_join, 0));
   p.built = true;
   p.built_prec = prec;
   // the current solution (if any) stays: it is the warm start for this density
@@ -1201,6 +1217,9 @@ int maple_ctx_destroy(maple_ctx* c) {
     drop_graphs(c);
     for (Lane& L : c->lanes) {
       if (L.cap_stream) cudaStreamDestroy(L.cap_stream);
+      if (L.side) cudaStreamDestroy(L.side);
+      if (L.side_fork) cudaEventDestroy(L.side_fork);
+      if (L.side_join) cudaEventDestroy(L.side_join);
       if (L.h_flags) cudaFreeHost(L.h_flags);
     }
     if (c->pen_work) cudaFree(c->pen_work);
