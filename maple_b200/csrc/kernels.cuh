@@ -931,6 +931,12 @@ __global__ void k_fill(T* __restrict__ p, size_t n, T v) {
   if (i < n) p[i] = v;
 }
 
+// two consecutive values loaded or stored as one vector access
+template <typename T>
+struct alignas(2 * sizeof(T)) Pair {
+  T lo, hi;
+};
+
 // ----------------------------------------------------------------------------
 // grid transfer: periodic trilinear P (EBE_GMG.py:38-79, 531-647)
 // ----------------------------------------------------------------------------
@@ -953,42 +959,66 @@ __global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ rc, int nc,
 #pragma unroll
   for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-    for (int dy = 0; dy < 3; ++dy)
+    for (int dy = 0; dy < 3; ++dy) {
+      // the z-run 2Z-1, 2Z, 2Z+1 of this (x, y) row: one scalar and one pair load
+      const T* row = base + ((size_t)fx[dx] * nf + fy[dy]) * nf;
+      const Pair<T> p = *reinterpret_cast<const Pair<T>*>(row + fz[1]);
+      const T v[3] = {__ldg(row + fz[0]), p.lo, p.hi};
 #pragma unroll
       for (int dz = 0; dz < 3; ++dz) {
         const T w = T((dx != 1 ? 0.5 : 1.0) * (dy != 1 ? 0.5 : 1.0) * (dz != 1 ? 0.5 : 1.0));
-        acc += w * __ldg(base + ((size_t)fx[dx] * nf + fy[dy]) * nf + fz[dz]);
+        acc += w * v[dz];
       }
+    }
   rc[((size_t)b * K + k) * Nc + idx] = acc;
 }
 
-// uf += P uc, one thread per (fine node, component)
+// uf += P uc, one thread per (coarse node, component): the thread reads the 8
+// coarse values of its coarse cell once and updates the 2 x 2 x 2 fine nodes
+// (2X + rx, 2Y + ry, 2Z + rz), the two z neighbours as one vector access.  A
+// fine coordinate that is even takes weight 1 from its own coarse node and 0
+// from the next one, an odd one 1/2 from each; each fine value is the sum over
+// the 8 corners in (x, y, z) order of weight x value.
 template <typename T, int K>
 __global__ void k_prolong_add(const T* __restrict__ uc, T* __restrict__ uf, int nc, const int* active) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
-  const int nf = 2 * nc, Nf = nf * nf * nf, Nc = nc * nc * nc;
+  const int nf = 2 * nc, Nc = nc * nc * nc;
+  const size_t Nf = (size_t)Nc * 8;
   const int t = blockIdx.x * kThreads + threadIdx.x;
-  if (t >= Nf * K) return;
-  const int k = t / Nf, idx = t - k * Nf;
-  const int z = idx % nf, y = (idx / nf) % nf, x = idx / (nf * nf);
-  const int bx = x >> 1, by = y >> 1, bz = z >> 1, rx = x & 1, ry = y & 1, rz = z & 1;
+  if (t >= Nc * K) return;
+  const int k = t / Nc, idx = t - k * Nc;
+  const int Z = idx % nc, Y = (idx / nc) % nc, X = idx / (nc * nc);
   const T* __restrict__ base = uc + ((size_t)b * K + k) * Nc;
-  const int cx[2] = {bx, bx + 1 == nc ? 0 : bx + 1};
-  const int cy[2] = {by, by + 1 == nc ? 0 : by + 1};
-  const int cz[2] = {bz, bz + 1 == nc ? 0 : bz + 1};
-  // branch-free: an even fine coordinate takes weight 1 from its own coarse
-  // node and 0 from the next one, an odd one 1/2 from each
-  const T wx[2] = {T(rx ? 0.5 : 1.0), T(rx ? 0.5 : 0.0)};
-  const T wy[2] = {T(ry ? 0.5 : 1.0), T(ry ? 0.5 : 0.0)};
-  const T wz[2] = {T(rz ? 0.5 : 1.0), T(rz ? 0.5 : 0.0)};
-  T acc = 0;
+  const int cx[2] = {X, X + 1 == nc ? 0 : X + 1};
+  const int cy[2] = {Y, Y + 1 == nc ? 0 : Y + 1};
+  const int cz[2] = {Z, Z + 1 == nc ? 0 : Z + 1};
+  T cv[8];
 #pragma unroll
-  for (int o = 0; o < 8; ++o) {
-    const int ox = (o >> 2) & 1, oy = (o >> 1) & 1, oz = o & 1;
-    acc += (wx[ox] * wy[oy] * wz[oz]) * __ldg(base + ((size_t)cx[ox] * nc + cy[oy]) * nc + cz[oz]);
-  }
-  uf[((size_t)b * K + k) * Nf + idx] += acc;
+  for (int o = 0; o < 8; ++o)
+    cv[o] = __ldg(base + ((size_t)cx[(o >> 2) & 1] * nc + cy[(o >> 1) & 1]) * nc + cz[o & 1]);
+  T* __restrict__ fb = uf + ((size_t)b * K + k) * Nf;
+#pragma unroll
+  for (int rx = 0; rx < 2; ++rx)
+#pragma unroll
+    for (int ry = 0; ry < 2; ++ry) {
+      const T wx[2] = {T(rx ? 0.5 : 1.0), T(rx ? 0.5 : 0.0)};
+      const T wy[2] = {T(ry ? 0.5 : 1.0), T(ry ? 0.5 : 0.0)};
+      T acc[2];
+#pragma unroll
+      for (int rz = 0; rz < 2; ++rz) {
+        const T wz[2] = {T(rz ? 0.5 : 1.0), T(rz ? 0.5 : 0.0)};
+        T a = 0;
+#pragma unroll
+        for (int o = 0; o < 8; ++o) a += (wx[(o >> 2) & 1] * wy[(o >> 1) & 1] * wz[o & 1]) * cv[o];
+        acc[rz] = a;
+      }
+      Pair<T>* dst = reinterpret_cast<Pair<T>*>(fb + ((size_t)(2 * X + rx) * nf + (2 * Y + ry)) * nf + 2 * Z);
+      Pair<T> v = *dst;
+      v.lo += acc[0];
+      v.hi += acc[1];
+      *dst = v;
+    }
 }
 
 // coarsest level: u = Ainv f with the FP64 (regularised) inverse, per cell;

@@ -558,7 +558,7 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
   const int nc = c->n[l + 1];
   KL(c, s, k_restrict<T, R * D><<<g2((size_t)nodes(nc) * R * D, B), kThreads, 0, s>>>(o.Res[l], o.F[l + 1], nc, act));
   vcycle<T, D, R>(c, p, o, l + 1, o.F[l + 1], act, nullptr, s);
-  KL(c, s, k_prolong_add<T, R * D><<<g2((size_t)nodes(c->n[l]) * R * D, B), kThreads, 0, s>>>(o.U[l + 1][1],
+  KL(c, s, k_prolong_add<T, R * D><<<g2((size_t)nodes(nc) * R * D, B), kThreads, 0, s>>>(o.U[l + 1][1],
                                                                                              o.U[l][cur], nc, act));
   for (int st = 0; st < deg; ++st) {
     ApplyArgs<T> a{};
