@@ -320,6 +320,67 @@ __device__ __forceinline__ void lds_node(const T* __restrict__ p, T (&v)[RD]) {
   }
 }
 
+// Packed FP32 pairs (two lanes of one 64-bit register) for fma.rn.f32x2: each
+// lane is rounded exactly like a scalar fma.rn.f32.
+__device__ __forceinline__ unsigned long long pk2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(unsigned long long v, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// The FP32 elastic operator (D = 3, R = 6) stages a node's values
+// component-major ([j][r]) so that load cases 2m, 2m+1 of one component are
+// adjacent: one 64-bit shared load gives a packed pair, and one fma.rn.f32x2
+// applies a coupling entry to both.  Every accumulator sums its terms in the
+// same (offset, j) order as the scalar form, so the results are identical.
+template <typename T, int D, int R>
+__host__ __device__ constexpr bool fine_packed() {
+  return sizeof(T) == 4 && D == 3 && R == 6;
+}
+
+template <int RW, int NS, int O>
+__device__ __forceinline__ void fine_tile_accumulate_pk(const float (&rq)[8], const float* __restrict__ base,
+                                                        unsigned long long (&acc2)[3][3], float (&C0)[3][3]) {
+  float C[3][3];
+  fine_block<float, 3, O>(rq, C);
+  constexpr int ox = O / 9, oy = (O / 3) % 3, oz = O % 3;
+  const float* un = base + (ox * (TY + 2) + oy) * RW + oz * NS;
+  unsigned long long u2[3][3];  // [j][m]: load cases 2m, 2m+1 of component j
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) u2[j][m] = reinterpret_cast<const unsigned long long*>(un + j * 6)[m];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const unsigned long long cc = pk2(C[i][j], C[i][j]);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) acc2[m][i] = ffma2(cc, u2[j][m], acc2[m][i]);
+    }
+  if constexpr (O == 13) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) C0[i][j] = C[i][j];
+  }
+}
+
+template <int RW, int NS, int... Os>
+__device__ __forceinline__ void fine_tile_all_pk(std::integer_sequence<int, Os...>, const float (&rq)[8],
+                                                 const float* __restrict__ base, unsigned long long (&acc2)[3][3],
+                                                 float (&C0)[3][3]) {
+  (fine_tile_accumulate_pk<RW, NS, Os>(rq, base, acc2, C0), ...);
+}
+
 template <typename T, int D, int R, int RW, int NS, int O>
 __device__ __forceinline__ void fine_tile_accumulate(const T (&rq)[8], const T* __restrict__ base, T (&acc)[R][D],
                                                      T (&C0)[D][D]) {
@@ -351,10 +412,13 @@ __device__ __forceinline__ void fine_tile_all(std::integer_sequence<int, Os...>,
 
 // Shared epilogue of both apply kernels.
 // vo = cell*R*D*N + node; component (r, i) lives at vo + (r*D + i) * N.
-template <typename T, int D, int R, int MODE, int NWARP = kThreads / 32>
+// uown (nullable) holds the node's own values at uown[(r*D + i) * uown_stride],
+// or at uown[(i*R + r) * uown_stride] when CM (component-major staging).
+template <typename T, int D, int R, int MODE, int NWARP = kThreads / 32, bool CM = false>
 __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, size_t vo, bool valid, T (&acc)[R][D],
                                                const T (&Di)[D][D], const T* uown = nullptr, size_t uown_stride = 0) {
   const size_t NN = (size_t)a.N;
+  auto own = [&](int r, int i) { return uown[(CM ? i * R + r : r * D + i) * uown_stride]; };
   constexpr int K = R;
   double dots[K];
 #pragma unroll
@@ -368,7 +432,7 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
           const T y = a.scale * acc[r][i];
           a.out[vo + (size_t)(r * D + i) * NN] = y;
           if (a.part)
-            dots[r] += (double)y * (double)(uown ? uown[(r * D + i) * uown_stride] : a.u[vo + (size_t)(r * D + i) * NN]);
+            dots[r] += (double)y * (double)(uown ? own(r, i) : a.u[vo + (size_t)(r * D + i) * NN]);
         }
     } else if constexpr (MODE == M_RES) {
 #pragma unroll
@@ -399,7 +463,7 @@ __device__ __forceinline__ void apply_epilogue(const ApplyArgs<T>& a, int b, siz
           T d = T(be) * z;
           if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + (size_t)(r * D + i) * NN];
           a.dout[vo + (size_t)(r * D + i) * NN] = d;
-          const T uo = uown ? uown[(r * D + i) * uown_stride] : a.u[vo + (size_t)(r * D + i) * NN];
+          const T uo = uown ? own(r, i) : a.u[vo + (size_t)(r * D + i) * NN];
           const T un = (MODE == M_JAC0) ? d : uo + d;
           a.out[vo + (size_t)(r * D + i) * NN] = un;
           if (a.dot_f_out) dots[r] += (double)a.f[vo + (size_t)(r * D + i) * NN] * (double)un;
@@ -435,6 +499,7 @@ template <typename T, int D, int R, int MODE>
 __global__ void __launch_bounds__(kFineThreads, fine_min_blocks<T, R * D>()) k_apply_fine(ApplyArgs<T> a) {
   using G = FineTile<T, R * D>;
   constexpr int RD = R * D;
+  constexpr bool PK = fine_packed<T, D, R>() && MODE != M_POWER;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);
   T* srho = su + G::RHO_OFF;
@@ -480,7 +545,11 @@ __global__ void __launch_bounds__(kFineThreads, fine_min_blocks<T, R * D>()) k_a
         const T* src = ub + ((size_t)gx * n + gy) * n + gz;
         T* dst = su + row * G::RW + iz * G::NS;
 #pragma unroll 6
-        for (int k = 0; k < RD; ++k) cp_async<sizeof(T)>(dst + k, src + (size_t)k * NN);
+        for (int k = 0; k < RD; ++k) {
+          // global component k = r*D + j; shared slot j*R + r when packed
+          const int sk = PK ? (k % D) * R + k / D : k;
+          cp_async<sizeof(T)>(dst + sk, src + (size_t)k * NN);
+        }
       }
     }
   }
@@ -500,6 +569,18 @@ __global__ void __launch_bounds__(kFineThreads, fine_min_blocks<T, R * D>()) k_a
   T C0[D][D];
   if constexpr (MODE == M_JAC0) {
     fine_block<T, D, 13>(rq, C0);
+  } else if constexpr (PK) {
+    const T* base = su + (tx * (TY + 2) + ty) * G::RW + tz * G::NS;
+    unsigned long long acc2[3][3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) acc2[m][i] = 0ull;
+    fine_tile_all_pk<G::RW, G::NS>(std::make_integer_sequence<int, 27>{}, rq, base, acc2, C0);
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) upk2(acc2[m][i], acc[2 * m][i], acc[2 * m + 1][i]);
   } else {
     const T* base = su + (tx * (TY + 2) + ty) * G::RW + tz * G::NS;
     fine_tile_all<T, D, R, G::RW, G::NS>(std::make_integer_sequence<int, 27>{}, rq, base, acc, C0);
@@ -537,7 +618,7 @@ __global__ void __launch_bounds__(kFineThreads, fine_min_blocks<T, R * D>()) k_a
     }
     // the node's own values are the centre of the staged tile (stride 1)
     const T* uown = (MODE == M_JAC0) ? nullptr : su + ((tx + 1) * (TY + 2) + (ty + 1)) * G::RW + (tz + 1) * G::NS;
-    apply_epilogue<T, D, R, MODE, kFineThreads / 32>(a, b, vo, valid, acc, Di, uown, 1);
+    apply_epilogue<T, D, R, MODE, kFineThreads / 32, PK>(a, b, vo, valid, acc, Di, uown, 1);
   }
 }
 
