@@ -333,7 +333,8 @@ def main():
         line = {
             "metric": METRIC, "value": round(res["value"], 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000 * res["t_dev"] / args.steps, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32" if args.precision == "mixed" else "f64",
             "data": "synthetic",
             "config": {"workload": f"OC iteration, {args.res}^3 periodic cell (config 1: precision)",
                        "res": args.res, "precision": args.precision, "rtol": args.rtol,
