@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <atomic>
 #include <map>
+#include <set>
 #include <exception>
 #include <mutex>
 #include <thread>
@@ -256,6 +257,21 @@ static T* dnew(maple_ctx* c, size_t count) {
   return reinterpret_cast<T*>(dalloc(c, count * sizeof(T)));
 }
 
+// Opt a kernel into `bytes` of dynamic shared memory on device `dev`, once per
+// (kernel, device): the attribute is per device, and several host threads
+// (the two physics lanes, or contexts of different threads) may launch the
+// same kernel for the first time together.
+static std::mutex g_attr_mu;
+static std::set<std::pair<const void*, int>> g_attr_done;
+template <typename K>
+static void smem_attr(K* kernel, size_t bytes, int dev) {
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  const std::pair<const void*, int> key{reinterpret_cast<const void*>(kernel), dev};
+  if (g_attr_done.count(key)) return;
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  g_attr_done.insert(key);
+}
+
 static inline unsigned nblk(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 static inline dim3 g2(size_t n, int B) { return dim3(nblk(n), (unsigned)B); }
 
@@ -333,12 +349,7 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
   if (l == 0) {
     a.rho = o.rho;
     using G = FineTile<T, R * D>;
-    static bool attr_set = false;  // one per template instantiation
-    if (!attr_set) {
-      CK(cudaFuncSetAttribute(k_apply_fine<T, D, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)G::BYTES));
-      attr_set = true;
-    }
+    smem_attr(k_apply_fine<T, D, R, MODE>, G::BYTES, c->dev);
     prof_begin(c, s);
     k_apply_fine<T, D, R, MODE><<<dim3(fine_tiles(a.n), c->B), kFineThreads, G::BYTES, s>>>(a);
     CKL();
@@ -366,11 +377,7 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
       if constexpr (R % 3 == 0) {
         if (c->split_min_n > 0 && a.n >= c->split_min_n && a.n % ST_Z == 0) {
           using G = SplitTile<T, D, R>;
-          static std::once_flag attr_once;  // one per template instantiation
-          std::call_once(attr_once, [] {
-            CK(cudaFuncSetAttribute(k_apply_stencil_split<T, D, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)G::BYTES));
-          });
+          smem_attr(k_apply_stencil_split<T, D, R, MODE>, G::BYTES, c->dev);
           const int tiles = (a.n / ST_Z) * (a.n / ST_Y) * (a.n / ST_X);
           k_apply_stencil_split<T, D, R, MODE><<<dim3(tiles, c->B), ST_THREADS, G::BYTES, s>>>(a);
           split = true;
@@ -379,12 +386,7 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
       if (split) {
       } else if (a.n % CT == 0) {
         using G = CoarseTile<T, D, R>;
-        static bool attr_set = false;  // one per template instantiation
-        if (!attr_set) {
-          CK(cudaFuncSetAttribute(k_apply_stencil_tile<T, D, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)G::BYTES));
-          attr_set = true;
-        }
+        smem_attr(k_apply_stencil_tile<T, D, R, MODE>, G::BYTES, c->dev);
         const int nt = a.n / CT;
         k_apply_stencil_tile<T, D, R, MODE><<<dim3(nt * nt * nt, c->B), G::THREADS, G::BYTES, s>>>(a);
       } else {
@@ -441,18 +443,22 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
   {
     const int nc = c->n[1];
     const size_t tot = (size_t)nodes(nc) * k * k;
+    // the level-1 coarsening table, uploaded once per device and kept for the
+    // process; looked up under the lock (contexts may build on several threads)
     const double* M = nullptr;
     static double* dM[128][2] = {};
-    int dev = c->dev;
-    if (!dM[dev][D == 3 ? 0 : 1]) {
+    {
       std::lock_guard<std::mutex> lk(g_mu);
-      double* m = nullptr;
-      const size_t bytes = (size_t)8 * k * k * sizeof(double);
-      CK(cudaMalloc(&m, bytes));
-      CK(cudaMemcpy(m, D == 3 ? g_tab.M3 : g_tab.M1, bytes, cudaMemcpyHostToDevice));
-      dM[dev][D == 3 ? 0 : 1] = m;
+      double*& slot = dM[c->dev][D == 3 ? 0 : 1];
+      if (!slot) {
+        double* m = nullptr;
+        const size_t bytes = (size_t)8 * k * k * sizeof(double);
+        CK(cudaMalloc(&m, bytes));
+        CK(cudaMemcpy(m, D == 3 ? g_tab.M3 : g_tab.M1, bytes, cudaMemcpyHostToDevice));
+        slot = m;
+      }
+      M = slot;
     }
-    M = dM[dev][D == 3 ? 0 : 1];
     KL(c, s, k_level1_elements<D><<<g2(tot, B), kThreads, 0, s>>>(p.o64.rho, M, p.KE[1], nc, p.kscale, act));
   }
   for (int l = 1; l < L; ++l) {
@@ -478,11 +484,7 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
       KL(c, s, k_dense_from_stencil<D><<<g2((size_t)N * 27, B), kThreads, 0, s>>>(p.S64c, p.Ainv, n, act));
       if (ndof <= kCholSmemMax) {
         const size_t sm = chol_smem_bytes(ndof);
-        static std::once_flag chol_attr;  // the largest size, once: both physics' builds may run concurrently
-        std::call_once(chol_attr, [] {
-          CK(cudaFuncSetAttribute(k_chol_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)chol_smem_bytes(kCholSmemMax)));
-        });
+        smem_attr(k_chol_inverse_smem, chol_smem_bytes(kCholSmemMax), c->dev);
         Lane& ln = LN(c);
         if (!ln.side) {
           CK(cudaStreamCreateWithFlags(&ln.side, cudaStreamNonBlocking));
