@@ -219,6 +219,7 @@ struct CavGeo {
 struct CavWork {
   double *void_uc, *vsc, *er, *vconn, *reach0, *reach1, *t1, *t2, *dil, *gr0, *gr1, *g1, *g2, *gvconn, *gvoid, *part;
   signed char *er_off, *di_off, *off;  // per-pass argmax offsets: [3][B][M] (opening) and [steps][3][B][M]
+  unsigned char* tape;                 // flood-fill radius 1: one packed byte per voxel and step [steps][B][M]
 };
 
 constexpr signed char kPadOff = 127;  // the pass picked a padding cell
@@ -246,8 +247,12 @@ static size_t cav_parts(const CavityPlan& p, void* work, CavWork* o) {
   c.reach1 = reinterpret_cast<double*>(take(B * M * 8));
   c.t1 = reinterpret_cast<double*>(take(B * M * 8));
   c.t2 = reinterpret_cast<double*>(take(B * M * 8));
-  c.dil = reinterpret_cast<double*>(take(B * M * S * 8));
-  c.off = reinterpret_cast<signed char*>(take(3 * B * M * S));
+  if (p.rad == 1) {
+    c.tape = reinterpret_cast<unsigned char*>(take(B * M * S));
+  } else {
+    c.dil = reinterpret_cast<double*>(take(B * M * S * 8));
+    c.off = reinterpret_cast<signed char*>(take(3 * B * M * S));
+  }
   c.gr0 = reinterpret_cast<double*>(take(B * M * 8));
   c.gr1 = reinterpret_cast<double*>(take(B * M * 8));
   c.g1 = reinterpret_cast<double*>(take(B * M * 8));
@@ -330,6 +335,177 @@ __global__ void k_cav_pass_adj(const double* __restrict__ gout, const signed cha
     acc += vmin ? min_grad(outv[base + q], vmin[base + q], g) : g;
   }
   gin[base + v] = accumulate ? gin[base + v] + acc : acc;
+}
+
+// ---------------------------------------------------------------------------
+// Flood-fill steps of radius 1, fused: one CTA per 8^3 tile runs the z, y and
+// x passes of the step's 3^3 max pool in shared memory (the z pass over the
+// tile and its x/y halo, the y pass over the tile and its x halo, the x pass
+// over the tile), with the same candidate order and padding rules as
+// k_cav_pass, so the dilation, its argmax offsets and reach = min(void_conn,
+// dil) are those of the three separate passes.  The step's tape is one byte per
+// voxel: bits 0-1, 2-3, 4-5 the z, y, x argmax codes (offset + 1; 3 = padding)
+// and bits 6-7 the comparison of void_conn with dil (0: <, 1: ==, 2: >), which
+// is all the backward step needs.  The backward kernel gathers through the x,
+// then y, then z adjoints over the same tile and halo, summing in the order of
+// k_cav_pass_adj.
+// ---------------------------------------------------------------------------
+constexpr int FT = 8, FH = FT + 2, FTHREADS = FT * FT * FT;
+
+struct FillTile {
+  int x0, y0, z0;
+  __device__ FillTile(const CavGeo& G) {
+    const int ntz = (G.Z + FT - 1) / FT, nty = (G.Y + FT - 1) / FT;
+    const int t = blockIdx.x;
+    z0 = (t % ntz) * FT;
+    y0 = ((t / ntz) % nty) * FT;
+    x0 = (t / (ntz * nty)) * FT;
+  }
+};
+
+__device__ __forceinline__ bool in_grid(const CavGeo& G, int x, int y, int z) {
+  return G.periodic || (x >= 0 && x < G.X && y >= 0 && y < G.Y && z >= 0 && z < G.Z);
+}
+
+__device__ __forceinline__ unsigned enc_off(int d) { return d == kPadOff ? 3u : (unsigned)(d + 1); }
+
+__global__ void __launch_bounds__(FTHREADS) k_cav_fill_fwd(const double* __restrict__ reach,
+                                                          const double* __restrict__ vconn,
+                                                          double* __restrict__ reach_out,
+                                                          unsigned char* __restrict__ tape, CavGeo G) {
+  __shared__ double s_in[FH][FH][FH];
+  __shared__ double t1[FH][FH][FT];
+  __shared__ double t2[FH][FT][FT];
+  __shared__ unsigned char cz[FT][FT][FT], cy[FT][FT][FT];
+  const FillTile T(G);
+  const size_t base = (size_t)blockIdx.y * G.M;
+  const int tid = threadIdx.x;
+  for (int w = tid; w < FH * FH * FH; w += FTHREADS) {
+    const int iz = w % FH, iy = (w / FH) % FH, ix = w / (FH * FH);
+    size_t q;
+    s_in[ix][iy][iz] = G.shift(T.x0 - 1 + ix, T.y0 - 1 + iy, T.z0 - 1 + iz, 0, 0, 0, q) ? reach[base + q] : 0.0;
+  }
+  __syncthreads();
+  for (int w = tid; w < FH * FH * FT; w += FTHREADS) {  // z pass
+    const int iz = w % FT, iy = (w / FT) % FH, ix = w / (FT * FH);
+    const int gx = T.x0 - 1 + ix, gy = T.y0 - 1 + iy, gz = T.z0 + iz;
+    double best = -INFINITY;
+    int bd = kPadOff;
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+      const bool inside = in_grid(G, gx, gy, gz + d);
+      const double v = inside ? s_in[ix][iy][iz + 1 + d] : 0.0;
+      if (v > best) {
+        best = v;
+        bd = inside ? d : kPadOff;
+      }
+    }
+    t1[ix][iy][iz] = best;
+    if (ix >= 1 && ix <= FT && iy >= 1 && iy <= FT) cz[ix - 1][iy - 1][iz] = (unsigned char)enc_off(bd);
+  }
+  __syncthreads();
+  for (int w = tid; w < FH * FT * FT; w += FTHREADS) {  // y pass
+    const int iz = w % FT, iy = (w / FT) % FT, ix = w / (FT * FT);
+    const int gx = T.x0 - 1 + ix, gy = T.y0 + iy, gz = T.z0 + iz;
+    double best = -INFINITY;
+    int bd = kPadOff;
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+      const bool inside = in_grid(G, gx, gy + d, gz);
+      const double v = inside ? t1[ix][iy + 1 + d][iz] : 0.0;
+      if (v > best) {
+        best = v;
+        bd = inside ? d : kPadOff;
+      }
+    }
+    t2[ix][iy][iz] = best;
+    if (ix >= 1 && ix <= FT) cy[ix - 1][iy][iz] = (unsigned char)enc_off(bd);
+  }
+  __syncthreads();
+  const int tz = tid % FT, ty = (tid / FT) % FT, tx = tid / (FT * FT);  // x pass, one thread per voxel
+  const int gx = T.x0 + tx, gy = T.y0 + ty, gz = T.z0 + tz;
+  if (gx >= G.X || gy >= G.Y || gz >= G.Z) return;
+  double best = -INFINITY;
+  int bd = kPadOff;
+#pragma unroll
+  for (int d = -1; d <= 1; ++d) {
+    const bool inside = in_grid(G, gx + d, gy, gz);
+    const double v = inside ? t2[tx + 1 + d][ty][tz] : 0.0;
+    if (v > best) {
+      best = v;
+      bd = inside ? d : kPadOff;
+    }
+  }
+  const size_t i = base + G.index(gx, gy, gz);
+  const double vc = vconn[i];
+  reach_out[i] = fmin(vc, best);
+  const unsigned cmp = vc < best ? 0u : (vc == best ? 1u : 2u);
+  tape[i] = (unsigned char)(cz[tx][ty][tz] | (cy[tx][ty][tz] << 2) | (enc_off(bd) << 4) | (cmp << 6));
+}
+
+// adjoint of k_cav_fill_fwd: gin = gradient at reach (overwritten), gvconn +=
+// the void_conn branch of the min, from gout = gradient at reach_out
+__global__ void __launch_bounds__(FTHREADS) k_cav_fill_bwd(const double* __restrict__ gout,
+                                                          const unsigned char* __restrict__ tape,
+                                                          double* __restrict__ gin, double* __restrict__ gvconn,
+                                                          CavGeo G) {
+  __shared__ double sg[FH][FH][FH];    // the dil branch of the min's gradient
+  __shared__ unsigned char st[FH][FH][FH];
+  __shared__ double ax[FT][FH][FH];    // after the x adjoint
+  __shared__ double ay[FT][FT][FH];    // after the y adjoint
+  const FillTile T(G);
+  const size_t base = (size_t)blockIdx.y * G.M;
+  const int tid = threadIdx.x;
+  for (int w = tid; w < FH * FH * FH; w += FTHREADS) {
+    const int iz = w % FH, iy = (w / FH) % FH, ix = w / (FH * FH);
+    size_t q;
+    unsigned char code = 0xFF;  // outside the grid: every code reads as padding
+    double g = 0.0;
+    if (G.shift(T.x0 - 1 + ix, T.y0 - 1 + iy, T.z0 - 1 + iz, 0, 0, 0, q)) {
+      code = tape[base + q];
+      const unsigned cmp = code >> 6;
+      const double go = gout[base + q];
+      g = cmp == 2 ? go : (cmp == 1 ? 0.5 * go : 0.0);
+    }
+    sg[ix][iy][iz] = g;
+    st[ix][iy][iz] = code;
+  }
+  __syncthreads();
+  for (int w = tid; w < FT * FH * FH; w += FTHREADS) {  // x adjoint
+    const int iz = w % FH, iy = (w / FH) % FH, jx = w / (FH * FH), ix = jx + 1;
+    double acc = 0.0;
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+      const unsigned code = (st[ix - d][iy][iz] >> 4) & 3u;
+      if (code == (unsigned)(d + 1)) acc += sg[ix - d][iy][iz];
+    }
+    ax[jx][iy][iz] = acc;
+  }
+  __syncthreads();
+  for (int w = tid; w < FT * FT * FH; w += FTHREADS) {  // y adjoint
+    const int iz = w % FH, jy = (w / FH) % FT, jx = w / (FH * FT), iy = jy + 1;
+    double acc = 0.0;
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+      const unsigned code = (st[jx + 1][iy - d][iz] >> 2) & 3u;
+      if (code == (unsigned)(d + 1)) acc += ax[jx][iy - d][iz];
+    }
+    ay[jx][jy][iz] = acc;
+  }
+  __syncthreads();
+  const int tz = tid % FT, ty = (tid / FT) % FT, tx = tid / (FT * FT);  // z adjoint, one thread per voxel
+  const int gx = T.x0 + tx, gy = T.y0 + ty, gz = T.z0 + tz;
+  if (gx >= G.X || gy >= G.Y || gz >= G.Z) return;
+  double acc = 0.0;
+#pragma unroll
+  for (int d = -1; d <= 1; ++d) {
+    const unsigned code = st[tx + 1][ty + 1][tz + 1 - d] & 3u;
+    if (code == (unsigned)(d + 1)) acc += ay[tx][ty][tz + 1 - d];
+  }
+  const size_t i = base + G.index(gx, gy, gz);
+  gin[i] = acc;
+  const unsigned cmp = st[tx + 1][ty + 1][tz + 1] >> 6;
+  if (cmp < 2) gvconn[i] += cmp == 0 ? gout[i] : 0.5 * gout[i];
 }
 
 __device__ __forceinline__ bool is_seed(const CavGeo& G, int seed, int x, int y, int z) {
@@ -483,8 +659,12 @@ void cavity(const double* rho, const CavityPlan& p, double* P, double* grad, voi
   double* reach = w.reach0;
   double* other = w.reach1;
   const int steps = p.rad > 0 ? p.nsteps : 0;
+  const dim3 gF((unsigned)(((G.X + FT - 1) / FT) * ((G.Y + FT - 1) / FT) * ((G.Z + FT - 1) / FT)), p.B);
   for (int t = 0; t < steps; ++t) {
-    pool3(reach, w.dil + (size_t)t * BM, w.off + (size_t)t * 3 * BM, p.rad, 1.0, 0.0, vconn, other);
+    if (p.rad == 1)
+      PR_LAUNCH(k_cav_fill_fwd<<<gF, FTHREADS, 0, s>>>(reach, vconn, other, w.tape + (size_t)t * BM, G));
+    else
+      pool3(reach, w.dil + (size_t)t * BM, w.off + (size_t)t * 3 * BM, p.rad, 1.0, 0.0, vconn, other);
     std::swap(reach, other);
   }
   PR_LAUNCH(k_cav_trapped<<<gM, kT, 0, s>>>(w.vsc, reach, w.part, G, focus));
@@ -494,9 +674,13 @@ void cavity(const double* rho, const CavityPlan& p, double* P, double* grad, voi
   double* gr_other = w.gr1;
   PR_LAUNCH(k_cav_bwd_init<<<gM, kT, 0, s>>>(w.vsc, reach, w.gvoid, gr, w.gvconn, G, focus, 1.0 / count));
   for (int t = steps - 1; t >= 0; --t) {
-    const double* dil = w.dil + (size_t)t * BM;
-    PR_LAUNCH(k_cav_min_vconn<<<gM, kT, 0, s>>>(gr, vconn, dil, w.gvconn, G.M));
-    pool3_adj(gr, w.off + (size_t)t * 3 * BM, gr_other, p.rad, 0, vconn, dil);
+    if (p.rad == 1) {
+      PR_LAUNCH(k_cav_fill_bwd<<<gF, FTHREADS, 0, s>>>(gr, w.tape + (size_t)t * BM, gr_other, w.gvconn, G));
+    } else {
+      const double* dil = w.dil + (size_t)t * BM;
+      PR_LAUNCH(k_cav_min_vconn<<<gM, kT, 0, s>>>(gr, vconn, dil, w.gvconn, G.M));
+      pool3_adj(gr, w.off + (size_t)t * 3 * BM, gr_other, p.rad, 0, vconn, dil);
+    }
     std::swap(gr, gr_other);
   }
   PR_LAUNCH(k_cav_bwd_seed<<<gM, kT, 0, s>>>(gr, w.gvconn, G, p.seed));

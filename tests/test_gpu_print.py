@@ -127,3 +127,31 @@ def test_optimize_with_penalties_follows_reference(golden, tmp_path, lib):
     assert abs(summary["J_total_init"] - (summary["J_raw_init"] - 0.9 * summary["P_print_init"]
                                           - 0.9 * summary["P_cavity_init"])) < 1e-12
     assert res.iters_run == 3
+
+
+@pytest.mark.parametrize("r,tiles,periodic", [(6, (1, 1, 1), True), (6, (1, 1, 1), False), (10, (2, 1, 1), False),
+                                              (6, (3, 3, 3), False), (10, (1, 1, 1), True)])
+def test_cavity_odd_grids_match_oracle(lib, r, tiles, periodic):
+    """Cavity penalty and gradient on (super)cells that are not multiples of
+    the 8^3 tile of the fused radius-1 flood fill, periodic or not, on a field
+    of exact ties and a continuous one, against the oracle: radius 1 with and
+    without the opening (fused kernels) and radius 2 (separable passes)."""
+    from maple_b200.core import HomogenizationContext
+    from oracle import ihd_oracle as O
+    rng = np.random.default_rng(r + sum(tiles))
+    fields = np.stack([rng.choice([0.0, 0.3, 0.5, 1.0], size=r ** 3), rng.random(r ** 3)])
+    rho = torch.tensor(fields, dtype=torch.float64, device=DEV)
+    ctx = HomogenizationContext(r, ncells=2, device=DEV)
+    for rad, mcr, iters in ((1, 0, 0), (1, 1, 5), (2, 0, 3)):
+        if periodic and tiles == (1, 1, 1) and (2 * rad + 1 > r or 2 * mcr + 1 > r):
+            continue
+        ctx.set_penalties(0.0, 45.0, 1.0, min_channel_rad=mcr, rad=rad, iters=iters, tiles=tiles, focus_center=True,
+                          periodic=periodic)
+        out = ctx.penalties(rho, overhang=False, cavity=True)
+        P, dP = out["P_cavity"].cpu().numpy(), out["dP_cavity"].cpu().numpy()
+        for b in range(2):
+            P0, g0 = O.cavity_penalty(fields[b], r, min_channel_rad=mcr, rad=rad, iters=iters, tiles=tiles,
+                                      periodic=periodic)
+            assert abs(P[b] - P0) <= 1e-13 * max(1.0, abs(P0)), (rad, mcr, b, P[b], P0)
+            np.testing.assert_allclose(dP[b], np.asarray(g0).reshape(-1), rtol=0, atol=1e-12)
+    ctx.close()
