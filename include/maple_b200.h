@@ -41,8 +41,12 @@ enum {
 enum { MAPLE_ELASTIC = 0, MAPLE_THERMAL = 1 };
 enum { MAPLE_FP64 = 0, MAPLE_MIXED = 1 };
 
-/* Per-cell solver status bits (maple_solve status_out). */
-enum { MAPLE_CELL_CONVERGED = 1, MAPLE_CELL_BREAKDOWN = 2, MAPLE_CELL_MAXIT = 4 };
+/* Per-cell solver status (maple_solve / maple_solve_rhs status_out): CONVERGED,
+ * BREAKDOWN (a load case's PCG hit p.Ap <= 0 or a non-finite value and was
+ * frozen at its last iterate) or MAXIT, plus the FALLBACK bit when a
+ * mixed-precision breakdown was solved again in plain FP64 (the status is then
+ * that solve's outcome, e.g. CONVERGED | FALLBACK). */
+enum { MAPLE_CELL_CONVERGED = 1, MAPLE_CELL_BREAKDOWN = 2, MAPLE_CELL_MAXIT = 4, MAPLE_CELL_FALLBACK = 8 };
 
 const char* maple_last_error_string(void);
 int maple_version(void);

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(_PKG, "libmaple_b200.so")
 MAPLE_OK = 0
 ELASTIC, THERMAL = 0, 1
 FP64, MIXED = 0, 1
-CELL_CONVERGED, CELL_BREAKDOWN, CELL_MAXIT = 1, 2, 4
+CELL_CONVERGED, CELL_BREAKDOWN, CELL_MAXIT, CELL_FALLBACK = 1, 2, 4, 8
 
 _P = C.c_void_p
 _I = C.c_int

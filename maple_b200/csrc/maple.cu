@@ -147,6 +147,8 @@ struct Lane {
   // power iterations of the other levels
   cudaStream_t side = nullptr;
   cudaEvent_t side_fork = nullptr, side_join = nullptr;
+  int* fb_mask = nullptr;  // cells re-solved in FP64 after a mixed-precision breakdown
+  int* fb_bad = nullptr;   // per cell: the iterate holds a non-finite value
 };
 
 // lane of the calling thread: set by LaneScope around each physics' work
@@ -412,7 +414,7 @@ static void reduce(maple_ctx* c, const double* part, unsigned nb, double* out, c
 // hierarchy
 // ---------------------------------------------------------------------------
 template <typename T, int D>
-static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
+static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s, const int* act) {
   // level 0: the element bound holds for every density
   KL(c, s, k_fill<double><<<nblk(c->B), kThreads, 0, s>>>(o.hi[0], c->B, g_tab.lam_elem[D == 3 ? 0 : 1]));
   for (int l = 1; l < c->L - 1; ++l) {
@@ -425,7 +427,7 @@ static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
       a.u = v;
       a.out = w;
       a.part = LN(c).part;
-      apply<T, D, 1, M_POWER>(c, p, o, l, a, c->active, s);
+      apply<T, D, 1, M_POWER>(c, p, o, l, a, act, s);
       std::swap(v, w);
     }
     reduce<2>(c, LN(c).part, ceil_div(Nl, kPowerNodes<D>), LN(c).red, s);
@@ -434,11 +436,11 @@ static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s) {
 }
 
 template <int D>
-static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
+static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s, const int* mask = nullptr) {
   Phys& p = c->ph[phys];
   bool side_inverse = false;
   const int B = c->B, k = 8 * D, L = c->L;
-  const int* act = c->active;
+  const int* act = mask ? mask : c->active;
   // level-1 element matrices from the fine densities
   {
     const int nc = c->n[1];
@@ -502,9 +504,9 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s) {
     }
   }
   if (prec == MAPLE_FP64)
-    power_bounds<double, D>(c, p, p.o64, s);
+    power_bounds<double, D>(c, p, p.o64, s, act);
   else
-    power_bounds<float, D>(c, p, p.o32, s);
+    power_bounds<float, D>(c, p, p.o32, s, act);
   if (side_inverse) CK(cudaStreamWaitEvent(s, LN(c).side_join, 0));
   p.built = true;
   p.built_prec = prec;
@@ -821,42 +823,122 @@ __global__ void k_outer_check(const double* rr, const double* bn, double rtol2, 
   run[b] = !all;
 }
 
+static void ensure_prec(maple_ctx* c, int phys, int prec);
+
+// per-cell outcome of the last PCG run of this lane: BREAKDOWN when a column was
+// frozen by a breakdown (p.Ap <= 0 or non-finite), else CONVERGED or MAXIT
+static void read_outcome(maple_ctx* c, int R, std::vector<int>& iters, std::vector<int>& status, cudaStream_t s) {
+  const int B = c->B;
+  std::vector<int> cd(B), dn((size_t)B * R);
+  iters.assign(B, 0);
+  status.assign(B, 0);
+  CK(cudaMemcpyAsync(iters.data(), LN(c).sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(cd.data(), LN(c).sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(dn.data(), LN(c).sc.done, (size_t)B * R * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int b = 0; b < B; ++b) {
+    bool brk = false;
+    for (int r = 0; r < R; ++r) brk |= dn[(size_t)b * R + r] == 2;
+    status[b] = brk ? MAPLE_CELL_BREAKDOWN : (cd[b] ? MAPLE_CELL_CONVERGED : MAPLE_CELL_MAXIT);
+  }
+}
+
+// flags[b] = 1 if cell b of x (B cells of len values) holds a non-finite value
+__global__ void k_nonfinite_cells(const double* __restrict__ x, size_t len, const int* mask, int* flags) {
+  const int b = blockIdx.y;
+  if (mask && !mask[b]) return;
+  const double* xb = x + (size_t)b * len;
+  bool bad = false;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (size_t)gridDim.x * blockDim.x)
+    bad |= !isfinite(xb[i]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags + b, 1);
+}
+
 template <int D, int R>
 static void solve_phys(maple_ctx* c, int phys, int prec, const double* F, double* x64, bool x_zero, double rtol,
                        int maxit, int* iters_host, int* status_host, cudaStream_t s) {
   Phys& p = c->ph[phys];
   const int B = c->B, N = nodes(c->n[0]);
-  const unsigned nb = nblk(N);
-  const size_t vb64 = (size_t)B * N * R * D * sizeof(double);
-  std::vector<int> it_total(B, 0);
-  int conv_all = 0;
+  const size_t vb64 = (size_t)B * N * R * D * sizeof(double), cell_len = (size_t)N * R * D;
+  std::vector<int> it, st;
   if (prec == MAPLE_FP64) {
     Ops<double>& o = p.o64;
     if (!x_zero) CK(cudaMemcpyAsync(o.x, x64, vb64, cudaMemcpyDeviceToDevice, s));
     pcg<double, D, R>(c, p, o, F, x_zero, rtol, maxit, nullptr, s);
     CK(cudaMemcpyAsync(x64, o.x, vb64, cudaMemcpyDeviceToDevice, s));
-    std::vector<int> it(B), cd(B);
-    CK(cudaMemcpyAsync(it.data(), LN(c).sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(cd.data(), LN(c).sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    for (int b = 0; b < B; ++b) {
-      it_total[b] = it[b];
-      if (status_host) status_host[b] = cd[b] ? MAPLE_CELL_CONVERGED : MAPLE_CELL_MAXIT;
-    }
+    read_outcome(c, R, it, st, s);
   } else {
     pcg_mixed<D, R>(c, p, F, x64, x_zero, rtol, maxit, s);
-    std::vector<int> it(B), cd(B);
-    CK(cudaMemcpyAsync(it.data(), LN(c).sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(cd.data(), LN(c).sc.cell_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    for (int b = 0; b < B; ++b) {
-      it_total[b] = it[b];
-      if (status_host) status_host[b] = cd[b] ? MAPLE_CELL_CONVERGED : MAPLE_CELL_MAXIT;
+    read_outcome(c, R, it, st, s);
+    // Fallback: a cell whose mixed-precision solve broke down is solved again
+    // in plain FP64 MG-PCG (FP64 hierarchy built for those cells only) from its
+    // last iterate, or from zero when that iterate is not finite or when the
+    // FP64 solve from it breaks down too.  The other
+    // cells and the FP32 hierarchy are untouched; the second host thread of
+    // an OC step never sees this lane's masks.
+    std::vector<int> fb(B, 0);
+    bool any = false;
+    for (int b = 0; b < B; ++b)
+      if (st[b] == MAPLE_CELL_BREAKDOWN && (c->h_active.empty() || c->h_active[b])) fb[b] = 1, any = true;
+    if (any) {
+      Lane& ln = LN(c);
+      if (!ln.fb_mask) {
+        ln.fb_mask = dnew<int>(c, B);
+        ln.fb_bad = dnew<int>(c, B);
+      }
+      CK(cudaMemcpyAsync(ln.fb_mask, fb.data(), B * sizeof(int), cudaMemcpyHostToDevice, s));
+      CK(cudaMemsetAsync(ln.fb_bad, 0, B * sizeof(int), s));
+      KL(c, s, k_nonfinite_cells<<<dim3(64, B), kThreads, 0, s>>>(x64, cell_len, ln.fb_mask, ln.fb_bad));
+      std::vector<int> bad(B, 0);
+      CK(cudaMemcpyAsync(bad.data(), ln.fb_bad, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      ensure_prec(c, phys, MAPLE_FP64);
+      build_hierarchy<D>(c, phys, MAPLE_FP64, s, ln.fb_mask);
+      Ops<double>& o = p.o64;
+      for (int b = 0; b < B; ++b) {
+        if (!fb[b]) continue;
+        double* xo = o.x + (size_t)b * cell_len;
+        if (bad[b])
+          CK(cudaMemsetAsync(xo, 0, cell_len * sizeof(double), s));
+        else
+          CK(cudaMemcpyAsync(xo, x64 + (size_t)b * cell_len, cell_len * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      }
+      std::vector<int> it2, st2;
+      // attempt 1 from the last iterate; attempt 2 from zero for the cells whose
+      // last iterate led into a breakdown again (e.g. a finite but wild guess,
+      // whose size puts the tolerance beyond reach)
+      for (int attempt = 0; attempt < 2 && any; ++attempt) {
+        if (attempt == 1) {
+          any = false;
+          for (int b = 0; b < B; ++b) {
+            fb[b] = fb[b] && st2[b] == MAPLE_CELL_BREAKDOWN && !bad[b];
+            if (fb[b]) {
+              any = true;
+              CK(cudaMemsetAsync(o.x + (size_t)b * cell_len, 0, cell_len * sizeof(double), s));
+            }
+          }
+          if (!any) break;
+          CK(cudaMemcpyAsync(ln.fb_mask, fb.data(), B * sizeof(int), cudaMemcpyHostToDevice, s));
+        }
+        pcg<double, D, R>(c, p, o, F, false, rtol, maxit, ln.fb_mask, s);
+        for (int b = 0; b < B; ++b)
+          if (fb[b])
+            CK(cudaMemcpyAsync(x64 + (size_t)b * cell_len, o.x + (size_t)b * cell_len, cell_len * sizeof(double),
+                               cudaMemcpyDeviceToDevice, s));
+        read_outcome(c, R, it2, st2, s);
+        for (int b = 0; b < B; ++b)
+          if (fb[b]) {
+            it[b] += it2[b];
+            st[b] = st2[b] | MAPLE_CELL_FALLBACK;
+          }
+      }
+      p.built_prec = MAPLE_MIXED;  // the FP32 hierarchy still serves the next mixed solves
     }
   }
-  if (iters_host)
-    for (int b = 0; b < B; ++b) iters_host[b] = it_total[b];
-  (void)conv_all;
+  for (int b = 0; b < B; ++b) {
+    if (iters_host) iters_host[b] = it[b];
+    if (status_host) status_host[b] = st[b];
+  }
 }
 
 static void dispatch_solve(maple_ctx* c, int phys, int prec, const double* F, double* x64, bool x_zero, double rtol,
