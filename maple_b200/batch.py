@@ -12,6 +12,7 @@ process / GPU in ``maple/pareto/densify_pareto_property_network_32.py:
 """
 from __future__ import annotations
 
+import os
 import time
 from dataclasses import dataclass, field
 from typing import Optional
@@ -19,6 +20,7 @@ from typing import Optional
 import numpy as np
 import torch
 
+from ._lib import MapleError
 from .core import HomogenizationContext
 
 
@@ -72,6 +74,23 @@ def seeded_design(seed, r, sigma, vf, scale=0.25, xmin=1e-3):
 
 ITER_LOG_COLUMNS = ["iter", "J_total", "J_raw", "P_print", "P_cavity", "mean_x", "mean_rho", "dx_max", "dx_mean",
                     "time_sec"]
+CHECKPOINT_VERSION = 1
+
+
+def save_checkpoint(path: str, state: dict) -> None:
+    """Write a batched OC state (numpy arrays and scalars) to `path` atomically
+    (a temporary file renamed over it)."""
+    tmp = path + ".tmp.npz"
+    np.savez(tmp, version=CHECKPOINT_VERSION, **state)
+    os.replace(tmp, path)
+
+
+def load_checkpoint(path: str) -> dict:
+    with np.load(path, allow_pickle=False) as f:
+        state = {k: f[k] for k in f.files}
+    if int(state.pop("version")) != CHECKPOINT_VERSION:
+        raise ValueError(f"{path}: unsupported checkpoint version")
+    return state
 # stall test of main_IHD_v3.py:611-618, 711-714
 STALL_TOL_X, STALL_TOL_J, STALL_PATIENCE, STALL_MIN_ITERS = 1e-3, 1e-4, 10, 10
 
@@ -81,7 +100,8 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
            rtol: float = 1e-8, maxit: int = 500, dx_tol: float = 0.01, max_iters: int = 200,
            ctx: Optional[HomogenizationContext] = None, device=None, record: bool = False,
            guess=None, symmetry: str = "none", penalties: Optional[dict] = None, stop_rule: str = "dx",
-           log_rows: bool = False) -> BatchResult:
+           log_rows: bool = False, checkpoint: Optional[str] = None, checkpoint_every: int = 0,
+           resume: bool = False, checkpoint_fields: bool = False) -> BatchResult:
     """Run B independent OC loops to their own stopping points (with the
     symmetry projection `symmetry`, a spec as in parse_symmetry).  `guess` =
     (elastic (B, 6, 3, N), thermal (B, 3, 1, N)) float64 fields: the initial
@@ -94,7 +114,17 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
     with max|dx| < STALL_TOL_X and |dJ|/|J_prev| < STALL_TOL_J.  `penalties`:
     keyword arguments of HomogenizationContext.set_penalties, applied to every
     cell (J is then the penalised objective).  log_rows: keep each cell's
-    iteration rows (ITER_LOG_COLUMNS, the optimizer's iter_log.csv)."""
+    iteration rows (ITER_LOG_COLUMNS, the optimizer's iter_log.csv).
+
+    Checkpoints: with `checkpoint` (a .npz path) and checkpoint_every = k > 0,
+    the state of every cell is written after every k-th iteration and at the
+    end.  The state is the design, iteration and PCG counts, stop state, last
+    objective terms and stall counters.  With checkpoint_fields it also holds
+    the solver fields, which are the next warm start.  resume=True continues
+    from an existing checkpoint instead of x0 (same cells, shapes and settings),
+    up to max_iters iterations in total.  With the fields the continuation
+    repeats the uninterrupted run exactly; without them its first solves start
+    from zero (same results to the solver tolerance)."""
     if stop_rule not in ("dx", "reference"):
         raise ValueError("stop_rule must be 'dx' or 'reference'")
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -127,10 +157,39 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
     terms = np.zeros((B, 3))
     hist = []
     logs = [[] for _ in range(B)]
+    it0 = 0
+    if resume:
+        if not checkpoint or not os.path.exists(checkpoint):
+            raise FileNotFoundError(f"no checkpoint to resume from: {checkpoint}")
+        ck = load_checkpoint(checkpoint)
+        if tuple(ck["x"].shape) != (B, N) or str(ck["stop_rule"]) != stop_rule:
+            raise ValueError("checkpoint does not match this run (cells, resolution or stop rule)")
+        x = torch.as_tensor(ck["x"], dtype=torch.float64).to(dev).contiguous()
+        active, iters, pcg, conv = (ck["active"].astype(np.int32), ck["iters"].astype(np.int64),
+                                    ck["pcg"].astype(np.int64), ck["conv"].astype(bool))
+        J, J_raw, P_print, P_cavity = ck["J"], ck["J_raw"], ck["P_print"], ck["P_cavity"]
+        J_prev, stall, terms, it0 = ck["J_prev"], ck["stall"].astype(np.int64), ck["terms"], int(ck["it"])
+        for phys in ("elastic", "thermal"):
+            if f"u_{phys}" in ck:
+                ctx.set_solution(phys, torch.as_tensor(ck[f"u_{phys}"]).to(dev).contiguous())
+
+    def write_checkpoint(it_next):
+        state = dict(x=x.cpu().numpy(), active=active, iters=iters, pcg=pcg, conv=conv, J=J, J_raw=J_raw,
+                     P_print=P_print, P_cavity=P_cavity, J_prev=J_prev, stall=stall, terms=terms, it=it_next,
+                     stop_rule=stop_rule)
+        if checkpoint_fields:
+            for phys in ("elastic", "thermal"):
+                try:
+                    state[f"u_{phys}"] = ctx.solution(phys).cpu().numpy()
+                except MapleError:  # that physics was never solved (no cell weights it)
+                    pass
+        save_checkpoint(checkpoint, state)
+
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
+    it = it0 - 1
     try:
-        for it in range(max_iters):
+        for it in range(it0, max_iters):
             if not active.any():
                 break
             ctx.set_active(active)
@@ -172,6 +231,10 @@ def oc_run(x0, weights, volfrac, *, r: Optional[int] = None, move: float = 0.2, 
             if record:
                 hist.append(dict(active=int(act.sum()), J=J.copy(), dx_max=st[:, 0].copy(),
                                  pcg=np.array(out["iters"])))
+            if checkpoint and checkpoint_every > 0 and (it + 1) % checkpoint_every == 0:
+                write_checkpoint(it + 1)
+        if checkpoint and checkpoint_every > 0:
+            write_checkpoint(it + 1)
         torch.cuda.synchronize(dev)
     finally:
         ctx.set_active(np.ones(B, dtype=np.int32))

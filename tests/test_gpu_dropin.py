@@ -199,3 +199,31 @@ def test_optimize_with_symmetry_follows_reference(ihd8, golden, tmp_path):
         assert abs(float(rows[1 + it][2]) - ref) < 1e-8 * ref
     assert res.iters_run == 3
     assert ihd8.homog_ctx is not None
+
+
+def test_checkpoint_resume_repeats_the_run(lib, tmp_path):
+    """A batched OC run interrupted after 3 iterations and resumed from its
+    checkpoint (with the solver fields) ends exactly where the uninterrupted
+    6-iteration run ends; without the fields the resumed solves start from
+    zero and agree to the solver tolerance."""
+    import os
+    from maple_b200.batch import oc_run, seeded_design
+    r = 16
+    x0 = np.stack([seeded_design(s, r, 2.0, 0.3).reshape(-1) for s in (0, 1)])
+    w = np.array([[0.5, 0.0, 0.5], [0.2, 0.3, 0.5]])
+    vf = np.array([0.3, 0.3])
+    kw = dict(precision="mixed", rtol=1e-10, stop_rule="reference", move=0.2)
+    full = oc_run(x0, w, vf, max_iters=6, **kw)
+    for fields in (True, False):
+        path = os.path.join(tmp_path, f"ck_{fields}.npz")
+        part = oc_run(x0, w, vf, max_iters=3, checkpoint=path, checkpoint_every=1, checkpoint_fields=fields, **kw)
+        assert list(part.iters_run) == [3, 3]
+        res = oc_run(x0, w, vf, max_iters=6, checkpoint=path, checkpoint_every=2, resume=True,
+                     checkpoint_fields=fields, **kw)
+        assert list(res.iters_run) == list(full.iters_run) == [6, 6]
+        if fields:
+            np.testing.assert_array_equal(res.x.cpu().numpy(), full.x.cpu().numpy())
+            np.testing.assert_array_equal(res.J, full.J)
+        else:
+            np.testing.assert_allclose(res.x.cpu().numpy(), full.x.cpu().numpy(), rtol=0, atol=1e-7)
+            np.testing.assert_allclose(res.J, full.J, rtol=1e-8)
