@@ -5,6 +5,8 @@
 #include "printability.h"
 #include "tables.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -134,6 +136,14 @@ struct Scalars {
 // convergence flags and capture stream of one solve in flight.  A context has
 // one lane per physics so that the elastic and thermal solves of an OC step
 // can run at the same time (from two host threads, on two streams).
+// NVTX range for profilers (nsys, ncu --nvtx): a no-op unless a tool is attached
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
+
 struct Lane {
   double* part = nullptr;  // partial sums [B][nblk0][32]
   double* red = nullptr;   // reduced values [B][32]
@@ -437,6 +447,7 @@ static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s, const
 
 template <int D>
 static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s, const int* mask = nullptr) {
+  Range range(D == 3 ? "maple:build elastic" : "maple:build thermal");
   Phys& p = c->ph[phys];
   bool side_inverse = false;
   const int B = c->B, k = 8 * D, L = c->L;
@@ -857,6 +868,8 @@ __global__ void k_nonfinite_cells(const double* __restrict__ x, size_t len, cons
 template <int D, int R>
 static void solve_phys(maple_ctx* c, int phys, int prec, const double* F, double* x64, bool x_zero, double rtol,
                        int maxit, int* iters_host, int* status_host, cudaStream_t s) {
+  Range range(D == 3 ? (prec == MAPLE_FP64 ? "maple:solve elastic fp64" : "maple:solve elastic mixed")
+                     : (prec == MAPLE_FP64 ? "maple:solve thermal fp64" : "maple:solve thermal mixed"));
   Phys& p = c->ph[phys];
   const int B = c->B, N = nodes(c->n[0]);
   const size_t vb64 = (size_t)B * N * R * D * sizeof(double), cell_len = (size_t)N * R * D;
@@ -987,6 +1000,7 @@ static void assemble_rhs(maple_ctx* c, int phys, const double* rho, double* F, c
 }
 
 static void homogenize(maple_ctx* c, int phys, cudaStream_t s) {
+  Range range("maple:homogenize");
   Phys& p = c->ph[phys];
   const int N = nodes(c->n[0]);
   const unsigned nb = nblk(N);
@@ -1072,6 +1086,7 @@ __global__ void k_penalise_J(double* J, const double* Pp, double lp, const doubl
 
 // the configured penalties of rho [B][N] and their gradients into the context
 static void run_penalties(maple_ctx* c, const double* rho, bool print, bool cavity, cudaStream_t s) {
+  Range range("maple:penalties");
   try {
     if (print) maple_pr::overhang(rho, c->oplan, c->P_print, c->dP_print, c->pen_work, s);
     if (cavity) maple_pr::cavity(rho, c->cplan, c->P_cav, c->dP_cav, c->pen_work, s);
@@ -1715,6 +1730,7 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
                   double move, double xmin, int filter_k, int prec, double rtol, int maxit, int warm, double* x_next,
                   double* J, double* terms, double* CH, double* kappa, double* stats, int* iters, maple_stream_t s) {
   return guarded([&] {
+    Range range("maple:oc_step");
     require(c != nullptr && x && w && vf && x_next, "NULL argument");
     require(x_next != x, "x_next must not alias x");
     require(prec == MAPLE_FP64 || prec == MAPLE_MIXED, "unknown precision");
