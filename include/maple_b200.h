@@ -85,6 +85,11 @@ int maple_set_graphs(maple_ctx* ctx, int enable);
  * faster below 32^3 nodes).  Results differ only by FP summation order. */
 int maple_set_stencil_split(maple_ctx* ctx, int min_n);
 
+/* Chebyshev degree of the smoother on multigrid levels 2 and deeper (level 0
+ * and 1 use the degree of maple_set_solver_options).  0 (default): automatic,
+ * 3 on fine grids of 64^3 nodes and up, else the common degree. */
+int maple_set_coarse_degree(maple_ctx* ctx, int deg);
+
 /* Elastic and thermal solves of maple_oc_step at the same time (default on):
  * the thermal build and solve run on a second stream driven by a second host
  * thread of the library.  Off runs them one after the other on the caller's

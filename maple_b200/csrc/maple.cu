@@ -221,6 +221,7 @@ struct maple_ctx {
   std::vector<Rec> recs;
   // options
   int cheb_degree = 2;
+  int cheb_degree_coarse = 0;  // levels >= 2; 0: automatic
   double cheb_ratio = 10.0;
   int power_iters = 12;
   double power_safety = 1.15;
@@ -538,7 +539,11 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
     KL(c, s, k_coarse_solve<T, R><<<dim3((ndof + 7) / 8, B), kThreads, 0, s>>>(p.Ainv, f, o.U[l][1], ndof, D, act));
     return;
   }
-  const int deg = c->cheb_degree;
+  // levels 2 and deeper: their own degree (automatic: 3 on grids of 64^3 and
+  // up, where the extra cheap sweeps save more PCG iterations than they cost)
+  const int coarse_deg = c->cheb_degree_coarse > 0 ? c->cheb_degree_coarse
+                                                   : (c->r >= 64 ? std::max(3, c->cheb_degree) : c->cheb_degree);
+  const int deg = l >= 2 ? coarse_deg : c->cheb_degree;
   int cur = 0;
   {
     ApplyArgs<T> a{};
@@ -1485,6 +1490,15 @@ int maple_set_stencil_split(maple_ctx* c, int min_n) {
     require(min_n >= 0, "min_n must be >= 0");
     drop_graphs(c);
     c->split_min_n = min_n;
+  });
+}
+
+int maple_set_coarse_degree(maple_ctx* c, int deg) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(deg >= 0 && deg <= 8, "chebyshev degree must be in [0, 8] (0: automatic)");
+    drop_graphs(c);
+    c->cheb_degree_coarse = deg;
   });
 }
 
