@@ -1579,50 +1579,6 @@ struct PcgScalars {
   int* iters;      // per cell
 };
 
-// after q = A p: alpha = rz / pq (0 once the column converged or on breakdown)
-__global__ void k_pcg_alpha(PcgScalars s, int total, int* breakdown) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  double a = 0.0;
-  if (!s.done[i]) {
-    const double pq = s.pq[i];
-    if (pq > 0.0 && isfinite(pq)) {
-      a = s.rz[i] / pq;
-    } else {
-      s.done[i] = 2;  // breakdown: freeze this column
-      if (breakdown) atomicOr(breakdown, 1);
-    }
-  }
-  s.alpha[i] = a;
-}
-
-// after the update: convergence test on ||r|| <= rtol ||b||
-// `count` = 1 inside the iteration loop: the per-cell iteration counter is
-// advanced on the device so that the launch parameters stay fixed (graphs).
-__global__ void k_pcg_check(PcgScalars s, int B, int R, double rtol2, int count) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B) return;
-  if (s.cell_done[b]) return;
-  if (count) s.iters[b] += 1;
-  int all = 1;
-  for (int c = 0; c < R; ++c) {
-    const int i = b * R + c;
-    if (!s.done[i] && s.rr[i] <= rtol2 * s.bnorm2[i]) s.done[i] = 1;
-    all &= (s.done[i] != 0);
-  }
-  if (all) s.cell_done[b] = 1;
-}
-
-// after z = M r: beta = rz_new / rz; rz = rz_new
-__global__ void k_pcg_beta(PcgScalars s, int total) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  double be = 0.0;
-  if (!s.done[i] && s.rz[i] != 0.0) be = s.rz_new[i] / s.rz[i];
-  s.beta[i] = be;
-  s.rz[i] = s.rz_new[i];
-}
-
 // convert an FP64 vector to FP32 with a per-(cell,rhs) scale; and back (add)
 template <int R, int D>
 __global__ void k_to_f32_scaled(const double* __restrict__ src, float* __restrict__ dst, const double* __restrict__ inv_scale,
@@ -1662,16 +1618,6 @@ __global__ void k_add_f32_scaled(double* __restrict__ dst, const float* __restri
   }
 }
 
-// per (cell, rhs): scale = 1/||r||, inv = ||r|| from the reduced r.r
-__global__ void k_col_scales(const double* __restrict__ rr, double* __restrict__ scale, double* __restrict__ inv,
-                             int total) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  const double nrm = sqrt(fmax(rr[i], 0.0));
-  scale[i] = nrm > 0 ? 1.0 / nrm : 0.0;
-  inv[i] = nrm;
-}
-
 // z = inv * z32 (FP64) with partial dots r.z and (optionally) q.z
 template <int R, int D>
 __global__ void k_precond_back(const float* __restrict__ z32, const double* __restrict__ inv, double* __restrict__ z,
@@ -1699,17 +1645,102 @@ __global__ void k_precond_back(const float* __restrict__ z32, const double* __re
   block_sum_store<2 * R>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * 2 * R);
 }
 
-// flexible (Polak-Ribiere) beta = -alpha (z.q) / (r.z)_old ; rz <- rz_new.
-// red holds [cell][rz_new (R), zq (R)].
-__global__ void k_pcg_beta_flex(PcgScalars s, const double* __restrict__ red, int B, int R, int first) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= B * R) return;
-  const int b = i / R, c = i % R;
-  const double rz_new = red[b * 2 * R + c], zq = red[b * 2 * R + R + c];
-  double be = 0.0;
-  if (!first && !s.done[i] && s.rz[i] != 0.0) be = -s.alpha[i] * zq / s.rz[i];
-  s.beta[i] = be;
-  s.rz[i] = rz_new;
+// A block per cell reduces that cell's partial sums (as k_reduce_partials) and
+// then its thread 0 applies the PCG scalar step that consumes them, one launch
+// instead of two:
+//   ALPHA      alpha = rz / p.q, or freeze the column (done = 2) on a breakdown
+//              (p.q <= 0 or non-finite)
+//   CHECK      advance the iteration count (count), mark columns with
+//              ||r||^2 <= rtol^2 ||b||^2 done, the cell done when all are, clear
+//              its run flag, and (scale != NULL) the column scales 1/||r||, ||r||
+//   BETA       beta = rz_new / rz, rz = rz_new
+//   BETA_FLEX  flexible beta = -alpha (q.z) / rz, rz = r.z (first: beta = 0)
+//   SET_RZ     rz = rz_new
+enum { RED_PLAIN = 0, RED_ALPHA = 1, RED_CHECK = 2, RED_BETA = 3, RED_BETA_FLEX = 4, RED_SET_RZ = 5 };
+struct RedOp {
+  PcgScalars s;
+  int R = 0;
+  int* breakdown = nullptr;  // ALPHA
+  double rtol2 = 0;          // CHECK
+  int count = 0;             // CHECK: advance the iteration counter
+  int* run = nullptr;        // CHECK: run flags cleared for finished cells
+  double* scale = nullptr;   // CHECK: column scales 1/||r|| and ||r|| (nullable)
+  double* inv = nullptr;
+  int first = 0;             // BETA_FLEX
+};
+
+template <int K, int OP>
+__global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* __restrict__ out, RedOp op) {
+  const int b = blockIdx.x;
+  double v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = 0;
+  for (int i = threadIdx.x; i < nblk; i += kThreads) {
+    const double* p = part + ((size_t)b * nblk + i) * K;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += p[k];
+  }
+  block_sum_store<K>(v, out + (size_t)b * K);
+  if constexpr (OP == RED_PLAIN) return;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  PcgScalars& s = op.s;
+  const int R = op.R;
+  if constexpr (OP == RED_ALPHA) {
+    for (int c = 0; c < R; ++c) {
+      const int i = b * R + c;
+      double a = 0.0;
+      if (!s.done[i]) {
+        const double pq = s.pq[i];
+        if (pq > 0.0 && isfinite(pq)) {
+          a = s.rz[i] / pq;
+        } else {
+          s.done[i] = 2;  // breakdown: freeze this column
+          if (op.breakdown) atomicOr(op.breakdown, 1);
+        }
+      }
+      s.alpha[i] = a;
+    }
+  } else if constexpr (OP == RED_CHECK) {
+    if (!s.cell_done[b]) {
+      if (op.count) s.iters[b] += 1;
+      int all = 1;
+      for (int c = 0; c < R; ++c) {
+        const int i = b * R + c;
+        if (!s.done[i] && s.rr[i] <= op.rtol2 * s.bnorm2[i]) s.done[i] = 1;
+        all &= (s.done[i] != 0);
+      }
+      if (all) s.cell_done[b] = 1;
+    }
+    if (s.cell_done[b]) op.run[b] = 0;
+    if (op.scale)
+      for (int c = 0; c < R; ++c) {
+        const int i = b * R + c;
+        const double nrm = sqrt(fmax(s.rr[i], 0.0));
+        op.scale[i] = nrm > 0 ? 1.0 / nrm : 0.0;
+        op.inv[i] = nrm;
+      }
+  } else if constexpr (OP == RED_BETA) {
+    for (int c = 0; c < R; ++c) {
+      const int i = b * R + c;
+      double be = 0.0;
+      if (!s.done[i] && s.rz[i] != 0.0) be = s.rz_new[i] / s.rz[i];
+      s.beta[i] = be;
+      s.rz[i] = s.rz_new[i];
+    }
+  } else if constexpr (OP == RED_BETA_FLEX) {
+    const double* red = out + (size_t)b * K;
+    for (int c = 0; c < R; ++c) {
+      const int i = b * R + c;
+      const double rz_new = red[c], zq = red[R + c];
+      double be = 0.0;
+      if (!op.first && !s.done[i] && s.rz[i] != 0.0) be = -s.alpha[i] * zq / s.rz[i];
+      s.beta[i] = be;
+      s.rz[i] = rz_new;
+    }
+  } else if constexpr (OP == RED_SET_RZ) {
+    for (int c = 0; c < R; ++c) s.rz[b * R + c] = s.rz_new[b * R + c];
+  }
 }
 
 // deterministic pseudo-random start vector for power iterations

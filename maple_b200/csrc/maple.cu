@@ -421,6 +421,12 @@ static void reduce(maple_ctx* c, const double* part, unsigned nb, double* out, c
   KL(c, s, k_reduce_partials<K><<<c->B, kThreads, 0, s>>>(part, (int)nb, out));
 }
 
+// reduce a cell's partial sums and apply the PCG scalar step OP in one launch
+template <int K, int OP>
+static void reduce_op(maple_ctx* c, const double* part, unsigned nb, double* out, const RedOp& op, cudaStream_t s) {
+  KL(c, s, k_reduce_op<K, OP><<<c->B, kThreads, 0, s>>>(part, (int)nb, out, op));
+}
+
 // ---------------------------------------------------------------------------
 // hierarchy
 // ---------------------------------------------------------------------------
@@ -620,17 +626,6 @@ __global__ void k_init_flags(const int* active, const int* outer_run, int* done,
   for (int r = 0; r < R; ++r) done[b * R + r] = a ? 0 : 1;
 }
 
-__global__ void k_sync_run(const int* cell_done, int* run, int B) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B) return;
-  if (cell_done[b]) run[b] = 0;
-}
-
-__global__ void k_set_rz(double* rz, const double* rz_new, int total) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < total) rz[i] = rz_new[i];
-}
-
 // Runs the PCG iteration body until every active cell has converged or maxit
 // iterations ran.  The body is captured once into a CUDA graph per
 // (physics, precision, rtol) and replayed; the convergence flags are read back
@@ -716,15 +711,20 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
   KL(c, s, k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, LN(c).part, N, run));
   reduce<R>(c, LN(c).part, nb, sc.bnorm2, s);
   KL(c, s, k_dot<T, R, D><<<g2(N, B), kThreads, 0, s>>>(o.r, o.r, LN(c).part, N, run));
-  reduce<R>(c, LN(c).part, nb, sc.rr, s);
-  KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0));
-  KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
+  RedOp op{};
+  op.s = ps;
+  op.R = R;
+  op.breakdown = LN(c).breakdown;
+  op.rtol2 = rtol * rtol;
+  op.run = sc.run;
+  RedOp op0 = op;  // before the loop: no iteration counted
+  reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op0, s);
   if (all_done(c, sc.cell_done, run, s)) return;
   // z = M r ; rz ; p = z
   vcycle<T, D, R>(c, p, o, 0, o.r, run, LN(c).part, s);
-  reduce<R>(c, LN(c).part, nbf, sc.rz_new, s);
-  KL(c, s, k_set_rz<<<nblk(B * R), kThreads, 0, s>>>(sc.rz, sc.rz_new, B * R));
+  reduce_op<R, RED_SET_RZ>(c, LN(c).part, nbf, sc.rz_new, op, s);
   CK(cudaMemcpyAsync(o.p, o.U[0][1], vbytes, cudaMemcpyDeviceToDevice, s));
+  op.count = 1;
   auto body = [&](cudaStream_t st) {
     {
       ApplyArgs<T> a{};
@@ -733,15 +733,11 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
       a.part = LN(c).part;
       apply<T, D, R, M_MV>(c, p, o, 0, a, run, st);
     }
-    reduce<R>(c, LN(c).part, nbf, sc.pq, st);
-    KL(c, st, k_pcg_alpha<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R, LN(c).breakdown));
+    reduce_op<R, RED_ALPHA>(c, LN(c).part, nbf, sc.pq, op, st);
     KL(c, st, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.x, o.r, o.p, o.q, sc.alpha, LN(c).part, N, run));
-    reduce<R>(c, LN(c).part, nb, sc.rr, st);
-    KL(c, st, k_pcg_check<<<nblk(B), kThreads, 0, st>>>(ps, B, R, rtol * rtol, 1));
-    KL(c, st, k_sync_run<<<nblk(B), kThreads, 0, st>>>(sc.cell_done, sc.run, B));
+    reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op, st);
     vcycle<T, D, R>(c, p, o, 0, o.r, run, LN(c).part, st);
-    reduce<R>(c, LN(c).part, nbf, sc.rz_new, st);
-    KL(c, st, k_pcg_beta<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R));
+    reduce_op<R, RED_BETA>(c, LN(c).part, nbf, sc.rz_new, op, st);
     KL(c, st, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.p, o.U[0][1], sc.beta, N, run));
   };
   run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_FP64], rtol, maxit, body, s);
@@ -751,17 +747,17 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
 // Mixed precision: FP64 flexible PCG (FP64 fine operator, residuals and dots)
 // preconditioned by the FP32 V-cycle; the coarsest solve stays FP64.
 // ---------------------------------------------------------------------------
+// z = M r with the column scales of r already in place (set by the fused
+// convergence check), then r.z, q.z and the flexible beta in one reduction
 template <int D, int R>
 static void precondition_f32(maple_ctx* c, Phys& p, const double* r, const double* q, const int* run,
-                             cudaStream_t s) {
+                             const RedOp& op, cudaStream_t s) {
   const int B = c->B, N = nodes(c->n[0]);
-  Scalars& sc = LN(c).sc;
   Ops<float>& o = p.o32;
-  KL(c, s, k_col_scales<<<nblk(B * R), kThreads, 0, s>>>(sc.rr, LN(c).o_scale, LN(c).o_inv, B * R));
   KL(c, s, k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, LN(c).o_scale, N, run));
   vcycle<float, D, R>(c, p, o, 0, o.r, run, nullptr, s);
   KL(c, s, k_precond_back<R, D><<<g2(N, B), kThreads, 0, s>>>(o.U[0][1], LN(c).o_inv, p.z64, r, q, LN(c).part, N, run));
-  reduce<2 * R>(c, LN(c).part, nblk(N), LN(c).red, s);
+  reduce_op<2 * R, RED_BETA_FLEX>(c, LN(c).part, nblk(N), LN(c).red, op, s);
 }
 
 template <int D, int R>
@@ -789,13 +785,21 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
   KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, LN(c).part, N, run));
   reduce<R>(c, LN(c).part, nb, sc.bnorm2, s);
   KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(r, r, LN(c).part, N, run));
-  reduce<R>(c, LN(c).part, nb, sc.rr, s);
-  KL(c, s, k_pcg_check<<<nblk(B), kThreads, 0, s>>>(ps, B, R, rtol * rtol, 0));
-  KL(c, s, k_sync_run<<<nblk(B), kThreads, 0, s>>>(sc.cell_done, sc.run, B));
+  RedOp op{};
+  op.s = ps;
+  op.R = R;
+  op.breakdown = LN(c).breakdown;
+  op.rtol2 = rtol * rtol;
+  op.run = sc.run;
+  op.scale = LN(c).o_scale;
+  op.inv = LN(c).o_inv;
+  RedOp op0 = op;  // before the loop: no iteration counted, first flexible beta
+  op0.first = 1;
+  reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op0, s);
   if (all_done(c, sc.cell_done, run, s)) return;
-  precondition_f32<D, R>(c, p, r, nullptr, run, s);
-  KL(c, s, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, s>>>(ps, LN(c).red, B, R, 1));
+  precondition_f32<D, R>(c, p, r, nullptr, run, op0, s);
   CK(cudaMemcpyAsync(pv, z, vbytes, cudaMemcpyDeviceToDevice, s));
+  op.count = 1;
   auto body = [&](cudaStream_t st) {
     {
       ApplyArgs<double> a{};
@@ -804,14 +808,10 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
       a.part = LN(c).part;
       apply<double, D, R, M_MV>(c, p, o64, 0, a, run, st);
     }
-    reduce<R>(c, LN(c).part, nbf, sc.pq, st);
-    KL(c, st, k_pcg_alpha<<<nblk(B * R), kThreads, 0, st>>>(ps, B * R, LN(c).breakdown));
+    reduce_op<R, RED_ALPHA>(c, LN(c).part, nbf, sc.pq, op, st);
     KL(c, st, k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, st>>>(x, r, pv, q, sc.alpha, LN(c).part, N, run));
-    reduce<R>(c, LN(c).part, nb, sc.rr, st);
-    KL(c, st, k_pcg_check<<<nblk(B), kThreads, 0, st>>>(ps, B, R, rtol * rtol, 1));
-    KL(c, st, k_sync_run<<<nblk(B), kThreads, 0, st>>>(sc.cell_done, sc.run, B));
-    precondition_f32<D, R>(c, p, r, q, run, st);
-    KL(c, st, k_pcg_beta_flex<<<nblk(B * R), kThreads, 0, st>>>(ps, LN(c).red, B, R, 0));
+    reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op, st);
+    precondition_f32<D, R>(c, p, r, q, run, op, st);
     KL(c, st, k_pcg_direction<double, R, D><<<g2(N, B), kThreads, 0, st>>>(pv, z, sc.beta, N, run));
   };
   run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_MIXED], rtol, maxit, body, s);
