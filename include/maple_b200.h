@@ -85,6 +85,13 @@ int maple_set_graphs(maple_ctx* ctx, int enable);
  * faster below 32^3 nodes).  Results differ only by FP summation order. */
 int maple_set_stencil_split(maple_ctx* ctx, int min_n);
 
+/* Coarse multigrid levels with n <= max_n nodes per axis apply their stencils
+ * with the nine-thread kernel (one thread per node and (x, y) offset pair;
+ * taken before the split kernel); 0 disables it.  Default 64: on B200 it is
+ * faster than the tile kernel on 8^3 and 16^3 levels and than the split
+ * kernel on 32^3 and 64^3 levels.  Results differ only by FP summation order. */
+int maple_set_stencil_nine(maple_ctx* ctx, int max_n);
+
 /* Chebyshev degree of the smoother on multigrid levels 2 and deeper (level 0
  * and 1 use the degree of maple_set_solver_options).  0 (default): automatic,
  * 3 on fine grids of 64^3 nodes and up, else the common degree. */

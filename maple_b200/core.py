@@ -161,6 +161,11 @@ class HomogenizationContext:
         split-offset stencil kernel (0: never)."""
         _lib.check(self._lib.maple_set_stencil_split(self._h, int(min_n)))
 
+    def set_stencil_nine(self, max_n: int = 64):
+        """Coarse levels with at most max_n nodes per axis use the nine-thread
+        stencil kernel (0: never)."""
+        _lib.check(self._lib.maple_set_stencil_nine(self._h, int(max_n)))
+
     def set_graphs(self, enable: bool):
         """Replay the PCG iteration body as a captured CUDA graph (default on)."""
         _lib.check(self._lib.maple_set_graphs(self._h, int(bool(enable))))

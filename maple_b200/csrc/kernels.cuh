@@ -952,6 +952,111 @@ __global__ void __launch_bounds__(ST_THREADS) k_apply_stencil_split(ApplyArgs<T>
   }
 }
 
+// Small coarse levels: nine threads per node, one per (x, y) offset pair, each
+// summing its 3 z offsets for all R load cases straight from global memory
+// (the whole level sits in L2), 32 nodes per CTA (a warp is 32 consecutive
+// nodes of one offset pair: coalesced stencil reads).  The nine partial sums
+// meet in shared memory, added in (x, y) offset order; thread (node, q < R)
+// finishes load case q (MV / RES / CHEB / JAC0 as in k_apply_stencil_tile).
+constexpr int NINE_NODES = 32;
+constexpr int NINE_THREADS = 9 * NINE_NODES;
+
+template <typename T, int D, int R, int MODE>
+__global__ void __launch_bounds__(NINE_THREADS) k_apply_stencil_nine(ApplyArgs<T> a) {
+  constexpr int RD = R * D;
+  static_assert(R <= 9, "one finishing thread per load case");
+  __shared__ T red[9][RD][NINE_NODES];
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
+  const int n = a.n, N = a.N;
+  const size_t NN = (size_t)N;
+  const int tn = threadIdx.x % NINE_NODES, q = threadIdx.x / NINE_NODES;  // q = 3 ox + oy
+  const int id = blockIdx.x * NINE_NODES + tn;
+  const bool valid = id < N;
+  const int z = id % n, y = (id / n) % n, x = id / (n * n);
+  if constexpr (MODE != M_JAC0) {
+    T acc[R][D];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < D; ++i) acc[r][i] = T(0);
+    if (valid) {
+      const int ox = q / 3, oy = q % 3;
+      const int xx = wrapn(x + ox - 1, n), yy = wrapn(y + oy - 1, n);
+      const T* __restrict__ ub = a.u + (size_t)b * RD * NN;
+      const T* __restrict__ S = a.S + (size_t)b * 27 * D * D * NN + id;
+#pragma unroll
+      for (int oz = 0; oz < 3; ++oz) {
+        const int o = q * 3 + oz;
+        const int nb = (xx * n + yy) * n + wrapn(z + oz - 1, n);
+        T sv[D][D];
+#pragma unroll
+        for (int i = 0; i < D; ++i)
+#pragma unroll
+          for (int j = 0; j < D; ++j) sv[i][j] = __ldg(S + (size_t)((o * D + i) * D + j) * NN);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+          for (int j = 0; j < D; ++j) {
+            const T uv = __ldg(ub + (size_t)(r * D + j) * NN + nb);
+#pragma unroll
+            for (int i = 0; i < D; ++i) acc[r][i] += sv[i][j] * uv;
+          }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < D; ++i) red[q][r * D + i][tn] = acc[r][i];
+  }
+  __shared__ double s_coef[2];
+  if constexpr (MODE == M_CHEB || MODE == M_JAC0) {
+    if (threadIdx.x == 0) cheb_coeffs(a.hi[b], a.ratio, MODE == M_JAC0 ? 0 : a.step, s_coef[0], s_coef[1]);
+  }
+  __syncthreads();
+  if (q >= R || !valid) return;
+  const int r = q;
+  T tot[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    T t = T(0);
+    if constexpr (MODE != M_JAC0) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) t += red[k][r * D + i][tn];
+    }
+    tot[i] = t;
+  }
+  const size_t vo = ((size_t)b * R + r) * D * NN + id;  // component i at vo + i*N
+  if constexpr (MODE == M_MV) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.out[vo + i * NN] = tot[i];
+  } else if constexpr (MODE == M_RES) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) a.out[vo + i * NN] = a.f[vo + i * NN] - tot[i];
+  } else {
+    const double al = s_coef[0], be = s_coef[1];
+    T Di[D][D];
+    const T* __restrict__ Dp = a.Dinv + (size_t)b * D * D * NN + id;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) Di[i][j] = __ldg(Dp + (size_t)(i * D + j) * NN);
+    T res[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) res[i] = (MODE == M_JAC0) ? a.f[vo + i * NN] : a.f[vo + i * NN] - tot[i];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      T zz = 0;
+#pragma unroll
+      for (int j = 0; j < D; ++j) zz += Di[i][j] * res[j];
+      T d = T(be) * zz;
+      if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + i * NN];
+      a.dout[vo + i * NN] = d;
+      a.out[vo + i * NN] = (MODE == M_JAC0) ? d : a.u[vo + i * NN] + d;
+    }
+  }
+}
+
 // power iteration step on a coarse level: w = Dinv A u and the Rayleigh terms.
 // One thread per (node, row i): a CTA covers kPowerNodes<D> nodes, rows
 // i-major so that consecutive threads read consecutive stencil entries; the

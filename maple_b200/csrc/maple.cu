@@ -199,6 +199,7 @@ struct maple_ctx {
   bool use_graphs = true;
   bool concurrent = true;  // elastic and thermal solves of an OC step on two streams
   int split_min_n = 32;    // coarse levels with n >= this (n % 8 == 0) use k_apply_stencil_split; 0: never
+  int nine_max_n = 64;     // coarse levels with n <= this use k_apply_stencil_nine; 0: never
   int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
   // manufacturability penalties of the OC objective (maple_set_penalties)
   double lambda_print = 0, lambda_cavity = 0;
@@ -387,8 +388,12 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
     } else {
       require(a.part == nullptr, "coarse-level applies produce no partial sums");
       bool split = false;
+      if (c->nine_max_n > 0 && a.n <= c->nine_max_n) {
+        k_apply_stencil_nine<T, D, R, MODE><<<dim3(ceil_div(a.N, NINE_NODES), c->B), NINE_THREADS, 0, s>>>(a);
+        split = true;
+      }
       if constexpr (R % 3 == 0) {
-        if (c->split_min_n > 0 && a.n >= c->split_min_n && a.n % ST_Z == 0) {
+        if (!split && c->split_min_n > 0 && a.n >= c->split_min_n && a.n % ST_Z == 0) {
           using G = SplitTile<T, D, R>;
           smem_attr(k_apply_stencil_split<T, D, R, MODE>, G::BYTES, c->dev);
           const int tiles = (a.n / ST_Z) * (a.n / ST_Y) * (a.n / ST_X);
@@ -1490,6 +1495,15 @@ int maple_set_stencil_split(maple_ctx* c, int min_n) {
     require(min_n >= 0, "min_n must be >= 0");
     drop_graphs(c);
     c->split_min_n = min_n;
+  });
+}
+
+int maple_set_stencil_nine(maple_ctx* c, int max_n) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(max_n >= 0, "max_n must be >= 0");
+    drop_graphs(c);
+    c->nine_max_n = max_n;
   });
 }
 

@@ -230,29 +230,33 @@ def test_multigrid_quality_iteration_counts(lib):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_split_stencil_matches_tile_kernel(lib, precision):
-    """Coarse levels applied by the split-offset kernel (every level with n >=
-    8) and by the shared-memory tile kernel (split off) solve alike: the same
-    C^H / kappa^H to summation-order accuracy and iteration counts within one,
-    on two different cells in one context."""
+def test_coarse_stencil_kernels_agree(lib, precision):
+    """The three coarse-level stencil kernels solve alike: the shared-memory
+    tile kernel (nine and split off), the split-offset kernel (every level with
+    n >= 8) and the nine-thread kernel (every level): the same C^H / kappa^H to
+    summation-order accuracy and iteration counts within one, on two different
+    cells in one context."""
     from maple_b200.core import HomogenizationContext
     r = 32
     rho = T(np.stack([simp(O.seed_density(s, r, 2.0, 0.25)).reshape(-1) for s in (0, 1)]))
     out = {}
-    for min_n in (0, 8):
+    for name, nine, split in (("tile", 0, 0), ("split", 0, 8), ("nine", 64, 0)):
         c = HomogenizationContext(r, ncells=2)
-        c.set_stencil_split(min_n)
+        c.set_stencil_nine(nine)
+        c.set_stencil_split(split)
         for phys in ("elastic", "thermal"):
             c.set_density(phys, rho, precision)
             info = c.solve(phys, precision, rtol=1e-10, maxit=300)
             assert (info.status & 1).all()
-            out[(min_n, phys)] = (c.homogenize(phys).cpu().numpy(), info.iters.copy())
+            out[(name, phys)] = (c.homogenize(phys).cpu().numpy(), info.iters.copy())
         c.close()
     for phys in ("elastic", "thermal"):
-        (H0, it0), (H1, it1) = out[(0, phys)], out[(8, phys)]
-        for b in range(2):
-            assert rel(H1[b], H0[b]) < (1e-12 if precision == "fp64" else 1e-9), (phys, b)
-        assert np.abs(it1.astype(int) - it0.astype(int)).max() <= 1, (phys, it0, it1)
+        H0, it0 = out[("tile", phys)]
+        for name in ("split", "nine"):
+            H1, it1 = out[(name, phys)]
+            for b in range(2):
+                assert rel(H1[b], H0[b]) < (1e-12 if precision == "fp64" else 1e-9), (name, phys, b)
+            assert np.abs(it1.astype(int) - it0.astype(int)).max() <= 1, (name, phys, it0, it1)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
