@@ -1751,8 +1751,8 @@ __global__ void k_precond_back(const float* __restrict__ z32, const double* __re
 }
 
 // A block per cell reduces that cell's partial sums (as k_reduce_partials) and
-// then its thread 0 applies the PCG scalar step that consumes them, one launch
-// instead of two:
+// then its first R lanes (one per load case) apply the PCG scalar step that
+// consumes them, one launch instead of two:
 //   ALPHA      alpha = rz / p.q, or freeze the column (done = 2) on a breakdown
 //              (p.q <= 0 or non-finite)
 //   CHECK      advance the iteration count (count), mark columns with
@@ -1788,12 +1788,14 @@ __global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* _
   block_sum_store<K>(v, out + (size_t)b * K);
   if constexpr (OP == RED_PLAIN) return;
   __syncthreads();
-  if (threadIdx.x != 0) return;
+  if (threadIdx.x >= 32) return;
+  // lane c < R handles load case c (the cell-level test is a warp vote)
   PcgScalars& s = op.s;
-  const int R = op.R;
+  const int R = op.R, c = threadIdx.x;
+  const bool col = c < R;
+  const int i = b * R + c;
   if constexpr (OP == RED_ALPHA) {
-    for (int c = 0; c < R; ++c) {
-      const int i = b * R + c;
+    if (col) {
       double a = 0.0;
       if (!s.done[i]) {
         const double pq = s.pq[i];
@@ -1807,36 +1809,38 @@ __global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* _
       s.alpha[i] = a;
     }
   } else if constexpr (OP == RED_CHECK) {
-    if (!s.cell_done[b]) {
-      if (op.count) s.iters[b] += 1;
-      int all = 1;
-      for (int c = 0; c < R; ++c) {
-        const int i = b * R + c;
-        if (!s.done[i] && s.rr[i] <= op.rtol2 * s.bnorm2[i]) s.done[i] = 1;
-        all &= (s.done[i] != 0);
+    const int was_done = s.cell_done[b];
+    int dn = 1;
+    if (col) {
+      dn = s.done[i];
+      if (!was_done && !dn && s.rr[i] <= op.rtol2 * s.bnorm2[i]) {
+        dn = 1;
+        s.done[i] = 1;
       }
-      if (all) s.cell_done[b] = 1;
     }
-    if (s.cell_done[b]) op.run[b] = 0;
-    if (op.scale)
-      for (int c = 0; c < R; ++c) {
-        const int i = b * R + c;
-        const double nrm = sqrt(fmax(s.rr[i], 0.0));
-        op.scale[i] = nrm > 0 ? 1.0 / nrm : 0.0;
-        op.inv[i] = nrm;
+    const bool all = __all_sync(0xffffffffu, dn != 0);
+    if (c == 0) {
+      if (!was_done) {
+        if (op.count) s.iters[b] += 1;
+        if (all) s.cell_done[b] = 1;
       }
+      if (was_done || all) op.run[b] = 0;
+    }
+    if (col && op.scale) {
+      const double nrm = sqrt(fmax(s.rr[i], 0.0));
+      op.scale[i] = nrm > 0 ? 1.0 / nrm : 0.0;
+      op.inv[i] = nrm;
+    }
   } else if constexpr (OP == RED_BETA) {
-    for (int c = 0; c < R; ++c) {
-      const int i = b * R + c;
+    if (col) {
       double be = 0.0;
       if (!s.done[i] && s.rz[i] != 0.0) be = s.rz_new[i] / s.rz[i];
       s.beta[i] = be;
       s.rz[i] = s.rz_new[i];
     }
   } else if constexpr (OP == RED_BETA_FLEX) {
-    const double* red = out + (size_t)b * K;
-    for (int c = 0; c < R; ++c) {
-      const int i = b * R + c;
+    if (col) {
+      const double* red = out + (size_t)b * K;
       const double rz_new = red[c], zq = red[R + c];
       double be = 0.0;
       if (!op.first && !s.done[i] && s.rz[i] != 0.0) be = -s.alpha[i] * zq / s.rz[i];
@@ -1844,7 +1848,7 @@ __global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* _
       s.rz[i] = rz_new;
     }
   } else if constexpr (OP == RED_SET_RZ) {
-    for (int c = 0; c < R; ++c) s.rz[b * R + c] = s.rz_new[b * R + c];
+    if (col) s.rz[i] = s.rz_new[i];
   }
 }
 
