@@ -550,11 +550,21 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
     KL(c, s, k_coarse_solve<T, R><<<dim3((ndof + 7) / 8, B), kThreads, 0, s>>>(p.Ainv, f, o.U[l][1], ndof, D, act));
     return;
   }
-  // levels 2 and deeper: their own degree (automatic: 3 on grids of 64^3 and
-  // up, where the extra cheap sweeps save more PCG iterations than they cost)
-  const int coarse_deg = c->cheb_degree_coarse > 0 ? c->cheb_degree_coarse
-                                                   : (c->r >= 64 ? std::max(3, c->cheb_degree) : c->cheb_degree);
-  const int deg = l >= 2 ? coarse_deg : c->cheb_degree;
+  // Chebyshev degree per level.  Automatic (cheb_degree_coarse == 0): coarse
+  // levels of at most 16^3 nodes take 4, other levels below level 1 take 3,
+  // where the extra cheap sweeps save more PCG iterations than they cost;
+  // levels 0 and 1 otherwise keep the common degree.  An explicit
+  // cheb_degree_coarse applies to levels 2 and deeper.
+  int deg = c->cheb_degree;
+  if (l >= 1) {
+    if (c->cheb_degree_coarse > 0) {
+      if (l >= 2) deg = c->cheb_degree_coarse;
+    } else if (c->n[l] <= 16) {
+      deg = std::max(4, deg);
+    } else if (l >= 2) {
+      deg = std::max(3, deg);
+    }
+  }
   int cur = 0;
   {
     ApplyArgs<T> a{};
