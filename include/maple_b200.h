@@ -69,8 +69,10 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
 int maple_ctx_destroy(maple_ctx* ctx);
 int maple_ctx_info(const maple_ctx* ctx, int* levels_out, int* coarsest_n_out, size_t* bytes_out);
 
-/* Solver tuning (defaults: chebyshev degree 2, interval ratio 10, 12 power
- * iterations, inner FP32 tolerance 1e-5, convergence check every iteration). */
+/* Solver tuning (defaults: chebyshev degree 1 on the fine level and on level 1
+ * (when it has more than 16^3 nodes; coarser levels: maple_set_coarse_degree),
+ * interval ratio 10, 12 power iterations, inner FP32 tolerance 1e-5,
+ * convergence check every iteration). */
 int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio, int power_iters, double inner_rtol,
                              int check_every);
 

@@ -54,7 +54,7 @@ class HomogenizationContext:
     """
 
     def __init__(self, r: int, ncells: int = 1, levels: int = 0, device=None, E: float = 1.0, nu: float = 0.3,
-                 kappa: float = 1.0, cheb_degree: int = 2, cheb_ratio: float = 10.0, power_iters: int = 12,
+                 kappa: float = 1.0, cheb_degree: int = 1, cheb_ratio: float = 10.0, power_iters: int = 12,
                  inner_rtol: float = 1e-5, check_every: int = 1):
         if not torch.cuda.is_available():
             raise RuntimeError("maple_b200 needs a CUDA device (there is no CPU path)")
@@ -92,7 +92,7 @@ class HomogenizationContext:
         _lib.check(self._lib.maple_ctx_info(self._h, None, None, C.byref(nb)))
         return nb.value
 
-    def set_options(self, cheb_degree=2, cheb_ratio=10.0, power_iters=12, inner_rtol=1e-5, check_every=1,
+    def set_options(self, cheb_degree=1, cheb_ratio=10.0, power_iters=12, inner_rtol=1e-5, check_every=1,
                     coarse_degree=0):
         """Smoother and solver settings; coarse_degree is the Chebyshev degree
         of multigrid levels 2 and deeper (0: automatic, 4 on coarse levels of

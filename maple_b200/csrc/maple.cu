@@ -221,7 +221,7 @@ struct maple_ctx {
   };
   std::vector<Rec> recs;
   // options
-  int cheb_degree = 2;
+  int cheb_degree = 1;         // levels 0 and 1 (level 1 of at most 16^3 nodes: see cheb_degree_coarse)
   int cheb_degree_coarse = 0;  // levels >= 2; 0: automatic
   double cheb_ratio = 10.0;
   int power_iters = 12;

@@ -207,15 +207,17 @@ def test_bad_arguments(lib):
 
 
 def test_multigrid_quality_iteration_counts(lib):
-    """A CPU emulation of this exact MG-PCG (Chebyshev-2 block-Jacobi smoothing,
-    Galerkin levels down to 4^3, dense FP64 coarsest) needs 25 elastic and 13
-    thermal iterations to rtol 1e-10 on this 32^3 density from zero; a defective
-    level (operator, transfer or smoother) shows up as extra iterations."""
+    """A CPU emulation of this exact MG-PCG (Chebyshev degree 2 block-Jacobi
+    smoothing on every level, Galerkin levels down to 4^3, dense FP64
+    coarsest) needs 25 elastic and 13 thermal iterations to rtol 1e-10 on this
+    32^3 density from zero; a defective level (operator, transfer or smoother)
+    shows up as extra iterations.  The context is set to that configuration."""
     from maple_b200.core import HomogenizationContext
     r = 32
     x = O.seed_density(0, r, 2.0, 0.25)
     rho = T(simp(x).reshape(1, -1))
     c = HomogenizationContext(r, ncells=1)
+    c.set_options(cheb_degree=2, coarse_degree=2)
     H = {}
     for prec in ("fp64", "mixed"):
         for phys, cap in (("elastic", 30), ("thermal", 16)):
