@@ -96,8 +96,8 @@ int maple_set_stencil_nine(maple_ctx* ctx, int max_n);
 
 /* Chebyshev degree of the smoother on multigrid levels 2 and deeper (level 0
  * and 1 use the degree of maple_set_solver_options).  0 (default): automatic,
- * 4 on coarse levels (level 1 included) of at most 16^3 nodes, 3 on the other
- * levels below level 1, never below the common degree. */
+ * 3 on every level below level 1 and on a level 1 of at most 16^3 nodes,
+ * never below the common degree. */
 int maple_set_coarse_degree(maple_ctx* ctx, int deg);
 
 /* Elastic and thermal solves of maple_oc_step at the same time (default on):

@@ -95,8 +95,8 @@ class HomogenizationContext:
     def set_options(self, cheb_degree=1, cheb_ratio=10.0, power_iters=12, inner_rtol=1e-5, check_every=1,
                     coarse_degree=0):
         """Smoother and solver settings; coarse_degree is the Chebyshev degree
-        of multigrid levels 2 and deeper (0: automatic, 4 on coarse levels of
-        at most 16^3 nodes, 3 on the other levels below level 1)."""
+        of multigrid levels 2 and deeper (0: automatic, 3 below level 1 and on
+        a level 1 of at most 16^3 nodes)."""
         _lib.check(self._lib.maple_set_solver_options(self._h, int(cheb_degree), float(cheb_ratio), int(power_iters),
                                                       float(inner_rtol), int(check_every)))
         _lib.check(self._lib.maple_set_coarse_degree(self._h, int(coarse_degree)))

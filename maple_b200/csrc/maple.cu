@@ -550,18 +550,16 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
     KL(c, s, k_coarse_solve<T, R><<<dim3((ndof + 7) / 8, B), kThreads, 0, s>>>(p.Ainv, f, o.U[l][1], ndof, D, act));
     return;
   }
-  // Chebyshev degree per level.  Automatic (cheb_degree_coarse == 0): coarse
-  // levels of at most 16^3 nodes take 4, other levels below level 1 take 3,
-  // where the extra cheap sweeps save more PCG iterations than they cost;
-  // levels 0 and 1 otherwise keep the common degree.  An explicit
+  // Chebyshev degree per level.  Automatic (cheb_degree_coarse == 0): 3 on
+  // every level below level 1 and on a level 1 of at most 16^3 nodes, where
+  // the extra cheap sweeps save more PCG iterations than they cost; the fine
+  // level and a larger level 1 keep the common degree.  An explicit
   // cheb_degree_coarse applies to levels 2 and deeper.
   int deg = c->cheb_degree;
   if (l >= 1) {
     if (c->cheb_degree_coarse > 0) {
       if (l >= 2) deg = c->cheb_degree_coarse;
-    } else if (c->n[l] <= 16) {
-      deg = std::max(4, deg);
-    } else if (l >= 2) {
+    } else if (l >= 2 || c->n[l] <= 16) {
       deg = std::max(3, deg);
     }
   }
