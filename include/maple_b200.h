@@ -94,6 +94,15 @@ int maple_set_stencil_split(maple_ctx* ctx, int min_n);
  * kernel on 32^3 and 64^3 levels.  Results differ only by FP summation order. */
 int maple_set_stencil_nine(maple_ctx* ctx, int max_n);
 
+/* FP32 V-cycles whose second-coarsest level has 8^3 nodes above a 4^3-node
+ * coarsest level run that level's smoothing, residual, restriction, the
+ * coarsest solve and the prolongation as one launch: a cluster of 8 CTAs per
+ * cell, each holding one x plane of the level in shared memory.  Default on;
+ * 0 runs the separate launches.  Same operand order, so the same results.
+ * The reference's V-cycle (utils/EBE_GMG.py:886-970, _v_cycle) recurses one
+ * level at a time; this changes only how the bottom two levels are launched. */
+int maple_set_tail_fused(maple_ctx* ctx, int enable);
+
 /* Chebyshev degree of the smoother on multigrid levels 2 and deeper (level 0
  * and 1 use the degree of maple_set_solver_options).  0 (default): automatic,
  * 3 on every level below level 1 and on a level 1 of at most 16^3 nodes,

@@ -167,6 +167,11 @@ class HomogenizationContext:
         stencil kernel (0: never)."""
         _lib.check(self._lib.maple_set_stencil_nine(self._h, int(max_n)))
 
+    def set_tail_fused(self, enable: bool = True):
+        """Run the FP32 8^3-node level and the 4^3-node coarsest solve of each
+        V-cycle as one cluster launch (default on; off: separate launches)."""
+        _lib.check(self._lib.maple_set_tail_fused(self._h, int(bool(enable))))
+
     def set_graphs(self, enable: bool):
         """Replay the PCG iteration body as a captured CUDA graph (default on)."""
         _lib.check(self._lib.maple_set_graphs(self._h, int(bool(enable))))

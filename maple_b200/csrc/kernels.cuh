@@ -9,6 +9,7 @@
 // The element stiffness of the fine level lives in __constant__ memory for a
 // voxel of edge 1; every kernel multiplies by the context's scale factor.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <utility>
@@ -56,6 +57,20 @@ __host__ __device__ constexpr int corner_y(int a) { return (a == 2 || a == 3 || 
 __host__ __device__ constexpr int corner_z(int a) { return a >= 4 ? 1 : 0; }
 
 __device__ __forceinline__ int wrapn(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// Explicitly rounded arithmetic (CUDA's _rn intrinsics): the compiler may not
+// contract or split these, so two kernels written with them round alike.  The
+// coarse-level nine-thread kernel, the grid transfers, the coarsest solve and
+// the fused V-cycle tail use them, and the tail reproduces the separate
+// launches bit for bit.
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 
 // ----------------------------------------------------------------------------
 // block reductions (deterministic: fixed shuffle tree + fixed warp order)
@@ -1000,7 +1015,7 @@ __global__ void __launch_bounds__(NINE_THREADS) k_apply_stencil_nine(ApplyArgs<T
           for (int j = 0; j < D; ++j) {
             const T uv = __ldg(ub + (size_t)(r * D + j) * NN + nb);
 #pragma unroll
-            for (int i = 0; i < D; ++i) acc[r][i] += sv[i][j] * uv;
+            for (int i = 0; i < D; ++i) acc[r][i] = fma_rn(sv[i][j], uv, acc[r][i]);
           }
       }
     }
@@ -1022,7 +1037,7 @@ __global__ void __launch_bounds__(NINE_THREADS) k_apply_stencil_nine(ApplyArgs<T
     T t = T(0);
     if constexpr (MODE != M_JAC0) {
 #pragma unroll
-      for (int k = 0; k < 9; ++k) t += red[k][r * D + i][tn];
+      for (int k = 0; k < 9; ++k) t = add_rn(t, red[k][r * D + i][tn]);
     }
     tot[i] = t;
   }
@@ -1032,7 +1047,7 @@ __global__ void __launch_bounds__(NINE_THREADS) k_apply_stencil_nine(ApplyArgs<T
     for (int i = 0; i < D; ++i) a.out[vo + i * NN] = tot[i];
   } else if constexpr (MODE == M_RES) {
 #pragma unroll
-    for (int i = 0; i < D; ++i) a.out[vo + i * NN] = a.f[vo + i * NN] - tot[i];
+    for (int i = 0; i < D; ++i) a.out[vo + i * NN] = sub_rn(a.f[vo + i * NN], tot[i]);
   } else {
     const double al = s_coef[0], be = s_coef[1];
     T Di[D][D];
@@ -1043,16 +1058,16 @@ __global__ void __launch_bounds__(NINE_THREADS) k_apply_stencil_nine(ApplyArgs<T
       for (int j = 0; j < D; ++j) Di[i][j] = __ldg(Dp + (size_t)(i * D + j) * NN);
     T res[D];
 #pragma unroll
-    for (int i = 0; i < D; ++i) res[i] = (MODE == M_JAC0) ? a.f[vo + i * NN] : a.f[vo + i * NN] - tot[i];
+    for (int i = 0; i < D; ++i) res[i] = (MODE == M_JAC0) ? a.f[vo + i * NN] : sub_rn(a.f[vo + i * NN], tot[i]);
 #pragma unroll
     for (int i = 0; i < D; ++i) {
-      T zz = 0;
+      T zz = mul_rn(Di[i][0], res[0]);
 #pragma unroll
-      for (int j = 0; j < D; ++j) zz += Di[i][j] * res[j];
-      T d = T(be) * zz;
-      if (MODE == M_CHEB && al != 0.0) d += T(al) * a.din[vo + i * NN];
+      for (int j = 1; j < D; ++j) zz = fma_rn(Di[i][j], res[j], zz);
+      T d = mul_rn(T(be), zz);
+      if (MODE == M_CHEB && al != 0.0) d = fma_rn(T(al), a.din[vo + i * NN], d);
       a.dout[vo + i * NN] = d;
-      a.out[vo + i * NN] = (MODE == M_JAC0) ? d : a.u[vo + i * NN] + d;
+      a.out[vo + i * NN] = (MODE == M_JAC0) ? d : add_rn(a.u[vo + i * NN], d);
     }
   }
 }
@@ -1153,7 +1168,7 @@ __global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ rc, int nc,
 #pragma unroll
       for (int dz = 0; dz < 3; ++dz) {
         const T w = T((dx != 1 ? 0.5 : 1.0) * (dy != 1 ? 0.5 : 1.0) * (dz != 1 ? 0.5 : 1.0));
-        acc += w * v[dz];
+        acc = fma_rn(w, v[dz], acc);
       }
     }
   rc[((size_t)b * K + k) * Nc + idx] = acc;
@@ -1196,13 +1211,13 @@ __global__ void k_prolong_add(const T* __restrict__ uc, T* __restrict__ uf, int 
         const T wz[2] = {T(rz ? 0.5 : 1.0), T(rz ? 0.5 : 0.0)};
         T a = 0;
 #pragma unroll
-        for (int o = 0; o < 8; ++o) a += (wx[(o >> 2) & 1] * wy[(o >> 1) & 1] * wz[o & 1]) * cv[o];
+        for (int o = 0; o < 8; ++o) a = fma_rn(wx[(o >> 2) & 1] * wy[(o >> 1) & 1] * wz[o & 1], cv[o], a);
         acc[rz] = a;
       }
       Pair<T>* dst = reinterpret_cast<Pair<T>*>(fb + ((size_t)(2 * X + rx) * nf + (2 * Y + ry)) * nf + 2 * Z);
       Pair<T> v = *dst;
-      v.lo += acc[0];
-      v.hi += acc[1];
+      v.lo = add_rn(v.lo, acc[0]);
+      v.hi = add_rn(v.hi, acc[1]);
       *dst = v;
     }
 }
@@ -1227,18 +1242,304 @@ __global__ void k_coarse_solve(const double* __restrict__ Ainv, const T* __restr
     const int node = col / D, c = col - node * D;
     const double a = A[col];
 #pragma unroll
-    for (int r = 0; r < R; ++r) acc[r] += a * (double)fb[(size_t)(r * D + c) * Nc + node];
+    for (int r = 0; r < R; ++r) acc[r] = fma_rn(a, (double)fb[(size_t)(r * D + c) * Nc + node], acc[r]);
   }
 #pragma unroll
   for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc[r] += __shfl_down_sync(0xffffffffu, acc[r], off);
+    for (int off = 16; off > 0; off >>= 1) acc[r] = add_rn(acc[r], __shfl_down_sync(0xffffffffu, acc[r], off));
   if (lane == 0) {
     const int node = row / D, c = row - node * D;
     T* ub = u + (size_t)b * ndof * R;
 #pragma unroll
     for (int r = 0; r < R; ++r) ub[(size_t)(r * D + c) * Nc + node] = (T)acc[r];
   }
+}
+
+// ----------------------------------------------------------------------------
+// Fused bottom of the V-cycle (FP32): the 8^3-node level above a 4^3-node
+// coarsest level -- Chebyshev pre-smoothing, residual, restriction, coarsest
+// solve, prolongation, post-smoothing -- in one launch, one cluster of 8 CTAs
+// per cell.  CTA p owns the x = p plane (64 nodes): its stencils, block
+// inverses, right-hand side, iterate, direction and residual stay in shared
+// memory for the whole cycle.  A sweep copies the x-1 and x+1 planes of the
+// iterate from the neighbouring CTAs' shared memory (distributed shared
+// memory) after a cluster barrier.  The iterate is double-buffered, so one
+// barrier per sweep suffices: a CTA overwrites a buffer two barriers after
+// its neighbours last copied it.  The restricted right-hand side and the
+// coarsest solution are written into every CTA of the cluster.  Every sum
+// keeps the operand order and the explicit rounding of the separate kernels
+// (k_apply_stencil_nine, k_restrict, k_coarse_solve, k_prolong_add), so the
+// cycle reproduces their launch sequence bit for bit.  Cluster barriers are
+// hardware barriers:
+// no thread of a cluster returns before the last one, and a cell's cluster
+// either runs all of them or (inactive cell) none.
+// ----------------------------------------------------------------------------
+constexpr int TAIL_N = 8, TAIL_NC = 4, TAIL_CTAS = 8, TAIL_P = 64, TAIL_THREADS = 9 * TAIL_P;
+constexpr int kTailMaxDegree = 8;
+
+struct TailArgs {
+  const float* S;      // level stencils [B][27][D*D][512]
+  const float* Dinv;   // block-diagonal inverses [B][D*D][512]
+  const float* f;      // level right-hand side [B][R][D][512]
+  float* u;            // resulting iterate [B][R][D][512]
+  const double* Ainv;  // coarsest inverse [B][64 D][64 D]
+  const double* hi;    // per-cell Chebyshev upper bound of the level
+  double ratio;        // Chebyshev interval ratio
+  int deg;             // Chebyshev steps per smoothing, 1..kTailMaxDegree
+  const int* active;   // per-cell flag (nullable)
+};
+
+template <int D, int R>
+struct TailSmem {
+  static constexpr int RD = R * D, P = TAIL_P, NCN = TAIL_NC * TAIL_NC * TAIL_NC;
+  static constexpr int S = 0;                    // [27 D D][P]
+  static constexpr int DI = S + 27 * D * D * P;  // [D D][P]
+  static constexpr int F = DI + D * D * P;       // [RD][P]
+  static constexpr int U = F + RD * P;           // [2][RD][P] iterate
+  static constexpr int H = U + 2 * RD * P;       // [2][RD][P] planes x-1, x+1
+  static constexpr int DD = H + 2 * RD * P;      // [RD][P] Chebyshev direction
+  static constexpr int RS = DD + RD * P;         // [RD][P] residual
+  static constexpr int RED = RS + RD * P;        // [9][RD][P] partial sums
+  static constexpr int FC = RED + 9 * RD * P;    // [RD][NCN] coarsest right-hand side
+  static constexpr int UC = FC + RD * NCN;       // [RD][NCN] coarsest solution
+  static constexpr int FLOATS = UC + RD * NCN;
+  static constexpr size_t BYTES = (size_t)FLOATS * sizeof(float) + 2 * kTailMaxDegree * sizeof(double);
+  static_assert(FLOATS % 4 == 0 && U % 4 == 0 && H % 4 == 0 && (RD * P) % 4 == 0, "16-byte aligned planes");
+};
+
+template <int D, int R>
+__global__ void __cluster_dims__(TAIL_CTAS, 1, 1) __launch_bounds__(TAIL_THREADS) k_tail_cycle(TailArgs a) {
+  namespace cg = cooperative_groups;
+  using L = TailSmem<D, R>;
+  constexpr int RD = R * D, P = TAIL_P, n = TAIL_N, nc = TAIL_NC, N = n * n * n, NCN = L::NCN, ndof = NCN * D;
+  constexpr int V4 = RD * P / 4;  // float4 per plane of the iterate
+  extern __shared__ __align__(16) float tsm[];
+  float* sS = tsm + L::S;
+  float* sDi = tsm + L::DI;
+  float* sF = tsm + L::F;
+  float* sU = tsm + L::U;
+  float* sH = tsm + L::H;
+  float* sDd = tsm + L::DD;
+  float* sRs = tsm + L::RS;
+  float* red = tsm + L::RED;
+  float* sFc = tsm + L::FC;
+  float* sUc = tsm + L::UC;
+  double* s_al = reinterpret_cast<double*>(tsm + L::FLOATS);
+  double* s_be = s_al + kTailMaxDegree;
+
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;  // the whole cluster belongs to cell b
+  cg::cluster_group cl = cg::this_cluster();
+  const int px = (int)cl.block_rank();
+  const int tid = threadIdx.x;
+  const int tn = tid % P, q = tid / P;  // node of the plane, (x, y) offset pair 3 ox + oy
+  const int deg = a.deg;
+
+  auto stage = [&](float* dst, const float* src, int rows) {
+    for (int t = tid; t < rows * (P / 4); t += TAIL_THREADS) {
+      const int k = t / (P / 4), m = t - k * (P / 4);
+      reinterpret_cast<float4*>(dst)[t] = __ldg(reinterpret_cast<const float4*>(src + (size_t)k * N) + m);
+    }
+  };
+  stage(sS, a.S + (size_t)b * 27 * D * D * N + px * P, 27 * D * D);
+  stage(sDi, a.Dinv + (size_t)b * D * D * N + px * P, D * D);
+  stage(sF, a.f + (size_t)b * RD * N + px * P, RD);
+  if (tid < deg) cheb_coeffs(a.hi[b], a.ratio, tid, s_al[tid], s_be[tid]);
+  __syncthreads();
+
+  // copy the x-1 and x+1 planes of iterate buffer `cur` from the neighbours
+  auto halo = [&](int cur) {
+    const float4* lo = reinterpret_cast<const float4*>(cl.map_shared_rank(sU + cur * RD * P, (px + TAIL_CTAS - 1) % TAIL_CTAS));
+    const float4* hi = reinterpret_cast<const float4*>(cl.map_shared_rank(sU + cur * RD * P, (px + 1) % TAIL_CTAS));
+    float4* h = reinterpret_cast<float4*>(sH);
+    for (int t = tid; t < 2 * V4; t += TAIL_THREADS) h[t] = t < V4 ? lo[t] : hi[t - V4];
+  };
+  // thread (tn, q): the 3 z offsets of offset pair q for all load cases
+  auto partials = [&](const float* own) {
+    const int ox = q / 3, oy = q % 3;
+    const float* plane = ox == 1 ? own : sH + (ox >> 1) * RD * P;
+    const int y = tn / n, z = tn % n;
+    const int yy = wrapn(y + oy - 1, n);
+    float acc[R][D];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < D; ++i) acc[r][i] = 0.f;
+#pragma unroll
+    for (int oz = 0; oz < 3; ++oz) {
+      const int o = q * 3 + oz;
+      const int nb = yy * n + wrapn(z + oz - 1, n);
+      float sv[D][D];
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) sv[i][j] = sS[((o * D + i) * D + j) * P + tn];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          const float uv = plane[(r * D + j) * P + nb];
+#pragma unroll
+          for (int i = 0; i < D; ++i) acc[r][i] = fma_rn(sv[i][j], uv, acc[r][i]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int i = 0; i < D; ++i) red[(q * RD + r * D + i) * P + tn] = acc[r][i];
+  };
+  // thread (tn, r = q < R): residual, or one Chebyshev step from buffer cur
+  // into buffer 1 - cur (the last one also to global memory)
+  auto finish = [&](int mode, int st, int cur, bool last) {
+    if (q >= R) return;
+    const int r = q;
+    float tot[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      float t = 0.f;
+      if (mode != M_JAC0) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) t = add_rn(t, red[(k * RD + r * D + i) * P + tn]);
+      }
+      tot[i] = t;
+    }
+    if (mode == M_RES) {
+#pragma unroll
+      for (int i = 0; i < D; ++i) sRs[(r * D + i) * P + tn] = sub_rn(sF[(r * D + i) * P + tn], tot[i]);
+      return;
+    }
+    const double al = s_al[st], be = s_be[st];
+    float Di[D][D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) Di[i][j] = sDi[(i * D + j) * P + tn];
+    float res[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) res[i] = mode == M_JAC0 ? sF[(r * D + i) * P + tn] : sub_rn(sF[(r * D + i) * P + tn], tot[i]);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      float zz = mul_rn(Di[i][0], res[0]);
+#pragma unroll
+      for (int j = 1; j < D; ++j) zz = fma_rn(Di[i][j], res[j], zz);
+      const int e = (r * D + i) * P + tn;
+      float d = mul_rn(float(be), zz);
+      if (mode == M_CHEB && al != 0.0) d = fma_rn(float(al), sDd[e], d);
+      sDd[e] = d;
+      const float un = mode == M_JAC0 ? d : add_rn(sU[cur * RD * P + e], d);
+      sU[(1 - cur) * RD * P + e] = un;
+      if (last) a.u[((size_t)b * RD + r * D + i) * N + px * P + tn] = un;
+    }
+  };
+  auto sweep = [&](int mode, int st, int cur, bool last) {
+    cl.sync();  // every plane's buffer `cur` is complete
+    halo(cur);
+    __syncthreads();
+    partials(sU + cur * RD * P);
+    __syncthreads();
+    finish(mode, st, cur, last);
+  };
+
+  // pre-smoothing: a step from the zero iterate into buffer 0, then deg - 1 steps
+  finish(M_JAC0, 0, 1, false);
+  int cur = 0;
+  for (int st = 1; st < deg; ++st, cur ^= 1) sweep(M_CHEB, st, cur, false);
+  sweep(M_RES, 0, cur, false);
+  cl.sync();  // every plane's residual is complete
+
+  // restriction: CTA p forms half of coarse plane X = p / 2, written to every CTA
+  {
+    constexpr int HALF = 8 * RD;  // 16 (Y, Z) x RD entries per coarse plane
+    const int X = px >> 1;
+    const int fx[3] = {wrapn(2 * X - 1, n), 2 * X, 2 * X + 1};
+    for (int t = tid; t < HALF; t += TAIL_THREADS) {
+      const int e = (px & 1) * HALF + t;
+      const int k = e / 16, Y = (e % 16) / nc, Z = e % nc;
+      const int fy[3] = {wrapn(2 * Y - 1, n), 2 * Y, 2 * Y + 1};
+      const int fz[3] = {wrapn(2 * Z - 1, n), 2 * Z, 2 * Z + 1};
+      float acc = 0.f;
+#pragma unroll
+      for (int dx = 0; dx < 3; ++dx) {
+        const float* pl = cl.map_shared_rank(sRs, fx[dx]) + k * P;
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy) {
+          const float* row = pl + fy[dy] * n;
+          const float v[3] = {row[fz[0]], row[fz[1]], row[fz[2]]};
+#pragma unroll
+          for (int dz = 0; dz < 3; ++dz) {
+            const float w = float((dx != 1 ? 0.5 : 1.0) * (dy != 1 ? 0.5 : 1.0) * (dz != 1 ? 0.5 : 1.0));
+            acc = fma_rn(w, v[dz], acc);
+          }
+        }
+      }
+      const int ci = k * NCN + (X * nc + Y) * nc + Z;
+#pragma unroll
+      for (int rk = 0; rk < TAIL_CTAS; ++rk) cl.map_shared_rank(sFc, rk)[ci] = acc;
+    }
+  }
+  cl.sync();
+
+  // coarsest solve u_c = Ainv f_c: CTA p takes rows [p ndof/8, (p+1) ndof/8),
+  // one warp per row, lanes over the columns (FP64 accumulation)
+  {
+    constexpr int ROWS = ndof / TAIL_CTAS;
+    static_assert(ndof % TAIL_CTAS == 0, "rows split evenly over the cluster");
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int rr = warp; rr < ROWS; rr += TAIL_THREADS / 32) {
+      const int row = px * ROWS + rr;
+      const double* A = a.Ainv + ((size_t)b * ndof + row) * ndof;
+      double acc[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r] = 0;
+      for (int col = lane; col < ndof; col += 32) {
+        const int node = col / D, c = col - node * D;
+        const double av = __ldg(A + col);
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = fma_rn(av, (double)sFc[(r * D + c) * NCN + node], acc[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc[r] = add_rn(acc[r], __shfl_down_sync(0xffffffffu, acc[r], off));
+      if (lane == 0) {
+        const int node = row / D, c = row - node * D;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float v = (float)acc[r];
+#pragma unroll
+          for (int rk = 0; rk < TAIL_CTAS; ++rk) cl.map_shared_rank(sUc, rk)[(r * D + c) * NCN + node] = v;
+        }
+      }
+    }
+  }
+  cl.sync();
+
+  // prolongation into this plane of buffer cur
+  {
+    const int X = px >> 1, rx = px & 1;
+    const int cx[2] = {X, (X + 1) % nc};
+    const float wx[2] = {rx ? 0.5f : 1.0f, rx ? 0.5f : 0.0f};
+    for (int t = tid; t < RD * P; t += TAIL_THREADS) {
+      const int k = t / P, m = t - k * P, y = m / n, z = m % n;
+      const int Y = y >> 1, ry = y & 1, Z = z >> 1, rz = z & 1;
+      const int cy[2] = {Y, (Y + 1) % nc};
+      const int cz[2] = {Z, (Z + 1) % nc};
+      const float wy[2] = {ry ? 0.5f : 1.0f, ry ? 0.5f : 0.0f};
+      const float wz[2] = {rz ? 0.5f : 1.0f, rz ? 0.5f : 0.0f};
+      float s = 0.f;
+#pragma unroll
+      for (int o = 0; o < 8; ++o) {
+        const float cv = sUc[k * NCN + (cx[(o >> 2) & 1] * nc + cy[(o >> 1) & 1]) * nc + cz[o & 1]];
+        s = fma_rn(wx[(o >> 2) & 1] * wy[(o >> 1) & 1] * wz[o & 1], cv, s);
+      }
+      sU[cur * RD * P + t] = add_rn(sU[cur * RD * P + t], s);
+    }
+  }
+
+  // post-smoothing; the last step also writes the iterate to global memory
+  for (int st = 0; st < deg; ++st, cur ^= 1) sweep(M_CHEB, st, cur, st == deg - 1);
+  cl.sync();  // no CTA leaves while a neighbour may still read its shared memory
 }
 
 // ----------------------------------------------------------------------------

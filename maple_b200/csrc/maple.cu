@@ -17,6 +17,7 @@
 #include <exception>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -200,6 +201,7 @@ struct maple_ctx {
   bool concurrent = true;  // elastic and thermal solves of an OC step on two streams
   int split_min_n = 32;    // coarse levels with n >= this (n % 8 == 0) use k_apply_stencil_split; 0: never
   int nine_max_n = 64;     // coarse levels with n <= this use k_apply_stencil_nine; 0: never
+  bool tail_fused = true;  // FP32 8^3 level + 4^3 coarsest solve as one cluster launch (k_tail_cycle)
   int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
   // manufacturability penalties of the OC objective (maple_set_penalties)
   double lambda_print = 0, lambda_cavity = 0;
@@ -541,6 +543,36 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s, co
 // ---------------------------------------------------------------------------
 // V-cycle (symmetric: Chebyshev pre/post, exact FP64 coarsest solve)
 // ---------------------------------------------------------------------------
+// Whether the FP32 V-cycle runs level l (8^3 nodes, above the 4^3-node
+// coarsest level) as one k_tail_cycle launch.  The first call per (D, R,
+// device) opts the kernel in to its shared memory and asks the occupancy
+// calculator whether one 8-CTA cluster of it fits on the device.
+template <int D, int R>
+static bool tail_fused_ok(maple_ctx* c, int l, int deg) {
+  if (!c->tail_fused || l < 1 || l != c->L - 2 || c->n[l] != TAIL_N || c->n[l + 1] != TAIL_NC ||
+      deg < 1 || deg > kTailMaxDegree)
+    return false;
+  static std::mutex mu;
+  static std::map<int, bool> fits;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = fits.find(c->dev);
+  if (it != fits.end()) return it->second;
+  const size_t bytes = TailSmem<D, R>::BYTES;
+  bool ok = cudaFuncSetAttribute(k_tail_cycle<D, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
+            cudaSuccess;
+  if (ok) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(TAIL_CTAS, 1, 1);
+    cfg.blockDim = dim3(TAIL_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = bytes;
+    int clusters = 0;
+    ok = cudaOccupancyMaxActiveClusters(&clusters, k_tail_cycle<D, R>, &cfg) == cudaSuccess && clusters > 0;
+  }
+  (void)cudaGetLastError();  // a refused query leaves the separate launches in use
+  fits[c->dev] = ok;
+  return ok;
+}
+
 template <typename T, int D, int R>
 static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const int* act, double* rz_part,
                    cudaStream_t s) {
@@ -561,6 +593,15 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
       if (l >= 2) deg = c->cheb_degree_coarse;
     } else if (l >= 2 || c->n[l] <= 16) {
       deg = std::max(3, deg);
+    }
+  }
+  if constexpr (std::is_same<T, float>::value) {
+    if (tail_fused_ok<D, R>(c, l, deg)) {
+      // smoothing, residual, restriction, coarsest solve and prolongation of
+      // this level in one launch; the result lands in U[l][1] as below
+      TailArgs ta{o.S[l], o.Dinv[l], f, o.U[l][1], p.Ainv, o.hi[l], c->cheb_ratio, deg, act};
+      KL(c, s, k_tail_cycle<D, R><<<dim3(TAIL_CTAS, c->B), TAIL_THREADS, TailSmem<D, R>::BYTES, s>>>(ta));
+      return;
     }
   }
   int cur = 0;
@@ -1512,6 +1553,14 @@ int maple_set_stencil_nine(maple_ctx* c, int max_n) {
     require(max_n >= 0, "max_n must be >= 0");
     drop_graphs(c);
     c->nine_max_n = max_n;
+  });
+}
+
+int maple_set_tail_fused(maple_ctx* c, int enable) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    drop_graphs(c);
+    c->tail_fused = enable != 0;
   });
 }
 

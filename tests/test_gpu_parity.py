@@ -261,6 +261,43 @@ def test_coarse_stencil_kernels_agree(lib, precision):
             assert np.abs(it1.astype(int) - it0.astype(int)).max() <= 1, (name, phys, it0, it1)
 
 
+@pytest.mark.parametrize("r", [16, 32])
+@pytest.mark.parametrize("coarse_degree", [0, 1, 5])
+def test_fused_tail_matches_separate_launches(lib, r, coarse_degree):
+    """The one-launch bottom of the FP32 V-cycle (8^3 level, restriction, 4^3
+    coarsest solve, prolongation; a cluster of 8 CTAs per cell) computes what
+    the separate launches compute, bit for bit: the same solutions, C^H /
+    kappa^H and iteration counts, with an inactive cell between two active
+    ones.  r = 16 puts the fused level at level 1, r = 32 at level 2;
+    Chebyshev degrees 1 and 5 cover the smoothing loops' ends."""
+    from maple_b200.core import HomogenizationContext
+    rho = T(np.stack([simp(O.seed_density(s, r, 2.0, 0.3)).reshape(-1) for s in (3, 4, 5)]))
+    out = {}
+    for fused in (False, True):
+        c = HomogenizationContext(r, ncells=3)
+        c.set_options(coarse_degree=coarse_degree)
+        c.set_tail_fused(fused)
+        c.set_active([1, 0, 1])
+        c.profile(True)
+        for phys in ("elastic", "thermal"):
+            c.set_density(phys, rho, "mixed")
+            info = c.solve(phys, "mixed", rtol=1e-10, maxit=300)
+            assert (info.status[[0, 2]] & 1).all()
+            out[(fused, phys)] = (c.homogenize(phys).cpu().numpy(), info.iters.copy(),
+                                  c.solution(phys)[[0, 2]].clone())
+        names = c.profile_read()
+        ran = any(k.startswith("k_tail_cycle") for k in names)
+        assert ran == fused, sorted(names)
+        c.close()
+    for phys in ("elastic", "thermal"):
+        H0, it0, u0 = out[(False, phys)]
+        H1, it1, u1 = out[(True, phys)]
+        assert torch.equal(u0, u1), (phys, (u0 - u1).abs().max().item())
+        for b in (0, 2):
+            assert np.array_equal(H1[b], H0[b]), (phys, b)
+            assert it1[b] == it0[b], (phys, b, it0, it1)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_graph_replay_matches_eager(lib, precision):
     """The captured PCG iteration replays the same launches: identical results
