@@ -221,7 +221,10 @@ def run_maple(args, rank, world, local_rank):
     prof = ctx.profile_read()
     ctx.profile(False)
     peak, peak_kind = measured_peaks()
-    top_name, top = max(prof.items(), key=lambda kv: kv[1]["total_ms"]) if prof else (None, None)
+    # the kernel class with the most device time among those with known
+    # algorithmic bytes (grid transfers and PCG vector updates carry none)
+    known = [kv for kv in prof.items() if kv[1]["bytes_per_launch"] > 0]
+    top_name, top = max(known, key=lambda kv: kv[1]["total_ms"]) if known else (None, None)
     roofline = None
     if top:
         avg_s = top["total_ms"] / top["launches"] / 1000.0

@@ -1971,6 +1971,32 @@ __global__ void k_pcg_direction(T* __restrict__ p, const T* __restrict__ z, cons
   }
 }
 
+// Mixed-precision direction update from the FP32 preconditioner output:
+// p = z + beta p with z = ||r|| z32 formed on the fly (the same explicitly
+// rounded product as k_precond_back), so z is never stored in FP64.  FIRST:
+// p = z (the first direction; p may hold anything before).
+template <int R, int D, bool FIRST>
+__global__ void k_pcg_direction_f32(double* __restrict__ p, const float* __restrict__ z32,
+                                    const double* __restrict__ inv, const double* __restrict__ beta, int N,
+                                    const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= N) return;
+  const size_t o = (size_t)b * N * R * D + idx;
+#pragma unroll
+  for (int c = 0; c < R; ++c) {
+    const double s = inv[b * R + c];
+    const double be = FIRST ? 0.0 : beta[b * R + c];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const size_t j = o + (size_t)(c * D + i) * N;
+      const double zv = mul_rn(s, (double)z32[j]);
+      p[j] = FIRST ? zv : fma_rn(be, p[j], zv);
+    }
+  }
+}
+
 // per-(cell,rhs) PCG scalar logic, one thread per (cell, rhs)
 struct PcgScalars {
   double* rz;      // r.z
@@ -2024,9 +2050,10 @@ __global__ void k_add_f32_scaled(double* __restrict__ dst, const float* __restri
   }
 }
 
-// z = inv * z32 (FP64) with partial dots r.z and (optionally) q.z
+// partial dots r.z and (optionally) q.z of z = inv * z32, formed in FP64 and
+// not stored (k_pcg_direction_f32 forms it again for the direction update)
 template <int R, int D>
-__global__ void k_precond_back(const float* __restrict__ z32, const double* __restrict__ inv, double* __restrict__ z,
+__global__ void k_precond_back(const float* __restrict__ z32, const double* __restrict__ inv,
                                const double* __restrict__ r, const double* __restrict__ q, double* __restrict__ part,
                                int N, const int* active) {
   const int b = blockIdx.y;
@@ -2041,8 +2068,7 @@ __global__ void k_precond_back(const float* __restrict__ z32, const double* __re
 #pragma unroll
       for (int i = 0; i < D; ++i) {
         const size_t j = o + (size_t)(c * D + i) * N;
-        const double zv = s * (double)z32[j];
-        z[j] = zv;
+        const double zv = mul_rn(s, (double)z32[j]);
         v[c] += r[j] * zv;
         if (q) v[R + c] += q[j] * zv;
       }

@@ -121,7 +121,7 @@ struct Phys {
   double* F64 = nullptr;         // RHS [B][N][R][D]
   double* u64 = nullptr;         // solution
   double* r64 = nullptr;         // residual (FP64)
-  double *p64 = nullptr, *q64 = nullptr, *z64 = nullptr;  // mixed-precision PCG vectors
+  double *p64 = nullptr, *q64 = nullptr;  // mixed-precision PCG vectors (z stays FP32)
   double* energy = nullptr;      // [B][N][R][R]
   double* H = nullptr;           // [B][R][R]
   Ops<double> o64;
@@ -418,7 +418,15 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
       static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
       const std::string nm = std::string("k_apply_stencil<") + (sizeof(T) == 8 ? "f64," : "f32,") +
                              std::to_string(D) + "," + std::to_string(R) + "," + mname[MODE] + ">@L" + std::to_string(l);
-      prof_end(c, s, nm.c_str(), 0);
+      // algorithmic bytes per node: the stencil (not for JAC0), the block
+      // inverse (CHEB, JAC0, POWER), each vector read or written once
+      const double es = sizeof(T), dd = D * D, rd = R * D;
+      const double per_node = MODE == M_MV     ? (27 * dd + 2 * rd) * es
+                              : MODE == M_RES  ? (27 * dd + 3 * rd) * es
+                              : MODE == M_CHEB ? (27 * dd + dd + 5 * rd) * es
+                              : MODE == M_JAC0 ? (dd + 3 * rd) * es
+                                               : (27 * dd + dd + 2 * D) * es;
+      prof_end(c, s, nm.c_str(), (double)c->B * a.N * per_node);
     }
   }
 }
@@ -600,7 +608,16 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
       // smoothing, residual, restriction, coarsest solve and prolongation of
       // this level in one launch; the result lands in U[l][1] as below
       TailArgs ta{o.S[l], o.Dinv[l], f, o.U[l][1], p.Ainv, o.hi[l], c->cheb_ratio, deg, act};
-      KL(c, s, k_tail_cycle<D, R><<<dim3(TAIL_CTAS, c->B), TAIL_THREADS, TailSmem<D, R>::BYTES, s>>>(ta));
+      prof_begin(c, s);
+      k_tail_cycle<D, R><<<dim3(TAIL_CTAS, c->B), TAIL_THREADS, TailSmem<D, R>::BYTES, s>>>(ta);
+      CKL();
+      if (prof_on(c)) {
+        // algorithmic bytes per cell: the level's stencils, block inverses,
+        // right-hand side and result once, and the coarsest inverse
+        const double N = nodes(TAIL_N), ndof = nodes(TAIL_NC) * D;
+        const double cell = (27.0 * D * D + D * D + 2.0 * R * D) * N * sizeof(float) + ndof * ndof * sizeof(double);
+        prof_end(c, s, ("k_tail_cycle<" + std::to_string(D) + "," + std::to_string(R) + ">").c_str(), c->B * cell);
+      }
       return;
     }
   }
@@ -810,7 +827,7 @@ static void precondition_f32(maple_ctx* c, Phys& p, const double* r, const doubl
   Ops<float>& o = p.o32;
   KL(c, s, k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, LN(c).o_scale, N, run));
   vcycle<float, D, R>(c, p, o, 0, o.r, run, nullptr, s);
-  KL(c, s, k_precond_back<R, D><<<g2(N, B), kThreads, 0, s>>>(o.U[0][1], LN(c).o_inv, p.z64, r, q, LN(c).part, N, run));
+  KL(c, s, k_precond_back<R, D><<<g2(N, B), kThreads, 0, s>>>(o.U[0][1], LN(c).o_inv, r, q, LN(c).part, N, run));
   reduce_op<2 * R, RED_BETA_FLEX>(c, LN(c).part, nblk(N), LN(c).red, op, s);
 }
 
@@ -823,7 +840,8 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
   const unsigned nb = nblk(N), nbf = (unsigned)fine_tiles(c->n[0]);
   PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
   Ops<double>& o64 = p.o64;
-  double *r = p.r64, *pv = p.p64, *q = p.q64, *z = p.z64;
+  double *r = p.r64, *pv = p.p64, *q = p.q64;
+  const float* z32 = p.o32.U[0][1];  // preconditioner output; z = ||r|| z32 is formed where it is used
   KL(c, s, k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, nullptr, sc.done, sc.cell_done, sc.run, sc.iters, B, R));
   const int* run = sc.run;
   if (x_zero) {
@@ -852,7 +870,7 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
   reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op0, s);
   if (all_done(c, sc.cell_done, run, s)) return;
   precondition_f32<D, R>(c, p, r, nullptr, run, op0, s);
-  CK(cudaMemcpyAsync(pv, z, vbytes, cudaMemcpyDeviceToDevice, s));
+  KL(c, s, k_pcg_direction_f32<R, D, true><<<g2(N, B), kThreads, 0, s>>>(pv, z32, LN(c).o_inv, nullptr, N, run));
   op.count = 1;
   auto body = [&](cudaStream_t st) {
     {
@@ -866,7 +884,7 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
     KL(c, st, k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, st>>>(x, r, pv, q, sc.alpha, LN(c).part, N, run));
     reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op, st);
     precondition_f32<D, R>(c, p, r, q, run, op, st);
-    KL(c, st, k_pcg_direction<double, R, D><<<g2(N, B), kThreads, 0, st>>>(pv, z, sc.beta, N, run));
+    KL(c, st, k_pcg_direction_f32<R, D, false><<<g2(N, B), kThreads, 0, st>>>(pv, z32, LN(c).o_inv, sc.beta, N, run));
   };
   run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_MIXED], rtol, maxit, body, s);
 }
@@ -1031,7 +1049,6 @@ static void ensure_prec(maple_ctx* c, int phys, int prec) {
       const size_t n = (size_t)c->B * nodes(c->n[0]) * p.R * p.D;
       p.p64 = dnew<double>(c, n);
       p.q64 = dnew<double>(c, n);
-      p.z64 = dnew<double>(c, n);
     }
   }
 }
