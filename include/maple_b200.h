@@ -103,6 +103,14 @@ int maple_set_stencil_nine(maple_ctx* ctx, int max_n);
  * level at a time; this changes only how the bottom two levels are launched. */
 int maple_set_tail_fused(maple_ctx* ctx, int enable);
 
+/* Launch the coarse-level stencil sweeps, the grid transfers and the fused
+ * V-cycle tail with programmatic dependent launch: each may start, and load
+ * the stencils built before the solve, while the previous kernel in the
+ * stream drains; it reads the previous kernel's output only after
+ * griddepcontrol.wait.  Default on; 0 launches them plainly.  Results are
+ * identical either way. */
+int maple_set_pdl(maple_ctx* ctx, int enable);
+
 /* Chebyshev degree of the smoother on multigrid levels 2 and deeper (level 0
  * and 1 use the degree of maple_set_solver_options).  0 (default): automatic,
  * 3 on every level below level 1 and on a level 1 of at most 16^3 nodes,

@@ -172,6 +172,11 @@ class HomogenizationContext:
         V-cycle as one cluster launch (default on; off: separate launches)."""
         _lib.check(self._lib.maple_set_tail_fused(self._h, int(bool(enable))))
 
+    def set_pdl(self, enable: bool = True):
+        """Launch the coarse-level sweeps, grid transfers and the fused V-cycle
+        tail with programmatic dependent launch (default on)."""
+        _lib.check(self._lib.maple_set_pdl(self._h, int(bool(enable))))
+
     def set_graphs(self, enable: bool):
         """Replay the PCG iteration body as a captured CUDA graph (default on)."""
         _lib.check(self._lib.maple_set_graphs(self._h, int(bool(enable))))

@@ -58,6 +58,21 @@ __host__ __device__ constexpr int corner_z(int a) { return a >= 4 ? 1 : 0; }
 
 __device__ __forceinline__ int wrapn(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// Programmatic dependent launch (sm_90+).  A kernel launched with the
+// programmatic-serialization attribute may start while its predecessor in the
+// stream still runs; griddep_wait() returns once every prerequisite grid has
+// completed and its memory operations are visible.  Kernels that use these
+// call griddep_wait() in every thread before reading anything an earlier
+// kernel of the solve wrote, and before returning, so completion stays
+// transitive along the stream; only data written before the solve (stencils,
+// block inverses, bounds) is read before it, and data written during the
+// solve is read with coherent (not read-only-path) loads.  griddep_launch(),
+// called after the wait, lets the next launch begin its own prologue, so at
+// most two kernels of a stream overlap.  Without the attribute both are
+// no-ops.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Explicitly rounded arithmetic (CUDA's _rn intrinsics): the compiler may not
 // contract or split these, so two kernels written with them round alike.  The
 // coarse-level nine-thread kernel, the grid transfers, the coarsest solve and
@@ -976,12 +991,16 @@ __global__ void __launch_bounds__(ST_THREADS) k_apply_stencil_split(ApplyArgs<T>
 constexpr int NINE_NODES = 32;
 constexpr int NINE_THREADS = 9 * NINE_NODES;
 
-template <typename T, int D, int R, int MODE>
+template <typename T, int D, int R, int MODE, bool PDL = false>
 __global__ void __launch_bounds__(NINE_THREADS) k_apply_stencil_nine(ApplyArgs<T> a) {
   constexpr int RD = R * D;
   static_assert(R <= 9, "one finishing thread per load case");
   __shared__ T red[9][RD][NINE_NODES];
   const int b = blockIdx.y;
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
   if (a.active && !a.active[b]) return;
   const int n = a.n, N = a.N;
   const size_t NN = (size_t)N;
@@ -998,7 +1017,7 @@ __global__ void __launch_bounds__(NINE_THREADS) k_apply_stencil_nine(ApplyArgs<T
     if (valid) {
       const int ox = q / 3, oy = q % 3;
       const int xx = wrapn(x + ox - 1, n), yy = wrapn(y + oy - 1, n);
-      const T* __restrict__ ub = a.u + (size_t)b * RD * NN;
+      const T* ub = a.u + (size_t)b * RD * NN;
       const T* __restrict__ S = a.S + (size_t)b * 27 * D * D * NN + id;
 #pragma unroll
       for (int oz = 0; oz < 3; ++oz) {
@@ -1013,7 +1032,9 @@ __global__ void __launch_bounds__(NINE_THREADS) k_apply_stencil_nine(ApplyArgs<T
         for (int r = 0; r < R; ++r)
 #pragma unroll
           for (int j = 0; j < D; ++j) {
-            const T uv = __ldg(ub + (size_t)(r * D + j) * NN + nb);
+            // under PDL the iterate was written during this grid's lifetime:
+            // a coherent load, not the read-only path
+            const T uv = PDL ? ub[(size_t)(r * D + j) * NN + nb] : __ldg(ub + (size_t)(r * D + j) * NN + nb);
 #pragma unroll
             for (int i = 0; i < D; ++i) acc[r][i] = fma_rn(sv[i][j], uv, acc[r][i]);
           }
@@ -1143,16 +1164,20 @@ struct alignas(2 * sizeof(T)) Pair {
 // ----------------------------------------------------------------------------
 // rc = P^T rf : coarse node gathers its 27 fine neighbours 2X+d, weight
 // prod(1-|d|/2).  One thread per (coarse node, component).
-template <typename T, int K>
-__global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ rc, int nc, const int* active) {
+template <typename T, int K, bool PDL = false>
+__global__ void k_restrict(const T* rf, T* rc, int nc, const int* active) {
   const int b = blockIdx.y;
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
   if (active && !active[b]) return;
   const int Nc = nc * nc * nc, nf = 2 * nc, Nf = Nc * 8;
   const int t = blockIdx.x * kThreads + threadIdx.x;
   if (t >= Nc * K) return;
   const int k = t / Nc, idx = t - k * Nc;
   const int Z = idx % nc, Y = (idx / nc) % nc, X = idx / (nc * nc);
-  const T* __restrict__ base = rf + ((size_t)b * K + k) * Nf;
+  const T* base = rf + ((size_t)b * K + k) * Nf;
   const int fx[3] = {wrapn(2 * X - 1, nf), 2 * X, 2 * X + 1};
   const int fy[3] = {wrapn(2 * Y - 1, nf), 2 * Y, 2 * Y + 1};
   const int fz[3] = {wrapn(2 * Z - 1, nf), 2 * Z, 2 * Z + 1};
@@ -1164,7 +1189,7 @@ __global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ rc, int nc,
       // the z-run 2Z-1, 2Z, 2Z+1 of this (x, y) row: one scalar and one pair load
       const T* row = base + ((size_t)fx[dx] * nf + fy[dy]) * nf;
       const Pair<T> p = *reinterpret_cast<const Pair<T>*>(row + fz[1]);
-      const T v[3] = {__ldg(row + fz[0]), p.lo, p.hi};
+      const T v[3] = {PDL ? row[fz[0]] : __ldg(row + fz[0]), p.lo, p.hi};
 #pragma unroll
       for (int dz = 0; dz < 3; ++dz) {
         const T w = T((dx != 1 ? 0.5 : 1.0) * (dy != 1 ? 0.5 : 1.0) * (dz != 1 ? 0.5 : 1.0));
@@ -1180,9 +1205,13 @@ __global__ void k_restrict(const T* __restrict__ rf, T* __restrict__ rc, int nc,
 // fine coordinate that is even takes weight 1 from its own coarse node and 0
 // from the next one, an odd one 1/2 from each; each fine value is the sum over
 // the 8 corners in (x, y, z) order of weight x value.
-template <typename T, int K>
-__global__ void k_prolong_add(const T* __restrict__ uc, T* __restrict__ uf, int nc, const int* active) {
+template <typename T, int K, bool PDL = false>
+__global__ void k_prolong_add(const T* uc, T* uf, int nc, const int* active) {
   const int b = blockIdx.y;
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
   if (active && !active[b]) return;
   const int nf = 2 * nc, Nc = nc * nc * nc;
   const size_t Nf = (size_t)Nc * 8;
@@ -1190,15 +1219,16 @@ __global__ void k_prolong_add(const T* __restrict__ uc, T* __restrict__ uf, int 
   if (t >= Nc * K) return;
   const int k = t / Nc, idx = t - k * Nc;
   const int Z = idx % nc, Y = (idx / nc) % nc, X = idx / (nc * nc);
-  const T* __restrict__ base = uc + ((size_t)b * K + k) * Nc;
+  const T* base = uc + ((size_t)b * K + k) * Nc;
   const int cx[2] = {X, X + 1 == nc ? 0 : X + 1};
   const int cy[2] = {Y, Y + 1 == nc ? 0 : Y + 1};
   const int cz[2] = {Z, Z + 1 == nc ? 0 : Z + 1};
   T cv[8];
 #pragma unroll
   for (int o = 0; o < 8; ++o)
-    cv[o] = __ldg(base + ((size_t)cx[(o >> 2) & 1] * nc + cy[(o >> 1) & 1]) * nc + cz[o & 1]);
-  T* __restrict__ fb = uf + ((size_t)b * K + k) * Nf;
+    cv[o] = PDL ? base[((size_t)cx[(o >> 2) & 1] * nc + cy[(o >> 1) & 1]) * nc + cz[o & 1]]
+                : __ldg(base + ((size_t)cx[(o >> 2) & 1] * nc + cy[(o >> 1) & 1]) * nc + cz[o & 1]);
+  T* fb = uf + ((size_t)b * K + k) * Nf;
 #pragma unroll
   for (int rx = 0; rx < 2; ++rx)
 #pragma unroll
@@ -1308,7 +1338,7 @@ struct TailSmem {
   static_assert(FLOATS % 4 == 0 && U % 4 == 0 && H % 4 == 0 && (RD * P) % 4 == 0, "16-byte aligned planes");
 };
 
-template <int D, int R>
+template <int D, int R, bool PDL = false>
 __global__ void __cluster_dims__(TAIL_CTAS, 1, 1) __launch_bounds__(TAIL_THREADS) k_tail_cycle(TailArgs a) {
   namespace cg = cooperative_groups;
   using L = TailSmem<D, R>;
@@ -1329,23 +1359,34 @@ __global__ void __cluster_dims__(TAIL_CTAS, 1, 1) __launch_bounds__(TAIL_THREADS
   double* s_be = s_al + kTailMaxDegree;
 
   const int b = blockIdx.y;
-  if (a.active && !a.active[b]) return;  // the whole cluster belongs to cell b
+  // the whole cluster belongs to cell b: an inactive cell's CTAs all return
+  // (under PDL only after the wait, which also covers the flag itself)
+  if (!PDL && a.active && !a.active[b]) return;
   cg::cluster_group cl = cg::this_cluster();
   const int px = (int)cl.block_rank();
   const int tid = threadIdx.x;
   const int tn = tid % P, q = tid / P;  // node of the plane, (x, y) offset pair 3 ox + oy
   const int deg = a.deg;
 
-  auto stage = [&](float* dst, const float* src, int rows) {
+  // stencils, inverses and bounds were built before the solve (under PDL they
+  // are staged before the wait); the right-hand side comes from the previous
+  // launch and is read coherently under PDL
+  auto stage = [&](float* dst, const float* src, int rows, bool coherent) {
     for (int t = tid; t < rows * (P / 4); t += TAIL_THREADS) {
       const int k = t / (P / 4), m = t - k * (P / 4);
-      reinterpret_cast<float4*>(dst)[t] = __ldg(reinterpret_cast<const float4*>(src + (size_t)k * N) + m);
+      const float4* g = reinterpret_cast<const float4*>(src + (size_t)k * N) + m;
+      reinterpret_cast<float4*>(dst)[t] = coherent ? *g : __ldg(g);
     }
   };
-  stage(sS, a.S + (size_t)b * 27 * D * D * N + px * P, 27 * D * D);
-  stage(sDi, a.Dinv + (size_t)b * D * D * N + px * P, D * D);
-  stage(sF, a.f + (size_t)b * RD * N + px * P, RD);
+  stage(sS, a.S + (size_t)b * 27 * D * D * N + px * P, 27 * D * D, false);
+  stage(sDi, a.Dinv + (size_t)b * D * D * N + px * P, D * D, false);
   if (tid < deg) cheb_coeffs(a.hi[b], a.ratio, tid, s_al[tid], s_be[tid]);
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+    if (a.active && !a.active[b]) return;
+  }
+  stage(sF, a.f + (size_t)b * RD * N + px * P, RD, PDL);
   __syncthreads();
 
   // copy the x-1 and x+1 planes of iterate buffer `cur` from the neighbours

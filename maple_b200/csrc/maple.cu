@@ -202,6 +202,7 @@ struct maple_ctx {
   int split_min_n = 32;    // coarse levels with n >= this (n % 8 == 0) use k_apply_stencil_split; 0: never
   int nine_max_n = 64;     // coarse levels with n <= this use k_apply_stencil_nine; 0: never
   bool tail_fused = true;  // FP32 8^3 level + 4^3 coarsest solve as one cluster launch (k_tail_cycle)
+  bool pdl = true;         // coarse-level launches with programmatic dependent launch
   int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
   // manufacturability penalties of the OC objective (maple_set_penalties)
   double lambda_print = 0, lambda_cavity = 0;
@@ -248,6 +249,8 @@ static void prof_end(maple_ctx* c, cudaStream_t s, const char* text, double byte
   const size_t cut = name.find("<<<");
   if (cut != std::string::npos) name = name.substr(0, cut);
   name.erase(std::remove(name.begin(), name.end(), ' '), name.end());
+  const std::string pdl = "launch_pdl(";  // launch_pdl(kernel<...>, grid, ...)
+  if (name.rfind(pdl, 0) == 0) name = name.substr(pdl.size(), name.find(",gt,") - pdl.size());
   c->recs.push_back({name, bytes, c->ev_used});
   c->ev_used += 2;
 }
@@ -286,6 +289,35 @@ static void smem_attr(K* kernel, size_t bytes, int dev) {
   if (g_attr_done.count(key)) return;
   CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   g_attr_done.insert(key);
+}
+
+// Programmatic dependent launch pays where a launch is a wave or two of
+// blocks: its prologue overlaps the previous kernel's drain.  On large grids
+// the per-block griddepcontrol.wait costs more than it saves (256 cells of
+// 32^3: +15% step time with it on every coarse launch), so only launches of
+// at most kPdlMaxBlocks blocks (the fused tail: one wave of clusters) use the
+// PDL instantiation of their kernel; the others launch the plain one.
+constexpr size_t kPdlMaxBlocks = 8 * 148;
+static bool use_pdl(const maple_ctx* c, dim3 grid, size_t max_blocks = kPdlMaxBlocks) {
+  return c->pdl && (size_t)grid.x * grid.y * grid.z <= max_blocks;
+}
+
+// Launch the PDL instantiation of a kernel (it calls griddep_wait before
+// reading its predecessors' output) with the programmatic-serialization
+// attribute: it may start while the previous kernel in the stream drains.
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, kernel, args...));  // counted by the caller's CKL
 }
 
 static inline unsigned nblk(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
@@ -391,7 +423,11 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
       require(a.part == nullptr, "coarse-level applies produce no partial sums");
       bool split = false;
       if (c->nine_max_n > 0 && a.n <= c->nine_max_n) {
-        k_apply_stencil_nine<T, D, R, MODE><<<dim3(ceil_div(a.N, NINE_NODES), c->B), NINE_THREADS, 0, s>>>(a);
+        const dim3 grid(ceil_div(a.N, NINE_NODES), c->B);
+        if (use_pdl(c, grid))
+          launch_pdl(k_apply_stencil_nine<T, D, R, MODE, true>, grid, dim3(NINE_THREADS), 0, s, a);
+        else
+          k_apply_stencil_nine<T, D, R, MODE><<<grid, NINE_THREADS, 0, s>>>(a);
         split = true;
       }
       if constexpr (R % 3 == 0) {
@@ -567,7 +603,9 @@ static bool tail_fused_ok(maple_ctx* c, int l, int deg) {
   if (it != fits.end()) return it->second;
   const size_t bytes = TailSmem<D, R>::BYTES;
   bool ok = cudaFuncSetAttribute(k_tail_cycle<D, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
-            cudaSuccess;
+                cudaSuccess &&
+            cudaFuncSetAttribute(k_tail_cycle<D, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
+                cudaSuccess;
   if (ok) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(TAIL_CTAS, 1, 1);
@@ -609,7 +647,11 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
       // this level in one launch; the result lands in U[l][1] as below
       TailArgs ta{o.S[l], o.Dinv[l], f, o.U[l][1], p.Ainv, o.hi[l], c->cheb_ratio, deg, act};
       prof_begin(c, s);
-      k_tail_cycle<D, R><<<dim3(TAIL_CTAS, c->B), TAIL_THREADS, TailSmem<D, R>::BYTES, s>>>(ta);
+      const dim3 grid(TAIL_CTAS, c->B);
+      if (use_pdl(c, grid, 148))
+        launch_pdl(k_tail_cycle<D, R, true>, grid, dim3(TAIL_THREADS), TailSmem<D, R>::BYTES, s, ta);
+      else
+        k_tail_cycle<D, R><<<grid, TAIL_THREADS, TailSmem<D, R>::BYTES, s>>>(ta);
       CKL();
       if (prof_on(c)) {
         // algorithmic bytes per cell: the level's stencils, block inverses,
@@ -653,10 +695,17 @@ static void vcycle(maple_ctx* c, Phys& p, Ops<T>& o, int l, const T* f, const in
     apply<T, D, R, M_RES>(c, p, o, l, a, act, s);
   }
   const int nc = c->n[l + 1];
-  KL(c, s, k_restrict<T, R * D><<<g2((size_t)nodes(nc) * R * D, B), kThreads, 0, s>>>(o.Res[l], o.F[l + 1], nc, act));
+  const dim3 gt = g2((size_t)nodes(nc) * R * D, B);
+  if (use_pdl(c, gt))
+    KL(c, s, launch_pdl(k_restrict<T, R * D, true>, gt, dim3(kThreads), 0, s, (const T*)o.Res[l], o.F[l + 1], nc, act));
+  else
+    KL(c, s, k_restrict<T, R * D><<<gt, kThreads, 0, s>>>(o.Res[l], o.F[l + 1], nc, act));
   vcycle<T, D, R>(c, p, o, l + 1, o.F[l + 1], act, nullptr, s);
-  KL(c, s, k_prolong_add<T, R * D><<<g2((size_t)nodes(nc) * R * D, B), kThreads, 0, s>>>(o.U[l + 1][1],
-                                                                                             o.U[l][cur], nc, act));
+  if (use_pdl(c, gt))
+    KL(c, s, launch_pdl(k_prolong_add<T, R * D, true>, gt, dim3(kThreads), 0, s, (const T*)o.U[l + 1][1], o.U[l][cur],
+                        nc, act));
+  else
+    KL(c, s, k_prolong_add<T, R * D><<<gt, kThreads, 0, s>>>(o.U[l + 1][1], o.U[l][cur], nc, act));
   for (int st = 0; st < deg; ++st) {
     ApplyArgs<T> a{};
     a.f = f;
@@ -1570,6 +1619,14 @@ int maple_set_stencil_nine(maple_ctx* c, int max_n) {
     require(max_n >= 0, "max_n must be >= 0");
     drop_graphs(c);
     c->nine_max_n = max_n;
+  });
+}
+
+int maple_set_pdl(maple_ctx* c, int enable) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    drop_graphs(c);
+    c->pdl = enable != 0;
   });
 }
 

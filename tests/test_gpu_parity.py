@@ -299,6 +299,36 @@ def test_fused_tail_matches_separate_launches(lib, r, coarse_degree):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("r", [16, 32])
+def test_pdl_matches_plain_launches(lib, precision, r):
+    """Programmatic dependent launch of the coarse sweeps, transfers and the
+    fused tail changes only when kernels start: solutions and iteration counts
+    are bit-identical to plain launches, for graph replays and eager runs,
+    with an inactive cell."""
+    from maple_b200.core import HomogenizationContext
+    rho = T(np.stack([simp(O.seed_density(s, r, 2.0, 0.3)).reshape(-1) for s in (6, 7, 8)]))
+    out = {}
+    for pdl in (False, True):
+        for graphs in (False, True):
+            c = HomogenizationContext(r, ncells=3)
+            c.set_pdl(pdl)
+            c.set_graphs(graphs)
+            c.set_active([1, 0, 1])
+            for phys in ("elastic", "thermal"):
+                c.set_density(phys, rho, precision)
+                info = c.solve(phys, precision, rtol=1e-10, maxit=300)
+                assert (info.status[[0, 2]] & 1).all()
+                out[(pdl, graphs, phys)] = (info.iters.copy(), c.solution(phys)[[0, 2]].clone())
+            c.close()
+    for phys in ("elastic", "thermal"):
+        it0, u0 = out[(False, False, phys)]
+        for key in ((False, True), (True, False), (True, True)):
+            it1, u1 = out[key + (phys,)]
+            assert torch.equal(u0, u1), (phys, key, (u0 - u1).abs().max().item())
+            assert np.array_equal(it0[[0, 2]], it1[[0, 2]]), (phys, key)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_graph_replay_matches_eager(lib, precision):
     """The captured PCG iteration replays the same launches: identical results
     and iteration counts with graphs on and off."""
