@@ -750,10 +750,6 @@ __global__ void k_init_flags(const int* active, const int* outer_run, int* done,
 // iterations ran.  The body is captured once into a CUDA graph per
 // (physics, precision, rtol) and replayed; the convergence flags are read back
 // after every replay (cells that converged skip all further work on device).
-// Runs the PCG iteration body until every active cell has converged or maxit
-// iterations ran.  The body is captured once into a CUDA graph per
-// (physics, precision, rtol) and replayed; the convergence flags are read back
-// after every replay (cells that converged skip all further work on device).
 // The first iteration of a solve always runs eagerly, which also performs the
 // one-time kernel attribute setup outside of any capture.
 template <typename Body>
