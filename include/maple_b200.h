@@ -230,7 +230,10 @@ int maple_box_filter(int r, int ncells, int k, const double* in, double* out, ma
 
 /* OC update: 60 bisection steps on lambda in [1e-12, 1e6] per cell
  * (main_IHD_v3.py:362-380).  volfrac [B] device, xnew [B][N]; stats [B][2]
- * = (max|dx|, mean|dx|) (nullable). */
+ * = (max|dx|, mean|dx|) (nullable).  The bisection runs in one cooperative
+ * launch whose blocks meet at grid barriers; every wait there is bounded.  The
+ * call waits for its stream and returns MAPLE_E_TIMEOUT if a wait ran out
+ * (xnew and stats are then incomplete); the context stays usable. */
 int maple_oc_update(maple_ctx* ctx, const double* x, const double* dJdx, const double* volfrac, double move, double xmin,
                     double* xnew, double* stats, maple_stream_t stream);
 
@@ -241,11 +244,24 @@ int maple_oc_update(maple_ctx* ctx, const double* x, const double* dJdx, const d
  * device array per GPU, held until the process exits.  N = elements per cell;
  * at most 8191 cells per call with stats given (5460 with stats NULL); larger
  * batches are rejected.  The first call on a device looks up the array's
- * address; make it before any stream capture.  Calls share the array, so calls
- * whose kernels overlap on the GPU race.  This entry point has no counterpart
- * in the reference. */
+ * address and keeps it for the life of the process: make that first call
+ * before any stream capture, and do not use the library across a reset of the
+ * device (cudaDeviceReset), which would leave the kept address stale.  Calls
+ * share the array, so calls whose kernels overlap on the GPU race.  Like
+ * maple_oc_update it waits for its stream at the end and returns
+ * MAPLE_E_TIMEOUT if a grid-barrier wait ran out.  This entry point has no
+ * counterpart in the reference. */
 int maple_oc_update_noalloc(int N, int ncells, const double* x, const double* dJdx, const double* volfrac, double move,
                             double xmin, double* xnew, double* stats, maple_stream_t stream);
+
+/* Testing aid for the bounded waits of the OC update: later OC updates
+ * launched from the calling thread (maple_oc_update, maple_oc_update_noalloc,
+ * maple_oc_step) give up a grid-barrier wait after max_polls polls (0 = the
+ * default bound of 2^24 polls) and wait for phantom_blocks more blocks than
+ * they launch, which never arrive.  With phantom_blocks > 0 every such call
+ * returns MAPLE_E_TIMEOUT after its bounded waits; (0, 0) restores the normal
+ * behaviour.  No counterpart in the reference. */
+int maple_test_wait_limit(long long max_polls, int phantom_blocks);
 
 /* One full OC iteration on device for every active cell (main_IHD_v3.py:
  * 620-716 with symmetry "none" and no manufacturing penalties): SIMP map,
@@ -254,7 +270,8 @@ int maple_oc_update_noalloc(int N, int ncells, const double* x, const double* dJ
  * analytic sensitivities, k^3 sensitivity filter and OC update.
  * x [B][N] in, x_next [B][N] out; weights [B][3] and volfrac [B] device.
  * Per-cell outputs (device, nullable): J [B], terms [B][3] (E, G, trace k),
- * CH [B][6][6], kappa [B][3][3], stats [B][2] (max|dx|, mean|dx|). */
+ * CH [B][6][6], kappa [B][3][3], stats [B][2] (max|dx|, mean|dx|).  Waits
+ * for its stream at the end; MAPLE_E_TIMEOUT as for maple_oc_update. */
 int maple_oc_step(maple_ctx* ctx, const double* x, const double* weights, const double* volfrac, double penal,
                   double rho_min, double move, double xmin, int filter_k, int precision, double rtol, int maxit,
                   int warm, double* x_next, double* J, double* terms, double* CH, double* kappa, double* stats,

@@ -13,6 +13,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libmaple_b200.so")
 
 MAPLE_OK = 0
+MAPLE_E_BADARG, MAPLE_E_CUDA, MAPLE_E_NOT_CONVERGED, MAPLE_E_BREAKDOWN, MAPLE_E_TIMEOUT, MAPLE_E_NOMEM = 1, 2, 3, 4, 5, 6
 ELASTIC, THERMAL = 0, 1
 FP64, MIXED = 0, 1
 CELL_CONVERGED, CELL_BREAKDOWN, CELL_MAXIT, CELL_FALLBACK = 1, 2, 4, 8
@@ -60,6 +61,7 @@ SIGNATURES = {
     "maple_box_filter": (_I, [_I, _I, _I, _P, _P, _P]),
     "maple_oc_update": (_I, [_P, _P, _P, _P, _D, _D, _P, _P, _P]),
     "maple_oc_update_noalloc": (_I, [_I, _I, _P, _P, _P, _D, _D, _P, _P, _P]),
+    "maple_test_wait_limit": (_I, [_L, _I]),
     "maple_launch_count": (C.c_ulonglong, []),
     "maple_profile_enable": (_I, [_P, _I, _I]),
     "maple_profile_read": (_I, [_P, C.c_char_p, _I]),

@@ -2550,33 +2550,53 @@ __global__ void k_box_filter(const double* __restrict__ in, double* __restrict__
   out[(size_t)b * N + e] = s / (double)(kf * kf * kf);
 }
 
-// Bounded grid barrier for co-resident (cooperatively launched) blocks: a spin
-// that gives up after `limit` polls and raises *err instead of hanging.
-__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err) {
+// Bounded grid barrier for co-resident (cooperatively launched) blocks.  A
+// block whose wait runs past `limit` polls, or that finds another block has
+// already given up, raises *err and returns false; the caller then returns at
+// once, so a barrier that cannot complete ends the kernel instead of hanging it
+// (and every later barrier of the launch gives up immediately).  `nblocks` is
+// the number of blocks expected to arrive.
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, unsigned nblocks, int* err,
+                                             long long limit) {
+  __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = gen;
-    const unsigned g = *vgen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(count, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(count, 0u);
-      __threadfence();
-      atomicAdd(gen, 1u);
+    volatile int* verr = err;
+    int ok = 1;
+    if (*verr) {
+      ok = 0;
     } else {
-      long polls = 0;
-      while (*vgen == g) {
-        if (++polls > (1L << 26)) {  // a few seconds at most, then report
-          atomicExch(err, 1);
-          break;
+      const unsigned g = *vgen;
+      __threadfence();
+      const unsigned arrived = atomicAdd(count, 1u);
+      if (arrived == nblocks - 1) {
+        atomicExch(count, 0u);
+        __threadfence();
+        atomicAdd(gen, 1u);
+      } else {
+        long long polls = 0;
+        while (*vgen == g) {
+          if (++polls > limit || *verr) {
+            atomicExch(err, 1);
+            ok = 0;
+            break;
+          }
+          if (polls > 4096) __nanosleep(32);
         }
-        if (polls > 4096) __nanosleep(32);
       }
+      __threadfence();
     }
-    __threadfence();
+    s_ok = ok;
   }
   __syncthreads();
+  return s_ok != 0;
 }
+
+// default poll limit of grid_barrier: the OC kernel's blocks arrive within
+// microseconds of each other; 2^24 polls (several seconds) only bound a wait
+// that can never end
+constexpr long long kBarrierPolls = 1LL << 24;
 
 // OC update with 60 bisection steps on lambda in [1e-12, 1e6]
 // (main_IHD_v3.py:362-380).  Grid (G, B): G co-resident blocks per cell.
@@ -2592,13 +2612,15 @@ struct OcArgs {
   double* stats;      // [B][2]: dx_max, dx_mean
   double* lam_out;    // [B]
   unsigned* bar;      // [2] barrier counter, generation
-  int* err;
+  int* err;           // set when a grid barrier gave up (the kernel then returns early)
   const int* active;
+  long long poll_limit;  // grid_barrier poll limit
+  unsigned phantom;      // extra blocks the barrier waits for (0; more only to test the bounded wait)
 };
 
 __global__ void __launch_bounds__(kThreads) k_oc_update(OcArgs a) {
   const int G = gridDim.x, g = blockIdx.x, b = blockIdx.y;
-  const unsigned nblocks = gridDim.x * gridDim.y;
+  const unsigned nblocks = gridDim.x * gridDim.y + a.phantom;
   const bool act = !a.active || a.active[b];
   const int N = a.N;
   const int chunk = (N + G - 1) / G;
@@ -2622,7 +2644,7 @@ __global__ void __launch_bounds__(kThreads) k_oc_update(OcArgs a) {
     }
     double v[1] = {s};
     block_sum_store<1>(v, a.part + ((size_t)b * 4 + (it & 1)) * G + g);
-    grid_barrier(a.bar, a.bar + 1, nblocks, a.err);
+    if (!grid_barrier(a.bar, a.bar + 1, nblocks, a.err, a.poll_limit)) return;
     if (act) {
       __shared__ double s_tot;
       if (threadIdx.x < 32) {
@@ -2663,7 +2685,7 @@ __global__ void __launch_bounds__(kThreads) k_oc_update(OcArgs a) {
   __syncthreads();
   block_sum_store<1>(v, a.part + ((size_t)b * 4 + 2) * G + g);
   if (threadIdx.x == 0) a.part[((size_t)b * 4 + 3) * G + g] = dmax;
-  grid_barrier(a.bar, a.bar + 1, nblocks, a.err);
+  if (!grid_barrier(a.bar, a.bar + 1, nblocks, a.err, a.poll_limit)) return;
   if (act && g == 0 && threadIdx.x == 0) {
     double m = 0, t = 0;
     for (int k = 0; k < G; ++k) {

@@ -187,7 +187,8 @@ struct maple_ctx {
   double *x_sym = nullptr, *dJdx = nullptr, *dJf = nullptr, *Jv = nullptr, *terms = nullptr, *G3 = nullptr,
          *G1 = nullptr, *stats = nullptr, *ocpart = nullptr, *ocvf = nullptr;
   unsigned* bar = nullptr;
-  int* err = nullptr;
+  int* err = nullptr;             // device: an OC grid barrier gave up
+  int* h_err = nullptr;           // pinned host copy of err
   int oc_G = 0;
   // captured PCG iteration bodies: [physics][precision]
   struct GraphEntry {
@@ -1139,6 +1140,12 @@ static void homogenize(maple_ctx* c, int phys, cudaStream_t s) {
   p.energies = true;
 }
 
+// Poll limit and phantom block count of the OC kernel's grid barriers for
+// launches from this thread (maple_test_wait_limit); the defaults are the
+// normal bound and no phantom blocks.
+static thread_local long long tl_wait_polls = kBarrierPolls;
+static thread_local unsigned tl_wait_phantom = 0;
+
 static void oc_update(maple_ctx* c, const double* x, const double* dJ, const double* vf, double move, double xmin,
                       double* xnew, double* stats, cudaStream_t s) {
   const int N = nodes(c->n[0]);
@@ -1150,6 +1157,9 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
   // cells per launch and blocks per cell
   const int want_G = std::max(1, std::min(sms, (N + 4 * kThreads - 1) / (4 * kThreads)));
   int cells_per_launch = std::max(1, std::min(c->B, maxres / want_G));
+  // cleared once per update: a launch that finds it set (an earlier launch's
+  // barrier gave up) returns at its first barrier
+  CK(cudaMemsetAsync(c->err, 0, sizeof(int), s));
   for (int c0 = 0; c0 < c->B; c0 += cells_per_launch) {
     const int nb = std::min(cells_per_launch, c->B - c0);
     const int G = std::max(1, std::min(want_G, maxres / nb));
@@ -1167,6 +1177,8 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
     a.bar = c->bar;
     a.err = c->err;
     a.active = c->active ? c->active + c0 : nullptr;
+    a.poll_limit = tl_wait_polls;
+    a.phantom = tl_wait_phantom;
     CK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned), s));
     void* args[] = {&a};
     prof_begin(c, s);
@@ -1174,6 +1186,16 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
     g_launches.fetch_add(1);
     prof_end(c, s, "k_oc_update", 0);
   }
+}
+
+// Waits for the stream and raises MAPLE_E_TIMEOUT if a grid barrier of the
+// last oc_update gave up (its outputs are then incomplete).
+static void check_oc_barrier(maple_ctx* c, cudaStream_t s) {
+  CK(cudaMemcpyAsync(c->h_err, c->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (*c->h_err)
+    throw Failure{MAPLE_E_TIMEOUT, "OC update: a grid barrier wait ran out (not every block of the cooperative "
+                                   "launch arrived); x_next and the statistics are incomplete"};
 }
 
 // ---------------------------------------------------------------------------
@@ -1366,10 +1388,12 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
       c->bar = dnew<unsigned>(c, 2);
       c->err = dnew<int>(c, 1);
       CK(cudaMemset(c->err, 0, sizeof(int)));
+      CK(cudaMallocHost(&c->h_err, sizeof(int)));
     } catch (...) {
       for (void* p : c->allocs) cudaFree(p);
       for (Lane& L : c->lanes)
         if (L.h_flags) cudaFreeHost(L.h_flags);
+      if (c->h_err) cudaFreeHost(c->h_err);
       delete c;
       throw;
     }
@@ -1443,6 +1467,7 @@ int maple_ctx_destroy(maple_ctx* c) {
       if (L.h_flags) cudaFreeHost(L.h_flags);
     }
     if (c->pen_work) cudaFree(c->pen_work);
+    if (c->h_err) cudaFreeHost(c->h_err);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     if (c->aux_fork) cudaEventDestroy(c->aux_fork);
     if (c->aux_join) cudaEventDestroy(c->aux_join);
@@ -1827,6 +1852,7 @@ int maple_oc_update(maple_ctx* c, const double* x, const double* dJdx, const dou
     require(c != nullptr && x && dJdx && vf && xnew, "NULL argument");
     require(xnew != x, "xnew must not alias x");
     oc_update(c, x, dJdx, vf, move, xmin, xnew, stats, S(s));
+    check_oc_barrier(c, S(s));
   });
 }
 
@@ -1855,6 +1881,9 @@ int maple_oc_update_noalloc(int N, int ncells, const double* x, const double* dJ
     const int cells_per_launch = std::max(1, std::min(ncells, maxres / want_G));
     unsigned* bar = reinterpret_cast<unsigned*>(scratch + kNoAllocScratch - kTail);
     int* err = reinterpret_cast<int*>(scratch + kNoAllocScratch - kTail + 2);
+    // the error word is cleared once per call and read after its last launch;
+    // the barrier words before every launch
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
     for (int c0 = 0; c0 < ncells; c0 += cells_per_launch) {
       const int nb = std::min(cells_per_launch, ncells - c0);
       const int stats_words = stats ? 0 : 2 * nb;
@@ -1873,11 +1902,21 @@ int maple_oc_update_noalloc(int N, int ncells, const double* x, const double* dJ
       a.bar = bar;
       a.err = err;
       a.active = nullptr;
-      CK(cudaMemsetAsync(scratch + kNoAllocScratch - kTail, 0, kTail * sizeof(double), st));
+      a.poll_limit = tl_wait_polls;
+      a.phantom = tl_wait_phantom;
+      CK(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st));
       void* args[] = {&a};
       CK(cudaLaunchCooperativeKernel((void*)k_oc_update, dim3(G, nb), dim3(kThreads), args, 0, st));
       g_launches.fetch_add(1);
     }
+    // a barrier that gave up is reported here: copying the word into host
+    // (stack) memory waits for the stream
+    int h_err = 0;
+    CK(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h_err)
+      throw Failure{MAPLE_E_TIMEOUT, "maple_oc_update_noalloc: a grid barrier wait ran out (not every block of the "
+                                     "cooperative launch arrived); xnew and the statistics are incomplete"};
   });
 }
 
@@ -2013,6 +2052,15 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
     if (stats) CK(cudaMemcpyAsync(stats, c->stats, 2 * B * sizeof(double), cudaMemcpyDeviceToDevice, st));
     if (iters)
       for (int b = 0; b < B; ++b) iters[b] = it_sum[b];
+    check_oc_barrier(c, st);
+  });
+}
+
+int maple_test_wait_limit(long long max_polls, int phantom_blocks) {
+  return guarded([&] {
+    require(max_polls >= 0 && phantom_blocks >= 0, "max_polls and phantom_blocks must be >= 0");
+    tl_wait_polls = max_polls > 0 ? max_polls : kBarrierPolls;
+    tl_wait_phantom = (unsigned)phantom_blocks;
   });
 }
 

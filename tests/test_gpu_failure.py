@@ -89,3 +89,43 @@ def test_garbage_finite_guess_recovers(lib):
 def test_iteration_cap_reports_maxit(lib, prec):
     info, _ = _solve(_rho((6, 7)), prec, maxit=2)
     assert list(info.status) == [MAXIT, MAXIT] and list(info.iters) == [2, 2]
+
+
+def _oc_inputs(B, N, seed=3):
+    rng = np.random.default_rng(seed)
+    x = np.clip(0.25 + 0.2 * rng.standard_normal((B, N)), 1e-3, 1.0)
+    dJ = np.abs(rng.standard_normal((B, N))) * 1e-2
+    return (torch.tensor(x, device=DEV), torch.tensor(dJ, device=DEV),
+            torch.tensor(np.full(B, 0.25), device=DEV))
+
+
+def test_oc_barrier_wait_runs_out_and_is_reported(lib):
+    """The OC bisection runs as one cooperative launch whose blocks meet at grid
+    barriers, each wait bounded by a poll limit.  A phantom block that never
+    arrives (maple_test_wait_limit) makes every wait run out: maple_oc_update
+    and maple_oc_step must return MAPLE_E_TIMEOUT instead of hanging or
+    reporting success, and the context must give the normal result afterwards."""
+    from maple_b200 import _lib
+    from maple_b200.core import HomogenizationContext
+    r, B = 8, 2
+    N = r ** 3
+    ctx = HomogenizationContext(r, ncells=B, device=DEV)
+    x, dJ, vf = _oc_inputs(B, N)
+    good, good_stats = ctx.oc_update(x, dJ, vf, move=0.2, xmin=1e-3)
+    good, good_stats = good.cpu().numpy(), good_stats.cpu().numpy()
+    w = torch.tensor([[0.5, 0.0, 0.5]] * B, dtype=torch.float64, device=DEV)
+    _lib.check(lib.maple_test_wait_limit(1 << 12, 1))
+    try:
+        with pytest.raises(_lib.MapleError) as e:
+            ctx.oc_update(x, dJ, vf, move=0.2, xmin=1e-3)
+        assert e.value.code == _lib.MAPLE_E_TIMEOUT
+        assert "grid barrier" in str(e.value)
+        with pytest.raises(_lib.MapleError, match="grid barrier") as e:
+            ctx.oc_step(x, w, vf, precision="fp64", rtol=1e-8)
+        assert e.value.code == _lib.MAPLE_E_TIMEOUT
+    finally:
+        _lib.check(lib.maple_test_wait_limit(0, 0))
+    again, again_stats = ctx.oc_update(x, dJ, vf, move=0.2, xmin=1e-3)
+    np.testing.assert_array_equal(again.cpu().numpy(), good)
+    np.testing.assert_array_equal(again_stats.cpu().numpy(), good_stats)
+    ctx.close()

@@ -58,3 +58,69 @@ def test_noalloc_rejects_batches_beyond_its_array(lib):
                                      C.c_void_p(torch.cuda.current_stream(DEV).cuda_stream))
     assert rc != 0
     assert "scratch" in lib.maple_last_error_string().decode()
+
+
+def _ctx_reference(r, B, x, dJ, vf):
+    from maple_b200.core import HomogenizationContext
+    ctx = HomogenizationContext(r, ncells=B, device=DEV)
+    ref, ref_stats = ctx.oc_update(x, dJ, vf, move=0.2, xmin=1e-3)
+    torch.cuda.synchronize()
+    out = ref.cpu().numpy(), ref_stats.cpu().numpy()
+    ctx.close()
+    return out
+
+
+def test_noalloc_cell_limits_and_multi_launch(lib):
+    """The documented limits, exactly: 8191 cells per call with a statistics
+    buffer, 5460 without.  At 8^3 so many cells need several cooperative
+    launches per call (each reuses the array's partial sums and clears the
+    barrier words again); every cell must still match maple_oc_update."""
+    r = 8
+    N = r ** 3
+    B = 8191
+    x, dJ, vf = _inputs(np.random.default_rng(5), B, N)
+    ref, ref_stats = _ctx_reference(r, B, x, dJ, vf)
+    stream = C.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)
+    out = torch.full_like(x, -1.0)
+    stats = torch.full((B, 2), -1.0, dtype=torch.float64, device=DEV)
+    assert lib.maple_oc_update_noalloc(N, B, _p(x), _p(dJ), _p(vf), 0.2, 1e-3, _p(out), _p(stats), stream) == 0
+    torch.cuda.synchronize()
+    assert np.abs(out.cpu().numpy() - ref).max() < 1e-10
+    assert np.abs(stats.cpu().numpy() - ref_stats).max() < 1e-12
+    big = torch.zeros((B + 1, N), dtype=torch.float64, device=DEV)
+    rc = lib.maple_oc_update_noalloc(N, B + 1, _p(big), _p(big), _p(big[:, 0].contiguous()), 0.2, 1e-3,
+                                     _p(torch.empty_like(big)), _p(torch.empty((B + 1, 2), dtype=torch.float64,
+                                                                             device=DEV)), stream)
+    assert rc != 0 and "8191 cells" in lib.maple_last_error_string().decode()
+    # without a statistics buffer the array also holds the statistics
+    Bn = 5460
+    out = torch.full_like(x[:Bn], -1.0)
+    assert lib.maple_oc_update_noalloc(N, Bn, _p(x), _p(dJ), _p(vf), 0.2, 1e-3, _p(out), None, stream) == 0
+    torch.cuda.synchronize()
+    assert np.abs(out.cpu().numpy() - ref[:Bn]).max() < 1e-10
+    rc = lib.maple_oc_update_noalloc(N, Bn + 1, _p(x), _p(dJ), _p(vf), 0.2, 1e-3, _p(torch.empty_like(x)), None,
+                                     stream)
+    assert rc != 0 and "5460 cells" in lib.maple_last_error_string().decode()
+
+
+def test_noalloc_reports_a_barrier_wait_that_runs_out(lib):
+    """With a phantom block that never arrives (maple_test_wait_limit) the
+    bounded barrier waits run out: the call returns MAPLE_E_TIMEOUT and the
+    next normal call gives the normal result."""
+    from maple_b200 import _lib
+    r, B = 8, 3
+    N = r ** 3
+    x, dJ, vf = _inputs(np.random.default_rng(21), B, N)
+    ref, _ = _ctx_reference(r, B, x, dJ, vf)
+    stream = C.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)
+    out = torch.full_like(x, -1.0)
+    _lib.check(lib.maple_test_wait_limit(1 << 12, 1))
+    try:
+        rc = lib.maple_oc_update_noalloc(N, B, _p(x), _p(dJ), _p(vf), 0.2, 1e-3, _p(out), None, stream)
+    finally:
+        _lib.check(lib.maple_test_wait_limit(0, 0))
+    assert rc == _lib.MAPLE_E_TIMEOUT
+    assert "grid barrier" in lib.maple_last_error_string().decode()
+    assert lib.maple_oc_update_noalloc(N, B, _p(x), _p(dJ), _p(vf), 0.2, 1e-3, _p(out), None, stream) == 0
+    torch.cuda.synchronize()
+    assert np.abs(out.cpu().numpy() - ref).max() < 1e-10
