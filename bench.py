@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--rtol", type=float, default=1e-10)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-fp64-arm", action="store_true", help="skip the plain-FP64 comparison arm")
+    p.add_argument("--no-chs", action="store_true", help="skip the C^H solves/s measurement")
     p.add_argument("--serial", action="store_true",
                    help="run the elastic and thermal solves one after the other on one host thread")
     return p.parse_args()
@@ -154,21 +156,89 @@ def max_over_ranks(value: float, world: int, device) -> float:
     return float(t.item())
 
 
+def _timed_oc_steps(ctx, x0, w, vf, kw, args, flush, barrier, sampler=None):
+    """W untimed warm-up steps, then K steps each bracketed by CUDA events on
+    the current stream (L2 flushed between steps, outside the events).
+    Returns the step times, PCG iterations, launches and the per-step C^H,
+    kappa^H and J of the timed steps."""
+    import torch
+
+    from maple_b200.core import launch_count
+    x = x0.clone()
+    for _ in range(args.warmup):
+        out = ctx.oc_step(x, w, vf, **kw)
+        x = out["x_next"].clone()
+    torch.cuda.synchronize()
+    if sampler is not None:
+        sampler.start()
+        time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    iters, recs = [], []
+    lc0 = launch_count()
+    t_wall = time.perf_counter()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record()
+        out = ctx.oc_step(x, w, vf, **kw)
+        ev[k][1].record()
+        x = out["x_next"].clone()
+        iters.append(int(out["iters"][0]))
+        recs.append((out["CH"][0].clone(), out["kappa"][0].clone(), out["J"][0].clone()))
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    launches = launch_count() - lc0
+    barrier()
+    clocks = sampler.stop() if sampler is not None else None
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    recs = [(c.cpu().numpy(), k.cpu().numpy(), float(j)) for c, k, j in recs]
+    return dict(step_ms=step_ms, iters=iters, launches=launches, wall=t_wall, clocks=clocks, recs=recs, x=x,
+                J=float(out["J"][0]))
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _chs_solves(ctx, x, precision, rtol, steps, flush):
+    """C^H solves: SIMP densities of x, then for both physics the hierarchy
+    build, the MG-PCG solve of every load case from a zero initial iterate to
+    rtol and the FP64 energy sums; `steps` solves timed with CUDA events."""
+    import torch
+    rho = (1e-9 + (1.0 - 1e-9) * x.clamp(1e-3, 1.0) ** 3).contiguous()
+    t = 0.0
+    its = []
+    for k in range(steps + 1):  # the first is an untimed warm-up
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        n = 0
+        for ph in ("elastic", "thermal"):
+            ctx.set_density(ph, rho, precision)
+            n += int(ctx.solve(ph, precision, rtol=rtol, maxit=500, warm=False).iters[0])
+            ctx.homogenize(ph)
+        e1.record()
+        torch.cuda.synchronize()
+        if k:
+            t += e0.elapsed_time(e1) / 1000.0
+            its.append(n)
+    return t, its
+
+
 def run_maple(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
 
-    from maple_b200.core import HomogenizationContext, launch_count
+    from maple_b200.core import HomogenizationContext
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     r = args.res
-    ctx = HomogenizationContext(r, ncells=1, device=dev)
-    ctx.set_concurrency(not args.serial)
     w = torch.tensor([[1 / 3, 1 / 3, 1 / 3]], dtype=torch.float64, device=dev)
     vf = torch.tensor([0.25], dtype=torch.float64, device=dev)
-    x0 = seeded_design(rank, r, sigma=r / 16.0, vf=0.25)
-    x = torch.tensor(x0.reshape(1, -1), dtype=torch.float64, device=dev)
+    x0 = torch.tensor(seeded_design(rank, r, sigma=r / 16.0, vf=0.25).reshape(1, -1), dtype=torch.float64,
+                      device=dev)
     kw = dict(penal=3.0, rho_min=1e-9, move=0.2, xmin=1e-3, filter_k=3, precision=args.precision, rtol=args.rtol,
               maxit=500, warm=True)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
@@ -177,39 +247,44 @@ def run_maple(args, rank, world, local_rank):
         if world > 1:
             dist.barrier()
 
-    # warm-up (advances the design)
-    out = None
-    for _ in range(args.warmup):
-        out = ctx.oc_step(x, w, vf, **kw)
-        x = out["x_next"].clone()
-    torch.cuda.synchronize()
-
-    # timed region: K steps, each bracketed by events; L2 flushed between steps
-    sampler = ClockSampler(local_rank)
-    sampler.start()
-    time.sleep(0.3)
-    barrier()
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    iters = []
-    lc0 = launch_count()
-    t_wall = time.perf_counter()
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        ev[k][0].record()
-        out = ctx.oc_step(x, w, vf, **kw)
-        ev[k][1].record()
-        x = out["x_next"]
-        iters.append(int(out["iters"][0]))
-        x = x.clone()
-    torch.cuda.synchronize()
-    t_wall = time.perf_counter() - t_wall
-    launches = launch_count() - lc0
-    barrier()
-    clocks = sampler.stop()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    t_dev = max_over_ranks(sum(step_ms) / 1000.0, world, dev)
+    # the benchmarked arm
+    ctx = HomogenizationContext(r, ncells=1, device=dev)
+    ctx.set_concurrency(not args.serial)
+    main_arm = _timed_oc_steps(ctx, x0, w, vf, kw, args, flush, barrier, ClockSampler(local_rank))
+    t_dev = max_over_ranks(sum(main_arm["step_ms"]) / 1000.0, world, dev)
     value = world * args.steps / t_dev
+    x = main_arm["x"]
+
+    # the plain FP64 arm: same cell, same start, same steps
+    fp64 = None
+    if args.precision == "mixed" and not args.no_fp64_arm:
+        ctx64 = HomogenizationContext(r, ncells=1, device=dev)
+        ctx64.set_concurrency(not args.serial)
+        arm64 = _timed_oc_steps(ctx64, x0, w, vf, dict(kw, precision="fp64"), args, flush, barrier)
+        t64 = max_over_ranks(sum(arm64["step_ms"]) / 1000.0, world, dev)
+        errs = [max(_rel(a[0], b[0]), _rel(a[1], b[1]), abs(a[2] - b[2]) / abs(b[2]))
+                for a, b in zip(main_arm["recs"], arm64["recs"])]
+        fp64 = dict(value=world * args.steps / t64, ms_per_step=1000 * t64 / args.steps, iters=arm64["iters"],
+                    err=errs, ctx=ctx64)
+
+    # C^H solves per second (every load case from zero, hierarchy builds included)
+    chs = None
+    if not args.no_chs:
+        nsol = max(3, min(args.steps, 10))
+        t_chs, its = _chs_solves(ctx, x, args.precision, args.rtol, nsol, flush)
+        t_chs = max_over_ranks(t_chs, world, dev)
+        chs = {"value": round(world * nsol / t_chs, 3), "unit": "C^H solves/s", "solves": nsol,
+               "pcg_iters_per_solve": its,
+               "what": "SIMP densities, hierarchy build, 6 elastic + 3 thermal load cases from a zero initial "
+                       f"iterate to rtol {args.rtol:g}, FP64 C^H / kappa^H; elastic then thermal"}
+        if fp64 is not None:
+            t64c, its64 = _chs_solves(fp64["ctx"], x, "fp64", args.rtol, nsol, flush)
+            t64c = max_over_ranks(t64c, world, dev)
+            chs["fp64_value"] = round(world * nsol / t64c, 3)
+            chs["fp64_pcg_iters_per_solve"] = its64
+    if fp64 is not None:
+        fp64["ctx"].close()
+        del fp64["ctx"]
 
     # live roofline of the dominant kernel class over K further steps
     ctx.profile(True, max_launches=200000)
@@ -262,52 +337,74 @@ def run_maple(args, rank, world, local_rank):
         t_e2e = max_over_ranks(e_ms / 1000.0, world, dev)
         e2e = {"value": round(world * args.steps / t_e2e, 3), "unit": UNIT,
                "h2d_bytes_per_step": int(x_host.numel() * 8), "d2h_bytes_per_step": int(x_out.numel() * 8 + 8)}
-
-    return dict(value=value, t_dev=t_dev, step_ms=step_ms, wall=t_wall, launches=launches, clocks=clocks,
-                roofline=roofline, e2e=e2e, iters=iters, levels=ctx.levels, J=float(out["J"][0]))
+    ctx.close()
+    return dict(value=value, t_dev=t_dev, step_ms=main_arm["step_ms"], wall=main_arm["wall"],
+                launches=main_arm["launches"], clocks=main_arm["clocks"], roofline=roofline, e2e=e2e,
+                iters=main_arm["iters"], levels=ctx.levels, J=main_arm["J"], fp64=fp64, chs=chs)
 
 
 # ---------------------------------------------------------------------------
-def _oracle_step(r, precision_note=None):
-    from oracle import ihd_oracle as O
-    x = seeded_design(0, r, sigma=r / 16.0, vf=0.25)
-    lv = int(np.log2(r // 4)) + 1
+# CPU path: the oracle's multithreaded C restatement of the reference's
+# algorithm (V-cycles with 8-colour Gauss-Seidel to the relative residual,
+# energy sums, adjoint sensitivities, filter, OC bisection) on every host core.
+# The reference itself is Python that lives outside this repository, so it
+# cannot run on the measuring host; oracle/port.c is pinned against the numpy
+# oracle, which is pinned against the reference's own outputs.
+TRI = {"stiffness": 1 / 3, "shear": 1 / 3, "thermal": 1 / 3}
+
+
+def _cpu_cell(res):
+    from oracle import port
+    port.build()
+    cores = port.set_threads(os.cpu_count() or 1)
+    levels = int(np.log2(res // 2))  # down to a 2^3 grid, as the oracle fixtures
+    return port, port.Cell(res, levels), cores, levels
+
+
+def cpu_baseline(args):
+    """One OC iteration of the benchmark cell (same seeded design, objective,
+    tolerance) by the C restatement on all host cores, from zero initial
+    iterates: a bounded sample of the workload, measured, not scaled."""
+    port, cell, cores, levels = _cpu_cell(args.res)
+    x = seeded_design(0, args.res, sigma=args.res / 16.0, vf=0.25).reshape(-1)
     t = time.perf_counter()
-    O.oc_iteration(x, r, {"stiffness": 1 / 3, "shear": 1 / 3, "thermal": 1 / 3}, volfrac=0.25, move=0.2,
-                   levels=lv, rtol=1e-10, max_cycles=500)
-    return time.perf_counter() - t
-
-
-def cpu_baseline(res):
-    """The FP64 oracle (the reference's V-cycle algorithm restated in numpy/scipy)
-    on the host cores: one OC iteration at 32^3, scaled to the bench cell by
-    element count."""
-    rs = 32
-    t = _oracle_step(rs)
-    scale = (res / rs) ** 3
-    return {"value": round(1.0 / (t * scale), 6), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"1 OC iteration at {rs}^3 (tri-objective, FP64 V-cycles to rtol 1e-10) = {t:.2f} s, "
-                      f"scaled x{scale:g} to {res}^3 by element count"}
+    _, info = port.oc_iteration(x, cell, TRI, volfrac=0.25, move=0.2, xmin=1e-3, filter_k=3, rtol=args.rtol,
+                                max_cycles=1000, warm=False)
+    t = time.perf_counter() - t
+    return {"value": round(1.0 / t, 6), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"1 OC iteration of the {args.res}^3 cell (tri-objective, FP64 V-cycles with 8-colour "
+                      f"Gauss-Seidel, {levels} levels, to rtol {args.rtol:g}; {info['cycles_elastic']} elastic + "
+                      f"{info['cycles_thermal']} thermal cycles from a zero start) = {t:.2f} s on {cores} threads"}
 
 
 def run_reference(args):
-    """Reference arm: the oracle port of the reference's CPU path, one bounded
-    sample per step (one OC iteration at 16^3, scaled to the bench cell)."""
-    rs = 16
-    scale = (args.res / rs) ** 3
+    """Reference arm: the reference's CPU algorithm (its C restatement,
+    oracle/port.c) on every host core, on the benchmark cell: W untimed OC
+    iterations from the seeded design, then K timed ones, each warm-started
+    from the previous solutions like the GPU arm."""
+    port, cell, cores, levels = _cpu_cell(args.res)
+    x = seeded_design(0, args.res, sigma=args.res / 16.0, vf=0.25).reshape(-1)
+    kw = dict(volfrac=0.25, move=0.2, xmin=1e-3, filter_k=3, rtol=args.rtol, max_cycles=1000, warm=True)
     for _ in range(args.warmup):
-        _oracle_step(rs)
-    ts = [_oracle_step(rs) for _ in range(args.steps)]
-    tot = sum(ts) * scale
+        x, _ = port.oc_iteration(x, cell, TRI, **kw)
+    ts, cyc = [], []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        x, info = port.oc_iteration(x, cell, TRI, **kw)
+        ts.append(time.perf_counter() - t)
+        cyc.append(info["cycles_elastic"] + info["cycles_thermal"])
+    tot = sum(ts)
     value = args.steps / tot
+    sample = (f"{args.steps} OC iterations of the {args.res}^3 cell after {args.warmup} untimed ones, FP64 V-cycles "
+              f"with 8-colour Gauss-Seidel ({levels} levels) to rtol {args.rtol:g}, warm-started; {cores} threads")
     return {"metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000 * tot / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"OC iteration, {args.res}^3 periodic cell, tri-objective, vf 0.25",
-                       "res": args.res},
-            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": f"{args.steps} x 1 OC iteration at {rs}^3 (FP64 V-cycles to 1e-10), "
-                                       f"scaled x{scale:g} by element count"},
+            "config": {"workload": f"OC iteration, {args.res}^3 periodic cell (config 1: precision)",
+                       "res": args.res, "rtol": args.rtol, "objective": "(E+G+kappa)/3", "volfrac": 0.25,
+                       "move": 0.2, "filter_k": 3, "mg_levels": levels, "cycles_per_step": cyc},
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -331,7 +428,7 @@ def main():
     res = run_maple(args, rank, world, local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.res)
+        cpu = cpu_baseline(args)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(res["value"], 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -346,9 +443,18 @@ def main():
                        "mg_levels": res["levels"], "l2": "flushed between steps (256 MiB write outside the events)",
                        "parallelism": f"replicas x{world}", "pcg_iters_per_step": res["iters"]},
             "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "roofline": res["roofline"],
-            "cpu_baseline": cpu, "e2e": res["e2e"], "wall_s": round(res["wall"], 3),
+            "cpu_baseline": cpu, "e2e": res["e2e"], "chs": res["chs"], "wall_s": round(res["wall"], 3),
             "step_ms": [round(v, 3) for v in res["step_ms"]], "J_last": res["J"],
         }
+        fp = res["fp64"]
+        if fp is not None:
+            line["fp64_arm"] = {"value": round(fp["value"], 3), "unit": UNIT, "ms_per_step": round(fp["ms_per_step"], 3),
+                                "pcg_iters_per_step": fp["iters"],
+                                "what": "plain FP64 MG-PCG, same cell, start design, warm-up and steps"}
+            line["mixed_over_fp64"] = round(res["value"] / fp["value"], 4)
+            line["err_vs_fp64"] = {"max": max(fp["err"]), "per_step": [float(f"{e:.3g}") for e in fp["err"]],
+                                   "what": "max relative difference of C^H, kappa^H and J between the mixed and "
+                                           "the plain FP64 trajectories, per timed step"}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
