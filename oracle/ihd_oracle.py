@@ -508,9 +508,12 @@ def seed_density(seed: int, r: int, sigma: float, vf: float, scale: float = 0.25
 # ---------------------------------------------------------------------------
 def solve_cell(rho: np.ndarray, r: int, elems: Elements | None = None, levels: int = 3,
                max_cycles: int = 200, rtol: float = 1e-12, physics=("elastic", "thermal"),
-               smooth_iter=(2, 2, 3, 4, 5)):
+               smooth_iter=(2, 2, 3, 4, 5), u0: dict | None = None):
     """Both physics on one cell: returns dict with CH, kappa, u3, u1 and the
-    per-element energies (dC/drho, dkappa/drho)."""
+    per-element energies (dC/drho, dkappa/drho).  ``u0`` (keys "u3" / "u1",
+    e.g. the previous OC iteration's solutions) is the initial iterate of the
+    V-cycles; the converged answer does not depend on it (the reference starts
+    from zero, EBE_GMG.py:851-858)."""
     elems = elems or Elements(r)
     out = {}
     rho = rho.reshape(-1)
@@ -519,8 +522,10 @@ def solve_cell(rho: np.ndarray, r: int, elems: Elements | None = None, levels: i
         Ke0, Fe0, X0 = elems.get(d)
         hier = Hierarchy(rho, Ke0, r, d, levels)
         F = assemble_F(rho, Fe0, r, d)
+        key_u = "u3" if d == 3 else "u1"
+        start = None if u0 is None else u0.get(key_u)
         u, res, cyc = gmg_solve(hier, F, max_cycles, smooth_iter,
-                                coarse_default=1 if d == 3 else None, rtol=rtol)
+                                coarse_default=1 if d == 3 else None, rtol=rtol, u0=start)
         H = homogenize(u, rho, Ke0, X0, r, d)
         dH = element_energy(u, Ke0, X0, r, d)
         key = "CH" if d == 3 else "kappa"
@@ -575,13 +580,16 @@ def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal:
                  rho_min: float = 1e-9, move: float = 0.2, xmin: float = 1e-3, filter_k: int = 3,
                  elems: Elements | None = None, levels: int = 3, rtol: float = 1e-12,
                  max_cycles: int = 200, symmetry: str = "none", lambda_print: float = 0.0,
-                 overhang_deg: float = 45.0, lambda_cavity: float = 0.0, cavity: dict | None = None):
+                 overhang_deg: float = 45.0, lambda_cavity: float = 0.0, cavity: dict | None = None,
+                 u0: dict | None = None):
     """One OC iteration of main_IHD_v3.py:620-716 with the analytic adjoint in
     place of autograd.  With a symmetry, the solve uses the projected design,
     the gradient is projected (the group average is self-adjoint) and so is
     the updated design.  Penalties (:649-686): J = J_raw - lambda_print *
     P_overhang - lambda_cavity * P_cavity, `cavity` holding cavity_penalty's
-    keywords.  Returns (x_next, info)."""
+    keywords.  ``u0`` is passed to ``solve_cell`` as the solves' initial
+    iterate (``info["res"]`` of the previous iteration serves).  Returns
+    (x_next, info)."""
     kind, axes = parse_symmetry(symmetry)
     x = x.reshape(-1)
     xc = np.clip(symmetrize(np.clip(x, xmin, 1.0), r, kind, axes), xmin, 1.0)
@@ -591,7 +599,7 @@ def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal:
         phys.append("elastic")
     if "thermal" in weights:
         phys.append("thermal")
-    res = solve_cell(rho, r, elems, levels, max_cycles, rtol, tuple(phys))
+    res = solve_cell(rho, r, elems, levels, max_cycles, rtol, tuple(phys), u0=u0)
     CH = res.get("CH")
     kap = res.get("kappa")
     J, gC, gK = objective_and_grads(weights, CH if CH is not None else np.eye(6),

@@ -2,7 +2,7 @@
 
 Run in a container where the reference source tree is available:
 
-    python tests/golden/make_golden.py /path/to/MAPLE/src
+    python tests/golden/make_golden.py /path/to/MAPLE/src [--only=<part>]
 
 It imports the reference package, runs its own functions in FP64 and writes
 ``tests/golden/*.npz``.  Nothing at test time reads the reference tree: the
@@ -121,6 +121,10 @@ def main(src, only=None):
             out["F_thermal"] = Ft.detach().numpy()
         return out
 
+    if only == "config0":
+        return config0_fixtures(Ob, homogenize)
+    if only == "config1":
+        return config1_fixtures(Ob, homogenize)
     if only == "symmetry":
         return symmetry_fixtures(M, Ob, homogenize, dev)
     if only == "generator":
@@ -223,6 +227,102 @@ def main(src, only=None):
         x = xn
         print("traj it", it, "J", J.item())
     np.savez_compressed(os.path.join(HERE, "traj_r8.npz"), **traj)
+
+
+def _oracle():
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle import ihd_oracle as O
+    return O
+
+
+def _reference_terms(Ob, homogenize, r, x, spec, cycles, levels, penal=3.0, rho_min=1e-9, xmin=1e-3):
+    """C^H, kappa^H and J of design x by the reference's own FP64 solvers."""
+    xt = torch.tensor(np.clip(x, xmin, 1.0).reshape(-1, 1))
+    rho = rho_min + (1 - rho_min) * xt ** penal
+    o = homogenize(r, rho, cycles, levels=levels)
+    J = Ob.objective_from_spec(obj=spec, CH=o["CH"], kappa=o["kappa"])
+    return (o["CH"].detach().numpy(), o["kappa"].detach().numpy(), float(J),
+            float(max(o["relres_elastic"].max(), o["relres_thermal"].max())))
+
+
+def config0_fixtures(Ob, homogenize):
+    """traj_r32.npz: the plain FP64 method of the 32^3 benchmark configuration
+    (seed 0, sigma 2, vf 0.25, J = 0.5 E + 0.5 kappa, move 0.2, 3^3 filter,
+    50 OC iterations).  The oracle runs the 50 iterations with its solves
+    converged to a relative residual of 1e-12 (warm-started from the previous
+    iteration; the converged answer is independent of the start); every
+    iteration's J, C^H, kappa^H and |dx| statistics and the designs at
+    iterations 1, 10, 49 and 50 are stored.  The reference's own FP64 GMG
+    solvers then evaluate C^H, kappa^H and J at the oracle's designs of
+    iterations 0, 1, 10 and 49 (the pins of the oracle trajectory)."""
+    import time
+    O = _oracle()
+    r, vf, spec = 32, 0.25, "stiffness:0.5,thermal:0.5"
+    w = O.parse_objective_spec(spec)
+    x = O.seed_density(0, r, 2.0, vf).reshape(-1)
+    el = O.Elements(r)
+    rec = dict(r=r, seed=0, sigma=2.0, vf=vf, move=0.2, filter_k=3, penal=3.0, rho_min=1e-9, xmin=1e-3,
+               iters=50, oracle_rtol=1e-12, x0=x.copy())
+    Js, CHs, Ks, dmax, dmean, xs, relres = [], [], [], [], [], {}, []
+    prev = None
+    t0 = time.time()
+    for it in range(50):
+        if it in (1, 10, 49):
+            xs[it] = x.copy()
+        xn, info = O.oc_iteration(x, r, w, volfrac=vf, move=0.2, elems=el, levels=5, rtol=1e-12,
+                                  max_cycles=400, u0=prev)
+        prev = info["res"]
+        Js.append(info["J"])
+        CHs.append(info["CH"])
+        Ks.append(info["kappa"])
+        dmax.append(info["dx_max"])
+        dmean.append(info["dx_mean"])
+        relres.append(max(prev["relres_elastic"].max(), prev["relres_thermal"].max()))
+        print(f"config0 oracle it {it} J {info['J']:.15g} cycles {prev['cycles_elastic']} {prev['cycles_thermal']} "
+              f"relres {relres[-1]:.2e} t {time.time() - t0:.0f}s", flush=True)
+        x = xn
+    rec.update(J=np.array(Js), CH=np.array(CHs), kappa=np.array(Ks), dx_max=np.array(dmax), dx_mean=np.array(dmean),
+               oracle_relres=np.array(relres), x50=x.copy())
+    for it, xv in xs.items():
+        rec[f"x{it}"] = xv
+    for it in (0, 1, 10, 49):
+        xv = rec["x0"] if it == 0 else xs[it]
+        CH, kap, J, rr = _reference_terms(Ob, homogenize, r, xv, spec, cycles=90, levels=5)
+        rec[f"ref_CH_{it}"], rec[f"ref_kappa_{it}"], rec[f"ref_J_{it}"], rec[f"ref_relres_{it}"] = CH, kap, J, rr
+        print(f"config0 reference it {it} J {J:.15g} (oracle {Js[it]:.15g}) relres {rr:.2e}", flush=True)
+    np.savez_compressed(os.path.join(HERE, "traj_r32.npz"), **rec)
+    print("wrote traj_r32.npz")
+
+
+def config1_fixtures(Ob, homogenize):
+    """spot_r64.npz: the 64^3 precision configuration (seed 0, sigma 4,
+    vf 0.25, J = (E + G + kappa)/3).  The oracle runs OC iteration 0 from the
+    seeded design (solves to a relative residual of 1e-12) and evaluates
+    iteration 1's design; the reference's own FP64 GMG solvers evaluate C^H,
+    kappa^H and J at both designs."""
+    import time
+    O = _oracle()
+    r, vf = 64, 0.25
+    spec = "stiffness:0.3333333333333333,shear:0.3333333333333333,thermal:0.3333333333333333"
+    w = O.parse_objective_spec(spec)
+    x0 = O.seed_density(0, r, 4.0, vf).reshape(-1)
+    el = O.Elements(r)
+    t0 = time.time()
+    x1, info0 = O.oc_iteration(x0, r, w, volfrac=vf, move=0.2, elems=el, levels=6, rtol=1e-12, max_cycles=400)
+    print(f"config1 oracle it 0 J {info0['J']:.15g} t {time.time() - t0:.0f}s", flush=True)
+    _, info1 = O.oc_iteration(x1, r, w, volfrac=vf, move=0.2, elems=el, levels=6, rtol=1e-12, max_cycles=400,
+                              u0=info0["res"])
+    print(f"config1 oracle it 1 J {info1['J']:.15g} t {time.time() - t0:.0f}s", flush=True)
+    rec = dict(r=r, seed=0, sigma=4.0, vf=vf, move=0.2, filter_k=3, penal=3.0, rho_min=1e-9, xmin=1e-3,
+               oracle_rtol=1e-12, x1=x1,
+               J=np.array([info0["J"], info1["J"]]), CH=np.array([info0["CH"], info1["CH"]]),
+               kappa=np.array([info0["kappa"], info1["kappa"]]))
+    for it, xv in ((0, x0), (1, x1)):
+        CH, kap, J, rr = _reference_terms(Ob, homogenize, r, xv, spec, cycles=90, levels=6)
+        rec[f"ref_CH_{it}"], rec[f"ref_kappa_{it}"], rec[f"ref_J_{it}"], rec[f"ref_relres_{it}"] = CH, kap, J, rr
+        print(f"config1 reference it {it} J {J:.15g} relres {rr:.2e} t {time.time() - t0:.0f}s", flush=True)
+    np.savez_compressed(os.path.join(HERE, "spot_r64.npz"), **rec)
+    print("wrote spot_r64.npz")
 
 
 def printability_fixtures(M, Ob, homogenize, dev, src):
@@ -390,4 +490,7 @@ def generator_fixtures():
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
     only = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")), None)
-    main(args[0] if args else "/root/reference/src", only)
+    if len(args) != 1:
+        sys.exit("usage: python tests/golden/make_golden.py <reference src dir> [--only=config0|config1|print|"
+                 "symmetry|generator]")
+    main(args[0], only)
