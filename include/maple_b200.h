@@ -76,6 +76,22 @@ int maple_ctx_info(const maple_ctx* ctx, int* levels_out, int* coarsest_n_out, s
 int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio, int power_iters, double inner_rtol,
                              int check_every);
 
+/* Form of the mixed-precision (MAPLE_MIXED) solve:
+ *   MAPLE_MIXED_FLEXIBLE  flexible FP64 PCG (FP64 fine operator, residuals and
+ *                         dot products every iteration) preconditioned by the
+ *                         FP32 V-cycle;
+ *   MAPLE_MIXED_REFINE    FP32 MG-PCG (FP32 fine operator and vectors, FP64
+ *                         accumulated dots) on the scaled FP64 residual inside
+ *                         FP64 iterative refinement: per outer pass one FP64
+ *                         residual r = b - A x, the convergence test, the inner
+ *                         solve to the inner tolerance of
+ *                         maple_set_solver_options, and x += ||r|| e in FP64.
+ * Both stop at the same FP64 residual test ||b - A x|| <= rtol ||b|| per load
+ * case.  The reference solves in one precision (utils/EBE_GMG.py:758-885,
+ * dtype argument). */
+enum { MAPLE_MIXED_FLEXIBLE = 0, MAPLE_MIXED_REFINE = 1 };
+int maple_set_mixed_mode(maple_ctx* ctx, int mode);
+
 /* CUDA-graph replay of the PCG iteration body (default on).  Off runs every
  * launch eagerly (same results). */
 int maple_set_graphs(maple_ctx* ctx, int enable);
@@ -224,6 +240,26 @@ int maple_assemble_rhs(maple_ctx* ctx, int physics, const double* rho, double* F
 /* y = K(rho) u on the fine level, FP64 (utils/EBE_GMG.py:412-430
  * EBEOperator.matvec with Ke_e = rho_e Ke0). */
 int maple_matvec(maple_ctx* ctx, int physics, const double* rho, const double* u, double* y, maple_stream_t stream);
+
+/* Galerkin element matrices of multigrid level `level` (1 <= level < levels)
+ * of the hierarchy the last maple_set_density built for `physics`: out
+ * [B][N_l][8D][8D] FP64, row-major, element id x*n*n + y*n + z of the level's
+ * n^3 grid, local index corner*D + component with the element-local corner
+ * order 000,100,110,010,001,101,111,011.  The coarse Ke of
+ * utils/EBE_GMG.py:226-337 sparse_coarsen_ke (scalar:
+ * utils/EBE_GMG_scalar.py:135-230). */
+int maple_get_level_elements(maple_ctx* ctx, int physics, int level, double* out, maple_stream_t stream);
+
+/* Periodic trilinear grid transfer between a (2 nc)^3 fine and an nc^3 coarse
+ * grid for ncells x K fields (K = 3 or 18), FP64, layout [ncells][K][nodes]:
+ * MAPLE_RESTRICT out = P^T in (fine in, coarse out); MAPLE_PROLONG_ADD
+ * out += P in (coarse in, fine out).  P interpolates a fine node at an even
+ * coordinate from its own coarse node and at an odd one half-and-half from
+ * the two neighbours, per axis.  ProlongStencil.prolong / restrict_PT
+ * (utils/EBE_GMG.py:38-79; weights of _build_prolongation_operator_robust,
+ * EBE_GMG.py:531-647). */
+enum { MAPLE_RESTRICT = 0, MAPLE_PROLONG_ADD = 1 };
+int maple_transfer(int op, int nc, int K, int ncells, const double* in, double* out, maple_stream_t stream);
 
 /* Periodic k^3 box filter of [B][N] (main_IHD_v3.py:342-359). */
 int maple_box_filter(int r, int ncells, int k, const double* in, double* out, maple_stream_t stream);

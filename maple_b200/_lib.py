@@ -37,6 +37,7 @@ SIGNATURES = {
     "maple_ctx_info": (_I, [_P, _IP, _IP, C.POINTER(C.c_size_t)]),
     "maple_set_solver_options": (_I, [_P, _I, _D, _I, _D, _I]),
     "maple_set_graphs": (_I, [_P, _I]),
+    "maple_set_mixed_mode": (_I, [_P, _I]),
     "maple_set_concurrency": (_I, [_P, _I]),
     "maple_set_stencil_split": (_I, [_P, _I]),
     "maple_set_coarse_degree": (_I, [_P, _I]),
@@ -59,6 +60,8 @@ SIGNATURES = {
     "maple_assemble_rhs": (_I, [_P, _I, _P, _P, _P]),
     "maple_matvec": (_I, [_P, _I, _P, _P, _P, _P]),
     "maple_box_filter": (_I, [_I, _I, _I, _P, _P, _P]),
+    "maple_get_level_elements": (_I, [_P, _I, _I, _P, _P]),
+    "maple_transfer": (_I, [_I, _I, _I, _I, _P, _P, _P]),
     "maple_oc_update": (_I, [_P, _P, _P, _P, _D, _D, _P, _P, _P]),
     "maple_oc_update_noalloc": (_I, [_I, _I, _P, _P, _P, _D, _D, _P, _P, _P]),
     "maple_test_wait_limit": (_I, [_L, _I]),

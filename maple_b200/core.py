@@ -177,6 +177,15 @@ class HomogenizationContext:
         tail with programmatic dependent launch (default on)."""
         _lib.check(self._lib.maple_set_pdl(self._h, int(bool(enable))))
 
+    def set_mixed_mode(self, mode: str = "flexible"):
+        """Form of the mixed-precision solve: "flexible" (FP64 flexible PCG
+        preconditioned by the FP32 V-cycle) or "refine" (FP32 MG-PCG inside
+        FP64 iterative refinement)."""
+        modes = {"flexible": 0, "refine": 1}
+        if mode not in modes:
+            raise ValueError(f"mixed mode must be one of {sorted(modes)}, got {mode!r}")
+        _lib.check(self._lib.maple_set_mixed_mode(self._h, modes[mode]))
+
     def set_graphs(self, enable: bool):
         """Replay the PCG iteration body as a captured CUDA graph (default on)."""
         _lib.check(self._lib.maple_set_graphs(self._h, int(bool(enable))))
@@ -257,6 +266,19 @@ class HomogenizationContext:
         with torch.cuda.device(self.device):
             _lib.check(self._lib.maple_set_solution(self._h, ph, _ptr(u), _stream(self.device)))
 
+    def level_elements(self, physics, level: int) -> torch.Tensor:
+        """Galerkin element matrices (B, N_l, 8D, 8D) of multigrid level
+        ``level`` (>= 1) of the last hierarchy built for ``physics``."""
+        ph = PHYSICS[physics]
+        D = DR[ph][0]
+        if not 1 <= level < self.levels:
+            raise ValueError(f"level must be in [1, {self.levels}), got {level}")
+        n = self.r >> level
+        out = torch.empty((self.B, n ** 3, 8 * D, 8 * D), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self._lib.maple_get_level_elements(self._h, ph, int(level), _ptr(out), _stream(self.device)))
+        return out
+
     def homogenize(self, physics, want_energy=False):
         """Returns H (B,R,R) and, if asked, the per-element energies (B,R,R,N)."""
         ph = PHYSICS[physics]
@@ -335,6 +357,33 @@ class HomogenizationContext:
                                                     _ptr(out["P_cavity"]), _stream(dev)))
         out["iters"] = it
         return out
+
+
+def transfer(op: str, x: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """Periodic trilinear grid transfer of (B, K, n^3) FP64 fields, K = 3 or
+    18: op "restrict" returns P^T x on the (n/2)^3 grid; "prolong_add"
+    returns out + P x on the (2n)^3 grid (out: zeros when None)."""
+    if x.dtype != torch.float64 or not x.is_cuda or not x.is_contiguous() or x.dim() != 3:
+        raise ValueError("x must be a contiguous (B, K, n^3) float64 CUDA tensor")
+    B, K, N = x.shape
+    n = int(round(N ** (1.0 / 3.0)))
+    if n ** 3 != N:
+        raise ValueError(f"{N} nodes do not form a periodic n^3 grid")
+    if op == "restrict":
+        if n % 2:
+            raise ValueError("restriction needs an even grid")
+        nc, code, shape = n // 2, 0, (B, K, (n // 2) ** 3)
+        out = torch.empty(shape, dtype=torch.float64, device=x.device)
+    elif op == "prolong_add":
+        nc, code, shape = n, 1, (B, K, (2 * n) ** 3)
+        out = torch.zeros(shape, dtype=torch.float64, device=x.device) if out is None else out
+        if tuple(out.shape) != shape or out.dtype != torch.float64 or not out.is_contiguous():
+            raise ValueError(f"out must be a contiguous float64 tensor of shape {shape}")
+    else:
+        raise ValueError(f"op must be 'restrict' or 'prolong_add', got {op!r}")
+    with torch.cuda.device(x.device):
+        _lib.check(_lib.load().maple_transfer(code, int(nc), int(K), int(B), _ptr(x), _ptr(out), _stream(x.device)))
+    return out
 
 
 def launch_count() -> int:

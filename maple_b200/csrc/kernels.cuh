@@ -2134,7 +2134,8 @@ struct RedOp {
   PcgScalars s;
   int R = 0;
   int* breakdown = nullptr;  // ALPHA
-  double rtol2 = 0;          // CHECK
+  double rtol2 = 0;          // CHECK (used when rtol2_dev is NULL)
+  const double* rtol2_dev = nullptr;  // CHECK: rtol^2 read on device, so captured graphs serve any tolerance
   int count = 0;             // CHECK: advance the iteration counter
   int* run = nullptr;        // CHECK: run flags cleared for finished cells
   double* scale = nullptr;   // CHECK: column scales 1/||r|| and ||r|| (nullable)
@@ -2181,7 +2182,8 @@ __global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* _
     int dn = 1;
     if (col) {
       dn = s.done[i];
-      if (!was_done && !dn && s.rr[i] <= op.rtol2 * s.bnorm2[i]) {
+      const double rt2 = op.rtol2_dev ? *op.rtol2_dev : op.rtol2;
+      if (!was_done && !dn && s.rr[i] <= rt2 * s.bnorm2[i]) {
         dn = 1;
         s.done[i] = 1;
       }

@@ -122,6 +122,7 @@ struct Phys {
   double* u64 = nullptr;         // solution
   double* r64 = nullptr;         // residual (FP64)
   double *p64 = nullptr, *q64 = nullptr;  // mixed-precision PCG vectors (z stays FP32)
+  float* b32 = nullptr;          // right-hand side of the FP32 inner solve (refinement mode)
   double* energy = nullptr;      // [B][N][R][R]
   double* H = nullptr;           // [B][R][R]
   Ops<double> o64;
@@ -130,6 +131,7 @@ struct Phys {
 
 struct Scalars {
   double *rz, *rz_new, *pq, *rr, *bnorm2, *alpha, *beta;
+  double* rtol2;  // [1] the tolerance of the running solve, squared
   int *done, *cell_done, *iters, *run;
 };
 
@@ -151,6 +153,7 @@ struct Lane {
   Scalars sc{};            // inner PCG scalars
   double *o_rr = nullptr, *o_bn = nullptr, *o_scale = nullptr, *o_inv = nullptr;  // outer refinement
   int *o_done = nullptr, *o_run = nullptr;
+  int* o_live = nullptr;   // refinement: cells still refined (active, not broken down)
   int* h_flags = nullptr;  // pinned host [B]
   int* breakdown = nullptr;
   cudaStream_t cap_stream = nullptr;
@@ -193,9 +196,8 @@ struct maple_ctx {
   // captured PCG iteration bodies: [physics][precision]
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
-    double rtol = -1;
     unsigned long long kernels = 0;  // kernel nodes per replay (for launch counting)
-  } graphs[2][2];
+  } graphs[2][3];  // [physics][FP64 PCG, flexible mixed PCG, FP32 inner PCG of refinement]
   cudaStream_t aux_stream = nullptr;  // second physics of a concurrent OC step
   cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
   bool use_graphs = true;
@@ -232,6 +234,7 @@ struct maple_ctx {
   double power_safety = 1.15;
   double inner_rtol = 1e-5;
   int check_every = 1;
+  int mixed_mode = 0;  // MAPLE_MIXED_FLEXIBLE or MAPLE_MIXED_REFINE
 };
 
 #define LN(c) ((c)->lanes[maple::tl_lane])
@@ -749,23 +752,20 @@ __global__ void k_init_flags(const int* active, const int* outer_run, int* done,
 
 // Runs the PCG iteration body until every active cell has converged or maxit
 // iterations ran.  The body is captured once into a CUDA graph per
-// (physics, precision, rtol) and replayed; the convergence flags are read back
+// (physics, solve form) and replayed (the tolerance is read on device, so one
+// graph serves every tolerance); the convergence flags are read back
 // after every replay (cells that converged skip all further work on device).
 // The first iteration of a solve always runs eagerly, which also performs the
 // one-time kernel attribute setup outside of any capture.
 template <typename Body>
-static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, double rtol, int maxit, Body& body,
+static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, int maxit, Body& body,
                            cudaStream_t s) {
   const bool graphs = c->use_graphs && !c->profiling;
   for (int it = 1; it <= maxit; ++it) {
     if (!graphs || it == 1) {
       body(s);
     } else {
-      if (ge.exec == nullptr || ge.rtol != rtol) {
-        if (ge.exec) {
-          CK(cudaGraphExecDestroy(ge.exec));
-          ge.exec = nullptr;
-        }
+      if (ge.exec == nullptr) {
         if (!LN(c).cap_stream) CK(cudaStreamCreateWithFlags(&LN(c).cap_stream, cudaStreamNonBlocking));
         cudaGraph_t graph = nullptr;
         const unsigned long long before = tl_launches;
@@ -780,7 +780,6 @@ static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, double rtol,
         CK(cudaStreamEndCapture(LN(c).cap_stream, &graph));
         CK(cudaGraphInstantiate(&ge.exec, graph, 0));
         CK(cudaGraphDestroy(graph));
-        ge.rtol = rtol;
         ge.kernels = tl_launches - before;
         g_launches.fetch_sub(ge.kernels);  // captured, not launched
         tl_launches -= ge.kernels;
@@ -799,7 +798,6 @@ static void drop_graphs(maple_ctx* c) {
     for (auto& ge : row) {
       if (ge.exec) cudaGraphExecDestroy(ge.exec);
       ge.exec = nullptr;
-      ge.rtol = -1;
     }
 }
 
@@ -833,6 +831,8 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
   op.R = R;
   op.breakdown = LN(c).breakdown;
   op.rtol2 = rtol * rtol;
+  op.rtol2_dev = sc.rtol2;
+  KL(c, s, k_fill<double><<<1, 32, 0, s>>>(sc.rtol2, 1, rtol * rtol));
   op.run = sc.run;
   RedOp op0 = op;  // before the loop: no iteration counted
   reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op0, s);
@@ -857,7 +857,8 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
     reduce_op<R, RED_BETA>(c, LN(c).part, nbf, sc.rz_new, op, st);
     KL(c, st, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.p, o.U[0][1], sc.beta, N, run));
   };
-  run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_FP64], rtol, maxit, body, s);
+  run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][std::is_same<T, float>::value ? 2 : MAPLE_FP64], maxit,
+                 body, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -908,6 +909,8 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
   op.R = R;
   op.breakdown = LN(c).breakdown;
   op.rtol2 = rtol * rtol;
+  op.rtol2_dev = sc.rtol2;
+  KL(c, s, k_fill<double><<<1, 32, 0, s>>>(sc.rtol2, 1, rtol * rtol));
   op.run = sc.run;
   op.scale = LN(c).o_scale;
   op.inv = LN(c).o_inv;
@@ -932,7 +935,7 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
     precondition_f32<D, R>(c, p, r, q, run, op, st);
     KL(c, st, k_pcg_direction_f32<R, D, false><<<g2(N, B), kThreads, 0, st>>>(pv, z32, LN(c).o_inv, sc.beta, N, run));
   };
-  run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_MIXED], rtol, maxit, body, s);
+  run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_MIXED], maxit, body, s);
 }
 
 // outer refinement bookkeeping: per (cell, rhs) residual scale and cell done
@@ -955,6 +958,115 @@ __global__ void k_outer_check(const double* rr, const double* bn, double rtol2, 
   }
   done[b] = all;
   run[b] = !all;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision, refinement form: FP32 MG-PCG (FP32 fine operator, FP32
+// vectors, FP64-accumulated dots) on the scaled FP64 residual, inside FP64
+// iterative refinement.  Per outer pass: r = b - A x in FP64, convergence test
+// ||r|| <= rtol ||b|| per load case, the inner FP32 solve of A e = r/||r|| to
+// the inner tolerance (tightened in the last pass to what the tolerance still
+// needs), then x += ||r|| e in FP64.  FP64 work per pass is one fine-level
+// residual and the vector updates; all per-iteration work is FP32.
+// ---------------------------------------------------------------------------
+constexpr int kMaxOuter = 12;
+
+template <int D, int R>
+static void pcg_refine(maple_ctx* c, Phys& p, const double* b, double* x, bool x_zero, double rtol, int maxit,
+                       std::vector<int>& iters, std::vector<int>& status, cudaStream_t s) {
+  const int B = c->B, N = nodes(c->n[0]);
+  const size_t vbytes = (size_t)B * N * R * D * sizeof(double);
+  Lane& ln = LN(c);
+  Ops<double>& o64 = p.o64;
+  Ops<float>& o32 = p.o32;
+  double* r = p.r64;
+  const unsigned nb = nblk(N);
+  iters.assign(B, 0);
+  status.assign(B, MAPLE_CELL_MAXIT);
+  std::vector<int> broken(B, 0), act(B, 1), done(B, 0), it_in(B), dn((size_t)B * R);
+  std::vector<double> rr((size_t)B * R), bn((size_t)B * R);
+  for (int b = 0; b < B; ++b) {
+    act[b] = c->h_active.empty() || c->h_active[b];
+    if (!act[b]) status[b] = MAPLE_CELL_CONVERGED;  // as read_outcome reports skipped cells
+  }
+  // cells still refined: active and not broken down (uploaded when it changes)
+  int* live = ln.o_live;
+  CK(cudaMemcpyAsync(live, act.data(), B * sizeof(int), cudaMemcpyHostToDevice, s));
+  if (x_zero) {
+    CK(cudaMemsetAsync(x, 0, vbytes, s));
+    CK(cudaMemcpyAsync(r, b, vbytes, cudaMemcpyDeviceToDevice, s));
+  } else {
+    ApplyArgs<double> a{};
+    a.u = x;
+    a.f = b;
+    a.out = r;
+    apply<double, D, R, M_RES>(c, p, o64, 0, a, c->active, s);
+  }
+  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, ln.part, N, c->active));
+  reduce<R>(c, ln.part, nb, ln.o_bn, s);
+  CK(cudaMemcpyAsync(bn.data(), ln.o_bn, (size_t)B * R * sizeof(double), cudaMemcpyDeviceToHost, s));
+  int used = 0;
+  for (int outer = 0;; ++outer) {
+    KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(r, r, ln.part, N, live));
+    reduce<R>(c, ln.part, nb, ln.o_rr, s);
+    KL(c, s, k_outer_check<<<nblk(B), kThreads, 0, s>>>(ln.o_rr, ln.o_bn, rtol * rtol, ln.o_scale, ln.o_inv,
+                                                        ln.o_done, ln.o_run, live, B, R));
+    CK(cudaMemcpyAsync(rr.data(), ln.o_rr, (size_t)B * R * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(done.data(), ln.o_done, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // the inner tolerance: the default, or looser when every unfinished load
+    // case needs less (0.5 x the reduction that reaches rtol)
+    double need = 1.0;
+    bool any = false;
+    for (int b = 0; b < B; ++b) {
+      if (!act[b] || broken[b]) continue;
+      if (done[b]) {
+        status[b] = MAPLE_CELL_CONVERGED;
+        continue;
+      }
+      any = true;
+      for (int k = 0; k < R; ++k) {
+        const double v = rr[(size_t)b * R + k];
+        if (v > rtol * rtol * bn[(size_t)b * R + k] && v > 0) need = std::min(need, rtol * std::sqrt(bn[(size_t)b * R + k] / v));
+      }
+    }
+    if (!any || used >= maxit || outer >= kMaxOuter) break;
+    const double tol = std::max(c->inner_rtol, 0.5 * need);
+    KL(c, s, k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, p.b32, ln.o_scale, N, ln.o_run));
+    pcg<float, D, R>(c, p, o32, p.b32, true, tol, maxit - used, ln.o_run, s);
+    CK(cudaMemcpyAsync(it_in.data(), ln.sc.iters, B * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(dn.data(), ln.sc.done, (size_t)B * R * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    bool newly_broken = false;
+    int most = 0;
+    for (int b = 0; b < B; ++b) {
+      if (!act[b] || broken[b] || done[b]) continue;
+      iters[b] += it_in[b];
+      most = std::max(most, it_in[b]);
+      for (int k = 0; k < R; ++k)
+        if (dn[(size_t)b * R + k] == 2) {
+          broken[b] = 1;
+          status[b] = MAPLE_CELL_BREAKDOWN;
+          newly_broken = true;
+        }
+    }
+    used += std::max(most, 1);
+    if (newly_broken) {
+      std::vector<int> lv(B);
+      for (int b = 0; b < B; ++b) lv[b] = act[b] && !broken[b];
+      CK(cudaMemcpyAsync(live, lv.data(), B * sizeof(int), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(ln.o_run, lv.data(), B * sizeof(int), cudaMemcpyHostToDevice, s));
+      // lv is read by the copies above before it goes out of scope
+      CK(cudaStreamSynchronize(s));
+    }
+    // x += ||r|| e ; r = b - A x (FP64)
+    KL(c, s, k_add_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(x, o32.x, ln.o_inv, N, ln.o_run));
+    ApplyArgs<double> a{};
+    a.u = x;
+    a.f = b;
+    a.out = r;
+    apply<double, D, R, M_RES>(c, p, o64, 0, a, ln.o_run, s);
+  }
 }
 
 static void ensure_prec(maple_ctx* c, int phys, int prec);
@@ -1004,8 +1116,12 @@ static void solve_phys(maple_ctx* c, int phys, int prec, const double* F, double
     CK(cudaMemcpyAsync(x64, o.x, vb64, cudaMemcpyDeviceToDevice, s));
     read_outcome(c, R, it, st, s);
   } else {
-    pcg_mixed<D, R>(c, p, F, x64, x_zero, rtol, maxit, s);
-    read_outcome(c, R, it, st, s);
+    if (c->mixed_mode == MAPLE_MIXED_REFINE) {
+      pcg_refine<D, R>(c, p, F, x64, x_zero, rtol, maxit, it, st, s);
+    } else {
+      pcg_mixed<D, R>(c, p, F, x64, x_zero, rtol, maxit, s);
+      read_outcome(c, R, it, st, s);
+    }
     // Fallback: a cell whose mixed-precision solve broke down is solved again
     // in plain FP64 MG-PCG (FP64 hierarchy built for those cells only) from its
     // last iterate, or from zero when that iterate is not finite or when the
@@ -1095,6 +1211,7 @@ static void ensure_prec(maple_ctx* c, int phys, int prec) {
       const size_t n = (size_t)c->B * nodes(c->n[0]) * p.R * p.D;
       p.p64 = dnew<double>(c, n);
       p.q64 = dnew<double>(c, n);
+      p.b32 = dnew<float>(c, n);
     }
   }
 }
@@ -1355,6 +1472,7 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
         L.sc.bnorm2 = dnew<double>(c, B * 6);
         L.sc.alpha = dnew<double>(c, B * 6);
         L.sc.beta = dnew<double>(c, B * 6);
+        L.sc.rtol2 = dnew<double>(c, 1);
         L.sc.done = dnew<int>(c, B * 6);
         L.sc.cell_done = dnew<int>(c, B);
         L.sc.iters = dnew<int>(c, B);
@@ -1365,6 +1483,7 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
         L.o_inv = dnew<double>(c, B * 6);
         L.o_done = dnew<int>(c, B);
         L.o_run = dnew<int>(c, B);
+        L.o_live = dnew<int>(c, B);
         L.breakdown = dnew<int>(c, 1);
         CK(cudaMemset(L.breakdown, 0, sizeof(int)));
         CK(cudaMallocHost(&L.h_flags, B * sizeof(int)));
@@ -1659,6 +1778,14 @@ int maple_set_tail_fused(maple_ctx* c, int enable) {
   });
 }
 
+int maple_set_mixed_mode(maple_ctx* c, int mode) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(mode == MAPLE_MIXED_FLEXIBLE || mode == MAPLE_MIXED_REFINE, "unknown mixed-precision mode");
+    c->mixed_mode = mode;
+  });
+}
+
 int maple_set_coarse_degree(maple_ctx* c, int deg) {
   return guarded([&] {
     require(c != nullptr, "ctx is NULL");
@@ -1832,6 +1959,42 @@ int maple_matvec(maple_ctx* c, int phys, const double* rho, const double* u, dou
       apply<double, 3, 6, M_MV>(c, p, o, 0, a, c->active, S(s));
     else
       apply<double, 1, 3, M_MV>(c, p, o, 0, a, c->active, S(s));
+  });
+}
+
+int maple_get_level_elements(maple_ctx* c, int phys, int level, double* out, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && out != nullptr, "NULL argument");
+    require(phys == MAPLE_ELASTIC || phys == MAPLE_THERMAL, "unknown physics");
+    require(level >= 1 && level < c->L, "level must be in [1, levels)");
+    Phys& p = c->ph[phys];
+    require(p.built, "no hierarchy built for this physics (call maple_set_density first)");
+    const size_t k = 8 * (size_t)p.D;
+    CK(cudaMemcpyAsync(out, p.KE[level], (size_t)c->B * nodes(c->n[level]) * k * k * sizeof(double),
+                       cudaMemcpyDeviceToDevice, S(s)));
+  });
+}
+
+int maple_transfer(int op, int nc, int K, int ncells, const double* in, double* out, maple_stream_t s) {
+  return guarded([&] {
+    require(in && out && in != out, "in and out must be distinct non-NULL pointers");
+    require(op == MAPLE_RESTRICT || op == MAPLE_PROLONG_ADD, "unknown transfer");
+    require(nc >= 2 && ncells >= 1 && ncells <= 65535, "nc must be >= 2 and ncells in [1, 65535]");
+    require(K == 3 || K == 18, "K must be 3 (thermal fields) or 18 (elastic fields)");
+    cudaStream_t st = S(s);
+    const dim3 g = g2((size_t)nodes(nc) * K, ncells);
+    if (op == MAPLE_RESTRICT) {
+      if (K == 3)
+        k_restrict<double, 3><<<g, kThreads, 0, st>>>(in, out, nc, nullptr);
+      else
+        k_restrict<double, 18><<<g, kThreads, 0, st>>>(in, out, nc, nullptr);
+    } else {
+      if (K == 3)
+        k_prolong_add<double, 3><<<g, kThreads, 0, st>>>(in, out, nc, nullptr);
+      else
+        k_prolong_add<double, 18><<<g, kThreads, 0, st>>>(in, out, nc, nullptr);
+    }
+    CKL();
   });
 }
 

@@ -170,6 +170,25 @@ def test_r16_matches_reference(lib, golden):
     c.close()
 
 
+@pytest.mark.parametrize("r,fixtures", [(8, ("homog_r8_s0.npz", "homog_r8_s1.npz")), (16, ("homog_r16_s0.npz",))])
+def test_refinement_mode_matches_reference(lib, golden, r, fixtures):
+    """The FP32-inner-PCG / FP64-refinement form of the mixed solve reaches the
+    reference's converged C^H and kappa^H like the flexible form."""
+    from maple_b200.core import HomogenizationContext
+    gs = [golden(f) for f in fixtures]
+    c = HomogenizationContext(r, ncells=len(gs))
+    c.set_mixed_mode("refine")
+    rho = T(np.stack([simp(g["x"]) for g in gs]))
+    for phys, key in (("elastic", "CH"), ("thermal", "kappa")):
+        c.set_density(phys, rho, "mixed")
+        info = c.solve(phys, "mixed", rtol=1e-12, maxit=500)
+        assert (info.status == 1).all(), info
+        H = c.homogenize(phys).cpu().numpy()
+        for b, g in enumerate(gs):
+            assert rel(H[b], g[key]) < 1e-9, (phys, b)
+    c.close()
+
+
 def test_solid_cell_known_answer(lib):
     from maple_b200.core import HomogenizationContext
     c = HomogenizationContext(8, ncells=1)
@@ -435,3 +454,45 @@ def test_symmetric_oc_step_trajectory(lib, golden, spec):
         assert abs(float(out["stats"][0, 0]) - dx.max()) < 1e-14 and abs(float(out["stats"][0, 1]) - dx.mean()) < 1e-14
         x = out["x_next"].clone()
     ctx.close()
+
+
+@pytest.mark.parametrize("r", [8, 16])
+def test_coarse_element_matrices_match_oracle(lib, r):
+    """Every level's Galerkin element matrices (k_level1_elements,
+    k_coarsen_elements) against the oracle's per-coarse-element P^T K P
+    (utils/EBE_GMG.py:226-337, utils/EBE_GMG_scalar.py:135-230)."""
+    from maple_b200.core import HomogenizationContext
+    xs = [O.seed_density(s, r, 2.0, 0.3).reshape(-1) for s in (3, 4)]
+    rho = np.stack([simp(x) for x in xs])
+    c = HomogenizationContext(r, ncells=2)
+    el = O.Elements(r)
+    for phys, d in (("elastic", 3), ("thermal", 1)):
+        c.set_density(phys, T(rho), "mixed" if r == 16 else "fp64")
+        Ke0 = el.get(d)[0]
+        for b in range(2):
+            ke, n = rho[b].reshape(-1, 1, 1) * Ke0[None], r
+            for level in range(1, c.levels):
+                ke = O.coarsen_elements(ke, n, d)
+                n //= 2
+                got = c.level_elements(phys, level)[b].cpu().numpy()
+                assert rel(got, ke) < 1e-12, (phys, b, level)
+    c.close()
+
+
+@pytest.mark.parametrize("nc,K", [(2, 3), (4, 18), (8, 3)])
+def test_grid_transfers_match_oracle_prolongation(lib, nc, K):
+    """k_restrict and k_prolong_add against the oracle's assembled periodic
+    trilinear P (utils/EBE_GMG.py:38-79, 531-647), element by element."""
+    from maple_b200.core import transfer
+    rng = np.random.default_rng(nc * 100 + K)
+    nf = 2 * nc
+    P = O.prolongation(nf, 1)  # per component: the same weights for every field
+    fine = rng.standard_normal((2, K, nf ** 3))
+    coarse = rng.standard_normal((2, K, nc ** 3))
+    base = rng.standard_normal((2, K, nf ** 3))
+    rc = transfer("restrict", T(fine)).cpu().numpy()
+    uf = transfer("prolong_add", T(coarse), out=T(base)).cpu().numpy()
+    for b in range(2):
+        for k in range(K):
+            assert rel(rc[b, k], P.T @ fine[b, k]) < 1e-14, (b, k)
+            assert rel(uf[b, k], base[b, k] + P @ coarse[b, k]) < 1e-14, (b, k)
