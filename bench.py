@@ -349,11 +349,15 @@ def run_maple(args, rank, world, local_rank):
 
 # ---------------------------------------------------------------------------
 # CPU path: the oracle's multithreaded C restatement of the reference's
-# algorithm (V-cycles with 8-colour Gauss-Seidel to the relative residual,
-# energy sums, adjoint sensitivities, filter, OC bisection) on every host core.
-# The reference itself is Python that lives outside this repository, so it
-# cannot run on the measuring host; oracle/port.c is pinned against the numpy
-# oracle, which is pinned against the reference's own outputs.
+# multigrid (Galerkin hierarchy, V-cycles with 8-colour Gauss-Seidel), energy
+# sums, adjoint sensitivities, filter and OC bisection on every host core.
+# The reference's plain V-cycle iteration stalls near a relative residual of
+# 2e-7 on designs with near-void regions (32^3, iteration 41 of the plain FP64
+# configuration), so the V-cycle preconditions a flexible CG here, as on the
+# GPU, and every solve reaches the benchmark tolerance.  The reference itself
+# is Python that lives outside this repository, so it cannot run on the
+# measuring host; oracle/port.c is pinned against the numpy oracle, which is
+# pinned against the reference's own outputs.
 TRI = {"stiffness": 1 / 3, "shear": 1 / 3, "thermal": 1 / 3}
 
 
@@ -373,12 +377,13 @@ def cpu_baseline(args):
     x = seeded_design(0, args.res, sigma=args.res / 16.0, vf=0.25).reshape(-1)
     t = time.perf_counter()
     _, info = port.oc_iteration(x, cell, TRI, volfrac=0.25, move=0.2, xmin=1e-3, filter_k=3, rtol=args.rtol,
-                                max_cycles=1000, warm=False)
+                                max_cycles=1000, warm=False, method="pcg")
     t = time.perf_counter() - t
     return {"value": round(1.0 / t, 6), "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"1 OC iteration of the {args.res}^3 cell (tri-objective, FP64 V-cycles with 8-colour "
-                      f"Gauss-Seidel, {levels} levels, to rtol {args.rtol:g}; {info['cycles_elastic']} elastic + "
-                      f"{info['cycles_thermal']} thermal cycles from a zero start) = {t:.2f} s on {cores} threads"}
+            "sample": f"1 OC iteration of the {args.res}^3 cell (tri-objective, FP64, the reference's V-cycle with "
+                      f"8-colour Gauss-Seidel ({levels} levels) preconditioning CG to rtol {args.rtol:g}; "
+                      f"{info['cycles_elastic']} elastic + {info['cycles_thermal']} thermal iterations from a zero "
+                      f"start) = {t:.2f} s on {cores} threads"}
 
 
 def run_reference(args):
@@ -388,7 +393,8 @@ def run_reference(args):
     from the previous solutions like the GPU arm."""
     port, cell, cores, levels = _cpu_cell(args.res)
     x = seeded_design(0, args.res, sigma=args.res / 16.0, vf=0.25).reshape(-1)
-    kw = dict(volfrac=0.25, move=0.2, xmin=1e-3, filter_k=3, rtol=args.rtol, max_cycles=1000, warm=True)
+    kw = dict(volfrac=0.25, move=0.2, xmin=1e-3, filter_k=3, rtol=args.rtol, max_cycles=1000, warm=True,
+              method="pcg")
     for _ in range(args.warmup):
         x, _ = port.oc_iteration(x, cell, TRI, **kw)
     ts, cyc = [], []
@@ -399,14 +405,15 @@ def run_reference(args):
         cyc.append(info["cycles_elastic"] + info["cycles_thermal"])
     tot = sum(ts)
     value = args.steps / tot
-    sample = (f"{args.steps} OC iterations of the {args.res}^3 cell after {args.warmup} untimed ones, FP64 V-cycles "
-              f"with 8-colour Gauss-Seidel ({levels} levels) to rtol {args.rtol:g}, warm-started; {cores} threads")
+    sample = (f"{args.steps} OC iterations of the {args.res}^3 cell after {args.warmup} untimed ones, FP64, the "
+              f"reference's V-cycle with 8-colour Gauss-Seidel ({levels} levels) preconditioning CG to rtol "
+              f"{args.rtol:g}, warm-started; {cores} threads")
     return {"metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000 * tot / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": f"OC iteration, {args.res}^3 periodic cell (config 1: precision)",
                        "res": args.res, "rtol": args.rtol, "objective": "(E+G+kappa)/3", "volfrac": 0.25,
-                       "move": 0.2, "filter_k": 3, "mg_levels": levels, "cycles_per_step": cyc},
+                       "move": 0.2, "filter_k": 3, "mg_levels": levels, "cg_iterations_per_step": cyc},
             "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

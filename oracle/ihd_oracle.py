@@ -322,19 +322,45 @@ class Hierarchy:
 
 
 def gmg_solve(hier: Hierarchy, f: np.ndarray, max_iter: int, smooth_iter=(2, 2, 3, 4, 5),
-              coarse_default: int | None = 1, rtol: float = 0.0, u0=None):
+              coarse_default: int | None = 1, rtol: float = 0.0, u0=None, method: str = "vcycle"):
     """V-cycle iteration from u=0 (EBE_GMG.py:758-885).  Returns (u, r, cycles).
     ``rtol`` > 0 stops early once ||r|| <= rtol ||f|| per column (the reference
-    has no test; it runs ``max_iter`` cycles)."""
+    has no test; it runs ``max_iter`` cycles).
+
+    ``method="pcg"``: the same V-cycle (one cycle from zero on the residual)
+    as the preconditioner of a flexible conjugate gradient (Polak-Ribiere
+    beta, per load case); it reaches residuals the plain cycle stalls above on
+    designs with large density contrast.  The converged answer is the same
+    (up to a rigid translation, which C^H ignores)."""
     u = np.zeros_like(f) if u0 is None else u0.copy()
     K = hier.levels[0].K
-    fn = np.linalg.norm(f, axis=0)
+    fn = np.maximum(np.linalg.norm(f, axis=0), 1e-300)
     it = 0
     r = f - K @ u
+    if method == "pcg":
+        if rtol > 0 and np.all(np.linalg.norm(r, axis=0) <= rtol * fn):
+            return u, r, 0
+        z = hier.vcycle(0, np.zeros_like(r), r, smooth_iter, coarse_default)
+        p = z.copy()
+        rz = np.sum(r * z, axis=0)
+        for it in range(1, max_iter + 1):
+            q = K @ p
+            pq = np.sum(p * q, axis=0)
+            alpha = np.where(pq > 0, rz / np.where(pq > 0, pq, 1.0), 0.0)
+            u = u + alpha * p
+            r_old = r
+            r = r - alpha * q
+            if rtol > 0 and np.all(np.linalg.norm(r, axis=0) <= rtol * fn):
+                break
+            z = hier.vcycle(0, np.zeros_like(r), r, smooth_iter, coarse_default)
+            beta = np.where(rz != 0, np.sum(z * (r - r_old), axis=0) / np.where(rz != 0, rz, 1.0), 0.0)
+            rz = np.sum(r * z, axis=0)
+            p = z + beta * p
+        return u, f - K @ u, it
     for it in range(1, max_iter + 1):
         u = hier.vcycle(0, u, f, smooth_iter, coarse_default)
         r = f - K @ u
-        if rtol > 0 and np.all(np.linalg.norm(r, axis=0) <= rtol * np.maximum(fn, 1e-300)):
+        if rtol > 0 and np.all(np.linalg.norm(r, axis=0) <= rtol * fn):
             break
     return u, r, it
 
@@ -508,12 +534,12 @@ def seed_density(seed: int, r: int, sigma: float, vf: float, scale: float = 0.25
 # ---------------------------------------------------------------------------
 def solve_cell(rho: np.ndarray, r: int, elems: Elements | None = None, levels: int = 3,
                max_cycles: int = 200, rtol: float = 1e-12, physics=("elastic", "thermal"),
-               smooth_iter=(2, 2, 3, 4, 5), u0: dict | None = None):
+               smooth_iter=(2, 2, 3, 4, 5), u0: dict | None = None, method: str = "vcycle"):
     """Both physics on one cell: returns dict with CH, kappa, u3, u1 and the
     per-element energies (dC/drho, dkappa/drho).  ``u0`` (keys "u3" / "u1",
     e.g. the previous OC iteration's solutions) is the initial iterate of the
     V-cycles; the converged answer does not depend on it (the reference starts
-    from zero, EBE_GMG.py:851-858)."""
+    from zero, EBE_GMG.py:851-858).  ``method`` as in ``gmg_solve``."""
     elems = elems or Elements(r)
     out = {}
     rho = rho.reshape(-1)
@@ -525,7 +551,7 @@ def solve_cell(rho: np.ndarray, r: int, elems: Elements | None = None, levels: i
         key_u = "u3" if d == 3 else "u1"
         start = None if u0 is None else u0.get(key_u)
         u, res, cyc = gmg_solve(hier, F, max_cycles, smooth_iter,
-                                coarse_default=1 if d == 3 else None, rtol=rtol, u0=start)
+                                coarse_default=1 if d == 3 else None, rtol=rtol, u0=start, method=method)
         H = homogenize(u, rho, Ke0, X0, r, d)
         dH = element_energy(u, Ke0, X0, r, d)
         key = "CH" if d == 3 else "kappa"
@@ -581,15 +607,15 @@ def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal:
                  elems: Elements | None = None, levels: int = 3, rtol: float = 1e-12,
                  max_cycles: int = 200, symmetry: str = "none", lambda_print: float = 0.0,
                  overhang_deg: float = 45.0, lambda_cavity: float = 0.0, cavity: dict | None = None,
-                 u0: dict | None = None):
+                 u0: dict | None = None, method: str = "vcycle"):
     """One OC iteration of main_IHD_v3.py:620-716 with the analytic adjoint in
     place of autograd.  With a symmetry, the solve uses the projected design,
     the gradient is projected (the group average is self-adjoint) and so is
     the updated design.  Penalties (:649-686): J = J_raw - lambda_print *
     P_overhang - lambda_cavity * P_cavity, `cavity` holding cavity_penalty's
     keywords.  ``u0`` is passed to ``solve_cell`` as the solves' initial
-    iterate (``info["res"]`` of the previous iteration serves).  Returns
-    (x_next, info)."""
+    iterate (``info["res"]`` of the previous iteration serves); ``method``
+    selects the solver as in ``gmg_solve``.  Returns (x_next, info)."""
     kind, axes = parse_symmetry(symmetry)
     x = x.reshape(-1)
     xc = np.clip(symmetrize(np.clip(x, xmin, 1.0), r, kind, axes), xmin, 1.0)
@@ -599,7 +625,7 @@ def oc_iteration(x: np.ndarray, r: int, weights: dict, *, volfrac: float, penal:
         phys.append("elastic")
     if "thermal" in weights:
         phys.append("thermal")
-    res = solve_cell(rho, r, elems, levels, max_cycles, rtol, tuple(phys), u0=u0)
+    res = solve_cell(rho, r, elems, levels, max_cycles, rtol, tuple(phys), u0=u0, method=method)
     CH = res.get("CH")
     kap = res.get("kappa")
     J, gC, gK = objective_and_grads(weights, CH if CH is not None else np.eye(6),

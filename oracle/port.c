@@ -177,6 +177,28 @@ static void coarsen(int n, int D, const double* ke, const double* rho, const dou
       }                                                                                                          \
     }                                                                                                            \
   }                                                                                                              \
+  static void matvec_##D(const Level* L, const double* u, double* out) {                                         \
+    const int n = L->n, N = n * n * n;                                                                           \
+    _Pragma("omp parallel for schedule(static)") for (int node = 0; node < N; ++node) {                          \
+      const int x = node / (n * n), y = (node / n) % n, z = node % n;                                            \
+      double acc[D * R];                                                                                         \
+      for (int i = 0; i < D * R; ++i) acc[i] = 0.0;                                                              \
+      const double* s = L->S + (size_t)node * 27 * D * D;                                                        \
+      int k = 0;                                                                                                 \
+      for (int dx = -1; dx <= 1; ++dx)                                                                           \
+        for (int dy = -1; dy <= 1; ++dy)                                                                         \
+          for (int dz = -1; dz <= 1; ++dz, ++k) {                                                                \
+            const double* un = u + (size_t)((wrapi(x + dx, n) * n + wrapi(y + dy, n)) * n + wrapi(z + dz, n)) * D * R; \
+            const double* sk = s + k * D * D;                                                                    \
+            for (int d = 0; d < D; ++d)                                                                          \
+              for (int c = 0; c < D; ++c) {                                                                      \
+                const double a = sk[d * D + c];                                                                  \
+                for (int q = 0; q < R; ++q) acc[d * R + q] += a * un[c * R + q];                                 \
+              }                                                                                                  \
+          }                                                                                                      \
+      for (int i = 0; i < D * R; ++i) out[(size_t)node * D * R + i] = acc[i];                                    \
+    }                                                                                                            \
+  }                                                                                                              \
   static void residual_##D(const Level* L, const double* u, const double* f, double* out) {                      \
     const int n = L->n, N = n * n * n;                                                                           \
     _Pragma("omp parallel for schedule(static)") for (int node = 0; node < N; ++node)                            \
@@ -350,6 +372,84 @@ static void assemble_rhs(int n, int D, int R, const double* rho, const double* F
   }
 }
 
+/* per-column sum of a*b over [N][D][R] */
+static void col_dots(size_t N, int D, int R, const double* a, const double* b, double* out) {
+  for (int q = 0; q < R; ++q) out[q] = 0.0;
+#pragma omp parallel
+  {
+    double loc[6] = {0, 0, 0, 0, 0, 0};
+#pragma omp for schedule(static)
+    for (size_t i = 0; i < N; ++i)
+      for (int d = 0; d < D; ++d)
+        for (int q = 0; q < R; ++q) loc[q] += a[i * D * R + d * R + q] * b[i * D * R + d * R + q];
+#pragma omp critical
+    for (int q = 0; q < R; ++q) out[q] += loc[q];
+  }
+}
+
+/* The V-cycle (one cycle from zero on the residual) as the preconditioner
+ * of a flexible conjugate gradient, per load case (Polak-Ribiere beta): the
+ * oracle's gmg_solve(method="pcg").  Returns the iterations. */
+static int solve_pcg(Hier* H, double* u, const double* f, double rtol, int max_it) {
+  Level* L0 = &H->lv[0];
+  const size_t N = (size_t)L0->n * L0->n * L0->n;
+  const int D = H->D, R = H->R, DR = D * R;
+  const size_t len = N * DR;
+  double *r = (double*)malloc(sizeof(double) * len), *z = (double*)malloc(sizeof(double) * len);
+  double *p = (double*)malloc(sizeof(double) * len), *q = (double*)malloc(sizeof(double) * len);
+  double* ro = (double*)malloc(sizeof(double) * len);
+  double fn[6], rn[6], rz[6], pq[6], zr[6], alpha[6], beta[6];
+  col_norms2(N, D, R, f, fn);
+  residual(L0, D, u, f, r);
+  int it = 0;
+  col_norms2(N, D, R, r, rn);
+  int ok = 1;
+  for (int c = 0; c < R; ++c) ok &= sqrt(rn[c]) <= rtol * fmax(sqrt(fn[c]), 1e-300);
+  if (!(rtol > 0 && ok)) {
+    memset(z, 0, sizeof(double) * len);
+    vcycle(H, 0, z, r);
+    memcpy(p, z, sizeof(double) * len);
+    col_dots(N, D, R, r, z, rz);
+    for (it = 1; it <= max_it; ++it) {
+      if (D == 3)
+        matvec_3(L0, p, q);
+      else
+        matvec_1(L0, p, q);
+      col_dots(N, D, R, p, q, pq);
+      for (int c = 0; c < R; ++c) alpha[c] = pq[c] > 0 ? rz[c] / pq[c] : 0.0;
+      memcpy(ro, r, sizeof(double) * len);
+#pragma omp parallel for schedule(static)
+      for (size_t i = 0; i < N; ++i)
+        for (int k = 0; k < DR; ++k) {
+          const double a = alpha[k % R];
+          u[i * DR + k] += a * p[i * DR + k];
+          r[i * DR + k] -= a * q[i * DR + k];
+        }
+      col_norms2(N, D, R, r, rn);
+      ok = 1;
+      for (int c = 0; c < R; ++c) ok &= sqrt(rn[c]) <= rtol * fmax(sqrt(fn[c]), 1e-300);
+      if (rtol > 0 && ok) break;
+      memset(z, 0, sizeof(double) * len);
+      vcycle(H, 0, z, r);
+#pragma omp parallel for schedule(static)
+      for (size_t i = 0; i < len; ++i) ro[i] = r[i] - ro[i];
+      col_dots(N, D, R, z, ro, zr);
+      for (int c = 0; c < R; ++c) beta[c] = rz[c] != 0 ? zr[c] / rz[c] : 0.0;
+      col_dots(N, D, R, r, z, rz);
+#pragma omp parallel for schedule(static)
+      for (size_t i = 0; i < N; ++i)
+        for (int k = 0; k < DR; ++k) p[i * DR + k] = z[i * DR + k] + beta[k % R] * p[i * DR + k];
+    }
+    if (it > max_it) it = max_it;
+  }
+  free(r);
+  free(z);
+  free(p);
+  free(q);
+  free(ro);
+  return it;
+}
+
 /* V-cycles until every column has ||f - K u|| <= rtol ||f||; returns cycles */
 static int solve(Hier* H, double* u, const double* f, double rtol, int max_cycles) {
   Level* L0 = &H->lv[0];
@@ -476,13 +576,18 @@ int port_threads(int nthreads) {
  * of one r^3 cell.  tabs: Ke3[576] Fe3[144] X03[144] Ke1[64] Fe1[24] X01[24]
  * of the voxel (edge 1/r).  w3: (w_E, w_G, w_kappa).  u3 [N][3][6] / u1
  * [N][1][3]: initial iterates when warm3 / warm1, else zero; they return
- * the solutions.  out: J, C^H[36], kappa[9], elastic cycles, thermal cycles,
- * max|dx|, mean|dx| (50 values).  Returns 0, or 1 on a bad argument.
+ * the solutions.  method 0: V-cycles to rtol (the reference's iteration);
+ * 1: the V-cycle as the preconditioner of a flexible CG.  out: J, C^H[36],
+ * kappa[9], elastic and thermal cycles (or CG iterations), max|dx|,
+ * mean|dx| (50 values).  Returns 0, or 1 on a bad argument.
  */
 int port_oc_iteration(int r, int levels, const double* tabs, const double* x, const double* w3, double vf,
                       double penal, double rho_min, double move, double xmin, int filter_k, double rtol,
-                      int max_cycles, double* u3, int warm3, double* u1, int warm1, double* x_next, double* out) {
-  if (r < 2 || r % 2 || levels < 1 || levels > 8 || (filter_k > 1 && filter_k % 2 == 0)) return 1;
+                      int max_cycles, int method, double* u3, int warm3, double* u1, int warm1, double* x_next,
+                      double* out) {
+  if (r < 2 || r % 2 || levels < 1 || levels > 8 || (filter_k > 1 && filter_k % 2 == 0) || method < 0 ||
+      method > 1)
+    return 1;
   const int N = r * r * r;
   const double *Ke3 = tabs, *Fe3 = tabs + 576, *X03 = tabs + 720, *Ke1 = tabs + 864, *Fe1 = tabs + 928,
                *X01 = tabs + 952;
@@ -511,7 +616,7 @@ int port_oc_iteration(int r, int levels, const double* tabs, const double* x, co
     build(&H, r, levels, D, R, rho, Ke0);
     double* F = (double*)malloc(sizeof(double) * (size_t)N * D * R);
     assemble_rhs(r, D, R, rho, Fe0, F);
-    cyc[ph] = solve(&H, u, F, rtol, max_cycles);
+    cyc[ph] = method == 1 ? solve_pcg(&H, u, F, rtol, max_cycles) : solve(&H, u, F, rtol, max_cycles);
     free(F);
     destroy(&H);
     double* en = (double*)malloc(sizeof(double) * (size_t)N * R * R);

@@ -41,8 +41,8 @@ def load():
         lib.port_threads.argtypes = [C.c_int]
         lib.port_oc_iteration.restype = C.c_int
         lib.port_oc_iteration.argtypes = [C.c_int, C.c_int, P, P, P, C.c_double, C.c_double, C.c_double,
-                                          C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, P, C.c_int, P,
-                                          C.c_int, P, P]
+                                          C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, P, C.c_int,
+                                          P, C.c_int, P, P]
         _lib = lib
     return _lib
 
@@ -74,9 +74,12 @@ class Cell:
 
 def oc_iteration(x, cell: Cell, weights: dict, *, volfrac: float, penal: float = 3.0, rho_min: float = 1e-9,
                  move: float = 0.2, xmin: float = 1e-3, filter_k: int = 3, rtol: float = 1e-12,
-                 max_cycles: int = 200, warm: bool = False):
+                 max_cycles: int = 200, warm: bool = False, method: str = "vcycle"):
     """One OC iteration of the cell's design x (N,); returns (x_next, info)
-    with J, CH, kappa, cycles_elastic, cycles_thermal, dx_max, dx_mean."""
+    with J, CH, kappa, cycles_elastic, cycles_thermal, dx_max, dx_mean.
+    ``method`` as in ``ihd_oracle.gmg_solve`` ("vcycle" or "pcg")."""
+    if method not in ("vcycle", "pcg"):
+        raise ValueError(f"unknown method {method!r}")
     lib = load()
     r = cell.r
     x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
@@ -85,7 +88,7 @@ def oc_iteration(x, cell: Cell, weights: dict, *, volfrac: float, penal: float =
     out = np.zeros(50)
     rc = lib.port_oc_iteration(r, cell.levels, _ptr(cell.tabs), _ptr(x), _ptr(w3), float(volfrac), float(penal),
                                float(rho_min), float(move), float(xmin), int(filter_k), float(rtol), int(max_cycles),
-                               _ptr(cell.u3), int(warm and cell.solved[0]), _ptr(cell.u1),
+                               1 if method == "pcg" else 0, _ptr(cell.u3), int(warm and cell.solved[0]), _ptr(cell.u1),
                                int(warm and cell.solved[1]), _ptr(xn), _ptr(out))
     if rc != 0:
         raise ValueError("port_oc_iteration: bad argument")

@@ -252,9 +252,14 @@ def config0_fixtures(Ob, homogenize):
     converged to a relative residual of 1e-12 (warm-started from the previous
     iteration; the converged answer is independent of the start); every
     iteration's J, C^H, kappa^H and |dx| statistics and the designs at
-    iterations 1, 10, 49 and 50 are stored.  The reference's own FP64 GMG
-    solvers then evaluate C^H, kappa^H and J at the oracle's designs of
-    iterations 0, 1, 10 and 49 (the pins of the oracle trajectory)."""
+    iterations 1, 10, 25, 49 and 50 are stored.  The oracle's solves are its
+    V-cycle used as the preconditioner of a flexible CG: the plain V-cycle
+    stalls near a relative residual of 2e-7 from iteration 41 on (the design
+    then holds near-void regions), the preconditioned one converges.  The
+    reference's own FP64 GMG solvers (90 V-cycles) then evaluate C^H, kappa^H
+    and J at the oracle's designs of iterations 0, 1, 10, 25 and 49, with the
+    relative residual they reach (the pins of the oracle trajectory where
+    that residual is small)."""
     import time
     O = _oracle()
     r, vf, spec = 32, 0.25, "stiffness:0.5,thermal:0.5"
@@ -267,10 +272,10 @@ def config0_fixtures(Ob, homogenize):
     prev = None
     t0 = time.time()
     for it in range(50):
-        if it in (1, 10, 49):
+        if it in (1, 10, 25, 49):
             xs[it] = x.copy()
         xn, info = O.oc_iteration(x, r, w, volfrac=vf, move=0.2, elems=el, levels=5, rtol=1e-12,
-                                  max_cycles=400, u0=prev)
+                                  max_cycles=400, u0=prev, method="pcg")
         prev = info["res"]
         Js.append(info["J"])
         CHs.append(info["CH"])
@@ -285,7 +290,7 @@ def config0_fixtures(Ob, homogenize):
                oracle_relres=np.array(relres), x50=x.copy())
     for it, xv in xs.items():
         rec[f"x{it}"] = xv
-    for it in (0, 1, 10, 49):
+    for it in (0, 1, 10, 25, 49):
         xv = rec["x0"] if it == 0 else xs[it]
         CH, kap, J, rr = _reference_terms(Ob, homogenize, r, xv, spec, cycles=90, levels=5)
         rec[f"ref_CH_{it}"], rec[f"ref_kappa_{it}"], rec[f"ref_J_{it}"], rec[f"ref_relres_{it}"] = CH, kap, J, rr

@@ -15,19 +15,21 @@ def _threads():
     P.set_threads(2)
 
 
-@pytest.mark.parametrize("r,levels,spec", [
-    (8, 3, "stiffness:0.5,thermal:0.5"),
-    (16, 4, "stiffness:0.3333333333333333,shear:0.3333333333333333,thermal:0.3333333333333333"),
-    (8, 2, "shear"),
+@pytest.mark.parametrize("r,levels,spec,method", [
+    (8, 3, "stiffness:0.5,thermal:0.5", "vcycle"),
+    (16, 4, "stiffness:0.3333333333333333,shear:0.3333333333333333,thermal:0.3333333333333333", "vcycle"),
+    (8, 2, "shear", "vcycle"),
+    (16, 4, "stiffness:0.5,thermal:0.5", "pcg"),
 ])
-def test_port_follows_the_oracle(r, levels, spec):
+def test_port_follows_the_oracle(r, levels, spec, method):
     w = O.parse_objective_spec(spec)
     x = O.seed_density(1, r, 2.0, 0.3).reshape(-1)
     cell = P.Cell(r, levels)
     prev = None
     for it in range(2):
-        xp, ip = P.oc_iteration(x, cell, w, volfrac=0.3, rtol=1e-12, max_cycles=400, warm=True)
-        xo, io = O.oc_iteration(x, r, w, volfrac=0.3, levels=levels, rtol=1e-12, max_cycles=400, u0=prev)
+        xp, ip = P.oc_iteration(x, cell, w, volfrac=0.3, rtol=1e-12, max_cycles=400, warm=True, method=method)
+        xo, io = O.oc_iteration(x, r, w, volfrac=0.3, levels=levels, rtol=1e-12, max_cycles=400, u0=prev,
+                                method=method)
         prev = io["res"]
         assert abs(ip["J"] - io["J"]) <= 1e-12 * abs(io["J"]), it
         if io["CH"] is not None:
