@@ -353,6 +353,15 @@ int maple_nn_conv3d_padded(const void* in, const void* W, const float* bias, con
                            float* out_f32, int B, int n, int cin, int cout, int ksize, int relu, int padding,
                            maple_stream_t stream);
 
+/* The convolutions of maple_nn_conv3d(_padded) run as an implicit GEMM on the
+ * fifth-generation tensor cores (tcgen05.mma, FP32 accumulator in tensor
+ * memory) when cin is a multiple of 8 and in / W are 16-byte aligned, else on
+ * warp-level MMA.  Their pipeline waits are bounded: a wait that runs out
+ * ends the kernel and sets a device flag.  maple_nn_wait_status waits for the
+ * stream, returns that flag in *timed_out_host (0: no wait ran out since the
+ * last call) and clears it.  No counterpart in the reference. */
+int maple_nn_wait_status(int* timed_out_host, maple_stream_t stream);
+
 /* dW += sum over cells and voxels of in(shifted by tap) x dz (FP32 [taps][cin][cout]);
  * db += sum of dz (nullable). */
 int maple_nn_conv3d_wgrad(const void* in, const void* dz, float* dW, float* db, int B, int n, int cin, int cout,

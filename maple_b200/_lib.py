@@ -94,6 +94,7 @@ SIGNATURES = {
     "maple_nn_prolong_fields": (_I, [_P, _P, _I, _I, _I, _P]),
     "maple_nn_restrict_density": (_I, [_P, _P, _I, _I, _I, _P]),
     "maple_nn_conv3d_padded": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _P]),
+    "maple_nn_wait_status": (_I, [_IP, _P]),
     # Stage-II density generator and warm-start post-processing
     "maple_gen_last_error_string": (C.c_char_p, []),
     "maple_gen_launch_count": (C.c_ulonglong, []),

@@ -24,6 +24,7 @@
 #include <string>
 
 #include "../../include/maple_b200.h"
+#include "tcgen05.cuh"
 
 namespace maple_nn {
 
@@ -141,6 +142,171 @@ __global__ void __launch_bounds__(NT) k_conv3d(const bf16* __restrict__ in, cons
     if (out) out[o] = __float2bfloat16(val);
     if (out_f32) out_f32[o] = val;
   }
+}
+
+// ---------------------------------------------------------------------------
+// The same convolution on the fifth-generation tensor cores (tcgen05):
+// an implicit GEMM whose rows are 128 output voxels, columns the output
+// channels (one tile of up to 256, zero-padded to a multiple of 16) and
+// reduction (tap, 16 input channels) steps.  Per step, the 128 threads gather
+// the A tile (each thread one voxel row: the tap's periodic or zero-padded
+// neighbour, two 16-byte chunks of 8 channels) and the B tile (weights, the
+// output channel contiguous: MN-major) with cp.async into one of TC_STAGES
+// shared-memory stages; one thread issues the step's tcgen05.mma (M = 128,
+// K = 16) into an FP32 accumulator in tensor memory and commits it to the
+// stage's mbarrier, which releases the stage for the load TC_STAGES steps
+// later.  The epilogue reads the accumulator rows back (tcgen05.ld, warp w
+// lanes 32w..32w+31) and applies bias, residual and ReLU as k_conv3d.
+// Every mbarrier wait is bounded; a wait that runs out sets g_nn_wait_err,
+// waits (bounded) for the issued MMAs and frees the tensor memory.
+// Requires cin % 8 == 0 (16-byte channel chunks).
+// ---------------------------------------------------------------------------
+constexpr int TC_BM = 128, TC_THREADS = 128, TC_STAGES = 4, TC_BN_MAX = 256;
+constexpr long long kTcPolls = 1LL << 24;
+__device__ int g_nn_wait_err;
+
+__host__ __device__ inline int tc_bn(int cout_left) {
+  const int c = cout_left < TC_BN_MAX ? cout_left : TC_BN_MAX;
+  return (c + 15) / 16 * 16;
+}
+__host__ __device__ inline int tc_tmem_cols(int bn) {
+  int c = 32;
+  while (c < bn) c <<= 1;
+  return c;
+}
+__host__ __device__ inline size_t tc_stage_bytes(int bn) { return (size_t)TC_BM * 32 + (size_t)bn * 32; }
+
+__device__ __forceinline__ void cp_async16_zfill(void* sdst, const void* gsrc, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(n) : "memory");
+}
+
+__global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict__ in, const bf16* __restrict__ W,
+                                                          const float* __restrict__ bias, const bf16* res, bf16* out,
+                                                          float* __restrict__ out_f32, int n, int cin, int cout,
+                                                          int taps, int relu, int zero_pad) {
+  using namespace maple_tc;
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  __shared__ __align__(8) uint64_t mma_bar[TC_STAGES];
+  __shared__ __align__(8) uint64_t done_bar;
+  __shared__ uint32_t tslot;
+  const int N = n * n * n;
+  const int b = blockIdx.z;
+  const int v0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN_MAX;
+  const int BN = tc_bn(cout - n0);
+  const uint32_t ncols = (uint32_t)tc_tmem_cols(BN);
+  const size_t stage = tc_stage_bytes(BN);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kc = (cin + 15) / 16, KS = taps * kc;
+  const bf16* inb = in + (size_t)b * N * cin;
+  const bool wvec = (cout % 8) == 0;
+  if (warp == 0) tmem_alloc(&tslot, ncols);
+  if (tid == 0) {
+    for (int i = 0; i < TC_STAGES; ++i) mbar_init(&mma_bar[i], 1);
+    mbar_init(&done_bar, 1);
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tslot;
+  const uint32_t idesc = idesc_bf16_f32(TC_BM, BN, 1);
+  const int m = tid;  // this thread's A row
+  const int v = v0 + m;
+  int issued = 0;     // MMA steps issued (thread 0)
+  bool timed_out = false;
+  for (int t = 0; t <= KS; ++t) {
+    if (t < KS) {
+      const int st = t % TC_STAGES;
+      if (t >= TC_STAGES) {
+        const bool ok = mbar_wait(&mma_bar[st], (uint32_t)((t / TC_STAGES - 1) & 1), kTcPolls);
+        if (__syncthreads_or(!ok)) {
+          timed_out = true;
+          break;
+        }
+      }
+      uint8_t* sA = tc_smem + st * stage;
+      uint8_t* sB = sA + TC_BM * 32;
+      const int tap = t / kc, c0 = (t - tap * kc) * 16;
+      int dx, dy, dz;
+      tap_offsets(tap, taps, dx, dy, dz);
+      int q = -1;
+      if (v < N) q = zero_pad ? neighbour_zp(v, n, dx, dy, dz) : neighbour(v, n, dx, dy, dz);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const bool ok = q >= 0 && c0 + 8 * h < cin;
+        const bf16* src = ok ? inb + (size_t)q * cin + c0 + 8 * h : inb;
+        cp_async16_zfill(sA + (m >> 3) * 256 + h * 128 + (m & 7) * 16, src, ok);
+      }
+      const int groups = BN / 8;
+      if (wvec) {
+        for (int i = tid; i < 16 * groups; i += TC_THREADS) {
+          const int k = i / groups, g = i - k * groups;
+          const int ci = c0 + k, co = n0 + 8 * g;
+          const bool ok = ci < cin && co < cout;
+          const bf16* src = ok ? W + ((size_t)tap * cin + ci) * cout + co : W;
+          cp_async16_zfill(sB + mnmajor_offset(8 * g, k, 128, 256), src, ok);
+        }
+      } else {
+        for (int i = tid; i < 16 * BN; i += TC_THREADS) {
+          const int k = i / BN, j = i - k * BN;
+          const int ci = c0 + k, co = n0 + j;
+          bf16 val = __float2bfloat16(0.0f);
+          if (ci < cin && co < cout) val = W[((size_t)tap * cin + ci) * cout + co];
+          *reinterpret_cast<bf16*>(sB + mnmajor_offset(j, k, 128, 256)) = val;
+        }
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    if (t >= 1) {
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        fence_after_sync();
+        const int s = t - 1, st = s % TC_STAGES;
+        const uint32_t a = smem_u32(tc_smem + st * stage);
+        mma_bf16(tmem, smem_desc(a, 128, 256), smem_desc(a + TC_BM * 32, 128, 256), idesc, s > 0 ? 1u : 0u);
+        mma_commit(&mma_bar[st]);
+        issued = s + 1;
+      }
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  // every issued MMA has completed once done_bar flips (also after a timeout)
+  if (tid == 0) {
+    if (issued == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&done_bar)) : "memory");
+    else mma_commit(&done_bar);
+  }
+  const bool fin = mbar_wait(&done_bar, 0, kTcPolls);
+  const bool bad = __syncthreads_or(timed_out || !fin);
+  if (bad) {
+    if (tid == 0) atomicExch(&g_nn_wait_err, 1);
+  } else {
+    fence_after_sync();
+    for (int c = 0; c < BN; c += 8) {
+      float acc[8];
+      tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c, acc);
+      const int vv = v0 + 32 * warp + lane;
+      if (vv < N) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int co = n0 + c + j;
+          if (co >= cout) continue;
+          const size_t o = ((size_t)b * N + vv) * cout + co;
+          float val = acc[j];
+          if (bias) val += bias[co];
+          if (res) val += __bfloat162float(res[o]);
+          if (relu) val = fmaxf(val, 0.0f);
+          if (out) out[o] = __float2bfloat16(val);
+          if (out_f32) out_f32[o] = val;
+        }
+      }
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, ncols);
 }
 
 // dW[tap][ci][co] += sum_{b,v} in[b][nbr(v,tap)][ci] * dz[b][v][co]  (FP32 atomics)
@@ -626,10 +792,28 @@ int maple_nn_conv3d_padded(const void* in, const void* W, const float* bias, con
     if (padding != MAPLE_NN_PAD_CIRCULAR && padding != MAPLE_NN_PAD_ZEROS) return "unknown padding mode";
     if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) != 0) return "input must be 16-byte aligned";
     const int N = n * n * n;
+    const int taps = ksize == 3 ? 27 : 1, zp = padding == MAPLE_NN_PAD_ZEROS ? 1 : 0;
+    if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(W) & 15) == 0) {
+      // tensor-core (tcgen05) implicit GEMM
+      const int bn0 = tc_bn(cout);
+      const size_t smem = TC_STAGES * tc_stage_bytes(bn0);
+      static bool attr_set[128] = {};
+      int dev = 0;
+      CKN(cudaGetDevice(&dev));
+      if (dev >= 0 && dev < 128 && !attr_set[dev]) {
+        CKN(cudaFuncSetAttribute(k_conv3d_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(TC_STAGES * tc_stage_bytes(TC_BN_MAX))));
+        attr_set[dev] = true;
+      }
+      dim3 g((N + TC_BM - 1) / TC_BM, (cout + TC_BN_MAX - 1) / TC_BN_MAX, B);
+      NNL((k_conv3d_tc<<<g, TC_THREADS, smem, Sx(s)>>>((const bf16*)in, (const bf16*)W, bias, (const bf16*)res,
+                                                        (bf16*)out, out_f32, n, cin, cout, taps, relu, zp)));
+      return nullptr;
+    }
+    // other channel counts: the warp-level MMA kernel
     dim3 g((N + BM - 1) / BM, (cout + BN - 1) / BN, B);
     NNL((k_conv3d<<<g, NT, 0, Sx(s)>>>((const bf16*)in, (const bf16*)W, bias, (const bf16*)res, (bf16*)out, out_f32,
-                                       n, cin, cout, ksize == 3 ? 27 : 1, relu,
-                                       padding == MAPLE_NN_PAD_ZEROS ? 1 : 0)));
+                                       n, cin, cout, taps, relu, zp)));
     return nullptr;
   });
 }
@@ -637,6 +821,20 @@ int maple_nn_conv3d_padded(const void* in, const void* W, const float* bias, con
 int maple_nn_conv3d(const void* in, const void* W, const float* bias, const void* res, void* out, float* out_f32,
                     int B, int n, int cin, int cout, int ksize, int relu, maple_stream_t s) {
   return maple_nn_conv3d_padded(in, W, bias, res, out, out_f32, B, n, cin, cout, ksize, relu, MAPLE_NN_PAD_CIRCULAR, s);
+}
+
+int maple_nn_wait_status(int* timed_out_host, maple_stream_t s) {
+  return nn_guard([&]() -> const char* {
+    if (!timed_out_host) return "NULL argument";
+    int v = 0;
+    CKN(cudaMemcpyFromSymbolAsync(&v, g_nn_wait_err, sizeof(int), 0, cudaMemcpyDeviceToHost, Sx(s)));
+    CKN(cudaStreamSynchronize(Sx(s)));
+    const int zero = 0;
+    if (v) CKN(cudaMemcpyToSymbolAsync(g_nn_wait_err, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, Sx(s)));
+    CKN(cudaStreamSynchronize(Sx(s)));
+    *timed_out_host = v;
+    return nullptr;
+  });
 }
 
 int maple_nn_conv3d_wgrad(const void* in, const void* dz, float* dW, float* db, int B, int n, int cin, int cout,

@@ -56,6 +56,33 @@ def test_conv3d_forward_matches_torch(lib, n, cin, cout, k, relu, B):
     assert (out.float().cpu() - ref).abs().max() <= 2 ** -7 * float(ref.abs().max())
 
 
+@pytest.mark.parametrize("n,cin,cout,pad,B", [(8, 32, 256, 0, 2), (4, 16, 300, 1, 2), (6, 40, 72, 1, 1)])
+def test_conv3d_tensor_core_tiles_match_torch(lib, n, cin, cout, pad, B):
+    """The tcgen05 convolution with output-channel tiles of 256 (a second,
+    partial tile for cout 300), odd grids (n 6: the last row tile partly past
+    the grid) and both paddings; its pipeline waits all complete."""
+    from maple_b200 import _lib
+    g = torch.Generator().manual_seed(31 * n + cin + cout)
+    N = n ** 3
+    x, xd = _bf(torch.randn(B, N, cin, generator=g))
+    W, Wd = _bf(torch.randn(27, cin, cout, generator=g) / np.sqrt(27 * cin))
+    bias = torch.randn(cout, generator=g)
+    out32 = torch.empty(B, N, cout, dtype=torch.float32, device=DEV)
+    _lib.nn_call("maple_nn_conv3d_padded", _p(xd), _p(Wd), _p(bias.to(DEV)), None, None, _p(out32), B, n, cin, cout,
+                 3, 0, pad, _s())
+    xs = ora._to_ncdhw(x, n)
+    if pad:
+        Wk = W.reshape(3, 3, 3, cin, cout).permute(4, 3, 0, 1, 2)
+        ref = ora._to_nvc(torch.nn.functional.conv3d(xs, Wk, bias, padding=1))
+    else:
+        ref = ora._to_nvc(ora.conv3d_periodic(xs, W, bias))
+    torch.cuda.synchronize()
+    assert (out32.cpu() - ref).abs().max() < 2e-4 * max(1.0, float(ref.abs().max()))
+    flag = C.c_int(-1)
+    _lib.nn_call("maple_nn_wait_status", C.byref(flag), _s())
+    assert flag.value == 0
+
+
 @pytest.mark.parametrize("n,cin,cout,k,B", [(8, 8, 32, 3, 2), (4, 96, 128, 3, 3), (8, 32, 21, 1, 2),
                                              (4, 21, 32, 3, 2), (16, 64, 64, 3, 1)])
 def test_conv3d_gradients_match_autograd(lib, n, cin, cout, k, B):
