@@ -261,6 +261,20 @@ int maple_get_level_elements(maple_ctx* ctx, int physics, int level, double* out
 enum { MAPLE_RESTRICT = 0, MAPLE_PROLONG_ADD = 1 };
 int maple_transfer(int op, int nc, int K, int ncells, const double* in, double* out, maple_stream_t stream);
 
+/* The fine-level elastic operator in element-batched form on the tensor
+ * cores, kept to measure it against the stencil form the solver uses:
+ * y = K(rho) u for FP32 u, y [B][6][3][N] of the density of the last mixed
+ * maple_set_density of the elastic physics, as the reference applies it
+ * (utils/EBE_GMG.py:412-430: gather u_e, Ke_e u_e by bmm, scatter back) but
+ * with the contraction of all elements and load cases as one tcgen05 GEMM,
+ * rows (cell, element, load case) x Ke0, TF32 operands with FP32
+ * accumulation (about 1e-3 relative).  rows_work and out_work hold
+ * B * N * 6 * 24 floats each (the gathered rows and the GEMM result).  N
+ * must make B * N * 6 a multiple of 128 (cell size a multiple of 4).  Waits
+ * for its stream; MAPLE_E_TIMEOUT if a pipeline wait ran out. */
+int maple_matvec_ebe_tc(maple_ctx* ctx, const float* u, float* y, float* rows_work, float* out_work,
+                        maple_stream_t stream);
+
 /* Periodic k^3 box filter of [B][N] (main_IHD_v3.py:342-359). */
 int maple_box_filter(int r, int ncells, int k, const double* in, double* out, maple_stream_t stream);
 

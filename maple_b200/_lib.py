@@ -62,6 +62,7 @@ SIGNATURES = {
     "maple_box_filter": (_I, [_I, _I, _I, _P, _P, _P]),
     "maple_get_level_elements": (_I, [_P, _I, _I, _P, _P]),
     "maple_transfer": (_I, [_I, _I, _I, _I, _P, _P, _P]),
+    "maple_matvec_ebe_tc": (_I, [_P, _P, _P, _P, _P, _P]),
     "maple_oc_update": (_I, [_P, _P, _P, _P, _D, _D, _P, _P, _P]),
     "maple_oc_update_noalloc": (_I, [_I, _I, _P, _P, _P, _D, _D, _P, _P, _P]),
     "maple_test_wait_limit": (_I, [_L, _I]),

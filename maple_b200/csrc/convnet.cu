@@ -148,20 +148,23 @@ __global__ void __launch_bounds__(NT) k_conv3d(const bf16* __restrict__ in, cons
 // The same convolution on the fifth-generation tensor cores (tcgen05):
 // an implicit GEMM whose rows are 128 output voxels, columns the output
 // channels (one tile of up to 256, zero-padded to a multiple of 16) and
-// reduction (tap, 16 input channels) steps.  Per step, the 128 threads gather
-// the A tile (each thread one voxel row: the tap's periodic or zero-padded
-// neighbour, two 16-byte chunks of 8 channels) and the B tile (weights, the
-// output channel contiguous: MN-major) with cp.async into one of TC_STAGES
-// shared-memory stages; one thread issues the step's tcgen05.mma (M = 128,
-// K = 16) into an FP32 accumulator in tensor memory and commits it to the
-// stage's mbarrier, which releases the stage for the load TC_STAGES steps
-// later.  The epilogue reads the accumulator rows back (tcgen05.ld, warp w
-// lanes 32w..32w+31) and applies bias, residual and ReLU as k_conv3d.
-// Every mbarrier wait is bounded; a wait that runs out sets g_nn_wait_err,
-// waits (bounded) for the issued MMAs and frees the tensor memory.
-// Requires cin % 8 == 0 (16-byte channel chunks).
+// reduction steps of (tap, KC input channels), KC = the input channel count
+// rounded up to 16, at most TC_KC_MAX.  (With TC_KC_MAX 64 the larger stages
+// left room for fewer CTAs per SM and the kernel ran slower on B200: 131 vs
+// 159 TFLOP/s at 128 channels, 68 vs 74 at 32; so the steps are 16 wide.)  Per step, the 128 threads
+// gather the A tile (each thread one voxel row: the tap's periodic or
+// zero-padded neighbour, KC/8 chunks of 8 channels, K-major) and the B tile
+// (weights, output channel contiguous: MN-major) with cp.async into one of
+// TC_STAGES shared-memory stages; one thread issues the step's KC/16
+// tcgen05.mma (M = 128, K = 16 each) into an FP32 accumulator in tensor
+// memory and commits them to the stage's mbarrier, which releases the stage
+// for the load TC_STAGES steps later.  The epilogue reads the accumulator
+// rows back (tcgen05.ld, warp w lanes 32w..32w+31) and applies bias,
+// residual and ReLU as k_conv3d.  Every mbarrier wait is bounded; a wait that
+// runs out sets g_nn_wait_err, waits (bounded) for the issued MMAs and frees
+// the tensor memory.  Requires cin % 8 == 0 (16-byte channel chunks).
 // ---------------------------------------------------------------------------
-constexpr int TC_BM = 128, TC_THREADS = 128, TC_STAGES = 4, TC_BN_MAX = 256;
+constexpr int TC_BM = 128, TC_THREADS = 128, TC_STAGES = 4, TC_BN_MAX = 256, TC_KC_MAX = 16;
 constexpr long long kTcPolls = 1LL << 24;
 __device__ int g_nn_wait_err;
 
@@ -169,12 +172,17 @@ __host__ __device__ inline int tc_bn(int cout_left) {
   const int c = cout_left < TC_BN_MAX ? cout_left : TC_BN_MAX;
   return (c + 15) / 16 * 16;
 }
+__host__ __device__ inline int tc_kc(int cin) {
+  const int c = (cin + 15) / 16 * 16;
+  return c < TC_KC_MAX ? c : TC_KC_MAX;
+}
 __host__ __device__ inline int tc_tmem_cols(int bn) {
   int c = 32;
   while (c < bn) c <<= 1;
   return c;
 }
-__host__ __device__ inline size_t tc_stage_bytes(int bn) { return (size_t)TC_BM * 32 + (size_t)bn * 32; }
+// one stage: A (128 x KC) and B (BN x KC) BF16
+__host__ __device__ inline size_t tc_stage_bytes(int bn, int kc) { return (size_t)(TC_BM + bn) * kc * 2; }
 
 __device__ __forceinline__ void cp_async16_zfill(void* sdst, const void* gsrc, bool valid) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
@@ -194,11 +202,11 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
   const int N = n * n * n;
   const int b = blockIdx.z;
   const int v0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN_MAX;
-  const int BN = tc_bn(cout - n0);
+  const int BN = tc_bn(cout - n0), KC = tc_kc(cin), KB = KC / 8;
   const uint32_t ncols = (uint32_t)tc_tmem_cols(BN);
-  const size_t stage = tc_stage_bytes(BN);
+  const size_t stage = tc_stage_bytes(BN, KC);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int kc = (cin + 15) / 16, KS = taps * kc;
+  const int kc = (cin + KC - 1) / KC, KS = taps * kc;
   const bf16* inb = in + (size_t)b * N * cin;
   const bool wvec = (cout % 8) == 0;
   if (warp == 0) tmem_alloc(&tslot, ncols);
@@ -211,6 +219,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
   fence_after_sync();
   const uint32_t tmem = tslot;
   const uint32_t idesc = idesc_bf16_f32(TC_BM, BN, 1);
+  // A: K-major, 8-row groups KB*128 bytes apart; B: MN-major, K-groups 128
+  // bytes apart, 8-column groups KC*16 bytes apart; each MMA takes 16 of K
+  const uint32_t sbo_a = (uint32_t)KB * 128, sbo_b = (uint32_t)KC * 16;
   const int m = tid;  // this thread's A row
   const int v = v0 + m;
   int issued = 0;     // MMA steps issued (thread 0)
@@ -226,34 +237,33 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
         }
       }
       uint8_t* sA = tc_smem + st * stage;
-      uint8_t* sB = sA + TC_BM * 32;
-      const int tap = t / kc, c0 = (t - tap * kc) * 16;
+      uint8_t* sB = sA + TC_BM * KC * 2;
+      const int tap = t / kc, c0 = (t - tap * kc) * KC;
       int dx, dy, dz;
       tap_offsets(tap, taps, dx, dy, dz);
       int q = -1;
       if (v < N) q = zero_pad ? neighbour_zp(v, n, dx, dy, dz) : neighbour(v, n, dx, dy, dz);
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      const bf16* rowp = inb + (size_t)(q < 0 ? 0 : q) * cin + c0;
+      for (int h = 0; h < KB; ++h) {
         const bool ok = q >= 0 && c0 + 8 * h < cin;
-        const bf16* src = ok ? inb + (size_t)q * cin + c0 + 8 * h : inb;
-        cp_async16_zfill(sA + (m >> 3) * 256 + h * 128 + (m & 7) * 16, src, ok);
+        cp_async16_zfill(sA + (m >> 3) * sbo_a + h * 128 + (m & 7) * 16, ok ? rowp + 8 * h : inb, ok);
       }
       const int groups = BN / 8;
       if (wvec) {
-        for (int i = tid; i < 16 * groups; i += TC_THREADS) {
+        for (int i = tid; i < KC * groups; i += TC_THREADS) {
           const int k = i / groups, g = i - k * groups;
           const int ci = c0 + k, co = n0 + 8 * g;
           const bool ok = ci < cin && co < cout;
           const bf16* src = ok ? W + ((size_t)tap * cin + ci) * cout + co : W;
-          cp_async16_zfill(sB + mnmajor_offset(8 * g, k, 128, 256), src, ok);
+          cp_async16_zfill(sB + mnmajor_offset(8 * g, k, 128, sbo_b), src, ok);
         }
       } else {
-        for (int i = tid; i < 16 * BN; i += TC_THREADS) {
+        for (int i = tid; i < KC * BN; i += TC_THREADS) {
           const int k = i / BN, j = i - k * BN;
           const int ci = c0 + k, co = n0 + j;
           bf16 val = __float2bfloat16(0.0f);
           if (ci < cin && co < cout) val = W[((size_t)tap * cin + ci) * cout + co];
-          *reinterpret_cast<bf16*>(sB + mnmajor_offset(j, k, 128, 256)) = val;
+          *reinterpret_cast<bf16*>(sB + mnmajor_offset(j, k, 128, sbo_b)) = val;
         }
       }
     }
@@ -265,8 +275,10 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
       if (tid == 0) {
         fence_after_sync();
         const int s = t - 1, st = s % TC_STAGES;
-        const uint32_t a = smem_u32(tc_smem + st * stage);
-        mma_bf16(tmem, smem_desc(a, 128, 256), smem_desc(a + TC_BM * 32, 128, 256), idesc, s > 0 ? 1u : 0u);
+        const uint32_t a = smem_u32(tc_smem + st * stage), bb = a + TC_BM * KC * 2;
+        for (int j = 0; j < KC / 16; ++j)
+          mma_bf16(tmem, smem_desc(a + j * 256, 128, sbo_a), smem_desc(bb + j * 256, 128, sbo_b), idesc,
+                   (s > 0 || j > 0) ? 1u : 0u);
         mma_commit(&mma_bar[st]);
         issued = s + 1;
       }
@@ -795,14 +807,13 @@ int maple_nn_conv3d_padded(const void* in, const void* W, const float* bias, con
     const int taps = ksize == 3 ? 27 : 1, zp = padding == MAPLE_NN_PAD_ZEROS ? 1 : 0;
     if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(W) & 15) == 0) {
       // tensor-core (tcgen05) implicit GEMM
-      const int bn0 = tc_bn(cout);
-      const size_t smem = TC_STAGES * tc_stage_bytes(bn0);
+      const size_t smem = TC_STAGES * tc_stage_bytes(tc_bn(cout), tc_kc(cin));
       static bool attr_set[128] = {};
       int dev = 0;
       CKN(cudaGetDevice(&dev));
       if (dev >= 0 && dev < 128 && !attr_set[dev]) {
         CKN(cudaFuncSetAttribute(k_conv3d_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(TC_STAGES * tc_stage_bytes(TC_BN_MAX))));
+                                 (int)(TC_STAGES * tc_stage_bytes(TC_BN_MAX, TC_KC_MAX))));
         attr_set[dev] = true;
       }
       dim3 g((N + TC_BM - 1) / TC_BM, (cout + TC_BN_MAX - 1) / TC_BN_MAX, B);

@@ -2,6 +2,7 @@
 // the C ABI declared in include/maple_b200.h.
 #include "../../include/maple_b200.h"
 #include "kernels.cuh"
+#include "ebe_tc.cuh"
 #include "printability.h"
 #include "tables.h"
 
@@ -1972,6 +1973,33 @@ int maple_get_level_elements(maple_ctx* c, int phys, int level, double* out, map
     const size_t k = 8 * (size_t)p.D;
     CK(cudaMemcpyAsync(out, p.KE[level], (size_t)c->B * nodes(c->n[level]) * k * k * sizeof(double),
                        cudaMemcpyDeviceToDevice, S(s)));
+  });
+}
+
+int maple_matvec_ebe_tc(maple_ctx* c, const float* u, float* y, float* rows_work, float* out_work, maple_stream_t s) {
+  return guarded([&] {
+    require(c != nullptr && u && y && rows_work && out_work, "NULL argument");
+    Phys& p = c->ph[MAPLE_ELASTIC];
+    require(p.built && p.o32.alloc && p.o32.rho, "build the elastic hierarchy in mixed precision first");
+    const int n = c->n[0], N = nodes(n), B = c->B;
+    const long long rows = (long long)B * N * 6;
+    require(rows % EBE_ROWS == 0, "the cell size must be a multiple of 4");
+    cudaStream_t st = S(s);
+    CK(cudaMemsetAsync(c->err, 0, sizeof(int), st));
+    const long long tot = (long long)B * 6 * N;
+    k_ebe_gather<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(u, rows_work, n, B);
+    CKL();
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
+    const long long ntiles = rows / EBE_ROWS;
+    const unsigned grid = (unsigned)std::min<long long>(ntiles, (long long)sms * 4);
+    k_ebe_gemm_tc<<<grid, EBE_ROWS, 0, st>>>(rows_work, p.o32.rho, out_work, ntiles, N, (float)p.kscale, c->err);
+    CKL();
+    k_ebe_scatter<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(out_work, y, n, B);
+    CKL();
+    CK(cudaMemcpyAsync(c->h_err, c->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (*c->h_err) throw Failure{MAPLE_E_TIMEOUT, "maple_matvec_ebe_tc: a tensor-core pipeline wait ran out"};
   });
 }
 

@@ -496,3 +496,30 @@ def test_grid_transfers_match_oracle_prolongation(lib, nc, K):
         for k in range(K):
             assert rel(rc[b, k], P.T @ fine[b, k]) < 1e-14, (b, k)
             assert rel(uf[b, k], base[b, k] + P @ coarse[b, k]) < 1e-14, (b, k)
+
+
+def test_element_batched_tensor_core_matvec(lib):
+    """The element-batched operator on tcgen05 (TF32 contraction of all
+    elements and load cases, the reference's EBE form) against the FP64
+    stencil operator, to the TF32 rounding."""
+    from maple_b200 import _lib
+    from maple_b200.core import HomogenizationContext
+    import ctypes as C
+    r, B = 16, 2
+    N = r ** 3
+    rho = np.stack([simp(O.seed_density(s, r, 2.0, 0.3).reshape(-1)) for s in (5, 6)])
+    c = HomogenizationContext(r, ncells=B)
+    c.set_density("elastic", T(rho), "mixed")
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal((B, 6, 3, N))
+    y64 = c.matvec("elastic", T(rho), T(u)).cpu().numpy()
+    u32 = torch.tensor(u, dtype=torch.float32, device=DEV).contiguous()
+    y32 = torch.empty_like(u32)
+    rows = torch.empty(B * N * 6 * 24, dtype=torch.float32, device=DEV)
+    outw = torch.empty_like(rows)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _lib.check(lib.maple_matvec_ebe_tc(c._h, C.c_void_p(u32.data_ptr()), C.c_void_p(y32.data_ptr()),
+                                       C.c_void_p(rows.data_ptr()), C.c_void_p(outw.data_ptr()), stream))
+    err = np.abs(y32.cpu().numpy() - y64).max() / np.abs(y64).max()
+    assert err < 5e-3, err
+    c.close()
