@@ -66,6 +66,8 @@ def seed_density(seed, r, sigma, vf, scale=0.25, xmin=1e-3):
 
 
 def main(src, only=None):
+    global SRC
+    SRC = src
     M, U, Mo, Ob, GMGSolver, GMGSolverScalar = _import_reference(src)
     # torch's default dtype stays float32: the reference's
     # isotropic_elastic_tensor (utils/_utils.py:42) relies on it
@@ -290,13 +292,69 @@ def config0_fixtures(Ob, homogenize):
                oracle_relres=np.array(relres), x50=x.copy())
     for it, xv in xs.items():
         rec[f"x{it}"] = xv
-    for it in (0, 1, 10, 25, 49):
-        xv = rec["x0"] if it == 0 else xs[it]
-        CH, kap, J, rr = _reference_terms(Ob, homogenize, r, xv, spec, cycles=90, levels=5)
+    # the reference's own solvers at the checkpoints, one process each (40
+    # cycles: C^H and J are quadratic in the solve error, so a relative
+    # residual near 1e-6 already pins them to about 1e-12)
+    import multiprocessing as mp
+    its = (0, 1, 10, 25, 49)
+    jobs = [(SRC, spec, r, rec["x0"] if it == 0 else xs[it], 40, 5) for it in its]
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+        outs = pool.map(_reference_job, jobs)
+    for it, (CH, kap, J, rr) in zip(its, outs):
         rec[f"ref_CH_{it}"], rec[f"ref_kappa_{it}"], rec[f"ref_J_{it}"], rec[f"ref_relres_{it}"] = CH, kap, J, rr
         print(f"config0 reference it {it} J {J:.15g} (oracle {Js[it]:.15g}) relres {rr:.2e}", flush=True)
     np.savez_compressed(os.path.join(HERE, "traj_r32.npz"), **rec)
     print("wrote traj_r32.npz")
+
+
+SRC = None  # the reference source tree of this run (set by main)
+
+
+def _reference_job(args):
+    """One reference evaluation in a fresh process (spawned): C^H, kappa^H, J
+    and the reached relative residual of design x."""
+    src, spec, r, x, cycles, levels = args
+    torch.set_num_threads(1)
+    M, U, Mo, Ob, GMGSolver, GMGSolverScalar = _import_reference(src)
+    dev = torch.device("cpu")
+    ihd = Mo.IHD.__new__(Mo.IHD)
+    torch.nn.Module.__init__(ihd)
+
+    def homogenize(r_, rho, cycles_, levels=3):
+        C = U.isotropic_elastic_tensor(1.0, 0.3).double()
+        Ke, Fe, X0 = U.hexahedron(r_, C)
+        K1, F1, X1 = U.hexahedron_scalar(r_, kappa=torch.tensor(1.0, dtype=torch.float64))
+        batch = M.build_unitcell_batch(dev, r_, rho.detach().reshape(r_, r_, r_))
+        rr = rho.reshape(-1, 1)
+        n = r_ ** 3
+        out = {}
+        F = U.assemble_F_fast(batch["node_index"], Fe, n, rr)
+        Ke_ = Ke.unsqueeze(0).expand(n, -1, -1) * rr.reshape(-1, 1, 1)
+        us, res = [], []
+        for i in range(6):
+            u, rv = GMGSolver().solve(Ke_, F[:, :, i], batch["coord"].int(), batch["elem_coords"], batch["node_index"],
+                                      max_iter=cycles_, smooth_iter=[2, 2, 3, 4, 5], max_levels=levels,
+                                      dtype=torch.float64)
+            us.append(u)
+            res.append((rv.norm() / F[:, :, i].norm()).item())
+        out["CH"] = ihd.homogenized_batch_3d(torch.cat(us, 1), Ke_, X0, batch["coord"][:, 0], batch["node_index"],
+                                             batch["voxel_batch_id"], 1)[0]
+        out["relres_elastic"] = np.array(res)
+        Ft = U.assemble_F_fast_scalar(batch["node_index"], F1, n, rr)
+        K1_ = K1.unsqueeze(0).expand(n, -1, -1) * rr.reshape(-1, 1, 1)
+        ut, res = [], []
+        for i in range(3):
+            u, rv = GMGSolverScalar().solve(K1_, Ft[:, i], batch["coord"].int(), batch["elem_coords"],
+                                            batch["node_index"], max_iter=cycles_, smooth_iter=[2, 2, 3, 4, 5],
+                                            max_levels=levels, dtype=torch.float64)
+            ut.append(u)
+            res.append((rv.norm() / Ft[:, i].norm()).item())
+        out["kappa"] = ihd.homogenized_batch_thermal(torch.cat(ut, 1), K1_, X1, batch["coord"][:, 0],
+                                                     batch["node_index"], batch["voxel_batch_id"], 1)[0]
+        out["relres_thermal"] = np.array(res)
+        return out
+
+    return _reference_terms(Ob, homogenize, r, x, spec, cycles, levels)
 
 
 def config1_fixtures(Ob, homogenize):

@@ -227,3 +227,44 @@ def test_checkpoint_resume_repeats_the_run(lib, tmp_path):
         else:
             np.testing.assert_allclose(res.x.cpu().numpy(), full.x.cpu().numpy(), rtol=0, atol=1e-7)
             np.testing.assert_allclose(res.J, full.J, rtol=1e-8)
+
+
+@pytest.mark.parametrize("solver,d,R", [("GMGSolver", 3, 6), ("GMGSolverScalar", 1, 3)])
+def test_gmg_solver_load_cases_share_one_solve(lib, golden, solver, d, R):
+    """The reference's homogenization calls GMGSolver.solve once per load case
+    (utils/model.py:111-124).  The first call solves every load case of the
+    density; the others return the stored columns (one kernel launch, the
+    right-hand side check), each equal to the reference's solution.  Any other
+    right-hand side is still solved."""
+    from maple_b200 import gmg
+    from maple_b200.core import launch_count
+    from maple_b200.optimize import build_unitcell_batch
+    from maple_b200.utils import hexahedron, hexahedron_scalar, isotropic_elastic_tensor
+    g = golden("homog_r8_s0.npz")
+    rho = torch.tensor(1e-9 + (1 - 1e-9) * g["x"] ** 3, dtype=torch.float64, device=DEV)
+    batch = build_unitcell_batch(DEV, 8, rho.reshape(8, 8, 8))
+    if d == 3:
+        Ke, _, _ = hexahedron(8, isotropic_elastic_tensor(1.0, 0.3).double().to(DEV))
+        Fs = [torch.tensor(g["F_elastic"][:, :, i], device=DEV) for i in range(R)]
+        Us = [g["u_elastic"][:, :, i] for i in range(R)]
+    else:
+        Ke, _, _ = hexahedron_scalar(8, torch.tensor(1.0, dtype=torch.float64, device=DEV))
+        Fs = [torch.tensor(g["F_thermal"][:, i], device=DEV) for i in range(R)]
+        Us = [g["u_thermal"][:, i:i + 1] for i in range(R)]
+    fine_ke = Ke.unsqueeze(0).expand(512, -1, -1) * rho.reshape(-1, 1, 1)
+    s = getattr(gmg, solver)()
+    args = (batch["coord"].int(), batch["elem_coords"], batch["node_index"])
+    launches = []
+    for i in range(R):
+        l0 = launch_count()
+        u, r = s.solve(fine_ke, Fs[i], *args, dtype=torch.float64)
+        torch.cuda.synchronize()
+        launches.append(launch_count() - l0)
+        un = u.cpu().numpy().reshape(512, d)
+        du = (un - un.mean(0)) - (Us[i] - Us[i].mean(0))
+        assert np.abs(du).max() / np.abs(Us[i]).max() < 1e-8, i
+        assert float(r.norm() / Fs[i].norm()) < 1e-9
+    assert launches[0] > 10 and all(n == 1 for n in launches[1:]), launches
+    other = 0.5 * Fs[0] + 0.25 * Fs[R - 1]
+    u, r = s.solve(fine_ke, other, *args, dtype=torch.float64)
+    assert float(r.norm() / other.norm()) < 1e-9
