@@ -11,8 +11,19 @@ on the GPU to ``rtol`` (keyword, default 1e-10) instead of a fixed number of
 V-cycles; ``max_iter`` is honoured as a lower bound of the PCG iteration cap.
 The converged u may differ from the reference's by a rigid translation (the
 periodic operator's null space), which leaves C^H unchanged.
-``init_list`` may carry a dense level-0 initial guess (a tensor of the shape
-of ``global_f``); per-level sparse (spconv) initial fields are not supported.
+``init_list`` is the reference's hook for network-predicted fields
+(EBE_GMG.py:648-757, 851-858, 943-952): a dense tensor shaped like
+``global_f``, or a list of per-level fields ordered coarse to fine as the
+reference's (its last entry is the fine level), each None, a dense
+(n_l^3, D) tensor or a sparse tensor with ``.indices`` ([b,]x,y,z) and
+``.features`` (``init_feat_slice`` selects the D components, ``init_batch``
+the batch entry), aligned to the level's nodes by coordinates as
+``_spconv_to_dense_u`` does.  The reference starts level 0 from its field and
+injects the coarse ones as the starting corrections of every V-cycle
+(``init_is_solution``: minus the restricted iterate).  A preconditioner for
+CG must be linear, so here the finest given field is the initial iterate
+(prolonged trilinearly to the fine grid when it is a coarse level's), with or
+without ``init_is_solution``; the converged answer is the same.
 
 The context solves all load cases of a physics at once (6 elastic, 3
 thermal).  The reference's homogenization calls ``solve`` once per load case
@@ -65,8 +76,9 @@ class GMGSolver(nn.Module):
         ctx = cached_context(r, dev)
         rho1 = rho.reshape(1, n).contiguous()
         fd = f.to(device=ctx.device, dtype=torch.float64)
-        if init_list is not None and not (isinstance(init_list, torch.Tensor) and init_list.numel() == n * D):
-            raise NotImplementedError("init_list: only a dense level-0 tensor shaped like global_f is supported")
+        u_init = None
+        if init_list is not None:
+            u_init = self._initial_iterate(init_list, r, init_batch, init_feat_slice, ctx.device)
         col = None
         if init_list is None:
             col = self._load_case_column(ctx, rho1, fd, precision, rtol, fine_ke.dtype)
@@ -79,9 +91,9 @@ class GMGSolver(nn.Module):
             F = torch.zeros((1, self.R, D, n), dtype=torch.float64, device=ctx.device)
             F[0, 0] = fd.T
             x0 = None
-            if init_list is not None:
+            if u_init is not None:
                 x0 = torch.zeros_like(F)
-                x0[0, 0] = init_list.reshape(n, D).to(device=ctx.device, dtype=torch.float64).T
+                x0[0, 0] = u_init.T
             u, res, _ = ctx.solve_rhs(self.PHYSICS, F, x0, precision=precision, rtol=rtol,
                                       maxit=max(int(max_iter), 500))
             out_u = u[0, 0].T.contiguous().to(device=dev, dtype=dtype)
@@ -90,6 +102,60 @@ class GMGSolver(nn.Module):
             return out_u.reshape(n, 1), out_r.reshape(n, 1)
         return out_u, out_r
 
+
+    def _level_field(self, item, nl, batch, feat_slice, device):
+        """One level's field as a dense (nl^3, D) FP64 tensor, or None."""
+        D, N = self.D, nl ** 3
+        if item is None:
+            return None
+        if isinstance(item, torch.Tensor):
+            if item.numel() != N * D:
+                raise ValueError(f"init_list field of {item.numel()} values does not fit {N} nodes x {D}")
+            return item.reshape(N, D).to(device=device, dtype=torch.float64)
+        idx, feat = getattr(item, "indices", None), getattr(item, "features", None)
+        if idx is None or feat is None:
+            raise TypeError("init_list entries must be tensors or carry .indices and .features")
+        idx = idx.to(device=device, dtype=torch.long)
+        vals = feat.to(device=device, dtype=torch.float64)[:, feat_slice]
+        if vals.shape[1] < D:
+            raise ValueError(f"init_list features hold {vals.shape[1]} components, {D} needed")
+        vals = vals[:, :D]
+        if idx.shape[1] == 4:
+            if batch is not None:
+                keep = idx[:, 0] == int(batch)
+                idx, vals = idx[keep], vals[keep]
+            idx = idx[:, 1:]
+        idx = idx % nl
+        lin = (idx[:, 0] * nl + idx[:, 1]) * nl + idx[:, 2]
+        out = torch.zeros((N, D), dtype=torch.float64, device=device)
+        out.index_add_(0, lin, vals)
+        return out
+
+    def _initial_iterate(self, init_list, r, batch, feat_slice, device):
+        """The fine-level initial iterate (n, D) from the reference's
+        ``init_list``: the finest given level, prolonged to the fine grid."""
+        from .core import transfer
+        D, n = self.D, r ** 3
+        if isinstance(init_list, torch.Tensor):
+            if init_list.numel() != n * D:
+                raise ValueError("a dense init_list must have the shape of global_f")
+            return init_list.reshape(n, D).to(device=device, dtype=torch.float64)
+        if not isinstance(init_list, (list, tuple)):
+            raise TypeError("init_list must be a tensor or a list of per-level fields (coarse to fine)")
+        for level, item in enumerate(reversed(init_list)):  # level 0 = the fine grid
+            if item is None:
+                continue
+            if r % (1 << level):
+                raise ValueError(f"level {level} does not exist for a {r}^3 cell")
+            nl = r >> level
+            u = self._level_field(item, nl, batch, feat_slice, device)
+            for _ in range(level):  # trilinear prolongation, one level at a time
+                f3 = torch.zeros((1, 3, nl ** 3), dtype=torch.float64, device=device)
+                f3[0, :D] = u.T
+                u = transfer("prolong_add", f3.contiguous())[0, :D].T.contiguous()
+                nl *= 2
+            return u
+        return None
 
     def _load_case_column(self, ctx, rho1, fd, precision, rtol, in_dtype):
         """Index of the load case of ``assemble_F_fast`` that ``fd`` (n, D) is,

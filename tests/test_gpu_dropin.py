@@ -268,3 +268,45 @@ def test_gmg_solver_load_cases_share_one_solve(lib, golden, solver, d, R):
     other = 0.5 * Fs[0] + 0.25 * Fs[R - 1]
     u, r = s.solve(fine_ke, other, *args, dtype=torch.float64)
     assert float(r.norm() / other.norm()) < 1e-9
+
+
+def test_gmg_solver_per_level_init_list(lib, golden):
+    """The reference's init_list hook: per-level fields ordered coarse to fine,
+    as sparse tensors (.indices [b,x,y,z], .features) aligned by coordinates.
+    A field at the fine level is the initial iterate; a coarse level's is
+    prolonged to the fine grid first.  Either way the solve reaches the
+    reference's solution."""
+    import types
+    from maple_b200 import gmg
+    from maple_b200.optimize import build_unitcell_batch
+    from maple_b200.utils import hexahedron, isotropic_elastic_tensor
+    g = golden("homog_r8_s0.npz")
+    rho = torch.tensor(1e-9 + (1 - 1e-9) * g["x"] ** 3, dtype=torch.float64, device=DEV)
+    batch = build_unitcell_batch(DEV, 8, rho.reshape(8, 8, 8))
+    Ke, _, _ = hexahedron(8, isotropic_elastic_tensor(1.0, 0.3).double().to(DEV))
+    fine_ke = Ke.unsqueeze(0).expand(512, -1, -1) * rho.reshape(-1, 1, 1)
+    f = torch.tensor(g["F_elastic"][:, :, 4], device=DEV)
+    ug = g["u_elastic"][:, :, 4]
+    args = (batch["coord"].int(), batch["elem_coords"], batch["node_index"])
+
+    def sparse(n, field):
+        xyz = torch.stack(torch.meshgrid(*[torch.arange(n, device=DEV)] * 3, indexing="ij"), -1).reshape(-1, 3)
+        idx = torch.cat([torch.zeros((n ** 3, 1), dtype=torch.long, device=DEV), xyz], 1)
+        feats = torch.cat([torch.as_tensor(field, device=DEV).reshape(n ** 3, 3),
+                           torch.zeros((n ** 3, 2), dtype=torch.float64, device=DEV)], 1)  # extra channels
+        return types.SimpleNamespace(indices=idx, features=feats)
+
+    def check(u):
+        un = u.cpu().numpy()
+        du = (un - un.mean(0)) - (ug - ug.mean(0))
+        assert np.abs(du).max() / np.abs(ug).max() < 1e-8
+
+    s = gmg.GMGSolver()
+    u, r = s.solve(fine_ke, f, *args, init_list=[None, sparse(8, ug)], dtype=torch.float64)
+    check(u)
+    coarse = ug.reshape(8, 8, 8, 3)[::2, ::2, ::2]  # injection to the 4^3 level
+    u, r = s.solve(fine_ke, f, *args, init_list=[sparse(4, coarse), None], init_is_solution=True,
+                   dtype=torch.float64)
+    check(u)
+    with pytest.raises(ValueError):
+        s.solve(fine_ke, f, *args, init_list=[torch.zeros(10, dtype=torch.float64, device=DEV), None])
