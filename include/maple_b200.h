@@ -92,6 +92,13 @@ int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio,
 enum { MAPLE_MIXED_FLEXIBLE = 0, MAPLE_MIXED_REFINE = 1 };
 int maple_set_mixed_mode(maple_ctx* ctx, int mode);
 
+/* Warm start of the solves of maple_oc_step (with warm = 1) along the OC
+ * trajectory: from u_k + theta (u_k - u_{k-1}), the last two steps'
+ * solutions, instead of u_k (theta = 0, the default).  Only the initial
+ * iterate changes; every solve still stops at its tolerance.  The reference
+ * starts every solve from zero (utils/EBE_GMG.py:851-858). */
+int maple_set_extrapolation(maple_ctx* ctx, double theta);
+
 /* CUDA-graph replay of the PCG iteration body (default on).  Off runs every
  * launch eagerly (same results). */
 int maple_set_graphs(maple_ctx* ctx, int enable);

@@ -38,6 +38,7 @@ SIGNATURES = {
     "maple_set_solver_options": (_I, [_P, _I, _D, _I, _D, _I]),
     "maple_set_graphs": (_I, [_P, _I]),
     "maple_set_mixed_mode": (_I, [_P, _I]),
+    "maple_set_extrapolation": (_I, [_P, _D]),
     "maple_set_concurrency": (_I, [_P, _I]),
     "maple_set_stencil_split": (_I, [_P, _I]),
     "maple_set_coarse_degree": (_I, [_P, _I]),

@@ -186,6 +186,11 @@ class HomogenizationContext:
             raise ValueError(f"mixed mode must be one of {sorted(modes)}, got {mode!r}")
         _lib.check(self._lib.maple_set_mixed_mode(self._h, modes[mode]))
 
+    def set_extrapolation(self, theta: float = 0.0):
+        """oc_step(warm=True) starts its solves from u_k + theta (u_k - u_{k-1})
+        (the last two steps' solutions); 0 starts from u_k."""
+        _lib.check(self._lib.maple_set_extrapolation(self._h, float(theta)))
+
     def set_graphs(self, enable: bool):
         """Replay the PCG iteration body as a captured CUDA graph (default on)."""
         _lib.check(self._lib.maple_set_graphs(self._h, int(bool(enable))))

@@ -124,6 +124,9 @@ struct Phys {
   double* r64 = nullptr;         // residual (FP64)
   double *p64 = nullptr, *q64 = nullptr;  // mixed-precision PCG vectors (z stays FP32)
   float* b32 = nullptr;          // right-hand side of the FP32 inner solve (refinement mode)
+  double* u_prev = nullptr;      // the solution of the OC step before the last (extrapolated warm start)
+  bool prev_valid = false;       // u_prev holds the previous OC step's solution of every active cell
+  bool from_oc = false;          // u64 is the solution of the last maple_oc_step
   double* energy = nullptr;      // [B][N][R][R]
   double* H = nullptr;           // [B][R][R]
   Ops<double> o64;
@@ -236,6 +239,7 @@ struct maple_ctx {
   double inner_rtol = 1e-5;
   int check_every = 1;
   int mixed_mode = 0;  // MAPLE_MIXED_FLEXIBLE or MAPLE_MIXED_REFINE
+  double extrap = 0.0;  // warm start of maple_oc_step: u + extrap * (u - u_prev)
 };
 
 #define LN(c) ((c)->lanes[maple::tl_lane])
@@ -376,6 +380,7 @@ static void alloc_phys(maple_ctx* c, int phys) {
   p.energy = dnew<double>(c, (size_t)B * N0 * R * R);
   p.H = dnew<double>(c, (size_t)B * R * R);
   CK(cudaMemset(p.u64, 0, (size_t)B * N0 * R * D * sizeof(double)));
+  if (c->extrap > 0) p.u_prev = dnew<double>(c, (size_t)B * N0 * R * D);
   p.alloc = true;
 }
 
@@ -937,6 +942,22 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
     KL(c, st, k_pcg_direction_f32<R, D, false><<<g2(N, B), kThreads, 0, st>>>(pv, z32, LN(c).o_inv, sc.beta, N, run));
   };
   run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_MIXED], maxit, body, s);
+}
+
+// Extrapolated warm start of an OC step: u <- u + theta (u - prev), prev <- u
+// (the solution this step starts from becomes the next step's "previous");
+// with theta = 0 only prev <- u.  Cells with active[b] == 0 are skipped.
+__global__ void k_extrapolate(double* __restrict__ u, double* __restrict__ prev, double theta, size_t len,
+                              const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  double* ub = u + (size_t)b * len;
+  double* pb = prev + (size_t)b * len;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (size_t)gridDim.x * blockDim.x) {
+    const double uv = ub[i];
+    if (theta != 0.0) ub[i] = fma(theta, uv - pb[i], uv);
+    pb[i] = uv;
+  }
 }
 
 // outer refinement bookkeeping: per (cell, rhs) residual scale and cell done
@@ -1779,6 +1800,18 @@ int maple_set_tail_fused(maple_ctx* c, int enable) {
   });
 }
 
+int maple_set_extrapolation(maple_ctx* c, double theta) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(theta >= 0 && theta <= 2, "theta must be in [0, 2]");
+    c->extrap = theta;
+    for (Phys& p : c->ph) {
+      if (theta > 0 && p.alloc && !p.u_prev) p.u_prev = dnew<double>(c, (size_t)c->B * nodes(c->n[0]) * p.R * p.D);
+      p.prev_valid = false;
+    }
+  });
+}
+
 int maple_set_mixed_mode(maple_ctx* c, int mode) {
   return guarded([&] {
     require(c != nullptr, "ctx is NULL");
@@ -1849,6 +1882,7 @@ int maple_solve(maple_ctx* c, int phys, int prec, double rtol, int maxit, int wa
     p.solved = true;
     p.current = true;
     p.energies = false;
+    p.from_oc = false;
   });
 }
 
@@ -1897,6 +1931,7 @@ int maple_set_solution(maple_ctx* c, int phys, const double* u, maple_stream_t s
     p.solved = true;
     p.current = false;
     p.energies = false;
+    p.from_oc = false;
   });
 }
 
@@ -2155,9 +2190,19 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       build(c, phys, prec, ps);
       assemble_rhs(c, phys, p.o64.rho, p.F64, ps);
       const bool was_solved = p.solved;
+      if (warm && was_solved && p.from_oc && c->extrap > 0 && p.u_prev) {
+        // start from the previous solution extrapolated along the OC trajectory
+        const size_t len = (size_t)nodes(c->n[0]) * p.R * p.D;
+        KL(c, ps, k_extrapolate<<<dim3(64, B), kThreads, 0, ps>>>(p.u64, p.u_prev, p.prev_valid ? c->extrap : 0.0,
+                                                                  len, c->active));
+        p.prev_valid = true;
+      } else {
+        p.prev_valid = false;
+      }
       dispatch_solve(c, phys, prec, p.F64, p.u64, !(warm && was_solved), rtol, maxit, it_out, nullptr, ps);
       p.solved = true;
       p.current = true;
+      p.from_oc = true;
       homogenize(c, phys, ps);
     };
     std::vector<int> it_el(B, 0), it_th(B, 0), it_sum(B, 0);

@@ -298,11 +298,16 @@ class Hierarchy:
                 u[rows] += lv.dinv[rows, None] * r
         return u
 
-    def vcycle(self, l: int, u, f, smooth_iter, coarse_default: int | None):
+    def vcycle(self, l: int, u, f, smooth_iter, coarse_default: int | None, symmetric: bool = False):
         """One V-cycle (EBE_GMG.py:886-984).  ``coarse_default`` reproduces the
         elastic solver's recursion, which does not forward ``smooth_iter`` and so
         smooths coarser levels with the default of 1 sweep (EBE_GMG.py:955-963);
-        the scalar solver forwards it (EBE_GMG_scalar.py:802-811): pass None."""
+        the scalar solver forwards it (EBE_GMG_scalar.py:802-811): pass None.
+
+        ``symmetric``: post-smoothing (and the coarsest level's second half)
+        runs the colours in reverse order, which makes the cycle a symmetric
+        operator (a preconditioner for plain CG); the reference's cycle runs
+        them forward both times."""
         lv = self.levels[l]
         if l > 0 and coarse_default is not None:
             nu = coarse_default
@@ -312,13 +317,13 @@ class Hierarchy:
             nu = int(smooth_iter)
         u = self.gs_sweeps(lv, u, f, nu)
         if l == len(self.levels) - 1:
-            return self.gs_sweeps(lv, u, f, 1)
+            return self.gs_sweeps(lv, u, f, nu if symmetric else 1, reverse=symmetric)
         r = f - lv.K @ u
         nxt = self.levels[l + 1]
         rc = nxt.P.T @ r
-        uc = self.vcycle(l + 1, np.zeros_like(rc), rc, smooth_iter, coarse_default)
+        uc = self.vcycle(l + 1, np.zeros_like(rc), rc, smooth_iter, coarse_default, symmetric)
         u = u + nxt.P @ uc
-        return self.gs_sweeps(lv, u, f, nu)
+        return self.gs_sweeps(lv, u, f, nu, reverse=symmetric)
 
 
 def gmg_solve(hier: Hierarchy, f: np.ndarray, max_iter: int, smooth_iter=(2, 2, 3, 4, 5),
@@ -327,11 +332,12 @@ def gmg_solve(hier: Hierarchy, f: np.ndarray, max_iter: int, smooth_iter=(2, 2, 
     ``rtol`` > 0 stops early once ||r|| <= rtol ||f|| per column (the reference
     has no test; it runs ``max_iter`` cycles).
 
-    ``method="pcg"``: the same V-cycle (one cycle from zero on the residual)
-    as the preconditioner of a flexible conjugate gradient (Polak-Ribiere
-    beta, per load case); it reaches residuals the plain cycle stalls above on
-    designs with large density contrast.  The converged answer is the same
-    (up to a rigid translation, which C^H ignores)."""
+    ``method="pcg"``: the V-cycle in its symmetric form (post-smoothing in
+    reverse colour order; one cycle from zero on the residual) as the
+    preconditioner of a conjugate gradient (Polak-Ribiere beta, per load
+    case); it reaches residuals the plain cycle stalls above on designs with
+    large density contrast.  The converged answer is the same (up to a rigid
+    translation, which C^H ignores)."""
     u = np.zeros_like(f) if u0 is None else u0.copy()
     K = hier.levels[0].K
     fn = np.maximum(np.linalg.norm(f, axis=0), 1e-300)
@@ -340,7 +346,7 @@ def gmg_solve(hier: Hierarchy, f: np.ndarray, max_iter: int, smooth_iter=(2, 2, 
     if method == "pcg":
         if rtol > 0 and np.all(np.linalg.norm(r, axis=0) <= rtol * fn):
             return u, r, 0
-        z = hier.vcycle(0, np.zeros_like(r), r, smooth_iter, coarse_default)
+        z = hier.vcycle(0, np.zeros_like(r), r, smooth_iter, coarse_default, True)
         p = z.copy()
         rz = np.sum(r * z, axis=0)
         for it in range(1, max_iter + 1):
@@ -352,7 +358,7 @@ def gmg_solve(hier: Hierarchy, f: np.ndarray, max_iter: int, smooth_iter=(2, 2, 
             r = r - alpha * q
             if rtol > 0 and np.all(np.linalg.norm(r, axis=0) <= rtol * fn):
                 break
-            z = hier.vcycle(0, np.zeros_like(r), r, smooth_iter, coarse_default)
+            z = hier.vcycle(0, np.zeros_like(r), r, smooth_iter, coarse_default, True)
             beta = np.where(rz != 0, np.sum(z * (r - r_old), axis=0) / np.where(rz != 0, rz, 1.0), 0.0)
             rz = np.sum(r * z, axis=0)
             p = z + beta * p

@@ -162,9 +162,10 @@ static void coarsen(int n, int D, const double* ke, const double* rho, const dou
       }                                                                                                          \
     }                                                                                                            \
   }                                                                                                              \
-  static void gs_##D(const Level* L, double* u, const double* f) {                                               \
+  static void gs_##D(const Level* L, double* u, const double* f, int reverse) {                                  \
     const int n = L->n, h = n / 2 > 0 ? n / 2 : 1;                                                               \
-    for (int c = 0; c < 8; ++c) {                                                                                \
+    for (int cc = 0; cc < 8; ++cc) {                                                                             \
+      const int c = reverse ? 7 - cc : cc;                                                                       \
       const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;                                                \
       _Pragma("omp parallel for schedule(static)") for (int i = 0; i < h * h * h; ++i) {                        \
         const int x = 2 * (i / (h * h)) + cx, y = 2 * ((i / h) % h) + cy, z = 2 * (i % h) + cz;                 \
@@ -208,12 +209,12 @@ static void coarsen(int n, int D, const double* ke, const double* rho, const dou
 DEF_OPS(3, 6)
 DEF_OPS(1, 3)
 
-static void gs_sweeps(const Level* L, int D, double* u, const double* f, int sweeps) {
+static void gs_sweeps(const Level* L, int D, double* u, const double* f, int sweeps, int reverse) {
   for (int s = 0; s < sweeps; ++s) {
     if (D == 3)
-      gs_3(L, u, f);
+      gs_3(L, u, f, reverse);
     else
-      gs_1(L, u, f);
+      gs_1(L, u, f, reverse);
   }
 }
 
@@ -279,21 +280,23 @@ static int smooth_count(int D, int l) {
   return si[l < 4 ? l : 4];
 }
 
-static void vcycle(Hier* H, int l, double* u, const double* f) {
+/* sym: post-smoothing (and the coarsest level's second half) in reverse
+ * colour order, a symmetric cycle (the oracle's vcycle(symmetric=True)) */
+static void vcycle(Hier* H, int l, double* u, const double* f, int sym) {
   Level* L = &H->lv[l];
   const int D = H->D, DR = H->D * H->R, nu = smooth_count(D, l);
-  gs_sweeps(L, D, u, f, nu);
+  gs_sweeps(L, D, u, f, nu, 0);
   if (l == H->L - 1) {
-    gs_sweeps(L, D, u, f, 1);
+    gs_sweeps(L, D, u, f, sym ? nu : 1, sym);
     return;
   }
   Level* C = &H->lv[l + 1];
   residual(L, D, u, f, L->r);
   restrict_(L->n, DR, L->r, C->f);
   memset(C->u, 0, sizeof(double) * (size_t)C->n * C->n * C->n * DR);
-  vcycle(H, l + 1, C->u, C->f);
+  vcycle(H, l + 1, C->u, C->f, sym);
   prolong_add(L->n, DR, C->u, u);
-  gs_sweeps(L, D, u, f, nu);
+  gs_sweeps(L, D, u, f, nu, sym);
 }
 
 static void build(Hier* H, int n, int levels, int D, int R, const double* rho, const double* Ke0) {
@@ -387,9 +390,9 @@ static void col_dots(size_t N, int D, int R, const double* a, const double* b, d
   }
 }
 
-/* The V-cycle (one cycle from zero on the residual) as the preconditioner
- * of a flexible conjugate gradient, per load case (Polak-Ribiere beta): the
- * oracle's gmg_solve(method="pcg").  Returns the iterations. */
+/* The symmetric V-cycle (one cycle from zero on the residual) as the
+ * preconditioner of a conjugate gradient, per load case (Polak-Ribiere
+ * beta): the oracle's gmg_solve(method="pcg").  Returns the iterations. */
 static int solve_pcg(Hier* H, double* u, const double* f, double rtol, int max_it) {
   Level* L0 = &H->lv[0];
   const size_t N = (size_t)L0->n * L0->n * L0->n;
@@ -407,7 +410,7 @@ static int solve_pcg(Hier* H, double* u, const double* f, double rtol, int max_i
   for (int c = 0; c < R; ++c) ok &= sqrt(rn[c]) <= rtol * fmax(sqrt(fn[c]), 1e-300);
   if (!(rtol > 0 && ok)) {
     memset(z, 0, sizeof(double) * len);
-    vcycle(H, 0, z, r);
+    vcycle(H, 0, z, r, 1);
     memcpy(p, z, sizeof(double) * len);
     col_dots(N, D, R, r, z, rz);
     for (it = 1; it <= max_it; ++it) {
@@ -430,7 +433,7 @@ static int solve_pcg(Hier* H, double* u, const double* f, double rtol, int max_i
       for (int c = 0; c < R; ++c) ok &= sqrt(rn[c]) <= rtol * fmax(sqrt(fn[c]), 1e-300);
       if (rtol > 0 && ok) break;
       memset(z, 0, sizeof(double) * len);
-      vcycle(H, 0, z, r);
+      vcycle(H, 0, z, r, 1);
 #pragma omp parallel for schedule(static)
       for (size_t i = 0; i < len; ++i) ro[i] = r[i] - ro[i];
       col_dots(N, D, R, z, ro, zr);
@@ -459,7 +462,7 @@ static int solve(Hier* H, double* u, const double* f, double rtol, int max_cycle
   col_norms2(N, D, R, f, fn);
   int it = 0;
   for (it = 1; it <= max_cycles; ++it) {
-    vcycle(H, 0, u, f);
+    vcycle(H, 0, u, f, 0);
     residual(L0, D, u, f, L0->r);
     col_norms2(N, D, R, L0->r, rn);
     int ok = 1;

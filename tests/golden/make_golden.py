@@ -125,6 +125,8 @@ def main(src, only=None):
 
     if only == "config0":
         return config0_fixtures(Ob, homogenize)
+    if only == "config0pins":
+        return config0_pins()
     if only == "config1":
         return config1_fixtures(Ob, homogenize)
     if only == "symmetry":
@@ -254,14 +256,14 @@ def config0_fixtures(Ob, homogenize):
     converged to a relative residual of 1e-12 (warm-started from the previous
     iteration; the converged answer is independent of the start); every
     iteration's J, C^H, kappa^H and |dx| statistics and the designs at
-    iterations 1, 10, 25, 49 and 50 are stored.  The oracle's solves are its
-    V-cycle used as the preconditioner of a flexible CG: the plain V-cycle
-    stalls near a relative residual of 2e-7 from iteration 41 on (the design
-    then holds near-void regions), the preconditioned one converges.  The
-    reference's own FP64 GMG solvers (90 V-cycles) then evaluate C^H, kappa^H
-    and J at the oracle's designs of iterations 0, 1, 10, 25 and 49, with the
-    relative residual they reach (the pins of the oracle trajectory where
-    that residual is small)."""
+    iterations 1, 10, 25, 49 and 50 are stored, with each iteration's oracle
+    residual.  The oracle's solves are its V-cycle in symmetric form used as
+    the preconditioner of CG: the reference's plain V-cycle iteration stalls
+    near a relative residual of 2e-7 from iteration 41 on (the design then
+    holds near-void regions), and so does a flexible CG preconditioned by the
+    non-symmetric cycle (3e-8 to 8e-8 after 400 iterations at iterations 42 and
+    43); the symmetric one reaches 1e-12 at every iteration.  config0_pins then
+    pins the trajectory with the reference's own solvers."""
     import time
     O = _oracle()
     r, vf, spec = 32, 0.25, "stiffness:0.5,thermal:0.5"
@@ -277,7 +279,7 @@ def config0_fixtures(Ob, homogenize):
         if it in (1, 10, 25, 49):
             xs[it] = x.copy()
         xn, info = O.oc_iteration(x, r, w, volfrac=vf, move=0.2, elems=el, levels=5, rtol=1e-12,
-                                  max_cycles=400, u0=prev, method="pcg")
+                                  max_cycles=2000, u0=prev, method="pcg")
         prev = info["res"]
         Js.append(info["J"])
         CHs.append(info["CH"])
@@ -292,18 +294,52 @@ def config0_fixtures(Ob, homogenize):
                oracle_relres=np.array(relres), x50=x.copy())
     for it, xv in xs.items():
         rec[f"x{it}"] = xv
-    # the reference's own solvers at the checkpoints, one process each (40
-    # cycles: C^H and J are quadratic in the solve error, so a relative
-    # residual near 1e-6 already pins them to about 1e-12)
-    import multiprocessing as mp
+    np.savez_compressed(os.path.join(HERE, "traj_r32.npz"), **rec)
+    print("wrote traj_r32.npz (oracle trajectory)")
+    config0_pins()
+
+
+def _oracle_fields(O, r, x, spec, el, levels):
+    """The oracle's converged solutions (rtol 1e-12) of design x, as the
+    reference's node fields: elastic (N, 3, 6), thermal (N, 3)."""
+    rho = 1e-9 + (1 - 1e-9) * np.clip(x, 1e-3, 1.0) ** 3
+    res = O.solve_cell(rho, r, el, levels, 1000, 1e-12, ("elastic", "thermal"), method="pcg")
+    N = r ** 3
+    return res["u3"].reshape(N, 3, 6), res["u1"].reshape(N, 3), res
+
+
+def _pin_jobs(O, r, spec, xs, levels):
+    el = O.Elements(r)
+    jobs = []
+    for x in xs:
+        u3, u1, _ = _oracle_fields(O, r, x, spec, el, levels)
+        jobs.append((SRC, spec, r, x, u3, u1, levels))
+    return jobs
+
+
+def config0_pins():
+    """The reference's pins of the 32^3 trajectory: at the oracle's designs of
+    iterations 0, 1, 10, 25 and 49 the reference's own solvers
+    (GMGSolver.solve / GMGSolverScalar.solve in FP64) are started from the
+    oracle's converged fields through their init_list hook (sparse tensors
+    aligned by node coordinates, EBE_GMG.py:648-757) and run 5 V-cycles; the
+    reference's residual of its own operator then says whether the oracle's
+    field solves the reference's system (the solution is unique up to a
+    rigid translation), and its energy sums give C^H, kappa^H and J."""
+    O = _oracle()
+    path = os.path.join(HERE, "traj_r32.npz")
+    rec = dict(np.load(path, allow_pickle=True))
+    r, spec = int(rec["r"]), "stiffness:0.5,thermal:0.5"
     its = (0, 1, 10, 25, 49)
-    jobs = [(SRC, spec, r, rec["x0"] if it == 0 else xs[it], 40, 5) for it in its]
+    jobs = _pin_jobs(O, r, spec, [rec["x0"] if it == 0 else rec[f"x{it}"] for it in its], 5)
+    import multiprocessing as mp
     with mp.get_context("spawn").Pool(len(jobs)) as pool:
         outs = pool.map(_reference_job, jobs)
     for it, (CH, kap, J, rr) in zip(its, outs):
         rec[f"ref_CH_{it}"], rec[f"ref_kappa_{it}"], rec[f"ref_J_{it}"], rec[f"ref_relres_{it}"] = CH, kap, J, rr
-        print(f"config0 reference it {it} J {J:.15g} (oracle {Js[it]:.15g}) relres {rr:.2e}", flush=True)
-    np.savez_compressed(os.path.join(HERE, "traj_r32.npz"), **rec)
+        print(f"config0 reference it {it} J {J:.15g} (oracle {float(rec['J'][it]):.15g}) relres {rr:.2e}",
+              flush=True)
+    np.savez_compressed(path, **rec)
     print("wrote traj_r32.npz")
 
 
@@ -312,8 +348,11 @@ SRC = None  # the reference source tree of this run (set by main)
 
 def _reference_job(args):
     """One reference evaluation in a fresh process (spawned): C^H, kappa^H, J
-    and the reached relative residual of design x."""
-    src, spec, r, x, cycles, levels = args
+    and the relative residual of design x, the reference's solvers started from
+    the given fields (u3 (N, 3, 6), u1 (N, 3)) through init_list."""
+    import types
+    src, spec, r, x, u3, u1, levels = args
+    cycles = 5
     torch.set_num_threads(1)
     M, U, Mo, Ob, GMGSolver, GMGSolverScalar = _import_reference(src)
     dev = torch.device("cpu")
@@ -330,11 +369,16 @@ def _reference_job(args):
         out = {}
         F = U.assemble_F_fast(batch["node_index"], Fe, n, rr)
         Ke_ = Ke.unsqueeze(0).expand(n, -1, -1) * rr.reshape(-1, 1, 1)
+        idx = batch["coord"].long()
+
+        def init(field):  # the reference's sparse-tensor hook: indices [b,x,y,z], features
+            return [types.SimpleNamespace(indices=idx, features=torch.tensor(field, dtype=torch.float64))]
+
         us, res = [], []
         for i in range(6):
             u, rv = GMGSolver().solve(Ke_, F[:, :, i], batch["coord"].int(), batch["elem_coords"], batch["node_index"],
                                       max_iter=cycles_, smooth_iter=[2, 2, 3, 4, 5], max_levels=levels,
-                                      dtype=torch.float64)
+                                      init_list=init(u3[:, :, i]), dtype=torch.float64)
             us.append(u)
             res.append((rv.norm() / F[:, :, i].norm()).item())
         out["CH"] = ihd.homogenized_batch_3d(torch.cat(us, 1), Ke_, X0, batch["coord"][:, 0], batch["node_index"],
@@ -346,7 +390,8 @@ def _reference_job(args):
         for i in range(3):
             u, rv = GMGSolverScalar().solve(K1_, Ft[:, i], batch["coord"].int(), batch["elem_coords"],
                                             batch["node_index"], max_iter=cycles_, smooth_iter=[2, 2, 3, 4, 5],
-                                            max_levels=levels, dtype=torch.float64)
+                                            max_levels=levels, init_list=init(u1[:, i:i + 1]),
+                                            dtype=torch.float64)
             ut.append(u)
             res.append((rv.norm() / Ft[:, i].norm()).item())
         out["kappa"] = ihd.homogenized_batch_thermal(torch.cat(ut, 1), K1_, X1, batch["coord"][:, 0],

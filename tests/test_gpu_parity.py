@@ -523,3 +523,27 @@ def test_element_batched_tensor_core_matvec(lib):
     err = np.abs(y32.cpu().numpy() - y64).max() / np.abs(y64).max()
     assert err < 5e-3, err
     c.close()
+
+
+def test_extrapolated_warm_start_keeps_the_answer(lib):
+    """maple_set_extrapolation only changes where the OC step's solves start:
+    the trajectory is the same to the solver tolerance."""
+    from maple_b200.core import HomogenizationContext
+    r, B = 16, 2
+    x0 = np.stack([O.seed_density(s, r, 2.0, 0.3).reshape(-1) for s in (1, 2)])
+    w = T(np.array([[1 / 3, 1 / 3, 1 / 3], [0.5, 0.0, 0.5]]))
+    vf = T(np.full(B, 0.3))
+    out = {}
+    for theta in (0.0, 1.0):
+        c = HomogenizationContext(r, ncells=B)
+        c.set_extrapolation(theta)
+        x, Js, its = T(x0), [], 0
+        for _ in range(6):
+            o = c.oc_step(x, w, vf, precision="mixed", rtol=1e-12, maxit=1000, warm=True)
+            x = o["x_next"].clone()
+            Js.append(o["J"].cpu().numpy())
+            its += int(o["iters"].sum())
+        out[theta] = (np.array(Js), x.cpu().numpy(), its)
+        c.close()
+    assert rel(out[1.0][0], out[0.0][0]) < 1e-10
+    assert np.abs(out[1.0][1] - out[0.0][1]).max() < 1e-8
