@@ -224,3 +224,39 @@ def test_penalised_trajectory_matches_reference(golden):
         assert abs(info["J"] - g[f"traj_J{it}"]) < 1e-8 * abs(g[f"traj_J{it}"]), it
         assert abs(info["P_print"] - g[f"traj_Pp{it}"]) < 1e-10 and abs(info["P_cavity"] - g[f"traj_Pc{it}"]) < 1e-10
         assert np.abs(x - g[f"traj_x{it + 1}"]).max() < 1e-7, it
+
+
+def test_oracle_meets_the_32cube_reference_pins(golden):
+    """The 32^3 trajectory fixture: the oracle's own evaluation of the design
+    of iteration 10 reproduces the recorded J, C^H and kappa^H, and these agree
+    with the reference's solvers at that design (its residual there is tiny)."""
+    g = golden("traj_r32.npz")
+    r = int(g["r"])
+    w = O.parse_objective_spec("stiffness:0.5,thermal:0.5")
+    _, info = O.oc_iteration(g["x10"], r, w, volfrac=float(g["vf"]), move=0.2, levels=5, rtol=1e-12,
+                             max_cycles=2000, method="pcg")
+    assert abs(info["J"] - float(g["J"][10])) < 1e-12 * float(g["J"][10])
+    assert np.abs(info["CH"] - g["CH"][10]).max() < 1e-11 * np.abs(g["CH"][10]).max()
+    assert abs(info["J"] - float(g["ref_J_10"])) < 1e-12 * float(g["J"][10])
+    assert np.abs(info["kappa"] - g["ref_kappa_10"]).max() < 1e-11 * np.abs(g["ref_kappa_10"]).max()
+    for it in (0, 1, 10, 25, 49):
+        assert float(g[f"ref_relres_{it}"]) < 1e-12
+
+
+def test_port_follows_the_32cube_trajectory(golden):
+    """The multithreaded C port (the bench's CPU path) follows the first three
+    iterations of the 32^3 trajectory fixture."""
+    from oracle import port as P
+    g = golden("traj_r32.npz")
+    P.build()
+    P.set_threads(4)
+    r = int(g["r"])
+    w = O.parse_objective_spec("stiffness:0.5,thermal:0.5")
+    cell = P.Cell(r, 5)
+    x = g["x0"]
+    for it in range(3):
+        x, info = P.oc_iteration(x, cell, w, volfrac=float(g["vf"]), rtol=1e-12, max_cycles=2000, warm=True,
+                                 method="pcg")
+        assert abs(info["J"] - float(g["J"][it])) < 1e-12 * float(g["J"][it]), it
+        if it == 0:
+            assert np.abs(x - g["x1"]).max() < 1e-12
