@@ -17,7 +17,7 @@
 namespace maple {
 
 constexpr int kThreads = 256;
-constexpr int TX = 4, TY = 4, TZ = 8;  // fine-level node tile per CTA (z fastest)
+constexpr int TX = 4, TY = 8, TZ = 8;  // fine-level node tile per CTA (z fastest)
 constexpr int kFineThreads = TX * TY * TZ;
 
 __constant__ double c_Ke3d[576];
@@ -517,12 +517,14 @@ static_assert(kFineThreads % 32 == 0 && TZ * 4 == 32, "a warp spans tz 0..7 x ty
 __host__ __device__ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 __host__ __device__ inline int fine_tiles(int n) { return ceil_div(n, TX) * ceil_div(n, TY) * ceil_div(n, TZ); }
 
-// CTAs per SM the register allocation must allow: 8 for the FP32 elastic
-// operator (64 registers, no spills; the default allocation leaves 7), 4 for
-// its FP64 form, 8 or 12 for the small ones (their default allocation).
+// CTAs per SM the register allocation must allow (256-thread tiles): 4 for
+// the FP32 elastic operator (64 registers, no spills), 2 for its FP64 form
+// (128 registers), 4 or 6 for the small ones.  4x8x8-node tiles measured
+// faster than 4x4x8 (FP64 K p 65 vs 76 us at 64^3, OC step +4%) and than
+// 8x4x8.
 template <typename T, int RD>
 constexpr int fine_min_blocks() {
-  return RD == 18 ? (sizeof(T) == 4 ? 8 : 4) : (RD == 3 && sizeof(T) == 8 ? 8 : 12);
+  return RD == 18 ? (sizeof(T) == 4 ? 4 : 2) : (RD == 3 && sizeof(T) == 8 ? 4 : 6);
 }
 
 template <typename T, int D, int R, int MODE>
