@@ -321,6 +321,155 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
   if (warp == 0) tmem_free(tmem, ncols);
 }
 
+// Weight gradient on the tcgen05 tensor cores:
+//   dW[tap][ci][co] += sum over (cell, voxel) of in[cell][nbr(v, tap)][ci] * dz[cell][v][co].
+// The rows of dW, r = tap * cin + ci, are one flat M dimension: a CTA owns 128
+// consecutive rows (16 groups of 8 channels, each group inside one tap, so
+// narrow layers put several taps in one tile), up to 256 output channels (N)
+// and a chunk of (cell, voxel) pairs, the reduction.  Both operands come
+// MN-major straight from the channels-last activations: per stage the 256
+// threads gather 64 pairs x 16 channel groups of the input (each group's own
+// periodic neighbour) and 64 rows of dz with cp.async into a 4-stage ring, in
+// four 16-pair slabs, and one thread issues the four K = 16 MMAs of the stage
+// into an FP32 accumulator in tensor memory while the next two stages load.
+// The epilogue adds the CTA's partial dW to global memory with FP32 atomics.
+// Waits are bounded as in k_conv3d_tc.  Requires cin % 8 == 0 and cout % 8 == 0.
+constexpr int WG_CI = 128;     // dW rows per CTA
+constexpr int WG_KP = 64;      // (cell, voxel) pairs per stage: four MMAs of K = 16
+constexpr int WG_STAGES = 4;   // ring depth; loads run WG_STAGES - 2 stages ahead
+constexpr int WG_THREADS = 256;
+__host__ __device__ inline size_t wg_stage_bytes(int bn) { return (size_t)(WG_CI + bn) * WG_KP * 2; }
+
+__global__ void __launch_bounds__(WG_THREADS) k_conv3d_wgrad_tc(const bf16* __restrict__ in,
+                                                                const bf16* __restrict__ dz, float* __restrict__ dW,
+                                                                int B, int n, int cin, int cout, int taps,
+                                                                long long chunk) {
+  using namespace maple_tc;
+  constexpr int LA = WG_STAGES - 2;
+  extern __shared__ __align__(1024) uint8_t wg_smem[];
+  __shared__ __align__(8) uint64_t mma_bar[WG_STAGES];
+  __shared__ __align__(8) uint64_t done_bar;
+  __shared__ uint32_t tslot;
+  const int N = n * n * n;
+  const int R = taps * cin;
+  const int r0 = blockIdx.x * WG_CI;
+  const int n0 = blockIdx.y * TC_BN_MAX;
+  const int BN = tc_bn(cout - n0);
+  const uint32_t ncols = (uint32_t)tc_tmem_cols(BN);
+  const size_t stage = wg_stage_bytes(BN);
+  const uint32_t slab_a = WG_CI * 32, slab_b = (uint32_t)BN * 32;  // one 16-pair slab of each operand
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // this thread's input group: dW rows ra .. ra + 7 = tap ra / cin, channels cia .. cia + 7
+  const int g = tid & 15, ra = r0 + 8 * g;
+  const bool row_ok = ra < R;
+  int ox = 0, oy = 0, oz = 0, cia = 0;
+  if (row_ok) {
+    const int tp = ra / cin;
+    cia = ra - tp * cin;
+    tap_offsets(tp, taps, ox, oy, oz);
+  }
+  const long long total = (long long)B * N;
+  const long long kbeg = (long long)blockIdx.z * chunk, kend = kbeg + chunk < total ? kbeg + chunk : total;
+  const int KS = (int)((kend - kbeg + WG_KP - 1) / WG_KP);
+  if (warp == 0) tmem_alloc(&tslot, ncols);
+  if (tid == 0) {
+    for (int i = 0; i < WG_STAGES; ++i) mbar_init(&mma_bar[i], 1);
+    mbar_init(&done_bar, 1);
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tslot;
+  // A (M = dW rows) and B (N = output channels) both MN-major: 8-row groups
+  // 256 bytes apart, the two 8-pair K-groups of a slab 128 bytes apart
+  const uint32_t idesc = idesc_bf16_f32(WG_CI, BN, 1, 1);
+  const int groups = BN / 8;
+  int issued = 0;
+  bool timed_out = false;
+  for (int t = 0; t < KS + LA; ++t) {
+    if (t < KS) {
+      const int st = t % WG_STAGES;
+      if (t >= WG_STAGES) {
+        const bool ok = mbar_wait(&mma_bar[st], (uint32_t)((t / WG_STAGES - 1) & 1), kTcPolls);
+        if (__syncthreads_or(!ok)) {
+          timed_out = true;
+          break;
+        }
+      }
+      uint8_t* sA = wg_smem + st * stage;
+      uint8_t* sB = sA + (WG_KP / 16) * slab_a;
+      const long long k0 = kbeg + (long long)WG_KP * t;
+#pragma unroll
+      for (int j = 0; j < WG_KP / 16; ++j) {
+        const int k = (tid >> 4) + 16 * j;
+        const long long kk = k0 + k;
+        const bool ok = row_ok && kk < kend;
+        const bf16* src = in;
+        if (ok) {
+          const long long b = kk / N;
+          const int v = (int)(kk - b * N);
+          src = in + ((size_t)b * N + neighbour(v, n, ox, oy, oz)) * cin + cia;
+        }
+        cp_async16_zfill(sA + j * slab_a + mnmajor_offset(8 * g, k & 15, 128, 256), src, ok);
+      }
+      for (int i = tid; i < WG_KP * groups; i += WG_THREADS) {
+        const int k = i / groups, h = i - k * groups;
+        const long long kk = k0 + k;
+        const bool ok = kk < kend && n0 + 8 * h < cout;
+        cp_async16_zfill(sB + (k >> 4) * slab_b + mnmajor_offset(8 * h, k & 15, 128, 256),
+                         ok ? dz + (size_t)kk * cout + n0 + 8 * h : dz, ok);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    const int s = t - LA;
+    if (s >= 0) {
+      asm volatile("cp.async.wait_group %0;\n" ::"n"(LA) : "memory");
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        fence_after_sync();
+        const int st = s % WG_STAGES;
+        const uint32_t a = smem_u32(wg_smem + st * stage), bb = a + (WG_KP / 16) * slab_a;
+#pragma unroll
+        for (int j = 0; j < WG_KP / 16; ++j)
+          mma_bf16(tmem, smem_desc(a + j * slab_a, 128, 256), smem_desc(bb + j * slab_b, 128, 256), idesc,
+                   (s > 0 || j > 0) ? 1u : 0u);
+        mma_commit(&mma_bar[st]);
+        issued = s + 1;
+      }
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  if (tid == 0) {
+    if (issued == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&done_bar)) : "memory");
+    else mma_commit(&done_bar);
+  }
+  const bool fin = mbar_wait(&done_bar, 0, kTcPolls);
+  const bool bad = __syncthreads_or(timed_out || !fin);
+  if (bad) {
+    if (tid == 0) atomicExch(&g_nn_wait_err, 1);
+  } else if (KS > 0) {
+    fence_after_sync();
+    // warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows), columns of half w / 4
+    const int q = warp & 3, r = r0 + 32 * q + lane;
+    const int cb = (warp >> 2) * (BN / 2);
+    for (int c = cb; c < cb + BN / 2; c += 8) {
+      float acc[8];
+      tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c, acc);
+      if (r < R) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int co = n0 + c + j;
+          if (co < cout) atomicAdd(&dW[(size_t)r * cout + co], acc[j]);
+        }
+      }
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, ncols);
+}
+
 // dW[tap][ci][co] += sum_{b,v} in[b][nbr(v,tap)][ci] * dz[b][v][co]  (FP32 atomics)
 // The reduction index kk runs over (b, v) flattened; CTA (x, y, z) owns
 // tap x / (cin tiles), a 64x64 (ci, co) tile and the z-th slice of kk.
@@ -858,6 +1007,47 @@ int maple_nn_conv3d_wgrad(const void* in, const void* dz, float* dW, float* db, 
     if ((cout % 8) == 0 && (reinterpret_cast<uintptr_t>(dz) & 15) != 0) return "gradient must be 16-byte aligned";
     const int N = n * n * n, taps = ksize == 3 ? 27 : 1;
     const long long total = (long long)B * N;
+    if ((cin % 8) == 0 && (cout % 8) == 0) {
+      // tensor-core (tcgen05) GEMM over the flat (tap, input channel) rows.
+      // The reduction is split so that the CTAs fill whole waves of the 148
+      // SMs (at the occupancy shared memory allows), each CTA reducing at
+      // least 4096 (cell, voxel) pairs.
+      const long long tiles = (long long)((taps * cin + WG_CI - 1) / WG_CI) * ((cout + TC_BN_MAX - 1) / TC_BN_MAX);
+      const size_t smem = WG_STAGES * wg_stage_bytes(tc_bn(cout));
+      const long long slots = 148LL * std::max(1, std::min(4, (int)(220 * 1024 / smem)));
+      const long long smax = std::max(1LL, std::min(total / 4096, 8 * slots));
+      long long splits = 1;
+      double best = -1.0;
+      for (long long sp = 1; sp <= smax; ++sp) {
+        const long long ctas = tiles * sp, waves = (ctas + slots - 1) / slots;
+        // fraction of the SM slots the last wave keeps busy, and whether the machine is full at all
+        const double eff = (double)ctas / (double)(waves * slots) - (ctas < slots ? 1.0 : 0.0);
+        if (eff > best + 0.05) {
+          best = eff;
+          splits = sp;
+        }
+      }
+      long long chunk = (total + splits - 1) / splits;
+      chunk = (chunk + WG_KP - 1) / WG_KP * WG_KP;
+      splits = (total + chunk - 1) / chunk;
+      static bool attr_set[128] = {};
+      int dev = 0;
+      CKN(cudaGetDevice(&dev));
+      if (dev >= 0 && dev < 128 && !attr_set[dev]) {
+        CKN(cudaFuncSetAttribute(k_conv3d_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(WG_STAGES * wg_stage_bytes(TC_BN_MAX))));
+        attr_set[dev] = true;
+      }
+      dim3 g((unsigned)((taps * cin + WG_CI - 1) / WG_CI), (cout + TC_BN_MAX - 1) / TC_BN_MAX, (unsigned)splits);
+      NNL((k_conv3d_wgrad_tc<<<g, WG_THREADS, smem, Sx(s)>>>((const bf16*)in, (const bf16*)dz, dW, B, n, cin, cout,
+                                                             taps, chunk)));
+      if (db) {
+        dim3 gb((unsigned)std::min<long long>(512, (total + 7) / 8), (cout + 31) / 32);
+        NNL((k_bias_grad<<<gb, 256, 0, Sx(s)>>>((const bf16*)dz, db, total, cout)));
+      }
+      return nullptr;
+    }
+    // other channel counts: the warp-level MMA kernel
     const long long tiles = (long long)taps * ((cin + BM - 1) / BM) * ((cout + BN - 1) / BN);
     // about 8 CTAs per SM, each reducing at least 1024 (cell, voxel) pairs
     long long splits = std::max(1LL, std::min((148LL * 8 + tiles - 1) / tiles, total / 1024));

@@ -1,7 +1,8 @@
 // Fifth-generation tensor core (tcgen05) helpers for sm_100a: shared-memory
 // matrix descriptors, instruction descriptors, tensor-memory allocation, MMA
 // issue, completion through an mbarrier and tensor-memory loads, as inline
-// PTX.  Used by the BF16 convolutions of the learned initial guess.
+// PTX.  Used by the BF16 convolutions of the learned initial guess (forward,
+// data and weight gradients) and the element-batched operator.
 //
 // Operand layout (K-major, no swizzle).  An operand tile of R rows and K
 // columns of 16-bit values is stored as "core matrices" of 8 rows x 16 bytes
@@ -39,10 +40,10 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
 }
 
 // instruction descriptor of kind::f16 with BF16 A and B, FP32 accumulator,
-// A K-major, B K-major (b_mn_major = 0) or MN-major (1), M x N tile
-__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N, int b_mn_major = 0) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)b_mn_major << 16) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
+// each operand K-major (0) or MN-major (1), M x N tile
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N, int b_mn_major = 0, int a_mn_major = 0) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn_major << 15) | ((uint32_t)b_mn_major << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 // MN-major operand layout (no swizzle), used for B when N is the contiguous

@@ -3,11 +3,14 @@ repetitions), for profiling and for the comparisons recorded with the
 design:
 
     python -m maple_b200.opbench conv --cells 16 --res 32 --cin 128 --cout 128
+    python -m maple_b200.opbench wgrad --cells 16 --res 32 --cin 128 --cout 128
     python -m maple_b200.opbench ebe --res 64
 
 ``conv``: the periodic 3x3x3 BF16 convolution of the learned guess
 (maple_nn_conv3d) on B cells of n^3 voxels; prints TFLOP/s (2 * voxels * 27 *
 cin * cout flops per launch).
+
+``wgrad``: its weight gradient (maple_nn_conv3d_wgrad), same flop count.
 
 ``ebe``: the fine-level elastic operator (6 load cases) of one seeded cell in
 the element-batched tensor-core form (maple_matvec_ebe_tc: gather, tcgen05
@@ -65,6 +68,24 @@ def conv(args):
     del lib
 
 
+def wgrad(args):
+    dev = torch.device("cuda", 0)
+    B, n, cin, cout = args.cells, args.res, args.cin, args.cout
+    N = n ** 3
+    g = torch.Generator(device=dev).manual_seed(0)
+    x = torch.randn(B, N, cin, device=dev, generator=g).to(torch.bfloat16)
+    dz = torch.randn(B, N, cout, device=dev, generator=g).to(torch.bfloat16)
+    dW = torch.zeros(27, cin, cout, dtype=torch.float32, device=dev)
+    s = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    us = _time_us(lambda: _lib.nn_call("maple_nn_conv3d_wgrad", _p(x), _p(dz), _p(dW), None, B, n, cin, cout, 3, s),
+                  dev, args.reps)
+    flag = C.c_int(-1)
+    _lib.nn_call("maple_nn_wait_status", C.byref(flag), s)
+    flops = 2.0 * B * N * 27 * cin * cout
+    print(f"conv3d weight gradient 3x3x3 B={B} n={n} cin={cin} cout={cout}: {us:.1f} us, "
+          f"{flops / us / 1e6:.1f} TFLOP/s, waits timed out: {flag.value}")
+
+
 def ebe(args):
     from .core import HomogenizationContext
     from .batch import seeded_design
@@ -101,11 +122,17 @@ def main(argv=None):
     a.add_argument("--cin", type=int, default=128)
     a.add_argument("--cout", type=int, default=128)
     a.add_argument("--reps", type=int, default=10)
+    w = sub.add_parser("wgrad")
+    w.add_argument("--cells", type=int, default=16)
+    w.add_argument("--res", type=int, default=32)
+    w.add_argument("--cin", type=int, default=128)
+    w.add_argument("--cout", type=int, default=128)
+    w.add_argument("--reps", type=int, default=10)
     b = sub.add_parser("ebe")
     b.add_argument("--res", type=int, default=64)
     b.add_argument("--reps", type=int, default=10)
     args = ap.parse_args(argv)
-    {"conv": conv, "ebe": ebe}[args.op](args)
+    {"conv": conv, "wgrad": wgrad, "ebe": ebe}[args.op](args)
 
 
 if __name__ == "__main__":
