@@ -134,6 +134,22 @@ int maple_set_tail_fused(maple_ctx* ctx, int enable);
  * identical either way. */
 int maple_set_pdl(maple_ctx* ctx, int enable);
 
+/* Run the PCG iterations of a solve as a loop on the device: the captured
+ * iteration body sits in a conditional WHILE graph node, whose last kernel
+ * counts the iteration and ends the loop once every active cell has converged
+ * or the iteration limit is reached, so the host waits once per solve instead
+ * of once per iteration (check_every of maple_set_solver_options then has no
+ * effect).  Default on; 0, or a runtime that refuses conditional graph nodes,
+ * replays one graph per iteration.  Results and iteration counts are
+ * identical either way.  The reference's loop (utils/EBE_GMG.py:858-885,
+ * GMGSolver.solve) tests the residual on the host after every cycle. */
+int maple_set_device_loop(maple_ctx* ctx, int enable);
+
+/* *state = 1 when a device-side loop graph of this context is built and in
+ * use, 0 when none has been built (no graph solve yet, or the loop is off),
+ * -1 when the runtime refused one and per-iteration graphs run instead. */
+int maple_get_device_loop(maple_ctx* ctx, int* state);
+
 /* Chebyshev degree of the smoother on multigrid levels 2 and deeper (level 0
  * and 1 use the degree of maple_set_solver_options).  0 (default): automatic,
  * 3 on every level below level 1 and on a level 1 of at most 16^3 nodes,

@@ -177,6 +177,19 @@ class HomogenizationContext:
         tail with programmatic dependent launch (default on)."""
         _lib.check(self._lib.maple_set_pdl(self._h, int(bool(enable))))
 
+    def set_device_loop(self, enable: bool = True):
+        """Loop the PCG iterations of a solve on the device (a conditional
+        graph node; the host waits once per solve).  Default on; off: one
+        graph replay and one host convergence check per iteration."""
+        _lib.check(self._lib.maple_set_device_loop(self._h, int(bool(enable))))
+
+    def device_loop_state(self) -> int:
+        """1: a device-side loop graph is in use; 0: none built yet; -1: the
+        runtime refused it (per-iteration graphs run instead)."""
+        v = C.c_int(0)
+        _lib.check(self._lib.maple_get_device_loop(self._h, C.byref(v)))
+        return int(v.value)
+
     def set_mixed_mode(self, mode: str = "flexible"):
         """Form of the mixed-precision solve: "flexible" (FP64 flexible PCG
         preconditioned by the FP32 V-cycle) or "refine" (FP32 MG-PCG inside

@@ -158,7 +158,8 @@ struct Lane {
   double *o_rr = nullptr, *o_bn = nullptr, *o_scale = nullptr, *o_inv = nullptr;  // outer refinement
   int *o_done = nullptr, *o_run = nullptr;
   int* o_live = nullptr;   // refinement: cells still refined (active, not broken down)
-  int* h_flags = nullptr;  // pinned host [B]
+  int* h_flags = nullptr;  // pinned host [B + 1]: convergence flags, then the device loop's count
+  int* loop = nullptr;     // device [2]: iterations run by the device-side loop, its limit
   int* breakdown = nullptr;
   cudaStream_t cap_stream = nullptr;
   // the coarsest-level inverse of a hierarchy build runs here, beside the
@@ -201,6 +202,10 @@ struct maple_ctx {
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
     unsigned long long kernels = 0;  // kernel nodes per replay (for launch counting)
+    // the same body inside a conditional WHILE node (the whole solve in one replay)
+    cudaGraphExec_t loop_exec = nullptr;
+    unsigned long long loop_kernels = 0;  // kernels per loop iteration
+    bool loop_failed = false;             // the runtime refused the conditional graph
   } graphs[2][3];  // [physics][FP64 PCG, flexible mixed PCG, FP32 inner PCG of refinement]
   cudaStream_t aux_stream = nullptr;  // second physics of a concurrent OC step
   cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
@@ -210,6 +215,7 @@ struct maple_ctx {
   int nine_max_n = 64;     // coarse levels with n <= this use k_apply_stencil_nine; 0: never
   bool tail_fused = true;  // FP32 8^3 level + 4^3 coarsest solve as one cluster launch (k_tail_cycle)
   bool pdl = true;         // coarse-level launches with programmatic dependent launch
+  bool device_loop = true; // PCG iterations looped on device (conditional graph node)
   int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
   // manufacturability penalties of the OC objective (maple_set_penalties)
   double lambda_print = 0, lambda_cavity = 0;
@@ -756,18 +762,106 @@ __global__ void k_init_flags(const int* active, const int* outer_run, int* done,
   for (int r = 0; r < R; ++r) done[b * R + r] = a ? 0 : 1;
 }
 
+// Ends one iteration of the device-side PCG loop: counts it and keeps the
+// loop running while an active cell has not converged and fewer than
+// loop[1] iterations ran.  One CTA.
+__global__ void k_loop_next(cudaGraphConditionalHandle h, const int* __restrict__ cell_done, int B, int* loop) {
+  int open = 0;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) open |= cell_done[b] == 0;
+  open = __syncthreads_or(open);
+  if (threadIdx.x == 0) {
+    const int n = loop[0] + 1;
+    loop[0] = n;
+    cudaGraphSetConditional(h, (open && n < loop[1]) ? 1u : 0u);
+  }
+}
+
+__global__ void k_loop_arm(int* loop, int limit) {
+  loop[0] = 0;
+  loop[1] = limit;
+}
+
+// Captures the iteration body, followed by k_loop_next, as the body of a
+// conditional WHILE node, so that one replay runs a whole solve with no host
+// round trip between iterations.  Returns false (and the caller keeps the
+// per-iteration graphs) when the runtime refuses any part of it.
+template <typename Body>
+static bool loop_graph(maple_ctx* c, maple_ctx::GraphEntry& ge, Body& body) {
+  if (ge.loop_exec) return true;
+  if (ge.loop_failed) return false;
+  Lane& ln = LN(c);
+  if (!ln.cap_stream) CK(cudaStreamCreateWithFlags(&ln.cap_stream, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  bool ok = false;
+  const unsigned long long before = tl_launches;
+  cudaGraphConditionalHandle h{};
+  cudaGraphNodeParams np{};
+  cudaGraphNode_t node{};
+  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess) {
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    if (cudaGraphAddNode(&node, g, nullptr, 0, &np) == cudaSuccess &&
+        cudaStreamBeginCaptureToGraph(ln.cap_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      bool captured = true;
+      try {
+        body(ln.cap_stream);
+        KL(c, ln.cap_stream, k_loop_next<<<1, 256, 0, ln.cap_stream>>>(h, ln.sc.cell_done, c->B, ln.loop));
+      } catch (const Failure&) {
+        captured = false;
+      }
+      cudaGraph_t out = nullptr;
+      const bool ended = cudaStreamEndCapture(ln.cap_stream, &out) == cudaSuccess;
+      ok = captured && ended && cudaGraphInstantiate(&ge.loop_exec, g, 0) == cudaSuccess;
+    }
+  }
+  (void)cudaGetLastError();  // a refused step leaves the per-iteration graphs in use
+  cudaGraphDestroy(g);
+  ge.loop_kernels = tl_launches - before;
+  g_launches.fetch_sub(ge.loop_kernels);  // captured, not launched
+  tl_launches -= ge.loop_kernels;
+  if (!ok) {
+    if (ge.loop_exec) cudaGraphExecDestroy(ge.loop_exec);
+    ge.loop_exec = nullptr;
+    ge.loop_failed = true;
+  }
+  return ok;
+}
+
 // Runs the PCG iteration body until every active cell has converged or maxit
-// iterations ran.  The body is captured once into a CUDA graph per
-// (physics, solve form) and replayed (the tolerance is read on device, so one
-// graph serves every tolerance); the convergence flags are read back
-// after every replay (cells that converged skip all further work on device).
-// The first iteration of a solve always runs eagerly, which also performs the
-// one-time kernel attribute setup outside of any capture.
+// iterations ran.  The first iteration of a solve always runs eagerly, which
+// also performs the one-time kernel attribute setup outside of any capture.
+// With graphs, the rest runs as one replay of the device-side loop
+// (loop_graph) and the host waits once per solve; where that is off or
+// refused, the body is captured once into a CUDA graph per (physics, solve
+// form) and replayed per iteration, the convergence flags read back after
+// every check_every replays.  Either graph serves every tolerance (it is read
+// on device); cells that converged skip all further work on device.
 template <typename Body>
 static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, int maxit, Body& body,
                            cudaStream_t s) {
   const bool graphs = c->use_graphs && !c->profiling;
-  for (int it = 1; it <= maxit; ++it) {
+  int first = 1;
+  if (graphs && c->device_loop && maxit > 1) {
+    body(s);
+    if (all_done(c, LN(c).sc.cell_done, nullptr, s)) return;
+    if (loop_graph(c, ge, body)) {
+      Lane& ln = LN(c);
+      KL(c, s, k_loop_arm<<<1, 1, 0, s>>>(ln.loop, maxit - 1));
+      CK(cudaGraphLaunch(ge.loop_exec, s));
+      CK(cudaMemcpyAsync(ln.h_flags + c->B, ln.loop, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      const unsigned long long n = (unsigned long long)std::max(ln.h_flags[c->B], 0) * ge.loop_kernels;
+      g_launches.fetch_add(n);
+      tl_launches += n;
+      return;
+    }
+    first = 2;
+  }
+  for (int it = first; it <= maxit; ++it) {
     if (!graphs || it == 1) {
       body(s);
     } else {
@@ -803,7 +897,10 @@ static void drop_graphs(maple_ctx* c) {
   for (auto& row : c->graphs)
     for (auto& ge : row) {
       if (ge.exec) cudaGraphExecDestroy(ge.exec);
+      if (ge.loop_exec) cudaGraphExecDestroy(ge.loop_exec);
       ge.exec = nullptr;
+      ge.loop_exec = nullptr;
+      ge.loop_failed = false;
     }
 }
 
@@ -1508,7 +1605,8 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
         L.o_live = dnew<int>(c, B);
         L.breakdown = dnew<int>(c, 1);
         CK(cudaMemset(L.breakdown, 0, sizeof(int)));
-        CK(cudaMallocHost(&L.h_flags, B * sizeof(int)));
+        L.loop = dnew<int>(c, 2);
+        CK(cudaMallocHost(&L.h_flags, (B + 1) * sizeof(int)));
       }
       c->active = dnew<int>(c, B);
       c->h_active.assign(B, 1);
@@ -1789,6 +1887,27 @@ int maple_set_pdl(maple_ctx* c, int enable) {
     require(c != nullptr, "ctx is NULL");
     drop_graphs(c);
     c->pdl = enable != 0;
+  });
+}
+
+int maple_set_device_loop(maple_ctx* c, int enable) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    drop_graphs(c);
+    c->device_loop = enable != 0;
+  });
+}
+
+int maple_get_device_loop(maple_ctx* c, int* state) {
+  return guarded([&] {
+    require(c != nullptr && state != nullptr, "NULL argument");
+    int st = 0;
+    for (auto& row : c->graphs)
+      for (auto& ge : row) {
+        if (ge.loop_failed) st = -1;
+        else if (ge.loop_exec && st == 0) st = 1;
+      }
+    *state = st;
   });
 }
 

@@ -347,6 +347,45 @@ def test_pdl_matches_plain_launches(lib, precision, r):
             assert np.array_equal(it0[[0, 2]], it1[[0, 2]]), (phys, key)
 
 
+@pytest.mark.parametrize("form", ["fp64", "mixed", "refine"])
+def test_device_loop_matches_host_loop(lib, form):
+    """The device-side PCG loop (conditional graph node, one host wait per
+    solve) runs the same iterations as the per-iteration graph replays with a
+    host convergence check after each: bit-identical solutions and iteration
+    counts, with an inactive cell, and the same stop at an iteration cap."""
+    from maple_b200.core import HomogenizationContext
+    r = 16
+    precision = "fp64" if form == "fp64" else "mixed"
+    rho = T(np.stack([simp(O.seed_density(s, r, 2.0, 0.3)).reshape(-1) for s in (11, 12, 13)]))
+    out = {}
+    for loop in (False, True):
+        c = HomogenizationContext(r, ncells=3)
+        c.set_device_loop(loop)
+        if form == "refine":
+            c.set_mixed_mode("refine")
+        c.set_active([1, 0, 1])
+        for phys in ("elastic", "thermal"):
+            c.set_density(phys, rho, precision)
+            info = c.solve(phys, precision, rtol=1e-10, maxit=300)
+            assert (info.status[[0, 2]] & 1).all()
+            out[(loop, phys)] = (info.iters.copy(), c.solution(phys)[[0, 2]].clone())
+            # capped: the loop stops at maxit with the cells unconverged
+            c.set_density(phys, rho, precision)
+            capped = c.solve(phys, precision, rtol=1e-14, maxit=4)
+            out[(loop, phys, "cap")] = (capped.iters.copy(), capped.status.copy(), c.solution(phys)[[0, 2]].clone())
+        assert c.device_loop_state() == (1 if loop else 0)
+        c.close()
+    for phys in ("elastic", "thermal"):
+        it0, u0 = out[(False, phys)]
+        it1, u1 = out[(True, phys)]
+        assert torch.equal(u0, u1), (phys, (u0 - u1).abs().max().item())
+        assert np.array_equal(it0[[0, 2]], it1[[0, 2]]), (phys, it0, it1)
+        c0, s0, v0 = out[(False, phys, "cap")]
+        c1, s1, v1 = out[(True, phys, "cap")]
+        assert np.array_equal(c0[[0, 2]], c1[[0, 2]]) and np.array_equal(s0[[0, 2]], s1[[0, 2]]), (phys, c0, c1)
+        assert torch.equal(v0, v1)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_graph_replay_matches_eager(lib, precision):
     """The captured PCG iteration replays the same launches: identical results
