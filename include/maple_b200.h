@@ -86,11 +86,29 @@ int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio,
  *                         residual r = b - A x, the convergence test, the inner
  *                         solve to the inner tolerance of
  *                         maple_set_solver_options, and x += ||r|| e in FP64.
- * Both stop at the same FP64 residual test ||b - A x|| <= rtol ||b|| per load
+ *   MAPLE_MIXED_RELIABLE  (default) FP32 MG-PCG (FP32 fine operator and vectors, FP64
+ *                         accumulated dots) on the residual scaled to unit
+ *                         norm, with reliable updates: when a load case's
+ *                         recurrence residual fell by the factor of
+ *                         maple_set_reliable_delta, or passes the tolerance
+ *                         test, the FP32 correction is folded into the FP64
+ *                         iterate and the residual is recomputed as b - A x in
+ *                         FP64 and continues the iteration (the direction is
+ *                         kept, not restarted).
+ * All stop at the same FP64 residual test ||b - A x|| <= rtol ||b|| per load
  * case.  The reference solves in one precision (utils/EBE_GMG.py:758-885,
  * dtype argument). */
-enum { MAPLE_MIXED_FLEXIBLE = 0, MAPLE_MIXED_REFINE = 1 };
+enum { MAPLE_MIXED_FLEXIBLE = 0, MAPLE_MIXED_REFINE = 1, MAPLE_MIXED_RELIABLE = 2 };
 int maple_set_mixed_mode(maple_ctx* ctx, int mode);
+
+/* MAPLE_MIXED_RELIABLE options: delta, the residual reduction per FP32
+ * segment, in (0, 1) (default 1e-3); handover, the iterations after which a
+ * cell that has not converged continues in the MAPLE_MIXED_FLEXIBLE form from
+ * its iterate, within the same iteration limit (default 120: FP32
+ * recurrences lose orthogonality on badly conditioned cells, e.g. near-void
+ * designs with floating stiff islands, where FP64 recurrences still
+ * converge). */
+int maple_set_reliable_options(maple_ctx* ctx, double delta, int handover);
 
 /* Warm start of the solves of maple_oc_step (with warm = 1) along the OC
  * trajectory: from u_k + theta (u_k - u_{k-1}), the last two steps'

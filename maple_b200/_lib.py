@@ -46,6 +46,7 @@ SIGNATURES = {
     "maple_set_tail_fused": (_I, [_P, _I]),
     "maple_set_pdl": (_I, [_P, _I]),
     "maple_set_device_loop": (_I, [_P, _I]),
+    "maple_set_reliable_options": (_I, [_P, _D, _I]),
     "maple_get_device_loop": (_I, [_P, _P]),
     "maple_set_symmetry": (_I, [_P, _I, _I]),
     "maple_set_penalties": (_I, [_P, _D, _D, _I, _D, _D, _D, _I, _I, _I, _I, _I, _I, _I, _I, _I]),

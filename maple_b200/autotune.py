@@ -18,8 +18,12 @@ Knobs (runtime settings of a ``HomogenizationContext``):
   tile kernel;
 * ``tail_fused``: the 8^3 level and the coarsest solve as one cluster launch;
 * ``pdl``: programmatic dependent launch of the small coarse-level launches;
-* ``check_every``: PCG iterations between host convergence checks;
-* ``mixed_mode`` (mixed precision only): flexible FP64 PCG or FP32 PCG in FP64
+* ``device_loop``: the PCG iterations looped on the device (one host wait
+  per solve) or one graph replay per iteration;
+* ``check_every``: PCG iterations between host convergence checks (without
+  the device loop);
+* ``mixed_mode`` (mixed precision only): FP32 PCG with FP64 residual
+  replacement (reliable updates), flexible FP64 PCG, or FP32 PCG in FP64
   refinement.
 
 Search: coordinate descent from the library defaults, two passes over the
@@ -45,10 +49,11 @@ import torch
 from .core import HomogenizationContext
 
 DEFAULTS = dict(fine_degree=1, coarse_degree=0, nine_max_n=64, split_min_n=32, tail_fused=True, pdl=True,
-                check_every=1, mixed_mode="flexible")
+                device_loop=True, check_every=1, mixed_mode="reliable")
 
 SPACE = dict(fine_degree=[1, 2], coarse_degree=[0, 2, 3, 4], nine_max_n=[0, 16, 32, 64], split_min_n=[0, 16, 32],
-             tail_fused=[True, False], pdl=[True, False], check_every=[1, 2], mixed_mode=["flexible", "refine"])
+             tail_fused=[True, False], pdl=[True, False], device_loop=[True, False], check_every=[1, 2],
+             mixed_mode=["reliable", "flexible", "refine"])
 
 CACHE = os.path.join(os.path.expanduser("~"), ".cache", "maple_b200", "autotune.json")
 
@@ -71,6 +76,7 @@ def apply(ctx: HomogenizationContext, settings: Dict[str, object]) -> None:
     ctx.set_stencil_split(int(s["split_min_n"]))
     ctx.set_tail_fused(bool(s["tail_fused"]))
     ctx.set_pdl(bool(s["pdl"]))
+    ctx.set_device_loop(bool(s["device_loop"]))
     ctx.set_mixed_mode(str(s["mixed_mode"]))
 
 

@@ -190,14 +190,21 @@ class HomogenizationContext:
         _lib.check(self._lib.maple_get_device_loop(self._h, C.byref(v)))
         return int(v.value)
 
-    def set_mixed_mode(self, mode: str = "flexible"):
-        """Form of the mixed-precision solve: "flexible" (FP64 flexible PCG
-        preconditioned by the FP32 V-cycle) or "refine" (FP32 MG-PCG inside
-        FP64 iterative refinement)."""
-        modes = {"flexible": 0, "refine": 1}
+    def set_mixed_mode(self, mode: str = "reliable"):
+        """Form of the mixed-precision solve: "reliable" (default: FP32
+        MG-PCG with FP64 residual replacement, the direction kept),
+        "flexible" (FP64 flexible PCG preconditioned by the FP32 V-cycle) or
+        "refine" (FP32 MG-PCG inside FP64 iterative refinement)."""
+        modes = {"flexible": 0, "refine": 1, "reliable": 2}
         if mode not in modes:
             raise ValueError(f"mixed mode must be one of {sorted(modes)}, got {mode!r}")
         _lib.check(self._lib.maple_set_mixed_mode(self._h, modes[mode]))
+
+    def set_reliable_options(self, delta: float = 1e-3, handover: int = 120):
+        """The "reliable" mixed form: residual reduction per FP32 segment, and
+        the iterations after which an unconverged cell continues in the
+        flexible form."""
+        _lib.check(self._lib.maple_set_reliable_options(self._h, float(delta), int(handover)))
 
     def set_extrapolation(self, theta: float = 0.0):
         """oc_step(warm=True) starts its solves from u_k + theta (u_k - u_{k-1})

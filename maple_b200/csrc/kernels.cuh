@@ -2093,6 +2093,57 @@ __global__ void k_add_f32_scaled(double* __restrict__ dst, const float* __restri
   }
 }
 
+// Reliable updates of the mixed-precision PCG (the iteration in FP32 on a
+// residual scaled to unit norm, FP64 residual replacement).  Cells with
+// flag[b] set fold the FP32 correction into the FP64 iterate,
+// x += inv * x32 (inv: the column's residual norm at the last replacement),
+// and restart the correction, x32 = 0.
+template <int R, int D>
+__global__ void k_flush_f32(double* __restrict__ x, float* __restrict__ x32, const double* __restrict__ inv, int N,
+                            const int* flag) {
+  const int b = blockIdx.y;
+  if (flag && !flag[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= N) return;
+  const size_t o = (size_t)b * N * R * D + idx;
+#pragma unroll
+  for (int c = 0; c < R; ++c) {
+    const double s = inv[b * R + c];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const size_t j = o + (size_t)(c * D + i) * N;
+      x[j] = fma(s, (double)x32[j], x[j]);
+      x32[j] = 0.0f;
+    }
+  }
+}
+
+// After the FP64 residual r of the flushed iterate: r32 = scale * r
+// (scale = 1 / ||r||), and the direction and its image rescaled to the new
+// unit, p32 *= t, q32 *= t (t = old ||r|| / new ||r||).  Cells with flag[b].
+template <int R, int D>
+__global__ void k_rel_rescale(const double* __restrict__ r, float* __restrict__ r32, float* __restrict__ p32,
+                              float* __restrict__ q32, const double* __restrict__ scale, const double* __restrict__ t,
+                              int N, const int* flag) {
+  const int b = blockIdx.y;
+  if (flag && !flag[b]) return;
+  const int idx = blockIdx.x * kThreads + threadIdx.x;
+  if (idx >= N) return;
+  const size_t o = (size_t)b * N * R * D + idx;
+#pragma unroll
+  for (int c = 0; c < R; ++c) {
+    const double sc = scale[b * R + c];
+    const float tc = (float)t[b * R + c];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const size_t j = o + (size_t)(c * D + i) * N;
+      r32[j] = (float)(r[j] * sc);
+      p32[j] *= tc;
+      q32[j] *= tc;
+    }
+  }
+}
+
 // partial dots r.z and (optionally) q.z of z = inv * z32, formed in FP64 and
 // not stored (k_pcg_direction_f32 forms it again for the direction update)
 template <int R, int D>
@@ -2131,7 +2182,17 @@ __global__ void k_precond_back(const float* __restrict__ z32, const double* __re
 //   BETA       beta = rz_new / rz, rz = rz_new
 //   BETA_FLEX  flexible beta = -alpha (q.z) / rz, rz = r.z (first: beta = 0)
 //   SET_RZ     rz = rz_new
-enum { RED_PLAIN = 0, RED_ALPHA = 1, RED_CHECK = 2, RED_BETA = 3, RED_BETA_FLEX = 4, RED_SET_RZ = 5 };
+//   RELCHECK   (reliable updates) advance the iteration count and flag the cell
+//              for a residual replacement (rel) when a live column's recurrence
+//              residual, in units of its last replaced residual (inv), fell
+//              below delta2 (squared) or passes the tolerance test; no column is
+//              marked done here
+//   RELSET     (flagged cells) the true residual norms of the replacement: mark
+//              columns with ||r||^2 <= rtol^2 ||b||^2 done (the cell done when
+//              all are, its run flag cleared), set scale = 1/||r||, t = old
+//              ||r|| / new ||r||, inv = ||r||, and rz *= t^2
+enum { RED_PLAIN = 0, RED_ALPHA = 1, RED_CHECK = 2, RED_BETA = 3, RED_BETA_FLEX = 4, RED_SET_RZ = 5,
+       RED_RELCHECK = 6, RED_RELSET = 7 };
 struct RedOp {
   PcgScalars s;
   int R = 0;
@@ -2143,6 +2204,12 @@ struct RedOp {
   double* scale = nullptr;   // CHECK: column scales 1/||r|| and ||r|| (nullable)
   double* inv = nullptr;
   int first = 0;             // BETA_FLEX
+  int* rel = nullptr;        // RELCHECK, RELSET: per cell, a residual replacement is due
+  double delta2 = 0;         // RELCHECK: squared reduction per FP32 segment
+  double* t = nullptr;       // RELSET: rescaling of the direction
+  // RELCHECK inside a captured graph of one cell: the conditional IF handle
+  // around the replacement, set to "a replacement is due" (0: none)
+  cudaGraphConditionalHandle cond = 0;
 };
 
 template <int K, int OP>
@@ -2221,7 +2288,53 @@ __global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* _
     }
   } else if constexpr (OP == RED_SET_RZ) {
     if (col) s.rz[i] = s.rz_new[i];
+  } else if constexpr (OP == RED_RELCHECK) {
+    const int was_done = s.cell_done[b];
+    int due = 0;
+    if (col && !was_done && !s.done[i]) {
+      const double rt2 = op.rtol2_dev ? *op.rtol2_dev : op.rtol2;
+      const double rr = s.rr[i], nrm = op.inv[i];
+      due = rr <= op.delta2 || rr * nrm * nrm <= rt2 * s.bnorm2[i];
+    }
+    const bool any = __any_sync(0xffffffffu, due != 0);
+    if (c == 0) {
+      if (!was_done && op.count) s.iters[b] += 1;
+      op.rel[b] = any ? 1 : 0;
+      if (op.cond) cudaGraphSetConditional(op.cond, any ? 1u : 0u);
+    }
+  } else if constexpr (OP == RED_RELSET) {
+    if (!op.rel[b]) return;
+    int dn = 1;
+    if (col) {
+      const double rr = out[(size_t)b * K + c];
+      const double rt2 = op.rtol2_dev ? *op.rtol2_dev : op.rtol2;
+      dn = s.done[i];
+      if (!dn && rr <= rt2 * s.bnorm2[i]) {
+        dn = 1;
+        s.done[i] = 1;
+      }
+      const double nrm = sqrt(fmax(rr, 0.0));
+      const double tt = nrm > 0 ? op.inv[i] / nrm : 0.0;
+      op.scale[i] = nrm > 0 ? 1.0 / nrm : 0.0;
+      op.t[i] = tt;
+      op.inv[i] = nrm;
+      s.rz[i] *= tt * tt;
+    }
+    const bool all = __all_sync(0xffffffffu, dn != 0);
+    if (c == 0 && all) {
+      s.cell_done[b] = 1;
+      op.run[b] = 0;
+    }
   }
+}
+
+// Sets a conditional IF handle to "some cell has a residual replacement due"
+// (several cells; one CTA).
+__global__ void k_rel_cond(cudaGraphConditionalHandle h, const int* __restrict__ rel, int B) {
+  int any = 0;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) any |= rel[b] != 0;
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
 }
 
 // deterministic pseudo-random start vector for power iterations

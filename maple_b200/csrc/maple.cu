@@ -158,10 +158,13 @@ struct Lane {
   double *o_rr = nullptr, *o_bn = nullptr, *o_scale = nullptr, *o_inv = nullptr;  // outer refinement
   int *o_done = nullptr, *o_run = nullptr;
   int* o_live = nullptr;   // refinement: cells still refined (active, not broken down)
+  int* rel = nullptr;      // reliable updates: per cell, a residual replacement is due
+  double* o_t = nullptr;   // reliable updates: per (cell, rhs) rescaling of the direction
   int* h_flags = nullptr;  // pinned host [B + 1]: convergence flags, then the device loop's count
   int* loop = nullptr;     // device [2]: iterations run by the device-side loop, its limit
   int* breakdown = nullptr;
   cudaStream_t cap_stream = nullptr;
+  cudaStream_t cap_stream2 = nullptr;  // captures the body of a conditional node inside a capture
   // the coarsest-level inverse of a hierarchy build runs here, beside the
   // power iterations of the other levels
   cudaStream_t side = nullptr;
@@ -206,7 +209,7 @@ struct maple_ctx {
     cudaGraphExec_t loop_exec = nullptr;
     unsigned long long loop_kernels = 0;  // kernels per loop iteration
     bool loop_failed = false;             // the runtime refused the conditional graph
-  } graphs[2][3];  // [physics][FP64 PCG, flexible mixed PCG, FP32 inner PCG of refinement]
+  } graphs[2][4];  // [physics][FP64 PCG, flexible mixed PCG, FP32 inner PCG of refinement, reliable updates]
   cudaStream_t aux_stream = nullptr;  // second physics of a concurrent OC step
   cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
   bool use_graphs = true;
@@ -244,7 +247,10 @@ struct maple_ctx {
   double power_safety = 1.15;
   double inner_rtol = 1e-5;
   int check_every = 1;
-  int mixed_mode = 0;  // MAPLE_MIXED_FLEXIBLE or MAPLE_MIXED_REFINE
+  int mixed_mode = 2;  // MAPLE_MIXED_FLEXIBLE, MAPLE_MIXED_REFINE or MAPLE_MIXED_RELIABLE (default)
+  double rel_delta = 1e-3;  // reliable updates: residual reduction per FP32 segment
+  int rel_handover = 120;   // reliable updates: iterations before an unconverged cell moves to the flexible form
+  bool rel_cond = true;     // reliable updates: the replacement in a conditional IF node of captured graphs
   double extrap = 0.0;  // warm start of maple_oc_step: u + extrap * (u - u_prev)
 };
 
@@ -983,7 +989,7 @@ static void precondition_f32(maple_ctx* c, Phys& p, const double* r, const doubl
 
 template <int D, int R>
 static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_zero, double rtol, int maxit,
-                      cudaStream_t s) {
+                      cudaStream_t s, const int* mask = nullptr) {
   const int B = c->B, N = nodes(c->n[0]);
   const size_t vbytes = (size_t)B * N * R * D * sizeof(double);
   Scalars& sc = LN(c).sc;
@@ -992,7 +998,7 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
   Ops<double>& o64 = p.o64;
   double *r = p.r64, *pv = p.p64, *q = p.q64;
   const float* z32 = p.o32.U[0][1];  // preconditioner output; z = ||r|| z32 is formed where it is used
-  KL(c, s, k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, nullptr, sc.done, sc.cell_done, sc.run, sc.iters, B, R));
+  KL(c, s, k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, mask, sc.done, sc.cell_done, sc.run, sc.iters, B, R));
   const int* run = sc.run;
   if (x_zero) {
     CK(cudaMemsetAsync(x, 0, vbytes, s));
@@ -1039,6 +1045,151 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
     KL(c, st, k_pcg_direction_f32<R, D, false><<<g2(N, B), kThreads, 0, st>>>(pv, z32, LN(c).o_inv, sc.beta, N, run));
   };
   run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MAPLE_MIXED], maxit, body, s);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision, reliable-update form: the whole PCG iteration in FP32 (FP32
+// fine operator, FP32 vectors, FP64-accumulated dots) on the residual scaled
+// to unit norm, with the FP64 iterate and residual replaced from time to time
+// instead of restarting.  A cell is flagged when a live column's recurrence
+// residual fell by delta since the last replacement, or passes the tolerance
+// test; its FP32 correction is folded into the FP64 iterate, the residual
+// b - A x is computed in FP64, tested (only this test marks a column
+// converged), scaled to unit norm and continues the iteration with the same
+// (rescaled) direction, so the Krylov space is kept.
+// ---------------------------------------------------------------------------
+constexpr int MIXED_RELIABLE_GRAPH = 3;
+
+template <int D, int R>
+static void pcg_reliable(maple_ctx* c, Phys& p, const double* b, double* x, bool x_zero, double rtol, int maxit,
+                         cudaStream_t s) {
+  const int B = c->B, N = nodes(c->n[0]);
+  const size_t vbytes = (size_t)B * N * R * D * sizeof(double), v32 = (size_t)B * N * R * D * sizeof(float);
+  Lane& ln = LN(c);
+  Scalars& sc = ln.sc;
+  const unsigned nb = nblk(N), nbf = (unsigned)fine_tiles(c->n[0]);
+  PcgScalars ps{sc.rz, sc.rz_new, sc.pq, sc.rr, sc.bnorm2, sc.alpha, sc.beta, sc.done, sc.cell_done, sc.iters};
+  Ops<double>& o64 = p.o64;
+  Ops<float>& o = p.o32;
+  double* r = p.r64;
+  const float* z = o.U[0][1];  // preconditioner output
+  KL(c, s, k_init_flags<<<nblk(B), kThreads, 0, s>>>(c->active, nullptr, sc.done, sc.cell_done, sc.run, sc.iters, B, R));
+  const int* run = sc.run;
+  if (x_zero) {
+    CK(cudaMemsetAsync(x, 0, vbytes, s));
+    CK(cudaMemcpyAsync(r, b, vbytes, cudaMemcpyDeviceToDevice, s));
+  } else {
+    ApplyArgs<double> a{};
+    a.u = x;
+    a.f = b;
+    a.out = r;
+    apply<double, D, R, M_RES>(c, p, o64, 0, a, run, s);
+  }
+  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(b, b, ln.part, N, run));
+  reduce<R>(c, ln.part, nb, sc.bnorm2, s);
+  KL(c, s, k_dot<double, R, D><<<g2(N, B), kThreads, 0, s>>>(r, r, ln.part, N, run));
+  RedOp op{};
+  op.s = ps;
+  op.R = R;
+  op.breakdown = ln.breakdown;
+  op.rtol2 = rtol * rtol;
+  op.rtol2_dev = sc.rtol2;
+  KL(c, s, k_fill<double><<<1, 32, 0, s>>>(sc.rtol2, 1, rtol * rtol));
+  op.run = sc.run;
+  op.scale = ln.o_scale;
+  op.inv = ln.o_inv;
+  op.rel = ln.rel;
+  op.t = ln.o_t;
+  op.delta2 = c->rel_delta * c->rel_delta;
+  RedOp op0 = op;  // before the loop: no iteration counted; column scales of the first residual
+  reduce_op<R, RED_CHECK>(c, ln.part, nb, sc.rr, op0, s);
+  if (all_done(c, sc.cell_done, run, s)) return;
+  CK(cudaMemsetAsync(o.x, 0, v32, s));
+  KL(c, s, k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, ln.o_scale, N, run));
+  vcycle<float, D, R>(c, p, o, 0, o.r, run, ln.part, s);
+  reduce_op<R, RED_SET_RZ>(c, ln.part, nbf, sc.rz_new, op, s);
+  CK(cudaMemcpyAsync(o.p, z, v32, cudaMemcpyDeviceToDevice, s));
+  op.count = 1;
+  auto body = [&](cudaStream_t st) {
+    {
+      ApplyArgs<float> a{};
+      a.u = o.p;
+      a.out = o.q;
+      a.part = ln.part;
+      apply<float, D, R, M_MV>(c, p, o, 0, a, run, st);
+    }
+    reduce_op<R, RED_ALPHA>(c, ln.part, nbf, sc.pq, op, st);
+    KL(c, st, k_pcg_update<float, R, D><<<g2(N, B), kThreads, 0, st>>>(o.x, o.r, o.p, o.q, sc.alpha, ln.part, N, run));
+    // Residual replacement of the flagged cells (every launch skips the
+    // others).  In a captured graph it sits in a conditional IF node, so the
+    // iterations without a replacement launch none of it.
+    auto replace = [&](cudaStream_t sr) {
+      KL(c, sr, k_flush_f32<R, D><<<g2(N, B), kThreads, 0, sr>>>(x, o.x, ln.o_inv, N, ln.rel));
+      ApplyArgs<double> a{};
+      a.u = x;
+      a.f = b;
+      a.out = r;
+      apply<double, D, R, M_RES>(c, p, o64, 0, a, ln.rel, sr);
+      KL(c, sr, k_dot<double, R, D><<<g2(N, B), kThreads, 0, sr>>>(r, r, ln.part, N, ln.rel));
+      reduce_op<R, RED_RELSET>(c, ln.part, nb, ln.o_rr, op, sr);
+      KL(c, sr, k_rel_rescale<R, D><<<g2(N, B), kThreads, 0, sr>>>(r, o.r, o.p, o.q, ln.o_scale, ln.o_t, N, ln.rel));
+    };
+    cudaGraphConditionalHandle h = 0;
+    cudaGraph_t cg = nullptr;
+    if (c->rel_cond) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg) != cudaSuccess || cs != cudaStreamCaptureStatusActive ||
+          cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+        h = 0;
+      (void)cudaGetLastError();
+    }
+    RedOp opc = op;
+    opc.cond = B == 1 ? h : 0;
+    reduce_op<R, RED_RELCHECK>(c, ln.part, nb, sc.rr, opc, st);
+    if (h && B > 1) KL(c, st, k_rel_cond<<<1, 256, 0, st>>>(h, ln.rel, B));
+    bool nested = false;
+    if (h) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t nd = 0;
+      cudaGraphNodeParams np{};
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = h;
+      np.conditional.type = cudaGraphCondTypeIf;
+      np.conditional.size = 1;
+      cudaGraphNode_t node{};
+      if (!ln.cap_stream2) CK(cudaStreamCreateWithFlags(&ln.cap_stream2, cudaStreamNonBlocking));
+      // the capture of st goes on after the IF node; its body is captured on
+      // the second stream
+      nested = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd) == cudaSuccess &&
+               cudaGraphAddNode(&node, cg, deps, nd, &np) == cudaSuccess &&
+               cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess &&
+               cudaStreamBeginCaptureToGraph(ln.cap_stream2, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      (void)cudaGetLastError();
+      if (nested) {
+        try {
+          replace(ln.cap_stream2);
+        } catch (...) {
+          cudaGraph_t tmp = nullptr;
+          cudaStreamEndCapture(ln.cap_stream2, &tmp);
+          throw;
+        }
+        cudaGraph_t tmp = nullptr;
+        CK(cudaStreamEndCapture(ln.cap_stream2, &tmp));
+      }
+    }
+    // without the IF node (eager, or refused: an IF node left with an empty
+    // body does nothing) the predicated launches run in line
+    if (!nested) replace(st);
+    // z = M r, r.z fused into the last smoothing step; p = z + beta p
+    vcycle<float, D, R>(c, p, o, 0, o.r, run, ln.part, st);
+    reduce_op<R, RED_BETA>(c, ln.part, nbf, sc.rz_new, op, st);
+    KL(c, st, k_pcg_direction<float, R, D><<<g2(N, B), kThreads, 0, st>>>(o.p, z, sc.beta, N, run));
+  };
+  run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MIXED_RELIABLE_GRAPH], maxit, body, s);
+  // cells stopped by the iteration limit keep their last FP32 correction
+  KL(c, s, k_flush_f32<R, D><<<g2(N, B), kThreads, 0, s>>>(x, o.x, ln.o_inv, N, c->active));
 }
 
 // Extrapolated warm start of an OC step: u <- u + theta (u - prev), prev <- u
@@ -1237,6 +1388,33 @@ static void solve_phys(maple_ctx* c, int phys, int prec, const double* F, double
   } else {
     if (c->mixed_mode == MAPLE_MIXED_REFINE) {
       pcg_refine<D, R>(c, p, F, x64, x_zero, rtol, maxit, it, st, s);
+    } else if (c->mixed_mode == MAPLE_MIXED_RELIABLE) {
+      // FP32 recurrences lose orthogonality on badly conditioned cells (near
+      // void, floating stiff islands), where the flexible form, with FP64
+      // recurrences, still converges: a cell still unconverged after
+      // rel_handover iterations continues in the flexible form from its
+      // iterate, within the same iteration limit.
+      const int cap = std::min(maxit, c->rel_handover);
+      pcg_reliable<D, R>(c, p, F, x64, x_zero, rtol, cap, s);
+      read_outcome(c, R, it, st, s);
+      if (cap < maxit) {
+        std::vector<int> ho(B, 0);
+        bool any = false;
+        for (int b = 0; b < B; ++b)
+          if (st[b] == MAPLE_CELL_MAXIT && (c->h_active.empty() || c->h_active[b])) ho[b] = 1, any = true;
+        if (any) {
+          Lane& ln = LN(c);
+          CK(cudaMemcpyAsync(ln.o_live, ho.data(), B * sizeof(int), cudaMemcpyHostToDevice, s));
+          pcg_mixed<D, R>(c, p, F, x64, false, rtol, maxit - cap, s, ln.o_live);
+          std::vector<int> it2, st2;
+          read_outcome(c, R, it2, st2, s);  // synchronises: ho is read before it goes out of scope
+          for (int b = 0; b < B; ++b)
+            if (ho[b]) {
+              it[b] += it2[b];
+              st[b] = st2[b];
+            }
+        }
+      }
     } else {
       pcg_mixed<D, R>(c, p, F, x64, x_zero, rtol, maxit, s);
       read_outcome(c, R, it, st, s);
@@ -1603,6 +1781,8 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
         L.o_done = dnew<int>(c, B);
         L.o_run = dnew<int>(c, B);
         L.o_live = dnew<int>(c, B);
+        L.rel = dnew<int>(c, B);
+        L.o_t = dnew<double>(c, B * 6);
         L.breakdown = dnew<int>(c, 1);
         CK(cudaMemset(L.breakdown, 0, sizeof(int)));
         L.loop = dnew<int>(c, 2);
@@ -1700,6 +1880,7 @@ int maple_ctx_destroy(maple_ctx* c) {
     drop_graphs(c);
     for (Lane& L : c->lanes) {
       if (L.cap_stream) cudaStreamDestroy(L.cap_stream);
+      if (L.cap_stream2) cudaStreamDestroy(L.cap_stream2);
       if (L.side) cudaStreamDestroy(L.side);
       if (L.side_fork) cudaEventDestroy(L.side_fork);
       if (L.side_join) cudaEventDestroy(L.side_join);
@@ -1934,8 +2115,19 @@ int maple_set_extrapolation(maple_ctx* c, double theta) {
 int maple_set_mixed_mode(maple_ctx* c, int mode) {
   return guarded([&] {
     require(c != nullptr, "ctx is NULL");
-    require(mode == MAPLE_MIXED_FLEXIBLE || mode == MAPLE_MIXED_REFINE, "unknown mixed-precision mode");
+    require(mode == MAPLE_MIXED_FLEXIBLE || mode == MAPLE_MIXED_REFINE || mode == MAPLE_MIXED_RELIABLE,
+            "unknown mixed-precision mode");
     c->mixed_mode = mode;
+  });
+}
+
+int maple_set_reliable_options(maple_ctx* c, double delta, int handover) {
+  return guarded([&] {
+    require(c != nullptr, "ctx is NULL");
+    require(delta > 0.0 && delta < 1.0, "delta must be in (0, 1)");
+    require(handover >= 1, "handover must be >= 1");
+    c->rel_delta = delta;
+    c->rel_handover = handover;
   });
 }
 

@@ -347,7 +347,7 @@ def test_pdl_matches_plain_launches(lib, precision, r):
             assert np.array_equal(it0[[0, 2]], it1[[0, 2]]), (phys, key)
 
 
-@pytest.mark.parametrize("form", ["fp64", "mixed", "refine"])
+@pytest.mark.parametrize("form", ["fp64", "flexible", "refine", "reliable"])
 def test_device_loop_matches_host_loop(lib, form):
     """The device-side PCG loop (conditional graph node, one host wait per
     solve) runs the same iterations as the per-iteration graph replays with a
@@ -361,8 +361,8 @@ def test_device_loop_matches_host_loop(lib, form):
     for loop in (False, True):
         c = HomogenizationContext(r, ncells=3)
         c.set_device_loop(loop)
-        if form == "refine":
-            c.set_mixed_mode("refine")
+        if form != "fp64":
+            c.set_mixed_mode(form)
         c.set_active([1, 0, 1])
         for phys in ("elastic", "thermal"):
             c.set_density(phys, rho, precision)
@@ -384,6 +384,44 @@ def test_device_loop_matches_host_loop(lib, form):
         c1, s1, v1 = out[(True, phys, "cap")]
         assert np.array_equal(c0[[0, 2]], c1[[0, 2]]) and np.array_equal(s0[[0, 2]], s1[[0, 2]]), (phys, c0, c1)
         assert torch.equal(v0, v1)
+
+
+def test_reliable_form_hands_slow_cells_to_flexible(lib):
+    """The reliable-update form: its answer matches the flexible form and
+    plain FP64 to the tolerance; a cell still unconverged after the handover
+    count continues in the flexible form from its iterate and converges, the
+    iterations of both parts counted, within the same limit."""
+    from maple_b200.core import HomogenizationContext
+    r = 16
+    rho = T(np.stack([simp(O.seed_density(s, r, 2.0, 0.3)).reshape(-1) for s in (21, 22)]))
+    sol = {}
+    for form, handover in (("fp64", None), ("flexible", None), ("reliable", 120), ("reliable", 5)):
+        c = HomogenizationContext(r, ncells=2)
+        prec = "fp64" if form == "fp64" else "mixed"
+        if form != "fp64":
+            c.set_mixed_mode(form)
+        if handover:
+            c.set_reliable_options(1e-3, handover)
+        for phys in ("elastic", "thermal"):
+            c.set_density(phys, rho, prec)
+            info = c.solve(phys, prec, rtol=1e-10, maxit=300)
+            assert (info.status == 1).all(), (form, handover, phys, info.status)
+            if handover == 5:
+                assert (info.iters > 5).all()
+            sol[(form, handover, phys)] = (c.solution(phys), info.iters.copy())
+        c.close()
+    def mean_free(u):  # the periodic solution is defined up to a translation
+        return u - u.mean(dim=-1, keepdim=True)
+
+    for phys in ("elastic", "thermal"):
+        ref, it_ref = sol[("fp64", None, phys)]
+        ref = mean_free(ref)
+        for key in (("flexible", None), ("reliable", 120), ("reliable", 5)):
+            u, it = sol[key + (phys,)]
+            err = ((mean_free(u) - ref).norm() / ref.norm()).item()
+            assert err < 1e-8, (key, phys, err)
+        # the reliable form keeps the Krylov space: about the FP64 iteration count
+        assert np.all(sol[("reliable", 120, phys)][1] <= it_ref + 3), (phys, sol[("reliable", 120, phys)][1], it_ref)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
