@@ -48,6 +48,11 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fp64-arm", action="store_true", help="skip the plain-FP64 comparison arm")
     p.add_argument("--no-chs", action="store_true", help="skip the C^H solves/s measurement")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="config 1: library defaults instead of the autotuner's choice (both arms)")
+    p.add_argument("--no-graph-conditionals", action="store_true",
+                   help="per-iteration graph replays without conditional nodes (for profilers that do not "
+                        "support them); same kernels and results")
     p.add_argument("--serial", action="store_true",
                    help="run the elastic and thermal solves one after the other on one host thread")
     p.add_argument("--config", type=int, default=1, choices=[1, 2, 4],
@@ -252,9 +257,29 @@ def run_maple(args, rank, world, local_rank):
         if world > 1:
             dist.barrier()
 
+    def arm_context(prec):
+        """A fresh context with the autotuner's settings for this precision
+        (chosen on a short trajectory from the same start design, untimed;
+        both arms get the same treatment)."""
+        from maple_b200.autotune import apply as apply_settings
+        from maple_b200.autotune import autotune
+        settings = None
+        if not args.no_autotune:
+            tctx = HomogenizationContext(r, ncells=1, device=dev)
+            tctx.set_concurrency(not args.serial)
+            settings = autotune(tctx, x0, w, vf, precision=prec, rtol=args.rtol, steps=3, passes=1,
+                                use_cache=False, cache=None).settings
+            tctx.close()
+        c = HomogenizationContext(r, ncells=1, device=dev)
+        c.set_concurrency(not args.serial)
+        if settings:
+            apply_settings(c, settings)
+        if args.no_graph_conditionals:
+            c.set_device_loop(False)
+        return c, settings
+
     # the benchmarked arm
-    ctx = HomogenizationContext(r, ncells=1, device=dev)
-    ctx.set_concurrency(not args.serial)
+    ctx, tuned = arm_context(args.precision)
     main_arm = _timed_oc_steps(ctx, x0, w, vf, kw, args, flush, barrier, ClockSampler(local_rank))
     t_dev = max_over_ranks(sum(main_arm["step_ms"]) / 1000.0, world, dev)
     value = world * args.steps / t_dev
@@ -263,14 +288,13 @@ def run_maple(args, rank, world, local_rank):
     # the plain FP64 arm: same cell, same start, same steps
     fp64 = None
     if args.precision == "mixed" and not args.no_fp64_arm:
-        ctx64 = HomogenizationContext(r, ncells=1, device=dev)
-        ctx64.set_concurrency(not args.serial)
+        ctx64, tuned64 = arm_context("fp64")
         arm64 = _timed_oc_steps(ctx64, x0, w, vf, dict(kw, precision="fp64"), args, flush, barrier)
         t64 = max_over_ranks(sum(arm64["step_ms"]) / 1000.0, world, dev)
         errs = [max(_rel(a[0], b[0]), _rel(a[1], b[1]), abs(a[2] - b[2]) / abs(b[2]))
                 for a, b in zip(main_arm["recs"], arm64["recs"])]
         fp64 = dict(value=world * args.steps / t64, ms_per_step=1000 * t64 / args.steps, iters=arm64["iters"],
-                    err=errs, ctx=ctx64)
+                    err=errs, ctx=ctx64, tuned=tuned64)
 
     # C^H solves per second (every load case from zero, hierarchy builds included)
     chs = None
@@ -345,7 +369,7 @@ def run_maple(args, rank, world, local_rank):
     ctx.close()
     return dict(value=value, t_dev=t_dev, step_ms=main_arm["step_ms"], wall=main_arm["wall"],
                 launches=main_arm["launches"], clocks=main_arm["clocks"], roofline=roofline, e2e=e2e,
-                iters=main_arm["iters"], levels=ctx.levels, J=main_arm["J"], fp64=fp64, chs=chs)
+                iters=main_arm["iters"], levels=ctx.levels, J=main_arm["J"], fp64=fp64, chs=chs, tuned=tuned)
 
 
 # ---------------------------------------------------------------------------
@@ -574,7 +598,8 @@ def main():
                        "solves": "one after the other" if args.serial else "elastic and thermal concurrent",
                        "objective": "(E+G+kappa)/3", "volfrac": 0.25, "move": 0.2, "filter_k": 3,
                        "mg_levels": res["levels"], "l2": "flushed between steps (256 MiB write outside the events)",
-                       "parallelism": f"replicas x{world}", "pcg_iters_per_step": res["iters"]},
+                       "parallelism": f"replicas x{world}", "pcg_iters_per_step": res["iters"],
+                       "autotuned": res["tuned"] or "off (library defaults)"},
             "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "roofline": res["roofline"],
             "cpu_baseline": cpu, "e2e": res["e2e"], "chs": res["chs"], "wall_s": round(res["wall"], 3),
             "step_ms": [round(v, 3) for v in res["step_ms"]], "J_last": res["J"],
@@ -582,7 +607,7 @@ def main():
         fp = res["fp64"]
         if fp is not None:
             line["fp64_arm"] = {"value": round(fp["value"], 3), "unit": UNIT, "ms_per_step": round(fp["ms_per_step"], 3),
-                                "pcg_iters_per_step": fp["iters"],
+                                "pcg_iters_per_step": fp["iters"], "autotuned": fp["tuned"] or "off",
                                 "what": "plain FP64 MG-PCG, same cell, start design, warm-up and steps"}
             line["mixed_over_fp64"] = round(res["value"] / fp["value"], 4)
             line["err_vs_fp64"] = {"max": max(fp["err"]), "per_step": [float(f"{e:.3g}") for e in fp["err"]],

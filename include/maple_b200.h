@@ -77,7 +77,7 @@ int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio,
                              int check_every);
 
 /* Form of the mixed-precision (MAPLE_MIXED) solve:
- *   MAPLE_MIXED_FLEXIBLE  flexible FP64 PCG (FP64 fine operator, residuals and
+ *   MAPLE_MIXED_FLEXIBLE  (default) flexible FP64 PCG (FP64 fine operator, residuals and
  *                         dot products every iteration) preconditioned by the
  *                         FP32 V-cycle;
  *   MAPLE_MIXED_REFINE    FP32 MG-PCG (FP32 fine operator and vectors, FP64
@@ -86,7 +86,7 @@ int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio,
  *                         residual r = b - A x, the convergence test, the inner
  *                         solve to the inner tolerance of
  *                         maple_set_solver_options, and x += ||r|| e in FP64.
- *   MAPLE_MIXED_RELIABLE  (default) FP32 MG-PCG (FP32 fine operator and vectors, FP64
+ *   MAPLE_MIXED_RELIABLE  FP32 MG-PCG (FP32 fine operator and vectors, FP64
  *                         accumulated dots) on the residual scaled to unit
  *                         norm, with reliable updates: when a load case's
  *                         recurrence residual fell by the factor of
@@ -94,7 +94,11 @@ int maple_set_solver_options(maple_ctx* ctx, int cheb_degree, double cheb_ratio,
  *                         test, the FP32 correction is folded into the FP64
  *                         iterate and the residual is recomputed as b - A x in
  *                         FP64 and continues the iteration (the direction is
- *                         kept, not restarted).
+ *                         kept, not restarted).  Faster where the cells are
+ *                         well conditioned (64^3 benchmark cell: same PCG
+ *                         iterations, 7% less time); on badly conditioned ones
+ *                         the FP32 recurrences need up to twice the iterations
+ *                         (128^3, vf 0.15), so the autotuner chooses per workload.
  * All stop at the same FP64 residual test ||b - A x|| <= rtol ||b|| per load
  * case.  The reference solves in one precision (utils/EBE_GMG.py:758-885,
  * dtype argument). */
@@ -157,9 +161,12 @@ int maple_set_pdl(maple_ctx* ctx, int enable);
  * counts the iteration and ends the loop once every active cell has converged
  * or the iteration limit is reached, so the host waits once per solve instead
  * of once per iteration (check_every of maple_set_solver_options then has no
- * effect).  Default on; 0, or a runtime that refuses conditional graph nodes,
- * replays one graph per iteration.  Results and iteration counts are
- * identical either way.  The reference's loop (utils/EBE_GMG.py:858-885,
+ * effect); the residual replacement of MAPLE_MIXED_RELIABLE sits in a
+ * conditional IF node of the captured iteration.  Default on; 0, or a runtime
+ * that refuses conditional graph nodes, replays one graph per iteration with
+ * the replacement's launches predicated on device flags (profilers that do
+ * not support conditional graphs see every kernel this way).  Results and
+ * iteration counts are identical either way.  The reference's loop (utils/EBE_GMG.py:858-885,
  * GMGSolver.solve) tests the residual on the host after every cycle. */
 int maple_set_device_loop(maple_ctx* ctx, int enable);
 

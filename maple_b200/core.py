@@ -190,10 +190,10 @@ class HomogenizationContext:
         _lib.check(self._lib.maple_get_device_loop(self._h, C.byref(v)))
         return int(v.value)
 
-    def set_mixed_mode(self, mode: str = "reliable"):
-        """Form of the mixed-precision solve: "reliable" (default: FP32
-        MG-PCG with FP64 residual replacement, the direction kept),
-        "flexible" (FP64 flexible PCG preconditioned by the FP32 V-cycle) or
+    def set_mixed_mode(self, mode: str = "flexible"):
+        """Form of the mixed-precision solve: "flexible" (default: FP64
+        flexible PCG preconditioned by the FP32 V-cycle), "reliable" (FP32
+        MG-PCG with FP64 residual replacement, the direction kept) or
         "refine" (FP32 MG-PCG inside FP64 iterative refinement)."""
         modes = {"flexible": 0, "refine": 1, "reliable": 2}
         if mode not in modes:

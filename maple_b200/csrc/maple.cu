@@ -41,6 +41,9 @@ struct Failure {
   } while (0)
 static std::atomic<unsigned long long> g_launches{0};
 static thread_local unsigned long long tl_launches = 0;  // this thread's launches (graph capture accounting)
+// kernels captured into the bodies of conditional IF nodes during the current
+// capture (they run only when the condition is set; counted apart)
+static thread_local unsigned long long tl_cond_kernels = 0;
 #define CKL()                         \
   do {                                \
     CK(cudaGetLastError());           \
@@ -160,8 +163,8 @@ struct Lane {
   int* o_live = nullptr;   // refinement: cells still refined (active, not broken down)
   int* rel = nullptr;      // reliable updates: per cell, a residual replacement is due
   double* o_t = nullptr;   // reliable updates: per (cell, rhs) rescaling of the direction
-  int* h_flags = nullptr;  // pinned host [B + 1]: convergence flags, then the device loop's count
-  int* loop = nullptr;     // device [2]: iterations run by the device-side loop, its limit
+  int* h_flags = nullptr;  // pinned host [B + 2]: convergence flags, the device loop's count, IF executions
+  int* loop = nullptr;     // device [3]: iterations run by the device-side loop, its limit, IF-node executions
   int* breakdown = nullptr;
   cudaStream_t cap_stream = nullptr;
   cudaStream_t cap_stream2 = nullptr;  // captures the body of a conditional node inside a capture
@@ -209,6 +212,7 @@ struct maple_ctx {
     cudaGraphExec_t loop_exec = nullptr;
     unsigned long long loop_kernels = 0;  // kernels per loop iteration
     bool loop_failed = false;             // the runtime refused the conditional graph
+    unsigned long long cond_kernels = 0;  // kernels of the IF-node body per execution (not in the counts above)
   } graphs[2][4];  // [physics][FP64 PCG, flexible mixed PCG, FP32 inner PCG of refinement, reliable updates]
   cudaStream_t aux_stream = nullptr;  // second physics of a concurrent OC step
   cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
@@ -218,7 +222,7 @@ struct maple_ctx {
   int nine_max_n = 64;     // coarse levels with n <= this use k_apply_stencil_nine; 0: never
   bool tail_fused = true;  // FP32 8^3 level + 4^3 coarsest solve as one cluster launch (k_tail_cycle)
   bool pdl = true;         // coarse-level launches with programmatic dependent launch
-  bool device_loop = true; // PCG iterations looped on device (conditional graph node)
+  bool device_loop = true; // conditional graph nodes: PCG iterations looped on device, IF node of the replacement
   int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
   // manufacturability penalties of the OC objective (maple_set_penalties)
   double lambda_print = 0, lambda_cavity = 0;
@@ -247,10 +251,9 @@ struct maple_ctx {
   double power_safety = 1.15;
   double inner_rtol = 1e-5;
   int check_every = 1;
-  int mixed_mode = 2;  // MAPLE_MIXED_FLEXIBLE, MAPLE_MIXED_REFINE or MAPLE_MIXED_RELIABLE (default)
+  int mixed_mode = 0;  // MAPLE_MIXED_FLEXIBLE (default), MAPLE_MIXED_REFINE or MAPLE_MIXED_RELIABLE
   double rel_delta = 1e-3;  // reliable updates: residual reduction per FP32 segment
   int rel_handover = 120;   // reliable updates: iterations before an unconverged cell moves to the flexible form
-  bool rel_cond = true;     // reliable updates: the replacement in a conditional IF node of captured graphs
   double extrap = 0.0;  // warm start of maple_oc_step: u + extrap * (u - u_prev)
 };
 
@@ -801,6 +804,7 @@ static bool loop_graph(maple_ctx* c, maple_ctx::GraphEntry& ge, Body& body) {
   CK(cudaGraphCreate(&g, 0));
   bool ok = false;
   const unsigned long long before = tl_launches;
+  tl_cond_kernels = 0;
   cudaGraphConditionalHandle h{};
   cudaGraphNodeParams np{};
   cudaGraphNode_t node{};
@@ -826,9 +830,11 @@ static bool loop_graph(maple_ctx* c, maple_ctx::GraphEntry& ge, Body& body) {
   }
   (void)cudaGetLastError();  // a refused step leaves the per-iteration graphs in use
   cudaGraphDestroy(g);
-  ge.loop_kernels = tl_launches - before;
-  g_launches.fetch_sub(ge.loop_kernels);  // captured, not launched
-  tl_launches -= ge.loop_kernels;
+  const unsigned long long captured = tl_launches - before;
+  ge.loop_kernels = captured - tl_cond_kernels;
+  ge.cond_kernels = tl_cond_kernels;
+  g_launches.fetch_sub(captured);  // captured, not launched
+  tl_launches -= captured;
   if (!ok) {
     if (ge.loop_exec) cudaGraphExecDestroy(ge.loop_exec);
     ge.loop_exec = nullptr;
@@ -875,6 +881,7 @@ static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, int maxit, B
         if (!LN(c).cap_stream) CK(cudaStreamCreateWithFlags(&LN(c).cap_stream, cudaStreamNonBlocking));
         cudaGraph_t graph = nullptr;
         const unsigned long long before = tl_launches;
+        tl_cond_kernels = 0;
         CK(cudaStreamBeginCapture(LN(c).cap_stream, cudaStreamCaptureModeThreadLocal));
         try {
           body(LN(c).cap_stream);
@@ -886,9 +893,11 @@ static void run_iterations(maple_ctx* c, maple_ctx::GraphEntry& ge, int maxit, B
         CK(cudaStreamEndCapture(LN(c).cap_stream, &graph));
         CK(cudaGraphInstantiate(&ge.exec, graph, 0));
         CK(cudaGraphDestroy(graph));
-        ge.kernels = tl_launches - before;
-        g_launches.fetch_sub(ge.kernels);  // captured, not launched
-        tl_launches -= ge.kernels;
+        const unsigned long long captured = tl_launches - before;
+        ge.kernels = captured - tl_cond_kernels;
+        ge.cond_kernels = tl_cond_kernels;
+        g_launches.fetch_sub(captured);  // captured, not launched
+        tl_launches -= captured;
       }
       CK(cudaGraphLaunch(ge.exec, s));
       g_launches.fetch_add(ge.kernels);
@@ -908,6 +917,35 @@ static void drop_graphs(maple_ctx* c) {
       ge.loop_exec = nullptr;
       ge.loop_failed = false;
     }
+}
+
+static inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// x += alpha p, r -= alpha q with the partial sums of r.r (16-byte vectors
+// when the node count and every pointer allow: a caller's buffer may be only
+// element-aligned); returns the number of partial blocks
+template <typename T, int R, int D>
+static unsigned pcg_update(maple_ctx* c, T* x, T* r, const T* p, const T* q, const double* alpha, double* part,
+                           int N, int B, const int* run, cudaStream_t s) {
+  constexpr int W = Vec16<T>::n;
+  if (N % W == 0 && al16(x) && al16(r) && al16(p) && al16(q)) {
+    const unsigned nb = nblk((size_t)(N / W));
+    KL(c, s, k_pcg_update_vec<T, R, D><<<dim3(nb, B), kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run));
+    return nb;
+  }
+  KL(c, s, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run));
+  return nblk(N);
+}
+
+// p = z + beta p
+template <typename T, int R, int D>
+static void pcg_direction(maple_ctx* c, T* p, const T* z, const double* beta, int N, int B, const int* run,
+                          cudaStream_t s) {
+  constexpr int W = Vec16<T>::n;
+  if (N % W == 0 && al16(p) && al16(z))
+    KL(c, s, k_pcg_direction_vec<T, R, D><<<dim3(nblk((size_t)(N / W)), B), kThreads, 0, s>>>(p, z, beta, N, run));
+  else
+    KL(c, s, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, s>>>(p, z, beta, N, run));
 }
 
 template <typename T, int D, int R>
@@ -960,11 +998,11 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
       apply<T, D, R, M_MV>(c, p, o, 0, a, run, st);
     }
     reduce_op<R, RED_ALPHA>(c, LN(c).part, nbf, sc.pq, op, st);
-    KL(c, st, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.x, o.r, o.p, o.q, sc.alpha, LN(c).part, N, run));
-    reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op, st);
+    const unsigned nbu = pcg_update<T, R, D>(c, o.x, o.r, o.p, o.q, sc.alpha, LN(c).part, N, B, run, st);
+    reduce_op<R, RED_CHECK>(c, LN(c).part, nbu, sc.rr, op, st);
     vcycle<T, D, R>(c, p, o, 0, o.r, run, LN(c).part, st);
     reduce_op<R, RED_BETA>(c, LN(c).part, nbf, sc.rz_new, op, st);
-    KL(c, st, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, st>>>(o.p, o.U[0][1], sc.beta, N, run));
+    pcg_direction<T, R, D>(c, o.p, o.U[0][1], sc.beta, N, B, run, st);
   };
   run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][std::is_same<T, float>::value ? 2 : MAPLE_FP64], maxit,
                  body, s);
@@ -1039,8 +1077,8 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
       apply<double, D, R, M_MV>(c, p, o64, 0, a, run, st);
     }
     reduce_op<R, RED_ALPHA>(c, LN(c).part, nbf, sc.pq, op, st);
-    KL(c, st, k_pcg_update<double, R, D><<<g2(N, B), kThreads, 0, st>>>(x, r, pv, q, sc.alpha, LN(c).part, N, run));
-    reduce_op<R, RED_CHECK>(c, LN(c).part, nb, sc.rr, op, st);
+    const unsigned nbu = pcg_update<double, R, D>(c, x, r, pv, q, sc.alpha, LN(c).part, N, B, run, st);
+    reduce_op<R, RED_CHECK>(c, LN(c).part, nbu, sc.rr, op, st);
     precondition_f32<D, R>(c, p, r, q, run, op, st);
     KL(c, st, k_pcg_direction_f32<R, D, false><<<g2(N, B), kThreads, 0, st>>>(pv, z32, LN(c).o_inv, sc.beta, N, run));
   };
@@ -1105,38 +1143,19 @@ static void pcg_reliable(maple_ctx* c, Phys& p, const double* b, double* x, bool
   reduce_op<R, RED_CHECK>(c, ln.part, nb, sc.rr, op0, s);
   if (all_done(c, sc.cell_done, run, s)) return;
   CK(cudaMemsetAsync(o.x, 0, v32, s));
+  CK(cudaMemsetAsync(ln.loop + 2, 0, sizeof(int), s));  // IF-node executions of this solve
   KL(c, s, k_to_f32_scaled<R, D><<<g2(N, B), kThreads, 0, s>>>(r, o.r, ln.o_scale, N, run));
   vcycle<float, D, R>(c, p, o, 0, o.r, run, ln.part, s);
   reduce_op<R, RED_SET_RZ>(c, ln.part, nbf, sc.rz_new, op, s);
   CK(cudaMemcpyAsync(o.p, z, v32, cudaMemcpyDeviceToDevice, s));
   op.count = 1;
   auto body = [&](cudaStream_t st) {
-    {
-      ApplyArgs<float> a{};
-      a.u = o.p;
-      a.out = o.q;
-      a.part = ln.part;
-      apply<float, D, R, M_MV>(c, p, o, 0, a, run, st);
-    }
-    reduce_op<R, RED_ALPHA>(c, ln.part, nbf, sc.pq, op, st);
-    KL(c, st, k_pcg_update<float, R, D><<<g2(N, B), kThreads, 0, st>>>(o.x, o.r, o.p, o.q, sc.alpha, ln.part, N, run));
-    // Residual replacement of the flagged cells (every launch skips the
-    // others).  In a captured graph it sits in a conditional IF node, so the
-    // iterations without a replacement launch none of it.
-    auto replace = [&](cudaStream_t sr) {
-      KL(c, sr, k_flush_f32<R, D><<<g2(N, B), kThreads, 0, sr>>>(x, o.x, ln.o_inv, N, ln.rel));
-      ApplyArgs<double> a{};
-      a.u = x;
-      a.f = b;
-      a.out = r;
-      apply<double, D, R, M_RES>(c, p, o64, 0, a, ln.rel, sr);
-      KL(c, sr, k_dot<double, R, D><<<g2(N, B), kThreads, 0, sr>>>(r, r, ln.part, N, ln.rel));
-      reduce_op<R, RED_RELSET>(c, ln.part, nb, ln.o_rr, op, sr);
-      KL(c, sr, k_rel_rescale<R, D><<<g2(N, B), kThreads, 0, sr>>>(r, o.r, o.p, o.q, ln.o_scale, ln.o_t, N, ln.rel));
-    };
+    // In a captured graph the residual replacement below sits in a
+    // conditional IF node (handle h), so iterations without one launch none
+    // of it; ALPHA clears the condition, RELCHECK sets it.
     cudaGraphConditionalHandle h = 0;
     cudaGraph_t cg = nullptr;
-    if (c->rel_cond) {
+    if (c->device_loop) {
       cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
       if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg) != cudaSuccess || cs != cudaStreamCaptureStatusActive ||
           cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault) != cudaSuccess)
@@ -1144,9 +1163,31 @@ static void pcg_reliable(maple_ctx* c, Phys& p, const double* b, double* x, bool
       (void)cudaGetLastError();
     }
     RedOp opc = op;
-    opc.cond = B == 1 ? h : 0;
-    reduce_op<R, RED_RELCHECK>(c, ln.part, nb, sc.rr, opc, st);
-    if (h && B > 1) KL(c, st, k_rel_cond<<<1, 256, 0, st>>>(h, ln.rel, B));
+    opc.cond = h;
+    {
+      ApplyArgs<float> a{};
+      a.u = o.p;
+      a.out = o.q;
+      a.part = ln.part;
+      apply<float, D, R, M_MV>(c, p, o, 0, a, run, st);
+    }
+    reduce_op<R, RED_ALPHA>(c, ln.part, nbf, sc.pq, opc, st);
+    const unsigned nbu = pcg_update<float, R, D>(c, o.x, o.r, o.p, o.q, sc.alpha, ln.part, N, B, run, st);
+    reduce_op<R, RED_RELCHECK>(c, ln.part, nbu, sc.rr, opc, st);
+    // residual replacement of the flagged cells (every launch skips the others)
+    auto replace = [&](cudaStream_t sr, bool in_if) {
+      KL(c, sr, k_flush_f32<R, D><<<g2(N, B), kThreads, 0, sr>>>(x, o.x, ln.o_inv, N, ln.rel));
+      ApplyArgs<double> a{};
+      a.u = x;
+      a.f = b;
+      a.out = r;
+      apply<double, D, R, M_RES>(c, p, o64, 0, a, ln.rel, sr);
+      KL(c, sr, k_dot<double, R, D><<<g2(N, B), kThreads, 0, sr>>>(r, r, ln.part, N, ln.rel));
+      RedOp ops = op;
+      if (in_if) ops.cond_count = ln.loop + 2;  // launches of the IF body are counted by executions
+      reduce_op<R, RED_RELSET>(c, ln.part, nb, ln.o_rr, ops, sr);
+      KL(c, sr, k_rel_rescale<R, D><<<g2(N, B), kThreads, 0, sr>>>(r, o.r, o.p, o.q, ln.o_scale, ln.o_t, N, ln.rel));
+    };
     bool nested = false;
     if (h) {
       cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -1168,8 +1209,10 @@ static void pcg_reliable(maple_ctx* c, Phys& p, const double* b, double* x, bool
                                              cudaStreamCaptureModeThreadLocal) == cudaSuccess;
       (void)cudaGetLastError();
       if (nested) {
+        const unsigned long long before = tl_launches;
         try {
-          replace(ln.cap_stream2);
+          replace(ln.cap_stream2, true);
+          tl_cond_kernels += tl_launches - before;
         } catch (...) {
           cudaGraph_t tmp = nullptr;
           cudaStreamEndCapture(ln.cap_stream2, &tmp);
@@ -1181,15 +1224,23 @@ static void pcg_reliable(maple_ctx* c, Phys& p, const double* b, double* x, bool
     }
     // without the IF node (eager, or refused: an IF node left with an empty
     // body does nothing) the predicated launches run in line
-    if (!nested) replace(st);
+    if (!nested) replace(st, false);
     // z = M r, r.z fused into the last smoothing step; p = z + beta p
     vcycle<float, D, R>(c, p, o, 0, o.r, run, ln.part, st);
     reduce_op<R, RED_BETA>(c, ln.part, nbf, sc.rz_new, op, st);
-    KL(c, st, k_pcg_direction<float, R, D><<<g2(N, B), kThreads, 0, st>>>(o.p, z, sc.beta, N, run));
+    pcg_direction<float, R, D>(c, o.p, z, sc.beta, N, B, run, st);
   };
-  run_iterations(c, c->graphs[&p == &c->ph[0] ? 0 : 1][MIXED_RELIABLE_GRAPH], maxit, body, s);
+  maple_ctx::GraphEntry& ge = c->graphs[&p == &c->ph[0] ? 0 : 1][MIXED_RELIABLE_GRAPH];
+  run_iterations(c, ge, maxit, body, s);
   // cells stopped by the iteration limit keep their last FP32 correction
   KL(c, s, k_flush_f32<R, D><<<g2(N, B), kThreads, 0, s>>>(x, o.x, ln.o_inv, N, c->active));
+  if (ge.cond_kernels) {  // launches of the replacements that ran inside graphs
+    CK(cudaMemcpyAsync(ln.h_flags + B + 1, ln.loop + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const unsigned long long n = (unsigned long long)std::max(ln.h_flags[B + 1], 0) * ge.cond_kernels;
+    g_launches.fetch_add(n);
+    tl_launches += n;
+  }
 }
 
 // Extrapolated warm start of an OC step: u <- u + theta (u - prev), prev <- u
@@ -1785,8 +1836,8 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
         L.o_t = dnew<double>(c, B * 6);
         L.breakdown = dnew<int>(c, 1);
         CK(cudaMemset(L.breakdown, 0, sizeof(int)));
-        L.loop = dnew<int>(c, 2);
-        CK(cudaMallocHost(&L.h_flags, (B + 1) * sizeof(int)));
+        L.loop = dnew<int>(c, 3);
+        CK(cudaMallocHost(&L.h_flags, (B + 2) * sizeof(int)));
       }
       c->active = dnew<int>(c, B);
       c->h_active.assign(B, 1);

@@ -31,7 +31,7 @@ def test_autotune_picks_from_its_space_and_keeps_the_answer(lib, tmp_path):
     ref_ctx.close()
     ctx = HomogenizationContext(r, ncells=B, device=DEV)
     cache = str(tmp_path / "tune.json")
-    space = dict(fine_degree=[1, 2], coarse_degree=[0, 4], nine_max_n=[0, 64], mixed_mode=["reliable", "flexible"])
+    space = dict(fine_degree=[1, 2], coarse_degree=[0, 4], nine_max_n=[0, 64], mixed_mode=["flexible", "reliable"])
     res = A.autotune(ctx, x, w, vf, precision="mixed", rtol=1e-10, steps=1, passes=1, cache=cache, space=space)
     for k, vals in space.items():
         assert res.settings[k] in vals

@@ -353,14 +353,19 @@ def test_device_loop_matches_host_loop(lib, form):
     solve) runs the same iterations as the per-iteration graph replays with a
     host convergence check after each: bit-identical solutions and iteration
     counts, with an inactive cell, and the same stop at an iteration cap."""
-    from maple_b200.core import HomogenizationContext
+    from maple_b200.core import HomogenizationContext, launch_count
     r = 16
     precision = "fp64" if form == "fp64" else "mixed"
     rho = T(np.stack([simp(O.seed_density(s, r, 2.0, 0.3)).reshape(-1) for s in (11, 12, 13)]))
     out = {}
-    for loop in (False, True):
+    launches = {}
+    for loop in (None, False, True):  # None: eager, no graphs
         c = HomogenizationContext(r, ncells=3)
-        c.set_device_loop(loop)
+        if loop is None:
+            c.set_graphs(False)
+        else:
+            c.set_device_loop(loop)
+        n0 = launch_count()
         if form != "fp64":
             c.set_mixed_mode(form)
         c.set_active([1, 0, 1])
@@ -373,8 +378,18 @@ def test_device_loop_matches_host_loop(lib, form):
             c.set_density(phys, rho, precision)
             capped = c.solve(phys, precision, rtol=1e-14, maxit=4)
             out[(loop, phys, "cap")] = (capped.iters.copy(), capped.status.copy(), c.solution(phys)[[0, 2]].clone())
+        launches[loop] = launch_count() - n0
         assert c.device_loop_state() == (1 if loop else 0)
         c.close()
+    # Launch counts: per-iteration graph replays launch what the eager runs
+    # launch.  With conditional nodes the device loop adds its counting kernel
+    # per iteration, and a reliable-update iteration runs its replacement (an
+    # IF node) only when one is due, where the others launch it predicated.
+    assert launches[False] == launches[None], launches
+    if form == "reliable":
+        assert launches[True] < launches[None], launches
+    else:
+        assert launches[True] > launches[None], launches
     for phys in ("elastic", "thermal"):
         it0, u0 = out[(False, phys)]
         it1, u1 = out[(True, phys)]
