@@ -1606,9 +1606,112 @@ __global__ void k_level1_elements(const double* __restrict__ rho, const double* 
   for (int c = 0; c < 8; ++c) {
     const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
     const double r = rb[((size_t)(2 * X + cx) * nf + (2 * Y + cy)) * nf + (2 * Z + cz)];
-    s += r * M[c * kk + ij];
+    s = fma(r, M[c * kk + ij], s);
   }
-  KE[((size_t)b * Nc + e) * kk + ij] = scale * s;
+  KE[((size_t)b * Nc + e) * kk + ij] = __dmul_rn(scale, s);
+}
+
+// Level-1 node stencils straight from the fine densities, without forming
+// the level-1 element matrices: the D x D block of node n and offset o sums,
+// over the level-1 elements holding both nodes, scale * sum_c rho_c M_c of
+// that element (the matrix k_level1_elements forms, with the same operations
+// in the same order, so these are the stencils k_stencil_from_elements builds
+// from its output); block-diagonal inverse at o = 13.  Consecutive threads are
+// consecutive nodes of one offset, so the table entries they read coincide.
+template <typename T, int D>
+__global__ void k_level1_stencils(const double* __restrict__ rho, const double* __restrict__ M, T* __restrict__ S,
+                                  T* __restrict__ Dinv, int n, double scale, const int* active) {
+  constexpr int k = 8 * D, kk = k * k;
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n, nf = 2 * n;
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= N * 27) return;
+  const int node = t % N, o = t / N;
+  const int z = node % n, y = (node / n) % n, x = node / (n * n);
+  const int ox = o / 9 - 1, oy = (o / 3) % 3 - 1, oz = o % 3 - 1;
+  const double* rb = rho + (size_t)b * nf * nf * nf;
+  double C[D][D] = {};
+  for (int q = 0; q < 8; ++q) {
+    const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
+    const int cx = 1 - qx, cy = 1 - qy, cz = 1 - qz;
+    const int nx = cx + ox, ny = cy + oy, nz = cz + oz;
+    if (nx < 0 || nx > 1 || ny < 0 || ny > 1 || nz < 0 || nz > 1) continue;
+    const int ex = wrapn(x + qx - 1, n), ey = wrapn(y + qy - 1, n), ez = wrapn(z + qz - 1, n);
+    double rc[8];
+#pragma unroll
+    for (int ch = 0; ch < 8; ++ch) {
+      const int hx = (ch >> 2) & 1, hy = (ch >> 1) & 1, hz = ch & 1;
+      rc[ch] = rb[((size_t)(2 * ex + hx) * nf + (2 * ey + hy)) * nf + (2 * ez + hz)];
+    }
+    const int aa = lidx(cx, cy, cz), bb = lidx(nx, ny, nz);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        const int ij = (D * aa + i) * k + D * bb + j;
+        double sum = 0;
+#pragma unroll
+        for (int ch = 0; ch < 8; ++ch) sum = fma(rc[ch], __ldg(M + ch * kk + ij), sum);
+        C[i][j] = __dadd_rn(C[i][j], __dmul_rn(scale, sum));
+      }
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) S[(((size_t)b * 27 + o) * D * D + i * D + j) * N + node] = (T)C[i][j];
+  if (o == 13) {
+    double Ci[D][D];
+    block_inverse<double, D>(C, Ci);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) Dinv[((size_t)b * D * D + i * D + j) * N + node] = (T)Ci[i][j];
+  }
+}
+
+// Level-2 element matrices straight from the fine densities:
+// K_2[E] = scale * sum over the 4^3 fine elements f of E of rho_f G_f, with
+// G_f the exact two-level Galerkin product of one fine element of unit
+// density (host table, f = (4 fx + fy) 4 + fz).  A block owns kL2Elems
+// elements, its threads the matrix entries: each G_f entry is read once per
+// block and used for all of them.
+constexpr int kL2Elems = 8;
+template <int D>
+__global__ void __launch_bounds__(kThreads) k_level2_elements(const double* __restrict__ rho,
+                                                              const double* __restrict__ G, double* __restrict__ KE,
+                                                              int nc, double scale, const int* active) {
+  constexpr int k = 8 * D, kk = k * k;
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int Nc = nc * nc * nc, nf = 4 * nc;
+  const int e0 = blockIdx.x * kL2Elems;
+  __shared__ double sr[64][kL2Elems];
+  for (int t = threadIdx.x; t < 64 * kL2Elems; t += kThreads) {
+    const int f = t / kL2Elems, el = t - f * kL2Elems, e = e0 + el;
+    double v = 0;
+    if (e < Nc) {
+      const int Z = e % nc, Y = (e / nc) % nc, X = e / (nc * nc);
+      const int fx = f >> 4, fy = (f >> 2) & 3, fz = f & 3;
+      v = rho[(size_t)b * nf * nf * nf + ((size_t)(4 * X + fx) * nf + (4 * Y + fy)) * nf + (4 * Z + fz)];
+    }
+    sr[f][el] = v;
+  }
+  __syncthreads();
+  for (int ij = threadIdx.x; ij < kk; ij += kThreads) {
+    double acc[kL2Elems];
+#pragma unroll
+    for (int el = 0; el < kL2Elems; ++el) acc[el] = 0;
+#pragma unroll 4
+    for (int f = 0; f < 64; ++f) {
+      const double g = __ldg(G + (size_t)f * kk + ij);
+#pragma unroll
+      for (int el = 0; el < kL2Elems; ++el) acc[el] = fma(sr[f][el], g, acc[el]);
+    }
+#pragma unroll
+    for (int el = 0; el < kL2Elems; ++el)
+      if (e0 + el < Nc) KE[((size_t)b * Nc + e0 + el) * kk + ij] = scale * acc[el];
+  }
 }
 
 // K_{l+1}[E] = sum_c (W_c (x) I)^T K_l[child c] (W_c (x) I), one block per coarse element
@@ -1779,31 +1882,47 @@ __global__ void k_chol_inverse(double* __restrict__ A, double* __restrict__ work
 // Same result for ndof <= kCholSmemMax, with the packed lower triangle of the
 // regularised matrix held in shared memory (one block of 1024 threads per cell).
 constexpr int kCholSmemMax = 192;
-constexpr int kCholThreads = 1024;
-// packed lower triangle of L (then of L^-1) and one column buffer
+constexpr int kCholThreads = 512;
+constexpr int kCholPanel = 8;  // columns per panel of the blocked factorisation and inversion
+// packed lower triangle of L (then of L^-1) and one panel of saved columns
 __host__ __device__ constexpr size_t chol_smem_bytes(int ndof) {
-  return ((size_t)ndof * (ndof + 1) / 2 + (size_t)ndof) * sizeof(double);
+  return ((size_t)ndof * (ndof + 1) / 2 + (size_t)kCholPanel * ndof) * sizeof(double);
 }
 
 // A <- (A + reg * I_blocks)^-1 for one cell per CTA, A symmetric positive
 // (semi-)definite of order ndof <= kCholSmemMax: Cholesky factor L in shared
-// memory, its inverse X = L^{-1} in place, then A^{-1} = X^T X.  Every phase
-// runs all columns at once (one barrier-separated step per pivot).  A zero or
-// negative pivot sets status[b] (nullable) and continues with a tiny pivot.
+// memory, its inverse X = L^{-1} in place, then A^{-1} = X^T X.  The
+// factorisation and the inversion run by panels of kCholPanel columns with
+// three block barriers each: one warp factors the panel's diagonal block in
+// registers, then every row below it is an independent triangular solve (one
+// thread per row), and the rest of the matrix takes the panel as one
+// rank-kCholPanel update.  The inversion mirrors it (the panel rows' columns
+// are independent triangular solves, then a rank-kCholPanel update of the rows
+// below).  A zero or negative pivot sets status[b] (nullable) and continues
+// with a tiny pivot.
 __global__ void __launch_bounds__(kCholThreads) k_chol_inverse_smem(double* __restrict__ A, int ndof, int D,
                                                                     const int* active, int* status) {
+  constexpr int NB = kCholPanel;
   const int b = blockIdx.x;
   if (active && !active[b]) return;
   extern __shared__ double Lp[];  // packed lower triangle, row i starts at i(i+1)/2
   double* M = A + (size_t)b * ndof * ndof;
   const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
-  double* colk = Lp + (size_t)ndof * (ndof + 1) / 2;  // column k of L below the pivot
+  double* P = Lp + (size_t)ndof * (ndof + 1) / 2;  // panel columns of the rows below: P[q * ndof + i]
+  // (column-major, so that lanes reading consecutive rows hit distinct banks)
+  auto at = [&](int i, int j) -> double& { return Lp[(size_t)i * (i + 1) / 2 + j]; };
+  __shared__ double sL[NB][NB];  // the panel's diagonal block of L
+  __shared__ double sR[NB];      // reciprocals of its diagonal
   __shared__ double s_alpha;
+  __shared__ int s_bad;
   if (warp == 0) {
     double t = 0;
     for (int i = lane; i < ndof; i += 32) t += M[(size_t)i * ndof + i];
     for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
-    if (lane == 0) s_alpha = t / ndof;
+    if (lane == 0) {
+      s_alpha = t / ndof;
+      s_bad = 0;
+    }
   }
   __syncthreads();
   const double reg = s_alpha / (ndof / D);
@@ -1811,47 +1930,127 @@ __global__ void __launch_bounds__(kCholThreads) k_chol_inverse_smem(double* __re
     for (int j = lane; j <= i; j += 32)
       Lp[(size_t)i * (i + 1) / 2 + j] = M[(size_t)i * ndof + j] + (((i - j) % D) == 0 ? reg : 0.0);
   __syncthreads();
-  for (int k = 0; k < ndof; ++k) {
-    const size_t kk = (size_t)k * (k + 1) / 2 + k;
-    // every thread forms the pivot from the same value; column k is scaled
-    // into place and into the contiguous copy read by the trailing update
-    double d = Lp[kk];
-    if (!(d > 0)) {
-      if (status && tid == 0) status[b] = 1;
-      d = 1e-300;
-    }
-    const double piv = sqrt(d);
-    for (int i = k + 1 + tid; i < ndof; i += nth) {
-      const size_t e = (size_t)i * (i + 1) / 2 + k;
-      const double v = Lp[e] / piv;
-      Lp[e] = v;
-      colk[i] = v;
+  // ---- factorisation A = L L^T
+  for (int k0 = 0; k0 < ndof; k0 += NB) {
+    const int kb = min(NB, ndof - k0), k1 = k0 + kb;
+    if (warp == 0) {
+      // diagonal block, lane i holding row i, right-looking over its columns
+      double a[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) a[q] = (lane < kb && q <= lane) ? at(k0 + lane, k0 + q) : 0.0;
+      bool bad = false;
+#pragma unroll
+      for (int j = 0; j < NB; ++j) {
+        if (j < kb) {
+          double d = __shfl_sync(0xffffffffu, a[j], j);
+          if (!(d > 0)) {
+            bad = true;
+            d = 1e-300;
+          }
+          const double piv = sqrt(d), rp = 1.0 / piv;
+          if (lane == j) a[j] = piv;
+          if (lane > j) a[j] *= rp;
+#pragma unroll
+          for (int q = j + 1; q < NB; ++q) {
+            const double lqj = __shfl_sync(0xffffffffu, a[j], q);
+            if (q < kb && lane >= q) a[q] -= a[j] * lqj;
+          }
+          if (lane == 0) sR[j] = rp;
+        }
+      }
+      if (lane < NB)
+#pragma unroll
+        for (int q = 0; q < NB; ++q) sL[lane][q] = a[q];
+      if (bad && lane == 0) s_bad = 1;
     }
     __syncthreads();
-    if (tid == 0) Lp[kk] = piv;
-    for (int i = k + 1 + warp; i < ndof; i += nw) {
-      const size_t ri = (size_t)i * (i + 1) / 2;
-      const double lik = colk[i];
-      for (int j = k + 1 + lane; j <= i; j += 32) Lp[ri + j] -= lik * colk[j];
+    // rows below the panel: L21 row i = A21 row i L11^{-T}
+    for (int i = k1 + tid; i < ndof; i += nth) {
+      double l[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        double v = q < kb ? at(i, k0 + q) : 0.0;
+#pragma unroll
+        for (int t = 0; t < q; ++t) v -= l[t] * sL[q][t];
+        l[q] = q < kb ? v * sR[q] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        if (q < kb) at(i, k0 + q) = l[q];
+        P[(size_t)q * ndof + i] = l[q];
+      }
+    }
+    if (tid < NB * NB) {
+      const int i = tid / NB, j = tid % NB;
+      if (i < kb && j <= i) at(k0 + i, k0 + j) = sL[i][j];
+    }
+    __syncthreads();
+    // trailing update: L[i][j] -= sum_q L[i][k0+q] L[j][k0+q], k1 <= j <= i
+    for (int i = k1 + warp; i < ndof; i += nw) {
+      double li[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) li[q] = P[(size_t)q * ndof + i];
+      double* row = Lp + (size_t)i * (i + 1) / 2;
+      for (int j = k1 + lane; j <= i; j += 32) {
+        double sum = 0;
+#pragma unroll
+        for (int q = 0; q < NB; ++q) sum = fma(li[q], P[(size_t)q * ndof + j], sum);
+        row[j] -= sum;
+      }
     }
     __syncthreads();
   }
-  // X = L^{-1} in place of L: forward substitution L X = I for all columns at
-  // once, right-looking over p.  Entry (i, j), j < i, holds the running
-  // b_ij = -sum_{q<p} L_iq x_qj until step p = i turns it into x_ij.  Rows go
-  // to warps, columns to lanes (no index divisions in the inner loops).
-  for (int p = 0; p < ndof; ++p) {
-    const size_t rp = (size_t)p * (p + 1) / 2;
-    const double inv = 1.0 / Lp[rp + p];
-    for (int i = p + 1 + tid; i < ndof; i += nth) colk[i] = Lp[(size_t)i * (i + 1) / 2 + p];
+  if (status && tid == 0 && s_bad) status[b] = 1;
+  // ---- X = L^{-1} in place of L.  Before panel p0, entry (i, j), j < p0 <= i,
+  // holds b_ij = -sum_{p<p0} L_ip x_pj; the entries j >= p0 still hold L.
+  for (int p0 = 0; p0 < ndof; p0 += NB) {
+    const int pb = min(NB, ndof - p0), p1 = p0 + pb;
+    if (tid < NB * NB) {
+      const int i = tid / NB, j = tid % NB;
+      sL[i][j] = (i < pb && j <= i) ? at(p0 + i, p0 + j) : 0.0;
+      if (j == 0) sR[i] = i < pb ? 1.0 / at(p0 + i, p0 + i) : 0.0;
+    }
+    for (int i = p1 + tid; i < ndof; i += nth)
+#pragma unroll
+      for (int q = 0; q < NB; ++q) P[(size_t)q * ndof + i] = q < pb ? at(i, p0 + q) : 0.0;
     __syncthreads();
-    for (int j = tid; j <= p; j += nth) Lp[rp + j] = (j == p) ? inv : Lp[rp + j] * inv;
+    // the panel rows: column j < p0 is x = L11^{-1} b (forward substitution);
+    // column p0 + c of the diagonal block is L11^{-1} e_c
+    for (int j = tid; j < p1; j += nth) {
+      double x[NB];
+      const int c = j - p0;  // >= 0 inside the diagonal block
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        double v;
+        if (c < 0)
+          v = q < pb ? at(p0 + q, j) : 0.0;
+        else
+          v = q == c ? 1.0 : 0.0;
+#pragma unroll
+        for (int t = 0; t < q; ++t) v -= sL[q][t] * x[t];
+        x[q] = q < pb ? v * sR[q] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q)
+        if (q < pb && (c < 0 || q >= c)) at(p0 + q, j) = x[q];
+    }
     __syncthreads();
-    for (int i = p + 1 + warp; i < ndof; i += nw) {
+    // rows below: entry (i, j), j < p1, becomes
+    // (j < p0 ? b_ij : 0) - sum_q L_i,p0+q x_p0+q,j   (x_pj = 0 for j > p)
+    for (int i = p1 + warp; i < ndof; i += nw) {
+      double li[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) li[q] = P[(size_t)q * ndof + i];
       double* row = Lp + (size_t)i * (i + 1) / 2;
-      const double lip = colk[i];
-      for (int j = lane; j < p; j += 32) row[j] -= lip * Lp[rp + j];
-      if (lane == 0) row[p] = -lip * Lp[rp + p];
+      for (int j = lane; j < p1; j += 32) {
+        double sum = 0;
+#pragma unroll
+        for (int q = 0; q < NB; ++q) {
+          const int p = p0 + q;
+          if (q < pb && j <= p) sum = fma(li[q], at(p, j), sum);
+        }
+        row[j] = (j < p0 ? row[j] : 0.0) - sum;
+      }
     }
     __syncthreads();
   }

@@ -9,6 +9,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
+#include <memory>
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
@@ -119,6 +120,7 @@ struct Phys {
   bool current = false;  // the solution belongs to the current density
   int built_prec = -1;
   double* KE[kMaxLevels] = {};   // FP64 element matrices of level l >= 1
+  bool ke1_formed = false;       // KE[1] holds this density's level-1 element matrices
   double* S64c = nullptr;        // FP64 coarsest stencil
   double* Ainv = nullptr;        // FP64 coarsest inverse [B][ndof][ndof]
   double* cwork = nullptr;
@@ -172,6 +174,12 @@ struct Lane {
   // power iterations of the other levels
   cudaStream_t side = nullptr;
   cudaEvent_t side_fork = nullptr, side_join = nullptr;
+  // power iterations of the levels below 1, concurrent: a stream, events and
+  // partial sums per level
+  cudaStream_t pw[kMaxLevels] = {};
+  cudaEvent_t pw_fork = nullptr, pw_join[kMaxLevels] = {};
+  double* pw_part[kMaxLevels] = {};
+  double* pw_red[kMaxLevels] = {};
   int* fb_mask = nullptr;  // cells re-solved in FP64 after a mixed-precision breakdown
   int* fb_bad = nullptr;   // per cell: the iterate holds a non-finite value
 };
@@ -510,22 +518,68 @@ template <typename T, int D>
 static void power_bounds(maple_ctx* c, Phys& p, Ops<T>& o, cudaStream_t s, const int* act) {
   // level 0: the element bound holds for every density
   KL(c, s, k_fill<double><<<nblk(c->B), kThreads, 0, s>>>(o.hi[0], c->B, g_tab.lam_elem[D == 3 ? 0 : 1]));
+  // Levels are independent: level 1 (the longest chain) runs on the
+  // caller's stream, the deeper levels each on a stream of their own with
+  // their own partial sums, joined back before the build returns.
+  Lane& ln = LN(c);
+  CK(cudaEventRecord(ln.pw_fork, s));
   for (int l = 1; l < c->L - 1; ++l) {
     const int Nl = nodes(c->n[l]);
+    const size_t len = (size_t)c->B * Nl * D;
+    cudaStream_t st = s;
+    if (l > 1) {
+      st = ln.pw[l];
+      CK(cudaStreamWaitEvent(st, ln.pw_fork, 0));
+    }
+    double* part = ln.pw_part[l];
+    double* red = ln.pw_red[l];
     T* v = o.U[l][0];
     T* w = o.U[l][1];
-    KL(c, s, k_power_init<T><<<nblk((size_t)c->B * Nl * D), kThreads, 0, s>>>(v, (size_t)c->B * Nl * D));
+    KL(c, st, k_power_init<T><<<nblk(len), kThreads, 0, st>>>(v, len));
     for (int it = 0; it < c->power_iters; ++it) {
       ApplyArgs<T> a{};
       a.u = v;
       a.out = w;
-      a.part = LN(c).part;
-      apply<T, D, 1, M_POWER>(c, p, o, l, a, act, s);
+      a.part = part;
+      apply<T, D, 1, M_POWER>(c, p, o, l, a, act, st);
       std::swap(v, w);
     }
-    reduce<2>(c, LN(c).part, ceil_div(Nl, kPowerNodes<D>), LN(c).red, s);
-    KL(c, s, k_power_finish<<<nblk(c->B), kThreads, 0, s>>>(LN(c).red, o.hi[l], c->B, c->power_safety));
+    reduce<2>(c, part, ceil_div(Nl, kPowerNodes<D>), red, st);
+    KL(c, st, k_power_finish<<<nblk(c->B), kThreads, 0, st>>>(red, o.hi[l], c->B, c->power_safety));
+    if (l > 1) {
+      CK(cudaEventRecord(ln.pw_join[l], st));
+      CK(cudaStreamWaitEvent(s, ln.pw_join[l], 0));
+    }
   }
+}
+
+// Per-device copies of the host coarsening tables (M: level-1 child
+// matrices, G: level-2 fine-element matrices), uploaded once and kept for the
+// process; looked up under the lock (contexts may build on several threads).
+enum { TAB_M = 0, TAB_G = 1 };
+static const double* device_table(maple_ctx* c, int D, int which) {
+  static double* slots[128][2][2] = {};
+  std::lock_guard<std::mutex> lk(g_mu);
+  double*& slot = slots[c->dev][D == 3 ? 0 : 1][which];
+  if (!slot) {
+    const int k = 8 * D;
+    const double* src = which == TAB_M ? (D == 3 ? g_tab.M3 : g_tab.M1) : (D == 3 ? g_tab.G3 : g_tab.G1);
+    const size_t bytes = (size_t)(which == TAB_M ? 8 : 64) * k * k * sizeof(double);
+    double* m = nullptr;
+    CK(cudaMalloc(&m, bytes));
+    CK(cudaMemcpy(m, src, bytes, cudaMemcpyHostToDevice));
+    slot = m;
+  }
+  return slot;
+}
+
+// level-1 element matrices into p.KE[1] (the direct build does not form them)
+template <int D>
+static void level1_elements(maple_ctx* c, Phys& p, cudaStream_t s, const int* act) {
+  const int nc = c->n[1], k = 8 * D;
+  const size_t tot = (size_t)nodes(nc) * k * k;
+  KL(c, s, k_level1_elements<D><<<g2(tot, c->B), kThreads, 0, s>>>(p.o64.rho, device_table(c, D, TAB_M), p.KE[1], nc,
+                                                                      p.kscale, act));
 }
 
 template <int D>
@@ -535,29 +589,28 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s, co
   bool side_inverse = false;
   const int B = c->B, k = 8 * D, L = c->L;
   const int* act = mask ? mask : c->active;
-  // level-1 element matrices from the fine densities
-  {
-    const int nc = c->n[1];
-    const size_t tot = (size_t)nodes(nc) * k * k;
-    // the level-1 coarsening table, uploaded once per device and kept for the
-    // process; looked up under the lock (contexts may build on several threads)
-    const double* M = nullptr;
-    static double* dM[128][2] = {};
-    {
-      std::lock_guard<std::mutex> lk(g_mu);
-      double*& slot = dM[c->dev][D == 3 ? 0 : 1];
-      if (!slot) {
-        double* m = nullptr;
-        const size_t bytes = (size_t)8 * k * k * sizeof(double);
-        CK(cudaMalloc(&m, bytes));
-        CK(cudaMemcpy(m, D == 3 ? g_tab.M3 : g_tab.M1, bytes, cudaMemcpyHostToDevice));
-        slot = m;
-      }
-      M = slot;
-    }
-    KL(c, s, k_level1_elements<D><<<g2(tot, B), kThreads, 0, s>>>(p.o64.rho, M, p.KE[1], nc, p.kscale, act));
+  // With a level 2, the level-1 stencils and the level-2 element matrices
+  // come straight from the fine densities (the level-1 element matrices,
+  // 4.6 KB per level-1 element, are never formed); otherwise level 1 is the
+  // coarsest and its element matrices are formed as before.
+  const bool direct = L >= 3;
+  if (direct) {
+    const int n1 = c->n[1], N1 = nodes(n1), n2 = c->n[2], N2 = nodes(n2);
+    const double* M = device_table(c, D, TAB_M);
+    if (prec == MAPLE_FP64)
+      KL(c, s, k_level1_stencils<double, D><<<g2((size_t)N1 * 27, B), kThreads, 0, s>>>(
+                   p.o64.rho, M, p.o64.S[1], p.o64.Dinv[1], n1, p.kscale, act));
+    else
+      KL(c, s, k_level1_stencils<float, D><<<g2((size_t)N1 * 27, B), kThreads, 0, s>>>(
+                   p.o64.rho, M, p.o32.S[1], p.o32.Dinv[1], n1, p.kscale, act));
+    KL(c, s, k_level2_elements<D><<<dim3((unsigned)ceil_div(N2, kL2Elems), B), kThreads, 0, s>>>(
+                 p.o64.rho, device_table(c, D, TAB_G), p.KE[2], n2, p.kscale, act));
+    p.ke1_formed = false;
+  } else {
+    level1_elements<D>(c, p, s, act);
+    p.ke1_formed = true;
   }
-  for (int l = 1; l < L; ++l) {
+  for (int l = direct ? 2 : 1; l < L; ++l) {
     const int n = c->n[l], N = nodes(n);
     if (l < L - 1) {
       if (prec == MAPLE_FP64) {
@@ -1753,7 +1806,8 @@ int maple_element_matrices(int r, double E, double nu, double kappa, double* Ke3
                            double* Ke1, double* Fe1, double* X01) {
   return guarded([&] {
     require(r >= 1, "resolution must be positive");
-    ElementTables t;
+    std::unique_ptr<ElementTables> tp(new ElementTables);  // about 0.4 MB: not on the stack
+    ElementTables& t = *tp;
     element_tables(E, nu, kappa, &t);
     const double h = 1.0 / r;
     for (int i = 0; i < 576; ++i) if (Ke3) Ke3[i] = t.Ke3[i] * h;
@@ -1834,6 +1888,15 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
         L.o_live = dnew<int>(c, B);
         L.rel = dnew<int>(c, B);
         L.o_t = dnew<double>(c, B * 6);
+        CK(cudaEventCreateWithFlags(&L.pw_fork, cudaEventDisableTiming));
+        for (int l = 1; l + 1 < c->L; ++l) {
+          L.pw_part[l] = dnew<double>(c, (size_t)B * nodes(c->n[l]) * 2);
+          L.pw_red[l] = dnew<double>(c, (size_t)B * 2);
+          if (l > 1) {
+            CK(cudaStreamCreateWithFlags(&L.pw[l], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&L.pw_join[l], cudaEventDisableTiming));
+          }
+        }
         L.breakdown = dnew<int>(c, 1);
         CK(cudaMemset(L.breakdown, 0, sizeof(int)));
         L.loop = dnew<int>(c, 3);
@@ -1861,8 +1924,14 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
       CK(cudaMallocHost(&c->h_err, sizeof(int)));
     } catch (...) {
       for (void* p : c->allocs) cudaFree(p);
-      for (Lane& L : c->lanes)
+      for (Lane& L : c->lanes) {
         if (L.h_flags) cudaFreeHost(L.h_flags);
+        if (L.pw_fork) cudaEventDestroy(L.pw_fork);
+        for (int l = 0; l < kMaxLevels; ++l) {
+          if (L.pw[l]) cudaStreamDestroy(L.pw[l]);
+          if (L.pw_join[l]) cudaEventDestroy(L.pw_join[l]);
+        }
+      }
       if (c->h_err) cudaFreeHost(c->h_err);
       delete c;
       throw;
@@ -1936,6 +2005,11 @@ int maple_ctx_destroy(maple_ctx* c) {
       if (L.side_fork) cudaEventDestroy(L.side_fork);
       if (L.side_join) cudaEventDestroy(L.side_join);
       if (L.h_flags) cudaFreeHost(L.h_flags);
+      if (L.pw_fork) cudaEventDestroy(L.pw_fork);
+      for (int l = 0; l < kMaxLevels; ++l) {
+        if (L.pw[l]) cudaStreamDestroy(L.pw[l]);
+        if (L.pw_join[l]) cudaEventDestroy(L.pw_join[l]);
+      }
     }
     if (c->pen_work) cudaFree(c->pen_work);
     if (c->h_err) cudaFreeHost(c->h_err);
@@ -2368,6 +2442,13 @@ int maple_get_level_elements(maple_ctx* c, int phys, int level, double* out, map
     Phys& p = c->ph[phys];
     require(p.built, "no hierarchy built for this physics (call maple_set_density first)");
     const size_t k = 8 * (size_t)p.D;
+    if (level == 1 && !p.ke1_formed) {
+      if (p.D == 3)
+        level1_elements<3>(c, p, S(s), c->active);
+      else
+        level1_elements<1>(c, p, S(s), c->active);
+      p.ke1_formed = true;
+    }
     CK(cudaMemcpyAsync(out, p.KE[level], (size_t)c->B * nodes(c->n[level]) * k * k * sizeof(double),
                        cudaMemcpyDeviceToDevice, S(s)));
   });

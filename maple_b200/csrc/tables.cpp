@@ -178,6 +178,27 @@ void element_tables(double E, double nu, double kappa, ElementTables* t) {
         t->M1[(c * 8 + a) * 8 + b] = s;
       }
   }
+  for (int f = 0; f < 64; ++f) {
+    const int fx = f >> 4, fy = (f >> 2) & 3, fz = f & 3;
+    const int c1 = ((fx >> 1) << 2) | ((fy >> 1) << 1) | (fz >> 1);
+    const int c0 = ((fx & 1) << 2) | ((fy & 1) << 1) | (fz & 1);
+    const double* W = &t->W[c1 * 64];
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) {
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            double s = 0;
+            for (int a2 = 0; a2 < 8; ++a2)
+              for (int b2 = 0; b2 < 8; ++b2)
+                s += W[a2 * 8 + a] * W[b2 * 8 + b] * t->M3[(c0 * 24 + 3 * a2 + i) * 24 + 3 * b2 + j];
+            t->G3[(f * 24 + 3 * a + i) * 24 + 3 * b + j] = s;
+          }
+        double s = 0;
+        for (int a2 = 0; a2 < 8; ++a2)
+          for (int b2 = 0; b2 < 8; ++b2) s += W[a2 * 8 + a] * W[b2 * 8 + b] * t->M1[(c0 * 8 + a2) * 8 + b2];
+        t->G1[(f * 8 + a) * 8 + b] = s;
+      }
+  }
   // Upper bound of lambda_max(D^-1 A) for any assembly of scaled copies of Ke0,
   // D = assembled (block) diagonal: max_e lambda_max(D_e^-1 K_e), obtained by
   // power iteration on the element matrix (it is the same for every element).

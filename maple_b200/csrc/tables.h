@@ -17,6 +17,12 @@ struct ElementTables {
   double W[8 * 8 * 8];      // child prolongation weights W[c][a][b]
   double M3[8 * 24 * 24];   // W_c^T Ke3 W_c
   double M1[8 * 8 * 8];     // W_c^T Ke1 W_c
+  // level-2 element matrix of one fine element of unit density at position
+  // f = (4 fx + fy) 4 + fz of the level-2 element's 4^3 fine elements:
+  // G_f = (W_c1 (x) I)^T M_c0 (W_c1 (x) I), c1 = the level-1 child (f / 2 per
+  // axis), c0 = the fine element inside it (f % 2 per axis)
+  double G3[64 * 24 * 24];
+  double G1[64 * 8 * 8];
   double lam_elem[2];       // lambda_max(D_e^-1 K_e): [elastic, thermal]
 };
 
