@@ -2700,6 +2700,85 @@ __global__ void __launch_bounds__(kThreads) k_homogenize(const double* __restric
   block_sum_store<K>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * K);
 }
 
+// The elastic form (D = 3, R = 6) with the same energies, register-lean:
+// warp s of a 192-thread block owns load case s of 32 consecutive elements,
+// eight such groups per block (256 elements: the generic kernel's partial-sum
+// count).  The six fields X0 - u_e of a group meet in shared memory, so a
+// thread holds only its K (X0 - u_e) column (the generic kernel held both
+// vectors of every pair and ran at one block per SM).  Energies are formed
+// with the generic kernel's operations in its order (bit-identical); the
+// block partial sums of C^H add in a different order.
+constexpr int kHomWarps = 6, kHomGroups = 8;
+__global__ void __launch_bounds__(32 * kHomWarps) k_homogenize_elastic(const double* __restrict__ u,
+                                                                      const double* __restrict__ rho,
+                                                                      double* __restrict__ energy,
+                                                                      double* __restrict__ part, int n,
+                                                                      double kscale, double xscale,
+                                                                      const int* active) {
+  constexpr int D = 3, R = 6, k = 24, K = 21;
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n;
+  const int s = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ double sL[R][k][33];
+  __shared__ double sv[K];
+  const double* __restrict__ ub = u + (size_t)b * N * R * D;
+  double vacc[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) vacc[r] = 0;
+  for (int grp = 0; grp < kHomGroups; ++grp) {
+    const int e = (blockIdx.x * kHomGroups + grp) * 32 + lane;
+    const bool valid = e < N;
+    const int ee = valid ? e : 0;
+    const int z = ee % n, y = (ee / n) % n, x = ee / (n * n);
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int node = (wrapn(x + corner_x(a), n) * n + wrapn(y + corner_y(a), n)) * n + wrapn(z + corner_z(a), n);
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+        sL[s][D * a + i][lane] = xscale * x0<D>(D * a + i, s) - __ldg(ub + (size_t)(s * D + i) * N + node);
+    }
+    __syncthreads();
+    double KL[k];
+#pragma unroll
+    for (int p = 0; p < k; ++p) KL[p] = 0;
+#pragma unroll
+    for (int q = 0; q < k; ++q) {
+      const double lq = sL[s][q][lane];
+#pragma unroll
+      for (int p = 0; p < k; ++p) KL[p] += ke<double, D>(p, q) * lq;
+    }
+#pragma unroll
+    for (int p = 0; p < k; ++p) KL[p] = kscale * KL[p];
+    const double re = valid ? rho[(size_t)b * N + ee] : 0.0;
+    double* eo = energy + (size_t)b * R * R * N + ee;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (r <= s) {
+        double acc = 0;
+#pragma unroll
+        for (int q = 0; q < k; ++q) acc += sL[r][q][lane] * KL[q];
+        vacc[r] += re * acc;
+        if (valid) {
+          eo[(size_t)(r * R + s) * N] = acc;
+          eo[(size_t)(s * R + r) * N] = acc;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // pair (r, s), r <= s: warp s, component r; packed upper-triangle index
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    double v = vacc[r];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0 && r <= s) sv[r * R - r * (r - 1) / 2 + (s - r)] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < K) part[((size_t)b * gridDim.x + blockIdx.x) * K + threadIdx.x] = sv[threadIdx.x];
+}
+
 // unpack reduced upper triangles into full symmetric matrices H[cell][R][R]
 __global__ void k_unpack_sym(const double* __restrict__ red, double* __restrict__ H, int B, int R) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -3087,6 +3166,146 @@ __global__ void __launch_bounds__(kThreads) k_oc_update(OcArgs a) {
     for (int k = 0; k < G; ++k) {
       t += __ldcg(a.part + ((size_t)b * 4 + 2) * G + k);
       m = fmax(m, __ldcg(a.part + ((size_t)b * 4 + 3) * G + k));
+    }
+    a.stats[2 * b] = m;
+    a.stats[2 * b + 1] = t / (double)N;
+    if (a.lam_out) a.lam_out[b] = lam;
+  }
+}
+
+// The same OC update resolving LV bisection steps per grid barrier: each pass
+// evaluates the volume at the 2^LV - 1 midpoints the next LV steps can visit
+// (the bisection tree below the current [l1, l2], each midpoint formed as
+// 0.5 (lo + hi) exactly as the step that would reach it), with the per-block
+// sums and their reduction over blocks in the order k_oc_update uses, then
+// walks the tree with those volumes, taking k_oc_update's branches; the
+// launch waits at 60 / LV + 1 barriers instead of 61.  Partial sums:
+// [cells][2][G][2^LV - 1], then the |dx| statistics [cells][2][G].
+constexpr int kOcMaxG = 160;  // blocks per cell k_oc_update_tree supports
+template <int LV>
+__global__ void __launch_bounds__(kThreads) k_oc_update_tree(OcArgs a) {
+  constexpr int NC = (1 << LV) - 1;
+  static_assert(60 % LV == 0, "LV must divide the 60 bisection steps");
+  const int G = gridDim.x, g = blockIdx.x, b = blockIdx.y;
+  const unsigned nblocks = gridDim.x * gridDim.y + a.phantom;
+  const bool act = !a.active || a.active[b];
+  const int N = a.N;
+  const int chunk = (N + G - 1) / G;
+  const int lo_i = g * chunk, hi_i = min(N, lo_i + chunk);
+  const double* xb = a.x + (size_t)b * N;
+  const double* db = a.dJ + (size_t)b * N;
+  const double vf = act ? a.volfrac[b] : 0.0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ double s_tot[NC];
+  double l1 = 1e-12, l2 = 1e6, lam = 0;
+  for (int pass = 0; pass < 60 / LV; ++pass) {
+    double lamc[NC];
+    {
+      double lo[NC], hi[NC];
+      lo[0] = l1;
+      hi[0] = l2;
+#pragma unroll
+      for (int h = 0; h < NC; ++h) {
+        const double m = 0.5 * (lo[h] + hi[h]);
+        lamc[h] = m;
+        if (2 * h + 2 < NC) {
+          lo[2 * h + 1] = lo[h];  // volume <= vf: l2 = m
+          hi[2 * h + 1] = m;
+          lo[2 * h + 2] = m;      // volume > vf: l1 = m
+          hi[2 * h + 2] = hi[h];
+        }
+      }
+    }
+    // sqrt(dJ / lambda) as sqrt(dJ) / sqrt(lambda): one square root per
+    // element and pass instead of a division and a root per candidate.  The
+    // volumes differ from k_oc_update's by rounding, which can only change a
+    // branch whose volume is within rounding of vf, i.e. at a midpoint within
+    // rounding of the root, so lambda agrees to rounding.
+    double rl[NC], sc[NC];
+#pragma unroll
+    for (int h = 0; h < NC; ++h) {
+      rl[h] = 1.0 / sqrt(lamc[h]);
+      sc[h] = 0;
+    }
+    if (act) {
+      for (int i = lo_i + threadIdx.x; i < hi_i; i += kThreads) {
+        const double xv = xb[i];
+        const double xs = xv * sqrt(fmax(db[i], 1e-12));
+        const double lo = fmax(xv - a.move, a.xmin), hi = fmin(xv + a.move, 1.0);
+#pragma unroll
+        for (int h = 0; h < NC; ++h) sc[h] += fmin(fmax(xs * rl[h], lo), hi);
+      }
+    }
+    double* pp = a.part + (((size_t)b * 2 + (pass & 1)) * G) * NC;
+    block_sum_store<NC>(sc, pp + (size_t)g * NC);
+    if (!grid_barrier(a.bar, a.bar + 1, nblocks, a.err, a.poll_limit)) return;
+    if (act) {
+      // the volumes over the G blocks, summed in k_oc_update's order (lane
+      // strided, then the shuffle tree); every load of a warp's candidates is
+      // issued before the first sum (G <= kOcMaxG)
+      constexpr int NW = kThreads / 32, KM = kOcMaxG / 32, HM = (NC + NW - 1) / NW;
+      double vals[HM][KM];
+#pragma unroll
+      for (int r = 0; r < HM; ++r)
+#pragma unroll
+        for (int m = 0; m < KM; ++m) {
+          const int h = warp + r * NW, k = lane + 32 * m;
+          vals[r][m] = (h < NC && k < G) ? __ldcg(pp + (size_t)k * NC + h) : 0.0;
+        }
+#pragma unroll
+      for (int r = 0; r < HM; ++r) {
+        const int h = warp + r * NW;
+        double t = 0;
+#pragma unroll
+        for (int m = 0; m < KM; ++m)
+          if (lane + 32 * m < G) t += vals[r][m];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+        if (lane == 0 && h < NC) s_tot[h] = t;
+      }
+      __syncthreads();
+      int h = 0;
+#pragma unroll
+      for (int lev = 0; lev < LV; ++lev) {
+        lam = lamc[h];
+        if (s_tot[h] / (double)N > vf) {
+          l1 = lam;
+          h = 2 * h + 2;
+        } else {
+          l2 = lam;
+          h = 2 * h + 1;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  double dmax = 0, dsum = 0;
+  if (act) {
+    double* xo = a.xnew + (size_t)b * N;
+    for (int i = lo_i + threadIdx.x; i < hi_i; i += kThreads) {
+      const double xv = xb[i];
+      const double dj = fmax(db[i], 1e-12);
+      double xn = xv * sqrt(dj / lam);
+      xn = fmin(fmax(xn, xv - a.move), xv + a.move);
+      xn = fmin(fmax(xn, a.xmin), 1.0);
+      xo[i] = xn;
+      const double d = fabs(xn - xv);
+      dmax = fmax(dmax, d);
+      dsum += d;
+    }
+  }
+  dmax = block_max(dmax);
+  double v[1] = {dsum};
+  __syncthreads();
+  double* st = a.part + (size_t)gridDim.y * 2 * G * NC;
+  block_sum_store<1>(v, st + ((size_t)b * 2 + 0) * G + g);
+  if (threadIdx.x == 0) st[((size_t)b * 2 + 1) * G + g] = dmax;
+  if (!grid_barrier(a.bar, a.bar + 1, nblocks, a.err, a.poll_limit)) return;
+  if (act && g == 0 && threadIdx.x == 0) {
+    double m = 0, t = 0;
+    for (int k = 0; k < G; ++k) {
+      t += __ldcg(st + ((size_t)b * 2 + 0) * G + k);
+      m = fmax(m, __ldcg(st + ((size_t)b * 2 + 1) * G + k));
     }
     a.stats[2 * b] = m;
     a.stats[2 * b + 1] = t / (double)N;

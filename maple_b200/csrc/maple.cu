@@ -1645,9 +1645,10 @@ static void homogenize(maple_ctx* c, int phys, cudaStream_t s) {
   const int N = nodes(c->n[0]);
   const unsigned nb = nblk(N);
   if (phys == MAPLE_ELASTIC) {
-    KL(c, s, k_homogenize<3, 6><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, LN(c).part, c->n[0], p.kscale,
-                                                        p.xscale, c->active));
-    reduce<21>(c, LN(c).part, nb, LN(c).red, s);
+    const unsigned nbe = (unsigned)ceil_div(N, 32 * kHomGroups);
+    KL(c, s, k_homogenize_elastic<<<dim3(nbe, c->B), 32 * kHomWarps, 0, s>>>(p.u64, p.o64.rho, p.energy, LN(c).part,
+                                                                            c->n[0], p.kscale, p.xscale, c->active));
+    reduce<21>(c, LN(c).part, nbe, LN(c).red, s);
     KL(c, s, k_unpack_sym<<<nblk(c->B), kThreads, 0, s>>>(LN(c).red, p.H, c->B, 6));
   } else {
     KL(c, s, k_homogenize<1, 3><<<g2(N, c->B), kThreads, 0, s>>>(p.u64, p.o64.rho, p.energy, LN(c).part, c->n[0], p.kscale,
@@ -1664,11 +1665,18 @@ static void homogenize(maple_ctx* c, int phys, cudaStream_t s) {
 static thread_local long long tl_wait_polls = kBarrierPolls;
 static thread_local unsigned tl_wait_phantom = 0;
 
+// The context's OC update resolves four bisection steps per grid barrier
+// (k_oc_update_tree: lambda and x as k_oc_update to rounding, 16 barriers instead
+// of 61); the allocation-free entry point keeps k_oc_update and its scratch
+// layout.
+constexpr int kOcLevels = 4;
+constexpr int kOcPartPerBlock = 2 * ((1 << kOcLevels) - 1) + 2;  // doubles per (cell, block)
+
 static void oc_update(maple_ctx* c, const double* x, const double* dJ, const double* vf, double move, double xmin,
                       double* xnew, double* stats, cudaStream_t s) {
   const int N = nodes(c->n[0]);
   int per_sm = 0, sms = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oc_update, kThreads, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oc_update_tree<kOcLevels>, kThreads, 0));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
   const int maxres = per_sm * sms;
   require(maxres >= 1, "OC kernel cannot be resident");
@@ -1680,7 +1688,7 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
   CK(cudaMemsetAsync(c->err, 0, sizeof(int), s));
   for (int c0 = 0; c0 < c->B; c0 += cells_per_launch) {
     const int nb = std::min(cells_per_launch, c->B - c0);
-    const int G = std::max(1, std::min(want_G, maxres / nb));
+    const int G = std::max(1, std::min({want_G, maxres / nb, kOcMaxG}));
     OcArgs a{};
     a.x = x + (size_t)c0 * N;
     a.dJ = dJ + (size_t)c0 * N;
@@ -1700,7 +1708,7 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
     CK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned), s));
     void* args[] = {&a};
     prof_begin(c, s);
-    CK(cudaLaunchCooperativeKernel((void*)k_oc_update, dim3(G, nb), dim3(kThreads), args, 0, s));
+    CK(cudaLaunchCooperativeKernel((void*)k_oc_update_tree<kOcLevels>, dim3(G, nb), dim3(kThreads), args, 0, s));
     g_launches.fetch_add(1);
     prof_end(c, s, "k_oc_update", 0);
   }
@@ -1917,7 +1925,7 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
       c->ocvf = dnew<double>(c, B);
       int sms = 0;
       CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
-      c->ocpart = dnew<double>(c, (size_t)4 * std::max(B, 1) * std::max(sms, 1) * 8);
+      c->ocpart = dnew<double>(c, (size_t)kOcPartPerBlock * std::max(B, 1) * std::max(sms, 1) * 8);
       c->bar = dnew<unsigned>(c, 2);
       c->err = dnew<int>(c, 1);
       CK(cudaMemset(c->err, 0, sizeof(int)));
