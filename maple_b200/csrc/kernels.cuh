@@ -3091,6 +3091,7 @@ struct OcArgs {
   const int* active;
   long long poll_limit;  // grid_barrier poll limit
   unsigned phantom;      // extra blocks the barrier waits for (0; more only to test the bounded wait)
+  int cache_chunk;       // k_oc_update_tree: elements per block its dynamic shared memory caches (0: none)
 };
 
 __global__ void __launch_bounds__(kThreads) k_oc_update(OcArgs a) {
@@ -3196,7 +3197,20 @@ __global__ void __launch_bounds__(kThreads) k_oc_update_tree(OcArgs a) {
   const double* db = a.dJ + (size_t)b * N;
   const double vf = act ? a.volfrac[b] : 0.0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __shared__ double s_tot[NC];
+  __shared__ double s_tot[NC], s_rl[NC];
+  // the block's x sqrt(dJ) and move bounds, formed once when the dynamic
+  // shared memory holds them (3 doubles per element of the chunk)
+  extern __shared__ double s_oc[];
+  const bool cached = a.cache_chunk >= chunk;
+  if (cached && act)
+    for (int i = lo_i + threadIdx.x; i < hi_i; i += kThreads) {
+      const double xv = xb[i];
+      const int j = i - lo_i;
+      s_oc[3 * j] = xv * sqrt(fmax(db[i], 1e-12));
+      s_oc[3 * j + 1] = fmax(xv - a.move, a.xmin);
+      s_oc[3 * j + 2] = fmin(xv + a.move, 1.0);
+    }
+  __syncthreads();
   double l1 = 1e-12, l2 = 1e6, lam = 0;
   for (int pass = 0; pass < 60 / LV; ++pass) {
     double lamc[NC];
@@ -3221,17 +3235,35 @@ __global__ void __launch_bounds__(kThreads) k_oc_update_tree(OcArgs a) {
     // volumes differ from k_oc_update's by rounding, which can only change a
     // branch whose volume is within rounding of vf, i.e. at a midpoint within
     // rounding of the root, so lambda agrees to rounding.
+    // 1 / sqrt(lambda) of the candidates, formed once per block
+    if (threadIdx.x < NC) {
+      double m = lamc[0];
+#pragma unroll
+      for (int h = 1; h < NC; ++h)
+        if (threadIdx.x == h) m = lamc[h];
+      s_rl[threadIdx.x] = 1.0 / sqrt(m);
+    }
+    __syncthreads();
     double rl[NC], sc[NC];
 #pragma unroll
     for (int h = 0; h < NC; ++h) {
-      rl[h] = 1.0 / sqrt(lamc[h]);
+      rl[h] = s_rl[h];
       sc[h] = 0;
     }
     if (act) {
       for (int i = lo_i + threadIdx.x; i < hi_i; i += kThreads) {
-        const double xv = xb[i];
-        const double xs = xv * sqrt(fmax(db[i], 1e-12));
-        const double lo = fmax(xv - a.move, a.xmin), hi = fmin(xv + a.move, 1.0);
+        double xs, lo, hi;
+        if (cached) {
+          const int j = i - lo_i;
+          xs = s_oc[3 * j];
+          lo = s_oc[3 * j + 1];
+          hi = s_oc[3 * j + 2];
+        } else {
+          const double xv = xb[i];
+          xs = xv * sqrt(fmax(db[i], 1e-12));
+          lo = fmax(xv - a.move, a.xmin);
+          hi = fmin(xv + a.move, 1.0);
+        }
 #pragma unroll
         for (int h = 0; h < NC; ++h) sc[h] += fmin(fmax(xs * rl[h], lo), hi);
       }

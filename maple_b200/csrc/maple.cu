@@ -1671,12 +1671,15 @@ static thread_local unsigned tl_wait_phantom = 0;
 // layout.
 constexpr int kOcLevels = 4;
 constexpr int kOcPartPerBlock = 2 * ((1 << kOcLevels) - 1) + 2;  // doubles per (cell, block)
+constexpr int kOcCacheElems = 2048;                                 // elements per block cached in shared memory
+constexpr size_t kOcCacheBytes = (size_t)3 * kOcCacheElems * sizeof(double);
 
 static void oc_update(maple_ctx* c, const double* x, const double* dJ, const double* vf, double move, double xmin,
                       double* xnew, double* stats, cudaStream_t s) {
   const int N = nodes(c->n[0]);
   int per_sm = 0, sms = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oc_update_tree<kOcLevels>, kThreads, 0));
+  smem_attr(k_oc_update_tree<kOcLevels>, kOcCacheBytes, c->dev);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oc_update_tree<kOcLevels>, kThreads, kOcCacheBytes));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
   const int maxres = per_sm * sms;
   require(maxres >= 1, "OC kernel cannot be resident");
@@ -1705,10 +1708,12 @@ static void oc_update(maple_ctx* c, const double* x, const double* dJ, const dou
     a.active = c->active ? c->active + c0 : nullptr;
     a.poll_limit = tl_wait_polls;
     a.phantom = tl_wait_phantom;
+    a.cache_chunk = kOcCacheElems;
     CK(cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned), s));
     void* args[] = {&a};
     prof_begin(c, s);
-    CK(cudaLaunchCooperativeKernel((void*)k_oc_update_tree<kOcLevels>, dim3(G, nb), dim3(kThreads), args, 0, s));
+    CK(cudaLaunchCooperativeKernel((void*)k_oc_update_tree<kOcLevels>, dim3(G, nb), dim3(kThreads), args,
+                                   kOcCacheBytes, s));
     g_launches.fetch_add(1);
     prof_end(c, s, "k_oc_update", 0);
   }
