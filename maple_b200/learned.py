@@ -4,8 +4,8 @@ A periodic 3-D U-Net maps a cell's element densities (r^3 voxels) to the 21
 fluctuation fields of its solves: 6 elastic load cases x 3 components and 3
 thermal load cases.  Its prediction is handed to the MG-PCG as the initial
 iterate; the solver still runs to the requested tolerance, so the network only
-changes how many iterations that takes (plain MG-PCG is its fallback and the
-judge of its error).  The reference has the hook for this in
+changes how many iterations that takes (plain MG-PCG is its fallback and what
+measures its error).  The reference has the hook for this in
 ``GMGSolver.solve(init_list=...)`` (utils/EBE_GMG.py:648-757, 851-858), which
 its live path never feeds.
 
