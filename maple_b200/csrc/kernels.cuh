@@ -527,7 +527,7 @@ constexpr int fine_min_blocks() {
   return RD == 18 ? (sizeof(T) == 4 ? 4 : 2) : (RD == 3 && sizeof(T) == 8 ? 4 : 6);
 }
 
-template <typename T, int D, int R, int MODE>
+template <typename T, int D, int R, int MODE, bool PDL = false>
 __global__ void __launch_bounds__(kFineThreads, fine_min_blocks<T, R * D>()) k_apply_fine(ApplyArgs<T> a) {
   using G = FineTile<T, R * D>;
   constexpr int RD = R * D;
@@ -535,6 +535,10 @@ __global__ void __launch_bounds__(kFineThreads, fine_min_blocks<T, R * D>()) k_a
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);
   T* srho = su + G::RHO_OFF;
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
   const int b = blockIdx.y;
   if (a.active && !a.active[b]) return;
   const int n = a.n;
@@ -2210,12 +2214,16 @@ struct Vec16<double> {
   static constexpr int n = 2;
 };
 
-template <typename T, int R, int D>
+template <typename T, int R, int D, bool PDL = false>
 __global__ void k_pcg_update_vec(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
                                  const T* __restrict__ q, const double* __restrict__ alpha, double* __restrict__ part,
                                  int N, const int* active) {
   using V = typename Vec16<T>::type;
   constexpr int W = Vec16<T>::n;
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   const int g = blockIdx.x * kThreads + threadIdx.x;
@@ -2250,11 +2258,15 @@ __global__ void k_pcg_update_vec(T* __restrict__ x, T* __restrict__ r, const T* 
   block_sum_store<R>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * R);
 }
 
-template <typename T, int R, int D>
+template <typename T, int R, int D, bool PDL = false>
 __global__ void k_pcg_direction_vec(T* __restrict__ p, const T* __restrict__ z, const double* __restrict__ beta, int N,
                                     const int* active) {
   using V = typename Vec16<T>::type;
   constexpr int W = Vec16<T>::n;
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   const int g = blockIdx.x * kThreads + threadIdx.x;
@@ -2498,8 +2510,12 @@ struct RedOp {
   int* cond_count = nullptr;
 };
 
-template <int K, int OP>
+template <int K, int OP, bool PDL = false>
 __global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* __restrict__ out, RedOp op) {
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
   const int b = blockIdx.x;
   double v[K];
 #pragma unroll

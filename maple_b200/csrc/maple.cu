@@ -431,8 +431,13 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
     a.rho = o.rho;
     using G = FineTile<T, R * D>;
     smem_attr(k_apply_fine<T, D, R, MODE>, G::BYTES, c->dev);
+    smem_attr(k_apply_fine<T, D, R, MODE, true>, G::BYTES, c->dev);
     prof_begin(c, s);
-    k_apply_fine<T, D, R, MODE><<<dim3(fine_tiles(a.n), c->B), kFineThreads, G::BYTES, s>>>(a);
+    const dim3 grid(fine_tiles(a.n), c->B);
+    if (use_pdl(c, grid) && !prof_on(c))
+      launch_pdl(k_apply_fine<T, D, R, MODE, true>, grid, dim3(kFineThreads), G::BYTES, s, a);
+    else
+      k_apply_fine<T, D, R, MODE><<<grid, kFineThreads, G::BYTES, s>>>(a);
     CKL();
     if (prof_on(c)) {
       static const char* mname[] = {"MV", "RES", "CHEB", "JAC0", "POWER"};
@@ -508,7 +513,10 @@ static void reduce(maple_ctx* c, const double* part, unsigned nb, double* out, c
 // reduce a cell's partial sums and apply the PCG scalar step OP in one launch
 template <int K, int OP>
 static void reduce_op(maple_ctx* c, const double* part, unsigned nb, double* out, const RedOp& op, cudaStream_t s) {
-  KL(c, s, k_reduce_op<K, OP><<<c->B, kThreads, 0, s>>>(part, (int)nb, out, op));
+  if (use_pdl(c, dim3(c->B)))
+    KL(c, s, launch_pdl(k_reduce_op<K, OP, true>, dim3(c->B), dim3(kThreads), 0, s, part, (int)nb, out, op));
+  else
+    KL(c, s, k_reduce_op<K, OP><<<c->B, kThreads, 0, s>>>(part, (int)nb, out, op));
 }
 
 // ---------------------------------------------------------------------------
@@ -983,7 +991,12 @@ static unsigned pcg_update(maple_ctx* c, T* x, T* r, const T* p, const T* q, con
   constexpr int W = Vec16<T>::n;
   if (N % W == 0 && al16(x) && al16(r) && al16(p) && al16(q)) {
     const unsigned nb = nblk((size_t)(N / W));
-    KL(c, s, k_pcg_update_vec<T, R, D><<<dim3(nb, B), kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run));
+    const dim3 grid(nb, B);
+    if (use_pdl(c, grid))
+      KL(c, s, launch_pdl(k_pcg_update_vec<T, R, D, true>, grid, dim3(kThreads), 0, s, x, r, p, q, alpha, part, N,
+                          run));
+    else
+      KL(c, s, k_pcg_update_vec<T, R, D><<<grid, kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run));
     return nb;
   }
   KL(c, s, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run));
@@ -995,9 +1008,13 @@ template <typename T, int R, int D>
 static void pcg_direction(maple_ctx* c, T* p, const T* z, const double* beta, int N, int B, const int* run,
                           cudaStream_t s) {
   constexpr int W = Vec16<T>::n;
-  if (N % W == 0 && al16(p) && al16(z))
-    KL(c, s, k_pcg_direction_vec<T, R, D><<<dim3(nblk((size_t)(N / W)), B), kThreads, 0, s>>>(p, z, beta, N, run));
-  else
+  if (N % W == 0 && al16(p) && al16(z)) {
+    const dim3 grid(nblk((size_t)(N / W)), B);
+    if (use_pdl(c, grid))
+      KL(c, s, launch_pdl(k_pcg_direction_vec<T, R, D, true>, grid, dim3(kThreads), 0, s, p, z, beta, N, run));
+    else
+      KL(c, s, k_pcg_direction_vec<T, R, D><<<grid, kThreads, 0, s>>>(p, z, beta, N, run));
+  } else
     KL(c, s, k_pcg_direction<T, R, D><<<g2(N, B), kThreads, 0, s>>>(p, z, beta, N, run));
 }
 
