@@ -84,10 +84,14 @@ def test_conv3d_tensor_core_tiles_match_torch(lib, n, cin, cout, pad, B):
 
 
 @pytest.mark.parametrize("n,cin,cout,k,B", [(8, 8, 32, 3, 2), (4, 96, 128, 3, 3), (8, 32, 21, 1, 2),
-                                             (4, 21, 32, 3, 2), (16, 64, 64, 3, 1)])
+                                             (4, 21, 32, 3, 2), (16, 64, 64, 3, 1), (4, 16, 264, 3, 1),
+                                             (8, 32, 32, 1, 2), (6, 40, 72, 3, 2)])
 def test_conv3d_gradients_match_autograd(lib, n, cin, cout, k, B):
     """Weight, bias and data gradients (the data gradient is the forward
-    kernel with flipped, transposed weights)."""
+    kernel with flipped, transposed weights).  Channel counts that are
+    multiples of 8 take the tcgen05 weight gradient (rows tap x cin + ci in
+    128-row tiles, a second output tile for cout 264, one tap for k 1, an odd
+    grid), the others the warp-level kernel; its pipeline waits all complete."""
     from maple_b200 import _lib
     g = torch.Generator().manual_seed(7 * n + cin)
     taps = 27 if k == 3 else 1
@@ -111,6 +115,9 @@ def test_conv3d_gradients_match_autograd(lib, n, cin, cout, k, B):
     assert _rel(dW, Wr.grad) < 1e-5
     assert _rel(db, br.grad) < 1e-5
     assert _rel(gx, xr.grad) < 1e-5
+    flag = C.c_int(-1)
+    _lib.nn_call("maple_nn_wait_status", C.byref(flag), _s())
+    assert flag.value == 0
 
 
 def test_resampling_and_adjoints(lib):
@@ -502,3 +509,32 @@ def test_prolonged_guess_equals_coarse_prediction_at_coarse_nodes(lib):
     assert torch.equal(at_coarse(ut_f, 3), ut_c.reshape(B, 3, -1))
     with pytest.raises(ValueError):
         net.predict_prolonged(rf, rc * s + 1)
+
+
+@pytest.mark.parametrize("nc,factor", [(4, 2), (4, 4), (3, 3)])
+def test_field_prolongation_and_density_restriction_match_numpy(lib, nc, factor):
+    """The 128^3 guess path (config 4): periodic trilinear prolongation of
+    nodal fields and the block average of element densities, against plain
+    numpy restatements (node and element id x n^2 + y n + z)."""
+    from maple_b200 import _lib
+    rng = np.random.default_rng(nc * 10 + factor)
+    nf, BF = nc * factor, 3
+    uc = rng.standard_normal((BF, nc, nc, nc))
+    # 1-D periodic linear interpolation matrix, applied along each axis
+    P = np.zeros((nf, nc))
+    for X in range(nf):
+        i0, t = X // factor, (X % factor) / factor
+        P[X, i0] += 1.0 - t
+        P[X, (i0 + 1) % nc] += t
+    ref = np.einsum("ai,bj,ck,fijk->fabc", P, P, P, uc).reshape(BF, -1)
+    d_uc = torch.tensor(uc.reshape(BF, -1), dtype=torch.float64, device=DEV)
+    d_uf = torch.empty((BF, nf ** 3), dtype=torch.float64, device=DEV)
+    _lib.nn_call("maple_nn_prolong_fields", _p(d_uc), _p(d_uf), BF, nc, factor, _s())
+    assert np.abs(d_uf.cpu().numpy() - ref).max() < 1e-14
+    B = 2
+    rf = rng.uniform(1e-3, 1.0, (B, nf, nf, nf))
+    refc = rf.reshape(B, nc, factor, nc, factor, nc, factor).mean(axis=(2, 4, 6)).reshape(B, -1)
+    d_rf = torch.tensor(rf.reshape(B, -1), dtype=torch.float64, device=DEV)
+    d_rc = torch.empty((B, nc ** 3), dtype=torch.float64, device=DEV)
+    _lib.nn_call("maple_nn_restrict_density", _p(d_rf), _p(d_rc), B, nc, factor, _s())
+    assert np.abs(d_rc.cpu().numpy() - refc).max() < 1e-14
