@@ -44,6 +44,27 @@ __device__ __forceinline__ int neighbour(int v, int n, int dx, int dy, int dz) {
   return (wrapc(x + dx, n) * n + wrapc(y + dy, n)) * n + wrapc(z + dz, n);
 }
 
+// q = v / n and r = v % n for 0 <= v < 2^24 with rn = 1/n (float): one
+// multiply and a correction instead of an integer division by a runtime value
+__device__ __forceinline__ void divmod_n(int v, int n, float rn, int& q, int& r) {
+  q = __float2int_rz((float)v * rn);
+  r = v - q * n;
+  if (r < 0) {
+    --q;
+    r += n;
+  } else if (r >= n) {
+    ++q;
+    r -= n;
+  }
+}
+
+// coordinates of node v (id x n^2 + y n + z)
+__device__ __forceinline__ void node_xyz(int v, int n, float rn, int& x, int& y, int& z) {
+  int t;
+  divmod_n(v, n, rn, t, z);
+  divmod_n(t, n, rn, x, y);
+}
+
 // neighbour with zero padding outside the grid: -1 there
 __device__ __forceinline__ int neighbour_zp(int v, int n, int dx, int dy, int dz) {
   const int z = v % n + dz, y = (v / n) % n + dy, x = v / (n * n) + dx;
@@ -224,8 +245,12 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
   const uint32_t sbo_a = (uint32_t)KB * 128, sbo_b = (uint32_t)KC * 16;
   const int m = tid;  // this thread's A row
   const int v = v0 + m;
+  // the row's coordinates, once (the taps only shift them)
+  int vx = 0, vy = 0, vz = 0;
+  if (v < N) node_xyz(v, n, 1.0f / (float)n, vx, vy, vz);
   int issued = 0;     // MMA steps issued (thread 0)
   bool timed_out = false;
+  int tap = 0, chunk = 0;  // step t = tap * kc + chunk
   for (int t = 0; t <= KS; ++t) {
     if (t < KS) {
       const int st = t % TC_STAGES;
@@ -238,11 +263,18 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
       }
       uint8_t* sA = tc_smem + st * stage;
       uint8_t* sB = sA + TC_BM * KC * 2;
-      const int tap = t / kc, c0 = (t - tap * kc) * KC;
+      const int c0 = chunk * KC;
       int dx, dy, dz;
       tap_offsets(tap, taps, dx, dy, dz);
       int q = -1;
-      if (v < N) q = zero_pad ? neighbour_zp(v, n, dx, dy, dz) : neighbour(v, n, dx, dy, dz);
+      if (v < N) {
+        int x = vx + dx, y = vy + dy, z = vz + dz;
+        if (zero_pad) {
+          if (x >= 0 && x < n && y >= 0 && y < n && z >= 0 && z < n) q = (x * n + y) * n + z;
+        } else {
+          q = (wrapc(x, n) * n + wrapc(y, n)) * n + wrapc(z, n);
+        }
+      }
       const bf16* rowp = inb + (size_t)(q < 0 ? 0 : q) * cin + c0;
       for (int h = 0; h < KB; ++h) {
         const bool ok = q >= 0 && c0 + 8 * h < cin;
@@ -265,6 +297,10 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
           if (ci < cin && co < cout) val = W[((size_t)tap * cin + ci) * cout + co];
           *reinterpret_cast<bf16*>(sB + mnmajor_offset(j, k, 128, sbo_b)) = val;
         }
+      }
+      if (++chunk == kc) {
+        chunk = 0;
+        ++tap;
       }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -333,7 +369,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3d_tc(const bf16* __restrict
 // four 16-pair slabs, and one thread issues the four K = 16 MMAs of the stage
 // into an FP32 accumulator in tensor memory while the next two stages load.
 // The epilogue adds the CTA's partial dW to global memory with FP32 atomics.
-// Waits are bounded as in k_conv3d_tc.  Requires cin % 8 == 0 and cout % 8 == 0.
+// Waits are bounded as in k_conv3d_tc.  Requires cin % 8 == 0, cout % 8 == 0
+// and 64 <= n^3 < 2^24 (a stage's pairs cross at most one cell boundary; the
+// coordinates come from a float reciprocal).
 constexpr int WG_CI = 128;     // dW rows per CTA
 constexpr int WG_KP = 64;      // (cell, voxel) pairs per stage: four MMAs of K = 16
 constexpr int WG_STAGES = 4;   // ring depth; loads run WG_STAGES - 2 stages ahead
@@ -371,6 +409,7 @@ __global__ void __launch_bounds__(WG_THREADS) k_conv3d_wgrad_tc(const bf16* __re
   const long long total = (long long)B * N;
   const long long kbeg = (long long)blockIdx.z * chunk, kend = kbeg + chunk < total ? kbeg + chunk : total;
   const int KS = (int)((kend - kbeg + WG_KP - 1) / WG_KP);
+  const float rn = 1.0f / (float)n;
   if (warp == 0) tmem_alloc(&tslot, ncols);
   if (tid == 0) {
     for (int i = 0; i < WG_STAGES; ++i) mbar_init(&mma_bar[i], 1);
@@ -399,6 +438,9 @@ __global__ void __launch_bounds__(WG_THREADS) k_conv3d_wgrad_tc(const bf16* __re
       uint8_t* sA = wg_smem + st * stage;
       uint8_t* sB = sA + (WG_KP / 16) * slab_a;
       const long long k0 = kbeg + (long long)WG_KP * t;
+      // the stage's first (cell, voxel) pair, once per stage; its 64 pairs
+      // wrap into the next cell at most once (N >= 64)
+      const int b0 = (int)(k0 / N), v0 = (int)(k0 - (long long)b0 * N);
 #pragma unroll
       for (int j = 0; j < WG_KP / 16; ++j) {
         const int k = (tid >> 4) + 16 * j;
@@ -406,9 +448,15 @@ __global__ void __launch_bounds__(WG_THREADS) k_conv3d_wgrad_tc(const bf16* __re
         const bool ok = row_ok && kk < kend;
         const bf16* src = in;
         if (ok) {
-          const long long b = kk / N;
-          const int v = (int)(kk - b * N);
-          src = in + ((size_t)b * N + neighbour(v, n, ox, oy, oz)) * cin + cia;
+          int b = b0, v = v0 + k;
+          if (v >= N) {
+            v -= N;
+            ++b;
+          }
+          int x, y, z;
+          node_xyz(v, n, rn, x, y, z);
+          const int q = (wrapc(x + ox, n) * n + wrapc(y + oy, n)) * n + wrapc(z + oz, n);
+          src = in + ((size_t)b * N + q) * cin + cia;
         }
         cp_async16_zfill(sA + j * slab_a + mnmajor_offset(8 * g, k & 15, 128, 256), src, ok);
       }
@@ -954,7 +1002,7 @@ int maple_nn_conv3d_padded(const void* in, const void* W, const float* bias, con
     if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) != 0) return "input must be 16-byte aligned";
     const int N = n * n * n;
     const int taps = ksize == 3 ? 27 : 1, zp = padding == MAPLE_NN_PAD_ZEROS ? 1 : 0;
-    if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(W) & 15) == 0) {
+    if ((cin % 8) == 0 && (reinterpret_cast<uintptr_t>(W) & 15) == 0 && (long long)n * n * n < (1 << 24)) {
       // tensor-core (tcgen05) implicit GEMM
       const size_t smem = TC_STAGES * tc_stage_bytes(tc_bn(cout), tc_kc(cin));
       static bool attr_set[128] = {};
@@ -1007,7 +1055,7 @@ int maple_nn_conv3d_wgrad(const void* in, const void* dz, float* dW, float* db, 
     if ((cout % 8) == 0 && (reinterpret_cast<uintptr_t>(dz) & 15) != 0) return "gradient must be 16-byte aligned";
     const int N = n * n * n, taps = ksize == 3 ? 27 : 1;
     const long long total = (long long)B * N;
-    if ((cin % 8) == 0 && (cout % 8) == 0) {
+    if ((cin % 8) == 0 && (cout % 8) == 0 && n >= 4 && N < (1 << 24)) {
       // tensor-core (tcgen05) GEMM over the flat (tap, input channel) rows.
       // The reduction is split so that the CTAs fill whole waves of the 148
       // SMs (at the occupancy shared memory allows), each CTA reducing at
