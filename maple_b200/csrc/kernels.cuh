@@ -658,6 +658,80 @@ __global__ void __launch_bounds__(kFineThreads, fine_min_blocks<T, R * D>()) k_a
   }
 }
 
+// Fine-level block-Jacobi inverse, stored once per hierarchy build: for each
+// node the inverse of scale * (its 3x3 (or 1x1) diagonal block), formed from
+// the eight surrounding element densities with the operations k_apply_fine
+// uses for it, so the stored values are the ones it forms on the fly.
+// Layout [cell][D*D][node].
+template <typename T, int D>
+__global__ void k_fine_dinv(const T* __restrict__ rho, T* __restrict__ Dinv, int n, T scale, const int* active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int N = n * n * n;
+  const int id = blockIdx.x * kThreads + threadIdx.x;
+  if (id >= N) return;
+  const int z = id % n, y = (id / n) % n, x = id / (n * n);
+  const T* rb = rho + (size_t)b * N;
+  T rq[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int qx = (q >> 2) & 1, qy = (q >> 1) & 1, qz = q & 1;
+    rq[q] = rb[((size_t)wrapn(x - 1 + qx, n) * n + wrapn(y - 1 + qy, n)) * n + wrapn(z - 1 + qz, n)];
+  }
+  T C0[D][D], C0s[D][D], Di[D][D];
+  fine_block<T, D, 13>(rq, C0);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) C0s[i][j] = scale * C0[i][j];
+  block_inverse<T, D>(C0s, Di);
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) Dinv[((size_t)b * D * D + i * D + j) * N + id] = Di[i][j];
+}
+
+// The first Chebyshev step from zero on the fine level with the stored block
+// inverse: d = beta * Dinv f, u = d (k_apply_fine's M_JAC0 epilogue, without
+// forming the diagonal block again).  A vector kernel: reads f and Dinv,
+// writes u and d.
+template <typename T, int D, int R, bool PDL = false>
+__global__ void __launch_bounds__(kThreads) k_fine_jac0(ApplyArgs<T> a) {
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
+  const int N = a.N;
+  const size_t NN = (size_t)N;
+  const int id = blockIdx.x * kThreads + threadIdx.x;
+  if (id >= N) return;
+  double al, be;
+  cheb_coeffs(a.hi[b], a.ratio, 0, al, be);
+  T Di[D][D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) Di[i][j] = a.Dinv[((size_t)b * D * D + i * D + j) * NN + id];
+  const size_t vo = (size_t)b * N * R * D + id;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    T res[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) res[i] = a.f[vo + (size_t)(r * D + i) * NN];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      T zz = 0;
+#pragma unroll
+      for (int j = 0; j < D; ++j) zz += Di[i][j] * res[j];
+      const T d = T(be) * zz;
+      a.dout[vo + (size_t)(r * D + i) * NN] = d;
+      a.out[vo + (size_t)(r * D + i) * NN] = d;
+    }
+  }
+}
+
 // Coarse levels: one thread per (node, load case) so that the small grids of
 // the deep levels still fill the machine; consecutive threads are consecutive
 // nodes of one load case (coalesced stencil and field loads).

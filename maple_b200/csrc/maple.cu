@@ -110,6 +110,7 @@ struct Ops {
   T* Dd[kMaxLevels] = {};                // Chebyshev direction
   T* Res[kMaxLevels] = {};               // residual
   double* hi[kMaxLevels] = {};           // per-cell Chebyshev upper bound
+  bool dinv0 = false;                    // Dinv[0] holds the fine-level block inverse of the current density
   T *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;  // PCG (level 0)
 };
 
@@ -380,6 +381,7 @@ static void alloc_ops(maple_ctx* c, Phys& p, Ops<T>& o, bool vectors) {
       o.Res[l] = dnew<T>(c, (size_t)B * Nl * RD);
       o.hi[l] = dnew<double>(c, B);
     }
+    o.Dinv[0] = dnew<T>(c, (size_t)B * N0 * DD);  // fine-level block inverse (k_fine_dinv)
     o.x = dnew<T>(c, (size_t)B * N0 * RD);
     o.r = dnew<T>(c, (size_t)B * N0 * RD);
     o.p = dnew<T>(c, (size_t)B * N0 * RD);
@@ -429,6 +431,24 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
   const dim3 g = g2(a.N, c->B);
   if (l == 0) {
     a.rho = o.rho;
+    if constexpr (MODE == M_JAC0) {
+      if (o.dinv0) {
+        a.Dinv = o.Dinv[0];
+        prof_begin(c, s);
+        const dim3 grid(nblk(a.N), c->B);
+        if (use_pdl(c, grid) && !prof_on(c))
+          launch_pdl(k_fine_jac0<T, D, R, true>, grid, dim3(kThreads), 0, s, a);
+        else
+          k_fine_jac0<T, D, R><<<grid, kThreads, 0, s>>>(a);
+        CKL();
+        if (prof_on(c)) {
+          const double bytes = (double)c->B * a.N * ((double)D * D + 3.0 * R * D) * sizeof(T);
+          prof_end(c, s, (std::string("k_fine_jac0<") + (sizeof(T) == 8 ? "f64," : "f32,") + std::to_string(D) +
+                          "," + std::to_string(R) + ">").c_str(), bytes);
+        }
+        return;
+      }
+    }
     using G = FineTile<T, R * D>;
     smem_attr(k_apply_fine<T, D, R, MODE>, G::BYTES, c->dev);
     smem_attr(k_apply_fine<T, D, R, MODE, true>, G::BYTES, c->dev);
@@ -656,6 +676,18 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s, co
       } else {
         KL(c, s, k_chol_inverse<<<B, 512, 0, s>>>(p.Ainv, p.cwork, ndof, D, act, nullptr));
       }
+    }
+  }
+  // the fine level's block inverse, for the first smoothing step
+  {
+    const int n0 = c->n[0];
+    const dim3 g(nblk(nodes(n0)), B);
+    if (prec == MAPLE_FP64) {
+      KL(c, s, k_fine_dinv<double, D><<<g, kThreads, 0, s>>>(p.o64.rho, p.o64.Dinv[0], n0, (double)p.kscale, act));
+      p.o64.dinv0 = true;
+    } else {
+      KL(c, s, k_fine_dinv<float, D><<<g, kThreads, 0, s>>>(p.o32.rho, p.o32.Dinv[0], n0, (float)p.kscale, act));
+      p.o32.dinv0 = true;
     }
   }
   if (prec == MAPLE_FP64)
