@@ -225,6 +225,11 @@ struct maple_ctx {
   } graphs[2][4];  // [physics][FP64 PCG, flexible mixed PCG, FP32 inner PCG of refinement, reliable updates]
   cudaStream_t aux_stream = nullptr;  // second physics of a concurrent OC step
   cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
+  // the elastic solve of a concurrent OC step runs on a stream of the highest
+  // priority: its chain is the longer one, the thermal solve fills the SMs it
+  // leaves free
+  cudaStream_t hi_stream = nullptr;
+  cudaEvent_t hi_fork = nullptr, hi_join = nullptr;
   bool use_graphs = true;
   bool concurrent = true;  // elastic and thermal solves of an OC step on two streams
   int split_min_n = 32;    // coarse levels with n >= this (n % 8 == 0) use k_apply_stencil_split; 0: never
@@ -664,7 +669,9 @@ static void build_hierarchy(maple_ctx* c, int phys, int prec, cudaStream_t s, co
         smem_attr(k_chol_inverse_smem, chol_smem_bytes(kCholSmemMax), c->dev);
         Lane& ln = LN(c);
         if (!ln.side) {
-          CK(cudaStreamCreateWithFlags(&ln.side, cudaStreamNonBlocking));
+          int least = 0, greatest = 0;
+          CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+          CK(cudaStreamCreateWithPriority(&ln.side, cudaStreamNonBlocking, tl_lane == 0 ? greatest : least));
           CK(cudaEventCreateWithFlags(&ln.side_fork, cudaEventDisableTiming));
           CK(cudaEventCreateWithFlags(&ln.side_join, cudaEventDisableTiming));
         }
@@ -1951,11 +1958,15 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
         L.rel = dnew<int>(c, B);
         L.o_t = dnew<double>(c, B * 6);
         CK(cudaEventCreateWithFlags(&L.pw_fork, cudaEventDisableTiming));
+        // the elastic lane's streams take the highest priority (see hi_stream)
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        const int prio = (&L == &c->lanes[0]) ? greatest : least;
         for (int l = 1; l + 1 < c->L; ++l) {
           L.pw_part[l] = dnew<double>(c, (size_t)B * nodes(c->n[l]) * 2);
           L.pw_red[l] = dnew<double>(c, (size_t)B * 2);
           if (l > 1) {
-            CK(cudaStreamCreateWithFlags(&L.pw[l], cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithPriority(&L.pw[l], cudaStreamNonBlocking, prio));
             CK(cudaEventCreateWithFlags(&L.pw_join[l], cudaEventDisableTiming));
           }
         }
@@ -2078,6 +2089,9 @@ int maple_ctx_destroy(maple_ctx* c) {
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     if (c->aux_fork) cudaEventDestroy(c->aux_fork);
     if (c->aux_join) cudaEventDestroy(c->aux_join);
+    if (c->hi_stream) cudaStreamDestroy(c->hi_stream);
+    if (c->hi_fork) cudaEventDestroy(c->hi_fork);
+    if (c->hi_join) cudaEventDestroy(c->hi_join);
     for (void* p : c->allocs) cudaFree(p);
     delete c;
   });
@@ -2724,12 +2738,21 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
     const bool aux_thermal = conc && need_ch && need_k, aux_pen = conc && pen && (need_ch || need_k);
     if (aux_thermal || aux_pen) {
       if (!c->aux_stream) {
-        CK(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&c->aux_stream, cudaStreamNonBlocking, least));
         CK(cudaEventCreateWithFlags(&c->aux_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->aux_join, cudaEventDisableTiming));
+        CK(cudaStreamCreateWithPriority(&c->hi_stream, cudaStreamNonBlocking, greatest));
+        CK(cudaEventCreateWithFlags(&c->hi_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->hi_join, cudaEventDisableTiming));
       }
       CK(cudaEventRecord(c->aux_fork, st));
       CK(cudaStreamWaitEvent(c->aux_stream, c->aux_fork, 0));
+      // the caller's stream hands its work to the high-priority stream and
+      // takes it back after the solves
+      cudaStream_t sm = aux_thermal ? c->hi_stream : st;
+      if (aux_thermal) CK(cudaStreamWaitEvent(c->hi_stream, c->aux_fork, 0));
       std::exception_ptr thermal_err;
       const int dev = c->dev;
       std::thread worker([&] {
@@ -2742,8 +2765,8 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
         }
       });
       try {
-        if (need_ch) run_phys(0, st, it_el.data());
-        if (need_k && !aux_thermal) run_phys(1, st, it_th.data());
+        if (need_ch) run_phys(0, sm, it_el.data());
+        if (need_k && !aux_thermal) run_phys(1, sm, it_th.data());
       } catch (...) {
         worker.join();
         throw;
@@ -2752,6 +2775,10 @@ int maple_oc_step(maple_ctx* c, const double* x, const double* w, const double* 
       if (thermal_err) std::rethrow_exception(thermal_err);
       CK(cudaEventRecord(c->aux_join, c->aux_stream));
       CK(cudaStreamWaitEvent(st, c->aux_join, 0));
+      if (aux_thermal) {
+        CK(cudaEventRecord(c->hi_join, c->hi_stream));
+        CK(cudaStreamWaitEvent(st, c->hi_join, 0));
+      }
     } else {
       if (pen) run_pen(st);
       if (need_ch) run_phys(0, st, it_el.data());
