@@ -200,6 +200,20 @@ __device__ __forceinline__ void cheb_coeffs(double hi, double ratio, int step, d
 // ----------------------------------------------------------------------------
 enum ApplyMode { M_MV = 0, M_RES = 1, M_CHEB = 2, M_JAC0 = 3, M_POWER = 4 };
 
+// 16-byte vector type of T and its width (vectorised vector kernels)
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+
 template <typename T>
 struct ApplyArgs {
   int n, N;
@@ -728,6 +742,53 @@ __global__ void __launch_bounds__(kThreads) k_fine_jac0(ApplyArgs<T> a) {
       const T d = T(be) * zz;
       a.dout[vo + (size_t)(r * D + i) * NN] = d;
       a.out[vo + (size_t)(r * D + i) * NN] = d;
+    }
+  }
+}
+
+// The same on 16-byte vectors: W = 16 / sizeof(T) consecutive nodes per thread
+// (the node count a multiple of W, every array 16-byte aligned).
+template <typename T, int D, int R, bool PDL = false>
+__global__ void __launch_bounds__(kThreads) k_fine_jac0_vec(ApplyArgs<T> a) {
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::n;
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
+  const int b = blockIdx.y;
+  if (a.active && !a.active[b]) return;
+  const int NG = a.N / W;
+  const int g = blockIdx.x * kThreads + threadIdx.x;
+  if (g >= NG) return;
+  double al, be;
+  cheb_coeffs(a.hi[b], a.ratio, 0, al, be);
+  const T tb = T(be);
+  V Di[D][D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+      Di[i][j] = reinterpret_cast<const V*>(a.Dinv)[((size_t)b * D * D + i * D + j) * NG + g];
+  const size_t vo = (size_t)b * NG * R * D + g;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    V res[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) res[i] = reinterpret_cast<const V*>(a.f)[vo + (size_t)(r * D + i) * NG];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      V dv;
+      T* ds = reinterpret_cast<T*>(&dv);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        T zz = 0;
+#pragma unroll
+        for (int j = 0; j < D; ++j) zz += reinterpret_cast<const T*>(&Di[i][j])[k] * reinterpret_cast<const T*>(&res[j])[k];
+        ds[k] = tb * zz;
+      }
+      reinterpret_cast<V*>(a.dout)[vo + (size_t)(r * D + i) * NG] = dv;
+      reinterpret_cast<V*>(a.out)[vo + (size_t)(r * D + i) * NG] = dv;
     }
   }
 }
@@ -2275,18 +2336,6 @@ __global__ void k_pcg_update(T* __restrict__ x, T* __restrict__ r, const T* __re
 // and load): twice to four times the bytes in flight per load instruction, which
 // the FP32 update needs to reach the HBM roofline.  Requires N % W == 0; the
 // partial sums are per block of kThreads vectors.
-template <typename T>
-struct Vec16;
-template <>
-struct Vec16<float> {
-  using type = float4;
-  static constexpr int n = 4;
-};
-template <>
-struct Vec16<double> {
-  using type = double2;
-  static constexpr int n = 2;
-};
 
 template <typename T, int R, int D, bool PDL = false>
 __global__ void k_pcg_update_vec(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,

@@ -359,6 +359,8 @@ static void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
 }
 
 static inline unsigned nblk(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+// 16-byte alignment of a pointer (vector accesses; a caller's buffer may be only element-aligned)
+static inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 static inline dim3 g2(size_t n, int B) { return dim3(nblk(n), (unsigned)B); }
 
 static int nodes(int n) { return n * n * n; }
@@ -440,11 +442,19 @@ static void apply(maple_ctx* c, Phys& p, Ops<T>& o, int l, ApplyArgs<T> a, const
       if (o.dinv0) {
         a.Dinv = o.Dinv[0];
         prof_begin(c, s);
-        const dim3 grid(nblk(a.N), c->B);
-        if (use_pdl(c, grid) && !prof_on(c))
+        constexpr int W = Vec16<T>::n;
+        const bool vec = a.N % W == 0 && al16(a.Dinv) && al16(a.f) && al16(a.out) && al16(a.dout);
+        const dim3 grid(nblk(vec ? a.N / W : a.N), c->B);
+        if (vec) {
+          if (use_pdl(c, grid) && !prof_on(c))
+            launch_pdl(k_fine_jac0_vec<T, D, R, true>, grid, dim3(kThreads), 0, s, a);
+          else
+            k_fine_jac0_vec<T, D, R><<<grid, kThreads, 0, s>>>(a);
+        } else if (use_pdl(c, grid) && !prof_on(c)) {
           launch_pdl(k_fine_jac0<T, D, R, true>, grid, dim3(kThreads), 0, s, a);
-        else
+        } else {
           k_fine_jac0<T, D, R><<<grid, kThreads, 0, s>>>(a);
+        }
         CKL();
         if (prof_on(c)) {
           const double bytes = (double)c->B * a.N * ((double)D * D + 3.0 * R * D) * sizeof(T);
@@ -1019,7 +1029,6 @@ static void drop_graphs(maple_ctx* c) {
     }
 }
 
-static inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // x += alpha p, r -= alpha q with the partial sums of r.r (16-byte vectors
 // when the node count and every pointer allow: a caller's buffer may be only
