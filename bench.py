@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-chs", action="store_true", help="skip the C^H solves/s measurement")
     p.add_argument("--no-autotune", action="store_true",
                    help="config 1: library defaults instead of the autotuner's choice (both arms)")
+    p.add_argument("--mixed-form", default=None, choices=["flexible", "reliable", "refine"],
+                   help="config 1: this mixed-precision form instead of the autotuner's choice (with --no-autotune)")
     p.add_argument("--no-graph-conditionals", action="store_true",
                    help="per-iteration graph replays without conditional nodes (for profilers that do not "
                         "support them); same kernels and results")
@@ -274,6 +276,8 @@ def run_maple(args, rank, world, local_rank):
         c.set_concurrency(not args.serial)
         if settings:
             apply_settings(c, settings)
+        if args.mixed_form and prec == "mixed":
+            c.set_mixed_mode(args.mixed_form)
         if args.no_graph_conditionals:
             c.set_device_loop(False)
         return c, settings
