@@ -2337,49 +2337,6 @@ __global__ void k_pcg_update(T* __restrict__ x, T* __restrict__ r, const T* __re
 // the FP32 update needs to reach the HBM roofline.  Requires N % W == 0; the
 // partial sums are per block of kThreads vectors.
 
-template <typename T, int R, int D, bool PDL = false>
-__global__ void k_pcg_update_vec(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
-                                 const T* __restrict__ q, const double* __restrict__ alpha, double* __restrict__ part,
-                                 int N, const int* active) {
-  using V = typename Vec16<T>::type;
-  constexpr int W = Vec16<T>::n;
-  if constexpr (PDL) {
-    griddep_wait();
-    griddep_launch();
-  }
-  const int b = blockIdx.y;
-  if (active && !active[b]) return;
-  const int g = blockIdx.x * kThreads + threadIdx.x;
-  const int NG = N / W;
-  double v[R] = {};
-  if (g < NG) {
-    const size_t o = (size_t)b * NG * R * D + g;
-#pragma unroll
-    for (int c = 0; c < R; ++c) {
-      const T a = (T)alpha[b * R + c];
-#pragma unroll
-      for (int i = 0; i < D; ++i) {
-        const size_t j = o + (size_t)(c * D + i) * NG;
-        V xv = reinterpret_cast<const V*>(x)[j], rv = reinterpret_cast<const V*>(r)[j];
-        const V pv = reinterpret_cast<const V*>(p)[j], qv = reinterpret_cast<const V*>(q)[j];
-        T* xs = reinterpret_cast<T*>(&xv);
-        T* rs = reinterpret_cast<T*>(&rv);
-        const T* ps = reinterpret_cast<const T*>(&pv);
-        const T* qs = reinterpret_cast<const T*>(&qv);
-#pragma unroll
-        for (int k = 0; k < W; ++k) {
-          xs[k] += a * ps[k];
-          const T rn = rs[k] - a * qs[k];
-          rs[k] = rn;
-          v[c] += (double)rn * (double)rn;
-        }
-        reinterpret_cast<V*>(x)[j] = xv;
-        reinterpret_cast<V*>(r)[j] = rv;
-      }
-    }
-  }
-  block_sum_store<R>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * R);
-}
 
 template <typename T, int R, int D, bool PDL = false>
 __global__ void k_pcg_direction_vec(T* __restrict__ p, const T* __restrict__ z, const double* __restrict__ beta, int N,
@@ -2633,20 +2590,19 @@ struct RedOp {
   int* cond_count = nullptr;
 };
 
-template <int K, int OP, bool PDL = false>
-__global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* __restrict__ out, RedOp op) {
-  if constexpr (PDL) {
-    griddep_wait();
-    griddep_launch();
-  }
-  const int b = blockIdx.x;
+// The body of k_reduce_op for cell b, run by a whole block of kThreads
+// threads (the partials are read through L2: the last block of the grid that
+// wrote them may run it, see k_pcg_update_vec).
+template <int K, int OP>
+__device__ __forceinline__ void reduce_op_cell(const double* __restrict__ part, int nblk, double* __restrict__ out,
+                                               RedOp& op, int b) {
   double v[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) v[k] = 0;
   for (int i = threadIdx.x; i < nblk; i += kThreads) {
     const double* p = part + ((size_t)b * nblk + i) * K;
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] += p[k];
+    for (int k = 0; k < K; ++k) v[k] += __ldcg(p + k);
   }
   block_sum_store<K>(v, out + (size_t)b * K);
   if constexpr (OP == RED_PLAIN) return;
@@ -2754,6 +2710,83 @@ __global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* _
     }
   }
 }
+
+template <int K, int OP, bool PDL = false>
+__global__ void k_reduce_op(const double* __restrict__ part, int nblk, double* __restrict__ out, RedOp op) {
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
+  reduce_op_cell<K, OP>(part, nblk, out, op, blockIdx.x);
+}
+
+// FIN (RED_CHECK or RED_RELCHECK; 0: none): the last block of a cell to
+// finish runs that reduction of the cell's partial sums itself (the block
+// count and summation order of k_reduce_op), so the step needs no separate
+// reduction launch; fin_count[cell] counts the finished blocks and is reset
+// by the last one.
+template <typename T, int R, int D, bool PDL = false, int FIN = 0>
+__global__ void k_pcg_update_vec(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                                 const T* __restrict__ q, const double* __restrict__ alpha, double* __restrict__ part,
+                                 int N, const int* active, unsigned* fin_count, double* fin_out, RedOp fin_op) {
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::n;
+  if constexpr (PDL) {
+    griddep_wait();
+    griddep_launch();
+  }
+  const int b = blockIdx.y;
+  if (active && !active[b]) {
+    // a finished or inactive cell: what the reduction would have left it
+    if constexpr (FIN == RED_RELCHECK) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) fin_op.rel[b] = 0;
+    }
+    return;
+  }
+  const int g = blockIdx.x * kThreads + threadIdx.x;
+  const int NG = N / W;
+  double v[R] = {};
+  if (g < NG) {
+    const size_t o = (size_t)b * NG * R * D + g;
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      const T a = (T)alpha[b * R + c];
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const size_t j = o + (size_t)(c * D + i) * NG;
+        V xv = reinterpret_cast<const V*>(x)[j], rv = reinterpret_cast<const V*>(r)[j];
+        const V pv = reinterpret_cast<const V*>(p)[j], qv = reinterpret_cast<const V*>(q)[j];
+        T* xs = reinterpret_cast<T*>(&xv);
+        T* rs = reinterpret_cast<T*>(&rv);
+        const T* ps = reinterpret_cast<const T*>(&pv);
+        const T* qs = reinterpret_cast<const T*>(&qv);
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          xs[k] += a * ps[k];
+          const T rn = rs[k] - a * qs[k];
+          rs[k] = rn;
+          v[c] += (double)rn * (double)rn;
+        }
+        reinterpret_cast<V*>(x)[j] = xv;
+        reinterpret_cast<V*>(r)[j] = rv;
+      }
+    }
+  }
+  block_sum_store<R>(v, part + ((size_t)b * gridDim.x + blockIdx.x) * R);
+  if constexpr (FIN != 0) {
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(fin_count + b, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      reduce_op_cell<R, FIN>(part, gridDim.x, fin_out, fin_op, b);
+      if (threadIdx.x == 0) fin_count[b] = 0;
+    }
+  }
+}
+
 
 // deterministic pseudo-random start vector for power iterations
 template <typename T>

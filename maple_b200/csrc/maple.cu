@@ -165,6 +165,7 @@ struct Lane {
   int *o_done = nullptr, *o_run = nullptr;
   int* o_live = nullptr;   // refinement: cells still refined (active, not broken down)
   int* rel = nullptr;      // reliable updates: per cell, a residual replacement is due
+  unsigned* fin_count = nullptr;  // per cell: blocks of a fused update-and-reduce launch that finished
   double* o_t = nullptr;   // reliable updates: per (cell, rhs) rescaling of the direction
   int* h_flags = nullptr;  // pinned host [B + 2]: convergence flags, the device loop's count, IF executions
   int* loop = nullptr;     // device [3]: iterations run by the device-side loop, its limit, IF-node executions
@@ -237,6 +238,7 @@ struct maple_ctx {
   bool tail_fused = true;  // FP32 8^3 level + 4^3 coarsest solve as one cluster launch (k_tail_cycle)
   bool pdl = true;         // coarse-level launches with programmatic dependent launch
   bool device_loop = true; // conditional graph nodes: PCG iterations looped on device, IF node of the replacement
+  bool fused_reduce = true; // the PCG update's last block per cell runs the convergence reduction
   int sym_kind = 0, sym_mask = 0;  // symmetry projection of the OC step (SYM_*)
   // manufacturability penalties of the OC objective (maple_set_penalties)
   double lambda_print = 0, lambda_cavity = 0;
@@ -1040,15 +1042,40 @@ static unsigned pcg_update(maple_ctx* c, T* x, T* r, const T* p, const T* q, con
   if (N % W == 0 && al16(x) && al16(r) && al16(p) && al16(q)) {
     const unsigned nb = nblk((size_t)(N / W));
     const dim3 grid(nb, B);
+    const RedOp none{};
     if (use_pdl(c, grid))
       KL(c, s, launch_pdl(k_pcg_update_vec<T, R, D, true>, grid, dim3(kThreads), 0, s, x, r, p, q, alpha, part, N,
-                          run));
+                          run, (unsigned*)nullptr, (double*)nullptr, none));
     else
-      KL(c, s, k_pcg_update_vec<T, R, D><<<grid, kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run));
+      KL(c, s, k_pcg_update_vec<T, R, D><<<grid, kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run, nullptr, nullptr,
+                                                                   none));
     return nb;
   }
   KL(c, s, k_pcg_update<T, R, D><<<g2(N, B), kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run));
   return nblk(N);
+}
+
+// The update followed by the reduction OP of its partial sums (RED_CHECK or
+// RED_RELCHECK into out): with the vector kernel, its last block per cell runs
+// the reduction (one launch instead of two); otherwise the separate launch.
+template <typename T, int R, int D, int OP>
+static void pcg_update_reduce(maple_ctx* c, T* x, T* r, const T* p, const T* q, const double* alpha, double* part,
+                              int N, int B, const int* run, double* out, const RedOp& op, cudaStream_t s) {
+  constexpr int W = Vec16<T>::n;
+  if (c->fused_reduce && N % W == 0 && al16(x) && al16(r) && al16(p) && al16(q)) {
+    const unsigned nb = nblk((size_t)(N / W));
+    const dim3 grid(nb, B);
+    unsigned* cnt = LN(c).fin_count;
+    if (use_pdl(c, grid))
+      KL(c, s, launch_pdl(k_pcg_update_vec<T, R, D, true, OP>, grid, dim3(kThreads), 0, s, x, r, p, q, alpha, part, N,
+                          run, cnt, out, op));
+    else
+      KL(c, s, k_pcg_update_vec<T, R, D, false, OP><<<grid, kThreads, 0, s>>>(x, r, p, q, alpha, part, N, run, cnt,
+                                                                              out, op));
+    return;
+  }
+  const unsigned nbu = pcg_update<T, R, D>(c, x, r, p, q, alpha, part, N, B, run, s);
+  reduce_op<R, OP>(c, part, nbu, out, op, s);
 }
 
 // p = z + beta p
@@ -1116,8 +1143,7 @@ static void pcg(maple_ctx* c, Phys& p, Ops<T>& o, const T* b, bool x_zero, doubl
       apply<T, D, R, M_MV>(c, p, o, 0, a, run, st);
     }
     reduce_op<R, RED_ALPHA>(c, LN(c).part, nbf, sc.pq, op, st);
-    const unsigned nbu = pcg_update<T, R, D>(c, o.x, o.r, o.p, o.q, sc.alpha, LN(c).part, N, B, run, st);
-    reduce_op<R, RED_CHECK>(c, LN(c).part, nbu, sc.rr, op, st);
+    pcg_update_reduce<T, R, D, RED_CHECK>(c, o.x, o.r, o.p, o.q, sc.alpha, LN(c).part, N, B, run, sc.rr, op, st);
     vcycle<T, D, R>(c, p, o, 0, o.r, run, LN(c).part, st);
     reduce_op<R, RED_BETA>(c, LN(c).part, nbf, sc.rz_new, op, st);
     pcg_direction<T, R, D>(c, o.p, o.U[0][1], sc.beta, N, B, run, st);
@@ -1195,8 +1221,7 @@ static void pcg_mixed(maple_ctx* c, Phys& p, const double* b, double* x, bool x_
       apply<double, D, R, M_MV>(c, p, o64, 0, a, run, st);
     }
     reduce_op<R, RED_ALPHA>(c, LN(c).part, nbf, sc.pq, op, st);
-    const unsigned nbu = pcg_update<double, R, D>(c, x, r, pv, q, sc.alpha, LN(c).part, N, B, run, st);
-    reduce_op<R, RED_CHECK>(c, LN(c).part, nbu, sc.rr, op, st);
+    pcg_update_reduce<double, R, D, RED_CHECK>(c, x, r, pv, q, sc.alpha, LN(c).part, N, B, run, sc.rr, op, st);
     precondition_f32<D, R>(c, p, r, q, run, op, st);
     KL(c, st, k_pcg_direction_f32<R, D, false><<<g2(N, B), kThreads, 0, st>>>(pv, z32, LN(c).o_inv, sc.beta, N, run));
   };
@@ -1290,8 +1315,7 @@ static void pcg_reliable(maple_ctx* c, Phys& p, const double* b, double* x, bool
       apply<float, D, R, M_MV>(c, p, o, 0, a, run, st);
     }
     reduce_op<R, RED_ALPHA>(c, ln.part, nbf, sc.pq, opc, st);
-    const unsigned nbu = pcg_update<float, R, D>(c, o.x, o.r, o.p, o.q, sc.alpha, ln.part, N, B, run, st);
-    reduce_op<R, RED_RELCHECK>(c, ln.part, nbu, sc.rr, opc, st);
+    pcg_update_reduce<float, R, D, RED_RELCHECK>(c, o.x, o.r, o.p, o.q, sc.alpha, ln.part, N, B, run, sc.rr, opc, st);
     // residual replacement of the flagged cells (every launch skips the others)
     auto replace = [&](cudaStream_t sr, bool in_if) {
       KL(c, sr, k_flush_f32<R, D><<<g2(N, B), kThreads, 0, sr>>>(x, o.x, ln.o_inv, N, ln.rel));
@@ -1965,6 +1989,8 @@ int maple_ctx_create(int r, int ncells, int levels, double E, double nu, double 
         L.o_run = dnew<int>(c, B);
         L.o_live = dnew<int>(c, B);
         L.rel = dnew<int>(c, B);
+        L.fin_count = dnew<unsigned>(c, B);
+        CK(cudaMemset(L.fin_count, 0, B * sizeof(unsigned)));
         L.o_t = dnew<double>(c, B * 6);
         CK(cudaEventCreateWithFlags(&L.pw_fork, cudaEventDisableTiming));
         // the elastic lane's streams take the highest priority (see hi_stream)
